@@ -1,0 +1,213 @@
+/*
+ * prolix_b200 C ABI: a B200 (sm_100a) implementation of prolix's
+ * implicit-solvent (OBC2 GBSA) energy/force function and its BAOAB Langevin
+ * integrator, batched over many systems of uneven size.
+ *
+ * Conventions
+ *  - Every entry point returns an int status: PB2_OK (0) or a negative
+ *    PB2_E* code; pb2_last_error() describes the most recent failure of the
+ *    context.  No C++ exception crosses this boundary.
+ *  - Units are AKMA, as in prolix (src/prolix/simulate.py:52-57, 770-772):
+ *    A, kcal/mol, e, amu, time in tau = 48.88821291839 fs.
+ *  - Host arrays are read only during the call.  Device state is owned by
+ *    the batch handle.  All GPU work is issued on the stream passed in
+ *    (NULL = the legacy default stream); calls that return host data
+ *    synchronise that stream.
+ *  - A context is used by one host thread at a time.
+ *
+ * Reference interfaces replaced (paths within maraxen/prolix):
+ *  - make_energy_fn(..., implicit_solvent=True)   src/prolix/physics/system.py:29-271
+ *  - -jax.grad of that energy / single_padded_force src/prolix/batched_energy.py:730-850
+ *  - nvt_langevin / langevin_with_constraints init_fn, apply_fn
+ *                                                  src/prolix/physics/settle.py:1637-1746
+ *  - batched BAOAB step over many systems          src/prolix/batched_simulate.py:218-382
+ *  - neighbour list allocate/update, skin rebuild  src/prolix/physics/neighbor_list.py:155-172,
+ *                                                  src/prolix/batched_simulate.py:1524-1640
+ * The reference has no compiled FFI of its own; these functions are what a
+ * jax.ffi custom-call registration (or the ctypes binding in
+ * prolix_b200/_lib.py) binds.
+ */
+#ifndef PROLIX_B200_H
+#define PROLIX_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PB2_ABI_VERSION 1
+
+/* status codes */
+#define PB2_OK 0
+#define PB2_EINVAL (-1)      /* bad argument */
+#define PB2_ENOMEM (-2)      /* device or host allocation failed */
+#define PB2_ECUDA (-3)       /* a CUDA runtime call failed */
+#define PB2_ENLOVERFLOW (-4) /* neighbour-list capacity exceeded (rebuild with more) */
+#define PB2_ENONFINITE (-5)  /* a non-finite force or position was produced */
+#define PB2_ETIMEOUT (-6)    /* a bounded device-side wait ran out */
+#define PB2_ENODEV (-7)      /* no usable sm_100 device */
+
+/* energy term slots (per system), in this order */
+#define PB2_TERM_BOND 0
+#define PB2_TERM_ANGLE 1
+#define PB2_TERM_DIHEDRAL 2
+#define PB2_TERM_CMAP 3
+#define PB2_TERM_LJ 4
+#define PB2_TERM_COULOMB 5
+#define PB2_TERM_GB 6
+#define PB2_TERM_NONPOLAR 7
+#define PB2_TERM_TOTAL 8
+#define PB2_NTERMS 9
+
+/* term-enable bits (pb2_run_params.terms) */
+#define PB2_USE_BONDED 0x1u    /* bonds, angles, torsions */
+#define PB2_USE_CMAP 0x2u
+#define PB2_USE_LJ 0x4u
+#define PB2_USE_COULOMB 0x8u
+#define PB2_USE_GB 0x10u       /* OBC2 Born radii + GB polar + ACE nonpolar */
+#define PB2_USE_ALL 0x1Fu
+
+/* per-system status bits (pb2_get_status) */
+#define PB2_STATUS_NONFINITE 0x1u
+#define PB2_STATUS_NLOVERFLOW 0x2u
+#define PB2_STATUS_FORCE_RANGE 0x4u /* |F| beyond the fixed-point range */
+
+/* One system, host arrays.  Atom indices are local to the system. */
+typedef struct pb2_system_desc {
+  int32_t n_atoms;
+  const double *positions;    /* (n, 3) */
+  const double *charges;      /* (n) e */
+  const double *sigmas;       /* (n) A, LJ sigma */
+  const double *epsilons;     /* (n) kcal/mol */
+  const double *radii;        /* (n) A, GB intrinsic radius rho */
+  const double *scaled_radii; /* (n) A, rho * OBC scale factor */
+  const double *masses;       /* (n) amu */
+
+  int32_t n_bonds;
+  const int32_t *bonds;       /* (n_bonds, 2) */
+  const double *bond_params;  /* (n_bonds, 2) = (r0, k), E = k/2 (r - r0)^2 */
+  int32_t n_angles;
+  const int32_t *angles;      /* (n_angles, 3) */
+  const double *angle_params; /* (n_angles, 2) = (theta0, k) */
+  int32_t n_torsions;
+  int32_t n_torsion_terms;    /* T terms per torsion */
+  const int32_t *torsions;    /* (n_torsions, 4) */
+  const double *torsion_params; /* (n_torsions, T, 3) = (n, phase, k) */
+
+  int32_t n_cmap;
+  const int32_t *cmap_rows;   /* (n_cmap, 5): phi = atoms 0-3, psi = atoms 1-4 */
+  const int32_t *cmap_map;    /* (n_cmap) map index */
+  int32_t n_cmap_maps;
+  int32_t cmap_grid;          /* G, grid points per angle */
+  const double *cmap_coeffs;  /* (n_cmap_maps, G, G, 16) bicubic patch coefficients,
+                                 c[a*4+b] multiplies u^a v^b, u along phi */
+
+  int32_t n_excl;
+  const int32_t *excl_pairs;  /* (n_excl, 2), i < j */
+  const int32_t *excl_kind;   /* (n_excl): 0 = excluded (1-2, 1-3), 1 = 1-4 scaled */
+
+  double lj14_scale;          /* LJ scale of 1-4 pairs (prolix: 0.5) */
+  double coul14_scale;        /* Coulomb scale of 1-4 pairs (prolix: 0.83333333) */
+  double eps_in, eps_out;     /* solute / solvent dielectric */
+  double k_gb;                /* Coulomb constant in the GB prefactor */
+  double k_coulomb;           /* Coulomb constant of the direct term (332.0637) */
+  uint32_t key[2];            /* threefry key of this system's noise stream */
+
+  double dt;                  /* tau */
+  double kT;                  /* kcal/mol */
+  double gamma;               /* 1/tau */
+} pb2_system_desc;
+
+/* Batch-wide settings. */
+typedef struct pb2_run_params {
+  uint32_t terms;       /* PB2_USE_* bits */
+  double cutoff;        /* A; <= 0: all pairs (no neighbour list) */
+  double skin;          /* A; neighbour-list skin (rebuild when any atom moved > skin/2) */
+  int32_t nl_capacity;  /* per-atom neighbour capacity; 0 = automatic */
+  int32_t tile_segment; /* tiles per work item; 0 = autotuned/default */
+  int32_t graph_chunk;  /* steps per captured CUDA graph; 0 = 50 */
+  int32_t partitionable_keys; /* 1: jax_threefry_partitionable layout (JAX default) */
+} pb2_run_params;
+
+typedef struct pb2_ctx pb2_ctx;
+typedef struct pb2_batch pb2_batch;
+
+int pb2_abi_version(void);
+
+/* Context: binds one CUDA device. */
+int pb2_ctx_create(int device, pb2_ctx **out);
+int pb2_ctx_destroy(pb2_ctx *ctx);
+const char *pb2_last_error(const pb2_ctx *ctx);
+
+/*
+ * Upload n_systems systems as one ragged batch (atoms of all systems
+ * concatenated, each system's tiles its own).  Replaces building
+ * PhysicsSystem/PaddedSystem pytrees (prolix typing.py:248-420,
+ * padding.py:21-26) and ExclusionSpec tables (physics/neighbor_list.py:25-303).
+ */
+int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_system_desc *systems,
+                     const pb2_run_params *params, pb2_batch **out);
+int pb2_batch_destroy(pb2_batch *batch);
+int pb2_batch_info(const pb2_batch *batch, int32_t *n_systems, int64_t *n_atoms_total);
+
+/*
+ * Energies and forces at the batch's current positions.  energies: NULL or
+ * (n_systems, PB2_NTERMS); forces: NULL or (n_atoms_total, 3), atoms in
+ * batch order.  Replaces total_energy / decomposed dict (system.py:229-270)
+ * and -jax.grad(total_energy).
+ */
+int pb2_energy_forces(pb2_batch *batch, double *energies, double *forces, void *stream);
+
+/* Born radii (n_atoms_total) at the current positions (system.py:204-216). */
+int pb2_born_radii(pb2_batch *batch, double *born, void *stream);
+
+/* Overwrite positions (n_atoms_total, 3). */
+int pb2_set_positions(pb2_batch *batch, const double *positions, void *stream);
+
+/*
+ * BAOAB state.  pb2_langevin_init replaces init_fn (settle.py:1676-1696):
+ * (key, sub) = split(key); p = sqrt(m kT) normal(sub); F = force(x).
+ * pb2_langevin_run replaces n_steps calls of apply_fn (settle.py:1698-1744)
+ * for every system of the batch; steps are issued as CUDA graphs of
+ * graph_chunk steps.
+ */
+int pb2_langevin_init(pb2_batch *batch, void *stream);
+int pb2_langevin_run(pb2_batch *batch, int32_t n_steps, void *stream);
+
+/* Read or write the integrator state; any pointer may be NULL.
+ * x, p, f: (n_atoms_total, 3); keys: (n_systems, 2); steps: (n_systems). */
+int pb2_get_state(pb2_batch *batch, double *x, double *p, double *f, uint32_t *keys,
+                  int64_t *steps, void *stream);
+int pb2_set_state(pb2_batch *batch, const double *x, const double *p, const uint32_t *keys,
+                  void *stream);
+
+/* Per-system status bits (PB2_STATUS_*) accumulated since the last clear. */
+int pb2_get_status(pb2_batch *batch, uint32_t *status, int clear, void *stream);
+
+/*
+ * Neighbour list (cutoff > 0 only).  pb2_nl_build rebuilds unconditionally;
+ * pb2_nl_check compares the displacement since the last build against
+ * skin/2 (batched_simulate.py:1600-1622) and rebuilds where exceeded;
+ * *rebuilt receives how many systems were rebuilt.  pb2_nl_get copies the
+ * per-atom list in jax_md layout: (n_atoms_total, capacity) int32 local
+ * indices, both (i, j) and (j, i) present, padded with the sentinel n_atoms
+ * of the atom's system.
+ */
+int pb2_nl_build(pb2_batch *batch, void *stream);
+int pb2_nl_check(pb2_batch *batch, int32_t *rebuilt, void *stream);
+int pb2_nl_capacity(const pb2_batch *batch, int32_t *capacity);
+int pb2_nl_get(pb2_batch *batch, int32_t *neighbors, void *stream);
+
+/* Device time of the last pb2_langevin_run / pb2_energy_forces, per kernel
+ * family: out[0] = pair kernels, out[1] = bonded, out[2] = integrator,
+ * out[3] = neighbour list, out[4] = whole call (milliseconds, CUDA events).
+ * Only filled when the batch was created with profiling enabled. */
+int pb2_set_profiling(pb2_batch *batch, int enable);
+int pb2_last_timings(pb2_batch *batch, double *out_ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PROLIX_B200_H */

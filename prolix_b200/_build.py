@@ -1,0 +1,76 @@
+"""In-tree build of the package's native libraries.
+
+* ``libprolix_b200.so``: the CUDA kernels and the C ABI (nvcc, sm_100a only).
+* ``libpb2_host.so``: host C helpers (synthetic chain growth).
+
+Both land next to this file so they travel with the source tree.
+"""
+
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+CSRC = PKG / "csrc"
+INCLUDE = PKG.parent / "include"
+CUDA_LIB = PKG / "libprolix_b200.so"
+HOST_LIB = PKG / "libpb2_host.so"
+
+CUDA_SOURCES = ["pb2_api.cu", "pb2_pair.cu", "pb2_bonded.cu", "pb2_integrate.cu",
+                "pb2_nlist.cu", "pb2_noalloc.cu"]
+CUDA_HEADERS = ["pb2_common.cuh", "pb2_pairmath.cuh", "pb2_threefry.cuh"]
+HOST_SOURCES = ["synth_chain.c"]
+
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-lineinfo", "-O3", "-std=c++17",
+    "--expt-relaxed-constexpr",
+    "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
+]
+
+
+def _nvcc() -> str:
+  for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+    if cand and Path(cand).exists():
+      return cand
+  raise RuntimeError("nvcc not found: the CUDA library cannot be built")
+
+
+def _stale(target: Path, sources) -> bool:
+  if not target.exists():
+    return True
+  t = target.stat().st_mtime
+  return any(s.exists() and s.stat().st_mtime > t for s in sources)
+
+
+def build_host(force: bool = False) -> Path:
+  srcs = [CSRC / s for s in HOST_SOURCES]
+  if force or _stale(HOST_LIB, srcs):
+    cc = shutil.which("gcc") or "cc"
+    tmp = HOST_LIB.with_suffix(".so.tmp")
+    subprocess.run([cc, "-O2", "-shared", "-fPIC", "-o", str(tmp), *map(str, srcs), "-lm"],
+                   check=True)
+    os.replace(tmp, HOST_LIB)
+  return HOST_LIB
+
+
+def build_cuda(force: bool = False, extra_flags=None) -> Path:
+  present = [s for s in CUDA_SOURCES if (CSRC / s).exists()]
+  srcs = [CSRC / s for s in present]
+  deps = srcs + [CSRC / h for h in CUDA_HEADERS] + [INCLUDE / "prolix_b200.h"]
+  if force or _stale(CUDA_LIB, deps):
+    nvcc = _nvcc()
+    tmp = CUDA_LIB.with_suffix(".so.tmp")
+    cmd = [nvcc, *NVCC_FLAGS, *(extra_flags or []), "-I", str(INCLUDE), "-I", str(CSRC),
+           "-shared", "-o", str(tmp), *map(str, srcs), "-lcuda"]
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, CUDA_LIB)
+  return CUDA_LIB
+
+
+def build_all(force: bool = False) -> None:
+  build_host(force)
+  build_cuda(force)

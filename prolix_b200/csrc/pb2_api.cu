@@ -1,0 +1,819 @@
+// C ABI of prolix_b200: context and batch management, force evaluation,
+// Langevin runs (captured as CUDA graphs), state access.
+//
+// Data layout in HBM (batch order = systems concatenated, atoms in input
+// order within a system):
+//   FP64 SoA state x, y, z, px, py, pz; int64 fixed-point forces fx, fy, fz;
+//   float4 posq (x, y, z relative to the system origin, charge) and
+//   float4 par (sigma/2, sqrt(eps), rho~, scaled radius) for the pair
+//   kernels; float4 born (B, 1/B, dB/dI); int64 descreening and dE/dB sums;
+//   per-system SysInfo records, keys (two buffers), step counters, status.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "pb2_common.cuh"
+#include "pb2_kernels.cuh"
+
+
+using namespace pb2;
+
+struct pb2_ctx {
+  int device = 0;
+  int sm_count = 148;
+  std::string err;
+};
+
+namespace {
+
+constexpr int kFamPair = 0, kFamBonded = 1, kFamInt = 2, kFamNl = 3, kFamAll = 4;
+
+struct Dev {
+  std::vector<void *> ptrs;
+  ~Dev() {
+    for (void *p : ptrs) cudaFree(p);
+  }
+  template <class T>
+  T *alloc(size_t n) {
+    void *p = nullptr;
+    if (n == 0) n = 1;
+    if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return nullptr;
+    ptrs.push_back(p);
+    return static_cast<T *>(p);
+  }
+};
+
+}  // namespace
+
+struct pb2_batch {
+  pb2_ctx *ctx = nullptr;
+  pb2_run_params params{};
+  int n_sys = 0;
+  int n_total = 0;
+  std::vector<int> off, nat;
+  std::vector<SysInfo> sys_host;
+  Dev dev;
+  SysInfo *sys = nullptr;
+  int32_t *atom_sys = nullptr;
+  double *x = nullptr, *y = nullptr, *z = nullptr, *px = nullptr, *py = nullptr, *pz = nullptr;
+  long long *fx = nullptr, *fy = nullptr, *fz = nullptr;
+  double *mass = nullptr, *sigma = nullptr, *charge = nullptr, *radius = nullptr;
+  float4 *posq = nullptr, *par = nullptr, *born = nullptr;
+  long long *born_acc = nullptr, *dedb_acc = nullptr, *energy = nullptr;
+  uint32_t *keys = nullptr, *status = nullptr;
+  long long *steps = nullptr;
+  TileItem *items = nullptr;
+  int n_items = 0;
+  int2 *excl_ent = nullptr;
+  ExclRow *excl_rows = nullptr;
+  BondedArgs bonded{};
+  int key_parity = 0;
+  int grid_pair[3] = {1, 1, 1};
+  int grid_pair_energy = 1;
+  int grid_bonded = 1;
+  cudaStream_t cap_stream = nullptr;
+  std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
+  bool profiling = false;
+  double timings[5] = {0, 0, 0, 0, 0};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+
+  ~pb2_batch() {
+    for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
+    if (cap_stream) cudaStreamDestroy(cap_stream);
+    for (auto &e : ev)
+      if (e) cudaEventDestroy(e);
+  }
+};
+
+static int fail(pb2_ctx *ctx, int code, const std::string &msg) {
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
+#define CUDA_TRY(ctx, expr)                                                                  \
+  do {                                                                                       \
+    cudaError_t e_ = (expr);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return fail((ctx), PB2_ECUDA, std::string(#expr) + ": " + cudaGetErrorString(e_));     \
+  } while (0)
+
+extern "C" int pb2_abi_version(void) { return PB2_ABI_VERSION; }
+
+extern "C" int pb2_ctx_create(int device, pb2_ctx **out) {
+  if (!out) return PB2_EINVAL;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= device || device < 0) return PB2_ENODEV;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return PB2_ENODEV;
+  if (prop.major != 10) return PB2_ENODEV;  // built for sm_100a only
+  if (cudaSetDevice(device) != cudaSuccess) return PB2_ENODEV;
+  auto *c = new (std::nothrow) pb2_ctx;
+  if (!c) return PB2_ENOMEM;
+  c->device = device;
+  c->sm_count = prop.multiProcessorCount;
+  *out = c;
+  return PB2_OK;
+}
+
+extern "C" int pb2_ctx_destroy(pb2_ctx *ctx) {
+  delete ctx;
+  return PB2_OK;
+}
+
+extern "C" const char *pb2_last_error(const pb2_ctx *ctx) {
+  return ctx ? ctx->err.c_str() : "null context";
+}
+
+// ------------------------------------------------------------ batch build
+
+static PairArgs pair_args(pb2_batch *b) {
+  PairArgs a;
+  a.sys = b->sys;
+  a.items = b->items;
+  a.n_items = b->n_items;
+  a.terms = b->params.terms;
+  a.excl_ent = b->excl_ent;
+  a.excl_rows = b->excl_rows;
+  a.posq = b->posq;
+  a.par = b->par;
+  a.born = b->born;
+  a.born_acc = b->born_acc;
+  a.dedb_acc = b->dedb_acc;
+  a.fx = b->fx;
+  a.fy = b->fy;
+  a.fz = b->fz;
+  a.energy = b->energy;
+  return a;
+}
+
+static IntArgs int_args(pb2_batch *b, int parity, int finish_prev) {
+  IntArgs a;
+  a.sys = b->sys;
+  a.atom_sys = b->atom_sys;
+  a.x = b->x; a.y = b->y; a.z = b->z;
+  a.px = b->px; a.py = b->py; a.pz = b->pz;
+  a.fx = b->fx; a.fy = b->fy; a.fz = b->fz;
+  a.mass = b->mass;
+  a.sigma = b->sigma;
+  a.charge = b->charge;
+  a.posq = b->posq;
+  a.keys = b->keys;
+  a.steps = b->steps;
+  a.status = b->status;
+  a.n_total = b->n_total;
+  a.n_sys = b->n_sys;
+  a.parity = parity;
+  a.finish_prev = finish_prev;
+  a.partitionable = b->params.partitionable_keys;
+  return a;
+}
+
+static int validate(pb2_ctx *ctx, const pb2_system_desc &d, int s) {
+  char buf[256];
+  auto bad = [&](const char *what) {
+    snprintf(buf, sizeof buf, "system %d: %s", s, what);
+    return fail(ctx, PB2_EINVAL, buf);
+  };
+  if (d.n_atoms <= 0) return bad("n_atoms must be > 0");
+  if (!d.positions || !d.charges || !d.sigmas || !d.epsilons || !d.radii || !d.scaled_radii ||
+      !d.masses)
+    return bad("per-atom arrays must not be NULL");
+  const int n = d.n_atoms;
+  for (int i = 0; i < n; ++i) {
+    if (!(d.masses[i] > 0.0)) return bad("masses must be > 0");
+    if (!(d.radii[i] > 0.0)) return bad("radii must be > 0");
+  }
+  auto check_idx = [&](const int32_t *idx, int64_t count, const char *what) -> bool {
+    for (int64_t k = 0; k < count; ++k)
+      if (idx[k] < 0 || idx[k] >= n) {
+        snprintf(buf, sizeof buf, "system %d: %s index %d out of range", s, what, idx[k]);
+        return false;
+      }
+    return true;
+  };
+  if (d.n_bonds < 0 || d.n_angles < 0 || d.n_torsions < 0 || d.n_cmap < 0 || d.n_excl < 0)
+    return bad("negative term count");
+  if (d.n_bonds && (!d.bonds || !d.bond_params)) return bad("bond arrays missing");
+  if (d.n_angles && (!d.angles || !d.angle_params)) return bad("angle arrays missing");
+  if (d.n_torsions && (!d.torsions || !d.torsion_params || d.n_torsion_terms <= 0))
+    return bad("torsion arrays missing");
+  if (d.n_cmap && (!d.cmap_rows || !d.cmap_map || !d.cmap_coeffs || d.n_cmap_maps <= 0 ||
+                   d.cmap_grid <= 0))
+    return bad("cmap arrays missing");
+  if (d.n_excl && (!d.excl_pairs || !d.excl_kind)) return bad("exclusion arrays missing");
+  if (!check_idx(d.bonds, 2LL * d.n_bonds, "bond") ||
+      !check_idx(d.angles, 3LL * d.n_angles, "angle") ||
+      !check_idx(d.torsions, 4LL * d.n_torsions, "torsion") ||
+      !check_idx(d.cmap_rows, 5LL * d.n_cmap, "cmap") ||
+      !check_idx(d.excl_pairs, 2LL * d.n_excl, "exclusion"))
+    return fail(ctx, PB2_EINVAL, buf);
+  for (int k = 0; k < d.n_cmap; ++k)
+    if (d.cmap_map[k] < 0 || d.cmap_map[k] >= d.n_cmap_maps) return bad("cmap map index out of range");
+  for (int k = 0; k < d.n_excl; ++k) {
+    if (d.excl_pairs[2 * k] >= d.excl_pairs[2 * k + 1]) return bad("exclusion pairs need i < j");
+    if (d.excl_kind[k] != 0 && d.excl_kind[k] != 1) return bad("exclusion kind must be 0 or 1");
+  }
+  if (!(d.dt > 0.0) || !(d.kT >= 0.0) || !(d.gamma >= 0.0)) return bad("dt > 0, kT >= 0, gamma >= 0");
+  if (!(d.eps_in > 0.0) || !(d.eps_out > 0.0)) return bad("dielectrics must be > 0");
+  return PB2_OK;
+}
+
+template <class T>
+static int upload(pb2_ctx *ctx, T *dst, const std::vector<T> &src) {
+  if (src.empty()) return PB2_OK;
+  CUDA_TRY(ctx, cudaMemcpy(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return PB2_OK;
+}
+
+extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_system_desc *systems,
+                                const pb2_run_params *params, pb2_batch **out) {
+  if (!ctx || !out || !systems || !params || n_systems <= 0) return fail(ctx, PB2_EINVAL, "bad arguments");
+  *out = nullptr;
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  for (int s = 0; s < n_systems; ++s) {
+    int rc = validate(ctx, systems[s], s);
+    if (rc) return rc;
+  }
+  std::unique_ptr<pb2_batch> b(new (std::nothrow) pb2_batch);
+  if (!b) return fail(ctx, PB2_ENOMEM, "host allocation");
+  b->ctx = ctx;
+  b->params = *params;
+  if (b->params.tile_segment <= 0) b->params.tile_segment = 8;
+  if (b->params.graph_chunk <= 0) b->params.graph_chunk = 50;
+  b->n_sys = n_systems;
+  const bool cutoff_mode = params->cutoff > 0.0;
+
+  // --- per-atom host arrays
+  int64_t total = 0;
+  int blocks_total = 0;
+  for (int s = 0; s < n_systems; ++s) {
+    b->off.push_back((int)total);
+    b->nat.push_back(systems[s].n_atoms);
+    total += systems[s].n_atoms;
+    blocks_total += (systems[s].n_atoms + 31) / 32;
+  }
+  if (total > (1LL << 30)) return fail(ctx, PB2_EINVAL, "too many atoms");
+  const int N = (int)total;
+  b->n_total = N;
+  std::vector<double> hx(N), hy(N), hz(N), hm(N), hsig(N), hq(N), hrad(N);
+  std::vector<float4> hposq(N), hpar(N);
+  std::vector<int32_t> hsys(N);
+  std::vector<SysInfo> sinfo(n_systems);
+  std::vector<uint32_t> hkeys(4 * (size_t)n_systems, 0u);
+  std::vector<int2> hent((size_t)blocks_total * kExclPerBlock, make_int2(-1, -1));
+  std::vector<ExclRow> hrows;
+  std::vector<TileItem> hitems;
+  int blk_base = 0;
+  for (int s = 0; s < n_systems; ++s) {
+    const pb2_system_desc &d = systems[s];
+    const int n = d.n_atoms, o = b->off[s];
+    SysInfo &S = sinfo[s];
+    memset(&S, 0, sizeof S);
+    S.n = n;
+    S.off = o;
+    S.nblk = (n + 31) / 32;
+    S.blk_base = blk_base;
+    const double pref = -0.5 * d.k_gb * (1.0 / d.eps_in - 1.0 / d.eps_out);
+    S.pref = (float)pref;
+    S.pref_d = pref;
+    S.kcoul = (float)d.k_coulomb;
+    S.lj14 = (float)d.lj14_scale;
+    S.coul14 = (float)d.coul14_scale;
+    S.cutoff2 = cutoff_mode ? (float)(params->cutoff * params->cutoff) : 0.f;
+    S.dt = d.dt;
+    S.half_dt = 0.5 * d.dt;
+    S.c1 = std::exp(-d.gamma * d.dt);
+    S.c2 = std::sqrt(1.0 - S.c1 * S.c1);
+    S.kT = d.kT;
+    S.skin_half2 = 0.25 * params->skin * params->skin;
+    double cx = 0, cy = 0, cz = 0;
+    for (int i = 0; i < n; ++i) {
+      cx += d.positions[3 * i];
+      cy += d.positions[3 * i + 1];
+      cz += d.positions[3 * i + 2];
+    }
+    S.ox = std::round(cx / n);
+    S.oy = std::round(cy / n);
+    S.oz = std::round(cz / n);
+    for (int i = 0; i < n; ++i) {
+      const int g = o + i;
+      hx[g] = d.positions[3 * i];
+      hy[g] = d.positions[3 * i + 1];
+      hz[g] = d.positions[3 * i + 2];
+      hm[g] = d.masses[i];
+      hsig[g] = S.c2 * std::sqrt(d.masses[i] * d.kT);
+      hq[g] = d.charges[i];
+      hrad[g] = d.radii[i];
+      hsys[g] = s;
+      hposq[g] = make_float4((float)(hx[g] - S.ox), (float)(hy[g] - S.oy), (float)(hz[g] - S.oz),
+                             (float)d.charges[i]);
+      double ro = d.radii[i] - kDielOffset;
+      if (cutoff_mode) ro = std::max(std::max(d.radii[i], 1e-6) - kDielOffset, 1e-4);
+      hpar[g] = make_float4((float)(0.5 * std::max(d.sigmas[i], 1e-6)),
+                            (float)std::sqrt(std::max(d.epsilons[i], 0.0)), (float)ro,
+                            (float)d.scaled_radii[i]);
+    }
+    hkeys[2 * (size_t)s] = d.key[0];
+    hkeys[2 * (size_t)s + 1] = d.key[1];
+    // exclusion masks, one 32-row block per (i-block, j-block) with exclusions
+    for (int k = 0; k < d.n_excl; ++k) {
+      const int i = d.excl_pairs[2 * k], j = d.excl_pairs[2 * k + 1];
+      const int ib = i >> 5, jb = j >> 5;
+      int2 *ent = &hent[(size_t)(blk_base + ib) * kExclPerBlock];
+      int slot = -1;
+      for (int e = 0; e < kExclPerBlock; ++e) {
+        if (ent[e].x == jb) { slot = e; break; }
+        if (ent[e].x < 0) {
+          ent[e] = make_int2(jb, (int)hrows.size());
+          hrows.resize(hrows.size() + 32, ExclRow{0u, 0u});
+          slot = e;
+          break;
+        }
+      }
+      if (slot < 0) {
+        char buf[200];
+        snprintf(buf, sizeof buf,
+                 "system %d: atoms %d..%d have exclusion partners in more than %d 32-atom blocks",
+                 s, ib * 32, ib * 32 + 31, kExclPerBlock);
+        return fail(ctx, PB2_EINVAL, buf);
+      }
+      ExclRow &row = hrows[ent[slot].y + (i & 31)];
+      if (d.excl_kind[k] == 0) row.excl |= 1u << (j & 31);
+      else row.s14 |= 1u << (j & 31);
+    }
+    // tile work items: row iblk, tiles jb in [iblk, nblk) in segments
+    const int seg = b->params.tile_segment;
+    for (int ib = 0; ib < S.nblk; ++ib)
+      for (int j0 = ib; j0 < S.nblk; j0 += seg)
+        hitems.push_back(TileItem{s, ib, j0, std::min(j0 + seg, S.nblk)});
+    blk_base += S.nblk;
+  }
+  std::stable_sort(hitems.begin(), hitems.end(), [](const TileItem &p, const TileItem &q) {
+    return (p.jb1 - p.jb0) > (q.jb1 - q.jb0);
+  });
+  b->n_items = (int)hitems.size();
+  b->sys_host = sinfo;
+
+  // --- bonded tables (global atom indices)
+  std::vector<int2> bidx;
+  std::vector<double2> bpar;
+  std::vector<int4> aidx;
+  std::vector<double2> apar;
+  std::vector<int4> tidx;
+  std::vector<double4> tpar;
+  std::vector<int32_t> cidx;
+  std::vector<double> ccoef;
+  std::vector<int32_t> cgrid;
+  std::vector<int64_t> cmoff;
+  for (int s = 0; s < n_systems; ++s) {
+    const pb2_system_desc &d = systems[s];
+    const int o = b->off[s];
+    for (int k = 0; k < d.n_bonds; ++k) {
+      bidx.push_back(make_int2(o + d.bonds[2 * k], o + d.bonds[2 * k + 1]));
+      bpar.push_back(make_double2(d.bond_params[2 * k], d.bond_params[2 * k + 1]));
+    }
+    for (int k = 0; k < d.n_angles; ++k) {
+      aidx.push_back(make_int4(o + d.angles[3 * k], o + d.angles[3 * k + 1], o + d.angles[3 * k + 2], 0));
+      apar.push_back(make_double2(d.angle_params[2 * k], d.angle_params[2 * k + 1]));
+    }
+    for (int k = 0; k < d.n_torsions; ++k)
+      for (int t = 0; t < d.n_torsion_terms; ++t) {
+        const double *p = d.torsion_params + ((size_t)k * d.n_torsion_terms + t) * 3;
+        tidx.push_back(make_int4(o + d.torsions[4 * k], o + d.torsions[4 * k + 1],
+                                 o + d.torsions[4 * k + 2], o + d.torsions[4 * k + 3]));
+        tpar.push_back(make_double4(p[0], p[1], p[2], 0.0));
+      }
+    const int map_base = (int)cgrid.size();
+    const size_t per_map = (size_t)d.cmap_grid * d.cmap_grid * 16;
+    for (int m = 0; m < d.n_cmap_maps && d.n_cmap > 0; ++m) {
+      cgrid.push_back(d.cmap_grid);
+      cmoff.push_back((int64_t)ccoef.size());
+      ccoef.insert(ccoef.end(), d.cmap_coeffs + m * per_map, d.cmap_coeffs + (m + 1) * per_map);
+    }
+    for (int k = 0; k < d.n_cmap; ++k) {
+      for (int c = 0; c < 5; ++c) cidx.push_back(o + d.cmap_rows[5 * k + c]);
+      cidx.push_back(map_base + d.cmap_map[k]);
+    }
+  }
+
+  // --- device allocation
+  Dev &D = b->dev;
+  b->sys = D.alloc<SysInfo>(n_systems);
+  b->atom_sys = D.alloc<int32_t>(N);
+  b->x = D.alloc<double>(N); b->y = D.alloc<double>(N); b->z = D.alloc<double>(N);
+  b->px = D.alloc<double>(N); b->py = D.alloc<double>(N); b->pz = D.alloc<double>(N);
+  b->fx = D.alloc<long long>(N); b->fy = D.alloc<long long>(N); b->fz = D.alloc<long long>(N);
+  b->mass = D.alloc<double>(N);
+  b->sigma = D.alloc<double>(N);
+  b->charge = D.alloc<double>(N);
+  b->radius = D.alloc<double>(N);
+  b->posq = D.alloc<float4>(N);
+  b->par = D.alloc<float4>(N);
+  b->born = D.alloc<float4>(N);
+  b->born_acc = D.alloc<long long>(N);
+  b->dedb_acc = D.alloc<long long>(N);
+  b->energy = D.alloc<long long>((size_t)n_systems * PB2_NTERMS);
+  b->keys = D.alloc<uint32_t>(4 * (size_t)n_systems);
+  b->steps = D.alloc<long long>(n_systems);
+  b->status = D.alloc<uint32_t>(n_systems);
+  b->items = D.alloc<TileItem>(hitems.size());
+  b->excl_ent = D.alloc<int2>(hent.size());
+  b->excl_rows = D.alloc<ExclRow>(hrows.size());
+  BondedArgs &B = b->bonded;
+  B.n_bond = (int)bidx.size();
+  B.n_angle = (int)aidx.size();
+  B.n_tors = (int)tidx.size();
+  B.n_cmap = (int)(cidx.size() / 6);
+  int2 *d_bidx = D.alloc<int2>(bidx.size());
+  double2 *d_bpar = D.alloc<double2>(bpar.size());
+  int4 *d_aidx = D.alloc<int4>(aidx.size());
+  double2 *d_apar = D.alloc<double2>(apar.size());
+  int4 *d_tidx = D.alloc<int4>(tidx.size());
+  double4 *d_tpar = D.alloc<double4>(tpar.size());
+  int32_t *d_cidx = D.alloc<int32_t>(cidx.size());
+  double *d_ccoef = D.alloc<double>(ccoef.size());
+  int32_t *d_cgrid = D.alloc<int32_t>(cgrid.size());
+  int64_t *d_cmoff = D.alloc<int64_t>(cmoff.size());
+  for (void *p : D.ptrs)
+    if (!p) return fail(ctx, PB2_ENOMEM, "device allocation failed");
+  if (!d_cmoff || !d_cgrid || !d_ccoef || !d_cidx || !b->excl_rows)
+    return fail(ctx, PB2_ENOMEM, "device allocation failed");
+
+  int rc;
+  if ((rc = upload(ctx, b->sys, sinfo)) || (rc = upload(ctx, b->atom_sys, hsys)) ||
+      (rc = upload(ctx, b->x, hx)) || (rc = upload(ctx, b->y, hy)) || (rc = upload(ctx, b->z, hz)) ||
+      (rc = upload(ctx, b->mass, hm)) || (rc = upload(ctx, b->sigma, hsig)) ||
+      (rc = upload(ctx, b->charge, hq)) || (rc = upload(ctx, b->radius, hrad)) ||
+      (rc = upload(ctx, b->posq, hposq)) || (rc = upload(ctx, b->par, hpar)) ||
+      (rc = upload(ctx, b->keys, hkeys)) || (rc = upload(ctx, b->items, hitems)) ||
+      (rc = upload(ctx, b->excl_ent, hent)) || (rc = upload(ctx, b->excl_rows, hrows)) ||
+      (rc = upload(ctx, d_bidx, bidx)) || (rc = upload(ctx, d_bpar, bpar)) ||
+      (rc = upload(ctx, d_aidx, aidx)) || (rc = upload(ctx, d_apar, apar)) ||
+      (rc = upload(ctx, d_tidx, tidx)) || (rc = upload(ctx, d_tpar, tpar)) ||
+      (rc = upload(ctx, d_cidx, cidx)) || (rc = upload(ctx, d_ccoef, ccoef)) ||
+      (rc = upload(ctx, d_cgrid, cgrid)) || (rc = upload(ctx, d_cmoff, cmoff)))
+    return rc;
+  CUDA_TRY(ctx, cudaMemset(b->px, 0, N * sizeof(double)));
+  CUDA_TRY(ctx, cudaMemset(b->py, 0, N * sizeof(double)));
+  CUDA_TRY(ctx, cudaMemset(b->pz, 0, N * sizeof(double)));
+  CUDA_TRY(ctx, cudaMemset(b->fx, 0, N * sizeof(long long)));
+  CUDA_TRY(ctx, cudaMemset(b->fy, 0, N * sizeof(long long)));
+  CUDA_TRY(ctx, cudaMemset(b->fz, 0, N * sizeof(long long)));
+  CUDA_TRY(ctx, cudaMemset(b->born_acc, 0, N * sizeof(long long)));
+  CUDA_TRY(ctx, cudaMemset(b->dedb_acc, 0, N * sizeof(long long)));
+  CUDA_TRY(ctx, cudaMemset(b->born, 0, N * sizeof(float4)));
+  CUDA_TRY(ctx, cudaMemset(b->steps, 0, n_systems * sizeof(long long)));
+  CUDA_TRY(ctx, cudaMemset(b->status, 0, n_systems * sizeof(uint32_t)));
+  B.atom_sys = b->atom_sys;
+  B.x = b->x; B.y = b->y; B.z = b->z;
+  B.fx = b->fx; B.fy = b->fy; B.fz = b->fz;
+  B.energy = b->energy;
+  B.terms = params->terms;
+  B.bond_idx = d_bidx; B.bond_par = d_bpar;
+  B.angle_idx = d_aidx; B.angle_par = d_apar;
+  B.tors_idx = d_tidx; B.tors_par = d_tpar;
+  B.cmap_idx = d_cidx; B.cmap_coeff = d_ccoef; B.cmap_grid = d_cgrid; B.cmap_map_off = d_cmoff;
+  if (!(params->terms & PB2_USE_BONDED)) B.n_bond = B.n_angle = B.n_tors = 0;
+  if (!(params->terms & PB2_USE_CMAP)) B.n_cmap = 0;
+
+  // launch shapes: persistent grids sized to the resident capacity
+  for (int p = 0; p < 3; ++p) {
+    const int cap = tile_kernel_occupancy(p, false) * ctx->sm_count;
+    b->grid_pair[p] = std::max(1, std::min(cap, (b->n_items + 7) / 8));
+  }
+  {
+    const int cap = tile_kernel_occupancy(PASS_FORCE, true) * ctx->sm_count;
+    b->grid_pair_energy = std::max(1, std::min(cap, (b->n_items + 7) / 8));
+  }
+  b->grid_bonded = 8 * ctx->sm_count;
+  CUDA_TRY(ctx, cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking));
+  CUDA_TRY(ctx, cudaEventCreate(&b->ev[0]));
+  CUDA_TRY(ctx, cudaEventCreate(&b->ev[1]));
+  CUDA_TRY(ctx, cudaDeviceSynchronize());
+  *out = b.release();
+  return PB2_OK;
+}
+
+extern "C" int pb2_batch_destroy(pb2_batch *b) {
+  if (!b) return PB2_OK;
+  cudaSetDevice(b->ctx->device);
+  cudaDeviceSynchronize();
+  delete b;
+  return PB2_OK;
+}
+
+extern "C" int pb2_batch_info(const pb2_batch *b, int32_t *n_systems, int64_t *n_atoms_total) {
+  if (!b) return PB2_EINVAL;
+  if (n_systems) *n_systems = b->n_sys;
+  if (n_atoms_total) *n_atoms_total = b->n_total;
+  return PB2_OK;
+}
+
+// ------------------------------------------------------------ force evaluation
+
+// Force kernels on the current posq; force accumulators must be zero (or
+// hold contributions to keep) and born_acc zero.
+static cudaError_t enqueue_forces(pb2_batch *b, cudaStream_t st, bool energy) {
+  cudaError_t e;
+  const PairArgs pa = pair_args(b);
+  const bool gb = (b->params.terms & PB2_USE_GB) != 0;
+  if (gb) {
+    if ((e = launch_tiles(PASS_BORN, false, pa, b->grid_pair[PASS_BORN], st)) != cudaSuccess) return e;
+    FinalizeArgs fa;
+    fa.sys = b->sys;
+    fa.atom_sys = b->atom_sys;
+    fa.radius = b->radius;
+    fa.charge = b->charge;
+    fa.born_acc = b->born_acc;
+    fa.born = b->born;
+    fa.dedb_acc = b->dedb_acc;
+    fa.energy = b->energy;
+    fa.n_total = b->n_total;
+    fa.energy_mode = energy ? 1 : 0;
+    if ((e = launch_born_finalize(fa, st)) != cudaSuccess) return e;
+  }
+  if ((e = launch_tiles(PASS_FORCE, energy, pa, energy ? b->grid_pair_energy : b->grid_pair[PASS_FORCE], st)) != cudaSuccess)
+    return e;
+  if (gb)
+    if ((e = launch_tiles(PASS_CHAIN, false, pa, b->grid_pair[PASS_CHAIN], st)) != cudaSuccess) return e;
+  BondedArgs ba = b->bonded;
+  ba.energy_mode = energy ? 1 : 0;
+  return launch_bonded(ba, b->grid_bonded, st);
+}
+
+static int fresh_forces(pb2_batch *b, cudaStream_t st, bool energy) {
+  pb2_ctx *ctx = b->ctx;
+  const size_t nb = (size_t)b->n_total * sizeof(long long);
+  CUDA_TRY(ctx, cudaMemsetAsync(b->fx, 0, nb, st));
+  CUDA_TRY(ctx, cudaMemsetAsync(b->fy, 0, nb, st));
+  CUDA_TRY(ctx, cudaMemsetAsync(b->fz, 0, nb, st));
+  if (energy)
+    CUDA_TRY(ctx, cudaMemsetAsync(b->energy, 0, (size_t)b->n_sys * PB2_NTERMS * sizeof(long long), st));
+  CUDA_TRY(ctx, launch_posq(int_args(b, b->key_parity, 0), st));
+  CUDA_TRY(ctx, enqueue_forces(b, st, energy));
+  return PB2_OK;
+}
+
+static int copy_forces(pb2_batch *b, double *forces, cudaStream_t st) {
+  pb2_ctx *ctx = b->ctx;
+  const int N = b->n_total;
+  std::vector<long long> hf(3 * (size_t)N);
+  CUDA_TRY(ctx, cudaMemcpyAsync(hf.data(), b->fx, N * sizeof(long long), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(ctx, cudaMemcpyAsync(hf.data() + N, b->fy, N * sizeof(long long), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(ctx, cudaMemcpyAsync(hf.data() + 2 * (size_t)N, b->fz, N * sizeof(long long), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  for (int i = 0; i < N; ++i)
+    for (int c = 0; c < 3; ++c) forces[3 * (size_t)i + c] = (double)hf[(size_t)c * N + i] * kForceInv;
+  return PB2_OK;
+}
+
+extern "C" int pb2_energy_forces(pb2_batch *b, double *energies, double *forces, void *stream) {
+  if (!b) return PB2_EINVAL;
+  pb2_ctx *ctx = b->ctx;
+  cudaStream_t st = (cudaStream_t)stream;
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  int rc = fresh_forces(b, st, energies != nullptr);
+  if (rc) return rc;
+  if (energies) {
+    std::vector<long long> he((size_t)b->n_sys * PB2_NTERMS);
+    CUDA_TRY(ctx, cudaMemcpyAsync(he.data(), b->energy, he.size() * sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    for (int s = 0; s < b->n_sys; ++s) {
+      double tot = 0.0;
+      for (int t = 0; t < PB2_TERM_TOTAL; ++t) {
+        const double v = (double)he[(size_t)s * PB2_NTERMS + t] * kForceInv;
+        energies[(size_t)s * PB2_NTERMS + t] = v;
+        tot += v;
+      }
+      energies[(size_t)s * PB2_NTERMS + PB2_TERM_TOTAL] = tot;
+    }
+  }
+  if (forces) return copy_forces(b, forces, st);
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  return PB2_OK;
+}
+
+extern "C" int pb2_born_radii(pb2_batch *b, double *out, void *stream) {
+  if (!b || !out) return PB2_EINVAL;
+  pb2_ctx *ctx = b->ctx;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!(b->params.terms & PB2_USE_GB)) return fail(ctx, PB2_EINVAL, "GB term disabled");
+  int rc = fresh_forces(b, st, false);
+  if (rc) return rc;
+  std::vector<float4> hb(b->n_total);
+  CUDA_TRY(ctx, cudaMemcpyAsync(hb.data(), b->born, hb.size() * sizeof(float4), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  for (int i = 0; i < b->n_total; ++i) out[i] = (double)hb[i].x;
+  return PB2_OK;
+}
+
+static int upload_soa3(pb2_batch *b, const double *aos, double *dx, double *dy, double *dz, cudaStream_t st) {
+  pb2_ctx *ctx = b->ctx;
+  const int N = b->n_total;
+  std::vector<double> h(3 * (size_t)N);
+  for (int i = 0; i < N; ++i)
+    for (int c = 0; c < 3; ++c) h[(size_t)c * N + i] = aos[3 * (size_t)i + c];
+  CUDA_TRY(ctx, cudaMemcpyAsync(dx, h.data(), N * sizeof(double), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(ctx, cudaMemcpyAsync(dy, h.data() + N, N * sizeof(double), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(ctx, cudaMemcpyAsync(dz, h.data() + 2 * (size_t)N, N * sizeof(double), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  return PB2_OK;
+}
+
+static int download_soa3(pb2_batch *b, double *aos, const double *dx, const double *dy, const double *dz,
+                         cudaStream_t st) {
+  pb2_ctx *ctx = b->ctx;
+  const int N = b->n_total;
+  std::vector<double> h(3 * (size_t)N);
+  CUDA_TRY(ctx, cudaMemcpyAsync(h.data(), dx, N * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(ctx, cudaMemcpyAsync(h.data() + N, dy, N * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(ctx, cudaMemcpyAsync(h.data() + 2 * (size_t)N, dz, N * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  for (int i = 0; i < N; ++i)
+    for (int c = 0; c < 3; ++c) aos[3 * (size_t)i + c] = h[(size_t)c * N + i];
+  return PB2_OK;
+}
+
+extern "C" int pb2_set_positions(pb2_batch *b, const double *positions, void *stream) {
+  if (!b || !positions) return PB2_EINVAL;
+  return upload_soa3(b, positions, b->x, b->y, b->z, (cudaStream_t)stream);
+}
+
+// ------------------------------------------------------------ Langevin
+
+static int run_eager(pb2_batch *b, int n_steps, cudaStream_t st) {
+  pb2_ctx *ctx = b->ctx;
+  for (int t = 0; t < n_steps; ++t) {
+    const int parity = b->key_parity;
+    if (b->profiling) CUDA_TRY(ctx, cudaEventRecord(b->ev[0], st));
+    CUDA_TRY(ctx, launch_step(int_args(b, parity, t > 0), st));
+    if (b->profiling) {
+      CUDA_TRY(ctx, cudaEventRecord(b->ev[1], st));
+      CUDA_TRY(ctx, cudaEventSynchronize(b->ev[1]));
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]);
+      b->timings[kFamInt] += ms;
+      CUDA_TRY(ctx, cudaEventRecord(b->ev[0], st));
+    }
+    CUDA_TRY(ctx, enqueue_forces(b, st, false));
+    if (b->profiling) {
+      CUDA_TRY(ctx, cudaEventRecord(b->ev[1], st));
+      CUDA_TRY(ctx, cudaEventSynchronize(b->ev[1]));
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]);
+      b->timings[kFamPair] += ms;
+    }
+    b->key_parity ^= 1;
+  }
+  CUDA_TRY(ctx, launch_finish(int_args(b, b->key_parity, 0), st));
+  return PB2_OK;
+}
+
+static int get_graph(pb2_batch *b, int chunk, int parity, cudaGraphExec_t *out) {
+  pb2_ctx *ctx = b->ctx;
+  auto key = std::make_pair(chunk, parity);
+  auto it = b->graphs.find(key);
+  if (it != b->graphs.end()) {
+    *out = it->second;
+    return PB2_OK;
+  }
+  cudaStream_t cs = b->cap_stream;
+  CUDA_TRY(ctx, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+  cudaError_t err = cudaSuccess;
+  int p = parity;
+  for (int t = 0; t < chunk && err == cudaSuccess; ++t) {
+    err = launch_step(int_args(b, p, t > 0), cs);
+    if (err == cudaSuccess) err = enqueue_forces(b, cs, false);
+    p ^= 1;
+  }
+  if (err == cudaSuccess) err = launch_finish(int_args(b, p, 0), cs);
+  cudaGraph_t g = nullptr;
+  cudaError_t e2 = cudaStreamEndCapture(cs, &g);
+  if (err != cudaSuccess || e2 != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return fail(ctx, PB2_ECUDA, std::string("graph capture failed: ") +
+                                    cudaGetErrorString(err != cudaSuccess ? err : e2));
+  }
+  cudaGraphExec_t ex = nullptr;
+  cudaError_t e3 = cudaGraphInstantiate(&ex, g, 0);
+  cudaGraphDestroy(g);
+  if (e3 != cudaSuccess) return fail(ctx, PB2_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e3));
+  b->graphs[key] = ex;
+  *out = ex;
+  return PB2_OK;
+}
+
+extern "C" int pb2_langevin_init(pb2_batch *b, void *stream) {
+  if (!b) return PB2_EINVAL;
+  pb2_ctx *ctx = b->ctx;
+  cudaStream_t st = (cudaStream_t)stream;
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  CUDA_TRY(ctx, launch_init(int_args(b, b->key_parity, 0), st));
+  b->key_parity ^= 1;
+  int rc = fresh_forces(b, st, false);
+  if (rc) return rc;
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  return PB2_OK;
+}
+
+extern "C" int pb2_langevin_run(pb2_batch *b, int32_t n_steps, void *stream) {
+  if (!b || n_steps < 0) return PB2_EINVAL;
+  pb2_ctx *ctx = b->ctx;
+  cudaStream_t st = (cudaStream_t)stream;
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  if (n_steps == 0) return PB2_OK;
+  if (b->profiling) {
+    for (double &t : b->timings) t = 0.0;
+    CUDA_TRY(ctx, cudaEventRecord(b->ev[0], st));
+    int rc = run_eager(b, n_steps, st);
+    if (rc) return rc;
+    CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    return PB2_OK;
+  }
+  const int chunk = b->params.graph_chunk;
+  int done = 0;
+  while (done < n_steps) {
+    const int c = std::min(chunk, n_steps - done);
+    cudaGraphExec_t ex;
+    int rc = get_graph(b, c, b->key_parity, &ex);
+    if (rc) return rc;
+    CUDA_TRY(ctx, cudaGraphLaunch(ex, st));
+    b->key_parity ^= (c & 1);
+    done += c;
+  }
+  return PB2_OK;
+}
+
+extern "C" int pb2_get_state(pb2_batch *b, double *x, double *p, double *f, uint32_t *keys,
+                             int64_t *steps, void *stream) {
+  if (!b) return PB2_EINVAL;
+  pb2_ctx *ctx = b->ctx;
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc;
+  if (x && (rc = download_soa3(b, x, b->x, b->y, b->z, st))) return rc;
+  if (p && (rc = download_soa3(b, p, b->px, b->py, b->pz, st))) return rc;
+  if (f && (rc = copy_forces(b, f, st))) return rc;
+  if (keys) {
+    CUDA_TRY(ctx, cudaMemcpyAsync(keys, b->keys + (size_t)b->key_parity * b->n_sys * 2,
+                                  (size_t)b->n_sys * 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  }
+  if (steps) {
+    std::vector<long long> h(b->n_sys);
+    CUDA_TRY(ctx, cudaMemcpyAsync(h.data(), b->steps, h.size() * sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    for (int s = 0; s < b->n_sys; ++s) steps[s] = h[s];
+  }
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  return PB2_OK;
+}
+
+extern "C" int pb2_set_state(pb2_batch *b, const double *x, const double *p, const uint32_t *keys,
+                             void *stream) {
+  if (!b) return PB2_EINVAL;
+  pb2_ctx *ctx = b->ctx;
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc;
+  if (x && (rc = upload_soa3(b, x, b->x, b->y, b->z, st))) return rc;
+  if (p && (rc = upload_soa3(b, p, b->px, b->py, b->pz, st))) return rc;
+  if (keys) {
+    CUDA_TRY(ctx, cudaMemcpyAsync(b->keys + (size_t)b->key_parity * b->n_sys * 2, keys,
+                                  (size_t)b->n_sys * 2 * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  }
+  if (x) {  // forces must follow the positions
+    rc = fresh_forces(b, st, false);
+    if (rc) return rc;
+    CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  }
+  return PB2_OK;
+}
+
+extern "C" int pb2_get_status(pb2_batch *b, uint32_t *status, int clear, void *stream) {
+  if (!b || !status) return PB2_EINVAL;
+  pb2_ctx *ctx = b->ctx;
+  cudaStream_t st = (cudaStream_t)stream;
+  CUDA_TRY(ctx, cudaMemcpyAsync(status, b->status, b->n_sys * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  if (clear) CUDA_TRY(ctx, cudaMemsetAsync(b->status, 0, b->n_sys * sizeof(uint32_t), st));
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  return PB2_OK;
+}
+
+extern "C" int pb2_set_profiling(pb2_batch *b, int enable) {
+  if (!b) return PB2_EINVAL;
+  b->profiling = enable != 0;
+  return PB2_OK;
+}
+
+extern "C" int pb2_last_timings(pb2_batch *b, double *out_ms) {
+  if (!b || !out_ms) return PB2_EINVAL;
+  for (int k = 0; k < 5; ++k) out_ms[k] = b->timings[k];
+  return PB2_OK;
+}
+
+// Neighbour-list entry points: the list is built in pb2_nlist.cu.

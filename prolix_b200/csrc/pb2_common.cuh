@@ -1,0 +1,78 @@
+// Shared device-side definitions: batch layout in HBM, fixed-point
+// accumulation, and launch helpers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "prolix_b200.h"
+
+namespace pb2 {
+
+constexpr int kWarp = 32;
+constexpr unsigned kFull = 0xffffffffu;
+
+// Fixed-point scales.  Forces, dE/dB and energies use 2^32 (range +-2.1e9,
+// resolution 2.3e-10); the descreening sums use 2^40 (range +-8.4e6).
+constexpr double kForceScale = 4294967296.0;
+constexpr double kForceInv = 1.0 / 4294967296.0;
+constexpr double kBornScale = 1099511627776.0;
+constexpr double kBornInv = 1.0 / 1099511627776.0;
+constexpr double kFixMax = 9.0e18;  // below 2^63: values beyond are flagged
+
+// OBC II constants (prolix physics/generalized_born.py:18-21) and ACE
+// constants (:628-647).
+constexpr double kObcAlpha = 1.0, kObcBeta = 0.8, kObcGamma = 4.85;
+constexpr double kDielOffset = 0.09;
+constexpr double kAceCoeff = 28.3919551, kKjToKcal = 0.239006;
+
+constexpr int kExclPerBlock = 8;  // distinct j-blocks with exclusions per i-block
+
+// Per-system constants, one 128-byte record per system.  Pair kernels see
+// positions relative to the system origin (its initial centroid), which keeps
+// float32 coordinates small.
+struct SysInfo {
+  int32_t n;          // atoms
+  int32_t off;        // first atom in the batch arrays
+  int32_t nblk;       // 32-atom blocks
+  int32_t blk_base;   // first block in the batch-wide block numbering
+  float pref;         // P = -0.5 k_gb (1/eps_in - 1/eps_out)
+  float kcoul;        // direct Coulomb constant
+  float lj14, coul14; // 1-4 scales
+  float cutoff2;      // 0: all pairs
+  int32_t nl_off;     // first row of this system in the neighbour arrays
+  int32_t pad0, pad1;
+  double pref_d;      // P in double (self / energy terms)
+  double dt, half_dt; // tau
+  double c1, c2;      // exp(-gamma dt), sqrt(1 - c1^2)
+  double kT;
+  double skin_half2;  // (skin/2)^2
+  double ox, oy, oz;  // origin subtracted before the float32 pair kernels
+};
+static_assert(sizeof(SysInfo) == 128, "SysInfo layout");
+
+// Work item of the tile kernels: tiles (iblk, jb) for jb in [jb0, jb1) of
+// system sys.  Block indices are local to the system.
+struct TileItem {
+  int32_t sys, iblk, jb0, jb1;
+};
+
+// Exclusion masks of one (i-block, j-block) tile: per i row, bit c set when
+// (row, col c) is excluded (1-2/1-3) or 1-4 scaled.
+struct ExclRow {
+  uint32_t excl, s14;
+};
+
+// Fixed-point helpers.  Conversion rounds to nearest; out-of-range values
+// saturate in the hardware conversion and are flagged by the integrator.
+__device__ __forceinline__ long long to_fix(double v, double scale) {
+  return __double2ll_rn(v * scale);
+}
+__device__ __forceinline__ long long to_fix_f(float v, float scale) {
+  return __float2ll_rn(v * scale);
+}
+__device__ __forceinline__ void atomic_add_fix(long long *addr, long long v) {
+  atomicAdd(reinterpret_cast<unsigned long long *>(addr), static_cast<unsigned long long>(v));
+}
+
+}  // namespace pb2

@@ -1,0 +1,87 @@
+// Argument records and launchers of the device kernels (shared by the
+// kernel translation units and the C ABI).
+#pragma once
+
+#include "pb2_common.cuh"
+
+namespace pb2 {
+
+enum { PASS_BORN = 0, PASS_FORCE = 1, PASS_CHAIN = 2 };
+struct PairArgs {
+  const SysInfo *sys;
+  const TileItem *items;
+  int32_t n_items;
+  uint32_t terms;
+  const int2 *excl_ent;
+  const ExclRow *excl_rows;
+  const float4 *posq;
+  const float4 *par;
+  const float4 *born;
+  long long *born_acc;
+  long long *dedb_acc;
+  long long *fx, *fy, *fz;
+  long long *energy;
+};
+struct FinalizeArgs {
+  const SysInfo *sys;
+  const int32_t *atom_sys;
+  const double *radius;
+  const double *charge;
+  long long *born_acc;
+  float4 *born;
+  long long *dedb_acc;
+  long long *energy;
+  int32_t n_total;
+  int32_t energy_mode;
+};
+struct BondedArgs {
+  const int32_t *atom_sys;
+  const double *x, *y, *z;
+  long long *fx, *fy, *fz;
+  long long *energy;
+  int32_t energy_mode;
+  uint32_t terms;
+  int32_t n_bond;
+  const int2 *bond_idx;
+  const double2 *bond_par;
+  int32_t n_angle;
+  const int4 *angle_idx;
+  const double2 *angle_par;
+  int32_t n_tors;
+  const int4 *tors_idx;
+  const double4 *tors_par;
+  int32_t n_cmap;
+  const int32_t *cmap_idx;
+  const double *cmap_coeff;
+  const int32_t *cmap_grid;
+  const int64_t *cmap_map_off;
+};
+struct IntArgs {
+  const SysInfo *sys;
+  const int32_t *atom_sys;
+  double *x, *y, *z;
+  double *px, *py, *pz;
+  long long *fx, *fy, *fz;
+  const double *mass;
+  const double *sigma;
+  const double *charge;
+  float4 *posq;
+  uint32_t *keys;
+  long long *steps;
+  uint32_t *status;
+  int32_t n_total;
+  int32_t n_sys;
+  int32_t parity;
+  int32_t finish_prev;
+  int32_t partitionable;
+};
+cudaError_t launch_tiles(int pass, bool energy, const PairArgs &a, int grid, cudaStream_t st);
+cudaError_t launch_born_finalize(const FinalizeArgs &a, cudaStream_t st);
+int tile_kernel_occupancy(int pass, bool energy);
+cudaError_t launch_bonded(const BondedArgs &a, int grid_cap, cudaStream_t st);
+cudaError_t launch_step(const IntArgs &a, cudaStream_t st);
+cudaError_t launch_finish(const IntArgs &a, cudaStream_t st);
+cudaError_t launch_init(const IntArgs &a, cudaStream_t st);
+cudaError_t launch_posq(const IntArgs &a, cudaStream_t st);
+
+}  // namespace pb2

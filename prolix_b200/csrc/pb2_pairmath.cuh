@@ -1,0 +1,93 @@
+// FP32 pair arithmetic of the OBC2 descreening integral.
+//
+// I(r; rho, s) follows prolix physics/generalized_born.py:211-263 (OpenMM's
+// CustomGBForce OBC2 form): L = max(rho, |r - s|), U = r + s,
+//   I = 1/2 (1/L - 1/U) + 1/4 ln(L/U)/r + 1/8 (r - s^2/r)(1/U^2 - 1/L^2),
+// zero unless r + s > rho, with floors of 1e-4 on L, U and r.
+//
+// Far field.  When r - s >= rho (so L = r - s) the expression simplifies,
+// with t = s/r, to I = (1/(2r)) (t/(1 - t^2) - atanh t), whose Taylor series
+//   I = (t^3 / r) sum_{k>=1} k/(2k+1) t^(2k-2),
+//   dI/dr = -(t^3 / r^2) sum_{k>=1} 2k(k+1)/(2k+1) t^(2k-2)
+// has only positive terms.  For t^2 <= 0.09 nine terms leave a relative
+// truncation error below 1e-9, and the series avoids both the logarithm and
+// the cancellation between the O(1/r) terms of the closed form (whose sum is
+// O(s^3/r^4)).  Nearer pairs use the closed form with an accurate logf.
+#pragma once
+
+namespace pb2 {
+
+constexpr float kSeriesU = 0.09f;
+
+__device__ __forceinline__ float obc_series_val(float u) {
+  // sum_{k=1..9} k/(2k+1) u^(k-1)
+  float p = 9.0f / 19.0f;
+  p = fmaf(p, u, 8.0f / 17.0f);
+  p = fmaf(p, u, 7.0f / 15.0f);
+  p = fmaf(p, u, 6.0f / 13.0f);
+  p = fmaf(p, u, 5.0f / 11.0f);
+  p = fmaf(p, u, 4.0f / 9.0f);
+  p = fmaf(p, u, 3.0f / 7.0f);
+  p = fmaf(p, u, 2.0f / 5.0f);
+  p = fmaf(p, u, 1.0f / 3.0f);
+  return p;
+}
+
+__device__ __forceinline__ float obc_series_der(float u) {
+  // sum_{k=1..9} 2k(k+1)/(2k+1) u^(k-1)
+  float p = 180.0f / 19.0f;
+  p = fmaf(p, u, 144.0f / 17.0f);
+  p = fmaf(p, u, 112.0f / 15.0f);
+  p = fmaf(p, u, 84.0f / 13.0f);
+  p = fmaf(p, u, 60.0f / 11.0f);
+  p = fmaf(p, u, 40.0f / 9.0f);
+  p = fmaf(p, u, 24.0f / 7.0f);
+  p = fmaf(p, u, 12.0f / 5.0f);
+  p = fmaf(p, u, 4.0f / 3.0f);
+  return p;
+}
+
+// I(r; rho, s).  inv_r = 1/r (already available to every caller).
+__device__ __forceinline__ float obc_integral(float r, float inv_r, float rho, float s) {
+  if (!(r + s > rho)) return 0.0f;
+  const float t = s * inv_r;
+  const float u = t * t;
+  if (u <= kSeriesU && r - s >= rho) return t * u * inv_r * obc_series_val(u);
+  const float rs = fmaxf(r, 1e-4f);
+  const float irs = 1.0f / rs;
+  const float L = fmaxf(fmaxf(rho, fabsf(r - s)), 1e-4f);
+  const float U = fmaxf(r + s, 1e-4f);
+  const float il = 1.0f / L, iu = 1.0f / U;
+  const float lg = logf(L * iu);
+  return 0.5f * (il - iu) + 0.25f * lg * irs + 0.125f * (r - s * s * irs) * (iu * iu - il * il);
+}
+
+// dI/dr(r; rho, s).
+__device__ __forceinline__ float obc_integral_dr(float r, float inv_r, float rho, float s) {
+  if (!(r + s > rho)) return 0.0f;
+  const float t = s * inv_r;
+  const float u = t * t;
+  if (u <= kSeriesU && r - s >= rho) return -t * u * inv_r * inv_r * obc_series_der(u);
+  const float rs = fmaxf(r, 1e-4f);
+  const float drs = r > 1e-4f ? 1.0f : 0.0f;
+  const float irs = 1.0f / rs;
+  const float d = fabsf(r - s);
+  const bool use_d = d > rho;
+  const float Lraw = use_d ? d : rho;
+  const float L = fmaxf(Lraw, 1e-4f);
+  const float dL = (use_d && Lraw > 1e-4f) ? copysignf(1.0f, r - s) : 0.0f;
+  const float Uraw = r + s;
+  const float U = fmaxf(Uraw, 1e-4f);
+  const float dU = Uraw > 1e-4f ? 1.0f : 0.0f;
+  const float il = 1.0f / L, iu = 1.0f / U;
+  const float lg = logf(L * iu);
+  const float t1 = 0.5f * (-dL * il * il + dU * iu * iu);
+  const float t2 = 0.25f * ((dL * il - dU * iu) * irs - lg * drs * irs * irs);
+  const float a = r - s * s * irs;
+  const float da = 1.0f + s * s * drs * irs * irs;
+  const float b = iu * iu - il * il;
+  const float db = -2.0f * dU * iu * iu * iu + 2.0f * dL * il * il * il;
+  return t1 + t2 + 0.125f * (da * b + a * db);
+}
+
+}  // namespace pb2

@@ -1,0 +1,304 @@
+"""Device-resident ragged batch of implicit-solvent systems (host wrapper of
+the C ABI).
+
+A ``Batch`` holds any number of systems of any sizes; one force evaluation
+or one Langevin step advances all of them with one launch per kernel.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+import threading
+
+import numpy as np
+
+from . import _lib, topology
+
+AKMA_TIME_FS = 48.88821291839  # prolix simulate.py:56
+KB_KCAL = 0.0019872041          # prolix simulate.py:57
+K_COULOMB = 332.0637            # prolix physics/system.py:135
+
+
+def akma_dt(dt_fs: float) -> float:
+  return dt_fs / AKMA_TIME_FS
+
+
+def akma_gamma(gamma_per_ps: float) -> float:
+  return gamma_per_ps * AKMA_TIME_FS * 1e-3
+
+
+class Context:
+  """One CUDA device.  Contexts are shared per device within a process."""
+
+  _cache: dict[int, "Context"] = {}
+  _lock = threading.Lock()
+
+  def __init__(self, device: int = 0):
+    self.lib = _lib.load()
+    h = ctypes.c_void_p()
+    rc = self.lib.pb2_ctx_create(int(device), ctypes.byref(h))
+    if rc != _lib.PB2_OK:
+      raise _lib.PB2Error(rc, f"cannot open device {device} (an sm_100 GPU is required)")
+    self.handle = h
+    self.device = device
+
+  @classmethod
+  def get(cls, device: int = 0) -> "Context":
+    with cls._lock:
+      if device not in cls._cache:
+        cls._cache[device] = Context(device)
+      return cls._cache[device]
+
+  def check(self, rc: int):
+    if rc != _lib.PB2_OK:
+      msg = self.lib.pb2_last_error(self.handle)
+      raise _lib.PB2Error(rc, msg.decode() if msg else "")
+
+
+def _f64(a, shape=None):
+  a = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+  if shape is not None:
+    a = a.reshape(shape)
+  return a
+
+
+def _i32(a, shape=None):
+  a = np.ascontiguousarray(np.asarray(a, dtype=np.int32))
+  if shape is not None:
+    a = a.reshape(shape)
+  return a
+
+
+def _dp(a):
+  return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _ip(a):
+  return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+
+
+def prepare_system(system: dict, *, dt=None, kT=None, gamma=None, key=None, eps_in=1.0,
+                   eps_out=78.5, k_gb=K_COULOMB, k_coulomb=K_COULOMB,
+                   lj14=topology.LJ14_DEFAULT, coul14=topology.COUL14_DEFAULT):
+  """Normalise a system dict into the arrays of one ``pb2_system_desc``."""
+  pos = _f64(system["positions"])
+  n = pos.reshape(-1, 3).shape[0]
+  pos = pos.reshape(n, 3)
+  out = {"n": n, "positions": pos}
+  for k in ("charges", "sigmas", "epsilons", "radii", "scaled_radii", "masses"):
+    if k not in system and k == "masses":
+      out[k] = np.ones(n)
+      continue
+    out[k] = _f64(system[k], (n,))
+  bonds = _i32(system.get("bonds", np.zeros((0, 2))), (-1, 2))
+  out["bonds"] = bonds
+  out["bond_params"] = _f64(system.get("bond_params", np.zeros((0, 2))), (-1, 2))
+  out["angles"] = _i32(system.get("angles", np.zeros((0, 3))), (-1, 3))
+  out["angle_params"] = _f64(system.get("angle_params", np.zeros((0, 2))), (-1, 2))
+  dih = system.get("dihedrals", system.get("proper_dihedrals"))
+  dih = _i32(np.zeros((0, 4)) if dih is None else dih, (-1, 4))
+  dp = system.get("dihedral_params", system.get("proper_dihedral_params"))
+  dp = np.zeros((0, 1, 3)) if dp is None else np.asarray(dp, dtype=np.float64)
+  if dp.ndim == 2:
+    dp = dp[:, None, :]
+  out["dihedrals"] = dih
+  out["dihedral_params"] = _f64(dp).reshape(dih.shape[0], -1, 3) if dih.shape[0] else np.zeros((0, 1, 3))
+  if "cmap_torsions" in system and len(system["cmap_torsions"]):
+    grids = np.asarray(system["cmap_energy_grids"], dtype=np.float64)
+    if grids.ndim == 2:
+      grids = grids[None]
+    out["cmap_rows"] = _i32(system["cmap_torsions"], (-1, 5))
+    out["cmap_map"] = _i32(system.get("cmap_indices", np.zeros(out["cmap_rows"].shape[0])))
+    out["cmap_coeffs"] = _f64(np.stack([topology.cmap_coefficients(g) for g in grids]))
+    out["cmap_grid"] = grids.shape[1]
+  else:
+    out["cmap_rows"] = np.zeros((0, 5), np.int32)
+    out["cmap_map"] = np.zeros(0, np.int32)
+    out["cmap_coeffs"] = np.zeros((1, 1, 1, 16))
+    out["cmap_grid"] = 1
+  if "excl_pairs" in system:
+    out["excl_pairs"] = _i32(system["excl_pairs"], (-1, 2))
+    out["excl_kind"] = _i32(system["excl_kind"])
+  else:
+    out["excl_pairs"], out["excl_kind"] = topology.exclusion_pairs(bonds, n)
+  out["scal"] = dict(lj14=float(system.get("lj14_scale", lj14)),
+                     coul14=float(system.get("coul14_scale", coul14)),
+                     eps_in=float(system.get("solute_dielectric", eps_in)),
+                     eps_out=float(system.get("solvent_dielectric", eps_out)),
+                     k_gb=float(k_gb), k_coulomb=float(k_coulomb))
+  k = system.get("key", key)
+  if k is None:
+    k = (0, int(system.get("seed", 0)) & 0xFFFFFFFF)
+  out["key"] = tuple(int(v) & 0xFFFFFFFF for v in np.asarray(k).reshape(2))
+  out["dt"] = float(system.get("dt", dt if dt is not None else akma_dt(1.0)))
+  out["kT"] = float(system.get("kT", kT if kT is not None else 300.0 * KB_KCAL))
+  out["gamma"] = float(system.get("gamma", gamma if gamma is not None else akma_gamma(1.0)))
+  return out
+
+
+def _desc(p) -> _lib.SystemDesc:
+  d = _lib.SystemDesc()
+  d.n_atoms = p["n"]
+  d.positions = _dp(p["positions"])
+  for k in ("charges", "sigmas", "epsilons", "radii", "scaled_radii", "masses"):
+    setattr(d, k, _dp(p[k]))
+  d.n_bonds = p["bonds"].shape[0]
+  d.bonds, d.bond_params = _ip(p["bonds"]), _dp(p["bond_params"])
+  d.n_angles = p["angles"].shape[0]
+  d.angles, d.angle_params = _ip(p["angles"]), _dp(p["angle_params"])
+  d.n_torsions = p["dihedrals"].shape[0]
+  d.n_torsion_terms = p["dihedral_params"].shape[1] if d.n_torsions else 1
+  d.torsions, d.torsion_params = _ip(p["dihedrals"]), _dp(p["dihedral_params"])
+  d.n_cmap = p["cmap_rows"].shape[0]
+  d.cmap_rows, d.cmap_map = _ip(p["cmap_rows"]), _ip(p["cmap_map"])
+  d.n_cmap_maps = p["cmap_coeffs"].shape[0]
+  d.cmap_grid = p["cmap_grid"]
+  d.cmap_coeffs = _dp(p["cmap_coeffs"])
+  d.n_excl = p["excl_pairs"].shape[0]
+  d.excl_pairs, d.excl_kind = _ip(p["excl_pairs"]), _ip(p["excl_kind"])
+  s = p["scal"]
+  d.lj14_scale, d.coul14_scale = s["lj14"], s["coul14"]
+  d.eps_in, d.eps_out = s["eps_in"], s["eps_out"]
+  d.k_gb, d.k_coulomb = s["k_gb"], s["k_coulomb"]
+  d.key[0], d.key[1] = p["key"]
+  d.dt, d.kT, d.gamma = p["dt"], p["kT"], p["gamma"]
+  return d
+
+
+class Batch:
+  """A ragged batch of systems resident on one GPU."""
+
+  def __init__(self, systems, *, cutoff=0.0, skin=2.0, terms=_lib.USE_ALL, device=0,
+               tile_segment=0, graph_chunk=50, partitionable_keys=True, nl_capacity=0,
+               **system_defaults):
+    if isinstance(systems, dict):
+      systems = [systems]
+    if not systems:
+      raise ValueError("a batch needs at least one system")
+    self.ctx = Context.get(device)
+    self.lib = self.ctx.lib
+    self.prepared = [prepare_system(s, **system_defaults) for s in systems]
+    self.sizes = np.array([p["n"] for p in self.prepared], dtype=np.int64)
+    self.offsets = np.concatenate([[0], np.cumsum(self.sizes)])
+    self.n_systems = len(self.prepared)
+    self.n_atoms = int(self.offsets[-1])
+    self.cutoff = float(cutoff)
+    descs = (_lib.SystemDesc * self.n_systems)(*[_desc(p) for p in self.prepared])
+    rp = _lib.RunParams(terms=int(terms), cutoff=float(cutoff), skin=float(skin),
+                        nl_capacity=int(nl_capacity), tile_segment=int(tile_segment),
+                        graph_chunk=int(graph_chunk),
+                        partitionable_keys=1 if partitionable_keys else 0)
+    h = ctypes.c_void_p()
+    self.ctx.check(self.lib.pb2_batch_create(self.ctx.handle, self.n_systems, descs,
+                                             ctypes.byref(rp), ctypes.byref(h)))
+    self.handle = h
+    self._stream = None
+
+  # ---------------------------------------------------------------- helpers
+  def _check(self, rc):
+    self.ctx.check(rc)
+
+  def split(self, flat):
+    """Split a batch-order (n_atoms, ...) array into per-system arrays."""
+    return [flat[self.offsets[s]:self.offsets[s + 1]] for s in range(self.n_systems)]
+
+  def close(self):
+    if getattr(self, "handle", None):
+      self.lib.pb2_batch_destroy(self.handle)
+      self.handle = None
+
+  def __del__(self):
+    try:
+      self.close()
+    except Exception:
+      pass
+
+  def __enter__(self):
+    return self
+
+  def __exit__(self, *exc):
+    self.close()
+
+  # ---------------------------------------------------------------- physics
+  def energy_forces(self, stream=None):
+    """(energies (n_systems, 9) with columns TERM_NAMES, forces (n_atoms, 3))."""
+    e = np.zeros((self.n_systems, _lib.NTERMS))
+    f = np.zeros((self.n_atoms, 3))
+    self._check(self.lib.pb2_energy_forces(self.handle, e.ctypes.data, f.ctypes.data, stream))
+    return e, f
+
+  def forces(self, stream=None):
+    f = np.zeros((self.n_atoms, 3))
+    self._check(self.lib.pb2_energy_forces(self.handle, None, f.ctypes.data, stream))
+    return f
+
+  def born_radii(self, stream=None):
+    b = np.zeros(self.n_atoms)
+    self._check(self.lib.pb2_born_radii(self.handle, b.ctypes.data, stream))
+    return b
+
+  def set_positions(self, positions, stream=None):
+    x = _f64(positions, (self.n_atoms, 3))
+    self._check(self.lib.pb2_set_positions(self.handle, x.ctypes.data, stream))
+
+  def langevin_init(self, stream=None):
+    self._check(self.lib.pb2_langevin_init(self.handle, stream))
+
+  def langevin_run(self, n_steps, stream=None):
+    self._check(self.lib.pb2_langevin_run(self.handle, int(n_steps), stream))
+
+  def get_state(self, stream=None):
+    x = np.zeros((self.n_atoms, 3))
+    p = np.zeros((self.n_atoms, 3))
+    f = np.zeros((self.n_atoms, 3))
+    k = np.zeros((self.n_systems, 2), dtype=np.uint32)
+    st = np.zeros(self.n_systems, dtype=np.int64)
+    self._check(self.lib.pb2_get_state(self.handle, x.ctypes.data, p.ctypes.data, f.ctypes.data,
+                                       k.ctypes.data, st.ctypes.data, stream))
+    return {"position": x, "momentum": p, "force": f, "key": k, "step": st}
+
+  def set_state(self, position=None, momentum=None, key=None, stream=None):
+    x = None if position is None else _f64(position, (self.n_atoms, 3))
+    p = None if momentum is None else _f64(momentum, (self.n_atoms, 3))
+    k = None if key is None else np.ascontiguousarray(np.asarray(key, dtype=np.uint32).reshape(-1, 2))
+    self._check(self.lib.pb2_set_state(self.handle, None if x is None else x.ctypes.data,
+                                       None if p is None else p.ctypes.data,
+                                       None if k is None else k.ctypes.data, stream))
+
+  def status(self, clear=False, stream=None):
+    s = np.zeros(self.n_systems, dtype=np.uint32)
+    self._check(self.lib.pb2_get_status(self.handle, s.ctypes.data, 1 if clear else 0, stream))
+    return s
+
+  def set_profiling(self, enable: bool):
+    self._check(self.lib.pb2_set_profiling(self.handle, 1 if enable else 0))
+
+  def last_timings(self):
+    t = np.zeros(5)
+    self._check(self.lib.pb2_last_timings(self.handle, t.ctypes.data))
+    return t
+
+  # neighbour list
+  def nl_build(self, stream=None):
+    self._check(self.lib.pb2_nl_build(self.handle, stream))
+
+  def nl_check(self, stream=None) -> int:
+    r = ctypes.c_int32(0)
+    self._check(self.lib.pb2_nl_check(self.handle, ctypes.byref(r), stream))
+    return int(r.value)
+
+  def nl_capacity(self) -> int:
+    c = ctypes.c_int32(0)
+    self._check(self.lib.pb2_nl_capacity(self.handle, ctypes.byref(c)))
+    return int(c.value)
+
+  def nl_get(self, stream=None):
+    k = self.nl_capacity()
+    out = np.zeros((self.n_atoms, k), dtype=np.int32)
+    self._check(self.lib.pb2_nl_get(self.handle, out.ctypes.data, stream))
+    return out
+
+
+def term_dict(row) -> dict:
+  return {name: float(row[i]) for i, name in enumerate(_lib.TERM_NAMES)}

@@ -1,0 +1,130 @@
+"""Host-side logic and the C ABI library surface (no GPU calls)."""
+
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import bonded as obonded
+from oracle import topology as otopo
+from prolix_b200 import _build, _lib, engine, synth, topology
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def header_symbols():
+  text = (ROOT / "include" / "prolix_b200.h").read_text()
+  return sorted(set(re.findall(r"\b(pb2_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+  lib = _lib.load()
+  declared = header_symbols()
+  assert len(declared) >= 20
+  for name in declared:
+    assert hasattr(lib, name), name
+  bound = {name for name, _, _ in _lib.SIGNATURES}
+  assert set(declared) <= bound | {"pb2_ctx_create"}
+  assert lib.pb2_abi_version() == 1
+
+
+def _struct_fields(text, name):
+  body = text[text.index("typedef struct " + name):text.index("} " + name + ";")]
+  body = body[body.index("{") + 1:]
+  body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+  out = []
+  for decl in body.split(";"):
+    decl = decl.strip()
+    if not decl:
+      continue
+    head, *rest = decl.split(",")
+    names = [head.split()[-1]] + [r.strip() for r in rest]
+    out.extend(n.lstrip("*").split("[")[0] for n in names)
+  return out
+
+
+def test_ctypes_struct_layout_matches_header():
+  text = (ROOT / "include" / "prolix_b200.h").read_text()
+  assert _struct_fields(text, "pb2_system_desc") == [f[0] for f in _lib.SystemDesc._fields_]
+  assert _struct_fields(text, "pb2_run_params") == [f[0] for f in _lib.RunParams._fields_]
+
+
+def test_no_device_reports_enodev():
+  lib = _lib.load()
+  h = ctypes.c_void_p()
+  try:
+    import torch
+    has_gpu = torch.cuda.is_available()
+  except Exception:
+    has_gpu = False
+  if has_gpu:
+    pytest.skip("a GPU is present")
+  assert lib.pb2_ctx_create(0, ctypes.byref(h)) == -7
+
+
+def test_synth_is_seed_deterministic():
+  a = synth.make_chain(300, 17, compact=True, cmap=True)
+  b = synth.make_chain(300, 17, compact=True, cmap=True)
+  for k in a:
+    np.testing.assert_array_equal(np.asarray(a[k]), np.asarray(b[k]))
+  c = synth.make_chain(300, 18, compact=True)
+  assert not np.array_equal(a["positions"], c["positions"])
+  assert abs(a["charges"].sum()) < 1e-12
+
+
+def test_synth_distributions_and_geometry():
+  s = synth.make_chain(2500, 3, compact=True)
+  n = 2500
+  assert s["positions"].shape == (n, 3)
+  assert (s["sigmas"] >= 1.0).all() and (s["sigmas"] <= 3.4).all()
+  assert (s["epsilons"] >= 0.01).all() and (s["epsilons"] <= 0.2).all()
+  assert (s["radii"] >= 1.2).all() and (s["radii"] <= 1.9).all()
+  sf = s["scaled_radii"] / s["radii"]
+  assert (sf >= 0.72).all() and (sf <= 0.85).all()
+  d = np.linalg.norm(np.diff(s["positions"], axis=0), axis=1)
+  np.testing.assert_allclose(d, s["bond_params"][:, 0], rtol=1e-9)
+  assert (d >= 1.0).all() and (d <= 1.53).all()
+  r = np.linalg.norm(s["positions"], axis=1)
+  assert r.max() < 1.5 * synth.globule_radius(n)
+  from scipy.spatial import cKDTree
+  pairs = cKDTree(s["positions"]).query_pairs(2.5, output_type="ndarray")
+  assert np.all(np.abs(pairs[:, 0] - pairs[:, 1]) < 3)
+
+
+def test_batch_sizes_log_uniform():
+  sizes = synth.batch_sizes(512, 2024)
+  assert sizes.min() >= 150 and sizes.max() <= 4000
+  assert 900 < sizes.mean() < 1500
+
+
+def test_exclusions_match_oracle_rule():
+  s = synth.make_chain(80, 2)
+  pairs, kind = topology.exclusion_pairs(s["bonds"], 80)
+  p12, p13, p14 = otopo.bonded_pairs(s["bonds"], 80)
+  assert len(pairs) == len(p12) + len(p13) + len(p14)
+  assert (kind == 1).sum() == len(p14)
+
+
+def test_cmap_coefficients_match_oracle():
+  g = np.random.default_rng(9).uniform(-2, 2, size=(24, 24))
+  np.testing.assert_allclose(topology.cmap_coefficients(g), obonded.cmap_coefficients(g),
+                             atol=1e-12)
+
+
+def test_prepare_system_defaults_and_units():
+  s = synth.make_chain(40, 1)
+  p = engine.prepare_system(s)
+  assert p["dt"] == pytest.approx(1.0 / 48.88821291839)
+  assert p["kT"] == pytest.approx(300 * 0.0019872041)
+  assert p["gamma"] == pytest.approx(1.0 * 48.88821291839e-3)
+  assert p["excl_pairs"].dtype == np.int32 and (p["excl_pairs"][:, 0] < p["excl_pairs"][:, 1]).all()
+  d = engine._desc(p)
+  assert d.n_atoms == 40 and d.n_bonds == 39 and d.n_torsion_terms == 1
+
+
+def test_build_flags_target_sm100a_only():
+  flags = " ".join(_build.NVCC_FLAGS)
+  assert "arch=compute_100a,code=sm_100a" in flags
+  assert "sm_90" not in flags
