@@ -64,6 +64,8 @@ struct pb2_batch {
   long long *fx = nullptr, *fy = nullptr, *fz = nullptr;
   double *mass = nullptr, *sigma = nullptr, *charge = nullptr, *radius = nullptr;
   float4 *posq = nullptr, *par = nullptr, *born = nullptr;
+  double *q64 = nullptr, *hs64 = nullptr, *se64 = nullptr, *ro64 = nullptr, *sr64 = nullptr;
+  double *born64 = nullptr;
   long long *born_acc = nullptr, *dedb_acc = nullptr, *energy = nullptr;
   uint32_t *keys = nullptr, *status = nullptr;
   long long *steps = nullptr;
@@ -73,8 +75,8 @@ struct pb2_batch {
   ExclRow *excl_rows = nullptr;
   BondedArgs bonded{};
   int key_parity = 0;
+  bool forces_valid = false;  // force accumulators hold F(x) of the current state
   int grid_pair[3] = {1, 1, 1};
-  int grid_pair_energy = 1;
   int grid_bonded = 1;
   cudaStream_t cap_stream = nullptr;
   std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
@@ -263,6 +265,7 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   b->n_total = N;
   std::vector<double> hx(N), hy(N), hz(N), hm(N), hsig(N), hq(N), hrad(N);
   std::vector<float4> hposq(N), hpar(N);
+  std::vector<double> hhs(N), hse(N), hro(N), hsr(N);
   std::vector<int32_t> hsys(N);
   std::vector<SysInfo> sinfo(n_systems);
   std::vector<uint32_t> hkeys(4 * (size_t)n_systems, 0u);
@@ -315,9 +318,11 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
                              (float)d.charges[i]);
       double ro = d.radii[i] - kDielOffset;
       if (cutoff_mode) ro = std::max(std::max(d.radii[i], 1e-6) - kDielOffset, 1e-4);
-      hpar[g] = make_float4((float)(0.5 * std::max(d.sigmas[i], 1e-6)),
-                            (float)std::sqrt(std::max(d.epsilons[i], 0.0)), (float)ro,
-                            (float)d.scaled_radii[i]);
+      hhs[g] = 0.5 * std::max(d.sigmas[i], 1e-6);
+      hse[g] = std::sqrt(std::max(d.epsilons[i], 0.0));
+      hro[g] = ro;
+      hsr[g] = d.scaled_radii[i];
+      hpar[g] = make_float4((float)hhs[g], (float)hse[g], (float)ro, (float)hsr[g]);
     }
     hkeys[2 * (size_t)s] = d.key[0];
     hkeys[2 * (size_t)s + 1] = d.key[1];
@@ -416,6 +421,12 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   b->posq = D.alloc<float4>(N);
   b->par = D.alloc<float4>(N);
   b->born = D.alloc<float4>(N);
+  b->q64 = D.alloc<double>(N);
+  b->hs64 = D.alloc<double>(N);
+  b->se64 = D.alloc<double>(N);
+  b->ro64 = D.alloc<double>(N);
+  b->sr64 = D.alloc<double>(N);
+  b->born64 = D.alloc<double>(N);
   b->born_acc = D.alloc<long long>(N);
   b->dedb_acc = D.alloc<long long>(N);
   b->energy = D.alloc<long long>((size_t)n_systems * PB2_NTERMS);
@@ -451,6 +462,9 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
       (rc = upload(ctx, b->mass, hm)) || (rc = upload(ctx, b->sigma, hsig)) ||
       (rc = upload(ctx, b->charge, hq)) || (rc = upload(ctx, b->radius, hrad)) ||
       (rc = upload(ctx, b->posq, hposq)) || (rc = upload(ctx, b->par, hpar)) ||
+      (rc = upload(ctx, b->q64, hq)) || (rc = upload(ctx, b->hs64, hhs)) ||
+      (rc = upload(ctx, b->se64, hse)) || (rc = upload(ctx, b->ro64, hro)) ||
+      (rc = upload(ctx, b->sr64, hsr)) ||
       (rc = upload(ctx, b->keys, hkeys)) || (rc = upload(ctx, b->items, hitems)) ||
       (rc = upload(ctx, b->excl_ent, hent)) || (rc = upload(ctx, b->excl_rows, hrows)) ||
       (rc = upload(ctx, d_bidx, bidx)) || (rc = upload(ctx, d_bpar, bpar)) ||
@@ -484,12 +498,8 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
 
   // launch shapes: persistent grids sized to the resident capacity
   for (int p = 0; p < 3; ++p) {
-    const int cap = tile_kernel_occupancy(p, false) * ctx->sm_count;
+    const int cap = tile_kernel_occupancy(p) * ctx->sm_count;
     b->grid_pair[p] = std::max(1, std::min(cap, (b->n_items + 7) / 8));
-  }
-  {
-    const int cap = tile_kernel_occupancy(PASS_FORCE, true) * ctx->sm_count;
-    b->grid_pair_energy = std::max(1, std::min(cap, (b->n_items + 7) / 8));
   }
   b->grid_bonded = 8 * ctx->sm_count;
   CUDA_TRY(ctx, cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking));
@@ -518,13 +528,14 @@ extern "C" int pb2_batch_info(const pb2_batch *b, int32_t *n_systems, int64_t *n
 // ------------------------------------------------------------ force evaluation
 
 // Force kernels on the current posq; force accumulators must be zero (or
-// hold contributions to keep) and born_acc zero.
-static cudaError_t enqueue_forces(pb2_batch *b, cudaStream_t st, bool energy) {
+// hold contributions to keep) and born_acc zero.  bonded_energy: also
+// accumulate the (FP64) bonded energies.
+static cudaError_t enqueue_forces(pb2_batch *b, cudaStream_t st, bool bonded_energy) {
   cudaError_t e;
   const PairArgs pa = pair_args(b);
   const bool gb = (b->params.terms & PB2_USE_GB) != 0;
   if (gb) {
-    if ((e = launch_tiles(PASS_BORN, false, pa, b->grid_pair[PASS_BORN], st)) != cudaSuccess) return e;
+    if ((e = launch_tiles(PASS_BORN, pa, b->grid_pair[PASS_BORN], st)) != cudaSuccess) return e;
     FinalizeArgs fa;
     fa.sys = b->sys;
     fa.atom_sys = b->atom_sys;
@@ -534,17 +545,53 @@ static cudaError_t enqueue_forces(pb2_batch *b, cudaStream_t st, bool energy) {
     fa.born = b->born;
     fa.dedb_acc = b->dedb_acc;
     fa.energy = b->energy;
+    fa.born64 = nullptr;
     fa.n_total = b->n_total;
-    fa.energy_mode = energy ? 1 : 0;
+    fa.energy_mode = 0;
     if ((e = launch_born_finalize(fa, st)) != cudaSuccess) return e;
   }
-  if ((e = launch_tiles(PASS_FORCE, energy, pa, energy ? b->grid_pair_energy : b->grid_pair[PASS_FORCE], st)) != cudaSuccess)
-    return e;
+  if ((e = launch_tiles(PASS_FORCE, pa, b->grid_pair[PASS_FORCE], st)) != cudaSuccess) return e;
   if (gb)
-    if ((e = launch_tiles(PASS_CHAIN, false, pa, b->grid_pair[PASS_CHAIN], st)) != cudaSuccess) return e;
+    if ((e = launch_tiles(PASS_CHAIN, pa, b->grid_pair[PASS_CHAIN], st)) != cudaSuccess) return e;
   BondedArgs ba = b->bonded;
-  ba.energy_mode = energy ? 1 : 0;
+  ba.energy_mode = bonded_energy ? 1 : 0;
   return launch_bonded(ba, b->grid_bonded, st);
+}
+
+// FP64 pair energies (GB polar incl. self, ACE, Coulomb, LJ) into b->energy.
+static cudaError_t enqueue_energy64(pb2_batch *b, cudaStream_t st) {
+  cudaError_t e;
+  Energy64Args ea;
+  ea.sys = b->sys;
+  ea.items = b->items;
+  ea.n_items = b->n_items;
+  ea.terms = b->params.terms;
+  ea.excl_ent = b->excl_ent;
+  ea.excl_rows = b->excl_rows;
+  ea.x = b->x; ea.y = b->y; ea.z = b->z;
+  ea.q = b->q64; ea.hs = b->hs64; ea.se = b->se64; ea.ro = b->ro64; ea.sr = b->sr64;
+  ea.born64 = b->born64;
+  ea.born_acc = b->born_acc;
+  ea.energy = b->energy;
+  const int grid = b->grid_pair[PASS_FORCE];
+  if (b->params.terms & PB2_USE_GB) {
+    if ((e = cudaMemsetAsync(b->born_acc, 0, (size_t)b->n_total * sizeof(long long), st)) != cudaSuccess) return e;
+    if ((e = launch_energy64(0, ea, grid, st)) != cudaSuccess) return e;
+    FinalizeArgs fa;
+    fa.sys = b->sys;
+    fa.atom_sys = b->atom_sys;
+    fa.radius = b->radius;
+    fa.charge = b->charge;
+    fa.born_acc = b->born_acc;
+    fa.born = b->born;
+    fa.dedb_acc = b->dedb_acc;
+    fa.energy = b->energy;
+    fa.born64 = b->born64;
+    fa.n_total = b->n_total;
+    fa.energy_mode = 1;
+    if ((e = launch_born_finalize(fa, st)) != cudaSuccess) return e;
+  }
+  return launch_energy64(1, ea, grid, st);
 }
 
 static int fresh_forces(pb2_batch *b, cudaStream_t st, bool energy) {
@@ -557,6 +604,8 @@ static int fresh_forces(pb2_batch *b, cudaStream_t st, bool energy) {
     CUDA_TRY(ctx, cudaMemsetAsync(b->energy, 0, (size_t)b->n_sys * PB2_NTERMS * sizeof(long long), st));
   CUDA_TRY(ctx, launch_posq(int_args(b, b->key_parity, 0), st));
   CUDA_TRY(ctx, enqueue_forces(b, st, energy));
+  if (energy) CUDA_TRY(ctx, enqueue_energy64(b, st));
+  b->forces_valid = true;
   return PB2_OK;
 }
 
@@ -642,6 +691,7 @@ static int download_soa3(pb2_batch *b, double *aos, const double *dx, const doub
 
 extern "C" int pb2_set_positions(pb2_batch *b, const double *positions, void *stream) {
   if (!b || !positions) return PB2_EINVAL;
+  b->forces_valid = false;
   return upload_soa3(b, positions, b->x, b->y, b->z, (cudaStream_t)stream);
 }
 
@@ -728,6 +778,10 @@ extern "C" int pb2_langevin_run(pb2_batch *b, int32_t n_steps, void *stream) {
   cudaStream_t st = (cudaStream_t)stream;
   CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   if (n_steps == 0) return PB2_OK;
+  if (!b->forces_valid) {
+    int rc = fresh_forces(b, st, false);
+    if (rc) return rc;
+  }
   if (b->profiling) {
     for (double &t : b->timings) t = 0.0;
     CUDA_TRY(ctx, cudaEventRecord(b->ev[0], st));

@@ -31,8 +31,22 @@ struct FinalizeArgs {
   float4 *born;
   long long *dedb_acc;
   long long *energy;
+  double *born64;   // NULL, or FP64 Born radii out
   int32_t n_total;
   int32_t energy_mode;
+};
+struct Energy64Args {
+  const SysInfo *sys;
+  const TileItem *items;
+  int32_t n_items;
+  uint32_t terms;
+  const int2 *excl_ent;
+  const ExclRow *excl_rows;
+  const double *x, *y, *z;
+  const double *q, *hs, *se, *ro, *sr;  // charge, sigma/2, sqrt(eps), rho~, scaled radius
+  const double *born64;
+  long long *born_acc;
+  long long *energy;
 };
 struct BondedArgs {
   const int32_t *atom_sys;
@@ -75,9 +89,10 @@ struct IntArgs {
   int32_t finish_prev;
   int32_t partitionable;
 };
-cudaError_t launch_tiles(int pass, bool energy, const PairArgs &a, int grid, cudaStream_t st);
+cudaError_t launch_tiles(int pass, const PairArgs &a, int grid, cudaStream_t st);
+cudaError_t launch_energy64(int pass, const Energy64Args &a, int grid, cudaStream_t st);
 cudaError_t launch_born_finalize(const FinalizeArgs &a, cudaStream_t st);
-int tile_kernel_occupancy(int pass, bool energy);
+int tile_kernel_occupancy(int pass);
 cudaError_t launch_bonded(const BondedArgs &a, int grid_cap, cudaStream_t st);
 cudaError_t launch_step(const IntArgs &a, cudaStream_t st);
 cudaError_t launch_finish(const IntArgs &a, cudaStream_t st);

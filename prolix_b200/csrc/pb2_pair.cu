@@ -29,13 +29,7 @@ __device__ __forceinline__ float shfl_next(float v, int lane) {
   return __shfl_sync(kFull, v, (lane + 1) & 31);
 }
 
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-  return v;
-}
-
-template <int PASS, bool ENERGY>
+template <int PASS>
 __global__ void __launch_bounds__(256) tile_kernel(const PairArgs a) {
   const int lane = threadIdx.x & 31;
   const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -69,7 +63,6 @@ __global__ void __launch_bounds__(256) tile_kernel(const PairArgs a) {
       ent = a.excl_ent[(S.blk_base + item.iblk) * kExclPerBlock + lane];
 
     long long ai0 = 0, ai1 = 0, ai2 = 0, ai3 = 0;  // i-side fixed-point sums
-    double e_gb = 0.0, e_coul = 0.0, e_lj = 0.0;
 
     for (int jb = item.jb0; jb < item.jb1; ++jb) {
       const int jl0 = jb * 32;
@@ -104,7 +97,6 @@ __global__ void __launch_bounds__(256) tile_kernel(const PairArgs a) {
 
       float ti0 = 0.f, ti1 = 0.f, ti2 = 0.f, ti3 = 0.f;  // i partials of this tile
       float tj0 = 0.f, tj1 = 0.f, tj2 = 0.f, tj3 = 0.f;  // j partials (rotate)
-      float te0 = 0.f, te1 = 0.f, te2 = 0.f;            // energy partials
 
 #pragma unroll 4
       for (int k = 0; k < 32; ++k) {
@@ -141,7 +133,6 @@ __global__ void __launch_bounds__(256) tile_kernel(const PairArgs a) {
               const float c = -pq * ex * fmaf(0.25f * r2, inv_d, 1.0f) * inv_f3;
               ti3 += c * bjB;
               tj3 += c * bi.x;
-              if (ENERGY) te0 += 2.0f * pq * inv_f;
             }
             const bool excluded = (exm >> jc) & 1u;
             if (!excluded && (use_lj || use_coul)) {
@@ -151,7 +142,6 @@ __global__ void __launch_bounds__(256) tile_kernel(const PairArgs a) {
               if (use_coul) {
                 const float ec = kcoul * qq * (is14 ? coul14 : 1.0f) * inv_r;
                 g += ec * inv_r2;
-                if (ENERGY) te1 += ec;
               }
               if (use_lj) {
                 const float sig = ci.x + cj.x;
@@ -159,7 +149,6 @@ __global__ void __launch_bounds__(256) tile_kernel(const PairArgs a) {
                 const float sr2 = sig * sig * inv_r2;
                 const float s6 = sr2 * sr2 * sr2;
                 g += 24.0f * eps * s6 * (2.0f * s6 - 1.0f) * inv_r2;
-                if (ENERGY) te2 += 4.0f * eps * s6 * (s6 - 1.0f);
               }
             }
             ti0 += g * dx; ti1 += g * dy; ti2 += g * dz;
@@ -207,11 +196,6 @@ __global__ void __launch_bounds__(256) tile_kernel(const PairArgs a) {
         ai2 += to_fix_f(ti2, (float)kForceScale);
         if (PASS == PASS_FORCE) ai3 += to_fix_f(ti3, (float)kForceScale);
       }
-      if (ENERGY) {
-        e_gb += (double)te0;
-        e_coul += (double)te1;
-        e_lj += (double)te2;
-      }
     }
 
     if (ivalid) {
@@ -222,17 +206,6 @@ __global__ void __launch_bounds__(256) tile_kernel(const PairArgs a) {
         atomic_add_fix(&a.fy[ig], ai1);
         atomic_add_fix(&a.fz[ig], ai2);
         if (PASS == PASS_FORCE && use_gb) atomic_add_fix(&a.dedb_acc[ig], ai3);
-      }
-    }
-    if (ENERGY) {
-      e_gb = warp_sum(e_gb);
-      e_coul = warp_sum(e_coul);
-      e_lj = warp_sum(e_lj);
-      if (lane == 0) {
-        long long *e = a.energy + (size_t)item.sys * PB2_NTERMS;
-        atomic_add_fix(&e[PB2_TERM_GB], to_fix(e_gb, kForceScale));
-        atomic_add_fix(&e[PB2_TERM_COULOMB], to_fix(e_coul, kForceScale));
-        atomic_add_fix(&e[PB2_TERM_LJ], to_fix(e_lj, kForceScale));
       }
     }
   }
@@ -268,6 +241,7 @@ __global__ void born_finalize(const FinalizeArgs a) {
     const double dpsi = (kObcAlpha - 2.0 * kObcBeta * psi + 3.0 * kObcGamma * psi * psi) * ro;
     const double dbdi = clamped ? 0.0 : B * B * (1.0 - th * th) / dr * dpsi;
     a.born[i] = make_float4((float)B, (float)inv_b, (float)dbdi, 0.f);
+    if (a.born64) a.born64[i] = B;
     const double q = a.charge[i];
     const double r_nm = (r_in - kDielOffset) / 10.0 + 0.009;
     const double x = r_nm / (B / 10.0);
@@ -285,14 +259,12 @@ __global__ void born_finalize(const FinalizeArgs a) {
 
 // --------------------------------------------------------------- launchers
 
-cudaError_t launch_tiles(int pass, bool energy, const PairArgs &a, int grid, cudaStream_t st) {
+cudaError_t launch_tiles(int pass, const PairArgs &a, int grid, cudaStream_t st) {
   if (a.n_items <= 0) return cudaSuccess;
   switch (pass) {
-    case PASS_BORN: tile_kernel<PASS_BORN, false><<<grid, 256, 0, st>>>(a); break;
-    case PASS_CHAIN: tile_kernel<PASS_CHAIN, false><<<grid, 256, 0, st>>>(a); break;
-    default:
-      if (energy) tile_kernel<PASS_FORCE, true><<<grid, 256, 0, st>>>(a);
-      else tile_kernel<PASS_FORCE, false><<<grid, 256, 0, st>>>(a);
+    case PASS_BORN: tile_kernel<PASS_BORN><<<grid, 256, 0, st>>>(a); break;
+    case PASS_CHAIN: tile_kernel<PASS_CHAIN><<<grid, 256, 0, st>>>(a); break;
+    default: tile_kernel<PASS_FORCE><<<grid, 256, 0, st>>>(a);
   }
   return cudaGetLastError();
 }
@@ -304,20 +276,17 @@ cudaError_t launch_born_finalize(const FinalizeArgs &a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-int tile_kernel_occupancy(int pass, bool energy) {
+int tile_kernel_occupancy(int pass) {
   int blocks = 0;
   switch (pass) {
     case PASS_BORN:
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, tile_kernel<PASS_BORN, false>, 256, 0);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, tile_kernel<PASS_BORN>, 256, 0);
       break;
     case PASS_CHAIN:
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, tile_kernel<PASS_CHAIN, false>, 256, 0);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, tile_kernel<PASS_CHAIN>, 256, 0);
       break;
     default:
-      if (energy)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, tile_kernel<PASS_FORCE, true>, 256, 0);
-      else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, tile_kernel<PASS_FORCE, false>, 256, 0);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, tile_kernel<PASS_FORCE>, 256, 0);
   }
   return blocks > 0 ? blocks : 1;
 }

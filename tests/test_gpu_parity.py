@@ -184,19 +184,53 @@ def test_full_langevin_short_run_stays_close_to_oracle():
   assert rel_rms(st["force"], o.force) < 1e-5
 
 
-def test_nve_energy_drift_all_pairs():
-  s = synth.make_chain(400, 12, compact=True)
-  dt = engine.akma_dt(0.5)
-  with engine.Batch([s], key=prng.prng_key(8), dt=dt, kT=300 * engine.KB_KCAL, gamma=0.0) as b:
-    b.langevin_init()
-    st0 = b.get_state()
+def test_nve_three_gb_particles():
+  # prolix tests/physics/test_generalized_born.py:138-end restated: three GB
+  # particles (mass 10, radius 1.5), 100 velocity Verlet steps of dt = 1e-3,
+  # initial velocities 0.1 * normal(key 0); |dH| / |H| < 1e-4.
+  s = {"positions": np.array([[0.0, 0.0, 0.0], [3.0, 0.0, 0.0], [0.0, 4.0, 0.0]]),
+       "charges": [0.5, -0.5, 0.5], "sigmas": [1.0] * 3, "epsilons": [0.0] * 3,
+       "radii": [1.5] * 3, "scaled_radii": [1.5] * 3, "masses": [10.0] * 3}
+  from prolix_b200._lib import USE_GB
+  v = prng.normal_f32(prng.prng_key(0), 9).astype(np.float64).reshape(3, 3) * 0.1
+  with engine.Batch([s], terms=USE_GB, dt=1e-3, kT=0.0, gamma=0.0) as b:
+    b.set_state(momentum=10.0 * v)
     e0, _ = b.energy_forces()
-    m = np.asarray(s["masses"])[:, None]
-    ke0 = 0.5 * np.sum(st0["momentum"] ** 2 / m)
-    b.langevin_run(1000)
-    st1 = b.get_state()
+    b.langevin_run(100)
+    st = b.get_state()
     e1, _ = b.energy_forces()
-  ke1 = 0.5 * np.sum(st1["momentum"] ** 2 / m)
-  h0 = e0[0][-1] + ke0
-  h1 = e1[0][-1] + ke1
+  h0 = e0[0][-1] + 0.5 * np.sum(10.0 * v * v)
+  h1 = e1[0][-1] + 0.5 * np.sum(st["momentum"] ** 2 / 10.0)
   assert abs(h1 - h0) / abs(h0) < 1e-4
+
+
+def _nve_h_change(s, dt_fs, total_fs=250.0, samples=41):
+  m = np.asarray(s["masses"])[:, None]
+  n = int(round(total_fs / dt_fs))
+  every = n // (samples - 1)
+  hs = []
+  with engine.Batch([s], key=prng.prng_key(8), dt=engine.akma_dt(dt_fs),
+                    kT=300 * engine.KB_KCAL, gamma=0.0) as b:
+    b.langevin_init()
+    for k in range(samples):
+      if k:
+        b.langevin_run(every)
+      st = b.get_state()
+      e, _ = b.energy_forces()
+      hs.append(e[0][-1] + 0.5 * np.sum(st["momentum"] ** 2 / m))
+  hs = np.array(hs)
+  return abs(hs[-8:].mean() - hs[:8].mean()), hs
+
+
+def test_nve_drift_is_second_order_in_dt():
+  # gamma = 0 turns BAOAB into velocity Verlet.  If the FP32 forces are the
+  # gradient of the FP64 energy, the change of H over a fixed time is
+  # Verlet's O(dt^2) error: halving dt divides it by ~4.  A force/energy
+  # mismatch would leave a dt-independent drift.
+  s = synth.make_chain(400, 12, compact=True)
+  d1, h1 = _nve_h_change(s, 0.5)
+  d2, h2 = _nve_h_change(s, 0.25)
+  rel = d1 / abs(h1.mean())
+  print(f"NVE |dH|/|H| over 250 fs: dt 0.5 fs {rel:.2e}, dt 0.25 fs {d2 / abs(h2.mean()):.2e}")
+  assert rel < 2e-4
+  assert d2 < 0.4 * d1
