@@ -97,6 +97,8 @@ static int fail(pb2_ctx *ctx, int code, const std::string &msg) {
   return code;
 }
 
+int pb2::set_error(pb2_ctx *ctx, int code, const char *msg) { return fail(ctx, code, msg); }
+
 #define CUDA_TRY(ctx, expr)                                                                  \
   do {                                                                                       \
     cudaError_t e_ = (expr);                                                                 \

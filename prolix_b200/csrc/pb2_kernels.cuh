@@ -6,6 +6,9 @@
 
 namespace pb2 {
 
+// Record a message as the context's last error (ctx may be NULL); returns code.
+int set_error(pb2_ctx *ctx, int code, const char *msg);
+
 enum { PASS_BORN = 0, PASS_FORCE = 1, PASS_CHAIN = 2 };
 struct PairArgs {
   const SysInfo *sys;
