@@ -206,6 +206,25 @@ int pb2_nl_get(pb2_batch *batch, int32_t *neighbors, void *stream);
 int pb2_set_profiling(pb2_batch *batch, int enable);
 int pb2_last_timings(pb2_batch *batch, double *out_ms);
 
+/*
+ * Born radii of one system with no device allocation (no counterpart in the
+ * reference: prolix allocates through JAX).  For callers that cannot call
+ * cudaMalloc -- an XLA custom-call handler, which may use only the buffers
+ * the runtime hands it; code running while a stream is captured into a CUDA
+ * graph; hosts that give the library a fixed memory pool.  The caller
+ * passes device buffers: positions (n, 3), radii (n), scaled_radii (n) and
+ * born (n) out, all FP64.  cutoff <= 0 sums all pairs.  The descreening
+ * scratch is a static 256 KiB device array shared by every call, so n_atoms
+ * is limited to PB2_NOALLOC_MAX_ATOMS; calls that overlap on the GPU race on
+ * it and must be serialised.  The first call on a device looks the array up
+ * (cudaGetSymbolAddress) with that device current: make it before any
+ * stream capture.  ctx may be NULL (errors are then not recorded).
+ */
+#define PB2_NOALLOC_MAX_ATOMS 32768
+int pb2_born_radii_noalloc(pb2_ctx *ctx, int32_t n_atoms, const double *positions,
+                           const double *radii, const double *scaled_radii, double cutoff,
+                           double *born, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -87,6 +87,9 @@ SIGNATURES = [
     ("pb2_nl_get", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("pb2_set_profiling", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("pb2_last_timings", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    ("pb2_born_radii_noalloc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
+                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
+                                              ctypes.c_void_p, ctypes.c_void_p]),
 ]
 
 _LOCK = threading.Lock()
