@@ -122,12 +122,16 @@ typedef struct pb2_system_desc {
 /* Batch-wide settings. */
 typedef struct pb2_run_params {
   uint32_t terms;       /* PB2_USE_* bits */
-  double cutoff;        /* A; <= 0: all pairs (no neighbour list) */
+  double cutoff;        /* A; LJ and Coulomb; <= 0: all pairs */
   double skin;          /* A; neighbour-list skin (rebuild when any atom moved > skin/2) */
   int32_t nl_capacity;  /* per-atom neighbour capacity; 0 = automatic */
   int32_t tile_segment; /* tiles per work item; 0 = autotuned/default */
   int32_t graph_chunk;  /* steps per captured CUDA graph; 0 = 50 */
   int32_t partitionable_keys; /* 1: jax_threefry_partitionable layout (JAX default) */
+  double gb_cutoff;     /* A; GB pairs and descreening: < 0 same as cutoff, 0 all pairs.
+                           prolix's make_energy_fn keeps GB all-pairs while LJ/Coulomb
+                           use the cutoff (system.py:196-216); with a GB cutoff the
+                           neighbour-list clamps of generalized_born.py:300-337 apply */
 } pb2_run_params;
 
 typedef struct pb2_ctx pb2_ctx;

@@ -151,10 +151,13 @@ def excl_dense_rows(pairs, s_vdw, s_elec, a, b, n):
 
 def nonbonded(system, pos, cutoff=0.0, eps_in=1.0, eps_out=78.5, k_gb=K_COULOMB,
               k_coul=K_COULOMB, lj14=topology.LJ14_SCALE, coul14=topology.COUL14_SCALE,
-              ace=True):
+              ace=True, gb_cutoff=None):
   """Energies (dict) and forces (N, 3) of GB polar, ACE, Coulomb and LJ.
 
-  ``ace=False`` drops the nonpolar term (``compute_gb_energy`` alone).
+  ``cutoff`` applies to Coulomb and LJ; ``gb_cutoff`` to the GB pair terms
+  and the descreening sums (None: the same as ``cutoff``; 0: all pairs, as
+  prolix's make_energy_fn does for GB, system.py:196-216).  ``ace=False``
+  drops the nonpolar term (``compute_gb_energy`` alone).
   """
   pos = np.asarray(pos, dtype=np.float64)
   n = pos.shape[0]
@@ -164,8 +167,9 @@ def nonbonded(system, pos, cutoff=0.0, eps_in=1.0, eps_out=78.5, k_gb=K_COULOMB,
   radii = np.asarray(system["radii"], np.float64)
   sr = np.asarray(system["scaled_radii"], np.float64)
   pairs, s_v, s_e = topology.pair_scales(system.get("bonds", np.zeros((0, 2))), n, lj14, coul14)
-  nl = cutoff > 0
-  born, isum, dbdi = born_radii(pos, radii, sr, cutoff)
+  gbc = cutoff if gb_cutoff is None else gb_cutoff
+  nl = gbc > 0
+  born, isum, dbdi = born_radii(pos, radii, sr, gbc)
   rad = np.maximum(radii, 1e-6) if nl else radii
   rho_off = rad - DIELECTRIC_OFFSET
   if nl:
@@ -186,7 +190,7 @@ def nonbonded(system, pos, cutoff=0.0, eps_in=1.0, eps_out=78.5, k_gb=K_COULOMB,
     m = ~selfm
     rg = np.sqrt(r2 + SAFE_EPS)
     if nl:
-      m &= rg < cutoff
+      m &= rg < gbc
     # GB pair terms (every pair, no exclusions)
     bi = born[a:b, None]
     bj = born[None, :]
@@ -205,7 +209,7 @@ def nonbonded(system, pos, cutoff=0.0, eps_in=1.0, eps_out=78.5, k_gb=K_COULOMB,
     # Coulomb / LJ with exclusion scales
     r = np.sqrt(r2)
     mc = ~selfm & (r > 0)
-    if nl:
+    if cutoff > 0:
       mc &= r < cutoff
     sv, se = excl_dense_rows(pairs, s_v, s_e, a, b, n)
     rs = np.where(mc, r, 1.0)
@@ -227,7 +231,7 @@ def nonbonded(system, pos, cutoff=0.0, eps_in=1.0, eps_out=78.5, k_gb=K_COULOMB,
     m = ~selfm
     rg = np.sqrt(r2 + SAFE_EPS)
     if nl:
-      m &= rg < cutoff
+      m &= rg < gbc
     d_ij = pair_integral_dr(rg, rho_off[a:b, None], sr[None, :])
     d_ji = pair_integral_dr(rg, rho_off[None, :], sr[a:b, None])
     g = np.where(m, (dedi[a:b, None] * d_ij + dedi[None, :] * d_ji) / rg, 0.0)

@@ -24,6 +24,10 @@ CUDA_SOURCES = ["pb2_api.cu", "pb2_pair.cu", "pb2_energy64.cu", "pb2_bonded.cu",
 CUDA_HEADERS = ["pb2_common.cuh", "pb2_kernels.cuh", "pb2_pairmath.cuh", "pb2_threefry.cuh"]
 HOST_SOURCES = ["synth_chain.c"]
 
+# extra flags per source: the pair kernels flush subnormals and use the
+# approximate divide (every value there is far from the subnormal range)
+FILE_FLAGS = {"pb2_pair.cu": ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"]}
+
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
@@ -62,11 +66,26 @@ def build_cuda(force: bool = False, extra_flags=None) -> Path:
   srcs = [CSRC / s for s in present]
   deps = srcs + [CSRC / h for h in CUDA_HEADERS] + [INCLUDE / "prolix_b200.h"]
   if force or _stale(CUDA_LIB, deps):
+    import concurrent.futures
+    import tempfile
     nvcc = _nvcc()
     tmp = CUDA_LIB.with_suffix(".so.tmp")
-    cmd = [nvcc, *NVCC_FLAGS, *(extra_flags or []), "-I", str(INCLUDE), "-I", str(CSRC),
-           "-shared", "-o", str(tmp), *map(str, srcs), "-lcuda"]
-    subprocess.run(cmd, check=True)
+    with tempfile.TemporaryDirectory() as td:
+      objs = [Path(td) / (s.stem + ".o") for s in srcs]
+
+      def compile_one(src_obj):
+        src, obj = src_obj
+        cmd = [nvcc, *NVCC_FLAGS, *FILE_FLAGS.get(src.name, []), *(extra_flags or []),
+               "-I", str(INCLUDE), "-I", str(CSRC), "-c", "-o", str(obj), str(src)]
+        return subprocess.run(cmd, capture_output=True, text=True)
+
+      with concurrent.futures.ThreadPoolExecutor(max_workers=8) as ex:
+        results = list(ex.map(compile_one, zip(srcs, objs)))
+      for src, res in zip(srcs, results):
+        if res.returncode != 0:
+          raise RuntimeError(f"nvcc failed on {src.name}:\n{res.stderr}")
+      subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o",
+                      str(tmp), *map(str, objs), "-lcuda"], check=True)
     os.replace(tmp, CUDA_LIB)
   return CUDA_LIB
 

@@ -2,12 +2,15 @@
 
 The CUDA library is required: there is no CPU fallback, and loading fails
 loudly when ``libprolix_b200.so`` is missing or no sm_100 device is present.
+``PROLIX_B200_LIB`` overrides the library path (an alternative build).
 """
 
 from __future__ import annotations
 
 import ctypes
+import os
 import threading
+from pathlib import Path
 
 from . import _build
 
@@ -57,6 +60,7 @@ class RunParams(ctypes.Structure):
       ("tile_segment", ctypes.c_int32),
       ("graph_chunk", ctypes.c_int32),
       ("partitionable_keys", ctypes.c_int32),
+      ("gb_cutoff", ctypes.c_double),
   ]
 
 
@@ -101,7 +105,8 @@ def load(path=None) -> ctypes.CDLL:
   global _LIB
   with _LOCK:
     if _LIB is None:
-      p = path or _build.CUDA_LIB
+      env = os.environ.get("PROLIX_B200_LIB")
+      p = Path(path or env or _build.CUDA_LIB)
       if not p.exists():
         _build.build_cuda()
       lib = ctypes.CDLL(str(p))

@@ -63,7 +63,9 @@ struct pb2_batch {
   double *x = nullptr, *y = nullptr, *z = nullptr, *px = nullptr, *py = nullptr, *pz = nullptr;
   long long *fx = nullptr, *fy = nullptr, *fz = nullptr;
   double *mass = nullptr, *sigma = nullptr, *charge = nullptr, *radius = nullptr;
-  float4 *posq = nullptr, *par = nullptr, *born = nullptr;
+  float4 *posq = nullptr, *par = nullptr, *born = nullptr, *bbox = nullptr;
+  int32_t *blk_sys = nullptr;
+  int n_blocks = 0;
   double *q64 = nullptr, *hs64 = nullptr, *se64 = nullptr, *ro64 = nullptr, *sr64 = nullptr;
   double *born64 = nullptr;
   long long *born_acc = nullptr, *dedb_acc = nullptr, *energy = nullptr;
@@ -75,7 +77,8 @@ struct pb2_batch {
   ExclRow *excl_rows = nullptr;
   BondedArgs bonded{};
   int key_parity = 0;
-  bool forces_valid = false;  // force accumulators hold F(x) of the current state
+  bool forces_valid = false;
+  bool cut = false;  // any cutoff active  // force accumulators hold F(x) of the current state
   int grid_pair[3] = {1, 1, 1};
   int grid_bonded = 1;
   cudaStream_t cap_stream = nullptr;
@@ -147,6 +150,8 @@ static PairArgs pair_args(pb2_batch *b) {
   a.posq = b->posq;
   a.par = b->par;
   a.born = b->born;
+  a.bbox = b->bbox;
+  a.cut = b->cut ? 1 : 0;
   a.born_acc = b->born_acc;
   a.dedb_acc = b->dedb_acc;
   a.fx = b->fx;
@@ -252,6 +257,8 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   if (b->params.graph_chunk <= 0) b->params.graph_chunk = 50;
   b->n_sys = n_systems;
   const bool cutoff_mode = params->cutoff > 0.0;
+  const double gb_cut = params->gb_cutoff < 0.0 ? (cutoff_mode ? params->cutoff : 0.0) : params->gb_cutoff;
+  const bool gb_cut_mode = gb_cut > 0.0;
 
   // --- per-atom host arrays
   int64_t total = 0;
@@ -272,6 +279,7 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   std::vector<SysInfo> sinfo(n_systems);
   std::vector<uint32_t> hkeys(4 * (size_t)n_systems, 0u);
   std::vector<int2> hent((size_t)blocks_total * kExclPerBlock, make_int2(-1, -1));
+  std::vector<int32_t> hblk_sys(blocks_total);
   std::vector<ExclRow> hrows;
   std::vector<TileItem> hitems;
   int blk_base = 0;
@@ -291,6 +299,8 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
     S.lj14 = (float)d.lj14_scale;
     S.coul14 = (float)d.coul14_scale;
     S.cutoff2 = cutoff_mode ? (float)(params->cutoff * params->cutoff) : 0.f;
+    S.gb_cutoff2 = gb_cut_mode ? (float)(gb_cut * gb_cut) : 0.f;
+    S.clamp = gb_cut_mode ? 1 : 0;
     S.dt = d.dt;
     S.half_dt = 0.5 * d.dt;
     S.c1 = std::exp(-d.gamma * d.dt);
@@ -319,13 +329,23 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
       hposq[g] = make_float4((float)(hx[g] - S.ox), (float)(hy[g] - S.oy), (float)(hz[g] - S.oz),
                              (float)d.charges[i]);
       double ro = d.radii[i] - kDielOffset;
-      if (cutoff_mode) ro = std::max(std::max(d.radii[i], 1e-6) - kDielOffset, 1e-4);
+      if (gb_cut_mode) ro = std::max(std::max(d.radii[i], 1e-6) - kDielOffset, 1e-4);
       hhs[g] = 0.5 * std::max(d.sigmas[i], 1e-6);
       hse[g] = std::sqrt(std::max(d.epsilons[i], 0.0));
       hro[g] = ro;
       hsr[g] = d.scaled_radii[i];
       hpar[g] = make_float4((float)hhs[g], (float)hse[g], (float)ro, (float)hsr[g]);
     }
+    {  // far-field tiles: every pair has r - s >= rho~ and (s/r)^2 <= 0.09
+      float smax = 0.f, romax = 0.f;
+      for (int i = 0; i < n; ++i) {
+        smax = std::max(smax, hpar[o + i].w);
+        romax = std::max(romax, hpar[o + i].z);
+      }
+      const double rfar = 1.001 * std::max((double)smax / 0.3, (double)smax + (double)romax);
+      S.far2 = (float)(rfar * rfar);
+    }
+    for (int bk = 0; bk < S.nblk; ++bk) hblk_sys[blk_base + bk] = s;
     hkeys[2 * (size_t)s] = d.key[0];
     hkeys[2 * (size_t)s + 1] = d.key[1];
     // exclusion masks, one 32-row block per (i-block, j-block) with exclusions
@@ -423,6 +443,10 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   b->posq = D.alloc<float4>(N);
   b->par = D.alloc<float4>(N);
   b->born = D.alloc<float4>(N);
+  b->bbox = D.alloc<float4>(2 * (size_t)blocks_total);
+  b->blk_sys = D.alloc<int32_t>(blocks_total);
+  b->n_blocks = blocks_total;
+  b->cut = cutoff_mode || gb_cut_mode;
   b->q64 = D.alloc<double>(N);
   b->hs64 = D.alloc<double>(N);
   b->se64 = D.alloc<double>(N);
@@ -467,7 +491,7 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
       (rc = upload(ctx, b->q64, hq)) || (rc = upload(ctx, b->hs64, hhs)) ||
       (rc = upload(ctx, b->se64, hse)) || (rc = upload(ctx, b->ro64, hro)) ||
       (rc = upload(ctx, b->sr64, hsr)) ||
-      (rc = upload(ctx, b->keys, hkeys)) || (rc = upload(ctx, b->items, hitems)) ||
+      (rc = upload(ctx, b->keys, hkeys)) || (rc = upload(ctx, b->blk_sys, hblk_sys)) || (rc = upload(ctx, b->items, hitems)) ||
       (rc = upload(ctx, b->excl_ent, hent)) || (rc = upload(ctx, b->excl_rows, hrows)) ||
       (rc = upload(ctx, d_bidx, bidx)) || (rc = upload(ctx, d_bpar, bpar)) ||
       (rc = upload(ctx, d_aidx, aidx)) || (rc = upload(ctx, d_apar, apar)) ||
@@ -500,7 +524,7 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
 
   // launch shapes: persistent grids sized to the resident capacity
   for (int p = 0; p < 3; ++p) {
-    const int cap = tile_kernel_occupancy(p) * ctx->sm_count;
+    const int cap = tile_kernel_occupancy(p, b->cut) * ctx->sm_count;
     b->grid_pair[p] = std::max(1, std::min(cap, (b->n_items + 7) / 8));
   }
   b->grid_bonded = 8 * ctx->sm_count;
@@ -536,6 +560,7 @@ static cudaError_t enqueue_forces(pb2_batch *b, cudaStream_t st, bool bonded_ene
   cudaError_t e;
   const PairArgs pa = pair_args(b);
   const bool gb = (b->params.terms & PB2_USE_GB) != 0;
+  if ((e = launch_bbox(b->sys, b->blk_sys, b->posq, b->bbox, b->n_blocks, st)) != cudaSuccess) return e;
   if (gb) {
     if ((e = launch_tiles(PASS_BORN, pa, b->grid_pair[PASS_BORN], st)) != cudaSuccess) return e;
     FinalizeArgs fa;

@@ -28,7 +28,7 @@ constexpr double kAceCoeff = 28.3919551, kKjToKcal = 0.239006;
 
 constexpr int kExclPerBlock = 8;  // distinct j-blocks with exclusions per i-block
 
-// Per-system constants, one 128-byte record per system.  Pair kernels see
+// Per-system constants, one 136-byte record per system.  Pair kernels see
 // positions relative to the system origin (its initial centroid), which keeps
 // float32 coordinates small.
 struct SysInfo {
@@ -39,8 +39,10 @@ struct SysInfo {
   float pref;         // P = -0.5 k_gb (1/eps_in - 1/eps_out)
   float kcoul;        // direct Coulomb constant
   float lj14, coul14; // 1-4 scales
-  float cutoff2;      // 0: all pairs
-  int32_t nl_off;     // first row of this system in the neighbour arrays
+  float cutoff2;      // LJ / Coulomb cutoff^2; 0: all pairs
+  float far2;         // tiles at least this far apart (squared) take the far-field series
+  float gb_cutoff2;   // GB / descreening cutoff^2; 0: all pairs
+  int32_t clamp;      // neighbour-list clamps on Born radii (GB cutoff set)
   int32_t pad0, pad1;
   double pref_d;      // P in double (self / energy terms)
   double dt, half_dt; // tau
@@ -49,7 +51,7 @@ struct SysInfo {
   double skin_half2;  // (skin/2)^2
   double ox, oy, oz;  // origin subtracted before the float32 pair kernels
 };
-static_assert(sizeof(SysInfo) == 128, "SysInfo layout");
+static_assert(sizeof(SysInfo) == 136, "SysInfo layout");
 
 // Work item of the tile kernels: tiles (iblk, jb) for jb in [jb0, jb1) of
 // system sys.  Block indices are local to the system.

@@ -48,7 +48,7 @@ __global__ void __launch_bounds__(256) energy64_kernel(const Energy64Args a) {
     const TileItem item = a.items[it];
     const SysInfo &S = a.sys[item.sys];
     const int n = S.n, off = S.off;
-    const double cut2 = S.cutoff2 > 0.f ? (double)S.cutoff2 : 0.0;
+    const double cut2 = (double)S.cutoff2, gcut2 = (double)S.gb_cutoff2;
     const double pref = S.pref_d, kcoul = (double)S.kcoul;
     const int il = item.iblk * 32 + lane;
     const bool ivalid = il < n;
@@ -86,7 +86,7 @@ __global__ void __launch_bounds__(256) energy64_kernel(const Energy64Args a) {
         bool ok = ivalid && (jl0 + jc < n) && (!diag || jc > lane);
         const double dx = xi - xj, dy = yi - yj, dz = zi - zj;
         const double r2 = dx * dx + dy * dy + dz * dz;
-        if (cut2 > 0.0) ok = ok && (r2 < cut2);
+        if (PASS == 0 && gcut2 > 0.0) ok = ok && (r2 < gcut2);
         if (ok) {
           if (PASS == 0) {
             const double r = sqrt(r2 + 1e-12);
@@ -94,13 +94,13 @@ __global__ void __launch_bounds__(256) energy64_kernel(const Energy64Args a) {
             acc_j += obc_integral_d(r, roj, sri);
           } else {
             const double qq = qi * qj;
-            if (use_gb) {
+            if (use_gb && (gcut2 == 0.0 || r2 < gcut2)) {
               const double rg2 = r2 + 1e-12;
               const double d = bi * bj;
               const double f = sqrt(rg2 + d * exp(-rg2 / (4.0 * d)));
               e_gb += 2.0 * pref * qq / f;
             }
-            if (!((exm >> jc) & 1u) && (use_lj || use_coul)) {
+            if (!((exm >> jc) & 1u) && (use_lj || use_coul) && (cut2 == 0.0 || r2 < cut2)) {
               const bool is14 = (s14m >> jc) & 1u;
               const double r = sqrt(r2);
               if (use_coul) e_coul += kcoul * qq * (is14 ? (double)S.coul14 : 1.0) / r;

@@ -20,10 +20,12 @@ struct PairArgs {
   const float4 *posq;
   const float4 *par;
   const float4 *born;
+  const float4 *bbox;       // per global block: (lo, hi) of the float32 positions
   long long *born_acc;
   long long *dedb_acc;
   long long *fx, *fy, *fz;
   long long *energy;
+  int32_t cut;              // any cutoff active
 };
 struct FinalizeArgs {
   const SysInfo *sys;
@@ -95,7 +97,9 @@ struct IntArgs {
 cudaError_t launch_tiles(int pass, const PairArgs &a, int grid, cudaStream_t st);
 cudaError_t launch_energy64(int pass, const Energy64Args &a, int grid, cudaStream_t st);
 cudaError_t launch_born_finalize(const FinalizeArgs &a, cudaStream_t st);
-int tile_kernel_occupancy(int pass);
+int tile_kernel_occupancy(int pass, bool cut);
+cudaError_t launch_bbox(const SysInfo *sys, const int32_t *blk_sys, const float4 *posq, float4 *bbox,
+                        int n_blocks, cudaStream_t st);
 cudaError_t launch_bonded(const BondedArgs &a, int grid_cap, cudaStream_t st);
 cudaError_t launch_step(const IntArgs &a, cudaStream_t st);
 cudaError_t launch_finish(const IntArgs &a, cudaStream_t st);

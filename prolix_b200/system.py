@@ -1,0 +1,163 @@
+"""Drop-in for prolix's energy factory on the implicit-solvent path.
+
+``make_energy_fn(displacement_fn, system, cutoff_distance=9.0,
+return_decomposed=False, implicit_solvent=False, exclusion_spec=None, **kw)``
+mirrors prolix physics/system.py:29-271 for ``implicit_solvent=True``:
+
+* GB polar (with self term) and the OBC2 Born radii use every pair, and
+  Coulomb and LJ use ``cutoff`` (the ``cutoff`` keyword wins over
+  ``cutoff_distance``, system.py:134; a cutoff <= 0 means all pairs), as the
+  reference does (system.py:184-216);
+* exclusions: 1-2 and 1-3 pairs excluded, 1-4 pairs scaled (LJ 0.5,
+  Coulomb 0.83333333), from the bonds or from ``exclusion_spec``;
+* the returned function gives the total energy; ``.forces(r)`` gives
+  -dE/dr, ``.energy_and_forces(r)`` both;
+* ``return_decomposed=True`` returns the reference's dict of per-term
+  callables (system.py:250-270).
+
+Positions are NumPy arrays (N, 3) in A; free space only (prolix's implicit
+runs use ``space.free()``).  Everything runs on the GPU through the C ABI.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from . import engine, topology
+from ._lib import TERM_NAMES, USE_ALL
+
+_SYSTEM_KEYS = ("charges", "sigmas", "epsilons", "radii", "scaled_radii", "masses", "bonds",
+                "bond_params", "angles", "angle_params", "dihedrals", "dihedral_params",
+                "proper_dihedrals", "proper_dihedral_params", "cmap_torsions", "cmap_indices",
+                "cmap_energy_grids", "excl_pairs", "excl_kind")
+
+
+def system_to_dict(system) -> dict:
+  """Accept a dict or any object with prolix's PhysicsSystem attribute names."""
+  if isinstance(system, dict):
+    return dict(system)
+  out = {}
+  for k in _SYSTEM_KEYS + ("positions",):
+    v = getattr(system, k, None)
+    if v is not None:
+      out[k] = np.asarray(v)
+  return out
+
+
+def _exclusions_from_spec(spec, n):
+  """(pairs, kind, lj14, coul14) from a prolix ExclusionSpec-like object."""
+  p1213 = np.asarray(getattr(spec, "idx_12_13", np.zeros((0, 2))), dtype=np.int64).reshape(-1, 2)
+  p14 = np.asarray(getattr(spec, "idx_14", np.zeros((0, 2))), dtype=np.int64).reshape(-1, 2)
+  rows = {}
+  for (i, j) in p1213:
+    a, b = (int(i), int(j)) if i < j else (int(j), int(i))
+    rows[(a, b)] = 0
+  for (i, j) in p14:
+    a, b = (int(i), int(j)) if i < j else (int(j), int(i))
+    rows.setdefault((a, b), 1)
+  keys = sorted(rows)
+  pairs = np.array(keys, dtype=np.int32).reshape(-1, 2)
+  kind = np.array([rows[k] for k in keys], dtype=np.int32)
+  lj14 = float(np.float32(getattr(spec, "scale_14_vdw", topology.LJ14_DEFAULT)))
+  c14 = float(np.float32(getattr(spec, "scale_14_elec", topology.COUL14_DEFAULT)))
+  return pairs, kind, lj14, c14
+
+
+class EnergyFn:
+  """Callable energy function backed by a one-system device batch."""
+
+  def __init__(self, system: dict, cutoff: float, *, eps_in=1.0, eps_out=78.5,
+               terms=USE_ALL, device=0, gb_cutoff=0.0, **defaults):
+    self.system = system
+    self.cutoff = float(cutoff)
+    self.gb_cutoff = float(gb_cutoff)
+    self._batch = engine.Batch([system], cutoff=self.cutoff, gb_cutoff=self.gb_cutoff,
+                               terms=terms, device=device, eps_in=eps_in, eps_out=eps_out,
+                               **defaults)
+    self._last = None
+
+  @property
+  def batch(self) -> engine.Batch:
+    return self._batch
+
+  @property
+  def n_atoms(self) -> int:
+    return self._batch.n_atoms
+
+  def _eval(self, r):
+    r = np.ascontiguousarray(np.asarray(r, dtype=np.float64).reshape(self.n_atoms, 3))
+    if self._last is not None and np.array_equal(self._last[0], r):
+      return self._last[1], self._last[2]
+    self._batch.set_positions(r)
+    e, f = self._batch.energy_forces()
+    self._last = (r.copy(), e[0], f)
+    return e[0], f
+
+  def terms(self, r) -> dict:
+    e, _ = self._eval(r)
+    return {name: float(e[i]) for i, name in enumerate(TERM_NAMES)}
+
+  def __call__(self, r, neighbor=None, **kwargs):
+    return float(self._eval(r)[0][-1])
+
+  def forces(self, r, neighbor=None, **kwargs):
+    return self._eval(r)[1].copy()
+
+  def energy_and_forces(self, r, neighbor=None, **kwargs):
+    e, f = self._eval(r)
+    return float(e[-1]), f.copy()
+
+  def born_radii(self, r):
+    r = np.asarray(r, dtype=np.float64).reshape(self.n_atoms, 3)
+    self._batch.set_positions(r)
+    self._last = None
+    return self._batch.born_radii()
+
+
+def make_energy_fn(displacement_fn, system, cutoff_distance: float = 9.0,
+                   return_decomposed: bool = False, implicit_solvent: bool = False,
+                   exclusion_spec=None, **kwargs):
+  """prolix ``make_energy_fn`` for ``implicit_solvent=True`` on the B200."""
+  if not implicit_solvent:
+    raise NotImplementedError(
+        "prolix_b200 implements the implicit-solvent path only (implicit_solvent=True)")
+  sysd = system_to_dict(system)
+  n = int(np.asarray(sysd["charges"]).shape[0])
+  if n == 0:
+    raise ValueError("make_energy_fn: system['charges'] is empty — cannot infer n_atoms")
+  if "positions" not in sysd:
+    sysd["positions"] = kwargs.get("positions", np.zeros((n, 3)))
+  if "radii" not in sysd or sysd["radii"] is None:
+    sysd["radii"] = np.ones(n)
+  if "scaled_radii" not in sysd or sysd["scaled_radii"] is None:
+    sysd["scaled_radii"] = np.asarray(sysd["radii"])
+  if exclusion_spec is not None and "excl_pairs" not in sysd:
+    pairs, kind, lj14, c14 = _exclusions_from_spec(exclusion_spec, n)
+    sysd["excl_pairs"], sysd["excl_kind"] = pairs, kind
+    sysd["lj14_scale"], sysd["coul14_scale"] = lj14, c14
+  cutoff = float(kwargs.get("cutoff", cutoff_distance))
+  eps_in = float(kwargs.get("solute_dielectric", 1.0))
+  eps_out = float(kwargs.get("solvent_dielectric", 78.5))
+  fn = EnergyFn(sysd, cutoff if cutoff > 0 else 0.0, eps_in=eps_in, eps_out=eps_out,
+                gb_cutoff=float(kwargs.get("gb_cutoff", 0.0)),
+                device=int(kwargs.get("device", 0)))
+  if not return_decomposed:
+    return fn
+
+  def term(name):
+    return lambda r, n=None: fn.terms(r)[name]
+
+  def electrostatics(r, neighbor=None):
+    t = fn.terms(r)
+    return t["gb"], t["coulomb"], fn.born_radii(r)
+
+  def nonpolar(r, born_radii=None):
+    return fn.terms(r)["nonpolar"]
+
+  zero = lambda r, n=None: 0.0
+  return {
+      "bond": term("bond"), "angle": term("angle"), "dihedral": term("dihedral"),
+      "improper": zero, "urey_bradley": zero, "cmap": term("cmap"), "lj": term("lj"),
+      "exception": zero, "electrostatics": electrostatics, "nonpolar": nonpolar,
+      "total": fn,
+  }

@@ -1,0 +1,104 @@
+"""The prolix-facing Python API (make_energy_fn, nvt_langevin,
+run_minimization, run_simulation) on the GPU, against the FP64 oracle."""
+
+import types
+
+import numpy as np
+import pytest
+
+from oracle import bonded as obonded
+from oracle import gbsa as ogbsa
+from oracle import integrator as ointeg
+from oracle import prng
+from prolix_b200 import engine, simulate, synth
+from prolix_b200.system import make_energy_fn
+
+pytestmark = pytest.mark.gpu
+
+
+def oracle_terms(s, pos, cutoff, gb_cutoff):
+  eb, fb = obonded.bonded_all(s, pos)
+  en, fn, ex = ogbsa.nonbonded(s, pos, cutoff, gb_cutoff=gb_cutoff)
+  e = {**eb, **en}
+  e["total"] = sum(e.values())
+  return e, fb + fn, ex
+
+
+def test_make_energy_fn_default_semantics():
+  # prolix: GB all pairs, LJ/Coulomb with cutoff_distance = 9.0
+  s = synth.make_chain(400, 6, compact=True, cmap=True)
+  fn = make_energy_fn(None, s, implicit_solvent=True)
+  e_ref, f_ref, _ = oracle_terms(s, s["positions"], 9.0, 0.0)
+  assert fn(s["positions"]) == pytest.approx(e_ref["total"], rel=1e-6, abs=1e-6)
+  f = fn.forces(s["positions"])
+  assert np.linalg.norm(f - f_ref) / np.linalg.norm(f_ref) < 1e-5
+  terms = fn.terms(s["positions"])
+  for k in ("bond", "angle", "dihedral", "cmap", "lj", "coulomb", "gb", "nonpolar"):
+    assert terms[k] == pytest.approx(e_ref[k], rel=1e-6, abs=1e-6), k
+
+
+def test_decomposed_dict_and_cutoff_keyword():
+  s = synth.make_chain(200, 7, compact=True)
+  d = make_energy_fn(None, s, implicit_solvent=True, return_decomposed=True, cutoff=0.0)
+  assert set(d) == {"bond", "angle", "dihedral", "improper", "urey_bradley", "cmap", "lj",
+                    "exception", "electrostatics", "nonpolar", "total"}
+  e_ref, _, ex = oracle_terms(s, s["positions"], 0.0, 0.0)
+  r = s["positions"]
+  e_gb, e_coul, born = d["electrostatics"](r)
+  assert e_gb == pytest.approx(e_ref["gb"], rel=1e-6)
+  assert e_coul == pytest.approx(e_ref["coulomb"], rel=1e-6)
+  np.testing.assert_allclose(born, ex["born_radii"], rtol=2e-6)
+  assert d["lj"](r) == pytest.approx(e_ref["lj"], rel=1e-6, abs=1e-6)
+  assert d["nonpolar"](r, born) == pytest.approx(e_ref["nonpolar"], rel=1e-6)
+  assert d["total"](r) == pytest.approx(e_ref["total"], rel=1e-6)
+
+
+def test_exclusion_spec_object():
+  s = synth.make_chain(120, 9)
+  from oracle import topology as otopo
+  p12, p13, p14 = otopo.bonded_pairs(s["bonds"], 120)
+  spec = types.SimpleNamespace(idx_12_13=np.concatenate([p12, p13]), idx_14=p14,
+                               scale_14_elec=0.83333333, scale_14_vdw=0.5)
+  fa = make_energy_fn(None, s, implicit_solvent=True, exclusion_spec=spec, cutoff=0.0)
+  fb = make_energy_fn(None, s, implicit_solvent=True, cutoff=0.0)
+  assert fa(s["positions"]) == fb(s["positions"])
+
+
+def test_separate_gb_and_direct_cutoffs():
+  s = synth.make_chain(900, 10, compact=True)
+  with engine.Batch([s], cutoff=8.0, gb_cutoff=12.0) as b:
+    e, f = b.energy_forces()
+    born = b.born_radii()
+  e_ref, f_ref, ex = oracle_terms(s, s["positions"], 8.0, 12.0)
+  assert np.linalg.norm(f - f_ref) / np.linalg.norm(f_ref) < 1e-5
+  np.testing.assert_allclose(born, ex["born_radii"], rtol=2e-6)
+  for i, k in enumerate(("bond", "angle", "dihedral", "cmap", "lj", "coulomb", "gb", "nonpolar")):
+    assert e[0][i] == pytest.approx(e_ref[k], rel=1e-6, abs=1e-6), k
+
+
+def test_nvt_langevin_protocol_matches_oracle():
+  s = synth.make_chain(150, 11)
+  fn = make_energy_fn(None, s, implicit_solvent=True, cutoff=0.0)
+  dt, kT, gamma = engine.akma_dt(1.0), 300 * engine.KB_KCAL, engine.akma_gamma(1.0)
+  key = prng.prng_key(17)
+  init_fn, apply_fn = simulate.nvt_langevin(fn, None, dt=dt, kT=kT, gamma=gamma, mass=s["masses"])
+  st = init_fn(key, s["positions"], mass=s["masses"])
+  for _ in range(3):
+    st = apply_fn(st)
+  force = lambda r: oracle_terms(s, r, 0.0, 0.0)[1]
+  o = ointeg.init(force, key, s["positions"], s["masses"], kT)
+  o = ointeg.run(o, force, 3, dt, kT, gamma)
+  assert st.step == 3
+  assert np.max(np.abs(st.position - o.position)) < 1e-7
+  np.testing.assert_array_equal(st.rng, o.key)
+
+
+def test_minimization_and_run_simulation():
+  s = synth.make_chain(300, 12, compact=True)
+  pos = s["positions"] + np.random.default_rng(0).normal(0, 0.15, size=s["positions"].shape)
+  fn = make_energy_fn(None, dict(s, positions=pos), implicit_solvent=True)
+  e0 = fn(pos)
+  r = simulate.run_minimization(fn, pos, sd_steps=30)
+  assert fn(r) < e0
+  out = simulate.run_simulation(s, pos, min_steps=10, therm_steps=20, key=prng.prng_key(2))
+  assert out.shape == pos.shape and np.isfinite(out).all()
