@@ -21,93 +21,11 @@
 #include "pb2_kernels.cuh"
 
 
+#include "pb2_internal.h"
+
 using namespace pb2;
 
-struct pb2_ctx {
-  int device = 0;
-  int sm_count = 148;
-  std::string err;
-};
-
-namespace {
-
-constexpr int kFamPair = 0, kFamBonded = 1, kFamInt = 2, kFamNl = 3, kFamAll = 4;
-
-struct Dev {
-  std::vector<void *> ptrs;
-  ~Dev() {
-    for (void *p : ptrs) cudaFree(p);
-  }
-  template <class T>
-  T *alloc(size_t n) {
-    void *p = nullptr;
-    if (n == 0) n = 1;
-    if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return nullptr;
-    ptrs.push_back(p);
-    return static_cast<T *>(p);
-  }
-};
-
-}  // namespace
-
-struct pb2_batch {
-  pb2_ctx *ctx = nullptr;
-  pb2_run_params params{};
-  int n_sys = 0;
-  int n_total = 0;
-  std::vector<int> off, nat;
-  std::vector<SysInfo> sys_host;
-  Dev dev;
-  SysInfo *sys = nullptr;
-  int32_t *atom_sys = nullptr;
-  double *x = nullptr, *y = nullptr, *z = nullptr, *px = nullptr, *py = nullptr, *pz = nullptr;
-  long long *fx = nullptr, *fy = nullptr, *fz = nullptr;
-  double *mass = nullptr, *sigma = nullptr, *charge = nullptr, *radius = nullptr;
-  float4 *posq = nullptr, *par = nullptr, *born = nullptr, *bbox = nullptr;
-  int32_t *blk_sys = nullptr;
-  int n_blocks = 0;
-  double *q64 = nullptr, *hs64 = nullptr, *se64 = nullptr, *ro64 = nullptr, *sr64 = nullptr;
-  double *born64 = nullptr;
-  long long *born_acc = nullptr, *dedb_acc = nullptr, *energy = nullptr;
-  uint32_t *keys = nullptr, *status = nullptr;
-  long long *steps = nullptr;
-  TileItem *items = nullptr;
-  int n_items = 0;
-  int2 *excl_ent = nullptr;
-  ExclRow *excl_rows = nullptr;
-  BondedArgs bonded{};
-  int key_parity = 0;
-  bool forces_valid = false;
-  bool cut = false;  // any cutoff active  // force accumulators hold F(x) of the current state
-  int grid_pair[3] = {1, 1, 1};
-  int grid_bonded = 1;
-  cudaStream_t cap_stream = nullptr;
-  std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
-  bool profiling = false;
-  double timings[5] = {0, 0, 0, 0, 0};
-  cudaEvent_t ev[2] = {nullptr, nullptr};
-
-  ~pb2_batch() {
-    for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
-    if (cap_stream) cudaStreamDestroy(cap_stream);
-    for (auto &e : ev)
-      if (e) cudaEventDestroy(e);
-  }
-};
-
-static int fail(pb2_ctx *ctx, int code, const std::string &msg) {
-  if (ctx) ctx->err = msg;
-  return code;
-}
-
 int pb2::set_error(pb2_ctx *ctx, int code, const char *msg) { return fail(ctx, code, msg); }
-
-#define CUDA_TRY(ctx, expr)                                                                  \
-  do {                                                                                       \
-    cudaError_t e_ = (expr);                                                                 \
-    if (e_ != cudaSuccess)                                                                   \
-      return fail((ctx), PB2_ECUDA, std::string(#expr) + ": " + cudaGetErrorString(e_));     \
-  } while (0)
 
 extern "C" int pb2_abi_version(void) { return PB2_ABI_VERSION; }
 
@@ -161,6 +79,8 @@ static PairArgs pair_args(pb2_batch *b) {
   return a;
 }
 
+IntArgs int_args_for_nl(pb2_batch *b);
+
 static IntArgs int_args(pb2_batch *b, int parity, int finish_prev) {
   IntArgs a;
   a.sys = b->sys;
@@ -182,6 +102,8 @@ static IntArgs int_args(pb2_batch *b, int parity, int finish_prev) {
   a.partitionable = b->params.partitionable_keys;
   return a;
 }
+
+IntArgs int_args_for_nl(pb2_batch *b) { return int_args(b, b->key_parity, 0); }
 
 static int validate(pb2_ctx *ctx, const pb2_system_desc &d, int s) {
   char buf[256];

@@ -1,0 +1,117 @@
+// Host-side definitions shared by the C ABI translation units: the context
+// and batch records and the error helpers.
+#pragma once
+
+#include <map>
+#include <string>
+#include <vector>
+
+#include "pb2_common.cuh"
+#include "pb2_kernels.cuh"
+
+using namespace pb2;
+
+
+struct pb2_ctx {
+  int device = 0;
+  int sm_count = 148;
+  std::string err;
+};
+
+// timing families of pb2_last_timings
+constexpr int kFamPair = 0, kFamBonded = 1, kFamInt = 2, kFamNl = 3, kFamAll = 4;
+
+// Device allocations owned by a batch, freed with it.
+struct Dev {
+  std::vector<void *> ptrs;
+  ~Dev() {
+    for (void *p : ptrs) cudaFree(p);
+  }
+  template <class T>
+  T *alloc(size_t n) {
+    void *p = nullptr;
+    if (n == 0) n = 1;
+    if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return nullptr;
+    ptrs.push_back(p);
+    return static_cast<T *>(p);
+  }
+  void release(void *p) {
+    for (auto &q : ptrs)
+      if (q == p) {
+        cudaFree(q);
+        q = nullptr;
+      }
+  }
+};
+
+struct pb2_batch {
+  pb2_ctx *ctx = nullptr;
+  pb2_run_params params{};
+  int n_sys = 0;
+  int n_total = 0;
+  std::vector<int> off, nat;
+  std::vector<SysInfo> sys_host;
+  Dev dev;
+  SysInfo *sys = nullptr;
+  int32_t *atom_sys = nullptr;
+  double *x = nullptr, *y = nullptr, *z = nullptr, *px = nullptr, *py = nullptr, *pz = nullptr;
+  long long *fx = nullptr, *fy = nullptr, *fz = nullptr;
+  double *mass = nullptr, *sigma = nullptr, *charge = nullptr, *radius = nullptr;
+  float4 *posq = nullptr, *par = nullptr, *born = nullptr, *bbox = nullptr;
+  int32_t *blk_sys = nullptr;
+  int n_blocks = 0;
+  double *q64 = nullptr, *hs64 = nullptr, *se64 = nullptr, *ro64 = nullptr, *sr64 = nullptr;
+  double *born64 = nullptr;
+  long long *born_acc = nullptr, *dedb_acc = nullptr, *energy = nullptr;
+  uint32_t *keys = nullptr, *status = nullptr;
+  long long *steps = nullptr;
+  TileItem *items = nullptr;
+  int n_items = 0;
+  int2 *excl_ent = nullptr;
+  ExclRow *excl_rows = nullptr;
+  BondedArgs bonded{};
+  int key_parity = 0;
+  bool forces_valid = false;
+  bool cut = false;  // any cutoff active  // force accumulators hold F(x) of the current state
+  int grid_pair[3] = {1, 1, 1};
+  int grid_bonded = 1;
+  cudaStream_t cap_stream = nullptr;
+  std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
+  bool profiling = false;
+  double timings[5] = {0, 0, 0, 0, 0};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  // neighbour list (allocated on first build)
+  Dev nl;
+  bool nl_built = false;
+  int nl_capacity = 0;
+  int nl_cells = 0;
+  NlGrid *nl_grid = nullptr;
+  int *nl_atom_cell = nullptr, *nl_cell_count = nullptr, *nl_cell_start = nullptr;
+  int *nl_cell_cursor = nullptr, *nl_cell_atoms = nullptr, *nl_rows = nullptr, *nl_counts = nullptr;
+  int *nl_max_disp2 = nullptr;
+  unsigned *nl_error = nullptr;
+  double *nl_xref = nullptr;
+
+  ~pb2_batch() {
+    for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
+    if (cap_stream) cudaStreamDestroy(cap_stream);
+    for (auto &e : ev)
+      if (e) cudaEventDestroy(e);
+  }
+};
+
+static inline int fail(pb2_ctx *ctx, int code, const std::string &msg) {
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
+
+IntArgs int_args_for_nl(pb2_batch *b);
+
+#define CUDA_TRY(ctx, expr)                                                                  \
+  do {                                                                                       \
+    cudaError_t e_ = (expr);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return fail((ctx), PB2_ECUDA, std::string(#expr) + ": " + cudaGetErrorString(e_));     \
+  } while (0)
+

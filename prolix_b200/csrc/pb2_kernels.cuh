@@ -75,6 +75,28 @@ struct BondedArgs {
   const int32_t *cmap_grid;
   const int64_t *cmap_map_off;
 };
+struct NlGrid {        // per-system cell grid of the neighbour-list build
+  float x0, y0, z0, inv_cell;
+  int32_t nx, ny, nz, cell_base;
+  int32_t n, atom_off;
+  float reach2;         // (cutoff + skin)^2
+  int32_t pad;
+};
+struct NlArgs {
+  const int32_t *atom_sys;
+  const NlGrid *grid;
+  const float4 *posq;
+  const double *x, *y, *z;
+  double *xref;         // positions at the last build, SoA (3, n_total)
+  int *atom_cell, *cell_count, *cell_start, *cell_cursor, *cell_atoms;
+  int *rows, *counts;
+  int32_t capacity, n_total, n_cells, n_sys;
+  uint32_t *status;
+  unsigned *error;
+  int *max_disp2;
+};
+cudaError_t nl_launch_build(const NlArgs &a, cudaStream_t st);
+cudaError_t nl_launch_disp(const NlArgs &a, cudaStream_t st);
 struct IntArgs {
   const SysInfo *sys;
   const int32_t *atom_sys;

@@ -1,0 +1,77 @@
+"""Cell-list neighbour lists (jax_md layout) against brute force."""
+
+import numpy as np
+import pytest
+
+from oracle import nlist as onl
+from prolix_b200 import _lib, engine, synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _check_rows(rows, systems, reach, tol=1e-3):
+  off = 0
+  for s in systems:
+    n = len(s["charges"])
+    tight = onl.neighbour_sets(s["positions"], reach - tol)
+    loose = onl.neighbour_sets(s["positions"], reach + tol)
+    for i in range(n):
+      row = rows[off + i]
+      got = row[row != n]
+      assert len(got) == len(set(got.tolist())), "duplicate neighbour"
+      g = set(got.tolist())
+      assert tight[i] <= g <= loose[i], (i, len(tight[i]), len(g), len(loose[i]))
+    off += n
+
+
+def test_cell_list_matches_brute_force_ragged():
+  systems = [synth.make_chain(n, 300 + k, compact=True) for k, n in enumerate([70, 640, 1500])]
+  with engine.Batch(systems, cutoff=8.0, skin=2.0) as b:
+    b.nl_build()
+    rows = b.nl_get()
+    assert b.nl_capacity() == rows.shape[1]
+    rows2 = b.nl_get()
+    b.nl_build()
+    rows3 = b.nl_get()
+  _check_rows(rows, systems, 10.0)
+  np.testing.assert_array_equal(rows2, rows3)  # deterministic order
+  # symmetric: j in row i <=> i in row j
+  off = 0
+  for s in systems:
+    n = len(s["charges"])
+    sets = [set(r[r != n].tolist()) for r in rows[off:off + n]]
+    for i in range(n):
+      for j in sets[i]:
+        assert i in sets[j]
+    off += n
+
+
+def test_skin_rebuild_rule():
+  s = synth.make_chain(500, 8, compact=True)
+  with engine.Batch([s], cutoff=9.0, skin=2.0) as b:
+    assert b.nl_check() == 1  # first call builds
+    pos = s["positions"].copy()
+    pos[7] += np.array([0.6, 0.0, 0.0])  # below skin/2
+    b.set_positions(pos)
+    assert b.nl_check() == 0
+    pos[7] += np.array([0.6, 0.0, 0.0])  # now 1.2 A > skin/2
+    b.set_positions(pos)
+    assert b.nl_check() == 1
+    rows = b.nl_get()
+  _check_rows(rows, [dict(s, positions=pos)], 11.0)
+
+
+def test_fixed_capacity_overflow_is_reported():
+  s = synth.make_chain(800, 9, compact=True)
+  with engine.Batch([s], cutoff=9.0, skin=2.0, nl_capacity=16) as b:
+    with pytest.raises(_lib.PB2Error) as e:
+      b.nl_build()
+    assert e.value.code == -4
+    assert b.status()[0] & _lib.STATUS_NLOVERFLOW
+
+
+def test_neighbour_list_needs_a_cutoff():
+  s = synth.make_chain(50, 1)
+  with engine.Batch([s]) as b:
+    with pytest.raises(_lib.PB2Error):
+      b.nl_build()
