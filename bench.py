@@ -1,6 +1,9 @@
 #!/usr/bin/env python3
 """Benchmark: aggregate atom-steps/s of the batched implicit-solvent
-Langevin step (ragged batch of seeded synthetic chains, all pairs).
+Langevin step (ragged batch of seeded synthetic chains, all pairs), with the
+plain one-batch-per-system path, end-to-end C-ABI throughput, a served
+request stream (p50/p99 latency), the roofline of the dominant kernel and a
+CPU baseline beside it.
 
 One "step" = one BAOAB step (force evaluation included) of every system of
 the batch.  Workload: 512 systems with atom counts log-uniform in
@@ -34,17 +37,36 @@ UNIT = "atom-steps/s"
 WORKLOAD_SEED = 2024
 N_SYSTEMS = 512
 
+# Algorithmic work per unique pair (i < j) of the far-field path, counted
+# from the kernel source with FMA = 2 flops (pb2_pair.cu run_tile):
+#   descreening: 3 (d) + 5 (r^2) + 2 x 23 (series value) + 2 (sums)      = 56
+#   force:       GB 31 + Coulomb 5 + LJ 12 + 6 (d, r^2 share) + 12 (F)   = 66
+#   chain:       8 (d, r^2) + 1 + 2 x 23 (series derivative) + 4 + 12    = 71
+FLOPS_PER_PAIR = {"born": 56, "force": 66, "chain": 71}
+MUFU_PER_PAIR = {"born": 1, "force": 3, "chain": 1}
+# integrator: read x, p (48 B), F (24 B), mass, sigma, charge (24 B); write
+# x, p (48 B), posq (16 B), clear F (24 B)
+BYTES_PER_ATOM_STEP = 184
+# DRAM traffic per launch of the force pass on this workload, from
+# `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum` (see
+# profiles/tile_kernels_ragged512.md); None until measured for the kernel version
+FORCE_TRAFFIC_BYTES = None
+
 
 def parse():
   ap = argparse.ArgumentParser()
   ap.add_argument("--gpus", type=int, default=1)
-  ap.add_argument("--steps", type=int, default=20)
+  ap.add_argument("--steps", type=int, default=40)
   ap.add_argument("--warmup", type=int, default=3)
   ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
   ap.add_argument("--systems", type=int, default=N_SYSTEMS)
   ap.add_argument("--no-plain", action="store_true")
   ap.add_argument("--no-cpu", action="store_true")
   ap.add_argument("--no-e2e", action="store_true")
+  ap.add_argument("--no-serving", action="store_true")
+  ap.add_argument("--serving-requests", type=int, default=32)
+  ap.add_argument("--serving-rate", type=float, default=20.0)
+  ap.add_argument("--serving-step-scale", type=float, default=0.05)
   return ap.parse_args()
 
 
@@ -60,6 +82,10 @@ def workload(rank: int, n_systems: int):
   return synth.make_batch(n_systems, WORKLOAD_SEED + 7919 * rank, 150, 4000, compact=True)
 
 
+def unique_pairs(systems) -> int:
+  return int(sum(len(s["charges"]) * (len(s["charges"]) - 1) // 2 for s in systems))
+
+
 def cpu_model():
   try:
     for line in open("/proc/cpuinfo"):
@@ -70,29 +96,27 @@ def cpu_model():
   return "unknown"
 
 
-def cpu_reference_run(systems, budget_s=12.0, steps_per_sys=1):
-  """Time the FP64 CPU restatement (oracle) on a bounded sample: one BAOAB
-  step (one force evaluation) per system, systems taken in workload order
-  until the budget is spent.  Returns (atom-steps/s, sample description)."""
-  from oracle import energy as oenergy
-  from oracle import integrator as ointeg
-  from oracle import prng
-  dt, kT, gamma = 1.0 / 48.88821291839, 300 * 0.0019872041, 48.88821291839e-3
-  atoms = 0
-  t_total = 0.0
-  used = 0
+def cpu_reference_run(systems, budget_s=12.0):
+  """The FP64 C/OpenMP restatement of prolix's force field (oracle/) on the
+  host's cores: one force evaluation per system (the O(N) integrator update,
+  under 0.1 % of a step, is left out, which favours the CPU), systems in
+  workload order until the budget is spent.  Returns (atom-steps/s, sample,
+  threads)."""
+  from oracle import cforces
+  threads = cforces.threads()
+  atoms, t_total, used = 0, 0.0, 0
   for s in systems:
-    force = lambda r, s=s: oenergy.energy_forces(s, r)[1]
-    st = ointeg.State(s["positions"], np.zeros_like(s["positions"]), np.zeros_like(s["positions"]),
-                      s["masses"], prng.prng_key(1))
     t0 = time.perf_counter()
-    ointeg.run(st, force, steps_per_sys, dt, kT, gamma)
+    cforces.energy_forces(s, threads=threads)
     t_total += time.perf_counter() - t0
-    atoms += len(s["charges"]) * steps_per_sys
+    atoms += len(s["charges"])
     used += 1
     if t_total > budget_s:
       break
-  return atoms / t_total, f"{used} of {len(systems)} systems x {steps_per_sys} step(s), {atoms} atom-steps"
+  sample = (f"{used} of {len(systems)} systems x 1 step ({atoms} atom-steps); FP64 C/OpenMP "
+            "restatement of prolix's formulas (the reference's JAX path cannot run here: JAX "
+            "is not installed)")
+  return atoms / t_total, sample, threads
 
 
 def clocks_start(path):
@@ -101,7 +125,7 @@ def clocks_start(path):
         ["nvidia-smi", "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
          "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"],
+         "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "100"],
         stdout=open(path, "w"), stderr=subprocess.DEVNULL)
   except OSError:
     return None
@@ -143,34 +167,69 @@ def run_reference(args):
   if rank != 0:
     return 0
   systems = workload(0, args.systems)
-  per_step = []
+  budget = max(2.0, 60.0 / max(args.steps, 1))
   for _ in range(args.warmup):
     cpu_reference_run(systems[:1], budget_s=0.0)
   t0 = time.perf_counter()
   vals = []
+  sample, threads = "", 1
   for _ in range(args.steps):
-    v, sample = cpu_reference_run(systems, budget_s=max(2.0, 60.0 / max(args.steps, 1)))
+    v, sample, threads = cpu_reference_run(systems, budget_s=budget)
     vals.append(v)
-  el = time.perf_counter() - t0
   value = float(np.mean(vals))
-  cores = 1
   line = {
       "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
       "steps": args.steps, "warmup": args.warmup,
-      "ms_per_step": 1e3 * sum(int(s["charges"].shape[0]) for s in systems) / value,
+      "ms_per_step": 1e3 * sum(len(s["charges"]) for s in systems) / value,
       "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
       "data": "synthetic (seeded chains)",
       "config": {"workload": f"{args.systems} systems, N log-uniform 150-4000, all pairs",
-                 "parallelism": "host cores"},
-      "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                       "sample": sample + "; FP64 NumPy restatement of prolix (the reference's "
-                       "JAX path cannot run here: JAX is not installed)",
-                       "cpu": cpu_model()},
+                 "parallelism": f"{threads} host threads"},
+      "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                       "sample": sample, "cpu": cpu_model()},
       "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-      "wall_s": el,
+      "wall_s": time.perf_counter() - t0,
   }
   print(json.dumps(line), flush=True)
   return 0
+
+
+def serving_bench(args):
+  from prolix_b200 import serving
+  reqs = serving.poisson_requests(args.serving_requests, args.serving_rate, WORKLOAD_SEED,
+                                  step_scale=args.serving_step_scale)
+  srv = serving.Server(chunk=50)
+  srv.run(reqs)
+  rep = srv.report()
+  rep.update({"rate_per_s": args.serving_rate, "atoms": "log-uniform 100-10,000",
+              "steps": f"log-uniform 1,000-50,000 x {args.serving_step_scale}",
+              "hbm_budget_gb": 150})
+  return rep
+
+
+def plain_run(systems, stream, steps):
+  """The same systems with one batch (and one set of launches) per system."""
+  import torch
+  from prolix_b200 import engine
+  batches = [engine.Batch([s]) for s in systems]
+  for b in batches:
+    b.langevin_init()
+    b.langevin_run(1, stream)
+  torch.cuda.synchronize()
+  e0 = torch.cuda.Event(enable_timing=True)
+  e1 = torch.cuda.Event(enable_timing=True)
+  e0.record()
+  for _ in range(steps):
+    for b in batches:
+      b.langevin_run(1, stream)
+  e1.record()
+  torch.cuda.synchronize()
+  ms = e0.elapsed_time(e1)
+  n = sum(len(s["charges"]) for s in systems)
+  for b in batches:
+    b.close()
+  return {"value": n * steps / (ms * 1e-3), "unit": UNIT, "steps": steps,
+          "note": "one batch per system, launches issued system after system"}
 
 
 def main():
@@ -190,12 +249,12 @@ def main():
   from prolix_b200 import engine
   systems = workload(rank, args.systems)
   n_atoms = int(sum(len(s["charges"]) for s in systems))
+  pairs = unique_pairs(systems)
   batch = engine.Batch(systems, device=local)
   batch.langevin_init()
   stream = torch.cuda.current_stream().cuda_stream
 
-  # warm-up (also captures the one-step graph)
-  for _ in range(args.warmup):
+  for _ in range(args.warmup):  # also captures the one-step graph
     batch.langevin_run(1, stream)
   torch.cuda.synchronize()
 
@@ -225,24 +284,43 @@ def main():
   status = batch.status()
   if np.any(status):
     print(f"rank {rank}: status flags {np.unique(status)}", file=sys.stderr)
+  value = n_atoms * ws * args.steps / (t_ms * 1e-3)
 
-  total_atoms = n_atoms * ws
-  value = total_atoms * args.steps / (t_ms * 1e-3)
-
-  # per-kernel device times (eager launches with events around each family)
+  # per-kernel device times: eager launches with CUDA events around each
   batch.set_profiling(True)
-  prof_steps = max(3, min(args.steps, 10))
+  prof_steps = 5
   batch.langevin_run(prof_steps, stream)
-  tim = batch.last_timings() / prof_steps
+  tim = batch.last_timings() / prof_steps  # ms per step
   batch.set_profiling(False)
+  names = ["born", "finalize", "force", "chain", "bonded", "integrator", "bbox"]
+  per_kernel = {n: float(v) for n, v in zip(names, tim[:7])}
 
-  # end to end through the C ABI with host buffers: upload state, one step,
-  # read positions back, every step
+  peak = ctypes_fp32_peak(batch)
+  passes = {}
+  for p in ("born", "force", "chain"):
+    ms = per_kernel[p]
+    tf = FLOPS_PER_PAIR[p] * pairs / (ms * 1e-3) / 1e12 if ms > 0 else None
+    passes[p] = {"ms": ms, "tflops": tf, "frac": (tf / peak if tf and peak else None),
+                 "mufu_tops": MUFU_PER_PAIR[p] * pairs / (ms * 1e-3) / 1e12 if ms > 0 else None}
+  dom = max(("born", "force", "chain"), key=lambda p: per_kernel[p])
+  roofline = {"kernel": f"tile_kernel pass '{dom}'", "bound": "fp32",
+              "achieved": passes[dom]["tflops"], "peak": peak, "unit": "TFLOP/s",
+              "frac": passes[dom]["frac"],
+              "traffic": FORCE_TRAFFIC_BYTES if dom == "force" else None,
+              "peak_source": "FP32 FMA throughput measured in this run (pb2_fp32_peak)",
+              "algorithmic_flops_per_launch": FLOPS_PER_PAIR[dom] * pairs,
+              "passes": passes}
+  integ_gbs = BYTES_PER_ATOM_STEP * n_atoms / (per_kernel["integrator"] * 1e-3) / 1e9
+  hbm_peak = _measured_hbm()
+  integrator = {"achieved_gbs": integ_gbs, "peak_gbs": hbm_peak,
+                "frac": integ_gbs / hbm_peak if hbm_peak else None,
+                "bytes_per_atom_step": BYTES_PER_ATOM_STEP}
+
   e2e = None
   if not args.no_e2e:
     st = batch.get_state()
     x_h, p_h = st["position"].copy(), st["momentum"].copy()
-    e2e_steps = max(2, min(args.steps, 5))
+    e2e_steps = 5
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
@@ -252,68 +330,64 @@ def main():
       x_h, p_h = out["position"], out["momentum"]
     torch.cuda.synchronize()
     t_e2e = time.perf_counter() - t0
-    e2e = {"value": total_atoms * e2e_steps / t_e2e, "unit": UNIT,
+    e2e = {"value": n_atoms * ws * e2e_steps / t_e2e, "unit": UNIT,
            "h2d_bytes_per_step": int(2 * 3 * 8 * n_atoms),
-           "d2h_bytes_per_step": int((3 * 3 * 8 + 3 * 8) * n_atoms),
-           "steps": e2e_steps}
+           "d2h_bytes_per_step": int((3 * 3 * 8) * n_atoms + 8 * 2 * len(systems)),
+           "steps": e2e_steps, "path": "pb2_set_state + pb2_langevin_run(1) + pb2_get_state"}
+  batch.close()
 
   plain = None
-  if rank == 0 and not args.no_plain:
-    plain = plain_run(systems, stream, steps=max(2, min(args.steps, 5)))
-
+  serving_rep = None
+  cpu = None
   if rank == 0:
-    cpu = None
+    if not args.no_plain:
+      plain = plain_run(systems, stream, steps=5)
+    if not args.no_serving:
+      serving_rep = serving_bench(args)
     if not args.no_cpu:
-      v, sample = cpu_reference_run(systems, budget_s=12.0)
-      cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
-             "sample": sample + "; FP64 NumPy restatement of prolix (reference JAX path unavailable)",
+      v, sample, threads = cpu_reference_run(systems, budget_s=12.0)
+      cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
              "cpu": cpu_model()}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32 pair / f64 state",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 pair (fixed-point sums) / f64 state",
         "data": "synthetic (seeded chains)",
         "config": {"workload": f"{args.systems} systems, N log-uniform 150-4000 (seed {WORKLOAD_SEED}), "
                                "OBC2 GB + Coulomb + LJ + bonded, all pairs, BAOAB dt 1 fs",
-                   "atoms_per_gpu": n_atoms, "parallelism": f"replicas x{ws}",
+                   "atoms_per_gpu": n_atoms, "unique_pairs_per_gpu": pairs,
+                   "parallelism": f"replicas x{ws}",
                    "l2": "256 MB buffer written between timed steps"},
         "clocks": clocks,
-        "kernel_ms_per_step": {"pair_and_bonded": tim[0], "integrator": tim[2]},
+        "roofline": roofline,
+        "integrator_roofline": integrator,
+        "kernel_ms_per_step": per_kernel,
         "plain": plain,
+        "ragged_over_plain": value / (plain["value"] * ws) if plain else None,
+        "serving": serving_rep,
         "e2e": e2e,
         "cpu_baseline": cpu,
-        "gpu_launches": int(args.steps * 6),
+        # per timed step: step, bbox, born, finalize, force, chain, bonded, finish
+        "gpu_launches": int(args.steps * 8),
     }
     print(json.dumps(line), flush=True)
-  batch.close()
   if pg:
     pg.destroy_process_group()
   return 0
 
 
-def plain_run(systems, stream, steps):
-  """The same systems with one batch (and one set of launches) per system."""
-  import torch
-  from prolix_b200 import engine
-  batches = [engine.Batch([s]) for s in systems]
-  for b in batches:
-    b.langevin_init()
-    b.langevin_run(1, stream)
-  torch.cuda.synchronize()
-  e0 = torch.cuda.Event(enable_timing=True)
-  e1 = torch.cuda.Event(enable_timing=True)
-  e0.record()
-  for _ in range(steps):
-    for b in batches:
-      b.langevin_run(1, stream)
-  e1.record()
-  torch.cuda.synchronize()
-  ms = e0.elapsed_time(e1)
-  n = sum(len(s["charges"]) for s in systems)
-  for b in batches:
-    b.close()
-  return {"value": n * steps / (ms * 1e-3), "unit": UNIT, "steps": steps,
-          "note": "one batch per system, launches issued system after system"}
+def ctypes_fp32_peak(batch):
+  import ctypes
+  v = ctypes.c_double(0.0)
+  rc = batch.lib.pb2_fp32_peak(batch.ctx.handle, ctypes.byref(v))
+  return v.value if rc == 0 else None
+
+
+def _measured_hbm():
+  try:
+    return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+  except (OSError, KeyError, ValueError):
+    return 6650.0  # the profiling recipe's fallback
 
 
 if __name__ == "__main__":

@@ -117,6 +117,9 @@ typedef struct pb2_system_desc {
   double dt;                  /* tau */
   double kT;                  /* kcal/mol */
   double gamma;               /* 1/tau */
+  int32_t use_origin;         /* 1: take origin below; 0: the rounded centroid of positions */
+  double origin[3];           /* A; float32 pair coordinates are taken relative to it, so a
+                                 system moved between batches keeps bit-identical forces */
 } pb2_system_desc;
 
 /* Batch-wide settings. */
@@ -203,12 +206,17 @@ int pb2_nl_check(pb2_batch *batch, int32_t *rebuilt, void *stream);
 int pb2_nl_capacity(const pb2_batch *batch, int32_t *capacity);
 int pb2_nl_get(pb2_batch *batch, int32_t *neighbors, void *stream);
 
-/* Device time of the last pb2_langevin_run / pb2_energy_forces, per kernel
- * family: out[0] = pair kernels, out[1] = bonded, out[2] = integrator,
- * out[3] = neighbour list, out[4] = whole call (milliseconds, CUDA events).
- * Only filled when the batch was created with profiling enabled. */
+/* Device time of the last pb2_langevin_run with profiling enabled (eager
+ * launches, CUDA events around each kernel), milliseconds summed over the
+ * run: out[0] descreening pass, out[1] Born finalize, out[2] force pass,
+ * out[3] chain pass, out[4] bonded, out[5] integrator, out[6] bounding boxes,
+ * out[7] whole run. */
 int pb2_set_profiling(pb2_batch *batch, int enable);
 int pb2_last_timings(pb2_batch *batch, double *out_ms);
+
+/* Measured FP32 FMA throughput of the context's GPU (TFLOP/s), the roofline
+ * denominator of the pair kernels.  Diagnostic: no reference counterpart. */
+int pb2_fp32_peak(pb2_ctx *ctx, double *tflops);
 
 /*
  * Born radii of one system with no device allocation (no counterpart in the

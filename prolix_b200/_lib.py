@@ -48,6 +48,7 @@ class SystemDesc(ctypes.Structure):
       ("k_gb", ctypes.c_double), ("k_coulomb", ctypes.c_double),
       ("key", ctypes.c_uint32 * 2),
       ("dt", ctypes.c_double), ("kT", ctypes.c_double), ("gamma", ctypes.c_double),
+      ("use_origin", ctypes.c_int32), ("origin", ctypes.c_double * 3),
   ]
 
 
@@ -91,6 +92,7 @@ SIGNATURES = [
     ("pb2_nl_get", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("pb2_set_profiling", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("pb2_last_timings", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    ("pb2_fp32_peak", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
     ("pb2_born_radii_noalloc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
                                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
                                               ctypes.c_void_p, ctypes.c_void_p]),

@@ -238,6 +238,11 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
     S.ox = std::round(cx / n);
     S.oy = std::round(cy / n);
     S.oz = std::round(cz / n);
+    if (d.use_origin) {
+      S.ox = d.origin[0];
+      S.oy = d.origin[1];
+      S.oz = d.origin[2];
+    }
     for (int i = 0; i < n; ++i) {
       const int g = o + i;
       hx[g] = d.positions[3 * i];
@@ -475,16 +480,37 @@ extern "C" int pb2_batch_info(const pb2_batch *b, int32_t *n_systems, int64_t *n
 
 // ------------------------------------------------------------ force evaluation
 
+// In profiling mode, time one launch with CUDA events (eager runs only).
+struct Timer {
+  pb2_batch *b;
+  cudaStream_t st;
+  template <class F>
+  cudaError_t operator()(int slot, F &&launch) {
+    if (!b->profiling) return launch();
+    cudaEventRecord(b->ev[0], st);
+    const cudaError_t e = launch();
+    cudaEventRecord(b->ev[1], st);
+    cudaEventSynchronize(b->ev[1]);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]);
+    b->timings[slot] += ms;
+    return e;
+  }
+};
+
 // Force kernels on the current posq; force accumulators must be zero (or
 // hold contributions to keep) and born_acc zero.  bonded_energy: also
 // accumulate the (FP64) bonded energies.
 static cudaError_t enqueue_forces(pb2_batch *b, cudaStream_t st, bool bonded_energy) {
   cudaError_t e;
+  Timer tm{b, st};
   const PairArgs pa = pair_args(b);
   const bool gb = (b->params.terms & PB2_USE_GB) != 0;
-  if ((e = launch_bbox(b->sys, b->blk_sys, b->posq, b->bbox, b->n_blocks, st)) != cudaSuccess) return e;
+  if ((e = tm(kTimBbox, [&] { return launch_bbox(b->sys, b->blk_sys, b->posq, b->bbox, b->n_blocks, st); })) != cudaSuccess)
+    return e;
   if (gb) {
-    if ((e = launch_tiles(PASS_BORN, pa, b->grid_pair[PASS_BORN], st)) != cudaSuccess) return e;
+    if ((e = tm(kTimBorn, [&] { return launch_tiles(PASS_BORN, pa, b->grid_pair[PASS_BORN], st); })) != cudaSuccess)
+      return e;
     FinalizeArgs fa;
     fa.sys = b->sys;
     fa.atom_sys = b->atom_sys;
@@ -497,14 +523,16 @@ static cudaError_t enqueue_forces(pb2_batch *b, cudaStream_t st, bool bonded_ene
     fa.born64 = nullptr;
     fa.n_total = b->n_total;
     fa.energy_mode = 0;
-    if ((e = launch_born_finalize(fa, st)) != cudaSuccess) return e;
+    if ((e = tm(kTimFinalize, [&] { return launch_born_finalize(fa, st); })) != cudaSuccess) return e;
   }
-  if ((e = launch_tiles(PASS_FORCE, pa, b->grid_pair[PASS_FORCE], st)) != cudaSuccess) return e;
+  if ((e = tm(kTimForce, [&] { return launch_tiles(PASS_FORCE, pa, b->grid_pair[PASS_FORCE], st); })) != cudaSuccess)
+    return e;
   if (gb)
-    if ((e = launch_tiles(PASS_CHAIN, pa, b->grid_pair[PASS_CHAIN], st)) != cudaSuccess) return e;
+    if ((e = tm(kTimChain, [&] { return launch_tiles(PASS_CHAIN, pa, b->grid_pair[PASS_CHAIN], st); })) != cudaSuccess)
+      return e;
   BondedArgs ba = b->bonded;
   ba.energy_mode = bonded_energy ? 1 : 0;
-  return launch_bonded(ba, b->grid_bonded, st);
+  return tm(kTimBonded, [&] { return launch_bonded(ba, b->grid_bonded, st); });
 }
 
 // FP64 pair energies (GB polar incl. self, ACE, Coulomb, LJ) into b->energy.
@@ -648,29 +676,15 @@ extern "C" int pb2_set_positions(pb2_batch *b, const double *positions, void *st
 
 static int run_eager(pb2_batch *b, int n_steps, cudaStream_t st) {
   pb2_ctx *ctx = b->ctx;
+  Timer tm{b, st};
   for (int t = 0; t < n_steps; ++t) {
-    const int parity = b->key_parity;
-    if (b->profiling) CUDA_TRY(ctx, cudaEventRecord(b->ev[0], st));
-    CUDA_TRY(ctx, launch_step(int_args(b, parity, t > 0), st));
-    if (b->profiling) {
-      CUDA_TRY(ctx, cudaEventRecord(b->ev[1], st));
-      CUDA_TRY(ctx, cudaEventSynchronize(b->ev[1]));
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]);
-      b->timings[kFamInt] += ms;
-      CUDA_TRY(ctx, cudaEventRecord(b->ev[0], st));
-    }
+    const IntArgs ia = int_args(b, b->key_parity, t > 0);
+    CUDA_TRY(ctx, tm(kTimStep, [&] { return launch_step(ia, st); }));
     CUDA_TRY(ctx, enqueue_forces(b, st, false));
-    if (b->profiling) {
-      CUDA_TRY(ctx, cudaEventRecord(b->ev[1], st));
-      CUDA_TRY(ctx, cudaEventSynchronize(b->ev[1]));
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]);
-      b->timings[kFamPair] += ms;
-    }
     b->key_parity ^= 1;
   }
-  CUDA_TRY(ctx, launch_finish(int_args(b, b->key_parity, 0), st));
+  const IntArgs fa = int_args(b, b->key_parity, 0);
+  CUDA_TRY(ctx, tm(kTimStep, [&] { return launch_finish(fa, st); }));
   return PB2_OK;
 }
 
@@ -733,8 +747,18 @@ extern "C" int pb2_langevin_run(pb2_batch *b, int32_t n_steps, void *stream) {
   }
   if (b->profiling) {
     for (double &t : b->timings) t = 0.0;
-    CUDA_TRY(ctx, cudaEventRecord(b->ev[0], st));
+    cudaEvent_t a0, a1;
+    cudaEventCreate(&a0);
+    cudaEventCreate(&a1);
+    cudaEventRecord(a0, st);
     int rc = run_eager(b, n_steps, st);
+    cudaEventRecord(a1, st);
+    cudaEventSynchronize(a1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a0, a1);
+    b->timings[kTimAll] = ms;
+    cudaEventDestroy(a0);
+    cudaEventDestroy(a1);
     if (rc) return rc;
     CUDA_TRY(ctx, cudaStreamSynchronize(st));
     return PB2_OK;
@@ -815,7 +839,7 @@ extern "C" int pb2_set_profiling(pb2_batch *b, int enable) {
 
 extern "C" int pb2_last_timings(pb2_batch *b, double *out_ms) {
   if (!b || !out_ms) return PB2_EINVAL;
-  for (int k = 0; k < 5; ++k) out_ms[k] = b->timings[k];
+  for (int k = 0; k < kTimSlots; ++k) out_ms[k] = b->timings[k];
   return PB2_OK;
 }
 

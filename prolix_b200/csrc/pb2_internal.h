@@ -18,8 +18,9 @@ struct pb2_ctx {
   std::string err;
 };
 
-// timing families of pb2_last_timings
-constexpr int kFamPair = 0, kFamBonded = 1, kFamInt = 2, kFamNl = 3, kFamAll = 4;
+// slots of pb2_last_timings
+constexpr int kTimBorn = 0, kTimFinalize = 1, kTimForce = 2, kTimChain = 3, kTimBonded = 4,
+              kTimStep = 5, kTimBbox = 6, kTimAll = 7, kTimSlots = 8;
 
 // Device allocations owned by a batch, freed with it.
 struct Dev {
@@ -78,7 +79,7 @@ struct pb2_batch {
   cudaStream_t cap_stream = nullptr;
   std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
   bool profiling = false;
-  double timings[5] = {0, 0, 0, 0, 0};
+  double timings[kTimSlots] = {0, 0, 0, 0, 0, 0, 0, 0};
   cudaEvent_t ev[2] = {nullptr, nullptr};
   // neighbour list (allocated on first build)
   Dev nl;

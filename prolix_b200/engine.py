@@ -134,7 +134,14 @@ def prepare_system(system: dict, *, dt=None, kT=None, gamma=None, key=None, eps_
   out["dt"] = float(system.get("dt", dt if dt is not None else akma_dt(1.0)))
   out["kT"] = float(system.get("kT", kT if kT is not None else 300.0 * KB_KCAL))
   out["gamma"] = float(system.get("gamma", gamma if gamma is not None else akma_gamma(1.0)))
+  out["origin"] = None if system.get("origin") is None else tuple(float(v) for v in system["origin"])
   return out
+
+
+def default_origin(positions) -> tuple:
+  """The origin a batch picks for a system: its rounded centroid (A)."""
+  c = np.asarray(positions, dtype=np.float64).reshape(-1, 3).mean(axis=0)
+  return tuple(float(v) for v in np.round(c))
 
 
 def _desc(p) -> _lib.SystemDesc:
@@ -163,6 +170,9 @@ def _desc(p) -> _lib.SystemDesc:
   d.k_gb, d.k_coulomb = s["k_gb"], s["k_coulomb"]
   d.key[0], d.key[1] = p["key"]
   d.dt, d.kT, d.gamma = p["dt"], p["kT"], p["gamma"]
+  if p["origin"] is not None:
+    d.use_origin = 1
+    d.origin[0], d.origin[1], d.origin[2] = p["origin"]
   return d
 
 
@@ -276,7 +286,9 @@ class Batch:
     self._check(self.lib.pb2_set_profiling(self.handle, 1 if enable else 0))
 
   def last_timings(self):
-    t = np.zeros(5)
+    """Device ms of the last profiled run: born, finalize, force, chain,
+    bonded, integrator, bounding boxes, whole run."""
+    t = np.zeros(8)
     self._check(self.lib.pb2_last_timings(self.handle, t.ctypes.data))
     return t
 

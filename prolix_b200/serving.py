@@ -1,0 +1,279 @@
+"""Continuous-batching server for "run K Langevin steps of system S" jobs.
+
+Requests that arrive while others run join the device batch at the next
+tick: each tick advances every active system by the same number of steps
+(at most ``chunk``, and never past the nearest completion), then finished,
+cancelled or failed requests leave and waiting requests are admitted while
+the batch stays inside the atom and HBM budgets.  All systems of a tick
+share one launch per kernel (the ragged batch), so short and long, small
+and large jobs overlap on the GPU.
+
+Systems never interact and forces use order-independent fixed-point sums,
+so a request's result is bit-identical whether it ran alone or in any mix
+(checked by tests/test_gpu_serving.py).  A request whose state turns
+non-finite is evicted with an error; the others carry on unchanged.
+
+This has no counterpart in prolix (whose batched runs are offline
+``batched_produce`` calls, batched_simulate.py:1125-1163); it drives the
+same BAOAB step.
+"""
+
+from __future__ import annotations
+
+import dataclasses
+import math
+import time
+from collections import deque
+
+import numpy as np
+
+from . import engine
+from ._lib import STATUS_FORCE_RANGE, STATUS_NONFINITE
+
+BYTES_PER_ATOM = 320  # device footprint of one atom in a batch (state, pair data, scratch)
+
+
+@dataclasses.dataclass
+class Request:
+  system: dict
+  n_steps: int
+  key: tuple = (0, 0)
+  dt: float = engine.akma_dt(1.0)
+  kT: float = 300.0 * engine.KB_KCAL
+  gamma: float = engine.akma_gamma(1.0)
+  arrival: float = 0.0          # seconds (server clock)
+  rid: int = -1
+
+
+@dataclasses.dataclass
+class Result:
+  rid: int
+  position: np.ndarray | None
+  momentum: np.ndarray | None
+  key: np.ndarray | None
+  steps: int
+  arrival: float
+  admitted: float
+  finished: float
+  error: str | None = None
+
+  @property
+  def latency(self) -> float:
+    return self.finished - self.arrival
+
+
+@dataclasses.dataclass
+class _Slot:
+  req: Request
+  x: np.ndarray
+  p: np.ndarray
+  key: np.ndarray
+  done: int
+  admitted: float
+
+
+def _percentile(v, q):
+  return float(np.percentile(np.asarray(v), q)) if len(v) else float("nan")
+
+
+class Server:
+  """Admission by budget, resident state, continuous batching."""
+
+  def __init__(self, device: int = 0, hbm_budget_bytes: float = 150e9,
+               max_batch_atoms: int = 1_000_000, chunk: int = 50, cutoff: float = 0.0,
+               clock=time.perf_counter, batch_factory=None):
+    self.device = device
+    self.batch_factory = batch_factory or engine.Batch
+    self.hbm_budget = float(hbm_budget_bytes)
+    self.max_atoms = int(max_batch_atoms)
+    self.chunk = int(chunk)
+    self.cutoff = float(cutoff)
+    self.clock = clock
+    self.t0 = clock()
+    self.queue: deque[Request] = deque()
+    self.active: list[_Slot] = []
+    self.results: dict[int, Result] = {}
+    self.cancelled: set[int] = set()
+    self._next_id = 0
+    self._batch = None
+    self._batch_ids = None
+    self.atom_steps = 0
+    self.ticks = 0
+
+  # ------------------------------------------------------------------ api
+  def now(self) -> float:
+    return self.clock() - self.t0
+
+  def submit(self, req: Request) -> int:
+    if req.rid < 0:
+      req.rid = self._next_id
+      self._next_id += 1
+    else:
+      self._next_id = max(self._next_id, req.rid + 1)
+    n = len(req.system["charges"])
+    if n * BYTES_PER_ATOM > self.hbm_budget or n > self.max_atoms:
+      self.results[req.rid] = Result(req.rid, None, None, None, 0, req.arrival, float("nan"),
+                                     self.now(), error="system larger than the server budget")
+      return req.rid
+    self.queue.append(req)
+    return req.rid
+
+  def cancel(self, rid: int):
+    self.cancelled.add(rid)
+
+  def idle(self) -> bool:
+    return not self.queue and not self.active
+
+  # ------------------------------------------------------------------ internals
+  def _used(self):
+    atoms = sum(len(s.req.system["charges"]) for s in self.active)
+    return atoms, atoms * BYTES_PER_ATOM
+
+  def _admit(self, now: float):
+    atoms, used = self._used()
+    admitted = []
+    while self.queue and self.queue[0].arrival <= now:
+      req = self.queue[0]
+      if req.rid in self.cancelled:
+        self.queue.popleft()
+        self.results[req.rid] = Result(req.rid, None, None, None, 0, req.arrival, float("nan"),
+                                       now, error="cancelled")
+        continue
+      n = len(req.system["charges"])
+      if atoms + n > self.max_atoms or used + n * BYTES_PER_ATOM > self.hbm_budget:
+        break  # first-come first-served: wait for room
+      self.queue.popleft()
+      admitted.append(req)
+      atoms += n
+      used += n * BYTES_PER_ATOM
+    if not admitted:
+      return False
+    # fix each system's float32 frame for its lifetime (bit-identical forces
+    # whatever batch it runs in), then draw initial momenta from its key
+    for r in admitted:
+      if r.system.get("origin") is None:
+        r.system = dict(r.system, origin=engine.default_origin(r.system["positions"]))
+    systems = [dict(r.system, key=r.key, dt=r.dt, kT=r.kT, gamma=r.gamma) for r in admitted]
+    with self.batch_factory(systems, cutoff=self.cutoff, device=self.device) as nb:
+      nb.langevin_init()
+      st = nb.get_state()
+      status = nb.status()
+    for k, r in enumerate(admitted):
+      lo, hi = nb.offsets[k], nb.offsets[k + 1]
+      if status[k] & (STATUS_NONFINITE | STATUS_FORCE_RANGE) or not np.isfinite(st["position"][lo:hi]).all():
+        self._fail(r, now, now, "non-finite initial state")
+        continue
+      self.active.append(_Slot(r, st["position"][lo:hi].copy(), st["momentum"][lo:hi].copy(),
+                               st["key"][k].copy(), 0, now))
+    return True
+
+  def _fail(self, req, admitted, now, msg):
+    self.results[req.rid] = Result(req.rid, None, None, None, 0, req.arrival, admitted, now,
+                                   error=msg)
+
+  def _build(self):
+    systems = [dict(s.req.system, positions=s.x, key=tuple(int(v) for v in s.key), dt=s.req.dt,
+                    kT=s.req.kT, gamma=s.req.gamma) for s in self.active]
+    if self._batch is not None:
+      self._batch.close()
+    self._batch = self.batch_factory(systems, cutoff=self.cutoff, device=self.device,
+                                     graph_chunk=self.chunk)
+    self._batch.set_state(position=np.concatenate([s.x for s in self.active]),
+                          momentum=np.concatenate([s.p for s in self.active]),
+                          key=np.stack([s.key for s in self.active]))
+    self._batch_ids = [s.req.rid for s in self.active]
+
+  def _save(self):
+    st = self._batch.get_state()
+    for k, s in enumerate(self.active):
+      lo, hi = self._batch.offsets[k], self._batch.offsets[k + 1]
+      s.x = st["position"][lo:hi].copy()
+      s.p = st["momentum"][lo:hi].copy()
+      s.key = st["key"][k].copy()
+    return self._batch.status(clear=True)
+
+  def tick(self) -> bool:
+    """Admit, advance every active system, retire.  False when idle."""
+    now = self.now()
+    changed = self._admit(now)
+    if self.cancelled:
+      keep = [s for s in self.active if s.req.rid not in self.cancelled]
+      for s in self.active:
+        if s.req.rid in self.cancelled and s.req.rid not in self.results:
+          self._fail(s.req, s.admitted, now, "cancelled")
+      changed |= len(keep) != len(self.active)
+      self.active = keep
+    if not self.active:
+      if self._batch is not None:
+        self._batch.close()
+        self._batch = None
+      return bool(self.queue)
+    if changed or self._batch is None or self._batch_ids != [s.req.rid for s in self.active]:
+      self._build()
+    n = min(self.chunk, min(s.req.n_steps - s.done for s in self.active))
+    self._batch.langevin_run(n)
+    status = self._save()
+    self.ticks += 1
+    now = self.now()
+    keep = []
+    for k, s in enumerate(self.active):
+      s.done += n
+      self.atom_steps += n * len(s.req.system["charges"])
+      if status[k] & (STATUS_NONFINITE | STATUS_FORCE_RANGE) or not np.isfinite(s.x).all():
+        self._fail(s.req, s.admitted, now, "non-finite state: evicted")
+      elif s.done >= s.req.n_steps:
+        self.results[s.req.rid] = Result(s.req.rid, s.x, s.p, s.key, s.done, s.req.arrival,
+                                         s.admitted, now)
+      else:
+        keep.append(s)
+    self.active = keep
+    return True
+
+  def run(self, requests=(), until_idle=True, sleep=time.sleep):
+    """Feed requests at their arrival times (server clock) and serve them."""
+    pending = deque(sorted(requests, key=lambda r: r.arrival))
+    while True:
+      now = self.now()
+      while pending and pending[0].arrival <= now:
+        self.submit(pending.popleft())
+      if self.active or (self.queue and self.queue[0].arrival <= now):
+        self.tick()
+      elif pending:
+        sleep(max(0.0, pending[0].arrival - self.now()))
+      elif self.queue:
+        sleep(max(0.0, self.queue[0].arrival - self.now()))
+      elif until_idle:
+        break
+    if self._batch is not None:
+      self._batch.close()
+      self._batch = None
+    return self.results
+
+  def report(self) -> dict:
+    ok = [r for r in self.results.values() if r.error is None]
+    lat = [r.latency for r in ok]
+    span = max((r.finished for r in ok), default=0.0) - min((r.arrival for r in ok), default=0.0)
+    return {"requests": len(self.results), "completed": len(ok),
+            "failed": len(self.results) - len(ok),
+            "p50_s": _percentile(lat, 50), "p99_s": _percentile(lat, 99),
+            "atom_steps": int(self.atom_steps), "span_s": span,
+            "atom_steps_per_s": self.atom_steps / span if span > 0 else float("nan"),
+            "ticks": self.ticks}
+
+
+def poisson_requests(n: int, rate: float, seed: int, n_lo=100, n_hi=10_000, k_lo=1_000,
+                     k_hi=50_000, step_scale=1.0):
+  """Seeded request stream: Poisson arrivals at ``rate``/s, atoms and steps
+  log-uniform; ``step_scale`` shrinks the step counts for bounded runs."""
+  from . import synth
+  rng = np.random.default_rng(seed)
+  t = np.cumsum(rng.exponential(1.0 / rate, size=n))
+  sizes = np.exp(rng.uniform(math.log(n_lo), math.log(n_hi), size=n)).astype(int)
+  steps = np.exp(rng.uniform(math.log(k_lo), math.log(k_hi), size=n))
+  steps = np.maximum(1, (steps * step_scale).astype(int))
+  reqs = []
+  for i in range(n):
+    sys_ = synth.make_chain(int(sizes[i]), seed * 100003 + i, compact=True)
+    reqs.append(Request(system=sys_, n_steps=int(steps[i]), key=(0, int(seed * 7 + i)),
+                        arrival=float(t[i]), rid=i))
+  return reqs
