@@ -70,6 +70,7 @@ static PairArgs pair_args(pb2_batch *b) {
   a.born = b->born;
   a.bbox = b->bbox;
   a.cut = b->cut ? 1 : 0;
+  a.sched = b->sched;
   a.born_acc = b->born_acc;
   a.dedb_acc = b->dedb_acc;
   a.fx = b->fx;
@@ -371,6 +372,7 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   b->par = D.alloc<float4>(N);
   b->born = D.alloc<float4>(N);
   b->bbox = D.alloc<float4>(2 * (size_t)blocks_total);
+  b->sched = D.alloc<int32_t>(8);
   b->blk_sys = D.alloc<int32_t>(blocks_total);
   b->n_blocks = blocks_total;
   b->cut = cutoff_mode || gb_cut_mode;
@@ -436,6 +438,7 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   CUDA_TRY(ctx, cudaMemset(b->dedb_acc, 0, N * sizeof(long long)));
   CUDA_TRY(ctx, cudaMemset(b->born, 0, N * sizeof(float4)));
   CUDA_TRY(ctx, cudaMemset(b->steps, 0, n_systems * sizeof(long long)));
+  CUDA_TRY(ctx, cudaMemset(b->sched, 0, 8 * sizeof(int32_t)));
   CUDA_TRY(ctx, cudaMemset(b->status, 0, n_systems * sizeof(uint32_t)));
   B.atom_sys = b->atom_sys;
   B.x = b->x; B.y = b->y; B.z = b->z;
@@ -451,6 +454,7 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
 
   // launch shapes: persistent grids sized to the resident capacity
   for (int p = 0; p < 3; ++p) {
+    // one resident wave; warps take items dynamically
     const int cap = tile_kernel_occupancy(p, b->cut) * ctx->sm_count;
     b->grid_pair[p] = std::max(1, std::min(cap, (b->n_items + 7) / 8));
   }
@@ -504,11 +508,12 @@ struct Timer {
 static cudaError_t enqueue_forces(pb2_batch *b, cudaStream_t st, bool bonded_energy) {
   cudaError_t e;
   Timer tm{b, st};
-  const PairArgs pa = pair_args(b);
+  PairArgs pa = pair_args(b);
   const bool gb = (b->params.terms & PB2_USE_GB) != 0;
   if ((e = tm(kTimBbox, [&] { return launch_bbox(b->sys, b->blk_sys, b->posq, b->bbox, b->n_blocks, st); })) != cudaSuccess)
     return e;
   if (gb) {
+    pa.sched = b->sched + 2 * PASS_BORN;
     if ((e = tm(kTimBorn, [&] { return launch_tiles(PASS_BORN, pa, b->grid_pair[PASS_BORN], st); })) != cudaSuccess)
       return e;
     FinalizeArgs fa;
@@ -525,8 +530,10 @@ static cudaError_t enqueue_forces(pb2_batch *b, cudaStream_t st, bool bonded_ene
     fa.energy_mode = 0;
     if ((e = tm(kTimFinalize, [&] { return launch_born_finalize(fa, st); })) != cudaSuccess) return e;
   }
+  pa.sched = b->sched + 2 * PASS_FORCE;
   if ((e = tm(kTimForce, [&] { return launch_tiles(PASS_FORCE, pa, b->grid_pair[PASS_FORCE], st); })) != cudaSuccess)
     return e;
+  pa.sched = b->sched + 2 * PASS_CHAIN;
   if (gb)
     if ((e = tm(kTimChain, [&] { return launch_tiles(PASS_CHAIN, pa, b->grid_pair[PASS_CHAIN], st); })) != cudaSuccess)
       return e;

@@ -60,6 +60,7 @@ struct pb2_batch {
   double *mass = nullptr, *sigma = nullptr, *charge = nullptr, *radius = nullptr;
   float4 *posq = nullptr, *par = nullptr, *born = nullptr, *bbox = nullptr;
   int32_t *blk_sys = nullptr;
+  int32_t *sched = nullptr;  // per pass: (next item, finished warps)
   int n_blocks = 0;
   double *q64 = nullptr, *hs64 = nullptr, *se64 = nullptr, *ro64 = nullptr, *sr64 = nullptr;
   double *born64 = nullptr;

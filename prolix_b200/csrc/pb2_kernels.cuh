@@ -26,6 +26,7 @@ struct PairArgs {
   long long *fx, *fy, *fz;
   long long *energy;
   int32_t cut;              // any cutoff active
+  int32_t *sched;           // (next item, finished warps) of this pass; zero between launches
 };
 struct FinalizeArgs {
   const SysInfo *sys;

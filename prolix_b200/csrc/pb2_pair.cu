@@ -34,6 +34,11 @@
 #ifndef PB2_UNROLL
 #define PB2_UNROLL 4
 #endif
+// Minimum resident blocks per SM asked of the register allocator (bounds
+// registers per thread at 65536 / (256 * PB2_MINB)).
+#ifndef PB2_MINB
+#define PB2_MINB 3
+#endif
 
 namespace pb2 {
 
@@ -67,8 +72,20 @@ __device__ __forceinline__ float obc_far_der(float s, float inv_r, float inv_r2)
 }
 
 struct PData {  // per-atom data a lane holds (its i atom, or the j atom passing through)
-  float x, y, z, q, hs, se, ro, sr, B, iB, dedi;
+  float x, y, z, q, hs, se, ro, sr, B, iB, dedi;  // iB = sqrt(log2 e / 4) / B
 };
+
+// Both directions of a pair inside the series' domain: r - s >= rho~ and
+// (s/r)^2 <= kSeriesU.
+__device__ __forceinline__ bool far_pair(float r, float r2, const PData &I, const PData &J) {
+  const float lim = kSeriesU * r2;
+  return (J.sr * J.sr <= lim) && (I.sr * I.sr <= lim) && (r - J.sr >= I.ro) && (r - I.sr >= J.ro);
+}
+
+// 4 / log2(e), and sqrt(log2(e) / 4): the force pass stores 1/B pre-scaled by
+// sqrt(log2(e)/4) so that exp(-r^2 / (4 B_i B_j)) = exp2(-r^2 iB_i iB_j).
+constexpr float kInvQuarterLog2e = 2.7725887222397811f;
+constexpr float kSqrtQuarterLog2e = 0.60056120439322491f;
 struct Acc {
   float a0, a1, a2, a3;
 };
@@ -90,44 +107,59 @@ __device__ __forceinline__ void run_tile(const PData &I, PData &J, Acc &ti, Acc 
     const float dx = I.x - J.x, dy = I.y - J.y, dz = I.z - J.z;
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
     if (PASS != PASS_FORCE && CUT) ok = ok && (K.gcut2 == 0.f || r2 < K.gcut2);
-    if (ok) {
+    if (PASS == PASS_BORN || PASS == PASS_CHAIN) {
+      // All lanes evaluate (results of invalid pairs are discarded), so the
+      // warp vote below is reached by every lane of the warp.
+      const float inv_r = rsqrtf(r2);
+      const float inv_r2 = inv_r * inv_r;
+      float vij, vji;
       if (PASS == PASS_BORN) {
-        const float inv_r = rsqrtf(r2);
-        if (FAR) {
-          ti.a0 += obc_far_val(J.sr, inv_r);
-          tj.a0 += obc_far_val(I.sr, inv_r);
-        } else {
-          const float r = r2 * inv_r;
-          ti.a0 += obc_integral(r, inv_r, I.ro, J.sr);
-          tj.a0 += obc_integral(r, inv_r, J.ro, I.sr);
-        }
-      } else if (PASS == PASS_CHAIN) {
-        const float inv_r = rsqrtf(r2);
-        float dij, dji;
-        if (FAR) {
-          const float inv_r2 = inv_r * inv_r;
-          dij = obc_far_der(J.sr, inv_r, inv_r2);
-          dji = obc_far_der(I.sr, inv_r, inv_r2);
-        } else {
-          const float r = r2 * inv_r;
-          dij = obc_integral_dr(r, inv_r, I.ro, J.sr);
-          dji = obc_integral_dr(r, inv_r, J.ro, I.sr);
-        }
-        const float g = (I.dedi * dij + J.dedi * dji) * inv_r;
-        ti.a0 -= g * dx; ti.a1 -= g * dy; ti.a2 -= g * dz;
-        tj.a0 += g * dx; tj.a1 += g * dy; tj.a2 += g * dz;
+        vij = obc_far_val(J.sr, inv_r);
+        vji = obc_far_val(I.sr, inv_r);
       } else {
+        vij = obc_far_der(J.sr, inv_r, inv_r2);
+        vji = obc_far_der(I.sr, inv_r, inv_r2);
+      }
+      if (!FAR) {
+        // near tile: the series holds for most pairs; the closed form runs
+        // only for lanes whose pair lies inside the far-field bound
+        const float r = r2 * inv_r;
+        const bool need = ok && !far_pair(r, r2, I, J);
+        if (__any_sync(kFull, need)) {
+          if (need) {
+            if (PASS == PASS_BORN) {
+              vij = obc_integral(r, inv_r, I.ro, J.sr);
+              vji = obc_integral(r, inv_r, J.ro, I.sr);
+            } else {
+              vij = obc_integral_dr(r, inv_r, I.ro, J.sr);
+              vji = obc_integral_dr(r, inv_r, J.ro, I.sr);
+            }
+          }
+        }
+      }
+      if (ok) {
+        if (PASS == PASS_BORN) {
+          ti.a0 += vij;
+          tj.a0 += vji;
+        } else {
+          const float g = (I.dedi * vij + J.dedi * vji) * inv_r;
+          ti.a0 -= g * dx; ti.a1 -= g * dy; ti.a2 -= g * dz;
+          tj.a0 += g * dx; tj.a1 += g * dy; tj.a2 += g * dz;
+        }
+      }
+    } else if (ok) {
+      {
         float g = 0.f;
         const float qq = I.q * J.q;
         if (K.use_gb && (!CUT || K.gcut2 == 0.f || r2 < K.gcut2)) {
-          const float inv_d = I.iB * J.iB;
-          const float ex = expf(-0.25f * r2 * inv_d);
+          const float w = r2 * (I.iB * J.iB);  // r^2 log2(e) / (4 B_i B_j)
+          const float ex = exp2f(-w);
           const float f2 = fmaf(I.B * J.B, ex, r2);
           const float inv_f = rsqrtf(f2);
           const float inv_f3 = inv_f * inv_f * inv_f;
           const float pq = K.pref * qq;
           g = 2.0f * pq * (1.0f - 0.25f * ex) * inv_f3;
-          const float c = -pq * ex * fmaf(0.25f * r2, inv_d, 1.0f) * inv_f3;
+          const float c = -pq * ex * fmaf(w, kInvQuarterLog2e * 0.25f, 1.0f) * inv_f3;
           ti.a3 += c * J.B;
           tj.a3 += c * I.B;
         }
@@ -182,15 +214,17 @@ __device__ __forceinline__ void load_pdata(const PairArgs &a, int g, int pass, b
   P.B = P.iB = P.dedi = 0.f;
   if ((pass == PASS_FORCE && use_gb) || pass == PASS_CHAIN) {
     const float4 b = a.born[g];
-    P.B = b.x; P.iB = b.y;
+    P.B = b.x; P.iB = b.y * kSqrtQuarterLog2e;
     if (pass == PASS_CHAIN) P.dedi = (float)((double)a.dedb_acc[g] * kForceInv) * b.z;
   }
 }
 
+// Work items are handed out dynamically: each warp takes the next item from
+// an atomic counter (items are sorted by cost, largest first), and the last
+// warp to finish resets the counter for the next launch.
 template <int PASS, bool CUT>
-__global__ void __launch_bounds__(256) tile_kernel(const PairArgs a) {
+__global__ void __launch_bounds__(256, PB2_MINB) tile_kernel(const PairArgs a) {
   const int lane = threadIdx.x & 31;
-  const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
   TileConst K;
   K.use_gb = (a.terms & PB2_USE_GB) != 0;
@@ -199,7 +233,11 @@ __global__ void __launch_bounds__(256) tile_kernel(const PairArgs a) {
   K.src = (lane + 1) & 31;
   const uint32_t diag_mask = lane == 31 ? 0u : (0xffffffffu << (lane + 1));
 
-  for (int it = warp; it < a.n_items; it += nwarps) {
+  for (;;) {
+    int it = 0;
+    if (lane == 0) it = atomicAdd(&a.sched[0], 1);
+    it = __shfl_sync(kFull, it, 0);
+    if (it >= a.n_items) break;
     const TileItem item = a.items[it];
     const SysInfo &S = a.sys[item.sys];
     const int n = S.n, off = S.off;
@@ -297,6 +335,11 @@ __global__ void __launch_bounds__(256) tile_kernel(const PairArgs a) {
         if (PASS == PASS_FORCE && K.use_gb) atomic_add_fix(&a.dedb_acc[ig], ai3);
       }
     }
+  }
+  if (lane == 0 && atomicAdd(&a.sched[1], 1) == nwarps - 1) {
+    // every warp has stopped taking items: reset for the next launch
+    a.sched[0] = 0;
+    a.sched[1] = 0;
   }
 }
 
