@@ -254,6 +254,8 @@ def main():
   batch.langevin_init()
   stream = torch.cuda.current_stream().cuda_stream
 
+  from prolix_b200 import autotune
+  tuned = autotune.tune(batch, candidates=(2, 4, 8, 16, 32), steps=3, use_cache=False)
   for _ in range(args.warmup):  # also captures the one-step graph
     batch.langevin_run(1, stream)
   torch.cuda.synchronize()
@@ -357,7 +359,9 @@ def main():
                                "OBC2 GB + Coulomb + LJ + bonded, all pairs, BAOAB dt 1 fs",
                    "atoms_per_gpu": n_atoms, "unique_pairs_per_gpu": pairs,
                    "parallelism": f"replicas x{ws}",
-                   "l2": "256 MB buffer written between timed steps"},
+                   "l2": "256 MB buffer written between timed steps",
+                   "tile_segment": tuned["segment"],
+                   "autotune_ms_per_step": tuned["timings"]},
         "clocks": clocks,
         "roofline": roofline,
         "integrator_roofline": integrator,

@@ -211,6 +211,12 @@ int pb2_nl_get(pb2_batch *batch, int32_t *neighbors, void *stream);
  * run: out[0] descreening pass, out[1] Born finalize, out[2] force pass,
  * out[3] chain pass, out[4] bonded, out[5] integrator, out[6] bounding boxes,
  * out[7] whole run. */
+/* Tiles per work item of the pair kernels (the autotuned knob).  Setting it
+ * rebuilds the work list and drops captured graphs.  No reference
+ * counterpart (prolix's tile sizes are fixed, physics/tiling.py:29-50). */
+int pb2_set_tile_segment(pb2_batch *batch, int32_t segment);
+int pb2_get_tile_segment(const pb2_batch *batch, int32_t *segment);
+
 int pb2_set_profiling(pb2_batch *batch, int enable);
 int pb2_last_timings(pb2_batch *batch, double *out_ms);
 

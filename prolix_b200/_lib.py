@@ -90,6 +90,8 @@ SIGNATURES = [
     ("pb2_nl_check", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32), ctypes.c_void_p]),
     ("pb2_nl_capacity", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]),
     ("pb2_nl_get", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("pb2_set_tile_segment", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    ("pb2_get_tile_segment", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]),
     ("pb2_set_profiling", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("pb2_last_timings", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     ("pb2_fp32_peak", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),

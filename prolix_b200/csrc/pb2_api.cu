@@ -106,6 +106,22 @@ static IntArgs int_args(pb2_batch *b, int parity, int finish_prev) {
 
 IntArgs int_args_for_nl(pb2_batch *b) { return int_args(b, b->key_parity, 0); }
 
+// Tile work items: for each system and i-block, its tiles (iblk, jb >= iblk)
+// cut into segments of `seg` tiles; sorted by tile count, largest first
+// (the kernels hand them out dynamically).
+static std::vector<TileItem> build_items(const std::vector<SysInfo> &sinfo, int seg) {
+  std::vector<TileItem> items;
+  for (int s = 0; s < (int)sinfo.size(); ++s) {
+    const int nblk = sinfo[s].nblk;
+    for (int ib = 0; ib < nblk; ++ib)
+      for (int j0 = ib; j0 < nblk; j0 += seg) items.push_back(TileItem{s, ib, j0, std::min(j0 + seg, nblk)});
+  }
+  std::stable_sort(items.begin(), items.end(), [](const TileItem &p, const TileItem &q) {
+    return (p.jb1 - p.jb0) > (q.jb1 - q.jb0);
+  });
+  return items;
+}
+
 static int validate(pb2_ctx *ctx, const pb2_system_desc &d, int s) {
   char buf[256];
   auto bad = [&](const char *what) {
@@ -302,16 +318,9 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
       if (d.excl_kind[k] == 0) row.excl |= 1u << (j & 31);
       else row.s14 |= 1u << (j & 31);
     }
-    // tile work items: row iblk, tiles jb in [iblk, nblk) in segments
-    const int seg = b->params.tile_segment;
-    for (int ib = 0; ib < S.nblk; ++ib)
-      for (int j0 = ib; j0 < S.nblk; j0 += seg)
-        hitems.push_back(TileItem{s, ib, j0, std::min(j0 + seg, S.nblk)});
     blk_base += S.nblk;
   }
-  std::stable_sort(hitems.begin(), hitems.end(), [](const TileItem &p, const TileItem &q) {
-    return (p.jb1 - p.jb0) > (q.jb1 - q.jb0);
-  });
+  hitems = build_items(sinfo, b->params.tile_segment);
   b->n_items = (int)hitems.size();
   b->sys_host = sinfo;
 
@@ -835,6 +844,34 @@ extern "C" int pb2_get_status(pb2_batch *b, uint32_t *status, int clear, void *s
   CUDA_TRY(ctx, cudaMemcpyAsync(status, b->status, b->n_sys * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
   if (clear) CUDA_TRY(ctx, cudaMemsetAsync(b->status, 0, b->n_sys * sizeof(uint32_t), st));
   CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  return PB2_OK;
+}
+
+extern "C" int pb2_set_tile_segment(pb2_batch *b, int32_t segment) {
+  if (!b || segment <= 0) return PB2_EINVAL;
+  pb2_ctx *ctx = b->ctx;
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  if (segment == b->params.tile_segment) return PB2_OK;
+  std::vector<TileItem> items = build_items(b->sys_host, segment);
+  CUDA_TRY(ctx, cudaDeviceSynchronize());
+  b->dev.release(b->items);
+  b->items = b->dev.alloc<TileItem>(items.size());
+  if (!b->items) return fail(ctx, PB2_ENOMEM, "work-item allocation failed");
+  CUDA_TRY(ctx, cudaMemcpy(b->items, items.data(), items.size() * sizeof(TileItem), cudaMemcpyHostToDevice));
+  b->n_items = (int)items.size();
+  b->params.tile_segment = segment;
+  for (int p = 0; p < 3; ++p) {
+    const int cap = tile_kernel_occupancy(p, b->cut) * ctx->sm_count;
+    b->grid_pair[p] = std::max(1, std::min(cap, (b->n_items + 7) / 8));
+  }
+  for (auto &kv : b->graphs) cudaGraphExecDestroy(kv.second);  // they captured the old list
+  b->graphs.clear();
+  return PB2_OK;
+}
+
+extern "C" int pb2_get_tile_segment(const pb2_batch *b, int32_t *segment) {
+  if (!b || !segment) return PB2_EINVAL;
+  *segment = b->params.tile_segment;
   return PB2_OK;
 }
 

@@ -282,6 +282,14 @@ class Batch:
     self._check(self.lib.pb2_get_status(self.handle, s.ctypes.data, 1 if clear else 0, stream))
     return s
 
+  def set_tile_segment(self, segment: int):
+    self._check(self.lib.pb2_set_tile_segment(self.handle, int(segment)))
+
+  def tile_segment(self) -> int:
+    v = ctypes.c_int32(0)
+    self._check(self.lib.pb2_get_tile_segment(self.handle, ctypes.byref(v)))
+    return int(v.value)
+
   def set_profiling(self, enable: bool):
     self._check(self.lib.pb2_set_profiling(self.handle, 1 if enable else 0))
 

@@ -1,0 +1,45 @@
+"""Autotuner bookkeeping (bucket keys, cache) on the CPU with a stand-in batch."""
+
+import numpy as np
+
+from prolix_b200 import autotune
+
+
+class FakeBatch:
+  def __init__(self, sizes, cutoff=0.0):
+    self.sizes = np.array(sizes)
+    self.n_systems = len(sizes)
+    self.n_atoms = int(self.sizes.sum())
+    self.cutoff = cutoff
+    self.seg = 8
+    self.state = {"position": np.arange(6.0).reshape(2, 3), "momentum": np.ones((2, 3)),
+                  "key": np.array([[1, 2]], dtype=np.uint32)}
+
+  def set_tile_segment(self, s):
+    self.seg = s
+
+  def get_state(self):
+    return {k: v.copy() for k, v in self.state.items()}
+
+  def set_state(self, position=None, momentum=None, key=None):
+    self.state = {"position": position, "momentum": momentum, "key": key}
+
+
+def test_bucket_key_rounds_to_powers_of_two():
+  a = autotune.bucket_key(FakeBatch([150, 3000]), "GPU")
+  b = autotune.bucket_key(FakeBatch([200, 2800]), "GPU")
+  c = autotune.bucket_key(FakeBatch([200, 2800], cutoff=9.0), "GPU")
+  assert a == b != c
+
+
+def test_tune_picks_fastest_and_caches(tmp_path, monkeypatch):
+  monkeypatch.setenv("PROLIX_B200_TUNE_CACHE", str(tmp_path / "t.json"))
+  cost = {2: 3.0, 4: 1.5, 8: 2.0}
+  monkeypatch.setattr(autotune, "measure", lambda b, s, steps=4: cost[s])
+  monkeypatch.setattr(autotune, "_gpu_name", lambda: "FAKE")
+  fb = FakeBatch([100, 200])
+  r = autotune.tune(fb, candidates=(2, 4, 8))
+  assert r["segment"] == 4 and fb.seg == 4 and not r["cached"]
+  fb2 = FakeBatch([100, 200])
+  r2 = autotune.tune(fb2, candidates=(2, 4, 8))
+  assert r2["cached"] and fb2.seg == 4
