@@ -78,8 +78,8 @@ def dist_env():
 
 
 def workload(rank: int, n_systems: int):
-  from prolix_b200 import synth
-  return synth.make_batch(n_systems, WORKLOAD_SEED + 7919 * rank, 150, 4000, compact=True)
+  from prolix_b200 import replicas, synth
+  return synth.make_batch(n_systems, replicas.rank_seed(WORKLOAD_SEED, rank), 150, 4000, compact=True)
 
 
 def unique_pairs(systems) -> int:
@@ -237,14 +237,10 @@ def main():
   if args.impl == "reference":
     return run_reference(args)
   import torch
-  ws, rank, local = dist_env()
+  from prolix_b200 import replicas
+  ws, rank, local = replicas.env()
   torch.cuda.set_device(local)
-  pg = None
-  if ws > 1:
-    import datetime
-    import torch.distributed as dist
-    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    pg = dist
+  pg = replicas.init("nccl", timeout_s=120.0)
 
   from prolix_b200 import engine
   systems = workload(rank, args.systems)
@@ -266,8 +262,7 @@ def main():
   clk_path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv")
   os.makedirs(os.path.dirname(clk_path), exist_ok=True)
   clk = clocks_start(clk_path)
-  if pg:
-    pg.barrier()
+  replicas.barrier()
   torch.cuda.synchronize()
   for k in range(args.steps):
     flush.zero_()  # evict L2 (256 MB > 126 MB) between timed steps
@@ -275,14 +270,9 @@ def main():
     batch.langevin_run(1, stream)
     ev1[k].record()
   torch.cuda.synchronize()
-  if pg:
-    pg.barrier()
+  replicas.barrier()
   clocks = clocks_summary(clk, clk_path, local)
-  t_ms = float(sum(a.elapsed_time(b) for a, b in zip(ev0, ev1)))
-  if pg:
-    t = torch.tensor([t_ms], device="cuda")
-    pg.all_reduce(t, op=pg.ReduceOp.MAX)
-    t_ms = float(t.item())
+  t_ms = replicas.reduce_max(float(sum(a.elapsed_time(b) for a, b in zip(ev0, ev1))), device="cuda")
   status = batch.status()
   if np.any(status):
     print(f"rank {rank}: status flags {np.unique(status)}", file=sys.stderr)

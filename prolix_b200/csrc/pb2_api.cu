@@ -235,6 +235,7 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
     S.pref = (float)pref;
     S.pref_d = pref;
     S.kcoul = (float)d.k_coulomb;
+    S.kcoul_d = d.k_coulomb;
     S.lj14 = (float)d.lj14_scale;
     S.coul14 = (float)d.coul14_scale;
     S.cutoff2 = cutoff_mode ? (float)(params->cutoff * params->cutoff) : 0.f;
@@ -629,7 +630,7 @@ extern "C" int pb2_energy_forces(pb2_batch *b, double *energies, double *forces,
     for (int s = 0; s < b->n_sys; ++s) {
       double tot = 0.0;
       for (int t = 0; t < PB2_TERM_TOTAL; ++t) {
-        const double v = (double)he[(size_t)s * PB2_NTERMS + t] * kForceInv;
+        const double v = (double)he[(size_t)s * PB2_NTERMS + t] * kEnergyInv;
         energies[(size_t)s * PB2_NTERMS + t] = v;
         tot += v;
       }

@@ -38,7 +38,7 @@ __device__ __forceinline__ void add_force(const BondedArgs &a, int i, D3 f) {
 __device__ __forceinline__ void add_energy(const BondedArgs &a, int atom, int term, double e) {
   if (!a.energy_mode) return;
   const int s = a.atom_sys[atom];
-  atomic_add_fix(&a.energy[(size_t)s * PB2_NTERMS + term], to_fix(e, kForceScale));
+  atomic_add_fix(&a.energy[(size_t)s * PB2_NTERMS + term], to_fix(e, kEnergyScale));
 }
 
 // Dihedral angle and its gradient w.r.t. the four atoms.

@@ -12,12 +12,15 @@ namespace pb2 {
 constexpr int kWarp = 32;
 constexpr unsigned kFull = 0xffffffffu;
 
-// Fixed-point scales.  Forces, dE/dB and energies use 2^32 (range +-2.1e9,
-// resolution 2.3e-10); the descreening sums use 2^40 (range +-8.4e6).
+// Fixed-point scales.  Forces and dE/dB use 2^32 (range +-2.1e9, resolution
+// 2.3e-10); the descreening sums use 2^40 (range +-8.4e6).
 constexpr double kForceScale = 4294967296.0;
 constexpr double kForceInv = 1.0 / 4294967296.0;
 constexpr double kBornScale = 1099511627776.0;
 constexpr double kBornInv = 1.0 / 1099511627776.0;
+// Energies: 2^24 (range +-5.5e11 kcal/mol, resolution 6e-8 kcal/mol).
+constexpr double kEnergyScale = 16777216.0;
+constexpr double kEnergyInv = 1.0 / 16777216.0;
 constexpr double kFixMax = 9.0e18;  // below 2^63: values beyond are flagged
 
 // OBC II constants (prolix physics/generalized_born.py:18-21) and ACE
@@ -43,7 +46,7 @@ struct SysInfo {
   float far2;         // tiles at least this far apart (squared) take the far-field series
   float gb_cutoff2;   // GB / descreening cutoff^2; 0: all pairs
   int32_t clamp;      // neighbour-list clamps on Born radii (GB cutoff set)
-  int32_t pad0, pad1;
+  double kcoul_d;     // direct Coulomb constant in double (energy path)
   double pref_d;      // P in double (self / energy terms)
   double dt, half_dt; // tau
   double c1, c2;      // exp(-gamma dt), sqrt(1 - c1^2)

@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(256) energy64_kernel(const Energy64Args a) {
     const SysInfo &S = a.sys[item.sys];
     const int n = S.n, off = S.off;
     const double cut2 = (double)S.cutoff2, gcut2 = (double)S.gb_cutoff2;
-    const double pref = S.pref_d, kcoul = (double)S.kcoul;
+    const double pref = S.pref_d, kcoul = S.kcoul_d;
     const int il = item.iblk * 32 + lane;
     const bool ivalid = il < n;
     const int ig = off + (ivalid ? il : n - 1);
@@ -132,9 +132,9 @@ __global__ void __launch_bounds__(256) energy64_kernel(const Energy64Args a) {
       e_lj = warp_sum_d(e_lj);
       if (lane == 0) {
         long long *e = a.energy + (size_t)item.sys * PB2_NTERMS;
-        atomic_add_fix(&e[PB2_TERM_GB], to_fix(e_gb, kForceScale));
-        atomic_add_fix(&e[PB2_TERM_COULOMB], to_fix(e_coul, kForceScale));
-        atomic_add_fix(&e[PB2_TERM_LJ], to_fix(e_lj, kForceScale));
+        atomic_add_fix(&e[PB2_TERM_GB], to_fix(e_gb, kEnergyScale));
+        atomic_add_fix(&e[PB2_TERM_COULOMB], to_fix(e_coul, kEnergyScale));
+        atomic_add_fix(&e[PB2_TERM_LJ], to_fix(e_lj, kEnergyScale));
       }
     }
   }

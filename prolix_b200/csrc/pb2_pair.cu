@@ -410,8 +410,8 @@ __global__ void born_finalize(const FinalizeArgs a) {
     a.dedb_acc[i] = to_fix(dedb, kForceScale);
     if (a.energy_mode) {
       long long *e = a.energy + (size_t)s * PB2_NTERMS;
-      atomic_add_fix(&e[PB2_TERM_GB], to_fix(S.pref_d * q * q * inv_b, kForceScale));
-      atomic_add_fix(&e[PB2_TERM_NONPOLAR], to_fix(ace, kForceScale));
+      atomic_add_fix(&e[PB2_TERM_GB], to_fix(S.pref_d * q * q * inv_b, kEnergyScale));
+      atomic_add_fix(&e[PB2_TERM_NONPOLAR], to_fix(ace, kEnergyScale));
     }
   }
 }

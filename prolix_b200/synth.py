@@ -8,8 +8,11 @@ order, so a seed names one system exactly:
   stay at least 2.5 A apart where the packing allows.  ``compact=True`` keeps
   the chain inside a sphere of radius (3N / (4 pi 0.075))^(1/3) A where it
   can (20 A at N=2,500; 40 A at N=20,000), giving a compact globule;
-* charges U(-0.8, 0.8) e shifted to net zero; LJ sigma U(1.0, 3.4) A and
-  epsilon U(0.01, 0.2) kcal/mol; GB intrinsic radii U(1.2, 1.9) A and OBC
+* charges U(-0.5, 0.5) e shifted to net zero; LJ sigma U(2.4, 3.4) A and
+  epsilon U(0.03, 0.2) kcal/mol (any two atoms of a random chain can meet,
+  so every atom keeps a real LJ core: a bare sigma-1 A site with a charge
+  of 0.8 e would collapse onto an opposite charge into a 0.5 A well that no
+  time step resolves); GB intrinsic radii U(1.2, 1.9) A and OBC
   scale factors U(0.72, 0.85), with ``scaled_radii = radii * scale``
   (the convention of prolix tests/physics/test_openmm_parity.py:113);
 * masses drawn from {1.008, 12.011, 14.007, 15.999} amu;
@@ -76,10 +79,10 @@ def make_chain(n_atoms: int, seed: int, *, compact: bool = False, cmap: bool = F
   pos, _, _ = _grow(lengths, angles, cand, compact, globule_radius(n), retry_seed)
   pos = pos - pos.mean(axis=0, keepdims=True)
 
-  q = rng.uniform(-0.8, 0.8, size=n)
+  q = rng.uniform(-0.5, 0.5, size=n)
   q = q - q.mean()
-  sigma = rng.uniform(1.0, 3.4, size=n)
-  eps = rng.uniform(0.01, 0.2, size=n)
+  sigma = rng.uniform(2.4, 3.4, size=n)
+  eps = rng.uniform(0.03, 0.2, size=n)
   radii = rng.uniform(1.2, 1.9, size=n)
   scale = rng.uniform(0.72, 0.85, size=n)
   masses = MASS_CHOICES[rng.integers(0, 4, size=n)]

@@ -107,6 +107,11 @@ class EnergyFn:
     e, f = self._eval(r)
     return float(e[-1]), f.copy()
 
+  def close(self):
+    """Release the device batch now rather than at garbage collection."""
+    self._batch.close()
+    self._last = None
+
   def born_radii(self, r):
     r = np.asarray(r, dtype=np.float64).reshape(self.n_atoms, 3)
     self._batch.set_positions(r)
