@@ -37,12 +37,43 @@ UNIT = "atom-steps/s"
 WORKLOAD_SEED = 2024
 N_SYSTEMS = 512
 
-# Algorithmic work per unique pair (i < j) of the far-field path, counted
-# from the kernel source with FMA = 2 flops (pb2_pair.cu run_tile):
-#   descreening: 3 (d) + 5 (r^2) + 2 x 23 (series value) + 2 (sums)      = 56
-#   force:       GB 31 + Coulomb 5 + LJ 12 + 6 (d, r^2 share) + 12 (F)   = 66
-#   chain:       8 (d, r^2) + 1 + 2 x 23 (series derivative) + 4 + 12    = 71
-FLOPS_PER_PAIR = {"born": 56, "force": 66, "chain": 71}
+# Algorithmic work per unique pair (i < j), counted from the kernel source
+# with FMA = 2 flops (pb2_pair.cu run_tile).  The descreening and chain
+# passes evaluate the far-field series with K terms (K + 1 for its
+# derivative), K chosen per tile from the bounding-box separation
+# (4, 6, 8 or 10); series_terms() gives the pair-weighted mean K.
+#   descreening: 3 (d) + 5 (r^2) + 2 x (2K + 3) (series value) + 2 (sums) = 4K + 16
+#   force:       GB 31 + Coulomb 5 + LJ 12 + 6 (d, r^2 share) + 12 (F)    = 66
+#   chain:       3 (d) + 5 (r^2) + 1 + 2 x (2(K+1) + 3) + 4 + 12 (F)      = 4K + 35
+def flops_per_pair(k_mean: float) -> dict:
+  return {"born": 4.0 * k_mean + 16.0, "force": 66.0, "chain": 4.0 * k_mean + 35.0}
+
+
+def series_terms(systems) -> float:
+  """Pair-weighted mean number of series terms per tile, by the same
+  bounding-box classification the kernels use (float32 radii)."""
+  tot_k = tot_w = 0.0
+  for sd in systems:
+    x = np.asarray(sd["positions"], dtype=np.float64)
+    n = len(x)
+    sr = np.asarray(sd["scaled_radii"], dtype=np.float32).astype(np.float64)
+    ro = (np.asarray(sd["radii"], dtype=np.float64) - 0.09).astype(np.float32).astype(np.float64)
+    smax, romax = sr.max(), ro.max()
+    b2 = lambda u: (1.001 * max(smax / math.sqrt(u), smax + romax)) ** 2
+    nb = (n + 31) // 32
+    m = np.minimum(32, n - 32 * np.arange(nb))
+    lo = np.array([x[32 * b:32 * b + 32].min(0) for b in range(nb)])
+    hi = np.array([x[32 * b:32 * b + 32].max(0) for b in range(nb)])
+    ib, jb = np.triu_indices(nb)
+    d = np.maximum(0.0, np.maximum(lo[ib] - hi[jb], lo[jb] - hi[ib]))
+    d2 = (d * d).sum(1)
+    k = np.select([d2 >= b2(0.0109), d2 >= b2(0.049), d2 >= b2(0.104)], [4.0, 6.0, 8.0], 10.0)
+    w = np.where(ib == jb, m[ib] * (m[ib] - 1) / 2.0, m[ib] * m[jb].astype(np.float64))
+    tot_k += float((k * w).sum())
+    tot_w += float(w.sum())
+  return tot_k / tot_w
+
+
 MUFU_PER_PAIR = {"born": 1, "force": 3, "chain": 1}
 # integrator: read x, p (48 B), F (24 B), mass, sigma, charge (24 B); write
 # x, p (48 B), posq (16 B), clear F (24 B)
@@ -56,7 +87,7 @@ FORCE_TRAFFIC_BYTES = None
 def parse():
   ap = argparse.ArgumentParser()
   ap.add_argument("--gpus", type=int, default=1)
-  ap.add_argument("--steps", type=int, default=40)
+  ap.add_argument("--steps", type=int, default=400)
   ap.add_argument("--warmup", type=int, default=3)
   ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
   ap.add_argument("--systems", type=int, default=N_SYSTEMS)
@@ -67,6 +98,8 @@ def parse():
   ap.add_argument("--serving-requests", type=int, default=32)
   ap.add_argument("--serving-rate", type=float, default=20.0)
   ap.add_argument("--serving-step-scale", type=float, default=0.05)
+  ap.add_argument("--segment", type=int, default=0,
+                  help="tile work-item segment; 0 runs the autotuner")
   return ap.parse_args()
 
 
@@ -251,7 +284,11 @@ def main():
   stream = torch.cuda.current_stream().cuda_stream
 
   from prolix_b200 import autotune
-  tuned = autotune.tune(batch, candidates=(2, 4, 8, 16, 32), steps=3, use_cache=False)
+  if args.segment > 0:
+    batch.set_tile_segment(args.segment)
+    tuned = {"segment": args.segment, "timings": None}
+  else:
+    tuned = autotune.tune(batch, candidates=(2, 4, 8, 16, 32), steps=3, use_cache=False)
   for _ in range(args.warmup):  # also captures the one-step graph
     batch.langevin_run(1, stream)
   torch.cuda.synchronize()
@@ -289,9 +326,11 @@ def main():
 
   peak = ctypes_fp32_peak(batch)
   passes = {}
+  k_mean = series_terms(systems)
+  fpp = flops_per_pair(k_mean)
   for p in ("born", "force", "chain"):
     ms = per_kernel[p]
-    tf = FLOPS_PER_PAIR[p] * pairs / (ms * 1e-3) / 1e12 if ms > 0 else None
+    tf = fpp[p] * pairs / (ms * 1e-3) / 1e12 if ms > 0 else None
     passes[p] = {"ms": ms, "tflops": tf, "frac": (tf / peak if tf and peak else None),
                  "mufu_tops": MUFU_PER_PAIR[p] * pairs / (ms * 1e-3) / 1e12 if ms > 0 else None}
   dom = max(("born", "force", "chain"), key=lambda p: per_kernel[p])
@@ -300,7 +339,8 @@ def main():
               "frac": passes[dom]["frac"],
               "traffic": FORCE_TRAFFIC_BYTES if dom == "force" else None,
               "peak_source": "FP32 FMA throughput measured in this run (pb2_fp32_peak)",
-              "algorithmic_flops_per_launch": FLOPS_PER_PAIR[dom] * pairs,
+              "algorithmic_flops_per_launch": fpp[dom] * pairs,
+              "flops_per_pair": fpp, "series_terms_mean": k_mean,
               "passes": passes}
   integ_gbs = BYTES_PER_ATOM_STEP * n_atoms / (per_kernel["integrator"] * 1e-3) / 1e9
   hbm_peak = _measured_hbm()
@@ -310,22 +350,27 @@ def main():
 
   e2e = None
   if not args.no_e2e:
-    st = batch.get_state()
-    x_h, p_h = st["position"].copy(), st["momentum"].copy()
-    e2e_steps = 5
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-      batch.set_state(position=x_h, momentum=p_h)
+    # every step: positions, momenta and forces in from page-locked host
+    # buffers (pb2_set_full_state), one BAOAB step, and the same three arrays
+    # back out (pb2_get_state); timed on the host clock around the calls
+    fields = ("position", "momentum", "force")
+    host = {f: torch.empty((n_atoms, 3), dtype=torch.float64, pin_memory=True).numpy() for f in fields}
+    batch.get_state(fields=fields, out=host)
+    e2e_steps = 10
+    for it in range(2 + e2e_steps):
+      if it == 2:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+      batch.set_full_state(host["position"], host["momentum"], host["force"], stream=stream)
       batch.langevin_run(1, stream)
-      out = batch.get_state()
-      x_h, p_h = out["position"], out["momentum"]
+      batch.get_state(stream=stream, fields=fields, out=host)
     torch.cuda.synchronize()
     t_e2e = time.perf_counter() - t0
+    nbytes = 3 * 3 * 8 * n_atoms
     e2e = {"value": n_atoms * ws * e2e_steps / t_e2e, "unit": UNIT,
-           "h2d_bytes_per_step": int(2 * 3 * 8 * n_atoms),
-           "d2h_bytes_per_step": int((3 * 3 * 8) * n_atoms + 8 * 2 * len(systems)),
-           "steps": e2e_steps, "path": "pb2_set_state + pb2_langevin_run(1) + pb2_get_state"}
+           "h2d_bytes_per_step": int(nbytes), "d2h_bytes_per_step": int(nbytes),
+           "steps": e2e_steps, "host_buffers": "page-locked",
+           "path": "pb2_set_full_state + pb2_langevin_run(1) + pb2_get_state (x, p, F)"}
   batch.close()
 
   plain = None

@@ -189,6 +189,14 @@ int pb2_get_state(pb2_batch *batch, double *x, double *p, double *f, uint32_t *k
 int pb2_set_state(pb2_batch *batch, const double *x, const double *p, const uint32_t *keys,
                   void *stream);
 
+/* Restore the whole BAOAB state (the fields of prolix's NVTLangevinState,
+ * typing.py:611-618: positions, momentum, force, rng) without evaluating
+ * forces: f must be the forces at x, as pb2_get_state returned them (the
+ * round trip is exact).  x, p, f required; keys may be NULL.  Transfers run
+ * at full PCIe speed when the host buffers are page-locked. */
+int pb2_set_full_state(pb2_batch *batch, const double *x, const double *p, const double *f,
+                       const uint32_t *keys, void *stream);
+
 /* Per-system status bits (PB2_STATUS_*) accumulated since the last clear. */
 int pb2_get_status(pb2_batch *batch, uint32_t *status, int clear, void *stream);
 

@@ -281,14 +281,21 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
       hsr[g] = d.scaled_radii[i];
       hpar[g] = make_float4((float)hhs[g], (float)hse[g], (float)ro, (float)hsr[g]);
     }
-    {  // far-field tiles: every pair has r - s >= rho~ and (s/r)^2 <= 0.09
+    {  // far-field tiles: every pair has r - s >= rho~ and (s/r)^2 <= u_K
       float smax = 0.f, romax = 0.f;
       for (int i = 0; i < n; ++i) {
         smax = std::max(smax, hpar[o + i].w);
         romax = std::max(romax, hpar[o + i].z);
       }
-      const double rfar = 1.001 * std::max((double)smax / 0.3, (double)smax + (double)romax);
-      S.far2 = (float)(rfar * rfar);
+      auto bound2 = [&](double u) {
+        const double r = 1.001 * std::max((double)smax / std::sqrt(u), (double)smax + (double)romax);
+        return (float)(r * r);
+      };
+      S.far2 = bound2(0.16);
+      S.far2_k8 = bound2(0.104);
+      S.far2_k6 = bound2(0.049);
+      S.far2_k4 = bound2(0.0109);
+      S.pad0 = 0;
     }
     for (int bk = 0; bk < S.nblk; ++bk) hblk_sys[blk_base + bk] = s;
     hkeys[2 * (size_t)s] = d.key[0];
@@ -392,6 +399,7 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   b->ro64 = D.alloc<double>(N);
   b->sr64 = D.alloc<double>(N);
   b->born64 = D.alloc<double>(N);
+  b->stage = D.alloc<double>(3 * (size_t)N);
   b->born_acc = D.alloc<long long>(N);
   b->dedb_acc = D.alloc<long long>(N);
   b->energy = D.alloc<long long>((size_t)n_systems * PB2_NTERMS);
@@ -606,13 +614,9 @@ static int fresh_forces(pb2_batch *b, cudaStream_t st, bool energy) {
 static int copy_forces(pb2_batch *b, double *forces, cudaStream_t st) {
   pb2_ctx *ctx = b->ctx;
   const int N = b->n_total;
-  std::vector<long long> hf(3 * (size_t)N);
-  CUDA_TRY(ctx, cudaMemcpyAsync(hf.data(), b->fx, N * sizeof(long long), cudaMemcpyDeviceToHost, st));
-  CUDA_TRY(ctx, cudaMemcpyAsync(hf.data() + N, b->fy, N * sizeof(long long), cudaMemcpyDeviceToHost, st));
-  CUDA_TRY(ctx, cudaMemcpyAsync(hf.data() + 2 * (size_t)N, b->fz, N * sizeof(long long), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(ctx, launch_fix_to_rows(b->fx, b->fy, b->fz, b->stage, N, st));
+  CUDA_TRY(ctx, cudaMemcpyAsync(forces, b->stage, 3 * (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, st));
   CUDA_TRY(ctx, cudaStreamSynchronize(st));
-  for (int i = 0; i < N; ++i)
-    for (int c = 0; c < 3; ++c) forces[3 * (size_t)i + c] = (double)hf[(size_t)c * N + i] * kForceInv;
   return PB2_OK;
 }
 
@@ -656,16 +660,15 @@ extern "C" int pb2_born_radii(pb2_batch *b, double *out, void *stream) {
   return PB2_OK;
 }
 
+// Row-major (n, 3) host arrays move through the device staging buffer in one
+// copy each; the (de)interleave runs on the device.  The staging buffer is
+// reused by the next transfer on the same stream, so each helper finishes
+// its copy before returning.
 static int upload_soa3(pb2_batch *b, const double *aos, double *dx, double *dy, double *dz, cudaStream_t st) {
   pb2_ctx *ctx = b->ctx;
   const int N = b->n_total;
-  std::vector<double> h(3 * (size_t)N);
-  for (int i = 0; i < N; ++i)
-    for (int c = 0; c < 3; ++c) h[(size_t)c * N + i] = aos[3 * (size_t)i + c];
-  CUDA_TRY(ctx, cudaMemcpyAsync(dx, h.data(), N * sizeof(double), cudaMemcpyHostToDevice, st));
-  CUDA_TRY(ctx, cudaMemcpyAsync(dy, h.data() + N, N * sizeof(double), cudaMemcpyHostToDevice, st));
-  CUDA_TRY(ctx, cudaMemcpyAsync(dz, h.data() + 2 * (size_t)N, N * sizeof(double), cudaMemcpyHostToDevice, st));
-  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  CUDA_TRY(ctx, cudaMemcpyAsync(b->stage, aos, 3 * (size_t)N * sizeof(double), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(ctx, launch_rows_to_soa(b->stage, dx, dy, dz, N, st));
   return PB2_OK;
 }
 
@@ -673,20 +676,19 @@ static int download_soa3(pb2_batch *b, double *aos, const double *dx, const doub
                          cudaStream_t st) {
   pb2_ctx *ctx = b->ctx;
   const int N = b->n_total;
-  std::vector<double> h(3 * (size_t)N);
-  CUDA_TRY(ctx, cudaMemcpyAsync(h.data(), dx, N * sizeof(double), cudaMemcpyDeviceToHost, st));
-  CUDA_TRY(ctx, cudaMemcpyAsync(h.data() + N, dy, N * sizeof(double), cudaMemcpyDeviceToHost, st));
-  CUDA_TRY(ctx, cudaMemcpyAsync(h.data() + 2 * (size_t)N, dz, N * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(ctx, launch_soa_to_rows(dx, dy, dz, b->stage, N, st));
+  CUDA_TRY(ctx, cudaMemcpyAsync(aos, b->stage, 3 * (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, st));
   CUDA_TRY(ctx, cudaStreamSynchronize(st));
-  for (int i = 0; i < N; ++i)
-    for (int c = 0; c < 3; ++c) aos[3 * (size_t)i + c] = h[(size_t)c * N + i];
   return PB2_OK;
 }
 
 extern "C" int pb2_set_positions(pb2_batch *b, const double *positions, void *stream) {
   if (!b || !positions) return PB2_EINVAL;
   b->forces_valid = false;
-  return upload_soa3(b, positions, b->x, b->y, b->z, (cudaStream_t)stream);
+  const int rc = upload_soa3(b, positions, b->x, b->y, b->z, (cudaStream_t)stream);
+  if (rc) return rc;
+  CUDA_TRY(b->ctx, cudaStreamSynchronize((cudaStream_t)stream));
+  return PB2_OK;
 }
 
 // ------------------------------------------------------------ Langevin
@@ -833,8 +835,29 @@ extern "C" int pb2_set_state(pb2_batch *b, const double *x, const double *p, con
   if (x) {  // forces must follow the positions
     rc = fresh_forces(b, st, false);
     if (rc) return rc;
-    CUDA_TRY(ctx, cudaStreamSynchronize(st));
   }
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  return PB2_OK;
+}
+
+extern "C" int pb2_set_full_state(pb2_batch *b, const double *x, const double *p, const double *f,
+                                  const uint32_t *keys, void *stream) {
+  if (!b || !x || !p || !f) return PB2_EINVAL;
+  pb2_ctx *ctx = b->ctx;
+  cudaStream_t st = (cudaStream_t)stream;
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  int rc;
+  if ((rc = upload_soa3(b, x, b->x, b->y, b->z, st))) return rc;
+  if ((rc = upload_soa3(b, p, b->px, b->py, b->pz, st))) return rc;
+  CUDA_TRY(ctx, cudaMemcpyAsync(b->stage, f, 3 * (size_t)b->n_total * sizeof(double), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(ctx, launch_rows_to_fix(b->stage, b->fx, b->fy, b->fz, b->n_total, st));
+  if (keys) {
+    CUDA_TRY(ctx, cudaMemcpyAsync(b->keys + (size_t)b->key_parity * b->n_sys * 2, keys,
+                                  (size_t)b->n_sys * 2 * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+  }
+  CUDA_TRY(ctx, launch_posq(int_args(b, b->key_parity, 0), st));
+  b->forces_valid = true;
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
   return PB2_OK;
 }
 

@@ -64,6 +64,7 @@ struct pb2_batch {
   int n_blocks = 0;
   double *q64 = nullptr, *hs64 = nullptr, *se64 = nullptr, *ro64 = nullptr, *sr64 = nullptr;
   double *born64 = nullptr;
+  double *stage = nullptr;  // (n_total, 3) row-major staging for host transfers
   long long *born_acc = nullptr, *dedb_acc = nullptr, *energy = nullptr;
   uint32_t *keys = nullptr, *status = nullptr;
   long long *steps = nullptr;

@@ -128,5 +128,12 @@ cudaError_t launch_step(const IntArgs &a, cudaStream_t st);
 cudaError_t launch_finish(const IntArgs &a, cudaStream_t st);
 cudaError_t launch_init(const IntArgs &a, cudaStream_t st);
 cudaError_t launch_posq(const IntArgs &a, cudaStream_t st);
+cudaError_t launch_rows_to_soa(const double *rows, double *x, double *y, double *z, int n, cudaStream_t st);
+cudaError_t launch_soa_to_rows(const double *x, const double *y, const double *z, double *rows, int n,
+                               cudaStream_t st);
+cudaError_t launch_fix_to_rows(const long long *fx, const long long *fy, const long long *fz, double *rows,
+                               int n, cudaStream_t st);
+cudaError_t launch_rows_to_fix(const double *rows, long long *fx, long long *fy, long long *fz, int n,
+                               cudaStream_t st);
 
 }  // namespace pb2

@@ -58,27 +58,29 @@ __device__ __forceinline__ float box_dist2(const float4 *bbox, int a, int b) {
   return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
 }
 
-// Far-field OBC integral and derivative (valid when r - s >= rho~ and
-// (s/r)^2 <= kSeriesU; the caller guarantees it for the whole tile).
+// Far-field OBC integral and derivative with K series terms (valid when
+// r - s >= rho~ and (s/r)^2 is inside K's domain; the caller guarantees it).
+template <int K>
 __device__ __forceinline__ float obc_far_val(float s, float inv_r) {
   const float t = s * inv_r;
   const float u = t * t;
-  return t * u * inv_r * obc_series_val(u);
+  return t * u * inv_r * obc_series_val_n<K>(u);
 }
+template <int K>
 __device__ __forceinline__ float obc_far_der(float s, float inv_r, float inv_r2) {
   const float t = s * inv_r;
   const float u = t * t;
-  return -t * u * inv_r2 * obc_series_der(u);
+  return -t * u * inv_r2 * obc_series_der_n<K + 1>(u);
 }
 
 struct PData {  // per-atom data a lane holds (its i atom, or the j atom passing through)
   float x, y, z, q, hs, se, ro, sr, B, iB, dedi;  // iB = sqrt(log2 e / 4) / B
 };
 
-// Both directions of a pair inside the series' domain: r - s >= rho~ and
-// (s/r)^2 <= kSeriesU.
+// Both directions of a pair inside the near-tile series' domain:
+// r - s >= rho~ and (s/r)^2 <= kSeriesUNear.
 __device__ __forceinline__ bool far_pair(float r, float r2, const PData &I, const PData &J) {
-  const float lim = kSeriesU * r2;
+  const float lim = kSeriesUNear * r2;
   return (J.sr * J.sr <= lim) && (I.sr * I.sr <= lim) && (r - J.sr >= I.ro) && (r - I.sr >= J.ro);
 }
 
@@ -96,8 +98,9 @@ struct TileConst {
 };
 
 // One 32 x 32 tile.  V: rotated validity mask (bit k = pair at step k);
-// E, S14: rotated exclusion / 1-4 masks.  FAR: series OBC without checks.
-template <int PASS, bool FAR, bool CUT, bool FULL, bool EXCL>
+// E, S14: rotated exclusion / 1-4 masks.  FAR: series OBC without checks;
+// NT: series terms (value; the derivative takes NT + 1).
+template <int PASS, bool FAR, bool CUT, bool FULL, bool EXCL, int NT = 10>
 __device__ __forceinline__ void run_tile(const PData &I, PData &J, Acc &ti, Acc &tj, uint32_t V,
                                          uint32_t E, uint32_t S14, const TileConst &K) {
   const int src = K.src;
@@ -114,11 +117,11 @@ __device__ __forceinline__ void run_tile(const PData &I, PData &J, Acc &ti, Acc 
       const float inv_r2 = inv_r * inv_r;
       float vij, vji;
       if (PASS == PASS_BORN) {
-        vij = obc_far_val(J.sr, inv_r);
-        vji = obc_far_val(I.sr, inv_r);
+        vij = obc_far_val<NT>(J.sr, inv_r);
+        vji = obc_far_val<NT>(I.sr, inv_r);
       } else {
-        vij = obc_far_der(J.sr, inv_r, inv_r2);
-        vji = obc_far_der(I.sr, inv_r, inv_r2);
+        vij = obc_far_der<NT>(J.sr, inv_r, inv_r2);
+        vji = obc_far_der<NT>(I.sr, inv_r, inv_r2);
       }
       if (!FAR) {
         // near tile: the series holds for most pairs; the closed form runs
@@ -243,7 +246,7 @@ __global__ void __launch_bounds__(256, PB2_MINB) tile_kernel(const PairArgs a) {
     const int n = S.n, off = S.off;
     K.cut2 = S.cutoff2; K.gcut2 = S.gb_cutoff2;
     K.pref = S.pref; K.kcoul = S.kcoul; K.lj14 = S.lj14; K.coul14 = S.coul14;
-    const float far2 = S.far2;
+    const float far2 = S.far2, far2_k8 = S.far2_k8, far2_k6 = S.far2_k6, far2_k4 = S.far2_k4;
     const int gib = S.blk_base + item.iblk;
     const int il = item.iblk * 32 + lane;
     const bool ivalid = il < n;
@@ -291,16 +294,20 @@ __global__ void __launch_bounds__(256, PB2_MINB) tile_kernel(const PairArgs a) {
           excl = true;
         }
       }
-      const bool far = (PASS != PASS_FORCE) && d2 >= far2;
-
       Acc ti = {0.f, 0.f, 0.f, 0.f}, tj = {0.f, 0.f, 0.f, 0.f};
       if (PASS == PASS_FORCE) {
         if (excl || !full) run_tile<PASS, false, CUT, false, true>(I, J, ti, tj, V, E, S14, K);
         else run_tile<PASS, false, CUT, true, false>(I, J, ti, tj, V, E, S14, K);
-      } else if (far) {
-        run_tile<PASS, true, CUT, false, false>(I, J, ti, tj, V, E, S14, K);
+      } else if (d2 >= far2_k4) {  // series length by the tiles' smallest separation
+        run_tile<PASS, true, CUT, false, false, 4>(I, J, ti, tj, V, E, S14, K);
+      } else if (d2 >= far2_k6) {
+        run_tile<PASS, true, CUT, false, false, 6>(I, J, ti, tj, V, E, S14, K);
+      } else if (d2 >= far2_k8) {
+        run_tile<PASS, true, CUT, false, false, 8>(I, J, ti, tj, V, E, S14, K);
+      } else if (d2 >= far2) {
+        run_tile<PASS, true, CUT, false, false, 10>(I, J, ti, tj, V, E, S14, K);
       } else {
-        run_tile<PASS, false, CUT, false, false>(I, J, ti, tj, V, E, S14, K);
+        run_tile<PASS, false, CUT, false, false, 10>(I, J, ti, tj, V, E, S14, K);
       }
 
       // j partials are back in their home lanes: flush them

@@ -9,15 +9,41 @@
 // with t = s/r, to I = (1/(2r)) (t/(1 - t^2) - atanh t), whose Taylor series
 //   I = (t^3 / r) sum_{k>=1} k/(2k+1) t^(2k-2),
 //   dI/dr = -(t^3 / r^2) sum_{k>=1} 2k(k+1)/(2k+1) t^(2k-2)
-// has only positive terms.  For t^2 <= 0.09 nine terms leave a relative
-// truncation error below 1e-9, and the series avoids both the logarithm and
-// the cancellation between the O(1/r) terms of the closed form (whose sum is
+// has only positive terms, and avoids both the logarithm and the
+// cancellation between the O(1/r) terms of the closed form (whose sum is
 // O(s^3/r^4)).  Nearer pairs use the closed form with an accurate logf.
+//
+// Truncation: K terms of the value series leave a relative error at most
+// 2e-8 (a third of a float32 ulp) for u = t^2 up to
+//   K:  4       6       8       9       10
+//   u:  0.0110  0.0493  0.1046  0.1345  0.1644
+// and the derivative series needs K + 1 terms for the same u.  The pair
+// kernels pick K per tile from the smallest distance between the two
+// blocks' bounding boxes.
 #pragma once
 
 namespace pb2 {
 
-constexpr float kSeriesU = 0.09f;
+constexpr float kSeriesU = 0.09f;      // closed-form helpers' series shortcut (9 terms)
+constexpr float kSeriesUNear = 0.16f;  // per-pair test in near tiles (10 / 11 terms)
+
+// sum_{k=1..K} k/(2k+1) u^(k-1), Horner; coefficients folded at compile time.
+template <int K>
+__device__ __forceinline__ float obc_series_val_n(float u) {
+  float p = (float)((double)K / (double)(2 * K + 1));
+#pragma unroll
+  for (int k = K - 1; k >= 1; --k) p = fmaf(p, u, (float)((double)k / (double)(2 * k + 1)));
+  return p;
+}
+
+// sum_{k=1..K} 2k(k+1)/(2k+1) u^(k-1).
+template <int K>
+__device__ __forceinline__ float obc_series_der_n(float u) {
+  float p = (float)(2.0 * K * (K + 1) / (double)(2 * K + 1));
+#pragma unroll
+  for (int k = K - 1; k >= 1; --k) p = fmaf(p, u, (float)(2.0 * k * (k + 1) / (double)(2 * k + 1)));
+  return p;
+}
 
 __device__ __forceinline__ float obc_series_val(float u) {
   // sum_{k=1..9} k/(2k+1) u^(k-1)

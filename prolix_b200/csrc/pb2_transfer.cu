@@ -1,0 +1,84 @@
+// Host <-> device state transfers.
+//
+// The C ABI exchanges (n_atoms, 3) row-major FP64 arrays, the layout of
+// prolix's jax_md state (NVTLangevinState.position / momentum / force);
+// the device keeps x, y, z (and forces as 64-bit fixed point) as separate
+// arrays.  One contiguous copy moves the row-major array between the host
+// buffer and a device staging buffer; these kernels convert on the device,
+// so the host does no per-atom work and the copy runs at full PCIe speed
+// when the caller's buffer is page-locked.
+#include "pb2_common.cuh"
+#include "pb2_kernels.cuh"
+
+namespace pb2 {
+
+__global__ void rows_to_soa(const double *__restrict__ rows, double *x, double *y, double *z, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    x[i] = rows[3 * (size_t)i];
+    y[i] = rows[3 * (size_t)i + 1];
+    z[i] = rows[3 * (size_t)i + 2];
+  }
+}
+
+__global__ void soa_to_rows(const double *__restrict__ x, const double *__restrict__ y,
+                            const double *__restrict__ z, double *rows, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    rows[3 * (size_t)i] = x[i];
+    rows[3 * (size_t)i + 1] = y[i];
+    rows[3 * (size_t)i + 2] = z[i];
+  }
+}
+
+// Fixed point -> FP64 is exact for |F| < 2^21 kcal/mol/A (|v| < 2^53), so a
+// get/set round trip restores the accumulators bit for bit.
+__global__ void fix_to_rows(const long long *__restrict__ fx, const long long *__restrict__ fy,
+                            const long long *__restrict__ fz, double *rows, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    rows[3 * (size_t)i] = (double)fx[i] * kForceInv;
+    rows[3 * (size_t)i + 1] = (double)fy[i] * kForceInv;
+    rows[3 * (size_t)i + 2] = (double)fz[i] * kForceInv;
+  }
+}
+
+__global__ void rows_to_fix(const double *__restrict__ rows, long long *fx, long long *fy, long long *fz,
+                            int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    fx[i] = to_fix(rows[3 * (size_t)i], kForceScale);
+    fy[i] = to_fix(rows[3 * (size_t)i + 1], kForceScale);
+    fz[i] = to_fix(rows[3 * (size_t)i + 2], kForceScale);
+  }
+}
+
+static int grid_for(int n) {
+  const int g = (n + 255) / 256;
+  return g < 1 ? 1 : (g > 4096 ? 4096 : g);
+}
+
+cudaError_t launch_rows_to_soa(const double *rows, double *x, double *y, double *z, int n, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  rows_to_soa<<<grid_for(n), 256, 0, st>>>(rows, x, y, z, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_soa_to_rows(const double *x, const double *y, const double *z, double *rows, int n,
+                               cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  soa_to_rows<<<grid_for(n), 256, 0, st>>>(x, y, z, rows, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fix_to_rows(const long long *fx, const long long *fy, const long long *fz, double *rows,
+                               int n, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  fix_to_rows<<<grid_for(n), 256, 0, st>>>(fx, fy, fz, rows, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rows_to_fix(const double *rows, long long *fx, long long *fy, long long *fz, int n,
+                               cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  rows_to_fix<<<grid_for(n), 256, 0, st>>>(rows, fx, fy, fz, n);
+  return cudaGetLastError();
+}
+
+}  // namespace pb2

@@ -259,15 +259,38 @@ class Batch:
   def langevin_run(self, n_steps, stream=None):
     self._check(self.lib.pb2_langevin_run(self.handle, int(n_steps), stream))
 
-  def get_state(self, stream=None):
-    x = np.zeros((self.n_atoms, 3))
-    p = np.zeros((self.n_atoms, 3))
-    f = np.zeros((self.n_atoms, 3))
-    k = np.zeros((self.n_systems, 2), dtype=np.uint32)
-    st = np.zeros(self.n_systems, dtype=np.int64)
-    self._check(self.lib.pb2_get_state(self.handle, x.ctypes.data, p.ctypes.data, f.ctypes.data,
-                                       k.ctypes.data, st.ctypes.data, stream))
-    return {"position": x, "momentum": p, "force": f, "key": k, "step": st}
+  def get_state(self, stream=None, fields=("position", "momentum", "force", "key", "step"),
+                out=None):
+    """Read the BAOAB state.  ``fields`` selects what is copied; ``out`` may
+    supply destination arrays by field name (C-contiguous, float64 (n, 3) for
+    position/momentum/force), e.g. page-locked buffers for full-speed copies."""
+    out = dict(out or {})
+    shapes = {"position": ((self.n_atoms, 3), np.float64), "momentum": ((self.n_atoms, 3), np.float64),
+              "force": ((self.n_atoms, 3), np.float64), "key": ((self.n_systems, 2), np.uint32),
+              "step": ((self.n_systems,), np.int64)}
+    res = {}
+    for name in fields:
+      shape, dt = shapes[name]
+      a = out.get(name)
+      if a is None:
+        a = np.zeros(shape, dtype=dt)
+      elif a.shape != shape or a.dtype != dt or not a.flags.c_contiguous:
+        raise ValueError(f"get_state: out[{name!r}] must be a C-contiguous {dt.__name__} {shape}")
+      res[name] = a
+    ptr = lambda name: res[name].ctypes.data if name in res else None
+    self._check(self.lib.pb2_get_state(self.handle, ptr("position"), ptr("momentum"), ptr("force"),
+                                       ptr("key"), ptr("step"), stream))
+    return res
+
+  def set_full_state(self, position, momentum, force, key=None, stream=None):
+    """Restore x, p, F (and optionally the keys) without a force evaluation;
+    ``force`` must be the forces at ``position`` as get_state returned them."""
+    x = _f64(position, (self.n_atoms, 3))
+    p = _f64(momentum, (self.n_atoms, 3))
+    f = _f64(force, (self.n_atoms, 3))
+    k = None if key is None else np.ascontiguousarray(np.asarray(key, dtype=np.uint32).reshape(-1, 2))
+    self._check(self.lib.pb2_set_full_state(self.handle, x.ctypes.data, p.ctypes.data, f.ctypes.data,
+                                            None if k is None else k.ctypes.data, stream))
 
   def set_state(self, position=None, momentum=None, key=None, stream=None):
     x = None if position is None else _f64(position, (self.n_atoms, 3))

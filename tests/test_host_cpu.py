@@ -128,3 +128,20 @@ def test_build_flags_target_sm100a_only():
   flags = " ".join(_build.NVCC_FLAGS)
   assert "arch=compute_100a,code=sm_100a" in flags
   assert "sm_90" not in flags
+
+
+def test_far_field_series_lengths_meet_float32_bound():
+  # The pair kernels evaluate the OBC far-field series with K terms (value)
+  # and K + 1 terms (derivative) on tiles whose smallest box separation keeps
+  # u = (s/r)^2 below u_K (pb2_api.cu far2_k*, pb2_pair.cu run_tile).  The
+  # relative truncation error must stay below 2e-8 there.
+  def val(u, k):
+    return sum(j / (2 * j + 1) * u ** (j - 1) for j in range(1, k + 1))
+
+  def der(u, k):
+    return sum(2 * j * (j + 1) / (2 * j + 1) * u ** (j - 1) for j in range(1, k + 1))
+
+  for k, u in ((4, 0.0109), (6, 0.049), (8, 0.104), (10, 0.16)):
+    ev = (val(u, 400) - val(u, k)) / val(u, 400)
+    ed = (der(u, 400) - der(u, k + 1)) / der(u, 400)
+    assert 0 <= ev < 2e-8 and 0 <= ed < 2e-8, (k, u, ev, ed)
