@@ -60,8 +60,8 @@ extern "C" const char *pb2_last_error(const pb2_ctx *ctx) {
 static PairArgs pair_args(pb2_batch *b) {
   PairArgs a;
   a.sys = b->sys;
-  a.items = b->items;
-  a.n_items = b->n_items;
+  a.items = b->items2;
+  a.n_items = b->n_items2;
   a.terms = b->params.terms;
   a.excl_ent = b->excl_ent;
   a.excl_rows = b->excl_rows;
@@ -120,6 +120,39 @@ static std::vector<TileItem> build_items(const std::vector<SysInfo> &sinfo, int 
     return (p.jb1 - p.jb0) > (q.jb1 - q.jb0);
   });
   return items;
+}
+
+// Work items of the two-i-block force kernel: even i-blocks ib (with ib + 1)
+// against j-blocks [j0, j1), j0 >= ib.
+static std::vector<TileItem> build_items2(const std::vector<SysInfo> &sinfo, int seg) {
+  std::vector<TileItem> items;
+  for (int s = 0; s < (int)sinfo.size(); ++s) {
+    const int nblk = sinfo[s].nblk;
+    for (int ib = 0; ib < nblk; ib += 2)
+      for (int j0 = ib; j0 < nblk; j0 += seg) items.push_back(TileItem{s, ib, j0, std::min(j0 + seg, nblk)});
+  }
+  std::stable_sort(items.begin(), items.end(), [](const TileItem &p, const TileItem &q) {
+    return (p.jb1 - p.jb0) > (q.jb1 - q.jb0);
+  });
+  return items;
+}
+
+// (Re)build the pair kernels' two-i-block work list and their grids (one
+// resident wave each; warps take items dynamically).
+static int setup_items2(pb2_batch *b, int seg) {
+  pb2_ctx *ctx = b->ctx;
+  std::vector<TileItem> items = build_items2(b->sys_host, seg);
+  b->dev.release(b->items2);
+  b->items2 = b->dev.alloc<TileItem>(std::max<size_t>(items.size(), 1));
+  if (!b->items2) return fail(ctx, PB2_ENOMEM, "work-item allocation failed");
+  if (!items.empty())
+    CUDA_TRY(ctx, cudaMemcpy(b->items2, items.data(), items.size() * sizeof(TileItem), cudaMemcpyHostToDevice));
+  b->n_items2 = (int)items.size();
+  for (int p = 0; p < 3; ++p) {
+    const int cap = tile_kernel_occupancy(p, b->cut) * ctx->sm_count;
+    b->grid_pair[p] = std::max(1, std::min(cap, (b->n_items2 + 7) / 8));
+  }
+  return PB2_OK;
 }
 
 static int validate(pb2_ctx *ctx, const pb2_system_desc &d, int s) {
@@ -470,13 +503,8 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   if (!(params->terms & PB2_USE_BONDED)) B.n_bond = B.n_angle = B.n_tors = 0;
   if (!(params->terms & PB2_USE_CMAP)) B.n_cmap = 0;
 
-  // launch shapes: persistent grids sized to the resident capacity
-  for (int p = 0; p < 3; ++p) {
-    // one resident wave; warps take items dynamically
-    const int cap = tile_kernel_occupancy(p, b->cut) * ctx->sm_count;
-    b->grid_pair[p] = std::max(1, std::min(cap, (b->n_items + 7) / 8));
-  }
   b->grid_bonded = 8 * ctx->sm_count;
+  if ((rc = setup_items2(b.get(), b->params.tile_segment))) return rc;
   CUDA_TRY(ctx, cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking));
   CUDA_TRY(ctx, cudaEventCreate(&b->ev[0]));
   CUDA_TRY(ctx, cudaEventCreate(&b->ev[1]));
@@ -884,10 +912,7 @@ extern "C" int pb2_set_tile_segment(pb2_batch *b, int32_t segment) {
   CUDA_TRY(ctx, cudaMemcpy(b->items, items.data(), items.size() * sizeof(TileItem), cudaMemcpyHostToDevice));
   b->n_items = (int)items.size();
   b->params.tile_segment = segment;
-  for (int p = 0; p < 3; ++p) {
-    const int cap = tile_kernel_occupancy(p, b->cut) * ctx->sm_count;
-    b->grid_pair[p] = std::max(1, std::min(cap, (b->n_items + 7) / 8));
-  }
+  if (int rc = setup_items2(b, segment)) return rc;
   for (auto &kv : b->graphs) cudaGraphExecDestroy(kv.second);  // they captured the old list
   b->graphs.clear();
   return PB2_OK;

@@ -68,8 +68,10 @@ struct pb2_batch {
   long long *born_acc = nullptr, *dedb_acc = nullptr, *energy = nullptr;
   uint32_t *keys = nullptr, *status = nullptr;
   long long *steps = nullptr;
-  TileItem *items = nullptr;
+  TileItem *items = nullptr;   // (i-block, j-range) items of the FP64 energy kernels
   int n_items = 0;
+  TileItem *items2 = nullptr;  // pair kernels: items over pairs of i-blocks
+  int n_items2 = 0;
   int2 *excl_ent = nullptr;
   ExclRow *excl_rows = nullptr;
   BondedArgs bonded{};

@@ -12,19 +12,22 @@
 // A per-atom pass between born and force turns the sums into Born radii and
 // adds the self (q^2/B) and ACE terms.
 //
-// Mapping: one warp per work item (system, i-block, range of j-blocks);
-// lane l owns atom i = 32*iblk + l for the whole item; the j-block's data and
-// j-side accumulators rotate through the lanes by shuffles, so lane l meets
-// j-lane (l + k) mod 32 at step k of a fully unrolled 32-step loop.  Per
-// tile, each lane's pair-validity and exclusion bit masks are rotated by its
-// lane index once, so step k tests bit k.  A per-block bounding box sorts
-// tiles: tiles whose boxes are at least the far-field distance apart
-// evaluate the OBC integral by its series without per-pair branches, and
+// Mapping: one warp per work item (system, two consecutive i-blocks, range
+// of j-blocks); lane l owns atom l of each i-block for the whole item; the
+// j-block's data and j-side accumulators rotate through the lanes by
+// shuffles, so lane l meets j-lane (l + k) mod 32 at step k of the 32-step
+// loop, once for each of its two i atoms.  Per tile, each lane's
+// pair-validity and exclusion bit masks are rotated by its lane index once,
+// so step k tests bit k.  A per-block bounding box sorts tiles: tiles whose
+// boxes are at least the far-field distance apart evaluate the OBC integral
+// by its series (4 to 10 terms by separation) without per-pair branches, and
 // (with a cutoff) tiles beyond every cutoff are skipped.
 //
 // Arithmetic is FP32; per-tile partial sums are converted to 64-bit fixed
 // point and combined with integer atomics, so results do not depend on
 // scheduling order.
+#include <algorithm>
+
 #include "pb2_common.cuh"
 #include "pb2_kernels.cuh"
 #include "pb2_pairmath.cuh"
@@ -34,15 +37,19 @@
 #ifndef PB2_UNROLL
 #define PB2_UNROLL 4
 #endif
-// Minimum resident blocks per SM asked of the register allocator (bounds
-// registers per thread at 65536 / (256 * PB2_MINB)).
-#ifndef PB2_MINB
-#define PB2_MINB 3
-#endif
 
 namespace pb2 {
 
+// The descreening / chain-rule loop is not unrolled: each kernel holds five
+// tile variants (series lengths, near tiles) of two pairs per step, and
+// unrolling them outgrows the instruction cache (unroll 2 cost 6 % and
+// unroll 4 doubled the chain pass on B200).
+#ifndef PB2_UNROLL_BC
+#define PB2_UNROLL_BC 1
+#endif
+
 constexpr int kUnroll = PB2_UNROLL;
+constexpr int kUnrollBC = PB2_UNROLL_BC;
 
 __device__ __forceinline__ float shfl_next(float v, int src) { return __shfl_sync(kFull, v, src); }
 
@@ -97,116 +104,53 @@ struct TileConst {
   int src;
 };
 
-// One 32 x 32 tile.  V: rotated validity mask (bit k = pair at step k);
-// E, S14: rotated exclusion / 1-4 masks.  FAR: series OBC without checks;
-// NT: series terms (value; the derivative takes NT + 1).
-template <int PASS, bool FAR, bool CUT, bool FULL, bool EXCL, int NT = 10>
-__device__ __forceinline__ void run_tile(const PData &I, PData &J, Acc &ti, Acc &tj, uint32_t V,
-                                         uint32_t E, uint32_t S14, const TileConst &K) {
-  const int src = K.src;
-#pragma unroll kUnroll
-  for (int k = 0; k < 32; ++k) {
-    bool ok = FULL ? true : ((V >> k) & 1u);
-    const float dx = I.x - J.x, dy = I.y - J.y, dz = I.z - J.z;
-    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-    if (PASS != PASS_FORCE && CUT) ok = ok && (K.gcut2 == 0.f || r2 < K.gcut2);
-    if (PASS == PASS_BORN || PASS == PASS_CHAIN) {
-      // All lanes evaluate (results of invalid pairs are discarded), so the
-      // warp vote below is reached by every lane of the warp.
-      const float inv_r = rsqrtf(r2);
-      const float inv_r2 = inv_r * inv_r;
-      float vij, vji;
-      if (PASS == PASS_BORN) {
-        vij = obc_far_val<NT>(J.sr, inv_r);
-        vji = obc_far_val<NT>(I.sr, inv_r);
-      } else {
-        vij = obc_far_der<NT>(J.sr, inv_r, inv_r2);
-        vji = obc_far_der<NT>(I.sr, inv_r, inv_r2);
-      }
-      if (!FAR) {
-        // near tile: the series holds for most pairs; the closed form runs
-        // only for lanes whose pair lies inside the far-field bound
-        const float r = r2 * inv_r;
-        const bool need = ok && !far_pair(r, r2, I, J);
-        if (__any_sync(kFull, need)) {
-          if (need) {
-            if (PASS == PASS_BORN) {
-              vij = obc_integral(r, inv_r, I.ro, J.sr);
-              vji = obc_integral(r, inv_r, J.ro, I.sr);
-            } else {
-              vij = obc_integral_dr(r, inv_r, I.ro, J.sr);
-              vji = obc_integral_dr(r, inv_r, J.ro, I.sr);
-            }
-          }
-        }
-      }
-      if (ok) {
-        if (PASS == PASS_BORN) {
-          ti.a0 += vij;
-          tj.a0 += vji;
-        } else {
-          const float g = (I.dedi * vij + J.dedi * vji) * inv_r;
-          ti.a0 -= g * dx; ti.a1 -= g * dy; ti.a2 -= g * dz;
-          tj.a0 += g * dx; tj.a1 += g * dy; tj.a2 += g * dz;
-        }
-      }
-    } else if (ok) {
-      {
-        float g = 0.f;
-        const float qq = I.q * J.q;
-        if (K.use_gb && (!CUT || K.gcut2 == 0.f || r2 < K.gcut2)) {
-          const float w = r2 * (I.iB * J.iB);  // r^2 log2(e) / (4 B_i B_j)
-          const float ex = exp2f(-w);
-          const float f2 = fmaf(I.B * J.B, ex, r2);
-          const float inv_f = rsqrtf(f2);
-          const float inv_f3 = inv_f * inv_f * inv_f;
-          const float pq = K.pref * qq;
-          g = 2.0f * pq * (1.0f - 0.25f * ex) * inv_f3;
-          const float c = -pq * ex * fmaf(w, kInvQuarterLog2e * 0.25f, 1.0f) * inv_f3;
-          ti.a3 += c * J.B;
-          tj.a3 += c * I.B;
-        }
-        const bool excluded = EXCL ? ((E >> k) & 1u) : false;
-        if (!excluded && (K.use_lj || K.use_coul) && (!CUT || K.cut2 == 0.f || r2 < K.cut2)) {
-          const bool is14 = EXCL ? ((S14 >> k) & 1u) : false;
-          const float inv_r = rsqrtf(r2);
-          const float inv_r2 = inv_r * inv_r;
-          if (K.use_coul) {
-            const float ec = K.kcoul * qq * (is14 ? K.coul14 : 1.0f) * inv_r;
-            g += ec * inv_r2;
-          }
-          if (K.use_lj) {
-            const float sig = I.hs + J.hs;
-            const float eps = I.se * J.se * (is14 ? K.lj14 : 1.0f);
-            const float sr2 = sig * sig * inv_r2;
-            const float s6 = sr2 * sr2 * sr2;
-            g += 24.0f * eps * s6 * (2.0f * s6 - 1.0f) * inv_r2;
-          }
-        }
-        ti.a0 += g * dx; ti.a1 += g * dy; ti.a2 += g * dz;
-        tj.a0 -= g * dx; tj.a1 -= g * dy; tj.a2 -= g * dz;
-      }
+// GB polar pair force and dE/dB (both atoms), direct Coulomb and LJ for one
+// pair; g accumulates -dE/dr / r.
+template <bool CUT>
+__device__ __forceinline__ void force_pair(const PData &I, const PData &J, float dx, float dy, float dz,
+                                           float r2, bool excluded, bool is14, Acc &ti, Acc &tj,
+                                           const TileConst &K) {
+  float g = 0.f;
+  const float qq = I.q * J.q;
+  if (K.use_gb && (!CUT || K.gcut2 == 0.f || r2 < K.gcut2)) {
+    const float w = r2 * (I.iB * J.iB);  // r^2 log2(e) / (4 B_i B_j)
+    const float ex = exp2f(-w);
+    const float f2 = fmaf(I.B * J.B, ex, r2);
+    const float inv_f = rsqrtf(f2);
+    const float inv_f3 = inv_f * inv_f * inv_f;
+    const float pq = K.pref * qq;
+    g = 2.0f * pq * (1.0f - 0.25f * ex) * inv_f3;
+    const float c = -pq * ex * fmaf(w, kInvQuarterLog2e * 0.25f, 1.0f) * inv_f3;
+    ti.a3 += c * J.B;
+    tj.a3 += c * I.B;
+  }
+  if (!excluded && (K.use_lj || K.use_coul) && (!CUT || K.cut2 == 0.f || r2 < K.cut2)) {
+    const float inv_r = rsqrtf(r2);
+    const float inv_r2 = inv_r * inv_r;
+    if (K.use_coul) {
+      const float ec = K.kcoul * qq * (is14 ? K.coul14 : 1.0f) * inv_r;
+      g += ec * inv_r2;
     }
-    // rotate the j data and j partials one lane down
-    J.x = shfl_next(J.x, src); J.y = shfl_next(J.y, src); J.z = shfl_next(J.z, src);
-    tj.a0 = shfl_next(tj.a0, src);
-    if (PASS == PASS_BORN) {
-      J.sr = shfl_next(J.sr, src);
-      if (!FAR) J.ro = shfl_next(J.ro, src);
-    } else if (PASS == PASS_CHAIN) {
-      J.sr = shfl_next(J.sr, src);
-      if (!FAR) J.ro = shfl_next(J.ro, src);
-      J.dedi = shfl_next(J.dedi, src);
-      tj.a1 = shfl_next(tj.a1, src); tj.a2 = shfl_next(tj.a2, src);
-    } else {
-      J.q = shfl_next(J.q, src);
-      if (K.use_lj) { J.hs = shfl_next(J.hs, src); J.se = shfl_next(J.se, src); }
-      tj.a1 = shfl_next(tj.a1, src); tj.a2 = shfl_next(tj.a2, src);
-      if (K.use_gb) {
-        J.B = shfl_next(J.B, src); J.iB = shfl_next(J.iB, src);
-        tj.a3 = shfl_next(tj.a3, src);
-      }
+    if (K.use_lj) {
+      const float sig = I.hs + J.hs;
+      const float eps = I.se * J.se * (is14 ? K.lj14 : 1.0f);
+      const float sr2 = sig * sig * inv_r2;
+      const float s6 = sr2 * sr2 * sr2;
+      g += 24.0f * eps * s6 * (2.0f * s6 - 1.0f) * inv_r2;
     }
+  }
+  ti.a0 += g * dx; ti.a1 += g * dy; ti.a2 += g * dz;
+  tj.a0 -= g * dx; tj.a1 -= g * dy; tj.a2 -= g * dz;
+}
+
+// Force-pass rotation of everything but x, y, z and tj.a0.
+__device__ __forceinline__ void rotate_force_rest(PData &J, Acc &tj, int src, const TileConst &K) {
+  J.q = shfl_next(J.q, src);
+  if (K.use_lj) { J.hs = shfl_next(J.hs, src); J.se = shfl_next(J.se, src); }
+  tj.a1 = shfl_next(tj.a1, src); tj.a2 = shfl_next(tj.a2, src);
+  if (K.use_gb) {
+    J.B = shfl_next(J.B, src); J.iB = shfl_next(J.iB, src);
+    tj.a3 = shfl_next(tj.a3, src);
   }
 }
 
@@ -222,19 +166,155 @@ __device__ __forceinline__ void load_pdata(const PairArgs &a, int g, int pass, b
   }
 }
 
-// Work items are handed out dynamically: each warp takes the next item from
-// an atomic counter (items are sorted by cost, largest first), and the last
+// ---------------------------------------------------------------- force pass
+
+// One step of a force tile pair: lane's atom of each i-block against the j
+// atom currently in the lane.  V*: rotated validity masks (bit k = step k);
+// E*, S*: rotated exclusion / 1-4 masks.
+template <bool CUT, bool FULL, bool EXCL>
+__device__ __forceinline__ void run_force_tile2(const PData &I0, const PData &I1, PData &J, Acc &t0,
+                                                Acc &t1, Acc &tj, uint32_t V0, uint32_t V1, uint32_t E0,
+                                                uint32_t E1, uint32_t S0, uint32_t S1,
+                                                const TileConst &K) {
+  const int src = K.src;
+#pragma unroll kUnroll
+  for (int k = 0; k < 32; ++k) {
+    {
+      const bool ok = FULL ? true : ((V0 >> k) & 1u);
+      const float dx = I0.x - J.x, dy = I0.y - J.y, dz = I0.z - J.z;
+      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      if (ok)
+        force_pair<CUT>(I0, J, dx, dy, dz, r2, EXCL ? ((E0 >> k) & 1u) != 0 : false,
+                        EXCL ? ((S0 >> k) & 1u) != 0 : false, t0, tj, K);
+    }
+    {
+      const bool ok = FULL ? true : ((V1 >> k) & 1u);
+      const float dx = I1.x - J.x, dy = I1.y - J.y, dz = I1.z - J.z;
+      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      if (ok)
+        force_pair<CUT>(I1, J, dx, dy, dz, r2, EXCL ? ((E1 >> k) & 1u) != 0 : false,
+                        EXCL ? ((S1 >> k) & 1u) != 0 : false, t1, tj, K);
+    }
+    J.x = shfl_next(J.x, src); J.y = shfl_next(J.y, src); J.z = shfl_next(J.z, src);
+    tj.a0 = shfl_next(tj.a0, src);
+    rotate_force_rest(J, tj, src, K);
+  }
+}
+
+// ------------------------------------------------ descreening and chain rule
+
+struct BCPair {  // one pair's geometry and both directions' integral terms
+  float dx, dy, dz, r2, inv_r, vij, vji;
+  bool ok;
+};
+
+// Series value (born) or derivative (chain) of both directions, NT terms.
+template <int PASS, bool CUT, int NT>
+__device__ __forceinline__ void bc_series(const PData &I, const PData &J, bool ok, BCPair &P,
+                                          const TileConst &K) {
+  P.dx = I.x - J.x; P.dy = I.y - J.y; P.dz = I.z - J.z;
+  P.r2 = fmaf(P.dx, P.dx, fmaf(P.dy, P.dy, P.dz * P.dz));
+  if (CUT) ok = ok && (K.gcut2 == 0.f || P.r2 < K.gcut2);
+  P.ok = ok;
+  // every lane evaluates (invalid pairs are discarded), so a warp vote that
+  // follows is reached by all lanes
+  P.inv_r = rsqrtf(P.r2);
+  if (PASS == PASS_BORN) {
+    P.vij = obc_far_val<NT>(J.sr, P.inv_r);
+    P.vji = obc_far_val<NT>(I.sr, P.inv_r);
+  } else {
+    const float inv_r2 = P.inv_r * P.inv_r;
+    P.vij = obc_far_der<NT>(J.sr, P.inv_r, inv_r2);
+    P.vji = obc_far_der<NT>(I.sr, P.inv_r, inv_r2);
+  }
+}
+
+// A valid pair outside the series' domain (near tiles only).
+__device__ __forceinline__ bool bc_need(const PData &I, const PData &J, const BCPair &P) {
+  return P.ok && !far_pair(P.r2 * P.inv_r, P.r2, I, J);
+}
+
+template <int PASS>
+__device__ __forceinline__ void bc_closed(const PData &I, const PData &J, BCPair &P) {
+  const float r = P.r2 * P.inv_r;
+  if (PASS == PASS_BORN) {
+    P.vij = obc_integral(r, P.inv_r, I.ro, J.sr);
+    P.vji = obc_integral(r, P.inv_r, J.ro, I.sr);
+  } else {
+    P.vij = obc_integral_dr(r, P.inv_r, I.ro, J.sr);
+    P.vji = obc_integral_dr(r, P.inv_r, J.ro, I.sr);
+  }
+}
+
+template <int PASS>
+__device__ __forceinline__ void bc_accumulate(const PData &I, const PData &J, const BCPair &P, Acc &ti,
+                                              Acc &tj) {
+  if (!P.ok) return;
+  if (PASS == PASS_BORN) {
+    ti.a0 += P.vij;
+    tj.a0 += P.vji;
+  } else {
+    const float g = (I.dedi * P.vij + J.dedi * P.vji) * P.inv_r;
+    ti.a0 -= g * P.dx; ti.a1 -= g * P.dy; ti.a2 -= g * P.dz;
+    tj.a0 += g * P.dx; tj.a1 += g * P.dy; tj.a2 += g * P.dz;
+  }
+}
+
+// FAR: both tiles lie in the series' domain (no per-pair test); otherwise
+// each pair is tested and the closed form runs, after a warp vote, only for
+// the lanes that need it.
+template <int PASS, bool FAR, bool CUT, int NT>
+__device__ __forceinline__ void run_bc_tile2(const PData &I0, const PData &I1, PData &J, Acc &t0, Acc &t1,
+                                             Acc &tj, uint32_t V0, uint32_t V1, const TileConst &K) {
+  const int src = K.src;
+#pragma unroll kUnrollBC
+  for (int k = 0; k < 32; ++k) {
+    BCPair P0, P1;
+    bc_series<PASS, CUT, NT>(I0, J, (V0 >> k) & 1u, P0, K);
+    bc_series<PASS, CUT, NT>(I1, J, (V1 >> k) & 1u, P1, K);
+    if (!FAR) {
+      const bool n0 = bc_need(I0, J, P0), n1 = bc_need(I1, J, P1);
+      if (__any_sync(kFull, n0 || n1)) {
+        if (n0) bc_closed<PASS>(I0, J, P0);
+        if (n1) bc_closed<PASS>(I1, J, P1);
+      }
+    }
+    bc_accumulate<PASS>(I0, J, P0, t0, tj);
+    bc_accumulate<PASS>(I1, J, P1, t1, tj);
+    J.x = shfl_next(J.x, src); J.y = shfl_next(J.y, src); J.z = shfl_next(J.z, src);
+    J.sr = shfl_next(J.sr, src);
+    if (!FAR) J.ro = shfl_next(J.ro, src);
+    tj.a0 = shfl_next(tj.a0, src);
+    if (PASS == PASS_CHAIN) {
+      J.dedi = shfl_next(J.dedi, src);
+      tj.a1 = shfl_next(tj.a1, src); tj.a2 = shfl_next(tj.a2, src);
+    }
+  }
+}
+
+// ------------------------------------------------------------------- kernel
+
+// One warp per work item (system, even i-block ib, j-blocks [jb0, jb1)):
+// lane l owns atom l of i-block ib and atom l of i-block ib + 1, and every
+// j-block's data rotates once through the lanes, meeting both.  Tile
+// (ib + 1, ib) lies below the diagonal and is skipped; (ib + 1, ib + 1) is
+// the second block's diagonal tile.
+//
+// Items are handed out dynamically: each warp takes the next item from an
+// atomic counter (items are sorted by cost, largest first), and the last
 // warp to finish resets the counter for the next launch.
-template <int PASS, bool CUT>
-__global__ void __launch_bounds__(256, PB2_MINB) tile_kernel(const PairArgs a) {
+// ALL: GB, Coulomb and LJ all enabled (the term switches fold away).
+template <int PASS, bool CUT, bool ALL = false>
+__global__ void __launch_bounds__(256, 2) tile2_kernel(const PairArgs a) {
   const int lane = threadIdx.x & 31;
   const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
   TileConst K;
-  K.use_gb = (a.terms & PB2_USE_GB) != 0;
-  K.use_lj = (a.terms & PB2_USE_LJ) != 0;
-  K.use_coul = (a.terms & PB2_USE_COULOMB) != 0;
+  K.use_gb = ALL || (a.terms & PB2_USE_GB) != 0;
+  K.use_lj = ALL || (a.terms & PB2_USE_LJ) != 0;
+  K.use_coul = ALL || (a.terms & PB2_USE_COULOMB) != 0;
   K.src = (lane + 1) & 31;
   const uint32_t diag_mask = lane == 31 ? 0u : (0xffffffffu << (lane + 1));
+  const float bscale = PASS == PASS_BORN ? (float)kBornScale : (float)kForceScale;
 
   for (;;) {
     int it = 0;
@@ -246,27 +326,37 @@ __global__ void __launch_bounds__(256, PB2_MINB) tile_kernel(const PairArgs a) {
     const int n = S.n, off = S.off;
     K.cut2 = S.cutoff2; K.gcut2 = S.gb_cutoff2;
     K.pref = S.pref; K.kcoul = S.kcoul; K.lj14 = S.lj14; K.coul14 = S.coul14;
-    const float far2 = S.far2, far2_k8 = S.far2_k8, far2_k6 = S.far2_k6, far2_k4 = S.far2_k4;
-    const int gib = S.blk_base + item.iblk;
-    const int il = item.iblk * 32 + lane;
-    const bool ivalid = il < n;
-    const int ig = off + (ivalid ? il : n - 1);
+    const int ib0 = item.iblk, ib1 = item.iblk + 1;
+    const bool has1 = ib1 < S.nblk;
+    const int gib0 = S.blk_base + ib0, gib1 = S.blk_base + (has1 ? ib1 : ib0);
+    const int il0 = ib0 * 32 + lane, il1 = ib1 * 32 + lane;
+    const bool iv0 = il0 < n, iv1 = il1 < n;  // il1 >= n whenever !has1
+    const int ig0 = off + (iv0 ? il0 : n - 1), ig1 = off + (iv1 ? il1 : n - 1);
     // largest distance at which this pass has any pair term (0: unbounded)
     float reach2 = 0.f;
     if (CUT) {
       if (PASS == PASS_FORCE) reach2 = (K.gcut2 == 0.f || K.cut2 == 0.f) ? 0.f : fmaxf(K.gcut2, K.cut2);
       else reach2 = K.gcut2;
     }
-    PData I;
-    load_pdata(a, ig, PASS, K.use_gb, I);
+    PData I0, I1;
+    load_pdata(a, ig0, PASS, K.use_gb, I0);
+    load_pdata(a, ig1, PASS, K.use_gb, I1);
+    // exclusion entries: lanes 0-7 for block ib, lanes 8-15 for block ib + 1
     int2 ent = make_int2(-1, -1);
-    if (PASS == PASS_FORCE && lane < kExclPerBlock) ent = a.excl_ent[gib * kExclPerBlock + lane];
+    if (PASS == PASS_FORCE) {
+      if (lane < kExclPerBlock) ent = a.excl_ent[gib0 * kExclPerBlock + lane];
+      else if (has1 && lane < 2 * kExclPerBlock) ent = a.excl_ent[gib1 * kExclPerBlock + lane - kExclPerBlock];
+    }
 
-    long long ai0 = 0, ai1 = 0, ai2 = 0, ai3 = 0;  // i-side fixed-point sums
-
+    long long p0 = 0, p1 = 0, p2 = 0, p3 = 0, q0 = 0, q1 = 0, q2 = 0, q3 = 0;  // i-side sums
     for (int jb = item.jb0; jb < item.jb1; ++jb) {
       const int gjb = S.blk_base + jb;
-      const float d2 = (CUT || PASS != PASS_FORCE) ? box_dist2(a.bbox, gib, gjb) : 0.f;
+      // smallest bounding-box separation over the live tiles of the pair
+      float d2 = 0.f;
+      if (CUT || PASS != PASS_FORCE) {
+        d2 = box_dist2(a.bbox, gib0, gjb);
+        if (has1 && jb > ib0) d2 = fminf(d2, box_dist2(a.bbox, gib1, gjb));
+      }
       if (CUT && reach2 > 0.f && d2 >= reach2) continue;  // no pair within reach
       const int jl0 = jb * 32;
       const int jl = jl0 + lane;
@@ -274,72 +364,79 @@ __global__ void __launch_bounds__(256, PB2_MINB) tile_kernel(const PairArgs a) {
       const int jg = off + (jvalid ? jl : n - 1);
       PData J;
       load_pdata(a, jg, PASS, K.use_gb, J);
-      // pair validity of lane i with j-lane c: both exist, j > i on the diagonal
+      // pair validity of lane i with j-lane c: both exist, j > i on a diagonal
       const int nj = n - jl0;
       const uint32_t jmask = nj >= 32 ? 0xffffffffu : ((1u << nj) - 1u);
-      uint32_t C = ivalid ? jmask : 0u;
-      if (jb == item.iblk) C &= diag_mask;
-      const uint32_t V = rotr32(C, lane);
-      const bool full = __all_sync(kFull, C == 0xffffffffu);
-
-      uint32_t E = 0u, S14 = 0u;
-      bool excl = false;
-      if (PASS == PASS_FORCE) {
-        const unsigned hit = __ballot_sync(kFull, ent.x == jb);
-        if (hit) {
-          const int roff = __shfl_sync(kFull, ent.y, __ffs(hit) - 1);
-          const ExclRow r = a.excl_rows[roff + lane];
-          E = rotr32(r.excl, lane);
-          S14 = rotr32(r.s14, lane);
-          excl = true;
-        }
+      uint32_t C0 = iv0 ? jmask : 0u, C1 = iv1 ? jmask : 0u;
+      if (jb == ib0) {
+        C0 &= diag_mask;
+        C1 = 0u;
+      } else if (jb == ib1) {
+        C1 &= diag_mask;
       }
-      Acc ti = {0.f, 0.f, 0.f, 0.f}, tj = {0.f, 0.f, 0.f, 0.f};
-      if (PASS == PASS_FORCE) {
-        if (excl || !full) run_tile<PASS, false, CUT, false, true>(I, J, ti, tj, V, E, S14, K);
-        else run_tile<PASS, false, CUT, true, false>(I, J, ti, tj, V, E, S14, K);
-      } else if (d2 >= far2_k4) {  // series length by the tiles' smallest separation
-        run_tile<PASS, true, CUT, false, false, 4>(I, J, ti, tj, V, E, S14, K);
-      } else if (d2 >= far2_k6) {
-        run_tile<PASS, true, CUT, false, false, 6>(I, J, ti, tj, V, E, S14, K);
-      } else if (d2 >= far2_k8) {
-        run_tile<PASS, true, CUT, false, false, 8>(I, J, ti, tj, V, E, S14, K);
-      } else if (d2 >= far2) {
-        run_tile<PASS, true, CUT, false, false, 10>(I, J, ti, tj, V, E, S14, K);
+      const uint32_t V0 = rotr32(C0, lane), V1 = rotr32(C1, lane);
+
+      Acc t0 = {0.f, 0.f, 0.f, 0.f}, t1 = {0.f, 0.f, 0.f, 0.f}, tj = {0.f, 0.f, 0.f, 0.f};
+      if constexpr (PASS == PASS_FORCE) {
+        const bool full = __all_sync(kFull, (C0 & C1) == 0xffffffffu);
+        uint32_t E0 = 0u, S0 = 0u, E1 = 0u, S1 = 0u;
+        const unsigned hit = __ballot_sync(kFull, ent.x == jb);
+        const unsigned hit0 = hit & 0xffu, hit1 = hit & 0xff00u;
+        if (hit0) {
+          const int roff = __shfl_sync(kFull, ent.y, __ffs(hit0) - 1);
+          const ExclRow r = a.excl_rows[roff + lane];
+          E0 = rotr32(r.excl, lane); S0 = rotr32(r.s14, lane);
+        }
+        if (hit1) {
+          const int roff = __shfl_sync(kFull, ent.y, __ffs(hit1) - 1);
+          const ExclRow r = a.excl_rows[roff + lane];
+          E1 = rotr32(r.excl, lane); S1 = rotr32(r.s14, lane);
+        }
+        if (hit || !full) run_force_tile2<CUT, false, true>(I0, I1, J, t0, t1, tj, V0, V1, E0, E1, S0, S1, K);
+        else run_force_tile2<CUT, true, false>(I0, I1, J, t0, t1, tj, V0, V1, E0, E1, S0, S1, K);
       } else {
-        run_tile<PASS, false, CUT, false, false, 10>(I, J, ti, tj, V, E, S14, K);
+        // series length by the tiles' smallest separation
+        if (d2 >= S.far2_k4) run_bc_tile2<PASS, true, CUT, 4>(I0, I1, J, t0, t1, tj, V0, V1, K);
+        else if (d2 >= S.far2_k6) run_bc_tile2<PASS, true, CUT, 6>(I0, I1, J, t0, t1, tj, V0, V1, K);
+        else if (d2 >= S.far2_k8) run_bc_tile2<PASS, true, CUT, 8>(I0, I1, J, t0, t1, tj, V0, V1, K);
+        else if (d2 >= S.far2) run_bc_tile2<PASS, true, CUT, 10>(I0, I1, J, t0, t1, tj, V0, V1, K);
+        else run_bc_tile2<PASS, false, CUT, 10>(I0, I1, J, t0, t1, tj, V0, V1, K);
       }
 
       // j partials are back in their home lanes: flush them
       if (jvalid) {
         if (PASS == PASS_BORN) {
-          if (tj.a0 != 0.f) atomic_add_fix(&a.born_acc[jg], to_fix_f(tj.a0, (float)kBornScale));
+          if (tj.a0 != 0.f) atomic_add_fix(&a.born_acc[jg], to_fix_f(tj.a0, bscale));
         } else {
-          atomic_add_fix(&a.fx[jg], to_fix_f(tj.a0, (float)kForceScale));
-          atomic_add_fix(&a.fy[jg], to_fix_f(tj.a1, (float)kForceScale));
-          atomic_add_fix(&a.fz[jg], to_fix_f(tj.a2, (float)kForceScale));
-          if (PASS == PASS_FORCE && K.use_gb)
-            atomic_add_fix(&a.dedb_acc[jg], to_fix_f(tj.a3, (float)kForceScale));
+          atomic_add_fix(&a.fx[jg], to_fix_f(tj.a0, bscale));
+          atomic_add_fix(&a.fy[jg], to_fix_f(tj.a1, bscale));
+          atomic_add_fix(&a.fz[jg], to_fix_f(tj.a2, bscale));
+          if (PASS == PASS_FORCE && K.use_gb) atomic_add_fix(&a.dedb_acc[jg], to_fix_f(tj.a3, bscale));
         }
       }
-      if (PASS == PASS_BORN) {
-        ai0 += to_fix_f(ti.a0, (float)kBornScale);
-      } else {
-        ai0 += to_fix_f(ti.a0, (float)kForceScale);
-        ai1 += to_fix_f(ti.a1, (float)kForceScale);
-        ai2 += to_fix_f(ti.a2, (float)kForceScale);
-        if (PASS == PASS_FORCE) ai3 += to_fix_f(ti.a3, (float)kForceScale);
+      p0 += to_fix_f(t0.a0, bscale);
+      q0 += to_fix_f(t1.a0, bscale);
+      if (PASS != PASS_BORN) {
+        p1 += to_fix_f(t0.a1, bscale); p2 += to_fix_f(t0.a2, bscale);
+        q1 += to_fix_f(t1.a1, bscale); q2 += to_fix_f(t1.a2, bscale);
+      }
+      if (PASS == PASS_FORCE) {
+        p3 += to_fix_f(t0.a3, bscale);
+        q3 += to_fix_f(t1.a3, bscale);
       }
     }
 
-    if (ivalid) {
-      if (PASS == PASS_BORN) {
-        if (ai0 != 0) atomic_add_fix(&a.born_acc[ig], ai0);
-      } else {
-        atomic_add_fix(&a.fx[ig], ai0);
-        atomic_add_fix(&a.fy[ig], ai1);
-        atomic_add_fix(&a.fz[ig], ai2);
-        if (PASS == PASS_FORCE && K.use_gb) atomic_add_fix(&a.dedb_acc[ig], ai3);
+    if (PASS == PASS_BORN) {
+      if (iv0 && p0 != 0) atomic_add_fix(&a.born_acc[ig0], p0);
+      if (iv1 && q0 != 0) atomic_add_fix(&a.born_acc[ig1], q0);
+    } else {
+      if (iv0) {
+        atomic_add_fix(&a.fx[ig0], p0); atomic_add_fix(&a.fy[ig0], p1); atomic_add_fix(&a.fz[ig0], p2);
+        if (PASS == PASS_FORCE && K.use_gb) atomic_add_fix(&a.dedb_acc[ig0], p3);
+      }
+      if (iv1) {
+        atomic_add_fix(&a.fx[ig1], q0); atomic_add_fix(&a.fy[ig1], q1); atomic_add_fix(&a.fz[ig1], q2);
+        if (PASS == PASS_FORCE && K.use_gb) atomic_add_fix(&a.dedb_acc[ig1], q3);
       }
     }
   }
@@ -425,21 +522,34 @@ __global__ void born_finalize(const FinalizeArgs a) {
 
 // --------------------------------------------------------------- launchers
 
+template <int PASS, bool CUT, bool ALL>
+static void launch_one(const PairArgs &a, int grid, cudaStream_t st) {
+  tile2_kernel<PASS, CUT, ALL><<<grid, 256, 0, st>>>(a);
+}
+
 cudaError_t launch_tiles(int pass, const PairArgs &a, int grid, cudaStream_t st) {
   if (a.n_items <= 0) return cudaSuccess;
   const bool cut = a.cut != 0;
   switch (pass) {
     case PASS_BORN:
-      if (cut) tile_kernel<PASS_BORN, true><<<grid, 256, 0, st>>>(a);
-      else tile_kernel<PASS_BORN, false><<<grid, 256, 0, st>>>(a);
+      if (cut) launch_one<PASS_BORN, true, false>(a, grid, st);
+      else launch_one<PASS_BORN, false, false>(a, grid, st);
       break;
     case PASS_CHAIN:
-      if (cut) tile_kernel<PASS_CHAIN, true><<<grid, 256, 0, st>>>(a);
-      else tile_kernel<PASS_CHAIN, false><<<grid, 256, 0, st>>>(a);
+      if (cut) launch_one<PASS_CHAIN, true, false>(a, grid, st);
+      else launch_one<PASS_CHAIN, false, false>(a, grid, st);
       break;
-    default:
-      if (cut) tile_kernel<PASS_FORCE, true><<<grid, 256, 0, st>>>(a);
-      else tile_kernel<PASS_FORCE, false><<<grid, 256, 0, st>>>(a);
+    default: {
+      const int all_terms = PB2_USE_GB | PB2_USE_LJ | PB2_USE_COULOMB;
+      const bool all = (a.terms & all_terms) == all_terms;
+      if (cut) {
+        if (all) launch_one<PASS_FORCE, true, true>(a, grid, st);
+        else launch_one<PASS_FORCE, true, false>(a, grid, st);
+      } else {
+        if (all) launch_one<PASS_FORCE, false, true>(a, grid, st);
+        else launch_one<PASS_FORCE, false, false>(a, grid, st);
+      }
+    }
   }
   return cudaGetLastError();
 }
@@ -459,17 +569,19 @@ cudaError_t launch_born_finalize(const FinalizeArgs &a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-template <int PASS>
-static int occ(bool cut) {
+template <int PASS, bool CUT, bool ALL>
+static int occ_one() {
   int blocks = 0;
-  if (cut) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, tile_kernel<PASS, true>, 256, 0);
-  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, tile_kernel<PASS, false>, 256, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, tile2_kernel<PASS, CUT, ALL>, 256, 0);
   return blocks;
 }
 
 int tile_kernel_occupancy(int pass, bool cut) {
-  const int blocks = pass == PASS_BORN ? occ<PASS_BORN>(cut)
-                     : (pass == PASS_CHAIN ? occ<PASS_CHAIN>(cut) : occ<PASS_FORCE>(cut));
+  int blocks;
+  if (pass == PASS_BORN) blocks = cut ? occ_one<PASS_BORN, true, false>() : occ_one<PASS_BORN, false, false>();
+  else if (pass == PASS_CHAIN) blocks = cut ? occ_one<PASS_CHAIN, true, false>() : occ_one<PASS_CHAIN, false, false>();
+  else if (cut) blocks = std::min(occ_one<PASS_FORCE, true, false>(), occ_one<PASS_FORCE, true, true>());
+  else blocks = std::min(occ_one<PASS_FORCE, false, false>(), occ_one<PASS_FORCE, false, true>());
   return blocks > 0 ? blocks : 1;
 }
 
