@@ -8,7 +8,10 @@ CPU baseline beside it.
 One "step" = one BAOAB step (force evaluation included) of every system of
 the batch.  Workload: 512 systems with atom counts log-uniform in
 150-4,000 (seed 2024), OBC2 GB + Coulomb + LJ + bonded terms, all pairs,
-dt = 1 fs, gamma = 1/ps, T = 300 K.
+dt = 1 fs, gamma = 1/ps, T = 300 K.  Charges and LJ parameters come from
+synth.PHYSICAL_RANGES (|q| <= 0.5 e, sigma 2.4-3.4 A): with the generator's
+wider default ranges nearly every system blows up within 100 steps, and the
+pair kernels would then be timed on exploded geometry.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 Under torchrun each rank runs its own batch (replicas; seed offset by rank),
@@ -112,7 +115,8 @@ def dist_env():
 
 def workload(rank: int, n_systems: int):
   from prolix_b200 import replicas, synth
-  return synth.make_batch(n_systems, replicas.rank_seed(WORKLOAD_SEED, rank), 150, 4000, compact=True)
+  return synth.make_batch(n_systems, replicas.rank_seed(WORKLOAD_SEED, rank), 150, 4000, compact=True,
+                          **synth.PHYSICAL_RANGES)
 
 
 def unique_pairs(systems) -> int:
@@ -129,16 +133,18 @@ def cpu_model():
   return "unknown"
 
 
-def cpu_reference_run(systems, budget_s=12.0):
+def cpu_reference_run(systems, budget_s=12.0, start=0):
   """The FP64 C/OpenMP restatement of prolix's force field (oracle/) on the
   host's cores: one force evaluation per system (the O(N) integrator update,
   under 0.1 % of a step, is left out, which favours the CPU), systems in
-  workload order until the budget is spent.  Returns (atom-steps/s, sample,
-  threads)."""
+  workload order from ``start`` (wrapping) until the budget is spent or every
+  system ran once.  Returns (atom-steps/s, sample, threads, next start)."""
   from oracle import cforces
   threads = cforces.threads()
   atoms, t_total, used = 0, 0.0, 0
-  for s in systems:
+  n = len(systems)
+  while used < n:
+    s = systems[(start + used) % n]
     t0 = time.perf_counter()
     cforces.energy_forces(s, threads=threads)
     t_total += time.perf_counter() - t0
@@ -146,10 +152,10 @@ def cpu_reference_run(systems, budget_s=12.0):
     used += 1
     if t_total > budget_s:
       break
-  sample = (f"{used} of {len(systems)} systems x 1 step ({atoms} atom-steps); FP64 C/OpenMP "
+  sample = (f"{used} of {n} systems x 1 step ({atoms} atom-steps); FP64 C/OpenMP "
             "restatement of prolix's formulas (the reference's JAX path cannot run here: JAX "
             "is not installed)")
-  return atoms / t_total, sample, threads
+  return atoms / t_total, sample, threads, (start + used) % n
 
 
 def clocks_start(path):
@@ -200,23 +206,34 @@ def run_reference(args):
   if rank != 0:
     return 0
   systems = workload(0, args.systems)
-  budget = max(2.0, 60.0 / max(args.steps, 1))
+  # about two minutes of CPU work in total; successive steps continue through
+  # the workload where the previous one stopped, so the steps together sample
+  # every system size in proportion
+  budget = max(0.2, 120.0 / max(args.steps, 1))
   for _ in range(args.warmup):
     cpu_reference_run(systems[:1], budget_s=0.0)
   t0 = time.perf_counter()
-  vals = []
+  atoms_total, time_total, nxt = 0.0, 0.0, 0
   sample, threads = "", 1
   for _ in range(args.steps):
-    v, sample, threads = cpu_reference_run(systems, budget_s=budget)
-    vals.append(v)
-  value = float(np.mean(vals))
+    v, sample, threads, start = cpu_reference_run(systems, budget_s=budget, start=nxt)
+    n_used = (start - nxt) % len(systems) or len(systems)
+    atoms = sum(len(systems[(nxt + k) % len(systems)]["charges"]) for k in range(n_used))
+    atoms_total += atoms
+    time_total += atoms / v
+    nxt = start
+  value = atoms_total / time_total
+  sample = (f"{args.steps} steps of about {budget:.2f} s each, continuing through the "
+            f"{len(systems)}-system workload ({int(atoms_total)} atom-steps in all); " + sample.split("; ", 1)[1])
   line = {
       "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
       "steps": args.steps, "warmup": args.warmup,
       "ms_per_step": 1e3 * sum(len(s["charges"]) for s in systems) / value,
       "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
       "data": "synthetic (seeded chains)",
-      "config": {"workload": f"{args.systems} systems, N log-uniform 150-4000, all pairs",
+      "config": {"workload": f"{args.systems} systems, N log-uniform 150-4000 (seed {WORKLOAD_SEED}), "
+                             "OBC2 GB + Coulomb + LJ + bonded, all pairs, BAOAB dt 1 fs",
+                 "parameters": "charges U(-0.5, 0.5) e, LJ sigma U(2.4, 3.4) A, eps U(0.03, 0.2)",
                  "parallelism": f"{threads} host threads"},
       "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                        "sample": sample, "cpu": cpu_model()},
@@ -382,7 +399,7 @@ def main():
     if not args.no_serving:
       serving_rep = serving_bench(args)
     if not args.no_cpu:
-      v, sample, threads = cpu_reference_run(systems, budget_s=12.0)
+      v, sample, threads, _ = cpu_reference_run(systems, budget_s=12.0)
       cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
              "cpu": cpu_model()}
     line = {
@@ -392,6 +409,7 @@ def main():
         "data": "synthetic (seeded chains)",
         "config": {"workload": f"{args.systems} systems, N log-uniform 150-4000 (seed {WORKLOAD_SEED}), "
                                "OBC2 GB + Coulomb + LJ + bonded, all pairs, BAOAB dt 1 fs",
+                   "parameters": "charges U(-0.5, 0.5) e, LJ sigma U(2.4, 3.4) A, eps U(0.03, 0.2)",
                    "atoms_per_gpu": n_atoms, "unique_pairs_per_gpu": pairs,
                    "parallelism": f"replicas x{ws}",
                    "l2": "256 MB buffer written between timed steps",

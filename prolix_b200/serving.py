@@ -262,10 +262,12 @@ class Server:
 
 
 def poisson_requests(n: int, rate: float, seed: int, n_lo=100, n_hi=10_000, k_lo=1_000,
-                     k_hi=50_000, step_scale=1.0):
+                     k_hi=50_000, step_scale=1.0, ranges=None):
   """Seeded request stream: Poisson arrivals at ``rate``/s, atoms and steps
-  log-uniform; ``step_scale`` shrinks the step counts for bounded runs."""
+  log-uniform; ``step_scale`` shrinks the step counts for bounded runs.
+  Systems use ``synth.PHYSICAL_RANGES`` unless ``ranges`` is given."""
   from . import synth
+  ranges = synth.PHYSICAL_RANGES if ranges is None else ranges
   rng = np.random.default_rng(seed)
   t = np.cumsum(rng.exponential(1.0 / rate, size=n))
   sizes = np.exp(rng.uniform(math.log(n_lo), math.log(n_hi), size=n)).astype(int)
@@ -273,7 +275,7 @@ def poisson_requests(n: int, rate: float, seed: int, n_lo=100, n_hi=10_000, k_lo
   steps = np.maximum(1, (steps * step_scale).astype(int))
   reqs = []
   for i in range(n):
-    sys_ = synth.make_chain(int(sizes[i]), seed * 100003 + i, compact=True)
+    sys_ = synth.make_chain(int(sizes[i]), seed * 100003 + i, compact=True, **ranges)
     reqs.append(Request(system=sys_, n_steps=int(steps[i]), key=(0, int(seed * 7 + i)),
                         arrival=float(t[i]), rid=i))
   return reqs

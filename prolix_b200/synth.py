@@ -8,11 +8,11 @@ order, so a seed names one system exactly:
   stay at least 2.5 A apart where the packing allows.  ``compact=True`` keeps
   the chain inside a sphere of radius (3N / (4 pi 0.075))^(1/3) A where it
   can (20 A at N=2,500; 40 A at N=20,000), giving a compact globule;
-* charges U(-0.5, 0.5) e shifted to net zero; LJ sigma U(2.4, 3.4) A and
-  epsilon U(0.03, 0.2) kcal/mol (any two atoms of a random chain can meet,
-  so every atom keeps a real LJ core: a bare sigma-1 A site with a charge
-  of 0.8 e would collapse onto an opposite charge into a 0.5 A well that no
-  time step resolves); GB intrinsic radii U(1.2, 1.9) A and OBC
+* charges U(-0.8, 0.8) e shifted to net zero; LJ sigma U(1.0, 3.4) A and
+  epsilon U(0.01, 0.2) kcal/mol (ranges adjustable: with these, two
+  opposite charges on small-sigma sites can meet in a ~0.5 A well, so
+  constant-energy runs start from a minimised, thermalised state); GB
+  intrinsic radii U(1.2, 1.9) A and OBC
   scale factors U(0.72, 0.85), with ``scaled_radii = radii * scale``
   (the convention of prolix tests/physics/test_openmm_parity.py:113);
 * masses drawn from {1.008, 12.011, 14.007, 15.999} amu;
@@ -65,8 +65,18 @@ def _grow(lengths, angles, cand, compact, confine, retry_seed):
   return pos, chosen, rc
 
 
+# Parameter ranges with a real LJ core on every site.  With the default
+# ranges (|q| <= 0.8 e, sigma from 1 A) opposite charges meet in ~0.55 A
+# wells whose compressed LJ wall has omega * dt > 2 for hydrogen masses even
+# at 0.5 fs: nearly every system of a 512-system batch passes 1,000 K within
+# 100 Langevin steps at 1 fs.  Dynamics workloads (timing, serving, energy
+# drift) use these ranges instead; the draw order is unchanged.
+PHYSICAL_RANGES = {"charge_range": (-0.5, 0.5), "sigma_range": (2.4, 3.4), "eps_range": (0.03, 0.2)}
+
+
 def make_chain(n_atoms: int, seed: int, *, compact: bool = False, cmap: bool = False,
-               n_cmap_maps: int = 1, cmap_grid: int = 24) -> dict:
+               n_cmap_maps: int = 1, cmap_grid: int = 24, charge_range=(-0.8, 0.8),
+               sigma_range=(1.0, 3.4), eps_range=(0.01, 0.2)) -> dict:
   """Build one seeded synthetic system of ``n_atoms`` atoms."""
   if n_atoms < 1:
     raise ValueError("n_atoms must be >= 1")
@@ -79,10 +89,10 @@ def make_chain(n_atoms: int, seed: int, *, compact: bool = False, cmap: bool = F
   pos, _, _ = _grow(lengths, angles, cand, compact, globule_radius(n), retry_seed)
   pos = pos - pos.mean(axis=0, keepdims=True)
 
-  q = rng.uniform(-0.5, 0.5, size=n)
+  q = rng.uniform(*charge_range, size=n)
   q = q - q.mean()
-  sigma = rng.uniform(2.4, 3.4, size=n)
-  eps = rng.uniform(0.03, 0.2, size=n)
+  sigma = rng.uniform(*sigma_range, size=n)
+  eps = rng.uniform(*eps_range, size=n)
   radii = rng.uniform(1.2, 1.9, size=n)
   scale = rng.uniform(0.72, 0.85, size=n)
   masses = MASS_CHOICES[rng.integers(0, 4, size=n)]
@@ -140,8 +150,9 @@ def batch_sizes(n_systems: int, seed: int, lo: int = 150, hi: int = 4000) -> np.
 
 
 def make_batch(n_systems: int, seed: int, lo: int = 150, hi: int = 4000, *,
-               compact: bool = True, cmap: bool = False) -> list[dict]:
-  """``n_systems`` systems with log-uniform sizes; system k uses seed ``seed + 1 + k``."""
+               compact: bool = True, cmap: bool = False, **ranges) -> list[dict]:
+  """``n_systems`` systems with log-uniform sizes; system k uses seed
+  ``seed + 1 + k``; ``ranges`` as make_chain's (e.g. PHYSICAL_RANGES)."""
   sizes = batch_sizes(n_systems, seed, lo, hi)
-  return [make_chain(int(n), seed + 1 + k, compact=compact, cmap=cmap)
+  return [make_chain(int(n), seed + 1 + k, compact=compact, cmap=cmap, **ranges)
           for k, n in enumerate(sizes)]
