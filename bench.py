@@ -81,10 +81,10 @@ MUFU_PER_PAIR = {"born": 1, "force": 3, "chain": 1}
 # integrator: read x, p (48 B), F (24 B), mass, sigma, charge (24 B); write
 # x, p (48 B), posq (16 B), clear F (24 B)
 BYTES_PER_ATOM_STEP = 184
-# DRAM traffic per launch of the force pass on this workload, from
-# `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum` (see
-# profiles/tile_kernels_ragged512.md); None until measured for the kernel version
-FORCE_TRAFFIC_BYTES = None
+# DRAM traffic per launch of each pair pass on this workload
+# (dram__bytes_read.sum + dram__bytes_write.sum of one `ncu --set full`
+# capture; profiles/pair_kernels_ragged512.md gives the command)
+TRAFFIC_BYTES = {"born": 24.15e6, "force": 57.45e6, "chain": 47.43e6}
 
 
 def parse():
@@ -354,7 +354,7 @@ def main():
   roofline = {"kernel": f"tile_kernel pass '{dom}'", "bound": "fp32",
               "achieved": passes[dom]["tflops"], "peak": peak, "unit": "TFLOP/s",
               "frac": passes[dom]["frac"],
-              "traffic": FORCE_TRAFFIC_BYTES if dom == "force" else None,
+              "traffic": TRAFFIC_BYTES.get(dom),
               "peak_source": "FP32 FMA throughput measured in this run (pb2_fp32_peak)",
               "algorithmic_flops_per_launch": fpp[dom] * pairs,
               "flops_per_pair": fpp, "series_terms_mean": k_mean,
