@@ -98,6 +98,8 @@ def parse():
   ap.add_argument("--no-cpu", action="store_true")
   ap.add_argument("--no-e2e", action="store_true")
   ap.add_argument("--no-serving", action="store_true")
+  ap.add_argument("--no-extra", action="store_true",
+                  help="skip the single-system, neighbour-list and serving-sweep legs")
   ap.add_argument("--serving-requests", type=int, default=32)
   ap.add_argument("--serving-rate", type=float, default=20.0)
   ap.add_argument("--serving-step-scale", type=float, default=0.05)
@@ -282,6 +284,66 @@ def plain_run(systems, stream, steps):
           "note": "one batch per system, launches issued system after system"}
 
 
+def single_system_runs(stream, hbm_peak):
+  """The single-system configurations: N = 2,500 with CMAP and a 20 A cutoff
+  (neighbour list with 2 A skin), and the 20,000-atom globule all pairs and
+  at 20 A.  Device atom-steps/s of 50-step graph chunks, plus the
+  neighbour-list build (one pb2_nl_build, wall time around the call, which
+  includes its capacity check) with the bytes its rows and reference
+  positions write against the measured HBM bandwidth."""
+  import torch
+  from prolix_b200 import engine, synth
+  out = {}
+  for name, n, cutoff, steps in (("n2500_cut20", 2500, 20.0, 200), ("n20000_all", 20000, 0.0, 50),
+                                 ("n20000_cut20", 20000, 20.0, 50)):
+    sd = synth.make_chain(n, 2500 if n == 2500 else 4242, compact=True, cmap=True,
+                          **synth.PHYSICAL_RANGES)
+    with engine.Batch([sd], cutoff=cutoff, skin=2.0) as b:
+      b.langevin_init()
+      b.langevin_run(50, stream)
+      torch.cuda.synchronize()
+      e0 = torch.cuda.Event(enable_timing=True)
+      e1 = torch.cuda.Event(enable_timing=True)
+      e0.record()
+      b.langevin_run(steps, stream)
+      e1.record()
+      torch.cuda.synchronize()
+      ms = e0.elapsed_time(e1)
+      rec = {"atoms": n, "cutoff": cutoff, "steps": steps, "ms_per_step": ms / steps,
+             "atom_steps_per_s": n * steps / (ms * 1e-3)}
+      if cutoff > 0:
+        b.nl_build(stream)  # sizes the rows
+        cap = b.nl_capacity()
+        reps = 10
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+          b.nl_build(stream)
+        torch.cuda.synchronize()
+        t = (time.perf_counter() - t0) / reps
+        nbytes = n * cap * 4 + n * 24  # rows + reference positions
+        rec["nlist"] = {"capacity": cap, "build_ms": t * 1e3, "bytes_written": nbytes,
+                        "achieved_gbs": nbytes / t / 1e9, "peak_gbs": hbm_peak,
+                        "frac": nbytes / t / 1e9 / hbm_peak,
+                        "note": "wall time of pb2_nl_build incl. host-side grid setup and capacity check"}
+      out[name] = rec
+  return out
+
+
+def serving_sweep(args):
+  from prolix_b200 import serving
+  res = {}
+  for rate in (10.0, 50.0, 200.0, 500.0):
+    reqs = serving.poisson_requests(args.serving_requests, rate, WORKLOAD_SEED + int(rate),
+                                    step_scale=args.serving_step_scale)
+    srv = serving.Server(chunk=50)
+    srv.run(reqs)
+    rep = srv.report()
+    res[str(int(rate))] = {k: rep[k] for k in ("completed", "failed", "p50_s", "p99_s",
+                                               "atom_steps_per_s", "ticks")}
+  return res
+
+
 def main():
   args = parse()
   if args.impl == "reference":
@@ -342,20 +404,25 @@ def main():
   per_kernel = {n: float(v) for n, v in zip(names, tim[:7])}
 
   peak = ctypes_fp32_peak(batch)
+  # XU (MUFU) peak: 16 lanes per SM per clock at the SM clock seen under load
+  sm_mhz = (clocks or {}).get("sm_mhz") or 1965.0
+  xu_peak = 16 * torch.cuda.get_device_properties(local).multi_processor_count * sm_mhz * 1e6 / 1e12
   passes = {}
   k_mean = series_terms(systems)
   fpp = flops_per_pair(k_mean)
   for p in ("born", "force", "chain"):
     ms = per_kernel[p]
     tf = fpp[p] * pairs / (ms * 1e-3) / 1e12 if ms > 0 else None
+    mufu = MUFU_PER_PAIR[p] * pairs / (ms * 1e-3) / 1e12 if ms > 0 else None
     passes[p] = {"ms": ms, "tflops": tf, "frac": (tf / peak if tf and peak else None),
-                 "mufu_tops": MUFU_PER_PAIR[p] * pairs / (ms * 1e-3) / 1e12 if ms > 0 else None}
+                 "mufu_tops": mufu, "xu_frac": mufu / xu_peak if mufu else None}
   dom = max(("born", "force", "chain"), key=lambda p: per_kernel[p])
   roofline = {"kernel": f"tile_kernel pass '{dom}'", "bound": "fp32",
               "achieved": passes[dom]["tflops"], "peak": peak, "unit": "TFLOP/s",
               "frac": passes[dom]["frac"],
               "traffic": TRAFFIC_BYTES.get(dom),
               "peak_source": "FP32 FMA throughput measured in this run (pb2_fp32_peak)",
+              "xu_peak_tops": xu_peak,
               "algorithmic_flops_per_launch": fpp[dom] * pairs,
               "flops_per_pair": fpp, "series_terms_mean": k_mean,
               "passes": passes}
@@ -398,6 +465,11 @@ def main():
       plain = plain_run(systems, stream, steps=5)
     if not args.no_serving:
       serving_rep = serving_bench(args)
+    extra = None
+    if not args.no_extra:
+      extra = {"single_system": single_system_runs(stream, hbm_peak)}
+      if not args.no_serving:
+        extra["serving_sweep"] = serving_sweep(args)
     if not args.no_cpu:
       v, sample, threads, _ = cpu_reference_run(systems, budget_s=12.0)
       cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
@@ -422,6 +494,7 @@ def main():
         "plain": plain,
         "ragged_over_plain": value / (plain["value"] * ws) if plain else None,
         "serving": serving_rep,
+        "extra": extra,
         "e2e": e2e,
         "cpu_baseline": cpu,
         # per timed step: step, bbox, born, finalize, force, chain, bonded, finish

@@ -328,7 +328,7 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
       S.far2_k8 = bound2(0.104);
       S.far2_k6 = bound2(0.049);
       S.far2_k4 = bound2(0.0109);
-      S.pad0 = 0;
+      S.ro_max = romax;
     }
     for (int bk = 0; bk < S.nblk; ++bk) hblk_sys[blk_base + bk] = s;
     hkeys[2 * (size_t)s] = d.key[0];

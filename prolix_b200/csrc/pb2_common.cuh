@@ -48,7 +48,7 @@ struct SysInfo {
   float gb_cutoff2;   // GB / descreening cutoff^2; 0: all pairs
   int32_t clamp;      // neighbour-list clamps on Born radii (GB cutoff set)
   float far2_k8, far2_k6, far2_k4;  // tiles this far apart need 8 / 6 / 4 series terms
-  int32_t pad0;
+  float ro_max;       // largest rho~ = radius - offset of the system
   double kcoul_d;     // direct Coulomb constant in double (energy path)
   double pref_d;      // P in double (self / energy terms)
   double dt, half_dt; // tau

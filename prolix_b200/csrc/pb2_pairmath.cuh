@@ -25,7 +25,7 @@
 namespace pb2 {
 
 constexpr float kSeriesU = 0.09f;      // closed-form helpers' series shortcut (9 terms)
-constexpr float kSeriesUNear = 0.16f;  // per-pair test in near tiles (10 / 11 terms)
+constexpr float kSeriesUNear = 0.16f;  // per-pair test in near tiles (10 / 11 terms); 1/sqrt = 2.5
 
 // sum_{k=1..K} k/(2k+1) u^(k-1), Horner; coefficients folded at compile time.
 template <int K>
