@@ -312,7 +312,8 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
       hse[g] = std::sqrt(std::max(d.epsilons[i], 0.0));
       hro[g] = ro;
       hsr[g] = d.scaled_radii[i];
-      hpar[g] = make_float4((float)hhs[g], (float)hse[g], (float)ro, (float)hsr[g]);
+      // float copy for the pair kernels: sqrt(24 eps), so eps_ij * 24 is one product
+      hpar[g] = make_float4((float)hhs[g], (float)(hse[g] * std::sqrt(24.0)), (float)ro, (float)hsr[g]);
     }
     {  // far-field tiles: every pair has r - s >= rho~ and (s/r)^2 <= u_K
       float smax = 0.f, romax = 0.f;

@@ -116,31 +116,30 @@ __device__ __forceinline__ void force_pair(const PData &I, const PData &J, float
   float g = 0.f;
   const float qq = I.q * J.q;
   if (K.use_gb && (!CUT || K.gcut2 == 0.f || r2 < K.gcut2)) {
+    // E = P qq / f, f^2 = r^2 + B_i B_j e^(-r^2 / 4 B_i B_j); A = P qq / f^3
     const float w = r2 * (I.iB * J.iB);  // r^2 log2(e) / (4 B_i B_j)
     const float ex = exp2f(-w);
     const float f2 = fmaf(I.B * J.B, ex, r2);
     const float inv_f = rsqrtf(f2);
-    const float inv_f3 = inv_f * inv_f * inv_f;
-    const float pq = K.pref * qq;
-    g = 2.0f * pq * (1.0f - 0.25f * ex) * inv_f3;
-    const float c = -pq * ex * fmaf(w, kInvQuarterLog2e * 0.25f, 1.0f) * inv_f3;
-    ti.a3 += c * J.B;
-    tj.a3 += c * I.B;
+    const float A = (K.pref * qq) * (inv_f * inv_f * inv_f);
+    g = A * fmaf(-0.5f, ex, 2.0f);  // -dE/dr / r
+    const float c = -(A * ex) * fmaf(w, kInvQuarterLog2e * 0.25f, 1.0f);  // dE/dB_i B_i = c B_j
+    ti.a3 = fmaf(c, J.B, ti.a3);
+    tj.a3 = fmaf(c, I.B, tj.a3);
   }
   if (!excluded && (K.use_lj || K.use_coul) && (!CUT || K.cut2 == 0.f || r2 < K.cut2)) {
     const float inv_r = rsqrtf(r2);
     const float inv_r2 = inv_r * inv_r;
-    if (K.use_coul) {
-      const float ec = K.kcoul * qq * (is14 ? K.coul14 : 1.0f) * inv_r;
-      g += ec * inv_r2;
-    }
+    float s = 0.f;  // (-dE/dr) r for Coulomb and LJ
+    if (K.use_coul) s = K.kcoul * qq * (is14 ? K.coul14 : 1.0f) * inv_r;
     if (K.use_lj) {
       const float sig = I.hs + J.hs;
-      const float eps = I.se * J.se * (is14 ? K.lj14 : 1.0f);
       const float sr2 = sig * sig * inv_r2;
       const float s6 = sr2 * sr2 * sr2;
-      g += 24.0f * eps * s6 * (2.0f * s6 - 1.0f) * inv_r2;
+      const float eps24 = I.se * J.se * (is14 ? K.lj14 : 1.0f);  // se = sqrt(24 eps)
+      s = fmaf(eps24 * s6, fmaf(2.0f, s6, -1.0f), s);
     }
+    g = fmaf(s, inv_r2, g);
   }
   ti.a0 += g * dx; ti.a1 += g * dy; ti.a2 += g * dz;
   tj.a0 -= g * dx; tj.a1 -= g * dy; tj.a2 -= g * dz;
