@@ -41,15 +41,18 @@ WORKLOAD_SEED = 2024
 N_SYSTEMS = 512
 
 # Algorithmic work per unique pair (i < j), counted from the kernel source
-# with FMA = 2 flops (pb2_pair.cu run_tile).  The descreening and chain
-# passes evaluate the far-field series with K terms (K + 1 for its
+# with FMA = 2 flops (pb2_pair.cu bc_series / force_pair).  The descreening
+# and chain passes evaluate the far-field series with K terms (K + 1 for its
 # derivative), K chosen per tile from the bounding-box separation
 # (4, 6, 8 or 10); series_terms() gives the pair-weighted mean K.
-#   descreening: 3 (d) + 5 (r^2) + 2 x (2K + 3) (series value) + 2 (sums) = 4K + 16
-#   force:       GB 31 + Coulomb 5 + LJ 12 + 6 (d, r^2 share) + 12 (F)    = 66
-#   chain:       3 (d) + 5 (r^2) + 1 + 2 x (2(K+1) + 3) + 4 + 12 (F)      = 4K + 35
+#   descreening: 3 (d) + 5 (r^2) + 2 (1/r^2, 1/r^4)
+#                + 2 x (1 + 2(K-1) + 1) (u, series, s^3) + 2 x 2 (sums)  = 4K + 14
+#   force:       8 (d, r^2) + 1 (q q) + GB 16 + 4 (dE/dB) + 1 (1/r^2)
+#                + Coulomb 2 + LJ 11 + 2 (sum) + 12 (F)                  = 57
+#   chain:       3 (d) + 5 (r^2) + 3 (1/r^2, -1/r^6)
+#                + 2 x (1 + 2K + 1) + 4 (g) + 12 (F)                      = 4K + 31
 def flops_per_pair(k_mean: float) -> dict:
-  return {"born": 4.0 * k_mean + 16.0, "force": 66.0, "chain": 4.0 * k_mean + 35.0}
+  return {"born": 4.0 * k_mean + 14.0, "force": 57.0, "chain": 4.0 * k_mean + 31.0}
 
 
 def series_terms(systems) -> float:

@@ -65,24 +65,11 @@ __device__ __forceinline__ float box_dist2(const float4 *bbox, int a, int b) {
   return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
 }
 
-// Far-field OBC integral and derivative with K series terms (valid when
-// r - s >= rho~ and (s/r)^2 is inside K's domain; the caller guarantees it).
-template <int K>
-__device__ __forceinline__ float obc_far_val(float s, float inv_r) {
-  const float t = s * inv_r;
-  const float u = t * t;
-  return t * u * inv_r * obc_series_val_n<K>(u);
-}
-template <int K>
-__device__ __forceinline__ float obc_far_der(float s, float inv_r, float inv_r2) {
-  const float t = s * inv_r;
-  const float u = t * t;
-  return -t * u * inv_r2 * obc_series_der_n<K + 1>(u);
-}
 
 struct PData {  // per-atom data a lane holds (its i atom, or the j atom passing through)
   float x, y, z, q, hs, se, ro, sr, B, iB, dedi;  // iB = sqrt(log2 e / 4) / B
   float t2;  // (max(s / sqrt(kSeriesUNear), s + rho~_max))^2: series reach of this atom
+  float s2, s3;  // s^2, s^3 of the scaled radius (far-field series)
 };
 
 // Both directions of a pair inside the near-tile series' domain.  r >= t_i
@@ -163,6 +150,8 @@ __device__ __forceinline__ void load_pdata(const PairArgs &a, int g, int pass, b
   P.hs = c.x; P.se = c.y; P.ro = c.z; P.sr = c.w;
   const float t = fmaxf(P.sr * 2.5f, P.sr + ro_max);  // 2.5 = 1 / sqrt(kSeriesUNear)
   P.t2 = t * t;
+  P.s2 = P.sr * P.sr;
+  P.s3 = P.s2 * P.sr;
   P.B = P.iB = P.dedi = 0.f;
   if ((pass == PASS_FORCE && use_gb) || pass == PASS_CHAIN) {
     const float4 b = a.born[g];
@@ -208,8 +197,13 @@ __device__ __forceinline__ void run_force_tile2(const PData &I0, const PData &I1
 
 // ------------------------------------------------ descreening and chain rule
 
-struct BCPair {  // one pair's geometry and both directions' integral terms
-  float dx, dy, dz, r2, inv_r, vij, vji;
+// One pair's geometry and both directions' integral terms.  The series path
+// keeps the radial factor apart: I = s^3 S(s^2/r^2) / r^4 and
+// (dI/dr) / r = -s^3 D(s^2/r^2) / r^6, so vij, vji hold s^3 S (or s^3 D)
+// and f the common 1/r^4 (or -1/r^6); the closed form stores I (or dI/dr)
+// with f = 1 (or 1/r).
+struct BCPair {
+  float dx, dy, dz, r2, inv_r, vij, vji, f;
   bool ok;
 };
 
@@ -230,13 +224,15 @@ __device__ __forceinline__ void bc_series(const PData &I, const PData &J, bool o
   P.r2 = ok ? r2 : kFarR2;
   // every lane evaluates, so a warp vote that follows is reached by all lanes
   P.inv_r = rsqrtf(P.r2);
+  const float inv_r2 = P.inv_r * P.inv_r;
   if (PASS == PASS_BORN) {
-    P.vij = obc_far_val<NT>(J.sr, P.inv_r);
-    P.vji = obc_far_val<NT>(I.sr, P.inv_r);
+    P.vij = J.s3 * obc_series_val_n<NT>(J.s2 * inv_r2);
+    P.vji = I.s3 * obc_series_val_n<NT>(I.s2 * inv_r2);
+    P.f = inv_r2 * inv_r2;
   } else {
-    const float inv_r2 = P.inv_r * P.inv_r;
-    P.vij = obc_far_der<NT>(J.sr, P.inv_r, inv_r2);
-    P.vji = obc_far_der<NT>(I.sr, P.inv_r, inv_r2);
+    P.vij = J.s3 * obc_series_der_n<NT + 1>(J.s2 * inv_r2);
+    P.vji = I.s3 * obc_series_der_n<NT + 1>(I.s2 * inv_r2);
+    P.f = -(inv_r2 * inv_r2) * inv_r2;
   }
 }
 
@@ -251,9 +247,11 @@ __device__ __forceinline__ void bc_closed(const PData &I, const PData &J, BCPair
   if (PASS == PASS_BORN) {
     P.vij = obc_integral(r, P.inv_r, I.ro, J.sr);
     P.vji = obc_integral(r, P.inv_r, J.ro, I.sr);
+    P.f = 1.0f;
   } else {
     P.vij = obc_integral_dr(r, P.inv_r, I.ro, J.sr);
     P.vji = obc_integral_dr(r, P.inv_r, J.ro, I.sr);
+    P.f = P.inv_r;
   }
 }
 
@@ -261,10 +259,10 @@ template <int PASS>
 __device__ __forceinline__ void bc_accumulate(const PData &I, const PData &J, const BCPair &P, Acc &ti,
                                               Acc &tj) {
   if (PASS == PASS_BORN) {
-    ti.a0 += P.vij;
-    tj.a0 += P.vji;
+    ti.a0 = fmaf(P.vij, P.f, ti.a0);
+    tj.a0 = fmaf(P.vji, P.f, tj.a0);
   } else {
-    const float g = (I.dedi * P.vij + J.dedi * P.vji) * P.inv_r;
+    const float g = (I.dedi * P.vij + J.dedi * P.vji) * P.f;
     ti.a0 -= g * P.dx; ti.a1 -= g * P.dy; ti.a2 -= g * P.dz;
     tj.a0 += g * P.dx; tj.a1 += g * P.dy; tj.a2 += g * P.dz;
   }
@@ -296,8 +294,9 @@ __device__ __forceinline__ void run_bc_tile2(const PData &I0, const PData &I1, P
     bc_accumulate<PASS>(I0, J, P0, t0, tj);
     bc_accumulate<PASS>(I1, J, P1, t1, tj);
     J.x = shfl_next(J.x, src); J.y = shfl_next(J.y, src); J.z = shfl_next(J.z, src);
-    J.sr = shfl_next(J.sr, src);
+    J.s2 = shfl_next(J.s2, src); J.s3 = shfl_next(J.s3, src);
     if (!FAR) {
+      J.sr = shfl_next(J.sr, src);
       J.ro = shfl_next(J.ro, src);
       J.t2 = shfl_next(J.t2, src);
     }
