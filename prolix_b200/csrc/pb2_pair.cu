@@ -72,15 +72,6 @@ struct PData {  // per-atom data a lane holds (its i atom, or the j atom passing
   float s2, s3;  // s^2, s^3 of the scaled radius (far-field series)
 };
 
-// Both directions of a pair inside the near-tile series' domain.  r >= t_i
-// and r >= t_j give (s/r)^2 <= kSeriesUNear for both radii and r - s >=
-// rho~_max >= rho~ for both directions: a sufficient test in two
-// instructions (the exact one triggers the closed form on 13.2 % of near-tile
-// steps of the benchmark batch, this one on 13.4 %).
-__device__ __forceinline__ bool far_pair(float r2, const PData &I, const PData &J) {
-  return r2 >= fmaxf(I.t2, J.t2);
-}
-
 // 4 / log2(e), and sqrt(log2(e) / 4): the force pass stores 1/B pre-scaled by
 // sqrt(log2(e)/4) so that exp(-r^2 / (4 B_i B_j)) = exp2(-r^2 iB_i iB_j).
 constexpr float kInvQuarterLog2e = 2.7725887222397811f;
@@ -196,75 +187,125 @@ __device__ __forceinline__ void run_force_tile2(const PData &I0, const PData &I1
 }
 
 // ------------------------------------------------ descreening and chain rule
+//
+// Both pairs of a step (the lane's atom of i-block ib and of ib + 1, against
+// the same j atom) run the same arithmetic, so it is issued as packed FP32
+// pairs (fma.rn.f32x2 and friends: .x = block ib, .y = block ib + 1), which
+// halves the FP32 instructions of these passes.  Per component the results
+// are those of the scalar fmaf / fmul / fadd.  Transcendentals (rsqrt, the
+// closed form) and the j-side sums, to which both pairs add, stay scalar.
 
-// One pair's geometry and both directions' integral terms.  The series path
-// keeps the radial factor apart: I = s^3 S(s^2/r^2) / r^4 and
-// (dI/dr) / r = -s^3 D(s^2/r^2) / r^6, so vij, vji hold s^3 S (or s^3 D)
-// and f the common 1/r^4 (or -1/r^6); the closed form stores I (or dI/dr)
-// with f = 1 (or 1/r).
-struct BCPair {
-  float dx, dy, dz, r2, inv_r, vij, vji, f;
-  bool ok;
+struct PData2 {  // the lane's two i atoms, packed
+  float2 x, y, z, sr, ro, t2, s2, s3, dedi;
+};
+__device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ PData2 pack2(const PData &a, const PData &b) {
+  PData2 p;
+  p.x = make_float2(a.x, b.x); p.y = make_float2(a.y, b.y); p.z = make_float2(a.z, b.z);
+  p.sr = make_float2(a.sr, b.sr); p.ro = make_float2(a.ro, b.ro); p.t2 = make_float2(a.t2, b.t2);
+  p.s2 = make_float2(a.s2, b.s2); p.s3 = make_float2(a.s3, b.s3); p.dedi = make_float2(a.dedi, b.dedi);
+  return p;
+}
+
+template <int K>
+__device__ __forceinline__ float2 obc_series_val2(float2 u) {
+  float2 p = dup2((float)((double)K / (double)(2 * K + 1)));
+#pragma unroll
+  for (int k = K - 1; k >= 1; --k) p = __ffma2_rn(p, u, dup2((float)((double)k / (double)(2 * k + 1))));
+  return p;
+}
+template <int K>
+__device__ __forceinline__ float2 obc_series_der2(float2 u) {
+  float2 p = dup2((float)(2.0 * K * (K + 1) / (double)(2 * K + 1)));
+#pragma unroll
+  for (int k = K - 1; k >= 1; --k) p = __ffma2_rn(p, u, dup2((float)(2.0 * k * (k + 1) / (double)(2 * k + 1))));
+  return p;
+}
+
+struct Acc2 {
+  float2 a0, a1, a2;
 };
 
 // Invalid pairs (padding lanes, j <= i on a diagonal, beyond the cutoff)
-// are evaluated at r^2 = kFarR2: their series terms flush to exactly zero
-// (s^3 / r^4 underflows; the kernels flush subnormals), so they are summed
-// without a select and never reach the closed form.
+// are evaluated at r^2 = kFarR2: their radial factor underflows to exactly
+// zero (1/r^4 = 1e-60), so they are summed without a select and never reach
+// the closed form.
 constexpr float kFarR2 = 1e30f;
 
-// Series value (born) or derivative (chain) of both directions, NT terms.
+// Both pairs' geometry and both directions' integral terms.  The series path
+// keeps the radial factor apart: I = s^3 S(s^2/r^2) / r^4 and
+// -(dI/dr) / r = s^3 D(s^2/r^2) / r^6, so vij, vji hold s^3 S (or s^3 D) and
+// f the common 1/r^4 (or 1/r^6); the closed form stores I (or dI/dr) with
+// f = 1 (or -1/r).
+struct BCPair2 {
+  float2 dx, dy, dz, r2, inv_r, vij, vji, f;
+  bool ok0, ok1;
+};
+
 template <int PASS, bool CUT, int NT>
-__device__ __forceinline__ void bc_series(const PData &I, const PData &J, bool ok, BCPair &P,
-                                          const TileConst &K) {
-  P.dx = I.x - J.x; P.dy = I.y - J.y; P.dz = I.z - J.z;
-  const float r2 = fmaf(P.dx, P.dx, fmaf(P.dy, P.dy, P.dz * P.dz));
-  if (CUT) ok = ok && (K.gcut2 == 0.f || r2 < K.gcut2);
-  P.ok = ok;
-  P.r2 = ok ? r2 : kFarR2;
+__device__ __forceinline__ void bc_series2(const PData2 &I, const PData &J, bool ok0, bool ok1, BCPair2 &P,
+                                           const TileConst &K) {
+  P.dx = __fadd2_rn(I.x, dup2(-J.x));
+  P.dy = __fadd2_rn(I.y, dup2(-J.y));
+  P.dz = __fadd2_rn(I.z, dup2(-J.z));
+  const float2 r2 = __ffma2_rn(P.dx, P.dx, __ffma2_rn(P.dy, P.dy, __fmul2_rn(P.dz, P.dz)));
+  if (CUT) {
+    ok0 = ok0 && (K.gcut2 == 0.f || r2.x < K.gcut2);
+    ok1 = ok1 && (K.gcut2 == 0.f || r2.y < K.gcut2);
+  }
+  P.ok0 = ok0;
+  P.ok1 = ok1;
+  P.r2 = make_float2(ok0 ? r2.x : kFarR2, ok1 ? r2.y : kFarR2);
   // every lane evaluates, so a warp vote that follows is reached by all lanes
-  P.inv_r = rsqrtf(P.r2);
-  const float inv_r2 = P.inv_r * P.inv_r;
+  P.inv_r = make_float2(rsqrtf(P.r2.x), rsqrtf(P.r2.y));
+  const float2 inv_r2 = __fmul2_rn(P.inv_r, P.inv_r);
+  const float2 inv_r4 = __fmul2_rn(inv_r2, inv_r2);
   if (PASS == PASS_BORN) {
-    P.vij = J.s3 * obc_series_val_n<NT>(J.s2 * inv_r2);
-    P.vji = I.s3 * obc_series_val_n<NT>(I.s2 * inv_r2);
-    P.f = inv_r2 * inv_r2;
+    P.vij = __fmul2_rn(dup2(J.s3), obc_series_val2<NT>(__fmul2_rn(dup2(J.s2), inv_r2)));
+    P.vji = __fmul2_rn(I.s3, obc_series_val2<NT>(__fmul2_rn(I.s2, inv_r2)));
+    P.f = inv_r4;
   } else {
-    P.vij = J.s3 * obc_series_der_n<NT + 1>(J.s2 * inv_r2);
-    P.vji = I.s3 * obc_series_der_n<NT + 1>(I.s2 * inv_r2);
-    P.f = -(inv_r2 * inv_r2) * inv_r2;
+    P.vij = __fmul2_rn(dup2(J.s3), obc_series_der2<NT + 1>(__fmul2_rn(dup2(J.s2), inv_r2)));
+    P.vji = __fmul2_rn(I.s3, obc_series_der2<NT + 1>(__fmul2_rn(I.s2, inv_r2)));
+    P.f = __fmul2_rn(inv_r4, inv_r2);
   }
 }
 
-// A valid pair outside the series' domain (near tiles only).
-__device__ __forceinline__ bool bc_need(const PData &I, const PData &J, const BCPair &P) {
-  return P.ok && !far_pair(P.r2, I, J);
-}
-
+// Closed form for one component (c = 0: block ib, 1: block ib + 1).
 template <int PASS>
-__device__ __forceinline__ void bc_closed(const PData &I, const PData &J, BCPair &P) {
-  const float r = P.r2 * P.inv_r;
+__device__ __forceinline__ void bc_closed2(const PData2 &I, const PData &J, BCPair2 &P, int c) {
+  const float r2 = c ? P.r2.y : P.r2.x, inv_r = c ? P.inv_r.y : P.inv_r.x;
+  const float ro = c ? I.ro.y : I.ro.x, sr = c ? I.sr.y : I.sr.x;
+  const float r = r2 * inv_r;
+  float vij, vji, f;
   if (PASS == PASS_BORN) {
-    P.vij = obc_integral(r, P.inv_r, I.ro, J.sr);
-    P.vji = obc_integral(r, P.inv_r, J.ro, I.sr);
-    P.f = 1.0f;
+    vij = obc_integral(r, inv_r, ro, J.sr);
+    vji = obc_integral(r, inv_r, J.ro, sr);
+    f = 1.0f;
   } else {
-    P.vij = obc_integral_dr(r, P.inv_r, I.ro, J.sr);
-    P.vji = obc_integral_dr(r, P.inv_r, J.ro, I.sr);
-    P.f = P.inv_r;
+    vij = obc_integral_dr(r, inv_r, ro, J.sr);
+    vji = obc_integral_dr(r, inv_r, J.ro, sr);
+    f = -inv_r;
   }
+  if (c) { P.vij.y = vij; P.vji.y = vji; P.f.y = f; }
+  else { P.vij.x = vij; P.vji.x = vji; P.f.x = f; }
 }
 
 template <int PASS>
-__device__ __forceinline__ void bc_accumulate(const PData &I, const PData &J, const BCPair &P, Acc &ti,
-                                              Acc &tj) {
+__device__ __forceinline__ void bc_accumulate2(const PData2 &I, const PData &J, const BCPair2 &P, Acc2 &ti,
+                                               Acc &tj) {
   if (PASS == PASS_BORN) {
-    ti.a0 = fmaf(P.vij, P.f, ti.a0);
-    tj.a0 = fmaf(P.vji, P.f, tj.a0);
+    ti.a0 = __ffma2_rn(P.vij, P.f, ti.a0);
+    tj.a0 = fmaf(P.vji.x, P.f.x, fmaf(P.vji.y, P.f.y, tj.a0));
   } else {
-    const float g = (I.dedi * P.vij + J.dedi * P.vji) * P.f;
-    ti.a0 -= g * P.dx; ti.a1 -= g * P.dy; ti.a2 -= g * P.dz;
-    tj.a0 += g * P.dx; tj.a1 += g * P.dy; tj.a2 += g * P.dz;
+    // h = -(dE/dI_i dI_ij/dr + dE/dI_j dI_ji/dr) / r; F_i += h d, F_j -= h d
+    const float2 h = __fmul2_rn(__ffma2_rn(I.dedi, P.vij, __fmul2_rn(dup2(J.dedi), P.vji)), P.f);
+    ti.a0 = __ffma2_rn(h, P.dx, ti.a0);
+    ti.a1 = __ffma2_rn(h, P.dy, ti.a1);
+    ti.a2 = __ffma2_rn(h, P.dz, ti.a2);
+    tj.a0 = fmaf(-h.x, P.dx.x, fmaf(-h.y, P.dx.y, tj.a0));
+    tj.a1 = fmaf(-h.x, P.dy.x, fmaf(-h.y, P.dy.y, tj.a1));
+    tj.a2 = fmaf(-h.x, P.dz.x, fmaf(-h.y, P.dz.y, tj.a2));
   }
 }
 
@@ -272,27 +313,30 @@ __device__ __forceinline__ void bc_accumulate(const PData &I, const PData &J, co
 // each pair is tested and the closed form runs, after a warp vote, only for
 // the lanes that need it.
 template <int PASS, bool FAR, bool CUT, int NT>
-__device__ __forceinline__ void run_bc_tile2(const PData &I0, const PData &I1, PData &J, Acc &t0, Acc &t1,
-                                             Acc &tj, uint32_t V0, uint32_t V1, const TileConst &K) {
+__device__ __forceinline__ void run_bc_tile2(const PData2 &I, PData &J, Acc2 &ti, Acc &tj, uint32_t V0,
+                                             uint32_t V1, const TileConst &K) {
   const int src = K.src;
   // step k tests the sign bit of the bit-reversed mask shifted left k times
   uint32_t R0 = __brev(V0), R1 = __brev(V1);
 #pragma unroll kUnrollBC
   for (int k = 0; k < 32; ++k) {
-    BCPair P0, P1;
-    bc_series<PASS, CUT, NT>(I0, J, (int32_t)R0 < 0, P0, K);
-    bc_series<PASS, CUT, NT>(I1, J, (int32_t)R1 < 0, P1, K);
+    BCPair2 P;
+    bc_series2<PASS, CUT, NT>(I, J, (int32_t)R0 < 0, (int32_t)R1 < 0, P, K);
     R0 <<= 1;
     R1 <<= 1;
     if (!FAR) {
-      const bool n0 = bc_need(I0, J, P0), n1 = bc_need(I1, J, P1);
+      // r >= t_i and r >= t_j give (s/r)^2 <= kSeriesUNear for both radii and
+      // r - s >= rho~_max >= rho~ for both directions: a sufficient test in two
+      // instructions (the exact one triggers the closed form on 13.2 % of
+      // near-tile steps of the benchmark batch, this one on 13.4 %)
+      const bool n0 = P.ok0 && !(P.r2.x >= fmaxf(I.t2.x, J.t2));
+      const bool n1 = P.ok1 && !(P.r2.y >= fmaxf(I.t2.y, J.t2));
       if (__any_sync(kFull, n0 || n1)) {
-        if (n0) bc_closed<PASS>(I0, J, P0);
-        if (n1) bc_closed<PASS>(I1, J, P1);
+        if (n0) bc_closed2<PASS>(I, J, P, 0);
+        if (n1) bc_closed2<PASS>(I, J, P, 1);
       }
     }
-    bc_accumulate<PASS>(I0, J, P0, t0, tj);
-    bc_accumulate<PASS>(I1, J, P1, t1, tj);
+    bc_accumulate2<PASS>(I, J, P, ti, tj);
     J.x = shfl_next(J.x, src); J.y = shfl_next(J.y, src); J.z = shfl_next(J.z, src);
     J.s2 = shfl_next(J.s2, src); J.s3 = shfl_next(J.s3, src);
     if (!FAR) {
@@ -321,7 +365,7 @@ __device__ __forceinline__ void run_bc_tile2(const PData &I0, const PData &I1, P
 // warp to finish resets the counter for the next launch.
 // ALL: GB, Coulomb and LJ all enabled (the term switches fold away).
 #ifndef PB2_MINB_BORN
-#define PB2_MINB_BORN 2
+#define PB2_MINB_BORN 3
 #endif
 #ifndef PB2_MINB_CHAIN
 #define PB2_MINB_CHAIN 2
@@ -364,6 +408,7 @@ __global__ void __launch_bounds__(256, PASS == PASS_BORN ? PB2_MINB_BORN : (PASS
     PData I0, I1;
     load_pdata(a, ig0, PASS, K.use_gb, S.ro_max, I0);
     load_pdata(a, ig1, PASS, K.use_gb, S.ro_max, I1);
+    const PData2 I2 = pack2(I0, I1);  // descreening / chain passes
     // exclusion entries: lanes 0-7 for block ib, lanes 8-15 for block ib + 1
     int2 ent = make_int2(-1, -1);
     if (PASS == PASS_FORCE) {
@@ -419,11 +464,14 @@ __global__ void __launch_bounds__(256, PASS == PASS_BORN ? PB2_MINB_BORN : (PASS
         else run_force_tile2<CUT, true, false>(I0, I1, J, t0, t1, tj, V0, V1, E0, E1, S0, S1, K);
       } else {
         // series length by the tiles' smallest separation
-        if (d2 >= S.far2_k4) run_bc_tile2<PASS, true, CUT, 4>(I0, I1, J, t0, t1, tj, V0, V1, K);
-        else if (d2 >= S.far2_k6) run_bc_tile2<PASS, true, CUT, 6>(I0, I1, J, t0, t1, tj, V0, V1, K);
-        else if (d2 >= S.far2_k8) run_bc_tile2<PASS, true, CUT, 8>(I0, I1, J, t0, t1, tj, V0, V1, K);
-        else if (d2 >= S.far2) run_bc_tile2<PASS, true, CUT, 10>(I0, I1, J, t0, t1, tj, V0, V1, K);
-        else run_bc_tile2<PASS, false, CUT, 10>(I0, I1, J, t0, t1, tj, V0, V1, K);
+        Acc2 ti = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+        if (d2 >= S.far2_k4) run_bc_tile2<PASS, true, CUT, 4>(I2, J, ti, tj, V0, V1, K);
+        else if (d2 >= S.far2_k6) run_bc_tile2<PASS, true, CUT, 6>(I2, J, ti, tj, V0, V1, K);
+        else if (d2 >= S.far2_k8) run_bc_tile2<PASS, true, CUT, 8>(I2, J, ti, tj, V0, V1, K);
+        else if (d2 >= S.far2) run_bc_tile2<PASS, true, CUT, 10>(I2, J, ti, tj, V0, V1, K);
+        else run_bc_tile2<PASS, false, CUT, 10>(I2, J, ti, tj, V0, V1, K);
+        t0.a0 = ti.a0.x; t0.a1 = ti.a1.x; t0.a2 = ti.a2.x;
+        t1.a0 = ti.a0.y; t1.a1 = ti.a1.y; t1.a2 = ti.a2.y;
       }
 
       // j partials are back in their home lanes: flush them
