@@ -42,6 +42,13 @@ extern "C" int pb2_ctx_create(int device, pb2_ctx **out) {
   if (!c) return PB2_ENOMEM;
   c->device = device;
   c->sm_count = prop.multiProcessorCount;
+  // keep memory freed by dropped batches in this process's pool (the
+  // attribute belongs to this process's context and ends with it)
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
   *out = c;
   return PB2_OK;
 }

@@ -23,23 +23,35 @@ constexpr int kTimBorn = 0, kTimFinalize = 1, kTimForce = 2, kTimChain = 3, kTim
               kTimStep = 5, kTimBbox = 6, kTimAll = 7, kTimSlots = 8;
 
 // Device allocations owned by a batch, freed with it.
+// Device allocations of one batch.  They come from the device's stream-ordered
+// memory pool (which pb2_ctx_create sets to keep freed memory), so building
+// and dropping batches -- what a serving loop does all the time -- reuses
+// memory instead of calling the driver's allocator and its implicit device
+// synchronisation.  Allocation completes before alloc() returns; frees are
+// ordered on the default stream after the owner has synchronised the device.
 struct Dev {
   std::vector<void *> ptrs;
   ~Dev() {
-    for (void *p : ptrs) cudaFree(p);
+    for (void *p : ptrs)
+      if (p) cudaFreeAsync(p, 0);
   }
   template <class T>
   T *alloc(size_t n) {
     void *p = nullptr;
     if (n == 0) n = 1;
-    if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return nullptr;
+    if (cudaMallocAsync(&p, n * sizeof(T), 0) != cudaSuccess) return nullptr;
+    if (cudaStreamSynchronize(0) != cudaSuccess) {
+      cudaFreeAsync(p, 0);
+      return nullptr;
+    }
     ptrs.push_back(p);
     return static_cast<T *>(p);
   }
-  void release(void *p) {
+  void release(void *p) {  // rare (rebuilds): wait for every user of p first
     for (auto &q : ptrs)
       if (q == p) {
-        cudaFree(q);
+        cudaDeviceSynchronize();
+        cudaFreeAsync(q, 0);
         q = nullptr;
       }
   }

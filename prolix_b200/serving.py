@@ -27,7 +27,7 @@ from collections import deque
 
 import numpy as np
 
-from . import engine
+from . import engine, topology
 from ._lib import STATUS_FORCE_RANGE, STATUS_NONFINITE
 
 BYTES_PER_ATOM = 320  # device footprint of one atom in a batch (state, pair data, scratch)
@@ -67,9 +67,13 @@ class _Slot:
   req: Request
   x: np.ndarray
   p: np.ndarray
+  f: np.ndarray   # forces at x: a rebuilt batch restores them instead of re-evaluating
   key: np.ndarray
   done: int
   admitted: float
+
+
+_FIELDS = ("position", "momentum", "force", "key")
 
 
 def _percentile(v, q):
@@ -99,6 +103,8 @@ class Server:
     self._batch_ids = None
     self.atom_steps = 0
     self.ticks = 0
+    if self.batch_factory is engine.Batch:
+      engine.Context.get(device)  # open the device now, not inside the first request
 
   # ------------------------------------------------------------------ api
   def now(self) -> float:
@@ -115,6 +121,9 @@ class Server:
       self.results[req.rid] = Result(req.rid, None, None, None, 0, req.arrival, float("nan"),
                                      self.now(), error="system larger than the server budget")
       return req.rid
+    if "excl_pairs" not in req.system:  # once per request, not on every batch rebuild
+      pairs, kind = topology.exclusion_pairs(req.system.get("bonds", np.zeros((0, 2))), n)
+      req.system = dict(req.system, excl_pairs=pairs, excl_kind=kind)
     self.queue.append(req)
     return req.rid
 
@@ -156,7 +165,7 @@ class Server:
     systems = [dict(r.system, key=r.key, dt=r.dt, kT=r.kT, gamma=r.gamma) for r in admitted]
     with self.batch_factory(systems, cutoff=self.cutoff, device=self.device) as nb:
       nb.langevin_init()
-      st = nb.get_state()
+      st = nb.get_state(fields=_FIELDS)
       status = nb.status()
     for k, r in enumerate(admitted):
       lo, hi = nb.offsets[k], nb.offsets[k + 1]
@@ -164,7 +173,7 @@ class Server:
         self._fail(r, now, now, "non-finite initial state")
         continue
       self.active.append(_Slot(r, st["position"][lo:hi].copy(), st["momentum"][lo:hi].copy(),
-                               st["key"][k].copy(), 0, now))
+                               st["force"][lo:hi].copy(), st["key"][k].copy(), 0, now))
     return True
 
   def _fail(self, req, admitted, now, msg):
@@ -178,17 +187,21 @@ class Server:
       self._batch.close()
     self._batch = self.batch_factory(systems, cutoff=self.cutoff, device=self.device,
                                      graph_chunk=self.chunk)
-    self._batch.set_state(position=np.concatenate([s.x for s in self.active]),
-                          momentum=np.concatenate([s.p for s in self.active]),
-                          key=np.stack([s.key for s in self.active]))
+    # forces are a function of each system's own float32 frame only, so the
+    # saved ones are bit-identical to a fresh evaluation in the new batch
+    self._batch.set_full_state(np.concatenate([s.x for s in self.active]),
+                               np.concatenate([s.p for s in self.active]),
+                               np.concatenate([s.f for s in self.active]),
+                               key=np.stack([s.key for s in self.active]))
     self._batch_ids = [s.req.rid for s in self.active]
 
   def _save(self):
-    st = self._batch.get_state()
+    st = self._batch.get_state(fields=_FIELDS)
     for k, s in enumerate(self.active):
       lo, hi = self._batch.offsets[k], self._batch.offsets[k + 1]
       s.x = st["position"][lo:hi].copy()
       s.p = st["momentum"][lo:hi].copy()
+      s.f = st["force"][lo:hi].copy()
       s.key = st["key"][k].copy()
     return self._batch.status(clear=True)
 

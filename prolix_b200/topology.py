@@ -4,9 +4,10 @@ coefficients.
 * Exclusions follow prolix's rule (utils/topology.py:26-93,
   physics/neighbor_list.py:52-142): pairs one, two or three bonds apart,
   each at its shortest separation; 1-2 and 1-3 pairs are excluded from
-  Coulomb and LJ, 1-4 pairs are scaled.  Computed here with sparse
-  adjacency powers: a pair joined by a walk of length k and by none shorter
-  is a 1-(k+1) pair.
+  Coulomb and LJ, 1-4 pairs are scaled.  Computed here from the bond
+  adjacency by vectorised walks: pairs of neighbours of one atom are the
+  two-bond candidates, pairs across the ends of one bond the three-bond
+  candidates, each kept only where no shorter separation exists.
 * CMAP coefficients follow prolix physics/cmap.py:166-286: periodic cubic
   spline derivatives at the grid points (d/dphi, d/dpsi, and d/dphi of
   d/dpsi), then one bicubic per patch matching values and
@@ -21,37 +22,68 @@ from __future__ import annotations
 import math
 
 import numpy as np
-import scipy.sparse as sp
 
 LJ14_DEFAULT = float(np.float32(0.5))
 COUL14_DEFAULT = float(np.float32(0.83333333))
 
 
+def _uniq(x):
+  """Sorted unique values (sort-based; faster here than np.unique's hashing)."""
+  x = np.sort(x)
+  if x.size:
+    x = x[np.concatenate([[True], x[1:] != x[:-1]])]
+  return x
+
+
+def _minus(a, b):
+  """Sorted unique a without the values of sorted unique b."""
+  if not b.size or not a.size:
+    return a
+  pos = np.minimum(np.searchsorted(b, a), b.size - 1)
+  return a[b[pos] != a]
+
+
 def exclusion_pairs(bonds, n_atoms: int):
   """(pairs (M, 2) int32 with i < j, kind (M,) int32: 0 = 1-2/1-3, 1 = 1-4)."""
   bonds = np.asarray(bonds, dtype=np.int64).reshape(-1, 2)
+  bonds = bonds[bonds[:, 0] != bonds[:, 1]]
   if bonds.shape[0] == 0 or n_atoms < 2:
     return np.zeros((0, 2), np.int32), np.zeros(0, np.int32)
-  a = sp.coo_matrix((np.ones(2 * len(bonds), dtype=np.int8),
-                     (np.concatenate([bonds[:, 0], bonds[:, 1]]),
-                      np.concatenate([bonds[:, 1], bonds[:, 0]]))),
-                    shape=(n_atoms, n_atoms)).tocsr()
-  a.data[:] = 1
-  a2 = (a @ a).tocsr()
-  a3 = (a2 @ a).tocsr()
+  n = int(n_atoms)
+  # adjacency in CSR form (both directions, duplicates removed)
+  key = _uniq(np.concatenate([bonds[:, 0] * n + bonds[:, 1], bonds[:, 1] * n + bonds[:, 0]]))
+  src, dst = key // n, key % n
+  start = np.searchsorted(src, np.arange(n + 1))
+  deg = np.diff(start)
+  maxdeg = int(deg.max())
 
-  def upper_pairs(m):
-    m = sp.triu(m, k=1).tocoo()
-    keep = m.data != 0
-    return set(zip(m.row[keep].tolist(), m.col[keep].tolist()))
+  def pair_keys(i, j):
+    keep = i != j
+    i, j = i[keep], j[keep]
+    return _uniq(np.minimum(i, j) * n + np.maximum(i, j))
 
-  s12 = upper_pairs(a)
-  s13 = upper_pairs(a2) - s12
-  s14 = upper_pairs(a3) - s12 - s13
-  rows = [(i, j, 0) for (i, j) in s12 | s13] + [(i, j, 1) for (i, j) in s14]
-  rows.sort()
-  arr = np.array(rows, dtype=np.int64).reshape(-1, 3)
-  return arr[:, :2].astype(np.int32), arr[:, 2].astype(np.int32)
+  k12 = pair_keys(src, dst)
+  # two bonds: neighbours k < l of a common atom c
+  cand13 = []
+  for k in range(maxdeg):
+    for l in range(k + 1, maxdeg):
+      c = np.nonzero(deg > l)[0]
+      cand13.append(pair_keys(dst[start[c] + k], dst[start[c] + l]))
+  k13 = _minus(_uniq(np.concatenate(cand13)) if cand13 else np.zeros(0, np.int64), k12)
+  # three bonds: a - b - c - d over every bond (b, c), a in N(b), d in N(c)
+  cand14 = []
+  for k in range(maxdeg):
+    for l in range(maxdeg):
+      e = np.nonzero((deg[src] > k) & (deg[dst] > l))[0]
+      cand14.append(pair_keys(dst[start[src[e]] + k], dst[start[dst[e]] + l]))
+  k12_13 = np.sort(np.concatenate([k12, k13]))
+  k14 = _minus(_uniq(np.concatenate(cand14)), k12_13)
+  keys = np.concatenate([k12_13, k14])
+  kind = np.concatenate([np.zeros(len(k12) + len(k13), np.int32), np.ones(len(k14), np.int32)])
+  order = np.argsort(keys, kind="stable")
+  keys, kind = keys[order], kind[order]
+  pairs = np.stack([keys // n, keys % n], axis=1).astype(np.int32)
+  return pairs, kind
 
 
 def _periodic_spline_slopes(y: np.ndarray) -> np.ndarray:

@@ -145,3 +145,52 @@ def test_far_field_series_lengths_meet_float32_bound():
     ev = (val(u, 400) - val(u, k)) / val(u, 400)
     ed = (der(u, 400) - der(u, k + 1)) / der(u, 400)
     assert 0 <= ev < 2e-8 and 0 <= ed < 2e-8, (k, u, ev, ed)
+
+
+def test_exclusion_pairs_match_breadth_first_search():
+  # 1-2 / 1-3 / 1-4 classes by shortest bond separation (prolix
+  # utils/topology.py:26-93) on chains, branched trees, rings and a
+  # multi-bond topology, against an independent breadth-first search.
+  from collections import deque
+
+  from prolix_b200 import topology
+
+  def bfs_classes(bonds, n):
+    adj = [[] for _ in range(n)]
+    for i, j in bonds:
+      if i != j:
+        adj[i].append(j)
+        adj[j].append(i)
+    out = {}
+    for s in range(n):
+      dist = {s: 0}
+      q = deque([s])
+      while q:
+        u = q.popleft()
+        if dist[u] == 3:
+          continue
+        for v in adj[u]:
+          if v not in dist:
+            dist[v] = dist[u] + 1
+            q.append(v)
+      for t, d in dist.items():
+        if t > s and d >= 1:
+          out[(s, t)] = 0 if d <= 2 else 1
+    return out
+
+  rng = np.random.default_rng(5)
+  cases = [np.stack([np.arange(30), np.arange(1, 31)], 1),                     # chain
+           np.array([[0, 1], [1, 2], [2, 3], [3, 4], [4, 5], [5, 0], [2, 6]]),  # ring + branch
+           np.array([[0, 1], [0, 2], [0, 3], [0, 4], [4, 5], [5, 6], [1, 1]])]  # star, self bond
+  for _ in range(5):  # random trees with extra ring-closing bonds
+    n = 60
+    par = np.array([rng.integers(0, k) for k in range(1, n)])
+    b = np.stack([par, np.arange(1, n)], 1)
+    extra = rng.integers(0, n, size=(4, 2))
+    cases.append(np.concatenate([b, extra, b[:3]]))
+  for b in cases:
+    n = int(b.max()) + 1
+    pairs, kind = topology.exclusion_pairs(b, n)
+    got = {(int(i), int(j)): int(k) for (i, j), k in zip(pairs, kind)}
+    assert got == bfs_classes(b.tolist(), n)
+    assert np.all(pairs[:, 0] < pairs[:, 1])

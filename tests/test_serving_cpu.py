@@ -33,8 +33,14 @@ class FakeBatch:
     self.x = self.x + 0.001 * n
     self.p = self.p + n
 
-  def get_state(self):
-    return {"position": self.x.copy(), "momentum": self.p.copy(), "key": self.k.copy()}
+  def get_state(self, fields=("position", "momentum", "key")):
+    st = {"position": self.x.copy(), "momentum": self.p.copy(), "key": self.k.copy(),
+          "force": -self.x.copy()}
+    return {f: st[f] for f in fields}
+
+  def set_full_state(self, position, momentum, force, key=None):
+    assert np.array_equal(force, -position)  # the forces saved with these positions
+    self.set_state(position=position, momentum=momentum, key=key)
 
   def set_state(self, position=None, momentum=None, key=None):
     self.x, self.p, self.k = position.copy(), momentum.copy(), key.copy()
