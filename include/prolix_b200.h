@@ -197,6 +197,30 @@ int pb2_set_state(pb2_batch *batch, const double *x, const double *p, const uint
 int pb2_set_full_state(pb2_batch *batch, const double *x, const double *p, const double *f,
                        const uint32_t *keys, void *stream);
 
+/*
+ * Batched energy minimisation (replaces prolix batched_simulate.py:682-960,
+ * `batched_minimize`, whose SD and FIRE stages run per system under vmap).
+ * pb2_min_setup stores the current positions as the restraint reference and
+ * the per-atom selections (heavy / backbone; NULL: heavy = mass > 1.1 amu,
+ * backbone = heavy).  Each call then runs one stage on every system:
+ *   pb2_min_sd   : restrained steepest descent, dr = F dt capped at max_dx
+ *                  per atom (batched_simulate.py:748-791);
+ *   pb2_min_fire : FIRE from zero momentum (jax_md fire_descent, called at
+ *                  :818-878) with a per-atom displacement cap max_disp; the
+ *                  state ends at the positions of the lowest force RMS seen;
+ * with restraint E = k/2 sum |r - r0|^2 on kind 0 all atoms, 1 heavy atoms,
+ * 2 backbone atoms.  A system that turns non-finite returns to r0 and gets
+ * PB2_STATUS_NONFINITE.  FIRE uses the momentum arrays: call
+ * pb2_langevin_init before dynamics.  pb2_min_rms: per-system RMS over atoms
+ * of the unrestrained force (the convergence gate, :944-951).
+ */
+int pb2_min_setup(pb2_batch *batch, const uint8_t *heavy, const uint8_t *backbone);
+int pb2_min_sd(pb2_batch *batch, int32_t n_steps, double k, int32_t kind, double dt, double max_dx,
+               void *stream);
+int pb2_min_fire(pb2_batch *batch, int32_t n_steps, double k, int32_t kind, double dt_start,
+                 double dt_max, double max_disp, void *stream);
+int pb2_min_rms(pb2_batch *batch, double *rms, void *stream);
+
 /* Per-system status bits (PB2_STATUS_*) accumulated since the last clear. */
 int pb2_get_status(pb2_batch *batch, uint32_t *status, int clear, void *stream);
 

@@ -85,6 +85,12 @@ SIGNATURES = [
     ("pb2_get_state", ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_void_p] * 6),
     ("pb2_set_state", ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_void_p] * 4),
     ("pb2_set_full_state", ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_void_p] * 5),
+    ("pb2_min_setup", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("pb2_min_sd", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_double, ctypes.c_int32,
+                                  ctypes.c_double, ctypes.c_double, ctypes.c_void_p]),
+    ("pb2_min_fire", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_double, ctypes.c_int32,
+                                    ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_void_p]),
+    ("pb2_min_rms", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("pb2_get_status", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                       ctypes.c_void_p]),
     ("pb2_nl_build", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),

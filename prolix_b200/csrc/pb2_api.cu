@@ -897,6 +897,192 @@ extern "C" int pb2_set_full_state(pb2_batch *b, const double *x, const double *p
   return PB2_OK;
 }
 
+
+// ------------------------------------------------------------ minimisation
+
+static MinArgs min_args(pb2_batch *b) {
+  MinArgs a;
+  a.sys = b->sys;
+  a.atom_sys = b->atom_sys;
+  a.x = b->x; a.y = b->y; a.z = b->z;
+  a.px = b->px; a.py = b->py; a.pz = b->pz;
+  a.fx = b->fx; a.fy = b->fy; a.fz = b->fz;
+  a.mass = b->mass;
+  a.charge = b->charge;
+  a.posq = b->posq;
+  a.x0 = b->m_x0;
+  a.sel = b->m_sel;
+  a.ft = b->m_ft; a.xb = b->m_xb; a.best = b->m_best;
+  a.sys_dt = b->m_sys;
+  a.sys_alpha = b->m_sys + b->n_sys;
+  a.sys_best = b->m_sys + 2 * (size_t)b->n_sys;
+  a.sys_npos = b->m_npos;
+  a.status = b->status;
+  a.par = b->m_par;
+  a.n_total = b->n_total;
+  a.n_sys = b->n_sys;
+  return a;
+}
+
+extern "C" int pb2_min_setup(pb2_batch *b, const uint8_t *heavy, const uint8_t *backbone) {
+  if (!b) return PB2_EINVAL;
+  pb2_ctx *ctx = b->ctx;
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  const size_t N = b->n_total;
+  if (!b->m_x0) {
+    Dev &D = b->mdev;
+    b->m_x0 = D.alloc<double>(3 * N);
+    b->m_ft = D.alloc<double>(3 * N);
+    b->m_xb = D.alloc<double>(3 * N);
+    b->m_best = D.alloc<double>(3 * N);
+    b->m_par = D.alloc<double>(kMinNPar);
+    b->m_sys = D.alloc<double>(4 * (size_t)b->n_sys);
+    b->m_npos = D.alloc<int32_t>(b->n_sys);
+    b->m_sel = D.alloc<uint8_t>(N);
+    if (!b->m_x0 || !b->m_ft || !b->m_xb || !b->m_best || !b->m_par || !b->m_sys || !b->m_npos || !b->m_sel)
+      return fail(ctx, PB2_ENOMEM, "minimiser allocation failed");
+  }
+  // selections: heavy atoms default to mass > 1.1 amu (prolix simulate.py:596),
+  // backbone to the heavy atoms
+  std::vector<double> hm(N);
+  CUDA_TRY(ctx, cudaMemcpy(hm.data(), b->mass, N * sizeof(double), cudaMemcpyDeviceToHost));
+  std::vector<uint8_t> sel(N);
+  for (size_t i = 0; i < N; ++i) {
+    const bool h = heavy ? heavy[i] != 0 : hm[i] > 1.1;
+    const bool bb = backbone ? backbone[i] != 0 : h;
+    sel[i] = (uint8_t)((h ? 1 : 0) | (bb ? 2 : 0));
+  }
+  CUDA_TRY(ctx, cudaMemcpy(b->m_sel, sel.data(), N, cudaMemcpyHostToDevice));
+  CUDA_TRY(ctx, cudaMemcpy(b->m_x0, b->x, N * sizeof(double), cudaMemcpyDeviceToDevice));
+  CUDA_TRY(ctx, cudaMemcpy(b->m_x0 + N, b->y, N * sizeof(double), cudaMemcpyDeviceToDevice));
+  CUDA_TRY(ctx, cudaMemcpy(b->m_x0 + 2 * N, b->z, N * sizeof(double), cudaMemcpyDeviceToDevice));
+  b->min_ready = true;
+  return PB2_OK;
+}
+
+// mode 0: steepest descent steps; mode 1: FIRE iterations
+static int min_graph(pb2_batch *b, int mode, int chunk, cudaGraphExec_t *out) {
+  pb2_ctx *ctx = b->ctx;
+  auto key = std::make_pair(mode, chunk);
+  auto it = b->min_graphs.find(key);
+  if (it != b->min_graphs.end()) {
+    *out = it->second;
+    return PB2_OK;
+  }
+  const MinArgs ma = min_args(b);
+  cudaStream_t cs = b->cap_stream;
+  CUDA_TRY(ctx, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+  cudaError_t err = cudaSuccess;
+  for (int t = 0; t < chunk && err == cudaSuccess; ++t) {
+    if (mode == 0) {
+      err = launch_min(kMinOpSd, ma, nullptr, cs);
+      if (err == cudaSuccess) err = enqueue_forces(b, cs, false);
+    } else {
+      err = launch_min(kMinOpFireBegin, ma, nullptr, cs);
+      if (err == cudaSuccess) err = launch_min(kMinOpFireDrift, ma, nullptr, cs);
+      if (err == cudaSuccess) err = enqueue_forces(b, cs, false);
+      if (err == cudaSuccess) err = launch_min(kMinOpFireMix, ma, nullptr, cs);
+    }
+  }
+  cudaGraph_t g = nullptr;
+  cudaError_t e2 = cudaStreamEndCapture(cs, &g);
+  if (err != cudaSuccess || e2 != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return fail(ctx, PB2_ECUDA, std::string("graph capture failed: ") +
+                                    cudaGetErrorString(err != cudaSuccess ? err : e2));
+  }
+  cudaGraphExec_t ex = nullptr;
+  cudaError_t e3 = cudaGraphInstantiate(&ex, g, 0);
+  cudaGraphDestroy(g);
+  if (e3 != cudaSuccess) return fail(ctx, PB2_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e3));
+  b->min_graphs[key] = ex;
+  *out = ex;
+  return PB2_OK;
+}
+
+static int min_run(pb2_batch *b, int mode, int n, cudaStream_t st) {
+  pb2_ctx *ctx = b->ctx;
+  int done = 0;
+  while (done < n) {
+    const int c = std::min(b->params.graph_chunk, n - done);
+    cudaGraphExec_t ex;
+    int rc = min_graph(b, mode, c, &ex);
+    if (rc) return rc;
+    CUDA_TRY(ctx, cudaGraphLaunch(ex, st));
+    done += c;
+  }
+  return PB2_OK;
+}
+
+static int min_begin(pb2_batch *b, int32_t n_steps, double k, int32_t kind, cudaStream_t st) {
+  pb2_ctx *ctx = b->ctx;
+  if (!b->min_ready) return fail(ctx, PB2_EINVAL, "call pb2_min_setup first");
+  if (n_steps < 0 || kind < 0 || kind > 2 || !(k >= 0.0)) return fail(ctx, PB2_EINVAL, "bad minimiser arguments");
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  b->m_par_host[kMinK] = k;
+  b->m_par_host[kMinKind] = kind;
+  CUDA_TRY(ctx, cudaMemcpyAsync(b->m_par, b->m_par_host, kMinNPar * sizeof(double), cudaMemcpyHostToDevice, st));
+  if (!b->forces_valid) {
+    int rc = fresh_forces(b, st, false);
+    if (rc) return rc;
+  }
+  return PB2_OK;
+}
+
+extern "C" int pb2_min_sd(pb2_batch *b, int32_t n_steps, double k, int32_t kind, double dt, double max_dx,
+                          void *stream) {
+  if (!b) return PB2_EINVAL;
+  if (!(dt > 0.0) || !(max_dx > 0.0)) return fail(b->ctx, PB2_EINVAL, "dt and max_dx must be > 0");
+  b->m_par_host[kMinSdDt] = dt;
+  b->m_par_host[kMinMaxDx] = max_dx;
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc = min_begin(b, n_steps, k, kind, st);
+  if (rc) return rc;
+  if ((rc = min_run(b, 0, n_steps, st))) return rc;
+  CUDA_TRY(b->ctx, launch_min(kMinOpRollback, min_args(b), nullptr, st));
+  b->forces_valid = false;  // a rolled-back system moved
+  CUDA_TRY(b->ctx, cudaStreamSynchronize(st));
+  return PB2_OK;
+}
+
+extern "C" int pb2_min_fire(pb2_batch *b, int32_t n_steps, double k, int32_t kind, double dt_start,
+                            double dt_max, double max_disp, void *stream) {
+  if (!b) return PB2_EINVAL;
+  if (!(dt_start > 0.0) || !(dt_max > 0.0) || !(max_disp > 0.0))
+    return fail(b->ctx, PB2_EINVAL, "dt_start, dt_max and max_disp must be > 0");
+  b->m_par_host[kMinDtStart] = dt_start;
+  b->m_par_host[kMinDtMax] = dt_max;
+  b->m_par_host[kMinMaxDisp] = max_disp;
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc = min_begin(b, n_steps, k, kind, st);
+  if (rc) return rc;
+  const MinArgs ma = min_args(b);
+  CUDA_TRY(b->ctx, launch_min(kMinOpFireInit, ma, nullptr, st));
+  if ((rc = min_run(b, 1, n_steps, st))) return rc;
+  CUDA_TRY(b->ctx, launch_min(kMinOpTakeBest, ma, nullptr, st));
+  CUDA_TRY(b->ctx, launch_min(kMinOpRollback, ma, nullptr, st));
+  b->forces_valid = false;
+  CUDA_TRY(b->ctx, cudaStreamSynchronize(st));
+  return PB2_OK;
+}
+
+extern "C" int pb2_min_rms(pb2_batch *b, double *rms, void *stream) {
+  if (!b || !rms) return PB2_EINVAL;
+  pb2_ctx *ctx = b->ctx;
+  if (!b->min_ready) return fail(ctx, PB2_EINVAL, "call pb2_min_setup first");
+  cudaStream_t st = (cudaStream_t)stream;
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  if (!b->forces_valid) {
+    int rc = fresh_forces(b, st, false);
+    if (rc) return rc;
+  }
+  double *out = b->m_sys + 3 * (size_t)b->n_sys;
+  CUDA_TRY(ctx, launch_min(kMinOpRms, min_args(b), out, st));
+  CUDA_TRY(ctx, cudaMemcpyAsync(rms, out, b->n_sys * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  return PB2_OK;
+}
+
 extern "C" int pb2_get_status(pb2_batch *b, uint32_t *status, int clear, void *stream) {
   if (!b || !status) return PB2_EINVAL;
   pb2_ctx *ctx = b->ctx;
@@ -923,6 +1109,8 @@ extern "C" int pb2_set_tile_segment(pb2_batch *b, int32_t segment) {
   if (int rc = setup_items2(b, segment)) return rc;
   for (auto &kv : b->graphs) cudaGraphExecDestroy(kv.second);  // they captured the old list
   b->graphs.clear();
+  for (auto &kv : b->min_graphs) cudaGraphExecDestroy(kv.second);
+  b->min_graphs.clear();
   return PB2_OK;
 }
 

@@ -97,6 +97,15 @@ struct pb2_batch {
   bool profiling = false;
   double timings[kTimSlots] = {0, 0, 0, 0, 0, 0, 0, 0};
   cudaEvent_t ev[2] = {nullptr, nullptr};
+  // minimiser state (allocated by pb2_min_setup)
+  Dev mdev;
+  bool min_ready = false;
+  double *m_x0 = nullptr, *m_ft = nullptr, *m_xb = nullptr, *m_best = nullptr, *m_par = nullptr;
+  double *m_sys = nullptr;  // dt, alpha, best rms, rms: (4, n_sys)
+  int32_t *m_npos = nullptr;
+  uint8_t *m_sel = nullptr;
+  std::map<std::pair<int, int>, cudaGraphExec_t> min_graphs;  // (mode, chunk)
+  double m_par_host[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   // neighbour list (allocated on first build)
   Dev nl;
   bool nl_built = false;
@@ -111,6 +120,7 @@ struct pb2_batch {
 
   ~pb2_batch() {
     for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
+    for (auto &kv : min_graphs) cudaGraphExecDestroy(kv.second);
     if (cap_stream) cudaStreamDestroy(cap_stream);
     for (auto &e : ev)
       if (e) cudaEventDestroy(e);

@@ -117,6 +117,31 @@ struct IntArgs {
   int32_t finish_prev;
   int32_t partitionable;
 };
+// Minimiser (pb2_minimize.cu).  Stage parameters live in device memory
+// (par[kMin*]) so that captured graphs serve every stage.
+enum { kMinK = 0, kMinKind, kMinSdDt, kMinMaxDx, kMinDtStart, kMinDtMax, kMinMaxDisp, kMinNPar };
+enum { kMinOpSd = 0, kMinOpRollback, kMinOpFireInit, kMinOpFireBegin, kMinOpFireDrift, kMinOpFireMix,
+       kMinOpTakeBest, kMinOpRms };
+// FIRE constants (Bitzek et al. 2006; jax_md fire_descent defaults)
+constexpr int kFireNmin = 5;
+constexpr double kFireFinc = 1.1, kFireFdec = 0.5, kFireAlphaStart = 0.1, kFireFalpha = 0.99;
+struct MinArgs {
+  const SysInfo *sys;
+  const int32_t *atom_sys;
+  double *x, *y, *z, *px, *py, *pz;
+  long long *fx, *fy, *fz;
+  const double *mass, *charge;
+  float4 *posq;
+  const double *x0;    // restraint reference, (3, n_total)
+  const uint8_t *sel;  // bit 0: heavy atom, bit 1: backbone atom
+  double *ft, *xb, *best;  // state force, positions before the step, best positions: (3, n_total)
+  double *sys_dt, *sys_alpha, *sys_best;
+  int32_t *sys_npos;
+  uint32_t *status;
+  const double *par;
+  int32_t n_total, n_sys;
+};
+cudaError_t launch_min(int op, const MinArgs &a, double *out, cudaStream_t st);
 cudaError_t launch_tiles(int pass, const PairArgs &a, int grid, cudaStream_t st);
 cudaError_t launch_energy64(int pass, const Energy64Args &a, int grid, cudaStream_t st);
 cudaError_t launch_born_finalize(const FinalizeArgs &a, cudaStream_t st);

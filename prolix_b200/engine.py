@@ -292,6 +292,35 @@ class Batch:
     self._check(self.lib.pb2_set_full_state(self.handle, x.ctypes.data, p.ctypes.data, f.ctypes.data,
                                             None if k is None else k.ctypes.data, stream))
 
+  # ------------------------------------------------------------ minimiser
+  def min_setup(self, heavy=None, backbone=None):
+    """Take the current positions as the restraint reference; per-atom
+    heavy / backbone selections (batch order), default mass > 1.1 amu."""
+    def mask(m):
+      if m is None:
+        return None
+      return np.ascontiguousarray(np.asarray(m, dtype=np.uint8).reshape(self.n_atoms))
+    h, bb = mask(heavy), mask(backbone)
+    self._min_masks = (h, bb)  # keep alive for the call
+    self._check(self.lib.pb2_min_setup(self.handle, None if h is None else h.ctypes.data,
+                                       None if bb is None else bb.ctypes.data))
+
+  MIN_KIND = {"all": 0, "heavy": 1, "backbone": 2}
+
+  def min_sd(self, n_steps, k=0.0, kind="all", dt=0.002, max_dx=0.01, stream=None):
+    self._check(self.lib.pb2_min_sd(self.handle, int(n_steps), float(k), self.MIN_KIND[kind],
+                                    float(dt), float(max_dx), stream))
+
+  def min_fire(self, n_steps, k=0.0, kind="all", dt_start=1e-4, dt_max=1e-3, max_disp=0.1, stream=None):
+    self._check(self.lib.pb2_min_fire(self.handle, int(n_steps), float(k), self.MIN_KIND[kind],
+                                      float(dt_start), float(dt_max), float(max_disp), stream))
+
+  def min_rms(self, stream=None):
+    """Per-system RMS over atoms of the unrestrained force, kcal/mol/A."""
+    out = np.zeros(self.n_systems)
+    self._check(self.lib.pb2_min_rms(self.handle, out.ctypes.data, stream))
+    return out
+
   def set_state(self, position=None, momentum=None, key=None, stream=None):
     x = None if position is None else _f64(position, (self.n_atoms, 3))
     p = None if momentum is None else _f64(momentum, (self.n_atoms, 3))
