@@ -333,6 +333,34 @@ def single_system_runs(stream, hbm_peak):
   return out
 
 
+def minimize_run(systems, stream):
+  """Throughput of the batched minimiser on the timing batch: 100 restrained
+  steepest-descent steps and 4 FIRE stages of 50 iterations (the
+  batched_minimize schedule, shortened), device time of the whole call."""
+  import torch
+  from prolix_b200 import engine, minimize
+  with engine.Batch(systems) as b:
+    b.min_setup()
+    rms0 = b.min_rms()
+    b.min_sd(5, k=minimize.SD_K, kind="heavy", dt=minimize.SD_DT, max_dx=minimize.SD_MAX_DX)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    b.min_sd(100, k=minimize.SD_K, kind="heavy", dt=minimize.SD_DT, max_dx=minimize.SD_MAX_DX)
+    for k, kind in zip(minimize.FIRE_K, minimize.FIRE_KIND):
+      b.min_fire(50, k=k, kind=kind, dt_start=minimize.FIRE_DT_START, dt_max=minimize.FIRE_DT_MAX,
+                 max_disp=minimize.FIRE_MAX_DISP)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    rms1 = b.min_rms()
+    n = b.n_atoms
+  iters = 100 + 4 * 50
+  return {"iterations": iters, "ms": ms, "atom_iterations_per_s": n * iters / (ms * 1e-3),
+          "rms_grad_median_before": float(np.median(rms0)), "rms_grad_median_after": float(np.median(rms1))}
+
+
 def serving_sweep(args):
   from prolix_b200 import serving
   res = {}
@@ -470,7 +498,8 @@ def main():
       serving_rep = serving_bench(args)
     extra = None
     if not args.no_extra:
-      extra = {"single_system": single_system_runs(stream, hbm_peak)}
+      extra = {"single_system": single_system_runs(stream, hbm_peak),
+               "minimize": minimize_run(systems, stream)}
       if not args.no_serving:
         extra["serving_sweep"] = serving_sweep(args)
     if not args.no_cpu:

@@ -221,6 +221,13 @@ int pb2_min_fire(pb2_batch *batch, int32_t n_steps, double k, int32_t kind, doub
                  double dt_max, double max_disp, void *stream);
 int pb2_min_rms(pb2_batch *batch, double *rms, void *stream);
 
+/* Replica exchange (replaces the state shuffle of prolix
+ * pt/replica_exchange.py:197-228): slot s takes the positions, momenta and
+ * forces of slot perm[s]; keys, step counters, kT and dt stay with the
+ * slots.  perm must be a permutation of 0..n_systems-1 pairing systems of
+ * equal atom count. */
+int pb2_permute_systems(pb2_batch *batch, const int32_t *perm, void *stream);
+
 /* Per-system status bits (PB2_STATUS_*) accumulated since the last clear. */
 int pb2_get_status(pb2_batch *batch, uint32_t *status, int clear, void *stream);
 

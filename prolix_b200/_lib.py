@@ -91,6 +91,7 @@ SIGNATURES = [
     ("pb2_min_fire", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_double, ctypes.c_int32,
                                     ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_void_p]),
     ("pb2_min_rms", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("pb2_permute_systems", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("pb2_get_status", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                       ctypes.c_void_p]),
     ("pb2_nl_build", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),

@@ -1083,6 +1083,40 @@ extern "C" int pb2_min_rms(pb2_batch *b, double *rms, void *stream) {
   return PB2_OK;
 }
 
+
+// Exchange the dynamical state of whole systems: slot s takes x, p and F of
+// slot perm[s].  Keys, step counters and per-system constants (kT, dt)
+// stay with their slots.  The systems swapped must have the same atom count.
+extern "C" int pb2_permute_systems(pb2_batch *b, const int32_t *perm, void *stream) {
+  if (!b || !perm) return PB2_EINVAL;
+  pb2_ctx *ctx = b->ctx;
+  cudaStream_t st = (cudaStream_t)stream;
+  std::vector<char> seen(b->n_sys, 0);
+  for (int s = 0; s < b->n_sys; ++s) {
+    const int t = perm[s];
+    if (t < 0 || t >= b->n_sys || seen[t]) return fail(ctx, PB2_EINVAL, "perm is not a permutation");
+    seen[t] = 1;
+    if (b->nat[t] != b->nat[s]) return fail(ctx, PB2_EINVAL, "permuted systems differ in atom count");
+  }
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  if (!b->d_perm) {
+    b->d_perm = b->dev.alloc<int32_t>(b->n_sys);
+    if (!b->d_perm) return fail(ctx, PB2_ENOMEM, "permutation buffer allocation failed");
+  }
+  CUDA_TRY(ctx, cudaMemcpyAsync(b->d_perm, perm, b->n_sys * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  const size_t N = b->n_total;
+  void *groups[3][3] = {{b->x, b->y, b->z}, {b->px, b->py, b->pz}, {b->fx, b->fy, b->fz}};
+  for (auto &g : groups) {
+    for (int c = 0; c < 3; ++c)
+      CUDA_TRY(ctx, launch_gather_systems(b->sys, b->atom_sys, b->d_perm, g[c], b->stage + c * N, b->n_total, st));
+    for (int c = 0; c < 3; ++c)
+      CUDA_TRY(ctx, cudaMemcpyAsync(g[c], b->stage + c * N, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  }
+  CUDA_TRY(ctx, launch_posq(int_args(b, b->key_parity, 0), st));
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  return PB2_OK;
+}
+
 extern "C" int pb2_get_status(pb2_batch *b, uint32_t *status, int clear, void *stream) {
   if (!b || !status) return PB2_EINVAL;
   pb2_ctx *ctx = b->ctx;

@@ -77,6 +77,7 @@ struct pb2_batch {
   double *q64 = nullptr, *hs64 = nullptr, *se64 = nullptr, *ro64 = nullptr, *sr64 = nullptr;
   double *born64 = nullptr;
   double *stage = nullptr;  // (n_total, 3) row-major staging for host transfers
+  int32_t *d_perm = nullptr;  // system permutation (replica exchange)
   long long *born_acc = nullptr, *dedb_acc = nullptr, *energy = nullptr;
   uint32_t *keys = nullptr, *status = nullptr;
   long long *steps = nullptr;

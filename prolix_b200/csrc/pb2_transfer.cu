@@ -49,6 +49,17 @@ __global__ void rows_to_fix(const double *__restrict__ rows, long long *fx, long
   }
 }
 
+// Gather whole systems: atom l of slot s takes atom l of slot perm[s]
+// (systems of equal size).  src and dst are (n, 8-byte word) arrays.
+__global__ void gather_systems(const SysInfo *sys, const int32_t *atom_sys, const int32_t *perm,
+                               const unsigned long long *__restrict__ src, unsigned long long *dst, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int s = atom_sys[i];
+    const int l = i - sys[s].off;
+    dst[i] = src[sys[perm[s]].off + l];
+  }
+}
+
 static int grid_for(int n) {
   const int g = (n + 255) / 256;
   return g < 1 ? 1 : (g > 4096 ? 4096 : g);
@@ -71,6 +82,14 @@ cudaError_t launch_fix_to_rows(const long long *fx, const long long *fy, const l
                                int n, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
   fix_to_rows<<<grid_for(n), 256, 0, st>>>(fx, fy, fz, rows, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather_systems(const SysInfo *sys, const int32_t *atom_sys, const int32_t *perm,
+                                  const void *src, void *dst, int n, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  gather_systems<<<grid_for(n), 256, 0, st>>>(sys, atom_sys, perm, (const unsigned long long *)src,
+                                              (unsigned long long *)dst, n);
   return cudaGetLastError();
 }
 

@@ -292,6 +292,12 @@ class Batch:
     self._check(self.lib.pb2_set_full_state(self.handle, x.ctypes.data, p.ctypes.data, f.ctypes.data,
                                             None if k is None else k.ctypes.data, stream))
 
+  def permute_systems(self, perm, stream=None):
+    """Slot s takes x, p and F of slot perm[s] (replica exchange); keys,
+    step counters, kT and dt stay with the slots."""
+    pm = np.ascontiguousarray(np.asarray(perm, dtype=np.int32).reshape(self.n_systems))
+    self._check(self.lib.pb2_permute_systems(self.handle, pm.ctypes.data, stream))
+
   # ------------------------------------------------------------ minimiser
   def min_setup(self, heavy=None, backbone=None):
     """Take the current positions as the restraint reference; per-atom
