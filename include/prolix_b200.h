@@ -169,6 +169,15 @@ int pb2_energy_forces(pb2_batch *batch, double *energies, double *forces, void *
 /* Born radii (n_atoms_total) at the current positions (system.py:204-216). */
 int pb2_born_radii(pb2_batch *batch, double *born, void *stream);
 
+/* The same with DEVICE pointers on the batch's device: positions (may be
+ * NULL: keep the current ones), energies (n_systems, PB2_NTERMS) and forces
+ * (n_atoms_total, 3), row-major FP64, either may be NULL.  Asynchronous on
+ * `stream`; allocates and synchronises nothing, so an XLA FFI handler (the
+ * binding a prolix maintainer adds for make_energy_fn, system.py:29-271)
+ * or a captured CUDA graph can call it. */
+int pb2_energy_forces_device(pb2_batch *batch, const double *positions, double *energies,
+                             double *forces, void *stream);
+
 /* Overwrite positions (n_atoms_total, 3). */
 int pb2_set_positions(pb2_batch *batch, const double *positions, void *stream);
 

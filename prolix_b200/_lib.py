@@ -92,6 +92,7 @@ SIGNATURES = [
                                     ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_void_p]),
     ("pb2_min_rms", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("pb2_permute_systems", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("pb2_energy_forces_device", ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_void_p] * 4),
     ("pb2_get_status", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                       ctypes.c_void_p]),
     ("pb2_nl_build", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),

@@ -656,6 +656,25 @@ static int copy_forces(pb2_batch *b, double *forces, cudaStream_t st) {
   return PB2_OK;
 }
 
+// Device-pointer variant: no host copy, no allocation, no synchronisation
+// (usable from an XLA custom call or under stream capture).
+extern "C" int pb2_energy_forces_device(pb2_batch *b, const double *positions, double *energies,
+                                        double *forces, void *stream) {
+  if (!b) return PB2_EINVAL;
+  pb2_ctx *ctx = b->ctx;
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t N = b->n_total;
+  if (positions) {
+    CUDA_TRY(ctx, cudaMemcpyAsync(b->stage, positions, 3 * N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(ctx, launch_rows_to_soa(b->stage, b->x, b->y, b->z, b->n_total, st));
+  }
+  int rc = fresh_forces(b, st, energies != nullptr);
+  if (rc) return rc;
+  if (energies) CUDA_TRY(ctx, launch_energies_to_double(b->energy, energies, b->n_sys, st));
+  if (forces) CUDA_TRY(ctx, launch_fix_to_rows(b->fx, b->fy, b->fz, forces, b->n_total, st));
+  return PB2_OK;
+}
+
 extern "C" int pb2_energy_forces(pb2_batch *b, double *energies, double *forces, void *stream) {
   if (!b) return PB2_EINVAL;
   pb2_ctx *ctx = b->ctx;

@@ -60,6 +60,20 @@ __global__ void gather_systems(const SysInfo *sys, const int32_t *atom_sys, cons
   }
 }
 
+// Per-system term energies (2^-24 fixed point) to FP64, with the total
+// summed in term order.
+__global__ void energies_to_double(const long long *__restrict__ e, double *out, int n_sys) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n_sys; s += gridDim.x * blockDim.x) {
+    double tot = 0.0;
+    for (int t = 0; t < PB2_TERM_TOTAL; ++t) {
+      const double v = (double)e[(size_t)s * PB2_NTERMS + t] * kEnergyInv;
+      out[(size_t)s * PB2_NTERMS + t] = v;
+      tot += v;
+    }
+    out[(size_t)s * PB2_NTERMS + PB2_TERM_TOTAL] = tot;
+  }
+}
+
 static int grid_for(int n) {
   const int g = (n + 255) / 256;
   return g < 1 ? 1 : (g > 4096 ? 4096 : g);
@@ -90,6 +104,12 @@ cudaError_t launch_gather_systems(const SysInfo *sys, const int32_t *atom_sys, c
   if (n <= 0) return cudaSuccess;
   gather_systems<<<grid_for(n), 256, 0, st>>>(sys, atom_sys, perm, (const unsigned long long *)src,
                                               (unsigned long long *)dst, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_energies_to_double(const long long *e, double *out, int n_sys, cudaStream_t st) {
+  if (n_sys <= 0) return cudaSuccess;
+  energies_to_double<<<grid_for(n_sys), 256, 0, st>>>(e, out, n_sys);
   return cudaGetLastError();
 }
 

@@ -292,6 +292,12 @@ class Batch:
     self._check(self.lib.pb2_set_full_state(self.handle, x.ctypes.data, p.ctypes.data, f.ctypes.data,
                                             None if k is None else k.ctypes.data, stream))
 
+  def energy_forces_device(self, positions_ptr, energies_ptr, forces_ptr, stream=None):
+    """pb2_energy_forces_device on raw device pointers (e.g. a torch tensor's
+    data_ptr()); any may be 0/None.  Asynchronous on ``stream``."""
+    self._check(self.lib.pb2_energy_forces_device(self.handle, positions_ptr or None, energies_ptr or None,
+                                                  forces_ptr or None, stream))
+
   def permute_systems(self, perm, stream=None):
     """Slot s takes x, p and F of slot perm[s] (replica exchange); keys,
     step counters, kT and dt stay with the slots."""

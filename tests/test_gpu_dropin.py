@@ -102,3 +102,36 @@ def test_minimization_and_run_simulation():
   assert fn(r) < e0
   out = simulate.run_simulation(s, pos, min_steps=10, therm_steps=20, key=prng.prng_key(2))
   assert out.shape == pos.shape and np.isfinite(out).all()
+
+
+def test_device_pointer_entry_point_and_graph_capture():
+  # pb2_energy_forces_device on torch device buffers equals the host entry
+  # point, and replays inside a captured CUDA graph on new positions.
+  import torch
+  systems = [synth.make_chain(n, 60 + n, compact=True, cmap=True) for n in (166, 300)]
+  with engine.Batch(systems) as b:
+    e_host, f_host = b.energy_forces()
+    n = b.n_atoms
+    pos = torch.tensor(np.concatenate([s["positions"] for s in systems]), dtype=torch.float64,
+                       device="cuda")
+    e_dev = torch.zeros((2, e_host.shape[1]), dtype=torch.float64, device="cuda")
+    f_dev = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    b.energy_forces_device(pos.data_ptr(), e_dev.data_ptr(), f_dev.data_ptr(), stream)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(f_dev.cpu().numpy(), f_host)
+    np.testing.assert_array_equal(e_dev.cpu().numpy(), e_host)
+
+    side = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=side):
+      b.energy_forces_device(pos.data_ptr(), e_dev.data_ptr(), f_dev.data_ptr(), side.cuda_stream)
+    moved = pos.cpu().numpy() + 0.05 * np.sin(np.arange(3 * n)).reshape(n, 3)
+    pos.copy_(torch.from_numpy(moved))
+    g.replay()
+    torch.cuda.synchronize()
+    b.set_positions(moved)
+    e_ref, f_ref = b.energy_forces()
+    np.testing.assert_array_equal(f_dev.cpu().numpy(), f_ref)
+    np.testing.assert_array_equal(e_dev.cpu().numpy(), e_ref)
+    del g
