@@ -46,6 +46,8 @@ def _minus(a, b):
 def exclusion_pairs(bonds, n_atoms: int):
   """(pairs (M, 2) int32 with i < j, kind (M,) int32: 0 = 1-2/1-3, 1 = 1-4)."""
   bonds = np.asarray(bonds, dtype=np.int64).reshape(-1, 2)
+  if bonds.size and (bonds.min() < 0 or bonds.max() >= n_atoms):
+    raise ValueError(f"bond index out of range for {n_atoms} atoms")
   bonds = bonds[bonds[:, 0] != bonds[:, 1]]
   if bonds.shape[0] == 0 or n_atoms < 2:
     return np.zeros((0, 2), np.int32), np.zeros(0, np.int32)

@@ -194,3 +194,13 @@ def test_exclusion_pairs_match_breadth_first_search():
     got = {(int(i), int(j)): int(k) for (i, j), k in zip(pairs, kind)}
     assert got == bfs_classes(b.tolist(), n)
     assert np.all(pairs[:, 0] < pairs[:, 1])
+
+
+def test_exclusion_finder_rejects_bad_bond_indices():
+  import pytest
+
+  from prolix_b200 import topology
+  with pytest.raises(ValueError, match="out of range"):
+    topology.exclusion_pairs(np.array([[0, 1], [2, 5]]), 5)
+  with pytest.raises(ValueError, match="out of range"):
+    topology.exclusion_pairs(np.array([[-1, 1]]), 5)
