@@ -237,6 +237,21 @@ int pb2_min_rms(pb2_batch *batch, double *rms, void *stream);
  * equal atom count. */
 int pb2_permute_systems(pb2_batch *batch, const int32_t *perm, void *stream);
 
+/*
+ * Trajectory frames (the state prolix's TrajectoryWriter stores,
+ * simulate.py:146-203, typing.py:652-707): a device ring of `capacity`
+ * frames of float32 positions and velocities (n_atoms_total, 3) plus every
+ * system's step counter.  pb2_traj_snapshot copies the current state into a
+ * slot asynchronously on `stream` (no host synchronisation; capturable);
+ * pb2_traj_fetch copies `count` slots from `first` to host buffers
+ * (frames in slot order, each (n_atoms_total, 3); steps (count, n_systems))
+ * and returns when they have arrived.  Any pointer may be NULL.
+ */
+int pb2_traj_setup(pb2_batch *batch, int32_t capacity);
+int pb2_traj_snapshot(pb2_batch *batch, int32_t slot, void *stream);
+int pb2_traj_fetch(pb2_batch *batch, int32_t first, int32_t count, float *positions, float *velocities,
+                   int64_t *steps, void *stream);
+
 /* Per-system status bits (PB2_STATUS_*) accumulated since the last clear. */
 int pb2_get_status(pb2_batch *batch, uint32_t *status, int clear, void *stream);
 

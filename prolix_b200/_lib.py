@@ -93,6 +93,9 @@ SIGNATURES = [
     ("pb2_min_rms", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("pb2_permute_systems", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("pb2_energy_forces_device", ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_void_p] * 4),
+    ("pb2_traj_setup", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    ("pb2_traj_snapshot", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]),
+    ("pb2_traj_fetch", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32] + [ctypes.c_void_p] * 4),
     ("pb2_get_status", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                       ctypes.c_void_p]),
     ("pb2_nl_build", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),

@@ -1136,6 +1136,65 @@ extern "C" int pb2_permute_systems(pb2_batch *b, const int32_t *perm, void *stre
   return PB2_OK;
 }
 
+
+// ------------------------------------------------------------ trajectories
+
+extern "C" int pb2_traj_setup(pb2_batch *b, int32_t capacity) {
+  if (!b || capacity <= 0) return PB2_EINVAL;
+  pb2_ctx *ctx = b->ctx;
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  const size_t f = 3 * (size_t)b->n_total;
+  if (capacity != b->traj_cap) {
+    if (b->traj_pos) {
+      b->tdev.release(b->traj_pos);
+      b->tdev.release(b->traj_vel);
+      b->tdev.release(b->traj_steps);
+    }
+    b->traj_pos = b->tdev.alloc<float>((size_t)capacity * f);
+    b->traj_vel = b->tdev.alloc<float>((size_t)capacity * f);
+    b->traj_steps = b->tdev.alloc<long long>((size_t)capacity * b->n_sys);
+    if (!b->traj_pos || !b->traj_vel || !b->traj_steps) {
+      b->traj_cap = 0;
+      return fail(ctx, PB2_ENOMEM, "trajectory ring allocation failed");
+    }
+    b->traj_cap = capacity;
+  }
+  return PB2_OK;
+}
+
+extern "C" int pb2_traj_snapshot(pb2_batch *b, int32_t slot, void *stream) {
+  if (!b) return PB2_EINVAL;
+  pb2_ctx *ctx = b->ctx;
+  if (slot < 0 || slot >= b->traj_cap) return fail(ctx, PB2_EINVAL, "trajectory slot out of range");
+  const size_t f = 3 * (size_t)b->n_total;
+  CUDA_TRY(ctx, launch_snapshot(b->x, b->y, b->z, b->px, b->py, b->pz, b->mass, b->steps,
+                                b->traj_pos + slot * f, b->traj_vel + slot * f,
+                                b->traj_steps + (size_t)slot * b->n_sys, b->n_total, b->n_sys,
+                                (cudaStream_t)stream));
+  return PB2_OK;
+}
+
+extern "C" int pb2_traj_fetch(pb2_batch *b, int32_t first, int32_t count, float *positions, float *velocities,
+                              int64_t *steps, void *stream) {
+  if (!b) return PB2_EINVAL;
+  pb2_ctx *ctx = b->ctx;
+  if (first < 0 || count < 0 || first + count > b->traj_cap)
+    return fail(ctx, PB2_EINVAL, "trajectory slots out of range");
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t f = 3 * (size_t)b->n_total;
+  if (positions)
+    CUDA_TRY(ctx, cudaMemcpyAsync(positions, b->traj_pos + first * f, count * f * sizeof(float),
+                                  cudaMemcpyDeviceToHost, st));
+  if (velocities)
+    CUDA_TRY(ctx, cudaMemcpyAsync(velocities, b->traj_vel + first * f, count * f * sizeof(float),
+                                  cudaMemcpyDeviceToHost, st));
+  if (steps)
+    CUDA_TRY(ctx, cudaMemcpyAsync(steps, b->traj_steps + (size_t)first * b->n_sys,
+                                  (size_t)count * b->n_sys * sizeof(long long), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  return PB2_OK;
+}
+
 extern "C" int pb2_get_status(pb2_batch *b, uint32_t *status, int clear, void *stream) {
   if (!b || !status) return PB2_EINVAL;
   pb2_ctx *ctx = b->ctx;

@@ -78,6 +78,12 @@ struct pb2_batch {
   double *born64 = nullptr;
   double *stage = nullptr;  // (n_total, 3) row-major staging for host transfers
   int32_t *d_perm = nullptr;  // system permutation (replica exchange)
+  // trajectory ring: capacity frames of float32 (n, 3) positions and
+  // velocities, and the step counters of every system
+  Dev tdev;
+  int traj_cap = 0;
+  float *traj_pos = nullptr, *traj_vel = nullptr;
+  long long *traj_steps = nullptr;
   long long *born_acc = nullptr, *dedb_acc = nullptr, *energy = nullptr;
   uint32_t *keys = nullptr, *status = nullptr;
   long long *steps = nullptr;

@@ -161,6 +161,9 @@ cudaError_t launch_fix_to_rows(const long long *fx, const long long *fy, const l
 cudaError_t launch_rows_to_fix(const double *rows, long long *fx, long long *fy, long long *fz, int n,
                                cudaStream_t st);
 cudaError_t launch_energies_to_double(const long long *e, double *out, int n_sys, cudaStream_t st);
+cudaError_t launch_snapshot(const double *x, const double *y, const double *z, const double *px,
+                            const double *py, const double *pz, const double *mass, const long long *steps,
+                            float *pos, float *vel, long long *frame_steps, int n, int n_sys, cudaStream_t st);
 cudaError_t launch_gather_systems(const SysInfo *sys, const int32_t *atom_sys, const int32_t *perm,
                                   const void *src, void *dst, int n, cudaStream_t st);
 

@@ -74,6 +74,26 @@ __global__ void energies_to_double(const long long *__restrict__ e, double *out,
   }
 }
 
+// Trajectory frame: float32 positions and velocities (p / m), (n, 3) each,
+// plus every system's step counter.
+__global__ void snapshot_frame(const double *__restrict__ x, const double *__restrict__ y,
+                               const double *__restrict__ z, const double *__restrict__ px,
+                               const double *__restrict__ py, const double *__restrict__ pz,
+                               const double *__restrict__ mass, const long long *__restrict__ steps,
+                               float *pos, float *vel, long long *frame_steps, int n, int n_sys) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double im = 1.0 / mass[i];
+    pos[3 * (size_t)i] = (float)x[i];
+    pos[3 * (size_t)i + 1] = (float)y[i];
+    pos[3 * (size_t)i + 2] = (float)z[i];
+    vel[3 * (size_t)i] = (float)(px[i] * im);
+    vel[3 * (size_t)i + 1] = (float)(py[i] * im);
+    vel[3 * (size_t)i + 2] = (float)(pz[i] * im);
+  }
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n_sys; s += gridDim.x * blockDim.x)
+    frame_steps[s] = steps[s];
+}
+
 static int grid_for(int n) {
   const int g = (n + 255) / 256;
   return g < 1 ? 1 : (g > 4096 ? 4096 : g);
@@ -110,6 +130,14 @@ cudaError_t launch_gather_systems(const SysInfo *sys, const int32_t *atom_sys, c
 cudaError_t launch_energies_to_double(const long long *e, double *out, int n_sys, cudaStream_t st) {
   if (n_sys <= 0) return cudaSuccess;
   energies_to_double<<<grid_for(n_sys), 256, 0, st>>>(e, out, n_sys);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_snapshot(const double *x, const double *y, const double *z, const double *px,
+                            const double *py, const double *pz, const double *mass, const long long *steps,
+                            float *pos, float *vel, long long *frame_steps, int n, int n_sys, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  snapshot_frame<<<grid_for(n), 256, 0, st>>>(x, y, z, px, py, pz, mass, steps, pos, vel, frame_steps, n, n_sys);
   return cudaGetLastError();
 }
 

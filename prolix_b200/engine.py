@@ -298,6 +298,23 @@ class Batch:
     self._check(self.lib.pb2_energy_forces_device(self.handle, positions_ptr or None, energies_ptr or None,
                                                   forces_ptr or None, stream))
 
+  # --------------------------------------------------------- trajectory ring
+  def traj_setup(self, capacity: int):
+    self._check(self.lib.pb2_traj_setup(self.handle, int(capacity)))
+    self.traj_capacity = int(capacity)
+
+  def traj_snapshot(self, slot: int, stream=None):
+    self._check(self.lib.pb2_traj_snapshot(self.handle, int(slot), stream))
+
+  def traj_fetch(self, first: int, count: int, stream=None):
+    """(positions (count, n_atoms, 3) float32, velocities, steps (count, n_systems))."""
+    pos = np.empty((count, self.n_atoms, 3), np.float32)
+    vel = np.empty((count, self.n_atoms, 3), np.float32)
+    steps = np.empty((count, self.n_systems), np.int64)
+    self._check(self.lib.pb2_traj_fetch(self.handle, int(first), int(count), pos.ctypes.data,
+                                        vel.ctypes.data, steps.ctypes.data, stream))
+    return pos, vel, steps
+
   def permute_systems(self, perm, stream=None):
     """Slot s takes x, p and F of slot perm[s] (replica exchange); keys,
     step counters, kT and dt stay with the slots."""
