@@ -85,44 +85,6 @@ struct TileConst {
   int src;
 };
 
-// GB polar pair force and dE/dB (both atoms), direct Coulomb and LJ for one
-// pair; g accumulates -dE/dr / r.
-template <bool CUT>
-__device__ __forceinline__ void force_pair(const PData &I, const PData &J, float dx, float dy, float dz,
-                                           float r2, bool excluded, bool is14, Acc &ti, Acc &tj,
-                                           const TileConst &K) {
-  float g = 0.f;
-  const float qq = I.q * J.q;
-  if (K.use_gb && (!CUT || K.gcut2 == 0.f || r2 < K.gcut2)) {
-    // E = P qq / f, f^2 = r^2 + B_i B_j e^(-r^2 / 4 B_i B_j); A = P qq / f^3
-    const float w = r2 * (I.iB * J.iB);  // r^2 log2(e) / (4 B_i B_j)
-    const float ex = exp2f(-w);
-    const float f2 = fmaf(I.B * J.B, ex, r2);
-    const float inv_f = rsqrtf(f2);
-    const float A = (K.pref * qq) * (inv_f * inv_f * inv_f);
-    g = A * fmaf(-0.5f, ex, 2.0f);  // -dE/dr / r
-    const float c = -(A * ex) * fmaf(w, kInvQuarterLog2e * 0.25f, 1.0f);  // dE/dB_i B_i = c B_j
-    ti.a3 = fmaf(c, J.B, ti.a3);
-    tj.a3 = fmaf(c, I.B, tj.a3);
-  }
-  if (!excluded && (K.use_lj || K.use_coul) && (!CUT || K.cut2 == 0.f || r2 < K.cut2)) {
-    const float inv_r = rsqrtf(r2);
-    const float inv_r2 = inv_r * inv_r;
-    float s = 0.f;  // (-dE/dr) r for Coulomb and LJ
-    if (K.use_coul) s = K.kcoul * qq * (is14 ? K.coul14 : 1.0f) * inv_r;
-    if (K.use_lj) {
-      const float sig = I.hs + J.hs;
-      const float sr2 = sig * sig * inv_r2;
-      const float s6 = sr2 * sr2 * sr2;
-      const float eps24 = I.se * J.se * (is14 ? K.lj14 : 1.0f);  // se = sqrt(24 eps)
-      s = fmaf(eps24 * s6, fmaf(2.0f, s6, -1.0f), s);
-    }
-    g = fmaf(s, inv_r2, g);
-  }
-  ti.a0 += g * dx; ti.a1 += g * dy; ti.a2 += g * dz;
-  tj.a0 -= g * dx; tj.a1 -= g * dy; tj.a2 -= g * dz;
-}
-
 // Force-pass rotation of everything but x, y, z and tj.a0.
 __device__ __forceinline__ void rotate_force_rest(PData &J, Acc &tj, int src, const TileConst &K) {
   J.q = shfl_next(J.q, src);
@@ -152,34 +114,93 @@ __device__ __forceinline__ void load_pdata(const PairArgs &a, int g, int pass, b
 }
 
 // ---------------------------------------------------------------- force pass
+//
+// The two pairs of a step run as packed f32x2 arithmetic (.x: i-block ib,
+// .y: ib + 1), branch-free: invalid pairs are evaluated at r^2 = kFarR2,
+// where every term underflows to zero; exclusions, 1-4 scales and cutoffs
+// become per-component factors.
 
-// One step of a force tile pair: lane's atom of each i-block against the j
-// atom currently in the lane.  V*: rotated validity masks (bit k = step k);
-// E*, S*: rotated exclusion / 1-4 masks.
+constexpr float kFarR2 = 1e30f;
+
+struct FData2 {  // the lane's two i atoms, packed, for the force pass
+  float2 x, y, z, q, hs, se, B, iB;
+};
+__device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 sel2(bool a, bool b, float va, float vb) {
+  return make_float2(a ? va : vb, b ? va : vb);
+}
+
+struct Acc2F {
+  float2 a0, a1, a2, a3;
+};
+
 template <bool CUT, bool FULL, bool EXCL>
-__device__ __forceinline__ void run_force_tile2(const PData &I0, const PData &I1, PData &J, Acc &t0,
-                                                Acc &t1, Acc &tj, uint32_t V0, uint32_t V1, uint32_t E0,
-                                                uint32_t E1, uint32_t S0, uint32_t S1,
-                                                const TileConst &K) {
+__device__ __forceinline__ void run_force_tile2(const FData2 &I, PData &J, Acc2F &ti, Acc &tj, uint32_t V0,
+                                                uint32_t V1, uint32_t E0, uint32_t E1, uint32_t S0,
+                                                uint32_t S1, const TileConst &K) {
   const int src = K.src;
+  // step k tests the sign bits of the bit-reversed masks shifted left k times
+  uint32_t R0 = __brev(V0), R1 = __brev(V1);
+  uint32_t X0 = __brev(E0), X1 = __brev(E1), Q0 = __brev(S0), Q1 = __brev(S1);
 #pragma unroll kUnroll
   for (int k = 0; k < 32; ++k) {
-    {
-      const bool ok = FULL ? true : ((V0 >> k) & 1u);
-      const float dx = I0.x - J.x, dy = I0.y - J.y, dz = I0.z - J.z;
-      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-      if (ok)
-        force_pair<CUT>(I0, J, dx, dy, dz, r2, EXCL ? ((E0 >> k) & 1u) != 0 : false,
-                        EXCL ? ((S0 >> k) & 1u) != 0 : false, t0, tj, K);
+    const float2 dx = __fadd2_rn(I.x, dup2(-J.x));
+    const float2 dy = __fadd2_rn(I.y, dup2(-J.y));
+    const float2 dz = __fadd2_rn(I.z, dup2(-J.z));
+    float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+    if (!FULL) {
+      r2 = make_float2((int32_t)R0 < 0 ? r2.x : kFarR2, (int32_t)R1 < 0 ? r2.y : kFarR2);
+      R0 <<= 1;
+      R1 <<= 1;
     }
-    {
-      const bool ok = FULL ? true : ((V1 >> k) & 1u);
-      const float dx = I1.x - J.x, dy = I1.y - J.y, dz = I1.z - J.z;
-      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-      if (ok)
-        force_pair<CUT>(I1, J, dx, dy, dz, r2, EXCL ? ((E1 >> k) & 1u) != 0 : false,
-                        EXCL ? ((S1 >> k) & 1u) != 0 : false, t1, tj, K);
+    const float2 qq = __fmul2_rn(I.q, dup2(J.q));
+    float2 g = make_float2(0.f, 0.f);
+    if (K.use_gb) {
+      // E = P qq / f, f^2 = r^2 + B_i B_j e^(-r^2 / 4 B_i B_j); A = P qq / f^3
+      const float2 w = __fmul2_rn(r2, __fmul2_rn(I.iB, dup2(J.iB)));  // r^2 log2(e) / (4 B_i B_j)
+      const float2 ex = make_float2(exp2f(-w.x), exp2f(-w.y));
+      const float2 f2 = __ffma2_rn(__fmul2_rn(I.B, dup2(J.B)), ex, r2);
+      const float2 inv_f = make_float2(rsqrtf(f2.x), rsqrtf(f2.y));
+      float2 A = __fmul2_rn(__fmul2_rn(dup2(K.pref), qq), __fmul2_rn(__fmul2_rn(inv_f, inv_f), inv_f));
+      if (CUT && K.gcut2 != 0.f) A = __fmul2_rn(A, sel2(r2.x < K.gcut2, r2.y < K.gcut2, 1.f, 0.f));
+      g = __fmul2_rn(A, __ffma2_rn(dup2(-0.5f), ex, dup2(2.0f)));  // -dE/dr / r
+      const float2 c = __fmul2_rn(__fmul2_rn(A, ex),
+                                  __ffma2_rn(w, dup2(-kInvQuarterLog2e * 0.25f), dup2(-1.0f)));
+      ti.a3 = __ffma2_rn(c, dup2(J.B), ti.a3);  // dE/dB_i B_i = c B_j
+      tj.a3 = fmaf(c.x, I.B.x, fmaf(c.y, I.B.y, tj.a3));
     }
+    if (K.use_lj || K.use_coul) {
+      const float2 inv_r = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+      const float2 inv_r2 = __fmul2_rn(inv_r, inv_r);
+      float2 sc_c = dup2(1.f), sc_l = dup2(1.f);  // exclusion and 1-4 factors
+      if (EXCL) {
+        const bool x0 = (int32_t)X0 < 0, x1 = (int32_t)X1 < 0, q0 = (int32_t)Q0 < 0, q1 = (int32_t)Q1 < 0;
+        sc_c = make_float2(x0 ? 0.f : (q0 ? K.coul14 : 1.f), x1 ? 0.f : (q1 ? K.coul14 : 1.f));
+        sc_l = make_float2(x0 ? 0.f : (q0 ? K.lj14 : 1.f), x1 ? 0.f : (q1 ? K.lj14 : 1.f));
+        X0 <<= 1; X1 <<= 1; Q0 <<= 1; Q1 <<= 1;
+      }
+      float2 s = make_float2(0.f, 0.f);  // (-dE/dr) r for Coulomb and LJ
+      if (K.use_coul) {
+        s = __fmul2_rn(__fmul2_rn(dup2(K.kcoul), qq), inv_r);
+        if (EXCL) s = __fmul2_rn(s, sc_c);
+      }
+      if (K.use_lj) {
+        const float2 sig = __fadd2_rn(I.hs, dup2(J.hs));
+        const float2 sr2 = __fmul2_rn(__fmul2_rn(sig, sig), inv_r2);
+        const float2 s6 = __fmul2_rn(__fmul2_rn(sr2, sr2), sr2);
+        float2 eps24 = __fmul2_rn(I.se, dup2(J.se));  // se = sqrt(24 eps)
+        if (EXCL) eps24 = __fmul2_rn(eps24, sc_l);
+        s = __ffma2_rn(__fmul2_rn(eps24, s6), __ffma2_rn(dup2(2.0f), s6, dup2(-1.0f)), s);
+      }
+      if (CUT && K.cut2 != 0.f) s = __fmul2_rn(s, sel2(r2.x < K.cut2, r2.y < K.cut2, 1.f, 0.f));
+      g = __ffma2_rn(s, inv_r2, g);
+    }
+    ti.a0 = __ffma2_rn(g, dx, ti.a0);
+    ti.a1 = __ffma2_rn(g, dy, ti.a1);
+    ti.a2 = __ffma2_rn(g, dz, ti.a2);
+    tj.a0 = fmaf(-g.x, dx.x, fmaf(-g.y, dx.y, tj.a0));
+    tj.a1 = fmaf(-g.x, dy.x, fmaf(-g.y, dy.y, tj.a1));
+    tj.a2 = fmaf(-g.x, dz.x, fmaf(-g.y, dz.y, tj.a2));
     J.x = shfl_next(J.x, src); J.y = shfl_next(J.y, src); J.z = shfl_next(J.z, src);
     tj.a0 = shfl_next(tj.a0, src);
     rotate_force_rest(J, tj, src, K);
@@ -198,7 +219,6 @@ __device__ __forceinline__ void run_force_tile2(const PData &I0, const PData &I1
 struct PData2 {  // the lane's two i atoms, packed
   float2 x, y, z, sr, ro, t2, s2, s3, dedi;
 };
-__device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
 __device__ __forceinline__ PData2 pack2(const PData &a, const PData &b) {
   PData2 p;
   p.x = make_float2(a.x, b.x); p.y = make_float2(a.y, b.y); p.z = make_float2(a.z, b.z);
@@ -230,7 +250,6 @@ struct Acc2 {
 // are evaluated at r^2 = kFarR2: their radial factor underflows to exactly
 // zero (1/r^4 = 1e-60), so they are summed without a select and never reach
 // the closed form.
-constexpr float kFarR2 = 1e30f;
 
 // Both pairs' geometry and both directions' integral terms.  The series path
 // keeps the radial factor apart: I = s^3 S(s^2/r^2) / r^4 and
@@ -460,8 +479,15 @@ __global__ void __launch_bounds__(256, PASS == PASS_BORN ? PB2_MINB_BORN : (PASS
           const ExclRow r = a.excl_rows[roff + lane];
           E1 = rotr32(r.excl, lane); S1 = rotr32(r.s14, lane);
         }
-        if (hit || !full) run_force_tile2<CUT, false, true>(I0, I1, J, t0, t1, tj, V0, V1, E0, E1, S0, S1, K);
-        else run_force_tile2<CUT, true, false>(I0, I1, J, t0, t1, tj, V0, V1, E0, E1, S0, S1, K);
+        const FData2 IF = {make_float2(I0.x, I1.x), make_float2(I0.y, I1.y), make_float2(I0.z, I1.z),
+                           make_float2(I0.q, I1.q), make_float2(I0.hs, I1.hs), make_float2(I0.se, I1.se),
+                           make_float2(I0.B, I1.B), make_float2(I0.iB, I1.iB)};
+        Acc2F tf = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+        if (hit) run_force_tile2<CUT, false, true>(IF, J, tf, tj, V0, V1, E0, E1, S0, S1, K);
+        else if (!full) run_force_tile2<CUT, false, false>(IF, J, tf, tj, V0, V1, E0, E1, S0, S1, K);
+        else run_force_tile2<CUT, true, false>(IF, J, tf, tj, V0, V1, E0, E1, S0, S1, K);
+        t0.a0 = tf.a0.x; t0.a1 = tf.a1.x; t0.a2 = tf.a2.x; t0.a3 = tf.a3.x;
+        t1.a0 = tf.a0.y; t1.a1 = tf.a1.y; t1.a2 = tf.a2.y; t1.a3 = tf.a3.y;
       } else {
         // series length by the tiles' smallest separation
         Acc2 ti = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
