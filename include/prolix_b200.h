@@ -215,8 +215,11 @@ int pb2_set_full_state(pb2_batch *batch, const double *x, const double *p, const
  *   pb2_min_sd   : restrained steepest descent, dr = F dt capped at max_dx
  *                  per atom (batched_simulate.py:748-791);
  *   pb2_min_fire : FIRE from zero momentum (jax_md fire_descent, called at
- *                  :818-878) with a per-atom displacement cap max_disp; the
- *                  state ends at the positions of the lowest force RMS seen;
+ *                  :818-878) with a per-atom displacement cap max_disp
+ *                  (0: none) and, for the first half kick, a per-atom force
+ *                  cap force_cap (0: none; prolix simulate.py:613-638);
+ *                  with PB2_FIRE_KEEP_BEST in flags the state ends at the
+ *                  positions of the lowest force RMS seen, else at the last;
  * with restraint E = k/2 sum |r - r0|^2 on kind 0 all atoms, 1 heavy atoms,
  * 2 backbone atoms.  A system that turns non-finite returns to r0 and gets
  * PB2_STATUS_NONFINITE.  FIRE uses the momentum arrays: call
@@ -226,8 +229,9 @@ int pb2_set_full_state(pb2_batch *batch, const double *x, const double *p, const
 int pb2_min_setup(pb2_batch *batch, const uint8_t *heavy, const uint8_t *backbone);
 int pb2_min_sd(pb2_batch *batch, int32_t n_steps, double k, int32_t kind, double dt, double max_dx,
                void *stream);
+#define PB2_FIRE_KEEP_BEST 1
 int pb2_min_fire(pb2_batch *batch, int32_t n_steps, double k, int32_t kind, double dt_start,
-                 double dt_max, double max_disp, void *stream);
+                 double dt_max, double max_disp, double force_cap, int32_t flags, void *stream);
 int pb2_min_rms(pb2_batch *batch, double *rms, void *stream);
 
 /* Replica exchange (replaces the state shuffle of prolix

@@ -49,8 +49,11 @@ def steepest_descent(system, r_start, r0, sel, n_steps, k, dt, max_dx, force_fn=
   return r
 
 
-def fire(system, r_start, r0, sel, masses, n_steps, k, dt_start, dt_max, max_disp, force_fn=None):
-  """Returns the lowest-RMS positions of the stage (and the final state)."""
+def fire(system, r_start, r0, sel, masses, n_steps, k, dt_start, dt_max, max_disp, force_fn=None,
+         force_cap=0.0):
+  """Returns the lowest-RMS positions of the stage and the final positions.
+  max_disp / force_cap 0 disable the caps; the force cap scales each atom's
+  state force for the first half kick (prolix simulate.py:613-621)."""
   m = np.asarray(masses, np.float64)[:, None]
   r = np.array(r_start, dtype=np.float64)
   p = np.zeros_like(r)
@@ -62,7 +65,10 @@ def fire(system, r_start, r0, sel, masses, n_steps, k, dt_start, dt_max, max_dis
     if rms < best_rms:
       best_r, best_rms = r.copy(), rms
     r_before = r
-    p = p + 0.5 * dt * f
+    fk = f
+    if force_cap > 0:
+      fk = f * np.minimum(1.0, force_cap / (np.linalg.norm(f, axis=1, keepdims=True) + 1e-8))
+    p = p + 0.5 * dt * fk
     r = r + dt * p / m
     f = total_force(system, r, r0, k, sel, force_fn)
     p = p + 0.5 * dt * f
@@ -79,7 +85,7 @@ def fire(system, r_start, r0, sel, masses, n_steps, k, dt_start, dt_max, max_dis
       alpha = ALPHA_START
       p = np.zeros_like(p)
     d = r - r_before
-    sc = np.minimum(1.0, max_disp / np.sqrt(np.sum(d * d, axis=1, keepdims=True) + 1e-30))
+    sc = np.minimum(1.0, max_disp / np.sqrt(np.sum(d * d, axis=1, keepdims=True) + 1e-30)) if max_disp > 0 else 1.0
     r = r_before + d * sc
     p = p * sc
   return best_r, r

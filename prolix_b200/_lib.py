@@ -89,7 +89,8 @@ SIGNATURES = [
     ("pb2_min_sd", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_double, ctypes.c_int32,
                                   ctypes.c_double, ctypes.c_double, ctypes.c_void_p]),
     ("pb2_min_fire", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_double, ctypes.c_int32,
-                                    ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_void_p]),
+                                    ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_int32, ctypes.c_void_p]),
     ("pb2_min_rms", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("pb2_permute_systems", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("pb2_energy_forces_device", ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_void_p] * 4),

@@ -1054,6 +1054,7 @@ extern "C" int pb2_min_sd(pb2_batch *b, int32_t n_steps, double k, int32_t kind,
   if (!(dt > 0.0) || !(max_dx > 0.0)) return fail(b->ctx, PB2_EINVAL, "dt and max_dx must be > 0");
   b->m_par_host[kMinSdDt] = dt;
   b->m_par_host[kMinMaxDx] = max_dx;
+  b->m_par_host[kMinForceCap] = 0.0;
   cudaStream_t st = (cudaStream_t)stream;
   int rc = min_begin(b, n_steps, k, kind, st);
   if (rc) return rc;
@@ -1065,20 +1066,21 @@ extern "C" int pb2_min_sd(pb2_batch *b, int32_t n_steps, double k, int32_t kind,
 }
 
 extern "C" int pb2_min_fire(pb2_batch *b, int32_t n_steps, double k, int32_t kind, double dt_start,
-                            double dt_max, double max_disp, void *stream) {
+                            double dt_max, double max_disp, double force_cap, int32_t flags, void *stream) {
   if (!b) return PB2_EINVAL;
-  if (!(dt_start > 0.0) || !(dt_max > 0.0) || !(max_disp > 0.0))
-    return fail(b->ctx, PB2_EINVAL, "dt_start, dt_max and max_disp must be > 0");
+  if (!(dt_start > 0.0) || !(dt_max > 0.0) || !(max_disp >= 0.0) || !(force_cap >= 0.0))
+    return fail(b->ctx, PB2_EINVAL, "dt_start, dt_max must be > 0; max_disp, force_cap >= 0");
   b->m_par_host[kMinDtStart] = dt_start;
   b->m_par_host[kMinDtMax] = dt_max;
   b->m_par_host[kMinMaxDisp] = max_disp;
+  b->m_par_host[kMinForceCap] = force_cap;
   cudaStream_t st = (cudaStream_t)stream;
   int rc = min_begin(b, n_steps, k, kind, st);
   if (rc) return rc;
   const MinArgs ma = min_args(b);
   CUDA_TRY(b->ctx, launch_min(kMinOpFireInit, ma, nullptr, st));
   if ((rc = min_run(b, 1, n_steps, st))) return rc;
-  CUDA_TRY(b->ctx, launch_min(kMinOpTakeBest, ma, nullptr, st));
+  if (flags & PB2_FIRE_KEEP_BEST) CUDA_TRY(b->ctx, launch_min(kMinOpTakeBest, ma, nullptr, st));
   CUDA_TRY(b->ctx, launch_min(kMinOpRollback, ma, nullptr, st));
   b->forces_valid = false;
   CUDA_TRY(b->ctx, cudaStreamSynchronize(st));

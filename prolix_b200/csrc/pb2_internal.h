@@ -112,7 +112,7 @@ struct pb2_batch {
   int32_t *m_npos = nullptr;
   uint8_t *m_sel = nullptr;
   std::map<std::pair<int, int>, cudaGraphExec_t> min_graphs;  // (mode, chunk)
-  double m_par_host[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double m_par_host[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // kMinNPar stage parameters
   // neighbour list (allocated on first build)
   Dev nl;
   bool nl_built = false;

@@ -119,7 +119,7 @@ struct IntArgs {
 };
 // Minimiser (pb2_minimize.cu).  Stage parameters live in device memory
 // (par[kMin*]) so that captured graphs serve every stage.
-enum { kMinK = 0, kMinKind, kMinSdDt, kMinMaxDx, kMinDtStart, kMinDtMax, kMinMaxDisp, kMinNPar };
+enum { kMinK = 0, kMinKind, kMinSdDt, kMinMaxDx, kMinDtStart, kMinDtMax, kMinMaxDisp, kMinForceCap, kMinNPar };
 enum { kMinOpSd = 0, kMinOpRollback, kMinOpFireInit, kMinOpFireBegin, kMinOpFireDrift, kMinOpFireMix,
        kMinOpTakeBest, kMinOpRms };
 // FIRE constants (Bitzek et al. 2006; jax_md fire_descent defaults)

@@ -175,12 +175,20 @@ __global__ void min_fire_begin_kernel(const MinArgs a) {
   }
 }
 
-// First half kick and drift; remembers the positions for the displacement cap.
+// First half kick and drift; remembers the positions for the displacement
+// cap.  With a force cap (prolix simulate.py:613-621) the state force of
+// each atom is scaled to at most that norm for this kick.
 __global__ void min_fire_drift_kernel(const MinArgs a) {
   const size_t N = a.n_total;
+  const double cap = a.par[kMinForceCap];
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_total; i += gridDim.x * blockDim.x) {
     const double dt = a.sys_dt[a.atom_sys[i]], h = 0.5 * dt, m = a.mass[i];
-    const double px = a.px[i] + h * a.ft[i], py = a.py[i] + h * a.ft[N + i], pz = a.pz[i] + h * a.ft[2 * N + i];
+    double f[3] = {a.ft[i], a.ft[N + i], a.ft[2 * N + i]};
+    if (cap > 0.0) {
+      const double sc = fmin(1.0, cap / (sqrt(f[0] * f[0] + f[1] * f[1] + f[2] * f[2]) + 1e-8));
+      f[0] *= sc; f[1] *= sc; f[2] *= sc;
+    }
+    const double px = a.px[i] + h * f[0], py = a.py[i] + h * f[1], pz = a.pz[i] + h * f[2];
     a.px[i] = px; a.py[i] = py; a.pz[i] = pz;
     a.xb[i] = a.x[i]; a.xb[N + i] = a.y[i]; a.xb[2 * N + i] = a.z[i];
     a.x[i] += dt * px / m;
@@ -241,7 +249,7 @@ __global__ void min_fire_mix_kernel(const MinArgs a) {
       for (int c = 0; c < 3; ++c) p[c] = zero_p ? 0.0 : p[c] + (mix_f * f[c] - mix_p * p[c]);
       const double dx = a.x[i] - a.xb[i], dy = a.y[i] - a.xb[N + i], dz = a.z[i] - a.xb[2 * N + i];
       const double dm = sqrt(dx * dx + dy * dy + dz * dz + 1e-30);
-      const double sc = fmin(1.0, max_disp / dm);
+      const double sc = max_disp > 0.0 ? fmin(1.0, max_disp / dm) : 1.0;  // 0: no cap
       a.x[i] = a.xb[i] + dx * sc;
       a.y[i] = a.xb[N + i] + dy * sc;
       a.z[i] = a.xb[2 * N + i] + dz * sc;

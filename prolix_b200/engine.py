@@ -340,9 +340,13 @@ class Batch:
     self._check(self.lib.pb2_min_sd(self.handle, int(n_steps), float(k), self.MIN_KIND[kind],
                                     float(dt), float(max_dx), stream))
 
-  def min_fire(self, n_steps, k=0.0, kind="all", dt_start=1e-4, dt_max=1e-3, max_disp=0.1, stream=None):
+  def min_fire(self, n_steps, k=0.0, kind="all", dt_start=1e-4, dt_max=1e-3, max_disp=0.1, force_cap=0.0,
+               keep_best=True, stream=None):
+    """One FIRE stage; max_disp / force_cap 0 disable the caps; keep_best
+    ends at the lowest-RMS positions (batched_minimize), else at the last."""
     self._check(self.lib.pb2_min_fire(self.handle, int(n_steps), float(k), self.MIN_KIND[kind],
-                                      float(dt_start), float(dt_max), float(max_disp), stream))
+                                      float(dt_start), float(dt_max), float(max_disp), float(force_cap),
+                                      1 if keep_best else 0, stream))
 
   def min_rms(self, stream=None):
     """Per-system RMS over atoms of the unrestrained force, kcal/mol/A."""

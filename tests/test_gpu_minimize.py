@@ -60,3 +60,31 @@ def test_batched_minimize_lowers_energy_and_force():
   for s, p in zip(systems, pos):
     assert np.isfinite(p).all()
     assert oenergy.total_energy(s, p) < oenergy.total_energy(s, s["positions"])
+
+
+def test_fire_force_cap_final_state_matches_oracle():
+  # prolix.simulate's stages: per-atom force cap on the first half kick, no
+  # displacement cap, the stage ends at its final positions
+  s = _sys(166, 14)
+  with engine.Batch([s]) as b:
+    b.min_setup()
+    b.min_fire(40, dt_start=1e-3, dt_max=1e-2, max_disp=0.0, force_cap=10.0, keep_best=False)
+    got = b.get_state(fields=("position",))["position"]
+  _, final = om.fire(s, s["positions"], s["positions"], np.zeros(166), s["masses"], 40, 0.0, 1e-3, 1e-2,
+                     0.0, force_cap=10.0)
+  assert np.max(np.abs(got - final)) < 1e-5
+
+
+def test_production_run_simulation(tmp_path):
+  from prolix_b200 import production, trajectory
+  s = _sys(166, 15)
+  spec = production.SimulationSpec(total_time_ns=0.002, save_interval_ns=0.0005, accumulate_steps=3,
+                                   save_path=str(tmp_path / "prod.pb2traj"),
+                                   physics=production.PhysicsSpec(dt=2.0))
+  stages = ((10.0, 100, True), (100.0, 100, True), (None, 200, False))
+  final = production.run_simulation(s, s["positions"], spec, key=(0, 9), fire_stages=stages)
+  frames = list(trajectory.read_trajectory(spec.save_path))
+  assert [f["step"] for f in frames] == [250, 500, 750, 1000]
+  assert all(np.isfinite(f["potential_energy"]) and f["kinetic_energy"] > 0 for f in frames)
+  assert final.step == 1000 and np.isfinite(final.positions).all()
+  np.testing.assert_array_equal(frames[-1]["positions"], final.positions.astype(np.float32))
