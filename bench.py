@@ -333,6 +333,28 @@ def single_system_runs(stream, hbm_peak):
   return out
 
 
+def split_run(systems, stream, born_cutoff=10.0, steps=100):
+  """The NL-Born + dense-GB option on the timing batch: descreening and its
+  chain rule within ``born_cutoff``, GB pair terms, Coulomb and LJ over all
+  pairs.  Device atom-steps/s (no L2 flush; 50-step graphs)."""
+  import torch
+  from prolix_b200 import engine
+  with engine.Batch(systems, born_cutoff=born_cutoff) as b:
+    b.langevin_init()
+    b.langevin_run(50, stream)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    b.langevin_run(steps, stream)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    n = b.n_atoms
+  return {"born_cutoff": born_cutoff, "ms_per_step": ms / steps,
+          "atom_steps_per_s": n * steps / (ms * 1e-3)}
+
+
 def minimize_run(systems, stream):
   """Throughput of the batched minimiser on the timing batch: 100 restrained
   steepest-descent steps and 4 FIRE stages of 50 iterations (the
@@ -499,7 +521,8 @@ def main():
     extra = None
     if not args.no_extra:
       extra = {"single_system": single_system_runs(stream, hbm_peak),
-               "minimize": minimize_run(systems, stream)}
+               "minimize": minimize_run(systems, stream),
+               "nl_born_dense_gb": split_run(systems, stream)}
       if not args.no_serving:
         extra["serving_sweep"] = serving_sweep(args)
     if not args.no_cpu:

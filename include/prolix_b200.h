@@ -135,6 +135,9 @@ typedef struct pb2_run_params {
                            prolix's make_energy_fn keeps GB all-pairs while LJ/Coulomb
                            use the cutoff (system.py:196-216); with a GB cutoff the
                            neighbour-list clamps of generalized_born.py:300-337 apply */
+  double born_cutoff;   /* A; > 0: descreening sums and their chain rule only (the NL-Born +
+                           dense-GB split, generalized_born.py:706-817); the GB pair terms keep
+                           gb_cutoff.  <= 0: the descreening uses gb_cutoff too */
 } pb2_run_params;
 
 typedef struct pb2_ctx pb2_ctx;

@@ -151,12 +151,14 @@ def excl_dense_rows(pairs, s_vdw, s_elec, a, b, n):
 
 def nonbonded(system, pos, cutoff=0.0, eps_in=1.0, eps_out=78.5, k_gb=K_COULOMB,
               k_coul=K_COULOMB, lj14=topology.LJ14_SCALE, coul14=topology.COUL14_SCALE,
-              ace=True, gb_cutoff=None):
+              ace=True, gb_cutoff=None, born_cutoff=None):
   """Energies (dict) and forces (N, 3) of GB polar, ACE, Coulomb and LJ.
 
   ``cutoff`` applies to Coulomb and LJ; ``gb_cutoff`` to the GB pair terms
   and the descreening sums (None: the same as ``cutoff``; 0: all pairs, as
-  prolix's make_energy_fn does for GB, system.py:196-216).  ``ace=False``
+  prolix's make_energy_fn does for GB, system.py:196-216).  ``born_cutoff``
+  > 0 applies to the descreening sums and their chain rule alone (the
+  NL-Born + dense-GB split, generalized_born.py:706-817).  ``ace=False``
   drops the nonpolar term (``compute_gb_energy`` alone).
   """
   pos = np.asarray(pos, dtype=np.float64)
@@ -169,10 +171,12 @@ def nonbonded(system, pos, cutoff=0.0, eps_in=1.0, eps_out=78.5, k_gb=K_COULOMB,
   pairs, s_v, s_e = topology.pair_scales(system.get("bonds", np.zeros((0, 2))), n, lj14, coul14)
   gbc = cutoff if gb_cutoff is None else gb_cutoff
   nl = gbc > 0
-  born, isum, dbdi = born_radii(pos, radii, sr, gbc)
-  rad = np.maximum(radii, 1e-6) if nl else radii
+  bc = born_cutoff if born_cutoff is not None and born_cutoff > 0 else gbc
+  nlb = bc > 0
+  born, isum, dbdi = born_radii(pos, radii, sr, bc)
+  rad = np.maximum(radii, 1e-6) if nlb else radii
   rho_off = rad - DIELECTRIC_OFFSET
-  if nl:
+  if nlb:
     rho_off = np.maximum(rho_off, 1e-4)
   pref = -0.5 * k_gb * (1.0 / eps_in - 1.0 / eps_out)
 
@@ -230,8 +234,8 @@ def nonbonded(system, pos, cutoff=0.0, eps_in=1.0, eps_out=78.5, k_gb=K_COULOMB,
     dx, r2, selfm = _block(pos, a, b)
     m = ~selfm
     rg = np.sqrt(r2 + SAFE_EPS)
-    if nl:
-      m &= rg < gbc
+    if nlb:
+      m &= rg < bc
     d_ij = pair_integral_dr(rg, rho_off[a:b, None], sr[None, :])
     d_ji = pair_integral_dr(rg, rho_off[None, :], sr[a:b, None])
     g = np.where(m, (dedi[a:b, None] * d_ij + dedi[None, :] * d_ji) / rg, 0.0)

@@ -62,6 +62,7 @@ class RunParams(ctypes.Structure):
       ("graph_chunk", ctypes.c_int32),
       ("partitionable_keys", ctypes.c_int32),
       ("gb_cutoff", ctypes.c_double),
+      ("born_cutoff", ctypes.c_double),
   ]
 
 

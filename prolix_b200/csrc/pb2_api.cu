@@ -238,6 +238,8 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   const bool cutoff_mode = params->cutoff > 0.0;
   const double gb_cut = params->gb_cutoff < 0.0 ? (cutoff_mode ? params->cutoff : 0.0) : params->gb_cutoff;
   const bool gb_cut_mode = gb_cut > 0.0;
+  const double born_cut = params->born_cutoff > 0.0 ? params->born_cutoff : gb_cut;
+  const bool born_mode = born_cut > 0.0;  // Born radii from a cutoff: its clamps apply
 
   // --- per-atom host arrays
   int64_t total = 0;
@@ -280,7 +282,8 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
     S.coul14 = (float)d.coul14_scale;
     S.cutoff2 = cutoff_mode ? (float)(params->cutoff * params->cutoff) : 0.f;
     S.gb_cutoff2 = gb_cut_mode ? (float)(gb_cut * gb_cut) : 0.f;
-    S.clamp = gb_cut_mode ? 1 : 0;
+    S.born_cut2 = born_mode ? (float)(born_cut * born_cut) : 0.f;
+    S.clamp = born_mode ? 1 : 0;
     S.dt = d.dt;
     S.half_dt = 0.5 * d.dt;
     S.c1 = std::exp(-d.gamma * d.dt);
@@ -314,7 +317,7 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
       hposq[g] = make_float4((float)(hx[g] - S.ox), (float)(hy[g] - S.oy), (float)(hz[g] - S.oz),
                              (float)d.charges[i]);
       double ro = d.radii[i] - kDielOffset;
-      if (gb_cut_mode) ro = std::max(std::max(d.radii[i], 1e-6) - kDielOffset, 1e-4);
+      if (born_mode) ro = std::max(std::max(d.radii[i], 1e-6) - kDielOffset, 1e-4);
       hhs[g] = 0.5 * std::max(d.sigmas[i], 1e-6);
       hse[g] = std::sqrt(std::max(d.epsilons[i], 0.0));
       hro[g] = ro;
@@ -433,7 +436,7 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   b->sched = D.alloc<int32_t>(8);
   b->blk_sys = D.alloc<int32_t>(blocks_total);
   b->n_blocks = blocks_total;
-  b->cut = cutoff_mode || gb_cut_mode;
+  b->cut = cutoff_mode || gb_cut_mode || born_mode;
   b->q64 = D.alloc<double>(N);
   b->hs64 = D.alloc<double>(N);
   b->se64 = D.alloc<double>(N);

@@ -48,7 +48,7 @@ __global__ void __launch_bounds__(256) energy64_kernel(const Energy64Args a) {
     const TileItem item = a.items[it];
     const SysInfo &S = a.sys[item.sys];
     const int n = S.n, off = S.off;
-    const double cut2 = (double)S.cutoff2, gcut2 = (double)S.gb_cutoff2;
+    const double cut2 = (double)S.cutoff2, gcut2 = (double)S.gb_cutoff2, bcut2 = (double)S.born_cut2;
     const double pref = S.pref_d, kcoul = S.kcoul_d;
     const int il = item.iblk * 32 + lane;
     const bool ivalid = il < n;
@@ -86,7 +86,7 @@ __global__ void __launch_bounds__(256) energy64_kernel(const Energy64Args a) {
         bool ok = ivalid && (jl0 + jc < n) && (!diag || jc > lane);
         const double dx = xi - xj, dy = yi - yj, dz = zi - zj;
         const double r2 = dx * dx + dy * dy + dz * dz;
-        if (PASS == 0 && gcut2 > 0.0) ok = ok && (r2 < gcut2);
+        if (PASS == 0 && bcut2 > 0.0) ok = ok && (r2 < bcut2);
         if (ok) {
           if (PASS == 0) {
             const double r = sqrt(r2 + 1e-12);

@@ -80,7 +80,7 @@ struct Acc {
   float a0, a1, a2, a3;
 };
 struct TileConst {
-  float cut2, gcut2, pref, kcoul, lj14, coul14;
+  float cut2, gcut2, bcut2, pref, kcoul, lj14, coul14;  // bcut2: descreening / chain rule
   bool use_gb, use_lj, use_coul;
   int src;
 };
@@ -269,8 +269,8 @@ __device__ __forceinline__ void bc_series2(const PData2 &I, const PData &J, bool
   P.dz = __fadd2_rn(I.z, dup2(-J.z));
   const float2 r2 = __ffma2_rn(P.dx, P.dx, __ffma2_rn(P.dy, P.dy, __fmul2_rn(P.dz, P.dz)));
   if (CUT) {
-    ok0 = ok0 && (K.gcut2 == 0.f || r2.x < K.gcut2);
-    ok1 = ok1 && (K.gcut2 == 0.f || r2.y < K.gcut2);
+    ok0 = ok0 && (K.bcut2 == 0.f || r2.x < K.bcut2);
+    ok1 = ok1 && (K.bcut2 == 0.f || r2.y < K.bcut2);
   }
   P.ok0 = ok0;
   P.ok1 = ok1;
@@ -410,7 +410,7 @@ __global__ void __launch_bounds__(256, PASS == PASS_BORN ? PB2_MINB_BORN : (PASS
     const TileItem item = a.items[it];
     const SysInfo &S = a.sys[item.sys];
     const int n = S.n, off = S.off;
-    K.cut2 = S.cutoff2; K.gcut2 = S.gb_cutoff2;
+    K.cut2 = S.cutoff2; K.gcut2 = S.gb_cutoff2; K.bcut2 = S.born_cut2;
     K.pref = S.pref; K.kcoul = S.kcoul; K.lj14 = S.lj14; K.coul14 = S.coul14;
     const int ib0 = item.iblk, ib1 = item.iblk + 1;
     const bool has1 = ib1 < S.nblk;
@@ -422,7 +422,7 @@ __global__ void __launch_bounds__(256, PASS == PASS_BORN ? PB2_MINB_BORN : (PASS
     float reach2 = 0.f;
     if (CUT) {
       if (PASS == PASS_FORCE) reach2 = (K.gcut2 == 0.f || K.cut2 == 0.f) ? 0.f : fmaxf(K.gcut2, K.cut2);
-      else reach2 = K.gcut2;
+      else reach2 = K.bcut2;
     }
     PData I0, I1;
     load_pdata(a, ig0, PASS, K.use_gb, S.ro_max, I0);

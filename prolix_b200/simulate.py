@@ -124,7 +124,7 @@ def nvt_langevin(energy_or_force_fn, shift_fn, dt: float, kT: float, gamma: floa
     n = efn.n_atoms
     m = np.broadcast_to(np.asarray(mass, dtype=np.float64).reshape(-1), (n,)).copy()
     sysd = dict(efn.system, positions=np.asarray(R, dtype=np.float64).reshape(n, 3), masses=m)
-    batch = engine.Batch([sysd], cutoff=efn.cutoff, gb_cutoff=efn.gb_cutoff,
+    batch = engine.Batch([sysd], cutoff=efn.cutoff, gb_cutoff=efn.gb_cutoff, born_cutoff=efn.born_cutoff,
                          key=np.asarray(key, dtype=np.uint32).reshape(2), dt=float(dt),
                          kT=_kT, gamma=float(gamma),
                          eps_in=efn.batch.prepared[0]["scal"]["eps_in"],

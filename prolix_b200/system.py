@@ -67,11 +67,13 @@ class EnergyFn:
   """Callable energy function backed by a one-system device batch."""
 
   def __init__(self, system: dict, cutoff: float, *, eps_in=1.0, eps_out=78.5,
-               terms=USE_ALL, device=0, gb_cutoff=0.0, **defaults):
+               terms=USE_ALL, device=0, gb_cutoff=0.0, born_cutoff=0.0, **defaults):
     self.system = system
     self.cutoff = float(cutoff)
     self.gb_cutoff = float(gb_cutoff)
+    self.born_cutoff = float(born_cutoff)
     self._batch = engine.Batch([system], cutoff=self.cutoff, gb_cutoff=self.gb_cutoff,
+                               born_cutoff=self.born_cutoff,
                                terms=terms, device=device, eps_in=eps_in, eps_out=eps_out,
                                **defaults)
     self._last = None
@@ -145,6 +147,7 @@ def make_energy_fn(displacement_fn, system, cutoff_distance: float = 9.0,
   eps_out = float(kwargs.get("solvent_dielectric", 78.5))
   fn = EnergyFn(sysd, cutoff if cutoff > 0 else 0.0, eps_in=eps_in, eps_out=eps_out,
                 gb_cutoff=float(kwargs.get("gb_cutoff", 0.0)),
+                born_cutoff=float(kwargs.get("born_cutoff", 0.0)),
                 device=int(kwargs.get("device", 0)))
   if not return_decomposed:
     return fn

@@ -284,3 +284,25 @@ def test_full_state_restore_is_bit_exact_without_force_evaluation():
     out = b2.get_state()
   for f in ("position", "momentum", "force", "key"):
     np.testing.assert_array_equal(out[f], ref[f])
+
+
+def test_nl_born_dense_gb_split():
+  # descreening and chain rule within 10 A, GB pair terms over all pairs
+  # (generalized_born.py:706-817); against the FP64 restatement
+  from oracle import bonded as obonded
+  from oracle import gbsa as ogbsa
+  s = synth.make_chain(600, 61, compact=True)
+  with engine.Batch([s], cutoff=0.0, gb_cutoff=0.0, born_cutoff=10.0) as b:
+    e, f = b.energy_forces()
+    born = b.born_radii()
+  en, fn, ex = ogbsa.nonbonded(s, s["positions"], 0.0, gb_cutoff=0.0, born_cutoff=10.0)
+  _, fb = obonded.bonded_all(s, s["positions"])
+  f_ref = fn + fb
+  assert np.linalg.norm(f - f_ref) / np.linalg.norm(f_ref) < 1e-5
+  np.testing.assert_allclose(born, ex["born_radii"], rtol=2e-6)
+  for k in ("gb", "nonpolar", "lj", "coulomb"):
+    i = TERM_NAMES.index(k)
+    assert abs(e[0][i] - en[k]) <= 1e-6 * abs(en[k]) + 1e-6, k
+  with engine.Batch([s]) as b:  # dense Born radii differ: the option is an approximation
+    born_dense = b.born_radii()
+  assert np.max(np.abs(born - born_dense) / born_dense) > 1e-4
