@@ -232,7 +232,25 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   if (!b) return fail(ctx, PB2_ENOMEM, "host allocation");
   b->ctx = ctx;
   b->params = *params;
-  if (b->params.tile_segment <= 0) b->params.tile_segment = 8;
+  if (b->params.tile_segment <= 0) {
+    // default work-item length: the longest (8, 4, 2 or 1 j-blocks) that
+    // still gives every resident warp of the force pass a few items, so a
+    // small batch spreads over the whole GPU
+    const long long want = 4LL * ctx->sm_count * 16;
+    int seg = 1;
+    for (int cand : {8, 4, 2}) {
+      long long items = 0;
+      for (int s = 0; s < n_systems; ++s) {
+        const int nb = (systems[s].n_atoms + 31) / 32;
+        for (int ib = 0; ib < nb; ib += 2) items += (nb - ib + cand - 1) / cand;
+      }
+      if (items >= want) {
+        seg = cand;
+        break;
+      }
+    }
+    b->params.tile_segment = seg;
+  }
   if (b->params.graph_chunk <= 0) b->params.graph_chunk = 50;
   b->n_sys = n_systems;
   const bool cutoff_mode = params->cutoff > 0.0;
