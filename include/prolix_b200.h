@@ -237,6 +237,15 @@ int pb2_min_fire(pb2_batch *batch, int32_t n_steps, double k, int32_t kind, doub
                  double dt_max, double max_disp, double force_cap, int32_t flags, void *stream);
 int pb2_min_rms(pb2_batch *batch, double *rms, void *stream);
 
+/* L-BFGS polish of every system (the reference's jaxopt stage,
+ * batched_simulate.py:885-936): history `hist` (<= 16), backtracking line
+ * search from t = min(1, max_step) by 0.8 over at most max_trials energy
+ * evaluations (Armijo 1e-4, curvature 0.9), stopping a system when its
+ * gradient norm falls below tol; converged (may be NULL) receives 1 per
+ * system that did.  Uses the unrestrained energy. */
+int pb2_min_lbfgs(pb2_batch *batch, int32_t n_iter, double tol, double max_step, int32_t hist,
+                  int32_t max_trials, int32_t *converged, void *stream);
+
 /* Replica exchange (replaces the state shuffle of prolix
  * pt/replica_exchange.py:197-228): slot s takes the positions, momenta and
  * forces of slot perm[s]; keys, step counters, kT and dt stay with the

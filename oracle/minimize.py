@@ -89,3 +89,60 @@ def fire(system, r_start, r0, sel, masses, n_steps, k, dt_start, dt_max, max_dis
     r = r_before + d * sc
     p = p * sc
   return best_r, r
+
+
+def lbfgs(system, r_start, n_iter, tol=1e-6, max_step=0.1, hist=10, max_trials=30, energy_fn=None):
+  """L-BFGS (Nocedal & Wright alg. 7.4/7.5) as the device polish runs it:
+  two-loop recursion with H0 = (s.y / y.y) I, backtracking from
+  t = min(1, max_step) by 0.8 until E(t) <= E0 + 1e-4 t g.d and
+  |g(t).d| <= 0.9 |g.d| (or the last trial), steepest descent when d is
+  not a descent direction, pairs kept only with s.y > 1e-12, stop when
+  |g| < tol.  (jaxopt's LBFGS, the reference's stage, is third-party and
+  absent; this is the published algorithm with the reference's settings.)"""
+  def ef(r):
+    if energy_fn is not None:
+      return energy_fn(r)
+    e, f, _ = energy.energy_forces(system, r)
+    return e["total"], f
+
+  x = np.array(r_start, dtype=np.float64)
+  e0, f = ef(x)
+  g = np.where(np.isfinite(-f), -f, 0.0)
+  hs, hy, rho = [], [], []
+  for _ in range(n_iter):
+    q = g.copy()
+    alphas = []
+    for s_, y_, r_ in zip(reversed(hs), reversed(hy), reversed(rho)):
+      a_ = r_ * np.sum(s_ * q)
+      alphas.append(a_)
+      q = q - a_ * y_
+    gamma = np.sum(hs[-1] * hy[-1]) / np.sum(hy[-1] * hy[-1]) if hs else 1.0
+    q = q * gamma
+    for s_, y_, r_, a_ in zip(hs, hy, rho, reversed(alphas)):
+      b_ = r_ * np.sum(y_ * q)
+      q = q + s_ * (a_ - b_)
+    d = -q
+    gd = np.sum(g * d)
+    if not gd < 0:
+      d = -g
+      gd = -np.sum(g * g)
+      hs, hy, rho = [], [], []
+    t = min(1.0, max_step)
+    for trial in range(max_trials):
+      xt = x + t * d
+      et, ft = ef(xt)
+      gt = np.where(np.isfinite(-ft), -ft, 0.0)
+      ok = np.isfinite(et) and et <= e0 + 1e-4 * t * gd and abs(np.sum(gt * d)) <= 0.9 * abs(gd)
+      if ok or trial == max_trials - 1:
+        break
+      t *= 0.8
+    s_, y_ = xt - x, gt - g
+    sy = np.sum(s_ * y_)
+    if sy > 1e-12:
+      hs.append(s_); hy.append(y_); rho.append(1.0 / sy)
+      if len(hs) > hist:
+        hs.pop(0); hy.pop(0); rho.pop(0)
+    x, g, e0 = xt, gt, et
+    if np.sqrt(np.sum(g * g)) < tol:
+      break
+  return x

@@ -93,6 +93,8 @@ SIGNATURES = [
                                     ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                     ctypes.c_int32, ctypes.c_void_p]),
     ("pb2_min_rms", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("pb2_min_lbfgs", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]),
     ("pb2_permute_systems", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("pb2_energy_forces_device", ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_void_p] * 4),
     ("pb2_traj_setup", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),

@@ -1108,6 +1108,88 @@ extern "C" int pb2_min_fire(pb2_batch *b, int32_t n_steps, double k, int32_t kin
   return PB2_OK;
 }
 
+
+static LbfgsArgs lbfgs_args(pb2_batch *b, double tol, double max_step) {
+  LbfgsArgs a;
+  a.m = min_args(b);
+  a.energy = b->lb_energy;
+  a.g = b->lb_g; a.d = b->lb_d; a.x0 = b->lb_x0;
+  a.hs = b->lb_hs; a.hy = b->lb_hy; a.rho = b->lb_rho;
+  a.e0 = b->lb_sys; a.gd = b->lb_sys + b->n_sys; a.t = b->lb_sys + 2 * (size_t)b->n_sys;
+  a.count = b->lb_int; a.head = b->lb_int + b->n_sys; a.flags = b->lb_int + 2 * (size_t)b->n_sys;
+  a.hist = b->lb_hist;
+  a.tol = tol;
+  a.max_step = max_step;
+  return a;
+}
+
+// Forces and FP64 energies at the current positions into lb_energy.
+static int lbfgs_eval(pb2_batch *b, cudaStream_t st) {
+  int rc = fresh_forces(b, st, true);
+  if (rc) return rc;
+  CUDA_TRY(b->ctx, launch_energies_to_double(b->energy, b->lb_energy, b->n_sys, st));
+  return PB2_OK;
+}
+
+extern "C" int pb2_min_lbfgs(pb2_batch *b, int32_t n_iter, double tol, double max_step, int32_t hist,
+                             int32_t max_trials, int32_t *converged, void *stream) {
+  if (!b) return PB2_EINVAL;
+  pb2_ctx *ctx = b->ctx;
+  if (!b->min_ready) return fail(ctx, PB2_EINVAL, "call pb2_min_setup first");
+  if (n_iter < 0 || hist < 1 || hist > kLbfgsMaxHist || !(max_step > 0.0) || !(tol >= 0.0) || max_trials < 1)
+    return fail(ctx, PB2_EINVAL, "bad L-BFGS arguments");
+  cudaStream_t st = (cudaStream_t)stream;
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  const size_t N3 = 3 * (size_t)b->n_total, S = b->n_sys;
+  if (b->lb_hist != hist) {
+    Dev &D = b->mdev;
+    for (void *p : {(void *)b->lb_g, (void *)b->lb_d, (void *)b->lb_x0, (void *)b->lb_hs, (void *)b->lb_hy,
+                    (void *)b->lb_rho, (void *)b->lb_sys, (void *)b->lb_energy, (void *)b->lb_int})
+      if (p) D.release(p);
+    b->lb_g = D.alloc<double>(N3);
+    b->lb_d = D.alloc<double>(N3);
+    b->lb_x0 = D.alloc<double>(N3);
+    b->lb_hs = D.alloc<double>(hist * N3);
+    b->lb_hy = D.alloc<double>(hist * N3);
+    b->lb_rho = D.alloc<double>(hist * S);
+    b->lb_sys = D.alloc<double>(3 * S);
+    b->lb_energy = D.alloc<double>(S * PB2_NTERMS);
+    b->lb_int = D.alloc<int32_t>(3 * S);
+    if (!b->lb_g || !b->lb_d || !b->lb_x0 || !b->lb_hs || !b->lb_hy || !b->lb_rho || !b->lb_sys ||
+        !b->lb_energy || !b->lb_int) {
+      b->lb_hist = 0;
+      return fail(ctx, PB2_ENOMEM, "L-BFGS allocation failed");
+    }
+    b->lb_hist = hist;
+  }
+  const LbfgsArgs la = lbfgs_args(b, tol, max_step);
+  int rc = lbfgs_eval(b, st);
+  if (rc) return rc;
+  CUDA_TRY(ctx, launch_lbfgs(kLbfgsOpBegin, la, 0, st));
+  std::vector<int32_t> flags(S);
+  for (int it = 0; it < n_iter; ++it) {
+    CUDA_TRY(ctx, launch_lbfgs(kLbfgsOpDirection, la, 0, st));
+    for (int trial = 0; trial < max_trials; ++trial) {
+      CUDA_TRY(ctx, launch_lbfgs(kLbfgsOpTrial, la, 0, st));
+      if ((rc = lbfgs_eval(b, st))) return rc;
+      CUDA_TRY(ctx, launch_lbfgs(kLbfgsOpCheck, la, trial == max_trials - 1, st));
+      CUDA_TRY(ctx, cudaMemcpyAsync(flags.data(), la.flags, S * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+      CUDA_TRY(ctx, cudaStreamSynchronize(st));
+      bool searching = false;
+      for (int32_t f : flags) searching |= !(f & (kLbfgsAccepted | kLbfgsDone));
+      if (!searching) break;
+    }
+    bool all_done = true;
+    for (int32_t f : flags) all_done &= (f & kLbfgsDone) != 0;
+    if (all_done) break;
+  }
+  if (converged)
+    for (size_t s = 0; s < S; ++s) converged[s] = (flags[s] & kLbfgsDone) ? 1 : 0;
+  b->forces_valid = true;  // the last evaluation is at the final positions
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  return PB2_OK;
+}
+
 extern "C" int pb2_min_rms(pb2_batch *b, double *rms, void *stream) {
   if (!b || !rms) return PB2_EINVAL;
   pb2_ctx *ctx = b->ctx;

@@ -112,6 +112,11 @@ struct pb2_batch {
   int32_t *m_npos = nullptr;
   uint8_t *m_sel = nullptr;
   std::map<std::pair<int, int>, cudaGraphExec_t> min_graphs;  // (mode, chunk)
+  // L-BFGS polish state (allocated on first use)
+  int lb_hist = 0;
+  double *lb_g = nullptr, *lb_d = nullptr, *lb_x0 = nullptr, *lb_hs = nullptr, *lb_hy = nullptr;
+  double *lb_rho = nullptr, *lb_sys = nullptr, *lb_energy = nullptr;  // lb_sys: e0, gd, t
+  int32_t *lb_int = nullptr;  // count, head, flags
   double m_par_host[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // kMinNPar stage parameters
   // neighbour list (allocated on first build)
   Dev nl;

@@ -142,6 +142,22 @@ struct MinArgs {
   int32_t n_total, n_sys;
 };
 cudaError_t launch_min(int op, const MinArgs &a, double *out, cudaStream_t st);
+// L-BFGS polish (pb2_minimize.cu)
+constexpr int kLbfgsMaxHist = 16;
+enum { kLbfgsAccepted = 1, kLbfgsDone = 2 };
+enum { kLbfgsOpBegin = 0, kLbfgsOpDirection, kLbfgsOpTrial, kLbfgsOpCheck };
+struct LbfgsArgs {
+  MinArgs m;
+  const double *energy;  // (n_sys, PB2_NTERMS) FP64 energies of the current positions
+  double *g, *d, *x0;    // gradient, direction, base positions: (3, n_total)
+  double *hs, *hy;       // history: (hist, 3, n_total)
+  double *rho;           // (hist, n_sys)
+  double *e0, *gd, *t;   // per system
+  int32_t *count, *head, *flags;
+  int32_t hist;
+  double tol, max_step;
+};
+cudaError_t launch_lbfgs(int op, const LbfgsArgs &a, int last_trial, cudaStream_t st);
 cudaError_t launch_tiles(int pass, const PairArgs &a, int grid, cudaStream_t st);
 cudaError_t launch_energy64(int pass, const Energy64Args &a, int grid, cudaStream_t st);
 cudaError_t launch_born_finalize(const FinalizeArgs &a, cudaStream_t st);

@@ -282,6 +282,186 @@ __global__ void min_rms_kernel(const MinArgs a, double *out) {
   }
 }
 
+// -------------------------------------------------------------------- L-BFGS
+//
+// Limited-memory BFGS (Nocedal & Wright, Numerical Optimization, alg. 7.4
+// and 7.5) per system, the polish stage of the reference (jaxopt LBFGS,
+// batched_simulate.py:885-936): history of the last m steps s = x' - x and
+// gradient changes y = g' - g, two-loop recursion for d = -H g with
+// H0 = (s.y / y.y) I of the newest pair, and a backtracking line search
+// (x0 + t d, t from min(1, max_step) shrinking by 0.8: jaxopt's
+// max_stepsize clips the step length) accepting the first t with
+// E(t) <= E0 + 1e-4 t g.d and |g(t).d| <= 0.9 |g.d|, or the last of the
+// trials.  The gradient is minus the force; energies come from the FP64
+// energy path.
+
+__device__ __forceinline__ double grad_c(const LbfgsArgs &a, int i, int c) {
+  const long long *f = c == 0 ? a.m.fx : (c == 1 ? a.m.fy : a.m.fz);
+  const double v = -fix_d(f[i]);
+  return isfinite(v) ? v : 0.0;
+}
+
+// A block sums one product over the system's 3n coordinates.
+__device__ __forceinline__ double sys_dot(const double *u, const double *v, const SysInfo &S, size_t N) {
+  double acc = 0.0, z0 = 0.0, z1 = 0.0;
+  for (int i = S.off + threadIdx.x; i < S.off + S.n; i += blockDim.x)
+    acc += u[i] * v[i] + u[N + i] * v[N + i] + u[2 * N + i] * v[2 * N + i];
+  block_sum3(acc, z0, z1);
+  return acc;
+}
+
+// g <- gradient at the current positions, x0 <- positions, E0 <- energy,
+// empty history.
+__global__ void lbfgs_begin_kernel(const LbfgsArgs a) {
+  const size_t N = a.m.n_total;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.m.n_total; i += gridDim.x * blockDim.x) {
+    a.g[i] = grad_c(a, i, 0); a.g[N + i] = grad_c(a, i, 1); a.g[2 * N + i] = grad_c(a, i, 2);
+    a.x0[i] = a.m.x[i]; a.x0[N + i] = a.m.y[i]; a.x0[2 * N + i] = a.m.z[i];
+  }
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < a.m.n_sys; s += gridDim.x * blockDim.x) {
+    a.e0[s] = a.energy[(size_t)s * PB2_NTERMS + PB2_TERM_TOTAL];
+    a.count[s] = 0;
+    a.head[s] = 0;
+    a.flags[s] = 0;
+  }
+}
+
+// Two-loop recursion: d = -H g; t = min(1, max_step); gd = g.d.
+__global__ void lbfgs_direction_kernel(const LbfgsArgs a) {
+  __shared__ double alpha[kLbfgsMaxHist];
+  __shared__ double coef;
+  const size_t N = a.m.n_total, H = 3 * N;
+  for (int s = blockIdx.x; s < a.m.n_sys; s += gridDim.x) {
+    const SysInfo &S = a.m.sys[s];
+    if (a.flags[s] & kLbfgsDone) continue;  // uniform over the block
+    const int cnt = a.count[s], head = a.head[s], m = a.hist;
+    for (int i = S.off + threadIdx.x; i < S.off + S.n; i += blockDim.x) {
+      a.d[i] = a.g[i]; a.d[N + i] = a.g[N + i]; a.d[2 * N + i] = a.g[2 * N + i];
+    }
+    __syncthreads();
+    for (int k = 0; k < cnt; ++k) {  // newest to oldest
+      const int h = (head - 1 - k + m) % m;
+      const double *sh = a.hs + h * H, *yh = a.hy + h * H;
+      const double al = a.rho[(size_t)h * a.m.n_sys + s] * sys_dot(sh, a.d, S, N);
+      if (threadIdx.x == 0) alpha[k] = al;
+      for (int i = S.off + threadIdx.x; i < S.off + S.n; i += blockDim.x) {
+        a.d[i] -= al * yh[i]; a.d[N + i] -= al * yh[N + i]; a.d[2 * N + i] -= al * yh[2 * N + i];
+      }
+      __syncthreads();
+    }
+    double gamma = 1.0;
+    if (cnt > 0) {
+      const int h = (head - 1 + m) % m;
+      const double sy = sys_dot(a.hs + h * H, a.hy + h * H, S, N);
+      const double yy = sys_dot(a.hy + h * H, a.hy + h * H, S, N);
+      if (yy > 0.0) gamma = sy / yy;
+    }
+    for (int i = S.off + threadIdx.x; i < S.off + S.n; i += blockDim.x) {
+      a.d[i] *= gamma; a.d[N + i] *= gamma; a.d[2 * N + i] *= gamma;
+    }
+    __syncthreads();
+    for (int k = cnt - 1; k >= 0; --k) {  // oldest to newest
+      const int h = (head - 1 - k + m) % m;
+      const double *sh = a.hs + h * H, *yh = a.hy + h * H;
+      const double be = a.rho[(size_t)h * a.m.n_sys + s] * sys_dot(yh, a.d, S, N);
+      const double c = alpha[k] - be;
+      for (int i = S.off + threadIdx.x; i < S.off + S.n; i += blockDim.x) {
+        a.d[i] += c * sh[i]; a.d[N + i] += c * sh[N + i]; a.d[2 * N + i] += c * sh[2 * N + i];
+      }
+      __syncthreads();
+    }
+    // d = -r; not a descent direction (or empty history start): steepest descent
+    double gd = -sys_dot(a.g, a.d, S, N);
+    if (threadIdx.x == 0) coef = (gd < 0.0) ? -1.0 : 0.0;
+    __syncthreads();
+    const bool sd = coef == 0.0;
+    for (int i = S.off + threadIdx.x; i < S.off + S.n; i += blockDim.x) {
+      for (int c = 0; c < 3; ++c) {
+        double &dv = a.d[c * N + i];
+        dv = sd ? -a.g[c * N + i] : -dv;
+      }
+    }
+    __syncthreads();
+    if (sd) gd = -sys_dot(a.g, a.g, S, N);
+    if (threadIdx.x == 0) {
+      if (sd) a.count[s] = 0;
+      a.gd[s] = gd;
+      a.t[s] = fmin(1.0, a.max_step);
+      a.flags[s] &= ~kLbfgsAccepted;
+    }
+    __syncthreads();
+  }
+}
+
+// Trial positions x0 + t d for the systems still searching.
+__global__ void lbfgs_trial_kernel(const LbfgsArgs a) {
+  const size_t N = a.m.n_total;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.m.n_total; i += gridDim.x * blockDim.x) {
+    const int s = a.m.atom_sys[i];
+    if (!(a.flags[s] & (kLbfgsDone | kLbfgsAccepted))) {
+      const double t = a.t[s];
+      a.m.x[i] = a.x0[i] + t * a.d[i];
+      a.m.y[i] = a.x0[N + i] + t * a.d[N + i];
+      a.m.z[i] = a.x0[2 * N + i] + t * a.d[2 * N + i];
+    }
+    a.m.fx[i] = 0; a.m.fy[i] = 0; a.m.fz[i] = 0;
+    put_posq(a.m, i);
+  }
+}
+
+// Line-search test; on acceptance (or the last trial) the history, gradient,
+// energy and base positions advance and convergence is checked.
+__global__ void lbfgs_check_kernel(const LbfgsArgs a, int last_trial) {
+  __shared__ int take;
+  const size_t N = a.m.n_total, H = 3 * N;
+  for (int s = blockIdx.x; s < a.m.n_sys; s += gridDim.x) {
+    const SysInfo &S = a.m.sys[s];
+    if (a.flags[s] & (kLbfgsDone | kLbfgsAccepted)) continue;
+    const double et = a.energy[(size_t)s * PB2_NTERMS + PB2_TERM_TOTAL];
+    double gtd = 0.0, z0 = 0.0, z1 = 0.0;
+    for (int i = S.off + threadIdx.x; i < S.off + S.n; i += blockDim.x)
+      gtd += grad_c(a, i, 0) * a.d[i] + grad_c(a, i, 1) * a.d[N + i] + grad_c(a, i, 2) * a.d[2 * N + i];
+    block_sum3(gtd, z0, z1);
+    if (threadIdx.x == 0) {
+      const double t = a.t[s], gd = a.gd[s];
+      const bool ok = isfinite(et) && et <= a.e0[s] + 1e-4 * t * gd && fabs(gtd) <= 0.9 * fabs(gd);
+      take = ok || last_trial;
+      if (!take) a.t[s] = t * 0.8;
+    }
+    __syncthreads();
+    if (take) {
+      const int m = a.hist, h = a.head[s];
+      double *sh = a.hs + h * H, *yh = a.hy + h * H;
+      double sy = 0.0, g2 = 0.0, z2 = 0.0;
+      for (int i = S.off + threadIdx.x; i < S.off + S.n; i += blockDim.x) {
+        const double xn[3] = {a.m.x[i], a.m.y[i], a.m.z[i]};
+        for (int c = 0; c < 3; ++c) {
+          const size_t k = c * N + i;
+          const double gn = grad_c(a, i, c);
+          sh[k] = xn[c] - a.x0[k];
+          yh[k] = gn - a.g[k];
+          sy += sh[k] * yh[k];
+          g2 += gn * gn;
+          a.g[k] = gn;
+          a.x0[k] = xn[c];
+        }
+      }
+      block_sum3(sy, g2, z2);
+      if (threadIdx.x == 0) {
+        if (sy > 1e-12) {  // keep the pair only with positive curvature
+          a.rho[(size_t)h * a.m.n_sys + s] = 1.0 / sy;
+          a.head[s] = (h + 1) % m;
+          a.count[s] = min(a.count[s] + 1, m);
+        }
+        a.e0[s] = et;
+        a.flags[s] |= kLbfgsAccepted;
+        if (sqrt(g2) < a.tol) a.flags[s] |= kLbfgsDone;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // ----------------------------------------------------------------- launchers
 
 static int atom_grid(int n) {
@@ -301,6 +481,19 @@ cudaError_t launch_min(int op, const MinArgs &a, double *out, cudaStream_t st) {
     case kMinOpFireMix: min_fire_mix_kernel<<<gs, kMinThreads, 0, st>>>(a); break;
     case kMinOpTakeBest: min_take_best_kernel<<<ga, kMinThreads, 0, st>>>(a); break;
     case kMinOpRms: min_rms_kernel<<<gs, kMinThreads, 0, st>>>(a, out); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lbfgs(int op, const LbfgsArgs &a, int last_trial, cudaStream_t st) {
+  if (a.m.n_total <= 0) return cudaSuccess;
+  const int ga = atom_grid(a.m.n_total), gs = a.m.n_sys;
+  switch (op) {
+    case kLbfgsOpBegin: lbfgs_begin_kernel<<<ga, kMinThreads, 0, st>>>(a); break;
+    case kLbfgsOpDirection: lbfgs_direction_kernel<<<gs, kMinThreads, 0, st>>>(a); break;
+    case kLbfgsOpTrial: lbfgs_trial_kernel<<<ga, kMinThreads, 0, st>>>(a); break;
+    case kLbfgsOpCheck: lbfgs_check_kernel<<<gs, kMinThreads, 0, st>>>(a, last_trial); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

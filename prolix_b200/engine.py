@@ -349,6 +349,13 @@ class Batch:
                                       float(dt_start), float(dt_max), float(max_disp), float(force_cap),
                                       1 if keep_best else 0, stream))
 
+  def min_lbfgs(self, n_iter, tol=1e-6, max_step=0.1, hist=10, max_trials=30, stream=None):
+    """L-BFGS polish of every system; returns the per-system converged flags."""
+    conv = np.zeros(self.n_systems, dtype=np.int32)
+    self._check(self.lib.pb2_min_lbfgs(self.handle, int(n_iter), float(tol), float(max_step), int(hist),
+                                       int(max_trials), conv.ctypes.data, stream))
+    return conv.astype(bool)
+
   def min_rms(self, stream=None):
     """Per-system RMS over atoms of the unrestrained force, kcal/mol/A."""
     out = np.zeros(self.n_systems)

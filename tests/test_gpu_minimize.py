@@ -88,3 +88,32 @@ def test_production_run_simulation(tmp_path):
   assert all(np.isfinite(f["potential_energy"]) and f["kinetic_energy"] > 0 for f in frames)
   assert final.step == 1000 and np.isfinite(final.positions).all()
   np.testing.assert_array_equal(frames[-1]["positions"], final.positions.astype(np.float32))
+
+
+def test_lbfgs_polish_matches_oracle_and_descends():
+  s = _sys(166, 16)
+  with engine.Batch([s]) as b:
+    b.min_setup()
+    b.min_lbfgs(3, tol=1e-6, max_step=0.1, hist=10)
+    got = b.get_state(fields=("position",))["position"]
+  ref = om.lbfgs(s, s["positions"], 3, tol=1e-6, max_step=0.1, hist=10)
+  assert np.max(np.abs(got - ref)) < 1e-5
+  assert np.max(np.abs(got - s["positions"])) > 1e-4
+  # a longer polish lowers energy and gradient (Armijo steps)
+  with engine.Batch([s]) as b:
+    b.min_setup()
+    e0, f0 = b.energy_forces()
+    conv = b.min_lbfgs(60, tol=1e-6, max_step=0.1, hist=10)
+    e1, f1 = b.energy_forces()
+  assert conv.shape == (1,)
+  assert e1[0][-1] < e0[0][-1] and np.linalg.norm(f1) < np.linalg.norm(f0)
+
+
+def test_batched_minimize_with_lbfgs_polish():
+  systems = [_sys(n, 40 + i) for i, n in enumerate((166, 300))]
+  _, _, rms_fire = batched_minimize(systems, max_steps=100, lbfgs_steps=0,
+                                    fire_stage_steps=(50, 50, 50, 100))
+  pos, converged, rms = batched_minimize(systems, max_steps=100, lbfgs_steps=100,
+                                         fire_stage_steps=(50, 50, 50, 100))
+  assert np.all(rms < rms_fire)
+  assert all(np.isfinite(p).all() for p in pos)

@@ -48,3 +48,17 @@ def test_restraint_and_nan_guard():
   f = om.total_force(None, r, r0, 50.0, np.array([1.0, 0.0, 1.0]),
                      force_fn=lambda x: np.array([[np.nan, 1.0, 2.0], [0.0, 0.0, 0.0], [1.0, 1.0, 1.0]]))
   np.testing.assert_array_equal(f, [[0.0, -49.0, -48.0], [0.0, 0.0, 0.0], [-49.0, -49.0, -49.0]])
+
+
+def test_lbfgs_restatement_minimises_a_quadratic():
+  rng = np.random.default_rng(3)
+  a = rng.normal(size=(12, 12))
+  hmat = a @ a.T + 12 * np.eye(12)
+  x_star = rng.normal(size=(4, 3))
+
+  def energy_fn(r):
+    d = (r - x_star).reshape(-1)
+    return 0.5 * d @ hmat @ d, -(hmat @ d).reshape(4, 3)
+
+  x = om.lbfgs(None, np.zeros((4, 3)), 200, tol=1e-9, max_step=1.0, energy_fn=energy_fn)
+  assert np.max(np.abs(x - x_star)) < 1e-6
