@@ -16,12 +16,14 @@
 // of j-blocks); lane l owns atom l of each i-block for the whole item; the
 // j-block's data and j-side accumulators rotate through the lanes by
 // shuffles, so lane l meets j-lane (l + k) mod 32 at step k of the 32-step
-// loop, once for each of its two i atoms.  Per tile, each lane's
-// pair-validity and exclusion bit masks are rotated by its lane index once,
-// so step k tests bit k.  A per-block bounding box sorts tiles: tiles whose
-// boxes are at least the far-field distance apart evaluate the OBC integral
-// by its series (4 to 10 terms by separation) without per-pair branches, and
-// (with a cutoff) tiles beyond every cutoff are skipped.
+// loop, once for each of its two i atoms; the two pairs of a step run as
+// packed f32x2 arithmetic.  Per tile, each lane's pair-validity and
+// exclusion bit masks are rotated by its lane index once, so step k tests
+// bit k (the sign bit of the bit-reversed mask shifted k times).  A
+// per-block bounding box sorts tiles: tiles whose boxes are at least the
+// far-field distance apart evaluate the OBC integral by its series (4 to 10
+// terms by separation) without per-pair branches, and (with a cutoff)
+// tiles beyond every cutoff are skipped.
 //
 // Arithmetic is FP32; per-tile partial sums are converted to 64-bit fixed
 // point and combined with integer atomics, so results do not depend on

@@ -45,40 +45,12 @@ __device__ __forceinline__ float obc_series_der_n(float u) {
   return p;
 }
 
-__device__ __forceinline__ float obc_series_val(float u) {
-  // sum_{k=1..9} k/(2k+1) u^(k-1)
-  float p = 9.0f / 19.0f;
-  p = fmaf(p, u, 8.0f / 17.0f);
-  p = fmaf(p, u, 7.0f / 15.0f);
-  p = fmaf(p, u, 6.0f / 13.0f);
-  p = fmaf(p, u, 5.0f / 11.0f);
-  p = fmaf(p, u, 4.0f / 9.0f);
-  p = fmaf(p, u, 3.0f / 7.0f);
-  p = fmaf(p, u, 2.0f / 5.0f);
-  p = fmaf(p, u, 1.0f / 3.0f);
-  return p;
-}
-
-__device__ __forceinline__ float obc_series_der(float u) {
-  // sum_{k=1..9} 2k(k+1)/(2k+1) u^(k-1)
-  float p = 180.0f / 19.0f;
-  p = fmaf(p, u, 144.0f / 17.0f);
-  p = fmaf(p, u, 112.0f / 15.0f);
-  p = fmaf(p, u, 84.0f / 13.0f);
-  p = fmaf(p, u, 60.0f / 11.0f);
-  p = fmaf(p, u, 40.0f / 9.0f);
-  p = fmaf(p, u, 24.0f / 7.0f);
-  p = fmaf(p, u, 12.0f / 5.0f);
-  p = fmaf(p, u, 4.0f / 3.0f);
-  return p;
-}
-
 // I(r; rho, s).  inv_r = 1/r (already available to every caller).
 __device__ __forceinline__ float obc_integral(float r, float inv_r, float rho, float s) {
   if (!(r + s > rho)) return 0.0f;
   const float t = s * inv_r;
   const float u = t * t;
-  if (u <= kSeriesU && r - s >= rho) return t * u * inv_r * obc_series_val(u);
+  if (u <= kSeriesU && r - s >= rho) return t * u * inv_r * obc_series_val_n<9>(u);
   const float rs = fmaxf(r, 1e-4f);
   const float irs = 1.0f / rs;
   const float L = fmaxf(fmaxf(rho, fabsf(r - s)), 1e-4f);
@@ -93,7 +65,7 @@ __device__ __forceinline__ float obc_integral_dr(float r, float inv_r, float rho
   if (!(r + s > rho)) return 0.0f;
   const float t = s * inv_r;
   const float u = t * t;
-  if (u <= kSeriesU && r - s >= rho) return -t * u * inv_r * inv_r * obc_series_der(u);
+  if (u <= kSeriesU && r - s >= rho) return -t * u * inv_r * inv_r * obc_series_der_n<9>(u);
   const float rs = fmaxf(r, 1e-4f);
   const float drs = r > 1e-4f ? 1.0f : 0.0f;
   const float irs = 1.0f / rs;
