@@ -81,6 +81,13 @@ def series_terms(systems) -> float:
 
 
 MUFU_PER_PAIR = {"born": 1, "force": 3, "chain": 1}
+# The same passes counted with the closed-form OBC formulas that prolix
+# evaluates for every pair (generalized_born.py:211-263 per ordered pair:
+# about 40 flops for I_ij, 45 for dI_ij/dr; analytical_forces.py:167-292
+# for GB + Coulomb + LJ: about 70 flops per unique pair), per unique pair.
+# The series kernels do less arithmetic than this, so the equivalent rate
+# can exceed the FP32 peak; it is reported beside the counted figure.
+CLOSED_FORM_FLOPS_PER_PAIR = {"born": 80.0, "force": 70.0, "chain": 90.0}
 # integrator: read x, p (48 B), F (24 B), mass, sigma, charge (24 B); write
 # x, p (48 B), posq (16 B), clear F (24 B)
 BYTES_PER_ATOM_STEP = 184
@@ -478,7 +485,13 @@ def main():
               "xu_peak_tops": xu_peak,
               "algorithmic_flops_per_launch": fpp[dom] * pairs,
               "flops_per_pair": fpp, "series_terms_mean": k_mean,
-              "passes": passes}
+              "passes": passes,
+              "closed_form_equivalent": {
+                  "flops_per_pair": CLOSED_FORM_FLOPS_PER_PAIR,
+                  "tflops": {p: CLOSED_FORM_FLOPS_PER_PAIR[p] * pairs / (per_kernel[p] * 1e-3) / 1e12
+                             for p in passes if per_kernel[p] > 0},
+                  "frac": {p: CLOSED_FORM_FLOPS_PER_PAIR[p] * pairs / (per_kernel[p] * 1e-3) / 1e12 / peak
+                           for p in passes if per_kernel[p] > 0 and peak}}}
   integ_gbs = BYTES_PER_ATOM_STEP * n_atoms / (per_kernel["integrator"] * 1e-3) / 1e9
   hbm_peak = _measured_hbm()
   integrator = {"achieved_gbs": integ_gbs, "peak_gbs": hbm_peak,
