@@ -41,24 +41,41 @@ WORKLOAD_SEED = 2024
 N_SYSTEMS = 512
 
 # Algorithmic work per unique pair (i < j), counted from the kernel source
-# with FMA = 2 flops (pb2_pair.cu bc_series / force_pair).  The descreening
-# and chain passes evaluate the far-field series with K terms (K + 1 for its
-# derivative), K chosen per tile from the bounding-box separation
-# (4, 6, 8 or 10); series_terms() gives the pair-weighted mean K.
+# with FMA = 2 flops (pb2_pair.cu bc_series2 / run_force_tile2).  The
+# descreening and chain passes evaluate the far-field series V (value) or D
+# (derivative) as a polynomial of K terms, K chosen per tile from the
+# bounding-box separation (pb2_obc_series.cuh tiers: V 3-6 terms, D 4-7);
+# series_terms() gives the pair-weighted mean K of each.
 #   descreening: 3 (d) + 5 (r^2) + 2 (1/r^2, 1/r^4)
-#                + 2 x (1 + 2(K-1) + 1) (u, series, s^3) + 2 x 2 (sums)  = 4K + 14
+#                + 2 x (1 + 2(K-1) + 1) (u, polynomial, s^3) + 2 x 2 (sums) = 4K + 14
 #   force:       8 (d, r^2) + 1 (q q) + GB 16 + 4 (dE/dB) + 1 (1/r^2)
 #                + Coulomb 2 + LJ 11 + 2 (sum) + 12 (F)                  = 57
 #   chain:       3 (d) + 5 (r^2) + 3 (1/r^2, -1/r^6)
-#                + 2 x (1 + 2K + 1) + 4 (g) + 12 (F)                      = 4K + 31
-def flops_per_pair(k_mean: float) -> dict:
-  return {"born": 4.0 * k_mean + 14.0, "force": 57.0, "chain": 4.0 * k_mean + 31.0}
+#                + 2 x (1 + 2(K-1) + 1) + 4 (g) + 12 (F)                  = 4K + 27
+def flops_per_pair(k_mean: dict) -> dict:
+  return {"born": 4.0 * k_mean["value"] + 14.0, "force": 57.0, "chain": 4.0 * k_mean["deriv"] + 27.0}
 
 
-def series_terms(systems) -> float:
-  """Pair-weighted mean number of series terms per tile, by the same
-  bounding-box classification the kernels use (float32 radii)."""
-  tot_k = tot_w = 0.0
+def series_tiers() -> dict:
+  """u bounds and term counts of the polynomial tiers the kernels use."""
+  import re
+  with open(os.path.join(ROOT, "prolix_b200", "csrc", "pb2_obc_series.cuh")) as f:
+    txt = f.read()
+  out = {}
+  for name in ("Value", "Deriv"):
+    u = re.search(r"k%sTierU\[4\] = \{([^}]*)\}" % name, txt).group(1)
+    k = re.search(r"k%sTierTerms\[4\] = \{([^}]*)\}" % name, txt).group(1)
+    out[name.lower()] = ([float(v) for v in u.split(",")], [int(v) for v in k.split(",")])
+  return out
+
+
+def series_terms(systems) -> dict:
+  """Pair-weighted mean number of polynomial terms per tile (value and
+  derivative series), by the same bounding-box classification the kernels
+  use (float32 radii)."""
+  tiers = series_tiers()
+  tot = {"value": 0.0, "deriv": 0.0}
+  tot_w = 0.0
   for sd in systems:
     x = np.asarray(sd["positions"], dtype=np.float64)
     n = len(x)
@@ -73,11 +90,13 @@ def series_terms(systems) -> float:
     ib, jb = np.triu_indices(nb)
     d = np.maximum(0.0, np.maximum(lo[ib] - hi[jb], lo[jb] - hi[ib]))
     d2 = (d * d).sum(1)
-    k = np.select([d2 >= b2(0.0109), d2 >= b2(0.049), d2 >= b2(0.104)], [4.0, 6.0, 8.0], 10.0)
     w = np.where(ib == jb, m[ib] * (m[ib] - 1) / 2.0, m[ib] * m[jb].astype(np.float64))
-    tot_k += float((k * w).sum())
+    for key, (us, ks) in tiers.items():
+      k = np.select([d2 >= b2(us[0]), d2 >= b2(us[1]), d2 >= b2(us[2])], [float(v) for v in ks[:3]],
+                    float(ks[3]))
+      tot[key] += float((k * w).sum())
     tot_w += float(w.sum())
-  return tot_k / tot_w
+  return {key: v / tot_w for key, v in tot.items()}
 
 
 MUFU_PER_PAIR = {"born": 1, "force": 3, "chain": 1}

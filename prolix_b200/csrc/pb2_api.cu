@@ -19,6 +19,7 @@
 
 #include "pb2_common.cuh"
 #include "pb2_kernels.cuh"
+#include "pb2_obc_series.cuh"
 
 
 #include "pb2_internal.h"
@@ -353,10 +354,11 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
         const double r = 1.001 * std::max((double)smax / std::sqrt(u), (double)smax + (double)romax);
         return (float)(r * r);
       };
-      S.far2 = bound2(0.16);
-      S.far2_k8 = bound2(0.104);
-      S.far2_k6 = bound2(0.049);
-      S.far2_k4 = bound2(0.0109);
+      S.far2 = bound2(kValueTierU[3]);
+      for (int t = 0; t < 3; ++t) {
+        S.tier2[0][t] = bound2(kValueTierU[t]);
+        S.tier2[1][t] = bound2(kDerivTierU[t]);
+      }
       S.ro_max = romax;
     }
     for (int bk = 0; bk < S.nblk; ++bk) hblk_sys[blk_base + bk] = s;

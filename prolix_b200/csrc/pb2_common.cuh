@@ -31,7 +31,7 @@ constexpr double kAceCoeff = 28.3919551, kKjToKcal = 0.239006;
 
 constexpr int kExclPerBlock = 8;  // distinct j-blocks with exclusions per i-block
 
-// Per-system constants, one 160-byte record per system.  Pair kernels see
+// Per-system constants, one 168-byte record per system.  Pair kernels see
 // positions relative to the system origin (its initial centroid), which keeps
 // float32 coordinates small.
 struct SysInfo {
@@ -44,13 +44,13 @@ struct SysInfo {
   float lj14, coul14; // 1-4 scales
   float cutoff2;      // LJ / Coulomb cutoff^2; 0: all pairs
   float far2;         // tiles at least this far apart (squared) take the far-field series
-                      // (10 terms); nearer tiles test each pair
+                      // of the widest tier; nearer tiles test each pair
   float gb_cutoff2;   // GB / descreening cutoff^2; 0: all pairs
   int32_t clamp;      // neighbour-list clamps on Born radii (GB cutoff set)
-  float far2_k8, far2_k6, far2_k4;  // tiles this far apart need 8 / 6 / 4 series terms
   float ro_max;       // largest rho~ = radius - offset of the system
   float born_cut2;    // descreening / chain-rule cutoff^2; 0: all pairs
-  int32_t pad1;
+  float tier2[2][3];  // [value, derivative][tier 0-2]: tiles at least this far apart
+                      // (squared) evaluate that tier's series polynomial
   double kcoul_d;     // direct Coulomb constant in double (energy path)
   double pref_d;      // P in double (self / energy terms)
   double dt, half_dt; // tau
@@ -59,7 +59,7 @@ struct SysInfo {
   double skin_half2;  // (skin/2)^2
   double ox, oy, oz;  // origin subtracted before the float32 pair kernels
 };
-static_assert(sizeof(SysInfo) == 160, "SysInfo layout");
+static_assert(sizeof(SysInfo) == 168, "SysInfo layout");
 
 // Work item of the tile kernels: tiles (iblk, jb) for jb in [jb0, jb1) of
 // system sys.  Block indices are local to the system.

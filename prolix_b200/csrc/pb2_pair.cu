@@ -21,9 +21,10 @@
 // exclusion bit masks are rotated by its lane index once, so step k tests
 // bit k (the sign bit of the bit-reversed mask shifted k times).  A
 // per-block bounding box sorts tiles: tiles whose boxes are at least the
-// far-field distance apart evaluate the OBC integral by its series (4 to 10
-// terms by separation) without per-pair branches, and (with a cutoff)
-// tiles beyond every cutoff are skipped.
+// far-field distance apart evaluate the OBC integral by a minimax
+// polynomial of its far-field series (3 to 7 terms by separation,
+// pb2_obc_series.cuh) without per-pair branches, and (with a cutoff) tiles
+// beyond every cutoff are skipped.
 //
 // Arithmetic is FP32; per-tile partial sums are converted to 64-bit fixed
 // point and combined with integer atomics, so results do not depend on
@@ -32,6 +33,7 @@
 
 #include "pb2_common.cuh"
 #include "pb2_kernels.cuh"
+#include "pb2_obc_series.cuh"
 #include "pb2_pairmath.cuh"
 
 // Unroll factor of the 32-step rotation loop (code size against loop
@@ -229,20 +231,10 @@ __device__ __forceinline__ PData2 pack2(const PData &a, const PData &b) {
   return p;
 }
 
-template <int K>
-__device__ __forceinline__ float2 obc_series_val2(float2 u) {
-  float2 p = dup2((float)((double)K / (double)(2 * K + 1)));
-#pragma unroll
-  for (int k = K - 1; k >= 1; --k) p = __ffma2_rn(p, u, dup2((float)((double)k / (double)(2 * k + 1))));
-  return p;
-}
-template <int K>
-__device__ __forceinline__ float2 obc_series_der2(float2 u) {
-  float2 p = dup2((float)(2.0 * K * (K + 1) / (double)(2 * K + 1)));
-#pragma unroll
-  for (int k = K - 1; k >= 1; --k) p = __ffma2_rn(p, u, dup2((float)(2.0 * k * (k + 1) / (double)(2 * k + 1))));
-  return p;
-}
+// The near-tile domain (per-pair test against kSeriesUNear) is the widest
+// tier of both polynomials.
+static_assert((float)kValueTierU[3] == kSeriesUNear && (float)kDerivTierU[3] == kSeriesUNear,
+              "series tiers");
 
 struct Acc2 {
   float2 a0, a1, a2;
@@ -263,7 +255,7 @@ struct BCPair2 {
   bool ok0, ok1;
 };
 
-template <int PASS, bool CUT, int NT>
+template <int PASS, bool CUT, int TIER>
 __device__ __forceinline__ void bc_series2(const PData2 &I, const PData &J, bool ok0, bool ok1, BCPair2 &P,
                                            const TileConst &K) {
   P.dx = __fadd2_rn(I.x, dup2(-J.x));
@@ -282,12 +274,12 @@ __device__ __forceinline__ void bc_series2(const PData2 &I, const PData &J, bool
   const float2 inv_r2 = __fmul2_rn(P.inv_r, P.inv_r);
   const float2 inv_r4 = __fmul2_rn(inv_r2, inv_r2);
   if (PASS == PASS_BORN) {
-    P.vij = __fmul2_rn(dup2(J.s3), obc_series_val2<NT>(__fmul2_rn(dup2(J.s2), inv_r2)));
-    P.vji = __fmul2_rn(I.s3, obc_series_val2<NT>(__fmul2_rn(I.s2, inv_r2)));
+    P.vij = __fmul2_rn(dup2(J.s3), ObcPoly<false, TIER>::eval2(__fmul2_rn(dup2(J.s2), inv_r2)));
+    P.vji = __fmul2_rn(I.s3, ObcPoly<false, TIER>::eval2(__fmul2_rn(I.s2, inv_r2)));
     P.f = inv_r4;
   } else {
-    P.vij = __fmul2_rn(dup2(J.s3), obc_series_der2<NT + 1>(__fmul2_rn(dup2(J.s2), inv_r2)));
-    P.vji = __fmul2_rn(I.s3, obc_series_der2<NT + 1>(__fmul2_rn(I.s2, inv_r2)));
+    P.vij = __fmul2_rn(dup2(J.s3), ObcPoly<true, TIER>::eval2(__fmul2_rn(dup2(J.s2), inv_r2)));
+    P.vji = __fmul2_rn(I.s3, ObcPoly<true, TIER>::eval2(__fmul2_rn(I.s2, inv_r2)));
     P.f = __fmul2_rn(inv_r4, inv_r2);
   }
 }
@@ -333,7 +325,7 @@ __device__ __forceinline__ void bc_accumulate2(const PData2 &I, const PData &J, 
 // FAR: both tiles lie in the series' domain (no per-pair test); otherwise
 // each pair is tested and the closed form runs, after a warp vote, only for
 // the lanes that need it.
-template <int PASS, bool FAR, bool CUT, int NT>
+template <int PASS, bool FAR, bool CUT, int TIER>
 __device__ __forceinline__ void run_bc_tile2(const PData2 &I, PData &J, Acc2 &ti, Acc &tj, uint32_t V0,
                                              uint32_t V1, const TileConst &K) {
   const int src = K.src;
@@ -342,7 +334,7 @@ __device__ __forceinline__ void run_bc_tile2(const PData2 &I, PData &J, Acc2 &ti
 #pragma unroll kUnrollBC
   for (int k = 0; k < 32; ++k) {
     BCPair2 P;
-    bc_series2<PASS, CUT, NT>(I, J, (int32_t)R0 < 0, (int32_t)R1 < 0, P, K);
+    bc_series2<PASS, CUT, TIER>(I, J, (int32_t)R0 < 0, (int32_t)R1 < 0, P, K);
     R0 <<= 1;
     R1 <<= 1;
     if (!FAR) {
@@ -491,13 +483,14 @@ __global__ void __launch_bounds__(256, PASS == PASS_BORN ? PB2_MINB_BORN : (PASS
         t0.a0 = tf.a0.x; t0.a1 = tf.a1.x; t0.a2 = tf.a2.x; t0.a3 = tf.a3.x;
         t1.a0 = tf.a0.y; t1.a1 = tf.a1.y; t1.a2 = tf.a2.y; t1.a3 = tf.a3.y;
       } else {
-        // series length by the tiles' smallest separation
+        // series tier by the tiles' smallest separation
+        const float *tier2 = S.tier2[PASS == PASS_BORN ? 0 : 1];
         Acc2 ti = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-        if (d2 >= S.far2_k4) run_bc_tile2<PASS, true, CUT, 4>(I2, J, ti, tj, V0, V1, K);
-        else if (d2 >= S.far2_k6) run_bc_tile2<PASS, true, CUT, 6>(I2, J, ti, tj, V0, V1, K);
-        else if (d2 >= S.far2_k8) run_bc_tile2<PASS, true, CUT, 8>(I2, J, ti, tj, V0, V1, K);
-        else if (d2 >= S.far2) run_bc_tile2<PASS, true, CUT, 10>(I2, J, ti, tj, V0, V1, K);
-        else run_bc_tile2<PASS, false, CUT, 10>(I2, J, ti, tj, V0, V1, K);
+        if (d2 >= tier2[0]) run_bc_tile2<PASS, true, CUT, 0>(I2, J, ti, tj, V0, V1, K);
+        else if (d2 >= tier2[1]) run_bc_tile2<PASS, true, CUT, 1>(I2, J, ti, tj, V0, V1, K);
+        else if (d2 >= tier2[2]) run_bc_tile2<PASS, true, CUT, 2>(I2, J, ti, tj, V0, V1, K);
+        else if (d2 >= S.far2) run_bc_tile2<PASS, true, CUT, 3>(I2, J, ti, tj, V0, V1, K);
+        else run_bc_tile2<PASS, false, CUT, 3>(I2, J, ti, tj, V0, V1, K);
         t0.a0 = ti.a0.x; t0.a1 = ti.a1.x; t0.a2 = ti.a2.x;
         t1.a0 = ti.a0.y; t1.a1 = ti.a1.y; t1.a2 = ti.a2.y;
       }

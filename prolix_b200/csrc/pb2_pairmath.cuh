@@ -13,13 +13,11 @@
 // cancellation between the O(1/r) terms of the closed form (whose sum is
 // O(s^3/r^4)).  Nearer pairs use the closed form with an accurate logf.
 //
-// Truncation: K terms of the value series leave a relative error at most
-// 2e-8 (a third of a float32 ulp) for u = t^2 up to
-//   K:  4       6       8       9       10
-//   u:  0.0110  0.0493  0.1046  0.1345  0.1644
-// and the derivative series needs K + 1 terms for the same u.  The pair
-// kernels pick K per tile from the smallest distance between the two
-// blocks' bounding boxes.
+// The pair kernels sort tiles into tiers by the smallest distance between
+// the two blocks' bounding boxes, and evaluate the two sums there by minimax
+// polynomials of 3 to 7 terms (pb2_obc_series.cuh, written by
+// gen_obc_series.py), each within 2e-8 relative of the full series on its
+// tier.  The closed-form helpers below take the Taylor series directly.
 #pragma once
 
 namespace pb2 {

@@ -130,21 +130,43 @@ def test_build_flags_target_sm100a_only():
   assert "sm_90" not in flags
 
 
-def test_far_field_series_lengths_meet_float32_bound():
-  # The pair kernels evaluate the OBC far-field series with K terms (value)
-  # and K + 1 terms (derivative) on tiles whose smallest box separation keeps
-  # u = (s/r)^2 below u_K (pb2_api.cu far2_k*, pb2_pair.cu run_tile).  The
-  # relative truncation error must stay below 2e-8 there.
-  def val(u, k):
-    return sum(j / (2 * j + 1) * u ** (j - 1) for j in range(1, k + 1))
+def test_far_field_polynomials_meet_float32_bound():
+  # The pair kernels evaluate the OBC far-field series V(u) (descreening) and
+  # D(u) (chain rule) by the tier polynomials of pb2_obc_series.cuh, on tiles
+  # whose smallest box separation keeps u = (s/r)^2 below the tier's bound
+  # (pb2_api.cu tier2, pb2_pair.cu tile2_kernel).  With the float32
+  # coefficients the kernels use, the relative error against the full series
+  # must stay below half a float32 ulp in exact arithmetic, and below one ulp
+  # when evaluated by float32 Horner steps.
+  txt = (ROOT / "prolix_b200" / "csrc" / "pb2_obc_series.cuh").read_text()
 
-  def der(u, k):
-    return sum(2 * j * (j + 1) / (2 * j + 1) * u ** (j - 1) for j in range(1, k + 1))
+  def exact(u, der):
+    k = np.arange(1, 301, dtype=np.float64)[:, None]
+    c = 2.0 * k * (k + 1) / (2 * k + 1) if der else k / (2 * k + 1)
+    return (c * u[None, :] ** (k - 1)).sum(0)
 
-  for k, u in ((4, 0.0109), (6, 0.049), (8, 0.104), (10, 0.16)):
-    ev = (val(u, 400) - val(u, k)) / val(u, 400)
-    ed = (der(u, 400) - der(u, k + 1)) / der(u, 400)
-    assert 0 <= ev < 2e-8 and 0 <= ed < 2e-8, (k, u, ev, ed)
+  bounds = {}
+  for name, der in (("Value", False), ("Deriv", True)):
+    us = re.search(r"k%sTierU\[4\] = \{([^}]*)\}" % name, txt).group(1)
+    bounds[der] = [float(v) for v in us.split(",")]
+  assert bounds[False][3] == bounds[True][3] == 0.16  # the near-tile per-pair test bound
+  n_poly = 0
+  for m in re.finditer(r"struct ObcPoly<(true|false), (\d)> \{(.*?)\n\};", txt, re.S):
+    der, tier = m.group(1) == "true", int(m.group(2))
+    coef = [float(v) for v in re.findall(r"make_float2\(([-0-9.e+]+)f,", m.group(3))]
+    assert coef and all(np.float32(c) == c for c in coef)
+    u = np.linspace(0.0, bounds[der][tier], 20001)
+    ref = exact(u, der)
+    p64 = np.zeros_like(u)
+    p32 = np.zeros_like(u, dtype=np.float32)
+    u32 = u.astype(np.float32)
+    for c in coef:  # highest power first
+      p64 = p64 * u + c
+      p32 = (p32.astype(np.float64) * u32 + c).astype(np.float32)  # one rounding per step, as fma
+    assert np.max(np.abs(p64 - ref) / ref) < 6e-8, (der, tier)
+    assert np.max(np.abs(p32 - ref) / ref) < 1.2e-7, (der, tier)
+    n_poly += 1
+  assert n_poly == 8
 
 
 def test_exclusion_pairs_match_breadth_first_search():
