@@ -126,6 +126,9 @@ def parse():
   ap.add_argument("--no-plain", action="store_true")
   ap.add_argument("--no-cpu", action="store_true")
   ap.add_argument("--no-e2e", action="store_true")
+  ap.add_argument("--e2e-groups", type=lambda v: [int(x) for x in v.split(",")], default=[12],
+                  help="streams the end-to-end leg splits the systems over (comma list; the first "
+                       "is the reported value)")
   ap.add_argument("--no-serving", action="store_true")
   ap.add_argument("--no-extra", action="store_true",
                   help="skip the single-system, neighbour-list and serving-sweep legs")
@@ -520,26 +523,34 @@ def main():
   e2e = None
   if not args.no_e2e:
     # every step: positions, momenta and forces in from page-locked host
-    # buffers (pb2_set_full_state), one BAOAB step, and the same three arrays
-    # back out (pb2_get_state); timed on the host clock around the calls
-    fields = ("position", "momentum", "force")
-    host = {f: torch.empty((n_atoms, 3), dtype=torch.float64, pin_memory=True).numpy() for f in fields}
-    batch.get_state(fields=fields, out=host)
+    # buffers, one BAOAB step, and the same three arrays back out, through
+    # pb2_langevin_run_host; the systems are split into groups of
+    # consecutive systems, each a batch on its own stream, so that one
+    # group's copies overlap another's steps (prolix_b200.streamed).  Timed
+    # on the host clock around the calls, which return once every group's
+    # state is back in host memory.
+    from prolix_b200 import streamed
     e2e_steps = 10
-    for it in range(2 + e2e_steps):
-      if it == 2:
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-      batch.set_full_state(host["position"], host["momentum"], host["force"], stream=stream)
-      batch.langevin_run(1, stream)
-      batch.get_state(stream=stream, fields=fields, out=host)
-    torch.cuda.synchronize()
-    t_e2e = time.perf_counter() - t0
     nbytes = 3 * 3 * 8 * n_atoms
-    e2e = {"value": n_atoms * ws * e2e_steps / t_e2e, "unit": UNIT,
+    by_groups = {}
+    for g in args.e2e_groups:
+      with streamed.StreamedEnsemble(systems, groups=g, device=local) as ens:
+        ens.langevin_init()
+        host = ens.get_state()
+        ens.synchronize()
+        for it in range(2 + e2e_steps):
+          if it == 2:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+          ens.run_host(host["position"], host["momentum"], host["force"], 1)
+        t_e2e = time.perf_counter() - t0
+        by_groups[str(len(ens.batches))] = n_atoms * ws * e2e_steps / t_e2e
+    head = str(min(args.e2e_groups[0], len(systems)))
+    e2e = {"value": by_groups[head], "unit": UNIT,
            "h2d_bytes_per_step": int(nbytes), "d2h_bytes_per_step": int(nbytes),
-           "steps": e2e_steps, "host_buffers": "page-locked",
-           "path": "pb2_set_full_state + pb2_langevin_run(1) + pb2_get_state (x, p, F)"}
+           "steps": e2e_steps, "host_buffers": "page-locked", "groups": int(head),
+           "by_groups": by_groups,
+           "path": "pb2_langevin_run_host(1 step, x, p, F) per group of systems, one stream per group"}
   batch.close()
 
   plain = None

@@ -209,6 +209,21 @@ int pb2_set_state(pb2_batch *batch, const double *x, const double *p, const uint
 int pb2_set_full_state(pb2_batch *batch, const double *x, const double *p, const double *f,
                        const uint32_t *keys, void *stream);
 
+/* n_steps BAOAB steps on a state the caller keeps in host memory: the
+ * functional form of apply_fn (settle.py:1698-1744, state in, new state
+ * out).  x, p, f ((n_atoms_total, 3), f the forces at x as pb2_get_state
+ * returned them) are copied to the device on `copy_in`, stepped on
+ * `stream`, and copied back into the same arrays on `copy_out`; the rng
+ * keys and step counters stay on the device.  Pass `stream` three times to
+ * use one stream.  Nothing waits: the arrays hold the new state once
+ * `copy_out` has finished (cudaStreamSynchronize), and must not be touched
+ * before.  With page-locked arrays the copies are asynchronous: batches
+ * stepped on their own streams but sharing one copy_in and one copy_out
+ * stream move their states one after another at full PCIe speed while
+ * other batches compute. */
+int pb2_langevin_run_host(pb2_batch *batch, double *x, double *p, double *f, int32_t n_steps,
+                          void *stream, void *copy_in, void *copy_out);
+
 /*
  * Batched energy minimisation (replaces prolix batched_simulate.py:682-960,
  * `batched_minimize`, whose SD and FIRE stages run per system under vmap).

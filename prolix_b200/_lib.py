@@ -86,6 +86,9 @@ SIGNATURES = [
     ("pb2_get_state", ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_void_p] * 6),
     ("pb2_set_state", ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_void_p] * 4),
     ("pb2_set_full_state", ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_void_p] * 5),
+    ("pb2_langevin_run_host", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
+                                             ctypes.c_void_p, ctypes.c_void_p]),
     ("pb2_min_setup", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("pb2_min_sd", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_double, ctypes.c_int32,
                                   ctypes.c_double, ctypes.c_double, ctypes.c_void_p]),

@@ -463,7 +463,7 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   b->ro64 = D.alloc<double>(N);
   b->sr64 = D.alloc<double>(N);
   b->born64 = D.alloc<double>(N);
-  b->stage = D.alloc<double>(3 * (size_t)N);
+  b->stage = D.alloc<double>(9 * (size_t)N);  // x, p, F rows of a host round trip
   b->born_acc = D.alloc<long long>(N);
   b->dedb_acc = D.alloc<long long>(N);
   b->energy = D.alloc<long long>((size_t)n_systems * PB2_NTERMS);
@@ -539,6 +539,7 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   CUDA_TRY(ctx, cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking));
   CUDA_TRY(ctx, cudaEventCreate(&b->ev[0]));
   CUDA_TRY(ctx, cudaEventCreate(&b->ev[1]));
+  for (auto &e : b->ev_io) CUDA_TRY(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   CUDA_TRY(ctx, cudaDeviceSynchronize());
   *out = b.release();
   return PB2_OK;
@@ -939,6 +940,40 @@ extern "C" int pb2_set_full_state(pb2_batch *b, const double *x, const double *p
   return PB2_OK;
 }
 
+
+extern "C" int pb2_langevin_run_host(pb2_batch *b, double *x, double *p, double *f, int32_t n_steps,
+                                     void *stream, void *copy_in, void *copy_out) {
+  if (!b || !x || !p || !f || n_steps < 0) return PB2_EINVAL;
+  pb2_ctx *ctx = b->ctx;
+  cudaStream_t st = (cudaStream_t)stream, ci = (cudaStream_t)copy_in, co = (cudaStream_t)copy_out;
+  const int N = b->n_total;
+  const size_t rows = 3 * (size_t)N, bytes = rows * sizeof(double);
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  // in: the previous round trip's copies out of the staging buffer are done;
+  // the three copies back to back, then one conversion
+  CUDA_TRY(ctx, cudaStreamWaitEvent(ci, b->ev_io[2], 0));
+  CUDA_TRY(ctx, cudaMemcpyAsync(b->stage, x, bytes, cudaMemcpyHostToDevice, ci));
+  CUDA_TRY(ctx, cudaMemcpyAsync(b->stage + rows, p, bytes, cudaMemcpyHostToDevice, ci));
+  CUDA_TRY(ctx, cudaMemcpyAsync(b->stage + 2 * rows, f, bytes, cudaMemcpyHostToDevice, ci));
+  CUDA_TRY(ctx, cudaEventRecord(b->ev_io[0], ci));
+  CUDA_TRY(ctx, cudaStreamWaitEvent(st, b->ev_io[0], 0));
+  CUDA_TRY(ctx, launch_state_from_rows(b->stage, b->x, b->y, b->z, b->px, b->py, b->pz, b->fx, b->fy, b->fz,
+                                       N, st));
+  CUDA_TRY(ctx, launch_posq(int_args(b, b->key_parity, 0), st));
+  b->forces_valid = true;
+  int rc = pb2_langevin_run(b, n_steps, stream);
+  if (rc) return rc;
+  // out: one conversion, then the three copies
+  CUDA_TRY(ctx, launch_state_to_rows(b->x, b->y, b->z, b->px, b->py, b->pz, b->fx, b->fy, b->fz, b->stage,
+                                     N, st));
+  CUDA_TRY(ctx, cudaEventRecord(b->ev_io[1], st));
+  CUDA_TRY(ctx, cudaStreamWaitEvent(co, b->ev_io[1], 0));
+  CUDA_TRY(ctx, cudaMemcpyAsync(x, b->stage, bytes, cudaMemcpyDeviceToHost, co));
+  CUDA_TRY(ctx, cudaMemcpyAsync(p, b->stage + rows, bytes, cudaMemcpyDeviceToHost, co));
+  CUDA_TRY(ctx, cudaMemcpyAsync(f, b->stage + 2 * rows, bytes, cudaMemcpyDeviceToHost, co));
+  CUDA_TRY(ctx, cudaEventRecord(b->ev_io[2], co));
+  return PB2_OK;
+}
 
 // ------------------------------------------------------------ minimisation
 

@@ -76,7 +76,7 @@ struct pb2_batch {
   int n_blocks = 0;
   double *q64 = nullptr, *hs64 = nullptr, *se64 = nullptr, *ro64 = nullptr, *sr64 = nullptr;
   double *born64 = nullptr;
-  double *stage = nullptr;  // (n_total, 3) row-major staging for host transfers
+  double *stage = nullptr;  // 3 x (n_total, 3) row-major staging for host transfers
   int32_t *d_perm = nullptr;  // system permutation (replica exchange)
   // trajectory ring: capacity frames of float32 (n, 3) positions and
   // velocities, and the step counters of every system
@@ -104,6 +104,9 @@ struct pb2_batch {
   bool profiling = false;
   double timings[kTimSlots] = {0, 0, 0, 0, 0, 0, 0, 0};
   cudaEvent_t ev[2] = {nullptr, nullptr};
+  // host round trips on separate copy streams: copies in done, steps done,
+  // copies out done
+  cudaEvent_t ev_io[3] = {nullptr, nullptr, nullptr};
   // minimiser state (allocated by pb2_min_setup)
   Dev mdev;
   bool min_ready = false;
@@ -135,6 +138,8 @@ struct pb2_batch {
     for (auto &kv : min_graphs) cudaGraphExecDestroy(kv.second);
     if (cap_stream) cudaStreamDestroy(cap_stream);
     for (auto &e : ev)
+      if (e) cudaEventDestroy(e);
+    for (auto &e : ev_io)
       if (e) cudaEventDestroy(e);
   }
 };

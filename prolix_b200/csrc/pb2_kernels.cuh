@@ -174,6 +174,12 @@ cudaError_t launch_soa_to_rows(const double *x, const double *y, const double *z
                                cudaStream_t st);
 cudaError_t launch_fix_to_rows(const long long *fx, const long long *fy, const long long *fz, double *rows,
                                int n, cudaStream_t st);
+cudaError_t launch_state_from_rows(const double *rows, double *x, double *y, double *z, double *px, double *py,
+                                   double *pz, long long *fx, long long *fy, long long *fz, int n,
+                                   cudaStream_t st);
+cudaError_t launch_state_to_rows(const double *x, const double *y, const double *z, const double *px,
+                                 const double *py, const double *pz, const long long *fx, const long long *fy,
+                                 const long long *fz, double *rows, int n, cudaStream_t st);
 cudaError_t launch_rows_to_fix(const double *rows, long long *fx, long long *fy, long long *fz, int n,
                                cudaStream_t st);
 cudaError_t launch_energies_to_double(const long long *e, double *out, int n_sys, cudaStream_t st);

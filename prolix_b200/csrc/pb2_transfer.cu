@@ -94,6 +94,36 @@ __global__ void snapshot_frame(const double *__restrict__ x, const double *__res
     frame_steps[s] = steps[s];
 }
 
+// The whole BAOAB state (x, p, F) from three consecutive (n, 3) row arrays
+// in one pass, and back: one launch on each side of a host round trip, so
+// that the three copies of each direction run back to back.
+__global__ void state_from_rows(const double *__restrict__ rows, double *x, double *y, double *z, double *px,
+                                double *py, double *pz, long long *fx, long long *fy, long long *fz, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double *r = rows + 3 * (size_t)i;
+    const double *q = rows + 3 * ((size_t)n + i);
+    const double *f = rows + 3 * (2 * (size_t)n + i);
+    x[i] = r[0]; y[i] = r[1]; z[i] = r[2];
+    px[i] = q[0]; py[i] = q[1]; pz[i] = q[2];
+    fx[i] = to_fix(f[0], kForceScale); fy[i] = to_fix(f[1], kForceScale); fz[i] = to_fix(f[2], kForceScale);
+  }
+}
+
+__global__ void state_to_rows(const double *__restrict__ x, const double *__restrict__ y,
+                              const double *__restrict__ z, const double *__restrict__ px,
+                              const double *__restrict__ py, const double *__restrict__ pz,
+                              const long long *__restrict__ fx, const long long *__restrict__ fy,
+                              const long long *__restrict__ fz, double *rows, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double *r = rows + 3 * (size_t)i;
+    double *q = rows + 3 * ((size_t)n + i);
+    double *f = rows + 3 * (2 * (size_t)n + i);
+    r[0] = x[i]; r[1] = y[i]; r[2] = z[i];
+    q[0] = px[i]; q[1] = py[i]; q[2] = pz[i];
+    f[0] = (double)fx[i] * kForceInv; f[1] = (double)fy[i] * kForceInv; f[2] = (double)fz[i] * kForceInv;
+  }
+}
+
 static int grid_for(int n) {
   const int g = (n + 255) / 256;
   return g < 1 ? 1 : (g > 4096 ? 4096 : g);
@@ -138,6 +168,22 @@ cudaError_t launch_snapshot(const double *x, const double *y, const double *z, c
                             float *pos, float *vel, long long *frame_steps, int n, int n_sys, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
   snapshot_frame<<<grid_for(n), 256, 0, st>>>(x, y, z, px, py, pz, mass, steps, pos, vel, frame_steps, n, n_sys);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_state_from_rows(const double *rows, double *x, double *y, double *z, double *px, double *py,
+                                   double *pz, long long *fx, long long *fy, long long *fz, int n,
+                                   cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  state_from_rows<<<grid_for(n), 256, 0, st>>>(rows, x, y, z, px, py, pz, fx, fy, fz, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_state_to_rows(const double *x, const double *y, const double *z, const double *px,
+                                 const double *py, const double *pz, const long long *fx, const long long *fy,
+                                 const long long *fz, double *rows, int n, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  state_to_rows<<<grid_for(n), 256, 0, st>>>(x, y, z, px, py, pz, fx, fy, fz, rows, n);
   return cudaGetLastError();
 }
 

@@ -293,6 +293,23 @@ class Batch:
     self._check(self.lib.pb2_set_full_state(self.handle, x.ctypes.data, p.ctypes.data, f.ctypes.data,
                                             None if k is None else k.ctypes.data, stream))
 
+  def langevin_run_host(self, position, momentum, force, n_steps, stream=None, copy_in=None, copy_out=None):
+    """pb2_langevin_run_host: step the state held in the three (n_atoms, 3)
+    float64 arrays and write the new state back into them.  Asynchronous:
+    copies in on ``copy_in``, steps on ``stream``, copies out on
+    ``copy_out`` (each defaults to ``stream``); the arrays must stay alive
+    and untouched until ``copy_out`` has finished.  Page-locked arrays let
+    the copies overlap other streams' work."""
+    copy_in = stream if copy_in is None else copy_in
+    copy_out = stream if copy_out is None else copy_out
+    arrs = (position, momentum, force)
+    for a in arrs:
+      if (not isinstance(a, np.ndarray) or a.shape != (self.n_atoms, 3) or a.dtype != np.float64
+          or not a.flags.c_contiguous or not a.flags.writeable):
+        raise ValueError(f"langevin_run_host: arrays must be writeable C-contiguous float64 ({self.n_atoms}, 3)")
+    self._check(self.lib.pb2_langevin_run_host(self.handle, position.ctypes.data, momentum.ctypes.data,
+                                               force.ctypes.data, int(n_steps), stream, copy_in, copy_out))
+
   def energy_forces_device(self, positions_ptr, energies_ptr, forces_ptr, stream=None):
     """pb2_energy_forces_device on raw device pointers (e.g. a torch tensor's
     data_ptr()); any may be 0/None.  Asynchronous on ``stream``."""

@@ -226,3 +226,16 @@ def test_exclusion_finder_rejects_bad_bond_indices():
     topology.exclusion_pairs(np.array([[0, 1], [2, 5]]), 5)
   with pytest.raises(ValueError, match="out of range"):
     topology.exclusion_pairs(np.array([[-1, 1]]), 5)
+
+
+def test_streamed_partition_covers_systems_in_balanced_ranges():
+  from prolix_b200 import streamed
+  rng = np.random.default_rng(5)
+  sizes = np.exp(rng.uniform(np.log(150), np.log(4000), 512)).astype(int)
+  r = streamed.partition(sizes, 4)
+  assert r[0][0] == 0 and r[-1][1] == len(sizes)
+  assert all(a < b for a, b in r) and all(r[g][1] == r[g + 1][0] for g in range(len(r) - 1))
+  work = [float(np.sum(sizes[a:b].astype(float) ** 2)) for a, b in r]
+  assert max(work) / min(work) < 1.2
+  assert streamed.partition([10, 20], 5) == [(0, 1), (1, 2)]
+  assert streamed.partition([10], 3) == [(0, 1)]
