@@ -135,6 +135,8 @@ def parse():
   ap.add_argument("--serving-requests", type=int, default=32)
   ap.add_argument("--serving-rate", type=float, default=20.0)
   ap.add_argument("--serving-step-scale", type=float, default=0.05)
+  ap.add_argument("--keep-atom-order", action="store_true",
+                  help="store atoms in input order instead of the default spatial order")
   ap.add_argument("--segment", type=int, default=0,
                   help="tile work-item segment; 0 runs the autotuner")
   return ap.parse_args()
@@ -460,7 +462,7 @@ def main():
   systems = workload(rank, args.systems)
   n_atoms = int(sum(len(s["charges"]) for s in systems))
   pairs = unique_pairs(systems)
-  batch = engine.Batch(systems, device=local)
+  batch = engine.Batch(systems, device=local, keep_atom_order=args.keep_atom_order)
   batch.langevin_init()
   stream = torch.cuda.current_stream().cuda_stream
 

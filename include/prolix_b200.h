@@ -138,6 +138,10 @@ typedef struct pb2_run_params {
   double born_cutoff;   /* A; > 0: descreening sums and their chain rule only (the NL-Born +
                            dense-GB split, generalized_born.py:706-817); the GB pair terms keep
                            gb_cutoff.  <= 0: the descreening uses gb_cutoff too */
+  int32_t keep_atom_order; /* 0: the batch stores each system's atoms in a spatial order
+                              (compact 32-atom blocks, which the pair kernels' bounding-box
+                              tests favour); 1: in input order.  Either way every array
+                              crossing this interface is in input order. */
 } pb2_run_params;
 
 typedef struct pb2_ctx pb2_ctx;

@@ -63,6 +63,7 @@ class RunParams(ctypes.Structure):
       ("partitionable_keys", ctypes.c_int32),
       ("gb_cutoff", ctypes.c_double),
       ("born_cutoff", ctypes.c_double),
+      ("keep_atom_order", ctypes.c_int32),
   ]
 
 

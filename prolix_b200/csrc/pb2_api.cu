@@ -94,6 +94,7 @@ static IntArgs int_args(pb2_batch *b, int parity, int finish_prev) {
   IntArgs a;
   a.sys = b->sys;
   a.atom_sys = b->atom_sys;
+  a.user = b->user;
   a.x = b->x; a.y = b->y; a.z = b->z;
   a.px = b->px; a.py = b->py; a.pz = b->pz;
   a.fx = b->fx; a.fy = b->fy; a.fz = b->fz;
@@ -117,6 +118,44 @@ IntArgs int_args_for_nl(pb2_batch *b) { return int_args(b, b->key_parity, 0); }
 // Tile work items: for each system and i-block, its tiles (iblk, jb >= iblk)
 // cut into segments of `seg` tiles; sorted by tile count, largest first
 // (the kernels hand them out dynamically).
+// Spatial order of one system's atoms: recursive bisection of the input
+// positions along the longest side of their bounding box, cut at a multiple
+// of 32 atoms near the middle, so that every 32-atom block is a compact
+// cluster (smaller block boxes: more tile pairs in the far field and beyond
+// cutoffs).  Ties go by input index, so the order depends on the positions
+// alone.  ord[l] = input index of the atom stored at l.  Non-finite
+// positions keep the input order.
+static void spatial_order(const double *pos, int n, std::vector<int> &ord) {
+  ord.resize(n);
+  for (int i = 0; i < n; ++i) ord[i] = i;
+  for (int i = 0; i < 3 * n; ++i)
+    if (!std::isfinite(pos[i])) return;
+  std::vector<std::pair<int, int>> todo{{0, n}};
+  while (!todo.empty()) {
+    const auto [a, e] = todo.back();
+    todo.pop_back();
+    if (e - a <= 32) continue;
+    double lo[3] = {pos[3 * ord[a]], pos[3 * ord[a] + 1], pos[3 * ord[a] + 2]};
+    double hi[3] = {lo[0], lo[1], lo[2]};
+    for (int k = a; k < e; ++k)
+      for (int c = 0; c < 3; ++c) {
+        lo[c] = std::min(lo[c], pos[3 * ord[k] + c]);
+        hi[c] = std::max(hi[c], pos[3 * ord[k] + c]);
+      }
+    int ax = 0;
+    for (int c = 1; c < 3; ++c)
+      if (hi[c] - lo[c] > hi[ax] - lo[ax]) ax = c;
+    std::sort(ord.begin() + a, ord.begin() + e, [&](int i, int j) {
+      const double ci = pos[3 * i + ax], cj = pos[3 * j + ax];
+      return ci < cj || (ci == cj && i < j);
+    });
+    const int half = (e - a) / 2;
+    const int m = a + std::max(32, std::min((half + 16) / 32 * 32, (e - a - 1) / 32 * 32));
+    todo.push_back({a, m});
+    todo.push_back({m, e});
+  }
+}
+
 static std::vector<TileItem> build_items(const std::vector<SysInfo> &sinfo, int seg) {
   std::vector<TileItem> items;
   for (int s = 0; s < (int)sinfo.size(); ++s) {
@@ -276,6 +315,9 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   std::vector<float4> hposq(N), hpar(N);
   std::vector<double> hhs(N), hse(N), hro(N), hsr(N);
   std::vector<int32_t> hsys(N);
+  b->user_host.resize(N);
+  b->dev_host.resize(N);
+  std::vector<std::vector<int>> inv_all(n_systems);  // per system: input index -> stored index
   std::vector<SysInfo> sinfo(n_systems);
   std::vector<uint32_t> hkeys(4 * (size_t)n_systems, 0u);
   std::vector<int2> hent((size_t)blocks_total * kExclPerBlock, make_int2(-1, -1));
@@ -323,8 +365,63 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
       S.oy = d.origin[1];
       S.oz = d.origin[2];
     }
-    for (int i = 0; i < n; ++i) {
-      const int g = o + i;
+    // atom order: spatial unless asked to keep the input order, or unless
+    // the spatial order gives an i-block exclusion partners in more j-blocks
+    // than the exclusion table holds
+    std::vector<int> ord;
+    std::vector<int> &inv = inv_all[s];
+    inv.resize(n);
+    const size_t rows_before = hrows.size();
+    int2 *ent_sys = &hent[(size_t)blk_base * kExclPerBlock];
+    auto build_excl = [&]() -> int {  // -1: fits; else the i-block that overflows
+      for (size_t e = 0; e < (size_t)S.nblk * kExclPerBlock; ++e) ent_sys[e] = make_int2(-1, -1);
+      hrows.resize(rows_before);
+      for (int k = 0; k < d.n_excl; ++k) {
+        const int p = inv[d.excl_pairs[2 * k]], q = inv[d.excl_pairs[2 * k + 1]];
+        const int i = std::min(p, q), j = std::max(p, q);
+        const int ib = i >> 5, jb = j >> 5;
+        int2 *ent = ent_sys + (size_t)ib * kExclPerBlock;
+        int slot = -1;
+        for (int e = 0; e < kExclPerBlock; ++e) {
+          if (ent[e].x == jb) { slot = e; break; }
+          if (ent[e].x < 0) {
+            ent[e] = make_int2(jb, (int)hrows.size());
+            hrows.resize(hrows.size() + 32, ExclRow{0u, 0u});
+            slot = e;
+            break;
+          }
+        }
+        if (slot < 0) return ib;
+        ExclRow &row = hrows[ent[slot].y + (i & 31)];
+        if (d.excl_kind[k] == 0) row.excl |= 1u << (j & 31);
+        else row.s14 |= 1u << (j & 31);
+      }
+      return -1;
+    };
+    if (params->keep_atom_order) {
+      ord.resize(n);
+      for (int i = 0; i < n; ++i) ord[i] = i;
+    } else {
+      spatial_order(d.positions, n, ord);
+    }
+    for (int l = 0; l < n; ++l) inv[ord[l]] = l;
+    int over = build_excl();
+    if (over >= 0 && !params->keep_atom_order) {
+      for (int l = 0; l < n; ++l) ord[l] = inv[l] = l;
+      over = build_excl();
+    }
+    if (over >= 0) {
+      char buf[200];
+      snprintf(buf, sizeof buf,
+               "system %d: atoms %d..%d have exclusion partners in more than %d 32-atom blocks",
+               s, over * 32, over * 32 + 31, kExclPerBlock);
+      return fail(ctx, PB2_EINVAL, buf);
+    }
+    for (int l = 0; l < n; ++l) {
+      const int i = ord[l];
+      const int g = o + l;
+      b->user_host[g] = o + i;
+      b->dev_host[o + i] = g;
       hx[g] = d.positions[3 * i];
       hy[g] = d.positions[3 * i + 1];
       hz[g] = d.positions[3 * i + 2];
@@ -364,32 +461,6 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
     for (int bk = 0; bk < S.nblk; ++bk) hblk_sys[blk_base + bk] = s;
     hkeys[2 * (size_t)s] = d.key[0];
     hkeys[2 * (size_t)s + 1] = d.key[1];
-    // exclusion masks, one 32-row block per (i-block, j-block) with exclusions
-    for (int k = 0; k < d.n_excl; ++k) {
-      const int i = d.excl_pairs[2 * k], j = d.excl_pairs[2 * k + 1];
-      const int ib = i >> 5, jb = j >> 5;
-      int2 *ent = &hent[(size_t)(blk_base + ib) * kExclPerBlock];
-      int slot = -1;
-      for (int e = 0; e < kExclPerBlock; ++e) {
-        if (ent[e].x == jb) { slot = e; break; }
-        if (ent[e].x < 0) {
-          ent[e] = make_int2(jb, (int)hrows.size());
-          hrows.resize(hrows.size() + 32, ExclRow{0u, 0u});
-          slot = e;
-          break;
-        }
-      }
-      if (slot < 0) {
-        char buf[200];
-        snprintf(buf, sizeof buf,
-                 "system %d: atoms %d..%d have exclusion partners in more than %d 32-atom blocks",
-                 s, ib * 32, ib * 32 + 31, kExclPerBlock);
-        return fail(ctx, PB2_EINVAL, buf);
-      }
-      ExclRow &row = hrows[ent[slot].y + (i & 31)];
-      if (d.excl_kind[k] == 0) row.excl |= 1u << (j & 31);
-      else row.s14 |= 1u << (j & 31);
-    }
     blk_base += S.nblk;
   }
   hitems = build_items(sinfo, b->params.tile_segment);
@@ -410,19 +481,21 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   for (int s = 0; s < n_systems; ++s) {
     const pb2_system_desc &d = systems[s];
     const int o = b->off[s];
+    const std::vector<int> &inv = inv_all[s];
+    auto at = [&](int32_t i) { return o + inv[i]; };  // stored batch index of input atom i
     for (int k = 0; k < d.n_bonds; ++k) {
-      bidx.push_back(make_int2(o + d.bonds[2 * k], o + d.bonds[2 * k + 1]));
+      bidx.push_back(make_int2(at(d.bonds[2 * k]), at(d.bonds[2 * k + 1])));
       bpar.push_back(make_double2(d.bond_params[2 * k], d.bond_params[2 * k + 1]));
     }
     for (int k = 0; k < d.n_angles; ++k) {
-      aidx.push_back(make_int4(o + d.angles[3 * k], o + d.angles[3 * k + 1], o + d.angles[3 * k + 2], 0));
+      aidx.push_back(make_int4(at(d.angles[3 * k]), at(d.angles[3 * k + 1]), at(d.angles[3 * k + 2]), 0));
       apar.push_back(make_double2(d.angle_params[2 * k], d.angle_params[2 * k + 1]));
     }
     for (int k = 0; k < d.n_torsions; ++k)
       for (int t = 0; t < d.n_torsion_terms; ++t) {
         const double *p = d.torsion_params + ((size_t)k * d.n_torsion_terms + t) * 3;
-        tidx.push_back(make_int4(o + d.torsions[4 * k], o + d.torsions[4 * k + 1],
-                                 o + d.torsions[4 * k + 2], o + d.torsions[4 * k + 3]));
+        tidx.push_back(make_int4(at(d.torsions[4 * k]), at(d.torsions[4 * k + 1]),
+                                 at(d.torsions[4 * k + 2]), at(d.torsions[4 * k + 3])));
         tpar.push_back(make_double4(p[0], p[1], p[2], 0.0));
       }
     const int map_base = (int)cgrid.size();
@@ -433,7 +506,7 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
       ccoef.insert(ccoef.end(), d.cmap_coeffs + m * per_map, d.cmap_coeffs + (m + 1) * per_map);
     }
     for (int k = 0; k < d.n_cmap; ++k) {
-      for (int c = 0; c < 5; ++c) cidx.push_back(o + d.cmap_rows[5 * k + c]);
+      for (int c = 0; c < 5; ++c) cidx.push_back(at(d.cmap_rows[5 * k + c]));
       cidx.push_back(map_base + d.cmap_map[k]);
     }
   }
@@ -464,6 +537,8 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   b->sr64 = D.alloc<double>(N);
   b->born64 = D.alloc<double>(N);
   b->stage = D.alloc<double>(9 * (size_t)N);  // x, p, F rows of a host round trip
+  b->user = D.alloc<int32_t>(N);
+  b->devidx = D.alloc<int32_t>(N);
   b->born_acc = D.alloc<long long>(N);
   b->dedb_acc = D.alloc<long long>(N);
   b->energy = D.alloc<long long>((size_t)n_systems * PB2_NTERMS);
@@ -501,7 +576,8 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
       (rc = upload(ctx, b->posq, hposq)) || (rc = upload(ctx, b->par, hpar)) ||
       (rc = upload(ctx, b->q64, hq)) || (rc = upload(ctx, b->hs64, hhs)) ||
       (rc = upload(ctx, b->se64, hse)) || (rc = upload(ctx, b->ro64, hro)) ||
-      (rc = upload(ctx, b->sr64, hsr)) ||
+      (rc = upload(ctx, b->sr64, hsr)) || (rc = upload(ctx, b->user, b->user_host)) ||
+      (rc = upload(ctx, b->devidx, b->dev_host)) ||
       (rc = upload(ctx, b->keys, hkeys)) || (rc = upload(ctx, b->blk_sys, hblk_sys)) || (rc = upload(ctx, b->items, hitems)) ||
       (rc = upload(ctx, b->excl_ent, hent)) || (rc = upload(ctx, b->excl_rows, hrows)) ||
       (rc = upload(ctx, d_bidx, bidx)) || (rc = upload(ctx, d_bpar, bpar)) ||
@@ -674,7 +750,7 @@ static int fresh_forces(pb2_batch *b, cudaStream_t st, bool energy) {
 static int copy_forces(pb2_batch *b, double *forces, cudaStream_t st) {
   pb2_ctx *ctx = b->ctx;
   const int N = b->n_total;
-  CUDA_TRY(ctx, launch_fix_to_rows(b->fx, b->fy, b->fz, b->stage, N, st));
+  CUDA_TRY(ctx, launch_fix_to_rows(b->fx, b->fy, b->fz, b->user, b->stage, N, st));
   CUDA_TRY(ctx, cudaMemcpyAsync(forces, b->stage, 3 * (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, st));
   CUDA_TRY(ctx, cudaStreamSynchronize(st));
   return PB2_OK;
@@ -690,12 +766,12 @@ extern "C" int pb2_energy_forces_device(pb2_batch *b, const double *positions, d
   const size_t N = b->n_total;
   if (positions) {
     CUDA_TRY(ctx, cudaMemcpyAsync(b->stage, positions, 3 * N * sizeof(double), cudaMemcpyDeviceToDevice, st));
-    CUDA_TRY(ctx, launch_rows_to_soa(b->stage, b->x, b->y, b->z, b->n_total, st));
+    CUDA_TRY(ctx, launch_rows_to_soa(b->stage, b->user, b->x, b->y, b->z, b->n_total, st));
   }
   int rc = fresh_forces(b, st, energies != nullptr);
   if (rc) return rc;
   if (energies) CUDA_TRY(ctx, launch_energies_to_double(b->energy, energies, b->n_sys, st));
-  if (forces) CUDA_TRY(ctx, launch_fix_to_rows(b->fx, b->fy, b->fz, forces, b->n_total, st));
+  if (forces) CUDA_TRY(ctx, launch_fix_to_rows(b->fx, b->fy, b->fz, b->user, forces, b->n_total, st));
   return PB2_OK;
 }
 
@@ -735,7 +811,7 @@ extern "C" int pb2_born_radii(pb2_batch *b, double *out, void *stream) {
   std::vector<float4> hb(b->n_total);
   CUDA_TRY(ctx, cudaMemcpyAsync(hb.data(), b->born, hb.size() * sizeof(float4), cudaMemcpyDeviceToHost, st));
   CUDA_TRY(ctx, cudaStreamSynchronize(st));
-  for (int i = 0; i < b->n_total; ++i) out[i] = (double)hb[i].x;
+  for (int g = 0; g < b->n_total; ++g) out[b->user_host[g]] = (double)hb[g].x;
   return PB2_OK;
 }
 
@@ -747,7 +823,7 @@ static int upload_soa3(pb2_batch *b, const double *aos, double *dx, double *dy, 
   pb2_ctx *ctx = b->ctx;
   const int N = b->n_total;
   CUDA_TRY(ctx, cudaMemcpyAsync(b->stage, aos, 3 * (size_t)N * sizeof(double), cudaMemcpyHostToDevice, st));
-  CUDA_TRY(ctx, launch_rows_to_soa(b->stage, dx, dy, dz, N, st));
+  CUDA_TRY(ctx, launch_rows_to_soa(b->stage, b->user, dx, dy, dz, N, st));
   return PB2_OK;
 }
 
@@ -755,7 +831,7 @@ static int download_soa3(pb2_batch *b, double *aos, const double *dx, const doub
                          cudaStream_t st) {
   pb2_ctx *ctx = b->ctx;
   const int N = b->n_total;
-  CUDA_TRY(ctx, launch_soa_to_rows(dx, dy, dz, b->stage, N, st));
+  CUDA_TRY(ctx, launch_soa_to_rows(dx, dy, dz, b->user, b->stage, N, st));
   CUDA_TRY(ctx, cudaMemcpyAsync(aos, b->stage, 3 * (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, st));
   CUDA_TRY(ctx, cudaStreamSynchronize(st));
   return PB2_OK;
@@ -929,7 +1005,7 @@ extern "C" int pb2_set_full_state(pb2_batch *b, const double *x, const double *p
   if ((rc = upload_soa3(b, x, b->x, b->y, b->z, st))) return rc;
   if ((rc = upload_soa3(b, p, b->px, b->py, b->pz, st))) return rc;
   CUDA_TRY(ctx, cudaMemcpyAsync(b->stage, f, 3 * (size_t)b->n_total * sizeof(double), cudaMemcpyHostToDevice, st));
-  CUDA_TRY(ctx, launch_rows_to_fix(b->stage, b->fx, b->fy, b->fz, b->n_total, st));
+  CUDA_TRY(ctx, launch_rows_to_fix(b->stage, b->user, b->fx, b->fy, b->fz, b->n_total, st));
   if (keys) {
     CUDA_TRY(ctx, cudaMemcpyAsync(b->keys + (size_t)b->key_parity * b->n_sys * 2, keys,
                                   (size_t)b->n_sys * 2 * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
@@ -957,15 +1033,15 @@ extern "C" int pb2_langevin_run_host(pb2_batch *b, double *x, double *p, double 
   CUDA_TRY(ctx, cudaMemcpyAsync(b->stage + 2 * rows, f, bytes, cudaMemcpyHostToDevice, ci));
   CUDA_TRY(ctx, cudaEventRecord(b->ev_io[0], ci));
   CUDA_TRY(ctx, cudaStreamWaitEvent(st, b->ev_io[0], 0));
-  CUDA_TRY(ctx, launch_state_from_rows(b->stage, b->x, b->y, b->z, b->px, b->py, b->pz, b->fx, b->fy, b->fz,
+  CUDA_TRY(ctx, launch_state_from_rows(b->stage, b->user, b->x, b->y, b->z, b->px, b->py, b->pz, b->fx, b->fy, b->fz,
                                        N, st));
   CUDA_TRY(ctx, launch_posq(int_args(b, b->key_parity, 0), st));
   b->forces_valid = true;
   int rc = pb2_langevin_run(b, n_steps, stream);
   if (rc) return rc;
   // out: one conversion, then the three copies
-  CUDA_TRY(ctx, launch_state_to_rows(b->x, b->y, b->z, b->px, b->py, b->pz, b->fx, b->fy, b->fz, b->stage,
-                                     N, st));
+  CUDA_TRY(ctx, launch_state_to_rows(b->x, b->y, b->z, b->px, b->py, b->pz, b->fx, b->fy, b->fz, b->user,
+                                     b->stage, N, st));
   CUDA_TRY(ctx, cudaEventRecord(b->ev_io[1], st));
   CUDA_TRY(ctx, cudaStreamWaitEvent(co, b->ev_io[1], 0));
   CUDA_TRY(ctx, cudaMemcpyAsync(x, b->stage, bytes, cudaMemcpyDeviceToHost, co));
@@ -1024,10 +1100,11 @@ extern "C" int pb2_min_setup(pb2_batch *b, const uint8_t *heavy, const uint8_t *
   std::vector<double> hm(N);
   CUDA_TRY(ctx, cudaMemcpy(hm.data(), b->mass, N * sizeof(double), cudaMemcpyDeviceToHost));
   std::vector<uint8_t> sel(N);
-  for (size_t i = 0; i < N; ++i) {
-    const bool h = heavy ? heavy[i] != 0 : hm[i] > 1.1;
-    const bool bb = backbone ? backbone[i] != 0 : h;
-    sel[i] = (uint8_t)((h ? 1 : 0) | (bb ? 2 : 0));
+  for (size_t g = 0; g < N; ++g) {  // heavy, backbone: caller's atom order
+    const int32_t u = b->user_host[g];
+    const bool h = heavy ? heavy[u] != 0 : hm[g] > 1.1;
+    const bool bb = backbone ? backbone[u] != 0 : h;
+    sel[g] = (uint8_t)((h ? 1 : 0) | (bb ? 2 : 0));
   }
   CUDA_TRY(ctx, cudaMemcpy(b->m_sel, sel.data(), N, cudaMemcpyHostToDevice));
   CUDA_TRY(ctx, cudaMemcpy(b->m_x0, b->x, N * sizeof(double), cudaMemcpyDeviceToDevice));
@@ -1269,7 +1346,8 @@ extern "C" int pb2_permute_systems(pb2_batch *b, const int32_t *perm, void *stre
   void *groups[3][3] = {{b->x, b->y, b->z}, {b->px, b->py, b->pz}, {b->fx, b->fy, b->fz}};
   for (auto &g : groups) {
     for (int c = 0; c < 3; ++c)
-      CUDA_TRY(ctx, launch_gather_systems(b->sys, b->atom_sys, b->d_perm, g[c], b->stage + c * N, b->n_total, st));
+      CUDA_TRY(ctx, launch_gather_systems(b->sys, b->atom_sys, b->d_perm, b->user, b->devidx, g[c], b->stage + c * N,
+                                            b->n_total, st));
     for (int c = 0; c < 3; ++c)
       CUDA_TRY(ctx, cudaMemcpyAsync(g[c], b->stage + c * N, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
   }
@@ -1309,7 +1387,7 @@ extern "C" int pb2_traj_snapshot(pb2_batch *b, int32_t slot, void *stream) {
   pb2_ctx *ctx = b->ctx;
   if (slot < 0 || slot >= b->traj_cap) return fail(ctx, PB2_EINVAL, "trajectory slot out of range");
   const size_t f = 3 * (size_t)b->n_total;
-  CUDA_TRY(ctx, launch_snapshot(b->x, b->y, b->z, b->px, b->py, b->pz, b->mass, b->steps,
+  CUDA_TRY(ctx, launch_snapshot(b->x, b->y, b->z, b->px, b->py, b->pz, b->mass, b->steps, b->user,
                                 b->traj_pos + slot * f, b->traj_vel + slot * f,
                                 b->traj_steps + (size_t)slot * b->n_sys, b->n_total, b->n_sys,
                                 (cudaStream_t)stream));

@@ -29,7 +29,7 @@ constexpr double kObcAlpha = 1.0, kObcBeta = 0.8, kObcGamma = 4.85;
 constexpr double kDielOffset = 0.09;
 constexpr double kAceCoeff = 28.3919551, kKjToKcal = 0.239006;
 
-constexpr int kExclPerBlock = 8;  // distinct j-blocks with exclusions per i-block
+constexpr int kExclPerBlock = 16;  // distinct j-blocks with exclusions per i-block
 
 // Per-system constants, one 168-byte record per system.  Pair kernels see
 // positions relative to the system origin (its initial centroid), which keeps

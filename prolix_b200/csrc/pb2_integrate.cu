@@ -39,6 +39,7 @@ __global__ void step_kernel(const IntArgs a) {
     const int s = a.atom_sys[i];
     const SysInfo &S = a.sys[s];
     const int loc = i - S.off;
+    const int rnd = a.user[i] - S.off;  // the atom's index in the caller's order: its noise
     const double h = S.half_dt;
     const double m = a.mass[i];
     const long long lfx = a.fx[i], lfy = a.fy[i], lfz = a.fz[i];
@@ -57,7 +58,7 @@ __global__ void step_kernel(const IntArgs a) {
       if (a.finish_prev) p[c] = __dadd_rn(p[c], __dmul_rn(h, f[c]));
       p[c] = __dadd_rn(p[c], __dmul_rn(h, f[c]));
       x[c] = __dadd_rn(x[c], __dmul_rn(h, __ddiv_rn(p[c], m)));
-      const float xi = normal_from_bits(random_bits32(sub, 3u * (uint32_t)loc + c, count, a.partitionable != 0));
+      const float xi = normal_from_bits(random_bits32(sub, 3u * (uint32_t)rnd + c, count, a.partitionable != 0));
       p[c] = __dadd_rn(__dmul_rn(c1, p[c]), __dmul_rn(sg, (double)xi));
       x[c] = __dadd_rn(x[c], __dmul_rn(h, __ddiv_rn(p[c], m)));
     }
@@ -97,6 +98,7 @@ __global__ void init_kernel(const IntArgs a) {
     const int s = a.atom_sys[i];
     const SysInfo &S = a.sys[s];
     const int loc = i - S.off;
+    const int rnd = a.user[i] - S.off;  // the atom's index in the caller's order: its noise
     const uint32_t *kin = a.keys + ((size_t)a.parity * a.n_sys + s) * 2;
     uint32_t knew[2], sub[2];
     split_key(kin[0], kin[1], a.partitionable != 0, knew, sub);
@@ -105,7 +107,7 @@ __global__ void init_kernel(const IntArgs a) {
     double p[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const float xi = normal_from_bits(random_bits32(sub, 3u * (uint32_t)loc + c, count, a.partitionable != 0));
+      const float xi = normal_from_bits(random_bits32(sub, 3u * (uint32_t)rnd + c, count, a.partitionable != 0));
       p[c] = __dmul_rn(sd, (double)xi);
     }
     a.px[i] = p[0]; a.py[i] = p[1]; a.pz[i] = p[2];

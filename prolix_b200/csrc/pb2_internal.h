@@ -77,6 +77,10 @@ struct pb2_batch {
   double *q64 = nullptr, *hs64 = nullptr, *se64 = nullptr, *ro64 = nullptr, *sr64 = nullptr;
   double *born64 = nullptr;
   double *stage = nullptr;  // 3 x (n_total, 3) row-major staging for host transfers
+  // atom order: the batch stores atom g where the caller's arrays hold atom
+  // user[g] (both batch-wide indices; systems keep their ranges)
+  int32_t *user = nullptr, *devidx = nullptr;  // device copies: g -> user, user -> g
+  std::vector<int32_t> user_host, dev_host;
   int32_t *d_perm = nullptr;  // system permutation (replica exchange)
   // trajectory ring: capacity frames of float32 (n, 3) positions and
   // velocities, and the step counters of every system

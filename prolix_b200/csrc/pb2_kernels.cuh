@@ -101,6 +101,7 @@ cudaError_t nl_launch_disp(const NlArgs &a, cudaStream_t st);
 struct IntArgs {
   const SysInfo *sys;
   const int32_t *atom_sys;
+  const int32_t *user;  // batch atom -> the caller's batch-wide index (noise streams follow it)
   double *x, *y, *z;
   double *px, *py, *pz;
   long long *fx, *fy, *fz;
@@ -169,24 +170,29 @@ cudaError_t launch_step(const IntArgs &a, cudaStream_t st);
 cudaError_t launch_finish(const IntArgs &a, cudaStream_t st);
 cudaError_t launch_init(const IntArgs &a, cudaStream_t st);
 cudaError_t launch_posq(const IntArgs &a, cudaStream_t st);
-cudaError_t launch_rows_to_soa(const double *rows, double *x, double *y, double *z, int n, cudaStream_t st);
-cudaError_t launch_soa_to_rows(const double *x, const double *y, const double *z, double *rows, int n,
+// Host transfers: `user` maps each batch atom to its row in the caller's
+// (n, 3) arrays.
+cudaError_t launch_rows_to_soa(const double *rows, const int32_t *user, double *x, double *y, double *z, int n,
                                cudaStream_t st);
-cudaError_t launch_fix_to_rows(const long long *fx, const long long *fy, const long long *fz, double *rows,
-                               int n, cudaStream_t st);
-cudaError_t launch_state_from_rows(const double *rows, double *x, double *y, double *z, double *px, double *py,
-                                   double *pz, long long *fx, long long *fy, long long *fz, int n,
-                                   cudaStream_t st);
+cudaError_t launch_soa_to_rows(const double *x, const double *y, const double *z, const int32_t *user,
+                               double *rows, int n, cudaStream_t st);
+cudaError_t launch_fix_to_rows(const long long *fx, const long long *fy, const long long *fz, const int32_t *user,
+                               double *rows, int n, cudaStream_t st);
+cudaError_t launch_rows_to_fix(const double *rows, const int32_t *user, long long *fx, long long *fy,
+                               long long *fz, int n, cudaStream_t st);
+cudaError_t launch_state_from_rows(const double *rows, const int32_t *user, double *x, double *y, double *z,
+                                   double *px, double *py, double *pz, long long *fx, long long *fy,
+                                   long long *fz, int n, cudaStream_t st);
 cudaError_t launch_state_to_rows(const double *x, const double *y, const double *z, const double *px,
                                  const double *py, const double *pz, const long long *fx, const long long *fy,
-                                 const long long *fz, double *rows, int n, cudaStream_t st);
-cudaError_t launch_rows_to_fix(const double *rows, long long *fx, long long *fy, long long *fz, int n,
-                               cudaStream_t st);
+                                 const long long *fz, const int32_t *user, double *rows, int n, cudaStream_t st);
 cudaError_t launch_energies_to_double(const long long *e, double *out, int n_sys, cudaStream_t st);
 cudaError_t launch_snapshot(const double *x, const double *y, const double *z, const double *px,
                             const double *py, const double *pz, const double *mass, const long long *steps,
-                            float *pos, float *vel, long long *frame_steps, int n, int n_sys, cudaStream_t st);
+                            const int32_t *user, float *pos, float *vel, long long *frame_steps, int n, int n_sys,
+                            cudaStream_t st);
 cudaError_t launch_gather_systems(const SysInfo *sys, const int32_t *atom_sys, const int32_t *perm,
-                                  const void *src, void *dst, int n, cudaStream_t st);
+                                  const int32_t *user, const int32_t *devidx, const void *src, void *dst, int n,
+                                  cudaStream_t st);
 
 }  // namespace pb2

@@ -410,8 +410,20 @@ extern "C" int pb2_nl_get(pb2_batch *b, int32_t *neighbors, void *stream) {
   pb2_ctx *ctx = b->ctx;
   if (!b->nl_built) return fail(ctx, PB2_EINVAL, "no neighbour list built yet");
   cudaStream_t st = (cudaStream_t)stream;
-  CUDA_TRY(ctx, cudaMemcpyAsync(neighbors, b->nl_rows, (size_t)b->n_total * b->nl_capacity * sizeof(int),
-                                cudaMemcpyDeviceToHost, st));
+  const size_t cap = (size_t)b->nl_capacity;
+  std::vector<int> rows((size_t)b->n_total * cap);
+  CUDA_TRY(ctx, cudaMemcpyAsync(rows.data(), b->nl_rows, rows.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
   CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  // rows and neighbour indices in the caller's atom order (local indices;
+  // the sentinel, the system's atom count, stays)
+  for (int s = 0; s < b->n_sys; ++s) {
+    const int off = b->off[s], n = b->nat[s];
+    for (int l = 0; l < n; ++l) {
+      const int g = off + l;
+      const int *src = &rows[(size_t)g * cap];
+      int32_t *dst = neighbors + (size_t)b->user_host[g] * cap;
+      for (size_t k = 0; k < cap; ++k) dst[k] = src[k] >= n ? src[k] : b->user_host[off + src[k]] - off;
+    }
+  }
   return PB2_OK;
 }

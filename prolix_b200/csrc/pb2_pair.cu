@@ -86,7 +86,7 @@ struct Acc {
 struct TileConst {
   float cut2, gcut2, bcut2, pref, kcoul, lj14, coul14;  // bcut2: descreening / chain rule
   bool use_gb, use_lj, use_coul;
-  int src;
+  int src, lane;
 };
 
 // Force-pass rotation of everything but x, y, z and tj.a0.
@@ -245,11 +245,11 @@ struct Acc2 {
 // zero (1/r^4 = 1e-60), so they are summed without a select and never reach
 // the closed form.
 
-// Both pairs' geometry and both directions' integral terms.  The series path
-// keeps the radial factor apart: I = s^3 S(s^2/r^2) / r^4 and
-// -(dI/dr) / r = s^3 D(s^2/r^2) / r^6, so vij, vji hold s^3 S (or s^3 D) and
-// f the common 1/r^4 (or 1/r^6); the closed form stores I (or dI/dr) with
-// f = 1 (or -1/r).
+// Both pairs' geometry and both directions' integral terms.  The series
+// keeps the radial factor apart: I = s^3 V(s^2/r^2) / r^4 and
+// -(dI/dr) / r = s^3 D(s^2/r^2) / r^6, so vij, vji hold s^3 V (or s^3 D) and
+// f the common 1/r^4 (or 1/r^6); a pair queued for the closed form has all
+// three zeroed.
 struct BCPair2 {
   float2 dx, dy, dz, r2, inv_r, vij, vji, f;
   bool ok0, ok1;
@@ -284,26 +284,6 @@ __device__ __forceinline__ void bc_series2(const PData2 &I, const PData &J, bool
   }
 }
 
-// Closed form for one component (c = 0: block ib, 1: block ib + 1).
-template <int PASS>
-__device__ __forceinline__ void bc_closed2(const PData2 &I, const PData &J, BCPair2 &P, int c) {
-  const float r2 = c ? P.r2.y : P.r2.x, inv_r = c ? P.inv_r.y : P.inv_r.x;
-  const float ro = c ? I.ro.y : I.ro.x, sr = c ? I.sr.y : I.sr.x;
-  const float r = r2 * inv_r;
-  float vij, vji, f;
-  if (PASS == PASS_BORN) {
-    vij = obc_integral(r, inv_r, ro, J.sr);
-    vji = obc_integral(r, inv_r, J.ro, sr);
-    f = 1.0f;
-  } else {
-    vij = obc_integral_dr(r, inv_r, ro, J.sr);
-    vji = obc_integral_dr(r, inv_r, J.ro, sr);
-    f = -inv_r;
-  }
-  if (c) { P.vij.y = vij; P.vji.y = vji; P.f.y = f; }
-  else { P.vij.x = vij; P.vji.x = vji; P.f.x = f; }
-}
-
 template <int PASS>
 __device__ __forceinline__ void bc_accumulate2(const PData2 &I, const PData &J, const BCPair2 &P, Acc2 &ti,
                                                Acc &tj) {
@@ -322,12 +302,77 @@ __device__ __forceinline__ void bc_accumulate2(const PData2 &I, const PData &J, 
   }
 }
 
+// Pairs of near tiles outside the series' domain take the closed form.
+// Evaluated in place they would idle most of the warp at every step where
+// one lane needs them (and a compact block of atoms holds many such pairs),
+// so each warp queues them as (i, j) atom pairs in shared memory and
+// evaluates them later, one pair per lane, adding each pair's two
+// contributions to the fixed-point accumulators by itself.  A pair's
+// contributions are the same whenever its queue is flushed, so results stay
+// independent of scheduling.
+constexpr int kCfCap = 256;  // queued pairs per warp (2 KB of shared memory)
+
+struct CfArgs {
+  const float4 *posq, *par, *born;
+  const long long *dedb_acc;
+  long long *born_acc, *fx, *fy, *fz;
+};
+
+__device__ __forceinline__ float dedi_of(const CfArgs &c, int g) {
+  return (float)((double)c.dedb_acc[g] * kForceInv) * c.born[g].z;  // as load_pdata
+}
+
+// Evaluates the n queued pairs (warp-convergent; the caller synchronises
+// the warp before and after): bc_series2's geometry, then the closed form
+// of both directions (I or dI/dr), then bc_accumulate2's sums, per pair.
+template <int PASS>
+__device__ __forceinline__ void cf_flush(const CfArgs c, const int2 *q, int n, int lane, float bscale) {
+  for (int e = lane; e < n; e += 32) {
+    const int2 pr = q[e];  // (i, j) batch atom indices
+    const float4 pi = c.posq[pr.x], pj = c.posq[pr.y];
+    const float4 ci = c.par[pr.x], cj = c.par[pr.y];
+    const float dx = pi.x + -pj.x, dy = pi.y + -pj.y, dz = pi.z + -pj.z;
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    const float inv_r = rsqrtf(r2);
+    const float r = r2 * inv_r;
+    if (PASS == PASS_BORN) {
+      atomic_add_fix(&c.born_acc[pr.x], to_fix_f(obc_integral(r, inv_r, ci.z, cj.w), bscale));
+      atomic_add_fix(&c.born_acc[pr.y], to_fix_f(obc_integral(r, inv_r, cj.z, ci.w), bscale));
+    } else {
+      const float vij = obc_integral_dr(r, inv_r, ci.z, cj.w);
+      const float vji = obc_integral_dr(r, inv_r, cj.z, ci.w);
+      const float h = fmaf(dedi_of(c, pr.x), vij, dedi_of(c, pr.y) * vji) * -inv_r;
+      const long long fx = to_fix_f(h * dx, bscale), fy = to_fix_f(h * dy, bscale),
+                      fz = to_fix_f(h * dz, bscale);
+      atomic_add_fix(&c.fx[pr.x], fx); atomic_add_fix(&c.fy[pr.x], fy); atomic_add_fix(&c.fz[pr.x], fz);
+      atomic_add_fix(&c.fx[pr.y], -fx); atomic_add_fix(&c.fy[pr.y], -fy); atomic_add_fix(&c.fz[pr.y], -fz);
+    }
+  }
+}
+
+// The warp's closed-form queue and what a push needs to name its pairs.
+struct CfQueue {
+  CfArgs c;
+  int2 *q;
+  int n;              // warp-uniform
+  int ig0, ig1, jg0;  // batch index of the lane's two i atoms; of the j-block's atom 0
+  float bscale;
+};
+
+template <int PASS>
+__device__ __forceinline__ void cf_drain(CfQueue &Q, int lane) {
+  __syncwarp();  // the lanes' queue writes are visible to every lane
+  cf_flush<PASS>(Q.c, Q.q, Q.n, lane, Q.bscale);
+  __syncwarp();  // every lane has read its entries before the queue is reused
+  Q.n = 0;
+}
+
 // FAR: both tiles lie in the series' domain (no per-pair test); otherwise
-// each pair is tested and the closed form runs, after a warp vote, only for
-// the lanes that need it.
+// each pair is tested, and those outside the domain go to the warp's
+// closed-form queue with their series terms zeroed.
 template <int PASS, bool FAR, bool CUT, int TIER>
 __device__ __forceinline__ void run_bc_tile2(const PData2 &I, PData &J, Acc2 &ti, Acc &tj, uint32_t V0,
-                                             uint32_t V1, const TileConst &K) {
+                                             uint32_t V1, const TileConst &K, CfQueue &Q) {
   const int src = K.src;
   // step k tests the sign bit of the bit-reversed mask shifted left k times
   uint32_t R0 = __brev(V0), R1 = __brev(V1);
@@ -344,19 +389,27 @@ __device__ __forceinline__ void run_bc_tile2(const PData2 &I, PData &J, Acc2 &ti
       // near-tile steps of the benchmark batch, this one on 13.4 %)
       const bool n0 = P.ok0 && !(P.r2.x >= fmaxf(I.t2.x, J.t2));
       const bool n1 = P.ok1 && !(P.r2.y >= fmaxf(I.t2.y, J.t2));
-      if (__any_sync(kFull, n0 || n1)) {
-        if (n0) bc_closed2<PASS>(I, J, P, 0);
-        if (n1) bc_closed2<PASS>(I, J, P, 1);
+      const unsigned b0 = __ballot_sync(kFull, n0), b1 = __ballot_sync(kFull, n1);
+      if (b0 | b1) {  // warp-uniform
+        const int c0 = __popc(b0), cnt = c0 + __popc(b1);
+        if (Q.n + cnt > kCfCap) cf_drain<PASS>(Q, K.lane);
+        const unsigned lt = (1u << K.lane) - 1u;
+        const int jg = Q.jg0 + ((K.lane + k) & 31);  // the j atom this lane holds at step k
+        if (n0) {
+          Q.q[Q.n + __popc(b0 & lt)] = make_int2(Q.ig0, jg);
+          P.vij.x = 0.f; P.vji.x = 0.f; P.f.x = 0.f;
+        }
+        if (n1) {
+          Q.q[Q.n + c0 + __popc(b1 & lt)] = make_int2(Q.ig1, jg);
+          P.vij.y = 0.f; P.vji.y = 0.f; P.f.y = 0.f;
+        }
+        Q.n += cnt;
       }
     }
     bc_accumulate2<PASS>(I, J, P, ti, tj);
     J.x = shfl_next(J.x, src); J.y = shfl_next(J.y, src); J.z = shfl_next(J.z, src);
     J.s2 = shfl_next(J.s2, src); J.s3 = shfl_next(J.s3, src);
-    if (!FAR) {
-      J.sr = shfl_next(J.sr, src);
-      J.ro = shfl_next(J.ro, src);
-      J.t2 = shfl_next(J.t2, src);
-    }
+    if (!FAR) J.t2 = shfl_next(J.t2, src);
     tj.a0 = shfl_next(tj.a0, src);
     if (PASS == PASS_CHAIN) {
       J.dedi = shfl_next(J.dedi, src);
@@ -393,6 +446,14 @@ __global__ void __launch_bounds__(256, PASS == PASS_BORN ? PB2_MINB_BORN : (PASS
   K.use_lj = ALL || (a.terms & PB2_USE_LJ) != 0;
   K.use_coul = ALL || (a.terms & PB2_USE_COULOMB) != 0;
   K.src = (lane + 1) & 31;
+  K.lane = lane;
+  // closed-form queues of the descreening and chain passes, one per warp
+  __shared__ int2 s_cfq[PASS == PASS_FORCE ? 1 : 8][PASS == PASS_FORCE ? 1 : kCfCap];
+  CfQueue Q;
+  Q.c = {a.posq, a.par, a.born, a.dedb_acc, a.born_acc, a.fx, a.fy, a.fz};
+  Q.q = s_cfq[PASS == PASS_FORCE ? 0 : (threadIdx.x >> 5)];
+  Q.n = 0;
+  Q.bscale = PASS == PASS_BORN ? (float)kBornScale : (float)kForceScale;
   const uint32_t diag_mask = lane == 31 ? 0u : (0xffffffffu << (lane + 1));
   const float bscale = PASS == PASS_BORN ? (float)kBornScale : (float)kForceScale;
 
@@ -422,7 +483,7 @@ __global__ void __launch_bounds__(256, PASS == PASS_BORN ? PB2_MINB_BORN : (PASS
     load_pdata(a, ig0, PASS, K.use_gb, S.ro_max, I0);
     load_pdata(a, ig1, PASS, K.use_gb, S.ro_max, I1);
     const PData2 I2 = pack2(I0, I1);  // descreening / chain passes
-    // exclusion entries: lanes 0-7 for block ib, lanes 8-15 for block ib + 1
+    // exclusion entries: lanes 0-15 for block ib, lanes 16-31 for block ib + 1
     int2 ent = make_int2(-1, -1);
     if (PASS == PASS_FORCE) {
       if (lane < kExclPerBlock) ent = a.excl_ent[gib0 * kExclPerBlock + lane];
@@ -462,7 +523,8 @@ __global__ void __launch_bounds__(256, PASS == PASS_BORN ? PB2_MINB_BORN : (PASS
         const bool full = __all_sync(kFull, (C0 & C1) == 0xffffffffu);
         uint32_t E0 = 0u, S0 = 0u, E1 = 0u, S1 = 0u;
         const unsigned hit = __ballot_sync(kFull, ent.x == jb);
-        const unsigned hit0 = hit & 0xffu, hit1 = hit & 0xff00u;
+        static_assert(2 * kExclPerBlock == 32, "one exclusion entry per lane");
+        const unsigned hit0 = hit & 0xffffu, hit1 = hit & 0xffff0000u;
         if (hit0) {
           const int roff = __shfl_sync(kFull, ent.y, __ffs(hit0) - 1);
           const ExclRow r = a.excl_rows[roff + lane];
@@ -486,11 +548,13 @@ __global__ void __launch_bounds__(256, PASS == PASS_BORN ? PB2_MINB_BORN : (PASS
         // series tier by the tiles' smallest separation
         const float *tier2 = S.tier2[PASS == PASS_BORN ? 0 : 1];
         Acc2 ti = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-        if (d2 >= tier2[0]) run_bc_tile2<PASS, true, CUT, 0>(I2, J, ti, tj, V0, V1, K);
-        else if (d2 >= tier2[1]) run_bc_tile2<PASS, true, CUT, 1>(I2, J, ti, tj, V0, V1, K);
-        else if (d2 >= tier2[2]) run_bc_tile2<PASS, true, CUT, 2>(I2, J, ti, tj, V0, V1, K);
-        else if (d2 >= S.far2) run_bc_tile2<PASS, true, CUT, 3>(I2, J, ti, tj, V0, V1, K);
-        else run_bc_tile2<PASS, false, CUT, 3>(I2, J, ti, tj, V0, V1, K);
+        Q.ig0 = ig0; Q.ig1 = ig1; Q.jg0 = off + jl0;
+        if (d2 >= tier2[0]) run_bc_tile2<PASS, true, CUT, 0>(I2, J, ti, tj, V0, V1, K, Q);
+        else if (d2 >= tier2[1]) run_bc_tile2<PASS, true, CUT, 1>(I2, J, ti, tj, V0, V1, K, Q);
+        else if (d2 >= tier2[2]) run_bc_tile2<PASS, true, CUT, 2>(I2, J, ti, tj, V0, V1, K, Q);
+        else if (d2 >= S.far2) run_bc_tile2<PASS, true, CUT, 3>(I2, J, ti, tj, V0, V1, K, Q);
+        else run_bc_tile2<PASS, false, CUT, 3>(I2, J, ti, tj, V0, V1, K, Q);
+        if (Q.n >= 32) cf_drain<PASS>(Q, lane);  // a pair for every lane
         t0.a0 = ti.a0.x; t0.a1 = ti.a1.x; t0.a2 = ti.a2.x;
         t1.a0 = ti.a0.y; t1.a1 = ti.a1.y; t1.a2 = ti.a2.y;
       }
@@ -531,6 +595,9 @@ __global__ void __launch_bounds__(256, PASS == PASS_BORN ? PB2_MINB_BORN : (PASS
         if (PASS == PASS_FORCE && K.use_gb) atomic_add_fix(&a.dedb_acc[ig1], q3);
       }
     }
+  }
+  if constexpr (PASS != PASS_FORCE) {
+    if (Q.n > 0) cf_drain<PASS>(Q, lane);
   }
   if (lane == 0 && atomicAdd(&a.sched[1], 1) == nwarps - 1) {
     // every warp has stopped taking items: reset for the next launch

@@ -182,7 +182,7 @@ class Batch:
   def __init__(self, systems, *, cutoff=0.0, gb_cutoff=-1.0, born_cutoff=0.0, skin=2.0, terms=_lib.USE_ALL,
                device=0,
                tile_segment=0, graph_chunk=50, partitionable_keys=True, nl_capacity=0,
-               **system_defaults):
+               keep_atom_order=False, **system_defaults):
     if isinstance(systems, dict):
       systems = [systems]
     if not systems:
@@ -200,7 +200,8 @@ class Batch:
                         nl_capacity=int(nl_capacity), tile_segment=int(tile_segment),
                         graph_chunk=int(graph_chunk),
                         partitionable_keys=1 if partitionable_keys else 0,
-                        gb_cutoff=float(gb_cutoff), born_cutoff=float(born_cutoff))
+                        gb_cutoff=float(gb_cutoff), born_cutoff=float(born_cutoff),
+                        keep_atom_order=1 if keep_atom_order else 0)
     h = ctypes.c_void_p()
     self.ctx.check(self.lib.pb2_batch_create(self.ctx.handle, self.n_systems, descs,
                                              ctypes.byref(rp), ctypes.byref(h)))

@@ -181,7 +181,9 @@ class Server:
                                    error=msg)
 
   def _build(self):
-    systems = [dict(s.req.system, positions=s.x, key=tuple(int(v) for v in s.key), dt=s.req.dt,
+    # each system is described by its submitted positions, which fix its
+    # stored atom order; its current state is restored below
+    systems = [dict(s.req.system, key=tuple(int(v) for v in s.key), dt=s.req.dt,
                     kT=s.req.kT, gamma=s.req.gamma) for s in self.active]
     if self._batch is not None:
       self._batch.close()

@@ -43,9 +43,9 @@ def test_term_subsets_add_up_to_the_full_force():
   assert rel < 1e-6
 
 
-def _bad(system, match):
+def _bad(system, match, **kw):
   with pytest.raises((_lib.PB2Error, ValueError), match=match):
-    engine.Batch([system]).close()
+    engine.Batch([system], **kw).close()
 
 
 def test_invalid_inputs_are_rejected():
@@ -53,10 +53,12 @@ def test_invalid_inputs_are_rejected():
   _bad(dict(s, masses=np.where(np.arange(100) == 7, 0.0, s["masses"])), "masses")
   _bad(dict(s, bonds=np.array([[0, 1], [5, 100]])), "index")
   _bad(dict(s, excl_pairs=np.array([[4, 2]]), excl_kind=np.array([0])), "i < j")
-  # atom 0 with exclusion partners in nine different 32-atom blocks
-  n = 300
-  far = dict(synth.make_chain(n, 4), excl_pairs=np.array([[0, 33 * k + 1] for k in range(9)]),
-             excl_kind=np.zeros(9, np.int32))
-  _bad(far, "more than 8")
+  # atom 0 with exclusion partners in seventeen different 32-atom blocks of
+  # the input order (a spatial order may gather them into fewer blocks, and
+  # is then accepted)
+  n = 600
+  far = dict(synth.make_chain(n, 4), excl_pairs=np.array([[0, 33 * k + 1] for k in range(17)]),
+             excl_kind=np.zeros(17, np.int32))
+  _bad(far, "more than 16", keep_atom_order=True)
   with pytest.raises(ValueError):
     engine.Batch([])

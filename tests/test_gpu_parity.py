@@ -236,20 +236,25 @@ def test_nve_drift_is_second_order_in_dt():
   assert d2 < 0.4 * d1
 
 
-def test_checkpoint_resume_is_bit_exact():
-  # A slot's state (FP64 x, p, threefry key) plus its float32 frame origin
-  # fully determines the trajectory: snapshot at step 10, restore into a new
-  # batch, continue -> identical to the uninterrupted run.
+@pytest.mark.parametrize("keep_order", [False, True])
+def test_checkpoint_resume_is_bit_exact(keep_order):
+  # A slot's state (FP64 x, p, threefry key), its float32 frame origin and
+  # its atom order fully determine the trajectory: snapshot at step 10,
+  # restore into a new batch, continue -> identical to the uninterrupted run.
+  # The stored atom order follows the positions a batch is created from, so
+  # the new batch is created from the same description (or keeps the input
+  # order, when any positions will do).
   s = synth.make_chain(420, 33, compact=True)
   s = dict(s, origin=engine.default_origin(s["positions"]))
   key = prng.prng_key(77)
-  with engine.Batch([s], key=key) as b:
+  with engine.Batch([s], key=key, keep_atom_order=keep_order) as b:
     b.langevin_init()
     b.langevin_run(10)
     snap = b.get_state()
     b.langevin_run(10)
     ref = b.get_state()
-  with engine.Batch([dict(s, positions=snap["position"])], key=key) as b2:
+  s2 = dict(s, positions=snap["position"]) if keep_order else s
+  with engine.Batch([s2], key=key, keep_atom_order=keep_order) as b2:
     b2.set_state(position=snap["position"], momentum=snap["momentum"], key=snap["key"])
     b2.langevin_run(10)
     out = b2.get_state()
@@ -276,7 +281,7 @@ def test_full_state_restore_is_bit_exact_without_force_evaluation():
     snap = {k: v.copy() for k, v in snap.items()}
     b.langevin_run(9)
     ref = b.get_state()
-  with engine.Batch([dict(s, positions=snap["position"])], key=(1, 2)) as b2:
+  with engine.Batch([s], key=(1, 2)) as b2:  # same description: same stored atom order
     b2.set_full_state(snap["position"], snap["momentum"], snap["force"], key=snap["key"])
     got = b2.get_state(fields=("force",))
     np.testing.assert_array_equal(got["force"], snap["force"])

@@ -66,3 +66,24 @@ def test_run_host_rejects_arrays_it_cannot_write_in_place():
       b.langevin_run_host(good, good, np.zeros((n, 3), dtype=np.float32), 1)
     with pytest.raises(ValueError):
       b.langevin_run_host(good, good, np.zeros((3, n)).T, 1)
+
+
+def test_spatial_atom_order_is_invisible_to_the_caller():
+  # the batch stores each system's atoms in a spatial order by default; every
+  # array that crosses the interface stays in the caller's order, so the two
+  # layouts give the same forces (to float32 summation order), energies,
+  # Born radii and, after steps, the same trajectory to within rounding
+  systems = synth.make_batch(3, 77, 300, 900, compact=True, **synth.PHYSICAL_RANGES)
+  with engine.Batch(systems) as a, engine.Batch(systems, keep_atom_order=True) as b:
+    ea, fa = a.energy_forces()
+    eb, fb = b.energy_forces()
+    np.testing.assert_allclose(ea, eb, rtol=1e-9, atol=1e-6)
+    assert np.linalg.norm(fa - fb) / np.linalg.norm(fb) < 1e-6
+    np.testing.assert_allclose(a.born_radii(), b.born_radii(), rtol=1e-6)
+    a.langevin_init()
+    b.langevin_init()
+    a.langevin_run(20)
+    b.langevin_run(20)
+    xa = a.get_state(fields=("position",))["position"]
+    xb = b.get_state(fields=("position",))["position"]
+    assert np.max(np.abs(xa - xb)) < 1e-4
