@@ -145,15 +145,19 @@ static void spatial_order(const double *pos, int n, std::vector<int> &ord) {
     int ax = 0;
     for (int c = 1; c < 3; ++c)
       if (hi[c] - lo[c] > hi[ax] - lo[ax]) ax = c;
-    std::sort(ord.begin() + a, ord.begin() + e, [&](int i, int j) {
+    const int half = (e - a) / 2;
+    const int m = a + std::max(32, std::min((half + 16) / 32 * 32, (e - a - 1) / 32 * 32));
+    // partition only: the atoms below the cut come first (a strict total
+    // order, so the result is the same on every run)
+    std::nth_element(ord.begin() + a, ord.begin() + m, ord.begin() + e, [&](int i, int j) {
       const double ci = pos[3 * i + ax], cj = pos[3 * j + ax];
       return ci < cj || (ci == cj && i < j);
     });
-    const int half = (e - a) / 2;
-    const int m = a + std::max(32, std::min((half + 16) / 32 * 32, (e - a - 1) / 32 * 32));
     todo.push_back({a, m});
     todo.push_back({m, e});
   }
+  // within each block, input order
+  for (int a = 0; a < n; a += 32) std::sort(ord.begin() + a, ord.begin() + std::min(n, a + 32));
 }
 
 static std::vector<TileItem> build_items(const std::vector<SysInfo> &sinfo, int seg) {
