@@ -217,8 +217,8 @@ __device__ __forceinline__ void run_force_tile2(const FData2 &I, PData &J, Acc2F
 // the same j atom) run the same arithmetic, so it is issued as packed FP32
 // pairs (fma.rn.f32x2 and friends: .x = block ib, .y = block ib + 1), which
 // halves the FP32 instructions of these passes.  Per component the results
-// are those of the scalar fmaf / fmul / fadd.  Transcendentals (rsqrt, the
-// closed form) and the j-side sums, to which both pairs add, stay scalar.
+// are those of the scalar fmaf / fmul / fadd.  The rsqrt and the j-side
+// sums, to which both pairs add, stay scalar.
 
 struct PData2 {  // the lane's two i atoms, packed
   float2 x, y, z, sr, ro, t2, s2, s3, dedi;
@@ -269,7 +269,7 @@ __device__ __forceinline__ void bc_series2(const PData2 &I, const PData &J, bool
   P.ok0 = ok0;
   P.ok1 = ok1;
   P.r2 = make_float2(ok0 ? r2.x : kFarR2, ok1 ? r2.y : kFarR2);
-  // every lane evaluates, so a warp vote that follows is reached by all lanes
+  // every lane evaluates, so the warp ballot that follows is reached by all lanes
   P.inv_r = make_float2(rsqrtf(P.r2.x), rsqrtf(P.r2.y));
   const float2 inv_r2 = __fmul2_rn(P.inv_r, P.inv_r);
   const float2 inv_r4 = __fmul2_rn(inv_r2, inv_r2);
@@ -385,8 +385,8 @@ __device__ __forceinline__ void run_bc_tile2(const PData2 &I, PData &J, Acc2 &ti
     if (!FAR) {
       // r >= t_i and r >= t_j give (s/r)^2 <= kSeriesUNear for both radii and
       // r - s >= rho~_max >= rho~ for both directions: a sufficient test in two
-      // instructions (the exact one triggers the closed form on 13.2 % of
-      // near-tile steps of the benchmark batch, this one on 13.4 %)
+      // instructions (it sends about 1.3 % of near-tile pairs of compact
+      // chains to the closed form, barely more than the exact test)
       const bool n0 = P.ok0 && !(P.r2.x >= fmaxf(I.t2.x, J.t2));
       const bool n1 = P.ok1 && !(P.r2.y >= fmaxf(I.t2.y, J.t2));
       const unsigned b0 = __ballot_sync(kFull, n0), b1 = __ballot_sync(kFull, n1);
