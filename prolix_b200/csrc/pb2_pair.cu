@@ -255,7 +255,7 @@ struct BCPair2 {
   bool ok0, ok1;
 };
 
-template <int PASS, bool CUT, int TIER>
+template <int PASS, bool CUT, bool FULL, int TIER>
 __device__ __forceinline__ void bc_series2(const PData2 &I, const PData &J, bool ok0, bool ok1, BCPair2 &P,
                                            const TileConst &K) {
   P.dx = __fadd2_rn(I.x, dup2(-J.x));
@@ -268,7 +268,8 @@ __device__ __forceinline__ void bc_series2(const PData2 &I, const PData &J, bool
   }
   P.ok0 = ok0;
   P.ok1 = ok1;
-  P.r2 = make_float2(ok0 ? r2.x : kFarR2, ok1 ? r2.y : kFarR2);
+  // FULL: every pair of the tile exists (no cutoff): no select
+  P.r2 = (FULL && !CUT) ? r2 : make_float2(ok0 ? r2.x : kFarR2, ok1 ? r2.y : kFarR2);
   // every lane evaluates, so the warp ballot that follows is reached by all lanes
   P.inv_r = make_float2(rsqrtf(P.r2.x), rsqrtf(P.r2.y));
   const float2 inv_r2 = __fmul2_rn(P.inv_r, P.inv_r);
@@ -370,7 +371,7 @@ __device__ __forceinline__ void cf_drain(CfQueue &Q, int lane) {
 // FAR: both tiles lie in the series' domain (no per-pair test); otherwise
 // each pair is tested, and those outside the domain go to the warp's
 // closed-form queue with their series terms zeroed.
-template <int PASS, bool FAR, bool CUT, int TIER>
+template <int PASS, bool FAR, bool CUT, bool FULL, int TIER>
 __device__ __forceinline__ void run_bc_tile2(const PData2 &I, PData &J, Acc2 &ti, Acc &tj, uint32_t V0,
                                              uint32_t V1, const TileConst &K, CfQueue &Q) {
   const int src = K.src;
@@ -379,9 +380,11 @@ __device__ __forceinline__ void run_bc_tile2(const PData2 &I, PData &J, Acc2 &ti
 #pragma unroll kUnrollBC
   for (int k = 0; k < 32; ++k) {
     BCPair2 P;
-    bc_series2<PASS, CUT, TIER>(I, J, (int32_t)R0 < 0, (int32_t)R1 < 0, P, K);
-    R0 <<= 1;
-    R1 <<= 1;
+    bc_series2<PASS, CUT, FULL, TIER>(I, J, FULL || (int32_t)R0 < 0, FULL || (int32_t)R1 < 0, P, K);
+    if (!FULL) {
+      R0 <<= 1;
+      R1 <<= 1;
+    }
     if (!FAR) {
       // r >= t_i and r >= t_j give (s/r)^2 <= kSeriesUNear for both radii and
       // r - s >= rho~_max >= rho~ for both directions: a sufficient test in two
@@ -549,11 +552,21 @@ __global__ void __launch_bounds__(256, PASS == PASS_BORN ? PB2_MINB_BORN : (PASS
         const float *tier2 = S.tier2[PASS == PASS_BORN ? 0 : 1];
         Acc2 ti = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
         Q.ig0 = ig0; Q.ig1 = ig1; Q.jg0 = off + jl0;
-        if (d2 >= tier2[0]) run_bc_tile2<PASS, true, CUT, 0>(I2, J, ti, tj, V0, V1, K, Q);
-        else if (d2 >= tier2[1]) run_bc_tile2<PASS, true, CUT, 1>(I2, J, ti, tj, V0, V1, K, Q);
-        else if (d2 >= tier2[2]) run_bc_tile2<PASS, true, CUT, 2>(I2, J, ti, tj, V0, V1, K, Q);
-        else if (d2 >= S.far2) run_bc_tile2<PASS, true, CUT, 3>(I2, J, ti, tj, V0, V1, K, Q);
-        else run_bc_tile2<PASS, false, CUT, 3>(I2, J, ti, tj, V0, V1, K, Q);
+        // far tiles whose 64 x 32 pairs all exist skip the validity masks
+        const bool full = __all_sync(kFull, (C0 & C1) == 0xffffffffu);
+        if (full) {
+          if (d2 >= tier2[0]) run_bc_tile2<PASS, true, CUT, true, 0>(I2, J, ti, tj, V0, V1, K, Q);
+          else if (d2 >= tier2[1]) run_bc_tile2<PASS, true, CUT, true, 1>(I2, J, ti, tj, V0, V1, K, Q);
+          else if (d2 >= tier2[2]) run_bc_tile2<PASS, true, CUT, true, 2>(I2, J, ti, tj, V0, V1, K, Q);
+          else if (d2 >= S.far2) run_bc_tile2<PASS, true, CUT, true, 3>(I2, J, ti, tj, V0, V1, K, Q);
+          else run_bc_tile2<PASS, false, CUT, false, 3>(I2, J, ti, tj, V0, V1, K, Q);
+        } else {
+          if (d2 >= tier2[0]) run_bc_tile2<PASS, true, CUT, false, 0>(I2, J, ti, tj, V0, V1, K, Q);
+          else if (d2 >= tier2[1]) run_bc_tile2<PASS, true, CUT, false, 1>(I2, J, ti, tj, V0, V1, K, Q);
+          else if (d2 >= tier2[2]) run_bc_tile2<PASS, true, CUT, false, 2>(I2, J, ti, tj, V0, V1, K, Q);
+          else if (d2 >= S.far2) run_bc_tile2<PASS, true, CUT, false, 3>(I2, J, ti, tj, V0, V1, K, Q);
+          else run_bc_tile2<PASS, false, CUT, false, 3>(I2, J, ti, tj, V0, V1, K, Q);
+        }
         if (Q.n >= 32) cf_drain<PASS>(Q, lane);  // a pair for every lane
         t0.a0 = ti.a0.x; t0.a1 = ti.a1.x; t0.a2 = ti.a2.x;
         t1.a0 = ti.a0.y; t1.a1 = ti.a1.y; t1.a2 = ti.a2.y;
