@@ -552,14 +552,14 @@ __global__ void __launch_bounds__(256, PASS == PASS_BORN ? PB2_MINB_BORN : (PASS
         const float *tier2 = S.tier2[PASS == PASS_BORN ? 0 : 1];
         Acc2 ti = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
         Q.ig0 = ig0; Q.ig1 = ig1; Q.jg0 = off + jl0;
-        // far tiles whose 64 x 32 pairs all exist skip the validity masks
+        // tiles whose 64 x 32 pairs all exist skip the validity masks
         const bool full = __all_sync(kFull, (C0 & C1) == 0xffffffffu);
         if (full) {
           if (d2 >= tier2[0]) run_bc_tile2<PASS, true, CUT, true, 0>(I2, J, ti, tj, V0, V1, K, Q);
           else if (d2 >= tier2[1]) run_bc_tile2<PASS, true, CUT, true, 1>(I2, J, ti, tj, V0, V1, K, Q);
           else if (d2 >= tier2[2]) run_bc_tile2<PASS, true, CUT, true, 2>(I2, J, ti, tj, V0, V1, K, Q);
           else if (d2 >= S.far2) run_bc_tile2<PASS, true, CUT, true, 3>(I2, J, ti, tj, V0, V1, K, Q);
-          else run_bc_tile2<PASS, false, CUT, false, 3>(I2, J, ti, tj, V0, V1, K, Q);
+          else run_bc_tile2<PASS, false, CUT, true, 3>(I2, J, ti, tj, V0, V1, K, Q);
         } else {
           if (d2 >= tier2[0]) run_bc_tile2<PASS, true, CUT, false, 0>(I2, J, ti, tj, V0, V1, K, Q);
           else if (d2 >= tier2[1]) run_bc_tile2<PASS, true, CUT, false, 1>(I2, J, ti, tj, V0, V1, K, Q);
