@@ -130,17 +130,23 @@ static void spatial_order(const double *pos, int n, std::vector<int> &ord) {
   for (int i = 0; i < n; ++i) ord[i] = i;
   for (int i = 0; i < 3 * n; ++i)
     if (!std::isfinite(pos[i])) return;
+  struct At {
+    double c[3];
+    int i;
+  };
+  std::vector<At> at(n);  // positions travel with their indices (contiguous)
+  for (int i = 0; i < n; ++i) at[i] = At{{pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]}, i};
   std::vector<std::pair<int, int>> todo{{0, n}};
   while (!todo.empty()) {
     const auto [a, e] = todo.back();
     todo.pop_back();
     if (e - a <= 32) continue;
-    double lo[3] = {pos[3 * ord[a]], pos[3 * ord[a] + 1], pos[3 * ord[a] + 2]};
+    double lo[3] = {at[a].c[0], at[a].c[1], at[a].c[2]};
     double hi[3] = {lo[0], lo[1], lo[2]};
     for (int k = a; k < e; ++k)
       for (int c = 0; c < 3; ++c) {
-        lo[c] = std::min(lo[c], pos[3 * ord[k] + c]);
-        hi[c] = std::max(hi[c], pos[3 * ord[k] + c]);
+        lo[c] = std::min(lo[c], at[k].c[c]);
+        hi[c] = std::max(hi[c], at[k].c[c]);
       }
     int ax = 0;
     for (int c = 1; c < 3; ++c)
@@ -149,13 +155,13 @@ static void spatial_order(const double *pos, int n, std::vector<int> &ord) {
     const int m = a + std::max(32, std::min((half + 16) / 32 * 32, (e - a - 1) / 32 * 32));
     // partition only: the atoms below the cut come first (a strict total
     // order, so the result is the same on every run)
-    std::nth_element(ord.begin() + a, ord.begin() + m, ord.begin() + e, [&](int i, int j) {
-      const double ci = pos[3 * i + ax], cj = pos[3 * j + ax];
-      return ci < cj || (ci == cj && i < j);
+    std::nth_element(at.begin() + a, at.begin() + m, at.begin() + e, [ax](const At &p, const At &q) {
+      return p.c[ax] < q.c[ax] || (p.c[ax] == q.c[ax] && p.i < q.i);
     });
     todo.push_back({a, m});
     todo.push_back({m, e});
   }
+  for (int l = 0; l < n; ++l) ord[l] = at[l].i;
   // within each block, input order
   for (int a = 0; a < n; a += 32) std::sort(ord.begin() + a, ord.begin() + std::min(n, a + 32));
 }
