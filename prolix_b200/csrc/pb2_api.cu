@@ -521,6 +521,25 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
     }
   }
 
+  // terms in order of their (central) atom: with atoms in spatial order, the
+  // threads of a warp then read and update nearby atoms
+  auto by_atom = [](auto &idx, auto &par, auto key) {
+    std::vector<int> o(idx.size());
+    for (size_t k = 0; k < o.size(); ++k) o[k] = (int)k;
+    std::stable_sort(o.begin(), o.end(), [&](int p, int q) { return key(idx[p]) < key(idx[q]); });
+    auto idx2 = idx;
+    auto par2 = par;
+    for (size_t k = 0; k < o.size(); ++k) {
+      idx2[k] = idx[o[k]];
+      par2[k] = par[o[k]];
+    }
+    idx.swap(idx2);
+    par.swap(par2);
+  };
+  by_atom(bidx, bpar, [](const int2 &t) { return std::min(t.x, t.y); });
+  by_atom(aidx, apar, [](const int4 &t) { return t.y; });
+  by_atom(tidx, tpar, [](const int4 &t) { return std::min(t.y, t.z); });
+
   // --- device allocation
   Dev &D = b->dev;
   b->sys = D.alloc<SysInfo>(n_systems);
