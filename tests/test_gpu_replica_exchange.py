@@ -38,6 +38,30 @@ def test_permute_systems_moves_whole_states():
       b.permute_systems(np.array([0, 0, 1]))
 
 
+def test_permute_systems_between_different_stored_orders():
+  # replicas created from different structures store their atoms in
+  # different spatial orders; a swap still moves each atom's state to the
+  # same atom of the other slot
+  s = synth.make_chain(300, 32, compact=True, **synth.PHYSICAL_RANGES)
+  rng = np.random.default_rng(5)
+  pos2 = s["positions"] + rng.normal(0.0, 0.4, s["positions"].shape)
+  origin = engine.default_origin(s["positions"])
+  reps = [dict(s, origin=origin, key=prng.prng_key(60)), dict(s, positions=pos2, origin=origin,
+                                                              key=prng.prng_key(61))]
+  with engine.Batch(reps) as b:
+    b.langevin_init()
+    st0 = b.get_state()
+    b.permute_systems(np.array([1, 0]))
+    st1 = b.get_state()
+    for f in ("position", "momentum", "force"):
+      old, new = b.split(st0[f]), b.split(st1[f])
+      np.testing.assert_array_equal(new[0], old[1])
+      np.testing.assert_array_equal(new[1], old[0])
+    # the forces the swap carried are the forces at the swapped positions
+    e, f = b.energy_forces()
+    assert np.linalg.norm(f - st1["force"]) / np.linalg.norm(f) < 1e-6
+
+
 def test_short_parallel_tempering_run():
   s = synth.make_chain(166, 32, compact=True, **synth.PHYSICAL_RANGES)
   spec = rx.ReplicaExchangeSpec(n_replicas=4, min_temp=300.0, max_temp=450.0, step_size_fs=1.0,
