@@ -278,8 +278,9 @@ def run_reference(args):
     time_total += atoms / v
     nxt = start
   value = atoms_total / time_total
-  sample = (f"{args.steps} steps of about {budget:.2f} s each, continuing through the "
-            f"{len(systems)}-system workload ({int(atoms_total)} atom-steps in all); " + sample.split("; ", 1)[1])
+  sample = (f"{args.steps} steps of at most {budget:.2f} s each ({time_total / max(args.steps, 1):.2f} s on "
+            f"average), continuing through the {len(systems)}-system workload ({int(atoms_total)} "
+            f"atom-steps in all); " + sample.split("; ", 1)[1])
   line = {
       "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
       "steps": args.steps, "warmup": args.warmup,
