@@ -89,15 +89,72 @@ struct TileConst {
   int src, lane;
 };
 
-// Force-pass rotation of everything but x, y, z and tj.a0.
-__device__ __forceinline__ void rotate_force_rest(PData &J, Acc &tj, int src, const TileConst &K) {
-  J.q = shfl_next(J.q, src);
-  if (K.use_lj) { J.hs = shfl_next(J.hs, src); J.se = shfl_next(J.se, src); }
-  tj.a1 = shfl_next(tj.a1, src); tj.a2 = shfl_next(tj.a2, src);
-  if (K.use_gb) {
-    J.B = shfl_next(J.B, src); J.iB = shfl_next(J.iB, src);
-    tj.a3 = shfl_next(tj.a3, src);
+// The j-block's data of a tile, in shared memory, one warp's share: four
+// float4 fields per atom, each holding two values as (v, v) pairs, so that
+// a step reads a packed operand straight into a register pair.  Field-major
+// (field, atom), so that the 32 lanes' 16-byte reads of one field are
+// conflict-free.  Force pass: (-x, -x, -y, -y), (-z, -z, q, q),
+// (hs, hs, se, se), (B, B, iB, iB).  Descreening: (-x, -x, -y, -y),
+// (-z, -z, s2, s2), (s3, s3, t2, t2).  Chain rule: the same with
+// (s3, s3, dedi, dedi) and (t2, t2, 0, 0).
+typedef float4 JTile[4][32];
+
+// What a lane reads of its j atom at a step.
+struct JF2 {  // force pass
+  float2 mx, my, mz, q, hs, se, B, iB;
+};
+struct JD2 {  // descreening and chain rule
+  float2 mx, my, mz, s2, s3, dedi;
+  float t2;
+};
+
+__device__ __forceinline__ float2 lo2(float4 v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); }
+
+__device__ __forceinline__ JF2 load_jf(const JTile &t, int e) {
+  const float4 a = t[0][e], b = t[1][e], c = t[2][e], d = t[3][e];
+  return JF2{lo2(a), hi2(a), lo2(b), hi2(b), lo2(c), hi2(c), lo2(d), hi2(d)};
+}
+
+template <int PASS, bool FAR>
+__device__ __forceinline__ JD2 load_jd(const JTile &t, int e) {
+  const float4 a = t[0][e], b = t[1][e], c = t[2][e];
+  JD2 j;
+  j.mx = lo2(a); j.my = hi2(a); j.mz = lo2(b); j.s2 = hi2(b); j.s3 = lo2(c);
+  j.dedi = make_float2(0.f, 0.f);
+  j.t2 = 0.f;
+  if (PASS == PASS_BORN) {
+    if (!FAR) j.t2 = c.z;
+  } else {
+    j.dedi = hi2(c);
+    if (!FAR) j.t2 = t[3][e].x;
   }
+  return j;
+}
+
+// Store the lane's j atom into the warp's tile (after the previous tile's
+// reads; the caller synchronises the warp before and after).
+template <int PASS>
+__device__ __forceinline__ void store_j(JTile &t, int lane, const PData &J) {
+  t[0][lane] = make_float4(-J.x, -J.x, -J.y, -J.y);
+  if (PASS == PASS_FORCE) {
+    t[1][lane] = make_float4(-J.z, -J.z, J.q, J.q);
+    t[2][lane] = make_float4(J.hs, J.hs, J.se, J.se);
+    t[3][lane] = make_float4(J.B, J.B, J.iB, J.iB);
+  } else if (PASS == PASS_BORN) {
+    t[1][lane] = make_float4(-J.z, -J.z, J.s2, J.s2);
+    t[2][lane] = make_float4(J.s3, J.s3, J.t2, J.t2);
+  } else {
+    t[1][lane] = make_float4(-J.z, -J.z, J.s2, J.s2);
+    t[2][lane] = make_float4(J.s3, J.s3, J.dedi, J.dedi);
+    t[3][lane] = make_float4(J.t2, J.t2, 0.f, 0.f);
+  }
+}
+
+// Force-pass rotation of the j-side sums but tj.a0.
+__device__ __forceinline__ void rotate_force_rest(Acc &tj, int src, const TileConst &K) {
+  tj.a1 = shfl_next(tj.a1, src); tj.a2 = shfl_next(tj.a2, src);
+  if (K.use_gb) tj.a3 = shfl_next(tj.a3, src);
 }
 
 __device__ __forceinline__ void load_pdata(const PairArgs &a, int g, int pass, bool use_gb, float ro_max,
@@ -139,7 +196,7 @@ struct Acc2F {
 };
 
 template <bool CUT, bool FULL, bool EXCL>
-__device__ __forceinline__ void run_force_tile2(const FData2 &I, PData &J, Acc2F &ti, Acc &tj, uint32_t V0,
+__device__ __forceinline__ void run_force_tile2(const FData2 &I, const JTile &jt, Acc2F &ti, Acc &tj, uint32_t V0,
                                                 uint32_t V1, uint32_t E0, uint32_t E1, uint32_t S0,
                                                 uint32_t S1, const TileConst &K) {
   const int src = K.src;
@@ -148,29 +205,30 @@ __device__ __forceinline__ void run_force_tile2(const FData2 &I, PData &J, Acc2F
   uint32_t X0 = __brev(E0), X1 = __brev(E1), Q0 = __brev(S0), Q1 = __brev(S1);
 #pragma unroll kUnroll
   for (int k = 0; k < 32; ++k) {
-    const float2 dx = __fadd2_rn(I.x, dup2(-J.x));
-    const float2 dy = __fadd2_rn(I.y, dup2(-J.y));
-    const float2 dz = __fadd2_rn(I.z, dup2(-J.z));
+    const JF2 J = load_jf(jt, (K.lane + k) & 31);  // lane l meets j-lane (l + k) mod 32
+    const float2 dx = __fadd2_rn(I.x, J.mx);
+    const float2 dy = __fadd2_rn(I.y, J.my);
+    const float2 dz = __fadd2_rn(I.z, J.mz);
     float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
     if (!FULL) {
       r2 = make_float2((int32_t)R0 < 0 ? r2.x : kFarR2, (int32_t)R1 < 0 ? r2.y : kFarR2);
       R0 <<= 1;
       R1 <<= 1;
     }
-    const float2 qq = __fmul2_rn(I.q, dup2(J.q));
+    const float2 qq = __fmul2_rn(I.q, J.q);
     float2 g = make_float2(0.f, 0.f);
     if (K.use_gb) {
       // E = P qq / f, f^2 = r^2 + B_i B_j e^(-r^2 / 4 B_i B_j); A = P qq / f^3
-      const float2 w = __fmul2_rn(r2, __fmul2_rn(I.iB, dup2(J.iB)));  // r^2 log2(e) / (4 B_i B_j)
+      const float2 w = __fmul2_rn(r2, __fmul2_rn(I.iB, J.iB));  // r^2 log2(e) / (4 B_i B_j)
       const float2 ex = make_float2(exp2f(-w.x), exp2f(-w.y));
-      const float2 f2 = __ffma2_rn(__fmul2_rn(I.B, dup2(J.B)), ex, r2);
+      const float2 f2 = __ffma2_rn(__fmul2_rn(I.B, J.B), ex, r2);
       const float2 inv_f = make_float2(rsqrtf(f2.x), rsqrtf(f2.y));
       float2 A = __fmul2_rn(__fmul2_rn(dup2(K.pref), qq), __fmul2_rn(__fmul2_rn(inv_f, inv_f), inv_f));
       if (CUT && K.gcut2 != 0.f) A = __fmul2_rn(A, sel2(r2.x < K.gcut2, r2.y < K.gcut2, 1.f, 0.f));
       g = __fmul2_rn(A, __ffma2_rn(dup2(-0.5f), ex, dup2(2.0f)));  // -dE/dr / r
       const float2 c = __fmul2_rn(__fmul2_rn(A, ex),
                                   __ffma2_rn(w, dup2(-kInvQuarterLog2e * 0.25f), dup2(-1.0f)));
-      ti.a3 = __ffma2_rn(c, dup2(J.B), ti.a3);  // dE/dB_i B_i = c B_j
+      ti.a3 = __ffma2_rn(c, J.B, ti.a3);  // dE/dB_i B_i = c B_j
       tj.a3 = fmaf(c.x, I.B.x, fmaf(c.y, I.B.y, tj.a3));
     }
     if (K.use_lj || K.use_coul) {
@@ -189,10 +247,10 @@ __device__ __forceinline__ void run_force_tile2(const FData2 &I, PData &J, Acc2F
         if (EXCL) s = __fmul2_rn(s, sc_c);
       }
       if (K.use_lj) {
-        const float2 sig = __fadd2_rn(I.hs, dup2(J.hs));
+        const float2 sig = __fadd2_rn(I.hs, J.hs);
         const float2 sr2 = __fmul2_rn(__fmul2_rn(sig, sig), inv_r2);
         const float2 s6 = __fmul2_rn(__fmul2_rn(sr2, sr2), sr2);
-        float2 eps24 = __fmul2_rn(I.se, dup2(J.se));  // se = sqrt(24 eps)
+        float2 eps24 = __fmul2_rn(I.se, J.se);  // se = sqrt(24 eps)
         if (EXCL) eps24 = __fmul2_rn(eps24, sc_l);
         s = __ffma2_rn(__fmul2_rn(eps24, s6), __ffma2_rn(dup2(2.0f), s6, dup2(-1.0f)), s);
       }
@@ -205,9 +263,8 @@ __device__ __forceinline__ void run_force_tile2(const FData2 &I, PData &J, Acc2F
     tj.a0 = fmaf(-g.x, dx.x, fmaf(-g.y, dx.y, tj.a0));
     tj.a1 = fmaf(-g.x, dy.x, fmaf(-g.y, dy.y, tj.a1));
     tj.a2 = fmaf(-g.x, dz.x, fmaf(-g.y, dz.y, tj.a2));
-    J.x = shfl_next(J.x, src); J.y = shfl_next(J.y, src); J.z = shfl_next(J.z, src);
     tj.a0 = shfl_next(tj.a0, src);
-    rotate_force_rest(J, tj, src, K);
+    rotate_force_rest(tj, src, K);
   }
 }
 
@@ -256,11 +313,11 @@ struct BCPair2 {
 };
 
 template <int PASS, bool CUT, bool FULL, int TIER>
-__device__ __forceinline__ void bc_series2(const PData2 &I, const PData &J, bool ok0, bool ok1, BCPair2 &P,
+__device__ __forceinline__ void bc_series2(const PData2 &I, const JD2 &J, bool ok0, bool ok1, BCPair2 &P,
                                            const TileConst &K) {
-  P.dx = __fadd2_rn(I.x, dup2(-J.x));
-  P.dy = __fadd2_rn(I.y, dup2(-J.y));
-  P.dz = __fadd2_rn(I.z, dup2(-J.z));
+  P.dx = __fadd2_rn(I.x, J.mx);
+  P.dy = __fadd2_rn(I.y, J.my);
+  P.dz = __fadd2_rn(I.z, J.mz);
   const float2 r2 = __ffma2_rn(P.dx, P.dx, __ffma2_rn(P.dy, P.dy, __fmul2_rn(P.dz, P.dz)));
   if (CUT) {
     ok0 = ok0 && (K.bcut2 == 0.f || r2.x < K.bcut2);
@@ -275,25 +332,25 @@ __device__ __forceinline__ void bc_series2(const PData2 &I, const PData &J, bool
   const float2 inv_r2 = __fmul2_rn(P.inv_r, P.inv_r);
   const float2 inv_r4 = __fmul2_rn(inv_r2, inv_r2);
   if (PASS == PASS_BORN) {
-    P.vij = __fmul2_rn(dup2(J.s3), ObcPoly<false, TIER>::eval2(__fmul2_rn(dup2(J.s2), inv_r2)));
+    P.vij = __fmul2_rn(J.s3, ObcPoly<false, TIER>::eval2(__fmul2_rn(J.s2, inv_r2)));
     P.vji = __fmul2_rn(I.s3, ObcPoly<false, TIER>::eval2(__fmul2_rn(I.s2, inv_r2)));
     P.f = inv_r4;
   } else {
-    P.vij = __fmul2_rn(dup2(J.s3), ObcPoly<true, TIER>::eval2(__fmul2_rn(dup2(J.s2), inv_r2)));
+    P.vij = __fmul2_rn(J.s3, ObcPoly<true, TIER>::eval2(__fmul2_rn(J.s2, inv_r2)));
     P.vji = __fmul2_rn(I.s3, ObcPoly<true, TIER>::eval2(__fmul2_rn(I.s2, inv_r2)));
     P.f = __fmul2_rn(inv_r4, inv_r2);
   }
 }
 
 template <int PASS>
-__device__ __forceinline__ void bc_accumulate2(const PData2 &I, const PData &J, const BCPair2 &P, Acc2 &ti,
+__device__ __forceinline__ void bc_accumulate2(const PData2 &I, const JD2 &J, const BCPair2 &P, Acc2 &ti,
                                                Acc &tj) {
   if (PASS == PASS_BORN) {
     ti.a0 = __ffma2_rn(P.vij, P.f, ti.a0);
     tj.a0 = fmaf(P.vji.x, P.f.x, fmaf(P.vji.y, P.f.y, tj.a0));
   } else {
     // h = -(dE/dI_i dI_ij/dr + dE/dI_j dI_ji/dr) / r; F_i += h d, F_j -= h d
-    const float2 h = __fmul2_rn(__ffma2_rn(I.dedi, P.vij, __fmul2_rn(dup2(J.dedi), P.vji)), P.f);
+    const float2 h = __fmul2_rn(__ffma2_rn(I.dedi, P.vij, __fmul2_rn(J.dedi, P.vji)), P.f);
     ti.a0 = __ffma2_rn(h, P.dx, ti.a0);
     ti.a1 = __ffma2_rn(h, P.dy, ti.a1);
     ti.a2 = __ffma2_rn(h, P.dz, ti.a2);
@@ -372,13 +429,14 @@ __device__ __forceinline__ void cf_drain(CfQueue &Q, int lane) {
 // each pair is tested, and those outside the domain go to the warp's
 // closed-form queue with their series terms zeroed.
 template <int PASS, bool FAR, bool CUT, bool FULL, int TIER>
-__device__ __forceinline__ void run_bc_tile2(const PData2 &I, PData &J, Acc2 &ti, Acc &tj, uint32_t V0,
+__device__ __forceinline__ void run_bc_tile2(const PData2 &I, const JTile &jt, Acc2 &ti, Acc &tj, uint32_t V0,
                                              uint32_t V1, const TileConst &K, CfQueue &Q) {
   const int src = K.src;
   // step k tests the sign bit of the bit-reversed mask shifted left k times
   uint32_t R0 = __brev(V0), R1 = __brev(V1);
 #pragma unroll kUnrollBC
   for (int k = 0; k < 32; ++k) {
+    const JD2 J = load_jd<PASS, FAR>(jt, (K.lane + k) & 31);  // lane l meets j-lane (l + k) mod 32
     BCPair2 P;
     bc_series2<PASS, CUT, FULL, TIER>(I, J, FULL || (int32_t)R0 < 0, FULL || (int32_t)R1 < 0, P, K);
     if (!FULL) {
@@ -410,12 +468,8 @@ __device__ __forceinline__ void run_bc_tile2(const PData2 &I, PData &J, Acc2 &ti
       }
     }
     bc_accumulate2<PASS>(I, J, P, ti, tj);
-    J.x = shfl_next(J.x, src); J.y = shfl_next(J.y, src); J.z = shfl_next(J.z, src);
-    J.s2 = shfl_next(J.s2, src); J.s3 = shfl_next(J.s3, src);
-    if (!FAR) J.t2 = shfl_next(J.t2, src);
     tj.a0 = shfl_next(tj.a0, src);
     if (PASS == PASS_CHAIN) {
-      J.dedi = shfl_next(J.dedi, src);
       tj.a1 = shfl_next(tj.a1, src); tj.a2 = shfl_next(tj.a2, src);
     }
   }
@@ -452,6 +506,9 @@ __global__ void __launch_bounds__(256, PASS == PASS_BORN ? PB2_MINB_BORN : (PASS
   K.lane = lane;
   // closed-form queues of the descreening and chain passes, one per warp
   __shared__ int2 s_cfq[PASS == PASS_FORCE ? 1 : 8][PASS == PASS_FORCE ? 1 : kCfCap];
+  // the j-block of the current tile, one JTile per warp (2 KB)
+  __shared__ JTile s_jt[8];
+  JTile &jt = s_jt[threadIdx.x >> 5];
   CfQueue Q;
   Q.c = {a.posq, a.par, a.born, a.dedb_acc, a.born_acc, a.fx, a.fy, a.fz};
   Q.q = s_cfq[PASS == PASS_FORCE ? 0 : (threadIdx.x >> 5)];
@@ -509,6 +566,9 @@ __global__ void __launch_bounds__(256, PASS == PASS_BORN ? PB2_MINB_BORN : (PASS
       const int jg = off + (jvalid ? jl : n - 1);
       PData J;
       load_pdata(a, jg, PASS, K.use_gb, S.ro_max, J);
+      __syncwarp();  // every lane is done with the previous tile's j data
+      store_j<PASS>(jt, lane, J);
+      __syncwarp();
       // pair validity of lane i with j-lane c: both exist, j > i on a diagonal
       const int nj = n - jl0;
       const uint32_t jmask = nj >= 32 ? 0xffffffffu : ((1u << nj) - 1u);
@@ -542,9 +602,9 @@ __global__ void __launch_bounds__(256, PASS == PASS_BORN ? PB2_MINB_BORN : (PASS
                            make_float2(I0.q, I1.q), make_float2(I0.hs, I1.hs), make_float2(I0.se, I1.se),
                            make_float2(I0.B, I1.B), make_float2(I0.iB, I1.iB)};
         Acc2F tf = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-        if (hit) run_force_tile2<CUT, false, true>(IF, J, tf, tj, V0, V1, E0, E1, S0, S1, K);
-        else if (!full) run_force_tile2<CUT, false, false>(IF, J, tf, tj, V0, V1, E0, E1, S0, S1, K);
-        else run_force_tile2<CUT, true, false>(IF, J, tf, tj, V0, V1, E0, E1, S0, S1, K);
+        if (hit) run_force_tile2<CUT, false, true>(IF, jt, tf, tj, V0, V1, E0, E1, S0, S1, K);
+        else if (!full) run_force_tile2<CUT, false, false>(IF, jt, tf, tj, V0, V1, E0, E1, S0, S1, K);
+        else run_force_tile2<CUT, true, false>(IF, jt, tf, tj, V0, V1, E0, E1, S0, S1, K);
         t0.a0 = tf.a0.x; t0.a1 = tf.a1.x; t0.a2 = tf.a2.x; t0.a3 = tf.a3.x;
         t1.a0 = tf.a0.y; t1.a1 = tf.a1.y; t1.a2 = tf.a2.y; t1.a3 = tf.a3.y;
       } else {
@@ -555,17 +615,17 @@ __global__ void __launch_bounds__(256, PASS == PASS_BORN ? PB2_MINB_BORN : (PASS
         // tiles whose 64 x 32 pairs all exist skip the validity masks
         const bool full = __all_sync(kFull, (C0 & C1) == 0xffffffffu);
         if (full) {
-          if (d2 >= tier2[0]) run_bc_tile2<PASS, true, CUT, true, 0>(I2, J, ti, tj, V0, V1, K, Q);
-          else if (d2 >= tier2[1]) run_bc_tile2<PASS, true, CUT, true, 1>(I2, J, ti, tj, V0, V1, K, Q);
-          else if (d2 >= tier2[2]) run_bc_tile2<PASS, true, CUT, true, 2>(I2, J, ti, tj, V0, V1, K, Q);
-          else if (d2 >= S.far2) run_bc_tile2<PASS, true, CUT, true, 3>(I2, J, ti, tj, V0, V1, K, Q);
-          else run_bc_tile2<PASS, false, CUT, true, 3>(I2, J, ti, tj, V0, V1, K, Q);
+          if (d2 >= tier2[0]) run_bc_tile2<PASS, true, CUT, true, 0>(I2, jt, ti, tj, V0, V1, K, Q);
+          else if (d2 >= tier2[1]) run_bc_tile2<PASS, true, CUT, true, 1>(I2, jt, ti, tj, V0, V1, K, Q);
+          else if (d2 >= tier2[2]) run_bc_tile2<PASS, true, CUT, true, 2>(I2, jt, ti, tj, V0, V1, K, Q);
+          else if (d2 >= S.far2) run_bc_tile2<PASS, true, CUT, true, 3>(I2, jt, ti, tj, V0, V1, K, Q);
+          else run_bc_tile2<PASS, false, CUT, true, 3>(I2, jt, ti, tj, V0, V1, K, Q);
         } else {
-          if (d2 >= tier2[0]) run_bc_tile2<PASS, true, CUT, false, 0>(I2, J, ti, tj, V0, V1, K, Q);
-          else if (d2 >= tier2[1]) run_bc_tile2<PASS, true, CUT, false, 1>(I2, J, ti, tj, V0, V1, K, Q);
-          else if (d2 >= tier2[2]) run_bc_tile2<PASS, true, CUT, false, 2>(I2, J, ti, tj, V0, V1, K, Q);
-          else if (d2 >= S.far2) run_bc_tile2<PASS, true, CUT, false, 3>(I2, J, ti, tj, V0, V1, K, Q);
-          else run_bc_tile2<PASS, false, CUT, false, 3>(I2, J, ti, tj, V0, V1, K, Q);
+          if (d2 >= tier2[0]) run_bc_tile2<PASS, true, CUT, false, 0>(I2, jt, ti, tj, V0, V1, K, Q);
+          else if (d2 >= tier2[1]) run_bc_tile2<PASS, true, CUT, false, 1>(I2, jt, ti, tj, V0, V1, K, Q);
+          else if (d2 >= tier2[2]) run_bc_tile2<PASS, true, CUT, false, 2>(I2, jt, ti, tj, V0, V1, K, Q);
+          else if (d2 >= S.far2) run_bc_tile2<PASS, true, CUT, false, 3>(I2, jt, ti, tj, V0, V1, K, Q);
+          else run_bc_tile2<PASS, false, CUT, false, 3>(I2, jt, ti, tj, V0, V1, K, Q);
         }
         if (Q.n >= 32) cf_drain<PASS>(Q, lane);  // a pair for every lane
         t0.a0 = ti.a0.x; t0.a1 = ti.a1.x; t0.a2 = ti.a2.x;
