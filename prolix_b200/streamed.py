@@ -9,8 +9,9 @@ them with ``pb2_langevin_run_host``.  All groups share one stream for their
 copies in and one for their copies out, so each direction moves one group's
 state at a time at full PCIe speed, in group order, while other groups'
 steps run: the transfers hide behind the arithmetic except for the first
-group's copy in and the last group's copy out.  Each system's trajectory is the one it has in any other batch
-(the pair kernels' sums do not depend on the batch a system runs in).
+group's copy in and the last group's copy out.  Each system's trajectory is
+the one it has in any other batch (the pair kernels' sums do not depend on
+the batch a system runs in).
 """
 
 from __future__ import annotations
