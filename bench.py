@@ -462,6 +462,8 @@ def main():
   from prolix_b200 import engine
   systems = workload(rank, args.systems)
   n_atoms = int(sum(len(s["charges"]) for s in systems))
+  # each rank has its own seeded systems: the job's atoms are their sum
+  job_atoms = int(round(replicas.reduce_sum(float(n_atoms), device="cuda")))
   pairs = unique_pairs(systems)
   batch = engine.Batch(systems, device=local, keep_atom_order=args.keep_atom_order)
   batch.langevin_init()
@@ -497,7 +499,7 @@ def main():
   status = batch.status()
   if np.any(status):
     print(f"rank {rank}: status flags {np.unique(status)}", file=sys.stderr)
-  value = n_atoms * ws * args.steps / (t_ms * 1e-3)
+  value = job_atoms * args.steps / (t_ms * 1e-3)
 
   # per-kernel device times: eager launches with CUDA events around each
   batch.set_profiling(True)
@@ -564,10 +566,12 @@ def main():
         for it in range(2 + e2e_steps):
           if it == 2:
             torch.cuda.synchronize()
+            replicas.barrier()
             t0 = time.perf_counter()
           ens.run_host(host["position"], host["momentum"], host["force"], 1)
-        t_e2e = time.perf_counter() - t0
-        by_groups[str(len(ens.batches))] = n_atoms * ws * e2e_steps / t_e2e
+        # every rank steps its own systems; the slowest rank's time counts
+        t_e2e = replicas.reduce_max(time.perf_counter() - t0, device="cuda")
+        by_groups[str(len(ens.batches))] = job_atoms * e2e_steps / t_e2e
     head = str(min(args.e2e_groups[0], len(systems)))
     e2e = {"value": by_groups[head], "unit": UNIT,
            "h2d_bytes_per_step": int(nbytes), "d2h_bytes_per_step": int(nbytes),
