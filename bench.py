@@ -48,12 +48,12 @@ N_SYSTEMS = 512
 # series_terms() gives the pair-weighted mean K of each.
 #   descreening: 3 (d) + 5 (r^2) + 2 (1/r^2, 1/r^4)
 #                + 2 x (1 + 2(K-1) + 1) (u, polynomial, s^3) + 2 x 2 (sums) = 4K + 14
-#   force:       8 (d, r^2) + 1 (q q) + GB 16 + 4 (dE/dB) + 1 (1/r^2)
-#                + Coulomb 2 + LJ 11 + 2 (sum) + 12 (F)                  = 57
+#   force:       8 (d, r^2) + GB 15 (w, f^2, 1/f^3, A2, g) + 4 (dE/dB)
+#                + 1 (1/r^2) + Coulomb 2 + LJ 11 + 2 (sum) + 12 (F)      = 55
 #   chain:       3 (d) + 5 (r^2) + 3 (1/r^2, -1/r^6)
 #                + 2 x (1 + 2(K-1) + 1) + 4 (g) + 12 (F)                  = 4K + 27
 def flops_per_pair(k_mean: dict) -> dict:
-  return {"born": 4.0 * k_mean["value"] + 14.0, "force": 57.0, "chain": 4.0 * k_mean["deriv"] + 27.0}
+  return {"born": 4.0 * k_mean["value"] + 14.0, "force": 55.0, "chain": 4.0 * k_mean["deriv"] + 27.0}
 
 
 def series_tiers() -> dict:

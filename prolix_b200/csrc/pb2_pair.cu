@@ -184,7 +184,9 @@ __device__ __forceinline__ void load_pdata(const PairArgs &a, int g, int pass, b
 constexpr float kFarR2 = 1e30f;
 
 struct FData2 {  // the lane's two i atoms, packed, for the force pass
-  float2 x, y, z, q, hs, se, B, iB;
+  float2 x, y, z, hs, se, B, iB;
+  float2 q2p;  // 2 P q_i: the GB factor A2 = 2 P q_i q_j / f^3 in one product
+  float2 qk;   // k_C q_i
 };
 __device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
 __device__ __forceinline__ float2 sel2(bool a, bool b, float va, float vb) {
@@ -215,19 +217,20 @@ __device__ __forceinline__ void run_force_tile2(const FData2 &I, const JTile &jt
       R0 <<= 1;
       R1 <<= 1;
     }
-    const float2 qq = __fmul2_rn(I.q, J.q);
     float2 g = make_float2(0.f, 0.f);
     if (K.use_gb) {
-      // E = P qq / f, f^2 = r^2 + B_i B_j e^(-r^2 / 4 B_i B_j); A = P qq / f^3
-      const float2 w = __fmul2_rn(r2, __fmul2_rn(I.iB, J.iB));  // r^2 log2(e) / (4 B_i B_j)
+      // E = P qq / f, f^2 = r^2 + B_i B_j e^(-r^2 / 4 B_i B_j); with
+      // A2 = 2 P qq / f^3:  -dE/dr / r = A2 (1 - e / 4),
+      // dE/dB_i B_i = A2 e (-1/2 - w / (2 log2 e)) B_j,  w = r^2 log2(e) / (4 B_i B_j)
+      const float2 w = __fmul2_rn(r2, __fmul2_rn(I.iB, J.iB));
       const float2 ex = make_float2(exp2f(-w.x), exp2f(-w.y));
       const float2 f2 = __ffma2_rn(__fmul2_rn(I.B, J.B), ex, r2);
       const float2 inv_f = make_float2(rsqrtf(f2.x), rsqrtf(f2.y));
-      float2 A = __fmul2_rn(__fmul2_rn(dup2(K.pref), qq), __fmul2_rn(__fmul2_rn(inv_f, inv_f), inv_f));
-      if (CUT && K.gcut2 != 0.f) A = __fmul2_rn(A, sel2(r2.x < K.gcut2, r2.y < K.gcut2, 1.f, 0.f));
-      g = __fmul2_rn(A, __ffma2_rn(dup2(-0.5f), ex, dup2(2.0f)));  // -dE/dr / r
-      const float2 c = __fmul2_rn(__fmul2_rn(A, ex),
-                                  __ffma2_rn(w, dup2(-kInvQuarterLog2e * 0.25f), dup2(-1.0f)));
+      float2 A2 = __fmul2_rn(__fmul2_rn(I.q2p, J.q), __fmul2_rn(__fmul2_rn(inv_f, inv_f), inv_f));
+      if (CUT && K.gcut2 != 0.f) A2 = __fmul2_rn(A2, sel2(r2.x < K.gcut2, r2.y < K.gcut2, 1.f, 0.f));
+      const float2 A2e = __fmul2_rn(A2, ex);
+      g = __ffma2_rn(dup2(-0.25f), A2e, A2);
+      const float2 c = __fmul2_rn(A2e, __ffma2_rn(w, dup2(-kInvQuarterLog2e * 0.125f), dup2(-0.5f)));
       ti.a3 = __ffma2_rn(c, J.B, ti.a3);  // dE/dB_i B_i = c B_j
       tj.a3 = fmaf(c.x, I.B.x, fmaf(c.y, I.B.y, tj.a3));
     }
@@ -243,7 +246,7 @@ __device__ __forceinline__ void run_force_tile2(const FData2 &I, const JTile &jt
       }
       float2 s = make_float2(0.f, 0.f);  // (-dE/dr) r for Coulomb and LJ
       if (K.use_coul) {
-        s = __fmul2_rn(__fmul2_rn(dup2(K.kcoul), qq), inv_r);
+        s = __fmul2_rn(__fmul2_rn(I.qk, J.q), inv_r);
         if (EXCL) s = __fmul2_rn(s, sc_c);
       }
       if (K.use_lj) {
@@ -599,8 +602,10 @@ __global__ void __launch_bounds__(256, PASS == PASS_BORN ? PB2_MINB_BORN : (PASS
           E1 = rotr32(r.excl, lane); S1 = rotr32(r.s14, lane);
         }
         const FData2 IF = {make_float2(I0.x, I1.x), make_float2(I0.y, I1.y), make_float2(I0.z, I1.z),
-                           make_float2(I0.q, I1.q), make_float2(I0.hs, I1.hs), make_float2(I0.se, I1.se),
-                           make_float2(I0.B, I1.B), make_float2(I0.iB, I1.iB)};
+                           make_float2(I0.hs, I1.hs), make_float2(I0.se, I1.se),
+                           make_float2(I0.B, I1.B), make_float2(I0.iB, I1.iB),
+                           make_float2(2.f * K.pref * I0.q, 2.f * K.pref * I1.q),
+                           make_float2(K.kcoul * I0.q, K.kcoul * I1.q)};
         Acc2F tf = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
         if (hit) run_force_tile2<CUT, false, true>(IF, jt, tf, tj, V0, V1, E0, E1, S0, S1, K);
         else if (!full) run_force_tile2<CUT, false, false>(IF, jt, tf, tj, V0, V1, E0, E1, S0, S1, K);
