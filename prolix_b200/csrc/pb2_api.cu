@@ -207,7 +207,8 @@ static int setup_items2(pb2_batch *b, int seg) {
   b->n_items2 = (int)items.size();
   for (int p = 0; p < 3; ++p) {
     const int cap = tile_kernel_occupancy(p, b->cut) * ctx->sm_count;
-    b->grid_pair[p] = std::max(1, std::min(cap, (b->n_items2 + 7) / 8));
+    const int w = tile_kernel_warps(p);
+    b->grid_pair[p] = std::max(1, std::min(cap, (b->n_items2 + w - 1) / w));
   }
   return PB2_OK;
 }

@@ -163,6 +163,7 @@ cudaError_t launch_tiles(int pass, const PairArgs &a, int grid, cudaStream_t st)
 cudaError_t launch_energy64(int pass, const Energy64Args &a, int grid, cudaStream_t st);
 cudaError_t launch_born_finalize(const FinalizeArgs &a, cudaStream_t st);
 int tile_kernel_occupancy(int pass, bool cut);
+int tile_kernel_warps(int pass);  // warps per block of a pair pass
 cudaError_t launch_bbox(const SysInfo *sys, const int32_t *blk_sys, const float4 *posq, float4 *bbox,
                         int n_blocks, cudaStream_t st);
 cudaError_t launch_bonded(const BondedArgs &a, int grid_cap, cudaStream_t st);

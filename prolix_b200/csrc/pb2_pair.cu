@@ -496,8 +496,26 @@ __device__ __forceinline__ void run_bc_tile2(const PData2 &I, const JTile &jt, A
 #ifndef PB2_MINB_CHAIN
 #define PB2_MINB_CHAIN 2
 #endif
+#ifndef PB2_MINB_FORCE
+#define PB2_MINB_FORCE 2
+#endif
+// threads per block of each pass (a multiple of 32, at most 256)
+#ifndef PB2_THREADS_BORN
+#define PB2_THREADS_BORN 256
+#endif
+#ifndef PB2_THREADS_FORCE
+#define PB2_THREADS_FORCE 256
+#endif
+#ifndef PB2_THREADS_CHAIN
+#define PB2_THREADS_CHAIN 256
+#endif
+template <int PASS>
+constexpr int kTileThreads =
+    PASS == PASS_BORN ? PB2_THREADS_BORN : (PASS == PASS_CHAIN ? PB2_THREADS_CHAIN : PB2_THREADS_FORCE);
+template <int PASS>
+constexpr int kTileMinBlocks = PASS == PASS_BORN ? PB2_MINB_BORN : (PASS == PASS_CHAIN ? PB2_MINB_CHAIN : PB2_MINB_FORCE);
 template <int PASS, bool CUT, bool ALL = false>
-__global__ void __launch_bounds__(256, PASS == PASS_BORN ? PB2_MINB_BORN : (PASS == PASS_CHAIN ? PB2_MINB_CHAIN : 2))
+__global__ void __launch_bounds__(kTileThreads<PASS>, kTileMinBlocks<PASS>)
     tile2_kernel(const PairArgs a) {
   const int lane = threadIdx.x & 31;
   const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
@@ -508,9 +526,10 @@ __global__ void __launch_bounds__(256, PASS == PASS_BORN ? PB2_MINB_BORN : (PASS
   K.src = (lane + 1) & 31;
   K.lane = lane;
   // closed-form queues of the descreening and chain passes, one per warp
-  __shared__ int2 s_cfq[PASS == PASS_FORCE ? 1 : 8][PASS == PASS_FORCE ? 1 : kCfCap];
+  constexpr int kWarps = kTileThreads<PASS> / 32;
+  __shared__ int2 s_cfq[PASS == PASS_FORCE ? 1 : kWarps][PASS == PASS_FORCE ? 1 : kCfCap];
   // the j-block of the current tile, one JTile per warp (2 KB)
-  __shared__ JTile s_jt[8];
+  __shared__ JTile s_jt[kWarps];
   JTile &jt = s_jt[threadIdx.x >> 5];
   CfQueue Q;
   Q.c = {a.posq, a.par, a.born, a.dedb_acc, a.born_acc, a.fx, a.fy, a.fz};
@@ -761,7 +780,7 @@ __global__ void born_finalize(const FinalizeArgs a) {
 
 template <int PASS, bool CUT, bool ALL>
 static void launch_one(const PairArgs &a, int grid, cudaStream_t st) {
-  tile2_kernel<PASS, CUT, ALL><<<grid, 256, 0, st>>>(a);
+  tile2_kernel<PASS, CUT, ALL><<<grid, kTileThreads<PASS>, 0, st>>>(a);
 }
 
 cudaError_t launch_tiles(int pass, const PairArgs &a, int grid, cudaStream_t st) {
@@ -809,8 +828,13 @@ cudaError_t launch_born_finalize(const FinalizeArgs &a, cudaStream_t st) {
 template <int PASS, bool CUT, bool ALL>
 static int occ_one() {
   int blocks = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, tile2_kernel<PASS, CUT, ALL>, 256, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, tile2_kernel<PASS, CUT, ALL>, kTileThreads<PASS>, 0);
   return blocks;
+}
+
+int tile_kernel_warps(int pass) {
+  return pass == PASS_BORN ? kTileThreads<PASS_BORN> / 32
+                           : (pass == PASS_CHAIN ? kTileThreads<PASS_CHAIN> / 32 : kTileThreads<PASS_FORCE> / 32);
 }
 
 int tile_kernel_occupancy(int pass, bool cut) {
