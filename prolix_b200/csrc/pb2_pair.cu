@@ -39,7 +39,7 @@
 // Unroll factor of the 32-step rotation loop (code size against loop
 // overhead; the instruction cache favours a partial unroll).
 #ifndef PB2_UNROLL
-#define PB2_UNROLL 4
+#define PB2_UNROLL 2
 #endif
 
 namespace pb2 {
