@@ -113,7 +113,7 @@ BYTES_PER_ATOM_STEP = 184
 # DRAM traffic per launch of each pair pass on this workload
 # (dram__bytes_read.sum + dram__bytes_write.sum of one `ncu --set full`
 # capture; profiles/pair_kernels_ragged512.md gives the command)
-TRAFFIC_BYTES = {"born": 24.17e6, "force": 71.88e6, "chain": 47.36e6}
+TRAFFIC_BYTES = {"born": 24.17e6, "force": 71.60e6, "chain": 47.37e6}
 
 
 def parse():
