@@ -546,6 +546,7 @@ def main():
                 "bytes_per_atom_step": BYTES_PER_ATOM_STEP}
 
   e2e = None
+  pipelined = None
   if not args.no_e2e:
     # every step: positions, momenta and forces in from page-locked host
     # buffers, one BAOAB step, and the same three arrays back out, through
@@ -572,12 +573,28 @@ def main():
         # every rank steps its own systems; the slowest rank's time counts
         t_e2e = replicas.reduce_max(time.perf_counter() - t0, device="cuda")
         by_groups[str(len(ens.batches))] = job_atoms * e2e_steps / t_e2e
+        if g == args.e2e_groups[0]:
+          # the same round trips queued without a host wait between steps
+          # (each step still copies x, p, F in from and out to the host
+          # arrays; the batches order each step's copy in after the previous
+          # copy out), synchronised once at the end
+          torch.cuda.synchronize()
+          replicas.barrier()
+          t0 = time.perf_counter()
+          for _ in range(e2e_steps):
+            ens.run_host(host["position"], host["momentum"], host["force"], 1, wait=False)
+          ens.synchronize()
+          t_pipe = replicas.reduce_max(time.perf_counter() - t0, device="cuda")
+          pipelined = job_atoms * e2e_steps / t_pipe
     head = str(min(args.e2e_groups[0], len(systems)))
     e2e = {"value": by_groups[head], "unit": UNIT,
            "h2d_bytes_per_step": int(nbytes), "d2h_bytes_per_step": int(nbytes),
            "steps": e2e_steps, "host_buffers": "page-locked", "groups": int(head),
            "by_groups": by_groups,
-           "path": "pb2_langevin_run_host(1 step, x, p, F) per group of systems, one stream per group"}
+           "pipelined_no_host_wait": pipelined,
+           "path": "pb2_langevin_run_host(1 step, x, p, F) per group of systems, one stream per group; "
+                   "the host waits for every step's state before the next (pipelined_no_host_wait: "
+                   "the same round trips without that wait)"}
   batch.close()
 
   plain = None

@@ -99,16 +99,21 @@ class StreamedEnsemble:
       bt.get_state(st.cuda_stream, fields=fields, out={f: self._views(out[f], g) for f in fields})
     return {f: out[f] for f in fields}
 
-  def run_host(self, position, momentum, force, n_steps: int):
+  def run_host(self, position, momentum, force, n_steps: int, wait: bool = True):
     """n_steps BAOAB steps of every system on the state in the three arrays,
-    written back in place; returns once all groups have finished."""
+    written back in place.  With ``wait`` it returns once all groups have
+    finished; without, it returns at once, and a later call on the same
+    arrays still reads each group's state only after that group's previous
+    copy out has landed (the batch orders its copies), so a caller can queue
+    several round trips and ``synchronize()`` before reading the arrays."""
     for a in (position, momentum, force):
       if not isinstance(a, np.ndarray) or a.shape != (self.n_atoms, 3):
         raise ValueError(f"run_host: arrays must be ({self.n_atoms}, 3)")
     for g, (bt, st) in enumerate(zip(self.batches, self.streams)):
       bt.langevin_run_host(self._views(position, g), self._views(momentum, g), self._views(force, g),
                            n_steps, st.cuda_stream, self.copy_in.cuda_stream, self.copy_out.cuda_stream)
-    self.synchronize()
+    if wait:
+      self.synchronize()
 
   def close(self):
     for bt in getattr(self, "batches", []):

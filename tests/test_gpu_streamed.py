@@ -87,3 +87,23 @@ def test_spatial_atom_order_is_invisible_to_the_caller():
     xa = a.get_state(fields=("position",))["position"]
     xb = b.get_state(fields=("position",))["position"]
     assert np.max(np.abs(xa - xb)) < 1e-4
+
+
+def test_queued_round_trips_without_host_waits():
+  # several host round trips queued back to back (each step copies the state
+  # in from and out to the same host arrays) give the state of the same
+  # steps run on the device alone
+  systems = _systems()
+  fields = ("position", "momentum", "force")
+  with engine.Batch(systems) as one, streamed.StreamedEnsemble(systems, groups=3) as ens:
+    one.langevin_init()
+    ens.langevin_init()
+    st = ens.get_state()
+    ens.synchronize()
+    for _ in range(4):
+      ens.run_host(st["position"], st["momentum"], st["force"], 2, wait=False)
+    ens.synchronize()
+    one.langevin_run(8)
+    ref = one.get_state(fields=fields)
+    for f in fields:
+      assert np.array_equal(st[f], ref[f]), f
