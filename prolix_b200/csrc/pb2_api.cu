@@ -9,12 +9,14 @@
 //   kernels; float4 born (B, 1/B, dB/dI); int64 descreening and dE/dB sums;
 //   per-system SysInfo records, keys (two buffers), step counters, status.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <map>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "pb2_common.cuh"
@@ -310,6 +312,32 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   const double born_cut = params->born_cutoff > 0.0 ? params->born_cutoff : gb_cut;
   const bool born_mode = born_cut > 0.0;  // Born radii from a cutoff: its clamps apply
 
+  // --- stored atom order of each system (spatial unless asked to keep the
+  // input order), computed for all systems at once on the host's cores
+  std::vector<std::vector<int>> orders(n_systems);
+  {
+    auto work = [&](int s) {
+      std::vector<int> &ord = orders[s];
+      const int n = systems[s].n_atoms;
+      if (params->keep_atom_order) {
+        ord.resize(n);
+        for (int i = 0; i < n; ++i) ord[i] = i;
+      } else {
+        spatial_order(systems[s].positions, n, ord);
+      }
+    };
+    const int n_threads =
+        std::max(1, std::min<int>(n_systems, std::min(16u, std::max(1u, std::thread::hardware_concurrency()))));
+    std::atomic<int> next{0};
+    auto worker = [&]() {
+      for (int s; (s = next.fetch_add(1)) < n_systems;) work(s);
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < n_threads; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto &t : pool) t.join();
+  }
+
   // --- per-atom host arrays
   int64_t total = 0;
   int blocks_total = 0;
@@ -409,12 +437,7 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
       }
       return -1;
     };
-    if (params->keep_atom_order) {
-      ord.resize(n);
-      for (int i = 0; i < n; ++i) ord[i] = i;
-    } else {
-      spatial_order(d.positions, n, ord);
-    }
+    ord.swap(orders[s]);
     for (int l = 0; l < n; ++l) inv[ord[l]] = l;
     int over = build_excl();
     if (over >= 0 && !params->keep_atom_order) {
@@ -524,15 +547,16 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
 
   // terms in order of their (central) atom: with atoms in spatial order, the
   // threads of a warp then read and update nearby atoms
-  auto by_atom = [](auto &idx, auto &par, auto key) {
-    std::vector<int> o(idx.size());
-    for (size_t k = 0; k < o.size(); ++k) o[k] = (int)k;
-    std::stable_sort(o.begin(), o.end(), [&](int p, int q) { return key(idx[p]) < key(idx[q]); });
+  auto by_atom = [N](auto &idx, auto &par, auto key) {  // stable counting sort by key in [0, N)
+    std::vector<int> start(N + 1, 0);
+    for (const auto &t : idx) ++start[key(t) + 1];
+    for (int a = 0; a < N; ++a) start[a + 1] += start[a];
     auto idx2 = idx;
     auto par2 = par;
-    for (size_t k = 0; k < o.size(); ++k) {
-      idx2[k] = idx[o[k]];
-      par2[k] = par[o[k]];
+    for (size_t k = 0; k < idx.size(); ++k) {
+      const int dst = start[key(idx[k])]++;
+      idx2[dst] = idx[k];
+      par2[dst] = par[k];
     }
     idx.swap(idx2);
     par.swap(par2);
