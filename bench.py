@@ -438,7 +438,7 @@ def minimize_run(systems, stream):
 def serving_sweep(args):
   from prolix_b200 import serving
   res = {}
-  for rate in (10.0, 50.0, 200.0, 500.0):
+  for rate in (10.0, 50.0, 100.0, 200.0, 500.0):
     reqs = serving.poisson_requests(args.serving_requests, rate, WORKLOAD_SEED + int(rate),
                                     step_scale=args.serving_step_scale)
     srv = serving.Server(chunk=50)
