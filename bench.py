@@ -439,7 +439,9 @@ def serving_sweep(args):
   from prolix_b200 import serving
   res = {}
   for rate in (10.0, 50.0, 100.0, 200.0, 500.0):
-    reqs = serving.poisson_requests(args.serving_requests, rate, WORKLOAD_SEED + int(rate),
+    # the same requests (sizes, step counts) as the 20 req/s leg, arriving
+    # at this rate
+    reqs = serving.poisson_requests(args.serving_requests, rate, WORKLOAD_SEED,
                                     step_scale=args.serving_step_scale)
     srv = serving.Server(chunk=50)
     srv.run(reqs)
