@@ -239,3 +239,16 @@ def test_streamed_partition_covers_systems_in_balanced_ranges():
   assert max(work) / min(work) < 1.2
   assert streamed.partition([10, 20], 5) == [(0, 1), (1, 2)]
   assert streamed.partition([10], 3) == [(0, 1)]
+
+
+def test_bench_reads_the_kernels_series_tiers():
+  # bench.py's flop counts follow the tier table the kernels compile
+  import bench
+  tiers = bench.series_tiers()
+  assert tiers["value"] == ([0.0075, 0.036, 0.089, 0.16], [3, 4, 5, 6])
+  assert tiers["deriv"] == ([0.027, 0.07, 0.129, 0.16], [4, 5, 6, 7])
+  systems = synth.make_batch(4, 11, 150, 600, compact=True, **synth.PHYSICAL_RANGES)
+  k = bench.series_terms(systems)
+  assert 3.0 <= k["value"] <= 6.0 and 4.0 <= k["deriv"] <= 7.0
+  f = bench.flops_per_pair(k)
+  assert f["born"] == 4 * k["value"] + 14 and f["chain"] == 4 * k["deriv"] + 27 and f["force"] == 55.0
