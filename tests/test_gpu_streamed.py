@@ -107,3 +107,20 @@ def test_queued_round_trips_without_host_waits():
     ref = one.get_state(fields=fields)
     for f in fields:
       assert np.array_equal(st[f], ref[f]), f
+
+
+def test_round_trip_of_zero_steps_leaves_the_state():
+  # copies in and out with no step between: x, p and F come back bit for bit
+  # (fixed point -> FP64 -> fixed point is exact for the forces)
+  systems = _systems()[:3]
+  with engine.Batch(systems) as b:
+    b.langevin_init()
+    b.langevin_run(2)
+    st = b.get_state(fields=("position", "momentum", "force"))
+    host = {f: streamed.pinned(st[f].shape) for f in st}
+    for f in st:
+      host[f][...] = st[f]
+    b.langevin_run_host(host["position"], host["momentum"], host["force"], 0)
+    torch.cuda.synchronize()
+    for f in st:
+      assert np.array_equal(host[f], st[f]), f
