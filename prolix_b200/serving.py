@@ -1,12 +1,15 @@
 """Continuous-batching server for "run K Langevin steps of system S" jobs.
 
 Requests that arrive while others run join the device batch at the next
-tick: each tick advances every active system by the same number of steps
+tick: each tick advances every running system by the same number of steps
 (at most ``chunk``, and never past the nearest completion), then finished,
-cancelled or failed requests leave and waiting requests are admitted while
-the batch stays inside the atom and HBM budgets.  All systems of a tick
-share one launch per kernel (the ragged batch), so short and long, small
-and large jobs overlap on the GPU.
+cancelled or failed requests end, and waiting requests are admitted while
+the running systems stay inside the atom and HBM budgets.  All systems of a
+tick share one launch per kernel (the ragged batch), so short and long,
+small and large jobs overlap on the GPU.  The batch is rebuilt when
+requests are admitted (their initial momenta and forces come from one
+langevin_init of the new batch) or when ended systems, which keep stepping
+unread until then, hold a quarter of its atoms.
 
 Systems never interact and forces use order-independent fixed-point sums,
 so a request's result is bit-identical whether it ran alone or in any mix
@@ -100,7 +103,7 @@ class Server:
     self.cancelled: set[int] = set()
     self._next_id = 0
     self._batch = None
-    self._batch_ids = None
+    self._slot_of: list = []  # batch system index -> running slot, None once its request ended
     self.atom_steps = 0
     self.ticks = 0
     if self.batch_factory is engine.Batch:
@@ -138,7 +141,9 @@ class Server:
     atoms = sum(len(s.req.system["charges"]) for s in self.active)
     return atoms, atoms * BYTES_PER_ATOM
 
-  def _admit(self, now: float):
+  def _admit(self, now: float) -> list:
+    """Take waiting requests while the budget allows (first come, first
+    served); they join the batch at the next rebuild."""
     atoms, used = self._used()
     admitted = []
     while self.queue and self.queue[0].arrival <= now:
@@ -152,96 +157,127 @@ class Server:
       if atoms + n > self.max_atoms or used + n * BYTES_PER_ATOM > self.hbm_budget:
         break  # first-come first-served: wait for room
       self.queue.popleft()
+      # fix the system's float32 frame for its lifetime (bit-identical forces
+      # whatever batch it runs in)
+      if req.system.get("origin") is None:
+        req.system = dict(req.system, origin=engine.default_origin(req.system["positions"]))
       admitted.append(req)
       atoms += n
       used += n * BYTES_PER_ATOM
-    if not admitted:
-      return False
-    # fix each system's float32 frame for its lifetime (bit-identical forces
-    # whatever batch it runs in), then draw initial momenta from its key
-    for r in admitted:
-      if r.system.get("origin") is None:
-        r.system = dict(r.system, origin=engine.default_origin(r.system["positions"]))
-    systems = [dict(r.system, key=r.key, dt=r.dt, kT=r.kT, gamma=r.gamma) for r in admitted]
-    with self.batch_factory(systems, cutoff=self.cutoff, device=self.device) as nb:
-      nb.langevin_init()
-      st = nb.get_state(fields=_FIELDS)
-      status = nb.status()
-    for k, r in enumerate(admitted):
-      lo, hi = nb.offsets[k], nb.offsets[k + 1]
-      if status[k] & (STATUS_NONFINITE | STATUS_FORCE_RANGE) or not np.isfinite(st["position"][lo:hi]).all():
-        self._fail(r, now, now, "non-finite initial state")
-        continue
-      self.active.append(_Slot(r, st["position"][lo:hi].copy(), st["momentum"][lo:hi].copy(),
-                               st["force"][lo:hi].copy(), st["key"][k].copy(), 0, now))
-    return True
+    return admitted
 
   def _fail(self, req, admitted, now, msg):
     self.results[req.rid] = Result(req.rid, None, None, None, 0, req.arrival, admitted, now,
                                    error=msg)
 
-  def _build(self):
-    # each system is described by its submitted positions, which fix its
-    # stored atom order; its current state is restored below
-    systems = [dict(s.req.system, key=tuple(int(v) for v in s.key), dt=s.req.dt,
-                    kT=s.req.kT, gamma=s.req.gamma) for s in self.active]
+  def _build(self, admitted, now):
+    """A new batch of the running systems and the admitted requests.  Each
+    system is described by its submitted positions, which fix its stored
+    atom order.  One langevin_init draws the admitted requests' momenta from
+    their keys and evaluates their forces (the same bits as alone); then every
+    running system's saved state is restored, forces included, since forces
+    depend only on the system's own float32 frame."""
+    run_sys = [dict(s.req.system, key=tuple(int(v) for v in s.key), dt=s.req.dt, kT=s.req.kT,
+                    gamma=s.req.gamma) for s in self.active]
+    new_sys = [dict(r.system, key=r.key, dt=r.dt, kT=r.kT, gamma=r.gamma) for r in admitted]
     if self._batch is not None:
       self._batch.close()
-    self._batch = self.batch_factory(systems, cutoff=self.cutoff, device=self.device,
-                                     graph_chunk=self.chunk)
-    # forces are a function of each system's own float32 frame only, so the
-    # saved ones are bit-identical to a fresh evaluation in the new batch
-    self._batch.set_full_state(np.concatenate([s.x for s in self.active]),
-                               np.concatenate([s.p for s in self.active]),
-                               np.concatenate([s.f for s in self.active]),
-                               key=np.stack([s.key for s in self.active]))
-    self._batch_ids = [s.req.rid for s in self.active]
+      self._batch = None
+    batch = self.batch_factory(run_sys + new_sys, cutoff=self.cutoff, device=self.device,
+                               graph_chunk=self.chunk)
+    self._batch = batch
+    nr = len(run_sys)
+    slot_of = list(self.active)
+    st = None
+    if admitted:
+      batch.langevin_init()
+      st = batch.get_state(fields=_FIELDS)
+      status = batch.status(clear=True)
+      for k, r in enumerate(admitted):
+        b = nr + k
+        lo, hi = batch.offsets[b], batch.offsets[b + 1]
+        x = st["position"][lo:hi]
+        if status[b] & (STATUS_NONFINITE | STATUS_FORCE_RANGE) or not np.isfinite(x).all():
+          self._fail(r, now, now, "non-finite initial state")
+          slot_of.append(None)
+          continue
+        slot_of.append(_Slot(r, x.copy(), st["momentum"][lo:hi].copy(), st["force"][lo:hi].copy(),
+                             st["key"][b].copy(), 0, now))
+    self._slot_of = slot_of  # batch system index -> running slot (None: its request ended)
+    self.active = [s for s in slot_of if s is not None]
+    if nr:
+      # the running systems' saved state (the admitted ones keep the init's)
+      def rows(field, st_field):
+        return np.concatenate([getattr(slot_of[b], field) if b < nr
+                               else st[st_field][batch.offsets[b]:batch.offsets[b + 1]]
+                               for b in range(len(slot_of))])
+      keys = np.stack([slot_of[b].key if b < nr else st["key"][b] for b in range(len(slot_of))])
+      batch.set_full_state(rows("x", "position"), rows("p", "momentum"), rows("f", "force"), key=keys)
 
   def _save(self):
     st = self._batch.get_state(fields=_FIELDS)
-    for k, s in enumerate(self.active):
-      lo, hi = self._batch.offsets[k], self._batch.offsets[k + 1]
+    for b, s in enumerate(self._slot_of):
+      if s is None:
+        continue
+      lo, hi = self._batch.offsets[b], self._batch.offsets[b + 1]
       s.x = st["position"][lo:hi].copy()
       s.p = st["momentum"][lo:hi].copy()
       s.f = st["force"][lo:hi].copy()
-      s.key = st["key"][k].copy()
+      s.key = st["key"][b].copy()
     return self._batch.status(clear=True)
 
+  def _ended_atoms(self) -> int:
+    return sum(self._batch.sizes[b] for b, s in enumerate(self._slot_of) if s is None)
+
   def tick(self) -> bool:
-    """Admit, advance every active system, retire.  False when idle."""
+    """Admit, advance every running system, retire.  False when idle.
+
+    The batch is rebuilt only when requests are admitted, or when systems
+    whose requests have ended make up more than a quarter of its atoms:
+    until then they keep stepping unread (each system is independent, so
+    the others' results do not change)."""
     now = self.now()
-    changed = self._admit(now)
+    admitted = self._admit(now)
     if self.cancelled:
-      keep = [s for s in self.active if s.req.rid not in self.cancelled]
+      for b, s in enumerate(self._slot_of):
+        if s is not None and s.req.rid in self.cancelled:
+          self._slot_of[b] = None
       for s in self.active:
         if s.req.rid in self.cancelled and s.req.rid not in self.results:
           self._fail(s.req, s.admitted, now, "cancelled")
-      changed |= len(keep) != len(self.active)
-      self.active = keep
-    if not self.active:
+      self.active = [s for s in self.active if s.req.rid not in self.cancelled]
+    if not self.active and not admitted:
       if self._batch is not None:
         self._batch.close()
         self._batch = None
+        self._slot_of = []
       return bool(self.queue)
-    if changed or self._batch is None or self._batch_ids != [s.req.rid for s in self.active]:
-      self._build()
+    if (admitted or self._batch is None
+        or self._ended_atoms() * 4 > int(np.sum(self._batch.sizes))):
+      self._build(admitted, now)
+      if not self.active:
+        return bool(self.queue)
     n = min(self.chunk, min(s.req.n_steps - s.done for s in self.active))
     self._batch.langevin_run(n)
     status = self._save()
     self.ticks += 1
     now = self.now()
-    keep = []
-    for k, s in enumerate(self.active):
+    for b, s in enumerate(self._slot_of):
+      if s is None:
+        continue
       s.done += n
       self.atom_steps += n * len(s.req.system["charges"])
-      if status[k] & (STATUS_NONFINITE | STATUS_FORCE_RANGE) or not np.isfinite(s.x).all():
+      ended = True
+      if status[b] & (STATUS_NONFINITE | STATUS_FORCE_RANGE) or not np.isfinite(s.x).all():
         self._fail(s.req, s.admitted, now, "non-finite state: evicted")
       elif s.done >= s.req.n_steps:
         self.results[s.req.rid] = Result(s.req.rid, s.x, s.p, s.key, s.done, s.req.arrival,
                                          s.admitted, now)
       else:
-        keep.append(s)
-    self.active = keep
+        ended = False
+      if ended:
+        self._slot_of[b] = None
+    self.active = [s for s in self._slot_of if s is not None]
     return True
 
   def run(self, requests=(), until_idle=True, sleep=time.sleep):
