@@ -404,9 +404,9 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
       S.oy = d.origin[1];
       S.oz = d.origin[2];
     }
-    // atom order: spatial unless asked to keep the input order, or unless
-    // the spatial order gives an i-block exclusion partners in more j-blocks
-    // than the exclusion table holds
+    // the stored atom order computed above, or the input order when that
+    // one gives an i-block exclusion partners in more j-blocks than the
+    // exclusion table holds
     std::vector<int> ord;
     std::vector<int> &inv = inv_all[s];
     inv.resize(n);
