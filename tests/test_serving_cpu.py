@@ -103,3 +103,26 @@ def test_poisson_stream_is_seeded():
   assert [r.arrival for r in a] == [r.arrival for r in b]
   assert [r.n_steps for r in a] == [r.n_steps for r in b]
   assert all(np.diff([r.arrival for r in a]) > 0)
+
+
+def test_ended_requests_do_not_force_a_rebuild():
+  # four requests admitted together, ending one after another: the batch is
+  # built once for the admission and rebuilt only when the ended systems
+  # hold more than a quarter of its atoms; every request still gets exactly
+  # its steps
+  clk = Clock()
+  built = []
+
+  def factory(systems, **kw):
+    built.append(len(systems))
+    return FakeBatch(systems, **kw)
+
+  srv = serving.Server(chunk=10, clock=clk, batch_factory=factory)
+  reqs = [_req(i, 10, steps, 0.0) for i, steps in enumerate((10, 20, 30, 40))]
+  res = srv.run(reqs, sleep=clk.sleep)
+  for r in reqs:
+    assert res[r.rid].error is None and res[r.rid].steps == r.n_steps
+    np.testing.assert_allclose(res[r.rid].momentum, r.n_steps)
+  # one build with all four; after two have ended (half the atoms) a
+  # rebuild with the remaining two; the last one alone when three have ended
+  assert built[0] == 4 and len(built) <= 3 and all(b < 4 for b in built[1:])
