@@ -41,3 +41,39 @@ def test_streamed_frames_match_the_state(tmp_path):
     np.testing.assert_array_equal(last["velocities"],
                                   (st30["momentum"][lo:hi] * (1.0 / masses[k])).astype(np.float32))
   assert st["step"][0] == 33
+
+
+class _Frames(tr.XtcWriterBackend):
+  def __init__(self):
+    self.frames, self.times = [], []
+
+  def write_frame(self, coords_angstrom, *, time_ps=0.0):
+    self.frames.append(np.array(coords_angstrom))
+    self.times.append(time_ps)
+
+  def close(self):
+    pass
+
+
+def test_xtc_sink_gets_the_ring_frames(tmp_path):
+  """XtcFrameSink as the run_with_trajectory writer: the same positions as
+  the msgpack records of an identical run, with time in ps."""
+  systems = [synth.make_chain(n, 40 + n, compact=True, **synth.PHYSICAL_RANGES) for n in (150, 201)]
+  paths = [str(tmp_path / f"s{k}.pb2traj") for k in range(2)]
+  with engine.Batch(systems, key=prng.prng_key(8)) as b:
+    b.langevin_init()
+    writers = [tr.TrajectoryWriter(p) for p in paths]
+    tr.run_with_trajectory(b, 20, 4, writers, capacity=3, dt_ns=[1e-6, 2e-6])
+    for w in writers:
+      w.close()
+  backends = [_Frames(), _Frames()]
+  with engine.Batch(systems, key=prng.prng_key(8)) as b:
+    b.langevin_init()
+    sinks = [tr.XtcFrameSink(tmp_path / f"s{k}.xtc", backend=be) for k, be in enumerate(backends)]
+    assert tr.run_with_trajectory(b, 20, 4, sinks, capacity=3, dt_ns=[1e-6, 2e-6]) == 5
+  for k, (p, be) in enumerate(zip(paths, backends)):
+    frames = list(tr.read_trajectory(p))
+    assert len(be.frames) == len(frames) == 5
+    np.testing.assert_allclose(be.times, [4e-3 * (k + 1) * (f + 1) for f in range(5)], rtol=1e-12)
+    for f, got in zip(frames, be.frames):
+      np.testing.assert_array_equal(got, f["positions"])
