@@ -291,6 +291,35 @@ int pb2_traj_fetch(pb2_batch *batch, int32_t first, int32_t count, float *positi
 int pb2_get_status(pb2_batch *batch, uint32_t *status, int clear, void *stream);
 
 /*
+ * Safeguards of prolix's batched Langevin step (make_langevin_step,
+ * batched_simulate.py:218-382; its production values are vlimit 20,
+ * max_dx 0.5 A, force_cap 1e4 kcal/mol/A).  Each limit <= 0 is off; all off
+ * (the default) is the plain BAOAB step of pb2_langevin_run.  With limits set
+ * a step is
+ *   p += dt/2 F;  where |p/m| > vlimit: p *= min(1, vlimit / (|p/m| + 1e-30));
+ *   x_old = x;  A;  O;  A;
+ *   s = min(1, max_dx / |x - x_old|);  x = x_old + (x - x_old) s;
+ *   where |x - x_old| > max_dx: p *= s;
+ *   F = force(x);  F *= min(1, force_cap / |F|);  p += dt/2 F
+ * with |v| = sqrt(v.v + 1e-30) (1e-12 for F).  The capped closing force also
+ * opens the next step (the reference keeps it as the state's force); a force
+ * that no step produced (after pb2_langevin_init, pb2_set_positions,
+ * pb2_set_state, pb2_set_full_state or minimisation) opens the next step as
+ * it is.  pb2_get_state and pb2_langevin_run_host hand out the uncapped
+ * force; a host round trip that passes it back unchanged continues the run
+ * exactly.  Setting new limits drops captured graphs.
+ */
+int pb2_set_safeguards(pb2_batch *batch, double vlimit, double max_dx, double force_cap);
+int pb2_get_safeguards(const pb2_batch *batch, double *vlimit, double *max_dx, double *force_cap);
+
+/* Per-system counts (n_systems, 4) of the steps in which each safeguard
+ * fired, in prolix's warn_counts order (typing.py:559-563): vlimit, force
+ * cap, constraint violation (always 0: no constraints), displacement cap.
+ * The force-cap column is the reference's cap_count.  reset != 0 zeroes the
+ * counts after reading them. */
+int pb2_get_warn_counts(pb2_batch *batch, int32_t *counts, int reset, void *stream);
+
+/*
  * Neighbour list (cutoff > 0 only).  pb2_nl_build rebuilds unconditionally;
  * pb2_nl_check compares the displacement since the last build against
  * skin/2 (batched_simulate.py:1600-1622) and rebuilds where exceeded;

@@ -112,7 +112,21 @@ static IntArgs int_args(pb2_batch *b, int parity, int finish_prev) {
   a.parity = parity;
   a.finish_prev = finish_prev;
   a.partitionable = b->params.partitionable_keys;
+  a.vlimit = b->guard[0];
+  a.max_dx = b->guard[1];
+  a.force_cap = b->guard[2];
+  a.guard_end = b->guard_end;
+  a.warn_flags = b->warn_flags;
+  a.warn_counts = b->warn_counts;
   return a;
+}
+
+// The force accumulators no longer hold a step's closing force (the state
+// was set or moved outside a Langevin step): the next step applies them as
+// they are, without the force cap.
+static int forces_not_from_step(pb2_batch *b, cudaStream_t st) {
+  CUDA_TRY(b->ctx, cudaMemsetAsync(b->guard_end, 0, sizeof(int32_t), st));
+  return PB2_OK;
 }
 
 IntArgs int_args_for_nl(pb2_batch *b) { return int_args(b, b->key_parity, 0); }
@@ -599,6 +613,9 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   b->keys = D.alloc<uint32_t>(4 * (size_t)n_systems);
   b->steps = D.alloc<long long>(n_systems);
   b->status = D.alloc<uint32_t>(n_systems);
+  b->guard_end = D.alloc<int32_t>(1);
+  b->warn_flags = D.alloc<uint32_t>(2 * (size_t)n_systems);
+  b->warn_counts = D.alloc<int32_t>((size_t)n_systems * kWarnTypes);
   b->items = D.alloc<TileItem>(hitems.size());
   b->excl_ent = D.alloc<int2>(hent.size());
   b->excl_rows = D.alloc<ExclRow>(hrows.size());
@@ -652,6 +669,9 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   CUDA_TRY(ctx, cudaMemset(b->steps, 0, n_systems * sizeof(long long)));
   CUDA_TRY(ctx, cudaMemset(b->sched, 0, 8 * sizeof(int32_t)));
   CUDA_TRY(ctx, cudaMemset(b->status, 0, n_systems * sizeof(uint32_t)));
+  CUDA_TRY(ctx, cudaMemset(b->guard_end, 0, sizeof(int32_t)));
+  CUDA_TRY(ctx, cudaMemset(b->warn_flags, 0, 2 * (size_t)n_systems * sizeof(uint32_t)));
+  CUDA_TRY(ctx, cudaMemset(b->warn_counts, 0, (size_t)n_systems * kWarnTypes * sizeof(int32_t)));
   B.atom_sys = b->atom_sys;
   B.x = b->x; B.y = b->y; B.z = b->z;
   B.fx = b->fx; B.fy = b->fy; B.fz = b->fz;
@@ -894,8 +914,8 @@ static int download_soa3(pb2_batch *b, double *aos, const double *dx, const doub
 extern "C" int pb2_set_positions(pb2_batch *b, const double *positions, void *stream) {
   if (!b || !positions) return PB2_EINVAL;
   b->forces_valid = false;
-  const int rc = upload_soa3(b, positions, b->x, b->y, b->z, (cudaStream_t)stream);
-  if (rc) return rc;
+  int rc = upload_soa3(b, positions, b->x, b->y, b->z, (cudaStream_t)stream);
+  if (rc || (rc = forces_not_from_step(b, (cudaStream_t)stream))) return rc;
   CUDA_TRY(b->ctx, cudaStreamSynchronize((cudaStream_t)stream));
   return PB2_OK;
 }
@@ -958,7 +978,7 @@ extern "C" int pb2_langevin_init(pb2_batch *b, void *stream) {
   CUDA_TRY(ctx, launch_init(int_args(b, b->key_parity, 0), st));
   b->key_parity ^= 1;
   int rc = fresh_forces(b, st, false);
-  if (rc) return rc;
+  if (rc || (rc = forces_not_from_step(b, st))) return rc;
   CUDA_TRY(ctx, cudaStreamSynchronize(st));
   return PB2_OK;
 }
@@ -1043,7 +1063,7 @@ extern "C" int pb2_set_state(pb2_batch *b, const double *x, const double *p, con
   }
   if (x) {  // forces must follow the positions
     rc = fresh_forces(b, st, false);
-    if (rc) return rc;
+    if (rc || (rc = forces_not_from_step(b, st))) return rc;
   }
   CUDA_TRY(ctx, cudaStreamSynchronize(st));
   return PB2_OK;
@@ -1066,6 +1086,7 @@ extern "C" int pb2_set_full_state(pb2_batch *b, const double *x, const double *p
   }
   CUDA_TRY(ctx, launch_posq(int_args(b, b->key_parity, 0), st));
   b->forces_valid = true;
+  if ((rc = forces_not_from_step(b, st))) return rc;
   CUDA_TRY(ctx, cudaStreamSynchronize(st));
   return PB2_OK;
 }
@@ -1250,6 +1271,7 @@ extern "C" int pb2_min_sd(pb2_batch *b, int32_t n_steps, double k, int32_t kind,
   if ((rc = min_run(b, 0, n_steps, st))) return rc;
   CUDA_TRY(b->ctx, launch_min(kMinOpRollback, min_args(b), nullptr, st));
   b->forces_valid = false;  // a rolled-back system moved
+  if ((rc = forces_not_from_step(b, st))) return rc;
   CUDA_TRY(b->ctx, cudaStreamSynchronize(st));
   return PB2_OK;
 }
@@ -1272,6 +1294,7 @@ extern "C" int pb2_min_fire(pb2_batch *b, int32_t n_steps, double k, int32_t kin
   if (flags & PB2_FIRE_KEEP_BEST) CUDA_TRY(b->ctx, launch_min(kMinOpTakeBest, ma, nullptr, st));
   CUDA_TRY(b->ctx, launch_min(kMinOpRollback, ma, nullptr, st));
   b->forces_valid = false;
+  if ((rc = forces_not_from_step(b, st))) return rc;
   CUDA_TRY(b->ctx, cudaStreamSynchronize(st));
   return PB2_OK;
 }
@@ -1354,6 +1377,7 @@ extern "C" int pb2_min_lbfgs(pb2_batch *b, int32_t n_iter, double tol, double ma
   if (converged)
     for (size_t s = 0; s < S; ++s) converged[s] = (flags[s] & kLbfgsDone) ? 1 : 0;
   b->forces_valid = true;  // the last evaluation is at the final positions
+  if (int rc2 = forces_not_from_step(b, st)) return rc2;
   CUDA_TRY(ctx, cudaStreamSynchronize(st));
   return PB2_OK;
 }
@@ -1476,6 +1500,51 @@ extern "C" int pb2_get_status(pb2_batch *b, uint32_t *status, int clear, void *s
   CUDA_TRY(ctx, cudaMemcpyAsync(status, b->status, b->n_sys * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
   if (clear) CUDA_TRY(ctx, cudaMemsetAsync(b->status, 0, b->n_sys * sizeof(uint32_t), st));
   CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  return PB2_OK;
+}
+
+extern "C" int pb2_set_safeguards(pb2_batch *b, double vlimit, double max_dx, double force_cap) {
+  if (!b) return PB2_EINVAL;
+  pb2_ctx *ctx = b->ctx;
+  if (!std::isfinite(vlimit) || !std::isfinite(max_dx) || !std::isfinite(force_cap))
+    return fail(ctx, PB2_EINVAL, "safeguard limits must be finite");
+  const double g[3] = {vlimit > 0.0 ? vlimit : 0.0, max_dx > 0.0 ? max_dx : 0.0,
+                       force_cap > 0.0 ? force_cap : 0.0};
+  if (g[0] == b->guard[0] && g[1] == b->guard[1] && g[2] == b->guard[2]) return PB2_OK;
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  CUDA_TRY(ctx, cudaDeviceSynchronize());
+  for (int k = 0; k < 3; ++k) b->guard[k] = g[k];
+  for (auto &kv : b->graphs) cudaGraphExecDestroy(kv.second);  // they captured the old limits
+  b->graphs.clear();
+  return PB2_OK;
+}
+
+extern "C" int pb2_get_safeguards(const pb2_batch *b, double *vlimit, double *max_dx, double *force_cap) {
+  if (!b) return PB2_EINVAL;
+  if (vlimit) *vlimit = b->guard[0];
+  if (max_dx) *max_dx = b->guard[1];
+  if (force_cap) *force_cap = b->guard[2];
+  return PB2_OK;
+}
+
+extern "C" int pb2_get_warn_counts(pb2_batch *b, int32_t *counts, int reset, void *stream) {
+  if (!b || !counts) return PB2_EINVAL;
+  pb2_ctx *ctx = b->ctx;
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t S = (size_t)b->n_sys;
+  std::vector<uint32_t> flags(2 * S);
+  CUDA_TRY(ctx, cudaMemcpyAsync(counts, b->warn_counts, S * kWarnTypes * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(ctx, cudaMemcpyAsync(flags.data(), b->warn_flags, 2 * S * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  if (reset) {
+    CUDA_TRY(ctx, cudaMemsetAsync(b->warn_counts, 0, S * kWarnTypes * sizeof(int32_t), st));
+    CUDA_TRY(ctx, cudaMemsetAsync(b->warn_flags, 0, 2 * S * sizeof(uint32_t), st));
+  }
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  // caps recorded by the last launch and not yet folded into the counts
+  for (size_t h = 0; h < 2; ++h)
+    for (size_t s = 0; s < S; ++s)
+      for (int k = 0; k < kWarnTypes; ++k)
+        if (flags[h * S + s] & (1u << k)) counts[s * kWarnTypes + k] += 1;
   return PB2_OK;
 }
 

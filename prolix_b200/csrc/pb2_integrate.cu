@@ -77,6 +77,138 @@ __global__ void step_kernel(const IntArgs a) {
   }
 }
 
+// Safeguarded step: prolix's batched Langevin step (batched_simulate.py:218-382)
+// without constraints, in its order:
+//   F <- F min(1, cap / sqrt(|F|^2 + 1e-12))     (a step's closing force, :336-340)
+//   p += dt/2 F;  where |p/m| > vlimit: p *= min(1, vlimit / (|p/m| + 1e-30))   (:263-274)
+//   x_old = x;  A;  O;  A                                                         (:277-288)
+//   s = min(1, max_dx / |dx|), |dx| = sqrt(|x - x_old|^2 + 1e-30);
+//   x = x_old + (x - x_old) s;  where |dx| > max_dx: p *= s                        (:290-305)
+// and a per-system count of the steps in which each cap fired (:361-367).  The
+// constraint projection of :307-324 is the identity without constraints.  The
+// force that closes step n opens step n+1 capped as well (the reference stores
+// the capped force in the state); a force that no step produced (after init or
+// a state load) opens the next step as it is.
+__device__ __forceinline__ double norm3(double a, double b, double c, double eps) {
+  return __dsqrt_rn(__dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)), __dmul_rn(c, c)), eps));
+}
+
+// Scale a closing force to at most force_cap; true when it was above.
+__device__ __forceinline__ bool cap_force(double f[3], double cap) {
+  const double fm = norm3(f[0], f[1], f[2], 1e-12);
+  const double sc = fmin(1.0, __ddiv_rn(cap, fm));
+#pragma unroll
+  for (int c = 0; c < 3; ++c) f[c] = __dmul_rn(f[c], sc);
+  return fm > cap;
+}
+
+// The thread of a system's first atom adds the caps recorded by the previous
+// launch (the other parity's flag word) to the system's counts and clears it.
+__device__ __forceinline__ void fold_warns(const IntArgs &a, int s) {
+  uint32_t *w = a.warn_flags + (size_t)(a.parity ^ 1) * a.n_sys + s;
+  const uint32_t fl = *w;
+  if (fl) {
+#pragma unroll
+    for (int k = 0; k < kWarnTypes; ++k)
+      if (fl & (1u << k)) a.warn_counts[(size_t)s * kWarnTypes + k] += 1;
+    *w = 0;
+  }
+}
+
+__global__ void step_guarded_kernel(const IntArgs a) {
+  const bool cap_open = a.finish_prev || *a.guard_end;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_total; i += gridDim.x * blockDim.x) {
+    const int s = a.atom_sys[i];
+    const SysInfo &S = a.sys[s];
+    const int loc = i - S.off;
+    const int rnd = a.user[i] - S.off;
+    const double h = S.half_dt;
+    const double m = a.mass[i];
+    const long long lfx = a.fx[i], lfy = a.fy[i], lfz = a.fz[i];
+    check_fix(a, s, lfx); check_fix(a, s, lfy); check_fix(a, s, lfz);
+    double f[3] = {fix_to_d(lfx), fix_to_d(lfy), fix_to_d(lfz)};
+    a.fx[i] = 0; a.fy[i] = 0; a.fz[i] = 0;
+    uint32_t bits = 0;
+    if (a.force_cap > 0.0 && cap_open && cap_force(f, a.force_cap) && a.finish_prev)
+      bits |= 1u << kWarnForceCap;  // counted once, by the launch that closes the step
+    double p[3] = {a.px[i], a.py[i], a.pz[i]};
+    double x[3] = {a.x[i], a.y[i], a.z[i]};
+    const double xo[3] = {x[0], x[1], x[2]};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      if (a.finish_prev) p[c] = __dadd_rn(p[c], __dmul_rn(h, f[c]));
+      p[c] = __dadd_rn(p[c], __dmul_rn(h, f[c]));
+    }
+    if (a.vlimit > 0.0) {
+      const double vm = norm3(__ddiv_rn(p[0], m), __ddiv_rn(p[1], m), __ddiv_rn(p[2], m), 1e-30);
+      if (vm > a.vlimit) {
+        const double sc = fmin(1.0, __ddiv_rn(a.vlimit, __dadd_rn(vm, 1e-30)));
+#pragma unroll
+        for (int c = 0; c < 3; ++c) p[c] = __dmul_rn(p[c], sc);
+        bits |= 1u << kWarnVlimit;
+      }
+    }
+    const uint32_t *kin = a.keys + ((size_t)a.parity * a.n_sys + s) * 2;
+    uint32_t knew[2], sub[2];
+    split_key(kin[0], kin[1], a.partitionable != 0, knew, sub);
+    const uint32_t count = 3u * (uint32_t)S.n;
+    const double c1 = S.c1, sg = a.sigma[i];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      x[c] = __dadd_rn(x[c], __dmul_rn(h, __ddiv_rn(p[c], m)));
+      const float xi = normal_from_bits(random_bits32(sub, 3u * (uint32_t)rnd + c, count, a.partitionable != 0));
+      p[c] = __dadd_rn(__dmul_rn(c1, p[c]), __dmul_rn(sg, (double)xi));
+      x[c] = __dadd_rn(x[c], __dmul_rn(h, __ddiv_rn(p[c], m)));
+    }
+    if (a.max_dx > 0.0) {
+      const double d[3] = {__dsub_rn(x[0], xo[0]), __dsub_rn(x[1], xo[1]), __dsub_rn(x[2], xo[2])};
+      const double dm = norm3(d[0], d[1], d[2], 1e-30);
+      const double sc = fmin(1.0, __ddiv_rn(a.max_dx, dm));
+#pragma unroll
+      for (int c = 0; c < 3; ++c) x[c] = __dadd_rn(xo[c], __dmul_rn(d[c], sc));
+      if (dm > a.max_dx) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) p[c] = __dmul_rn(p[c], sc);
+        bits |= 1u << kWarnDxCap;
+      }
+    }
+    a.px[i] = p[0]; a.py[i] = p[1]; a.pz[i] = p[2];
+    a.x[i] = x[0]; a.y[i] = x[1]; a.z[i] = x[2];
+    write_posq(a, i, S, x[0], x[1], x[2]);
+    if (!(isfinite(x[0]) && isfinite(x[1]) && isfinite(x[2]) && isfinite(p[0]) &&
+          isfinite(p[1]) && isfinite(p[2])))
+      atomicOr(&a.status[s], (uint32_t)PB2_STATUS_NONFINITE);
+    if (bits) atomicOr(&a.warn_flags[(size_t)a.parity * a.n_sys + s], bits);
+    if (loc == 0) {
+      uint32_t *kout = a.keys + ((size_t)(a.parity ^ 1) * a.n_sys + s) * 2;
+      kout[0] = knew[0];
+      kout[1] = knew[1];
+      a.steps[s] += 1;
+      fold_warns(a, s);
+    }
+  }
+}
+
+__global__ void finish_guarded_kernel(const IntArgs a) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_total; i += gridDim.x * blockDim.x) {
+    const int s = a.atom_sys[i];
+    const double h = a.sys[s].half_dt;
+    const long long lfx = a.fx[i], lfy = a.fy[i], lfz = a.fz[i];
+    check_fix(a, s, lfx); check_fix(a, s, lfy); check_fix(a, s, lfz);
+    double f[3] = {fix_to_d(lfx), fix_to_d(lfy), fix_to_d(lfz)};
+    if (a.force_cap > 0.0 && cap_force(f, a.force_cap))
+      atomicOr(&a.warn_flags[(size_t)a.parity * a.n_sys + s], 1u << kWarnForceCap);
+    const double px = __dadd_rn(a.px[i], __dmul_rn(h, f[0]));
+    const double py = __dadd_rn(a.py[i], __dmul_rn(h, f[1]));
+    const double pz = __dadd_rn(a.pz[i], __dmul_rn(h, f[2]));
+    a.px[i] = px; a.py[i] = py; a.pz[i] = pz;
+    if (!(isfinite(px) && isfinite(py) && isfinite(pz)))
+      atomicOr(&a.status[s], (uint32_t)PB2_STATUS_NONFINITE);
+    if (i == a.sys[s].off) fold_warns(a, s);
+    if (i == 0) *a.guard_end = 1;
+  }
+}
+
 __global__ void finish_kernel(const IntArgs a) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_total; i += gridDim.x * blockDim.x) {
     const int s = a.atom_sys[i];
@@ -133,12 +265,20 @@ static int grid_for(int n) {
   return g > 0 ? g : 1;
 }
 
+static bool guarded(const IntArgs &a) { return a.vlimit > 0.0 || a.max_dx > 0.0 || a.force_cap > 0.0; }
+
 cudaError_t launch_step(const IntArgs &a, cudaStream_t st) {
-  step_kernel<<<grid_for(a.n_total), 256, 0, st>>>(a);
+  if (guarded(a))
+    step_guarded_kernel<<<grid_for(a.n_total), 256, 0, st>>>(a);
+  else
+    step_kernel<<<grid_for(a.n_total), 256, 0, st>>>(a);
   return cudaGetLastError();
 }
 cudaError_t launch_finish(const IntArgs &a, cudaStream_t st) {
-  finish_kernel<<<grid_for(a.n_total), 256, 0, st>>>(a);
+  if (guarded(a))
+    finish_guarded_kernel<<<grid_for(a.n_total), 256, 0, st>>>(a);
+  else
+    finish_kernel<<<grid_for(a.n_total), 256, 0, st>>>(a);
   return cudaGetLastError();
 }
 cudaError_t launch_init(const IntArgs &a, cudaStream_t st) {

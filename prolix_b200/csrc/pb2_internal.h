@@ -91,6 +91,12 @@ struct pb2_batch {
   long long *born_acc = nullptr, *dedb_acc = nullptr, *energy = nullptr;
   uint32_t *keys = nullptr, *status = nullptr;
   long long *steps = nullptr;
+  // safeguards of the batched Langevin step (vlimit, max_dx, force_cap; <= 0
+  // off), the closing-force flag and the per-system cap counters
+  double guard[3] = {0.0, 0.0, 0.0};
+  int32_t *guard_end = nullptr;
+  uint32_t *warn_flags = nullptr;
+  int32_t *warn_counts = nullptr;
   TileItem *items = nullptr;   // (i-block, j-range) items of the FP64 energy kernels
   int n_items = 0;
   TileItem *items2 = nullptr;  // pair kernels: items over pairs of i-blocks

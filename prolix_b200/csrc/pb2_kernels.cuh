@@ -117,7 +117,17 @@ struct IntArgs {
   int32_t parity;
   int32_t finish_prev;
   int32_t partitionable;
+  // Safeguards of prolix's batched Langevin step (batched_simulate.py:263-356);
+  // each <= 0 is off, all off is the plain BAOAB step.
+  double vlimit;     // |p/m| limit after the opening half kick
+  double max_dx;     // per-step displacement limit (A)
+  double force_cap;  // |F| limit of a step's closing force
+  int32_t *guard_end;     // 1: the force accumulators hold a step's closing force
+  uint32_t *warn_flags;   // (2, n_sys) caps that fired, by key parity; kWarnBit*
+  int32_t *warn_counts;   // (n_sys, 4) in prolix's warn order (typing.py:559-563)
 };
+// warn_counts columns (prolix typing.py:559-563) and their warn_flags bits
+enum { kWarnVlimit = 0, kWarnForceCap = 1, kWarnConstr = 2, kWarnDxCap = 3, kWarnTypes = 4 };
 // Minimiser (pb2_minimize.cu).  Stage parameters live in device memory
 // (par[kMin*]) so that captured graphs serve every stage.
 enum { kMinK = 0, kMinKind, kMinSdDt, kMinMaxDx, kMinDtStart, kMinDtMax, kMinMaxDisp, kMinForceCap, kMinNPar };

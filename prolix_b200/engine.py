@@ -17,6 +17,9 @@ from . import _lib, topology
 
 AKMA_TIME_FS = 48.88821291839  # prolix simulate.py:56
 KB_KCAL = 0.0019872041          # prolix simulate.py:57
+# the limits of prolix's batched Langevin step (batched_simulate.py:269, 290, 338)
+BATCHED_SAFEGUARDS = {"vlimit": 20.0, "max_dx": 0.5, "force_cap": 1e4}
+WARN_VLIMIT, WARN_FORCE_CAP, WARN_CONSTR_VIOL, WARN_DX_CAP = 0, 1, 2, 3  # typing.py:559-562
 K_COULOMB = 332.0637            # prolix physics/system.py:135
 
 
@@ -392,6 +395,27 @@ class Batch:
     s = np.zeros(self.n_systems, dtype=np.uint32)
     self._check(self.lib.pb2_get_status(self.handle, s.ctypes.data, 1 if clear else 0, stream))
     return s
+
+  def set_safeguards(self, vlimit=0.0, max_dx=0.0, force_cap=0.0):
+    """Safeguards of prolix's batched Langevin step (batched_simulate.py:263-356):
+    speed limit on |p/m| after the opening half kick, per-step displacement
+    limit (A) and closing-force limit (kcal/mol/A); 0 turns each off.
+    ``set_safeguards(**BATCHED_SAFEGUARDS)`` gives the reference's values."""
+    self._check(self.lib.pb2_set_safeguards(self.handle, float(vlimit), float(max_dx),
+                                            float(force_cap)))
+
+  def safeguards(self) -> dict:
+    v = [ctypes.c_double(0.0) for _ in range(3)]
+    self._check(self.lib.pb2_get_safeguards(self.handle, *[ctypes.byref(x) for x in v]))
+    return dict(zip(("vlimit", "max_dx", "force_cap"), (x.value for x in v)))
+
+  def warn_counts(self, reset=False, stream=None):
+    """(n_systems, 4) int32: steps in which each safeguard fired, columns in
+    prolix's order (WARN_VLIMIT, WARN_FORCE_CAP, WARN_CONSTR_VIOL,
+    WARN_DX_CAP; typing.py:559-563).  Column 1 is the reference's cap_count."""
+    c = np.zeros((self.n_systems, 4), dtype=np.int32)
+    self._check(self.lib.pb2_get_warn_counts(self.handle, c.ctypes.data, 1 if reset else 0, stream))
+    return c
 
   def set_tile_segment(self, segment: int):
     self._check(self.lib.pb2_set_tile_segment(self.handle, int(segment)))
