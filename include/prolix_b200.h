@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define PB2_ABI_VERSION 1
+#define PB2_ABI_VERSION 2
 
 /* status codes */
 #define PB2_OK 0
@@ -57,8 +57,9 @@ extern "C" {
 #define PB2_TERM_COULOMB 5
 #define PB2_TERM_GB 6
 #define PB2_TERM_NONPOLAR 7
-#define PB2_TERM_TOTAL 8
-#define PB2_NTERMS 9
+#define PB2_TERM_EXCEPTION 8 /* explicit 1-4 exception pairs (prolix bonded.py:186-230) */
+#define PB2_TERM_TOTAL 9
+#define PB2_NTERMS 10
 
 /* term-enable bits (pb2_run_params.terms) */
 #define PB2_USE_BONDED 0x1u    /* bonds, angles, torsions */
@@ -120,6 +121,17 @@ typedef struct pb2_system_desc {
   int32_t use_origin;         /* 1: take origin below; 0: the rounded centroid of positions */
   double origin[3];           /* A; float32 pair coordinates are taken relative to it, so a
                                  system moved between batches keeps bit-identical forces */
+
+  /* Explicit 1-4 exception pairs (prolix ExclusionSpec.exception_*,
+   * physics/neighbor_list.py:44-50; energy bonded.py:186-230): per pair,
+   * d = sqrt(r^2 + 1e-12), E = 4 eps ((sigma/d)^12 - (sigma/d)^6) + k_coulomb qq / d,
+   * parameters already scaled.  The LJ part follows PB2_USE_LJ, the Coulomb
+   * part PB2_USE_COULOMB.  As in ExclusionSpec.from_protein, these pairs
+   * should also be listed as excluded (kind 0) so that the main LJ/Coulomb
+   * terms skip them; GB keeps every pair. */
+  int32_t n_exceptions;
+  const int32_t *exception_pairs;  /* (n_exceptions, 2) */
+  const double *exception_params;  /* (n_exceptions, 3) = (charge product, sigma, epsilon) */
 } pb2_system_desc;
 
 /* Batch-wide settings. */

@@ -234,6 +234,31 @@ def cmap(pos, torsion_rows, map_idx, grids):
   return float(e.sum()), f
 
 
+def exception_pairs(pos, pairs, sigmas, epsilons, chargeprods, k_coul=332.0637):
+  """Explicit 1-4 exception pairs (prolix bonded.py:186-230): per pair, with
+  parameters already scaled, d = sqrt(|r_i - r_j|^2 + 1e-12) and
+  E = 4 eps ((sigma/d)^12 - (sigma/d)^6) + k_coul qq / d.  Returns
+  (energy, forces)."""
+  pos = np.asarray(pos, np.float64)
+  f = np.zeros_like(pos)
+  pairs = np.asarray(pairs, np.int64).reshape(-1, 2)
+  if pairs.shape[0] == 0:
+    return 0.0, f
+  sig = np.asarray(sigmas, np.float64)
+  eps = np.asarray(epsilons, np.float64)
+  qq = np.asarray(chargeprods, np.float64)
+  dr = pos[pairs[:, 0]] - pos[pairs[:, 1]]
+  d = np.sqrt(np.sum(dr * dr, axis=1) + 1e-12)
+  s6 = (sig / d) ** 6
+  e_lj = 4.0 * eps * (s6 * s6 - s6)
+  e_c = k_coul * qq / d
+  dedd = (4.0 * eps * (-12.0 * s6 * s6 + 6.0 * s6) - e_c) / d
+  g = (dedd / d)[:, None] * dr  # dE/dr_i
+  np.add.at(f, pairs[:, 0], -g)
+  np.add.at(f, pairs[:, 1], g)
+  return float(np.sum(e_lj + e_c)), f
+
+
 def bonded_all(system, pos):
   """Energies (dict: bond, angle, dihedral, cmap) and the summed force."""
   pos = np.asarray(pos, np.float64)

@@ -168,7 +168,15 @@ def nonbonded(system, pos, cutoff=0.0, eps_in=1.0, eps_out=78.5, k_gb=K_COULOMB,
   eps = np.asarray(system["epsilons"], np.float64)
   radii = np.asarray(system["radii"], np.float64)
   sr = np.asarray(system["scaled_radii"], np.float64)
-  pairs, s_v, s_e = topology.pair_scales(system.get("bonds", np.zeros((0, 2))), n, lj14, coul14)
+  if "excl_pairs" in system:
+    # an explicit table (ExclusionSpec idx_12_13 -> kind 0, idx_14 -> kind 1;
+    # neighbor_list.py:33-50), e.g. with 1-4 pairs moved to exception terms
+    pairs = np.asarray(system["excl_pairs"], np.int64).reshape(-1, 2)
+    kind = np.asarray(system["excl_kind"], np.int64).reshape(-1)
+    s_v = np.where(kind == 1, lj14, 0.0)
+    s_e = np.where(kind == 1, coul14, 0.0)
+  else:
+    pairs, s_v, s_e = topology.pair_scales(system.get("bonds", np.zeros((0, 2))), n, lj14, coul14)
   gbc = cutoff if gb_cutoff is None else gb_cutoff
   nl = gbc > 0
   bc = born_cutoff if born_cutoff is not None and born_cutoff > 0 else gbc

@@ -21,8 +21,10 @@ ERRORS = {
     -7: "no usable sm_100 device",
 }
 
-TERM_NAMES = ("bond", "angle", "dihedral", "cmap", "lj", "coulomb", "gb", "nonpolar", "total")
-NTERMS = 9
+TERM_NAMES = ("bond", "angle", "dihedral", "cmap", "lj", "coulomb", "gb", "nonpolar", "exception",
+              "total")
+NTERMS = 10
+ABI_VERSION = 2  # PB2_ABI_VERSION of the structures mirrored below
 USE_BONDED, USE_CMAP, USE_LJ, USE_COULOMB, USE_GB = 0x1, 0x2, 0x4, 0x8, 0x10
 USE_ALL = 0x1F
 STATUS_NONFINITE, STATUS_NLOVERFLOW, STATUS_FORCE_RANGE = 0x1, 0x2, 0x4
@@ -49,6 +51,7 @@ class SystemDesc(ctypes.Structure):
       ("key", ctypes.c_uint32 * 2),
       ("dt", ctypes.c_double), ("kT", ctypes.c_double), ("gamma", ctypes.c_double),
       ("use_origin", ctypes.c_int32), ("origin", ctypes.c_double * 3),
+      ("n_exceptions", ctypes.c_int32), ("exception_pairs", _c_ip), ("exception_params", _c_dp),
   ]
 
 
@@ -143,6 +146,9 @@ def load(path=None) -> ctypes.CDLL:
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
+      if lib.pb2_abi_version() != ABI_VERSION:
+        raise RuntimeError(f"{p}: ABI version {lib.pb2_abi_version()}, this package needs "
+                           f"{ABI_VERSION}; rebuild the library")
       _LIB = lib
   return _LIB
 

@@ -252,7 +252,8 @@ static int validate(pb2_ctx *ctx, const pb2_system_desc &d, int s) {
       }
     return true;
   };
-  if (d.n_bonds < 0 || d.n_angles < 0 || d.n_torsions < 0 || d.n_cmap < 0 || d.n_excl < 0)
+  if (d.n_bonds < 0 || d.n_angles < 0 || d.n_torsions < 0 || d.n_cmap < 0 || d.n_excl < 0 ||
+      d.n_exceptions < 0)
     return bad("negative term count");
   if (d.n_bonds && (!d.bonds || !d.bond_params)) return bad("bond arrays missing");
   if (d.n_angles && (!d.angles || !d.angle_params)) return bad("angle arrays missing");
@@ -262,11 +263,13 @@ static int validate(pb2_ctx *ctx, const pb2_system_desc &d, int s) {
                    d.cmap_grid <= 0))
     return bad("cmap arrays missing");
   if (d.n_excl && (!d.excl_pairs || !d.excl_kind)) return bad("exclusion arrays missing");
+  if (d.n_exceptions && (!d.exception_pairs || !d.exception_params)) return bad("exception arrays missing");
   if (!check_idx(d.bonds, 2LL * d.n_bonds, "bond") ||
       !check_idx(d.angles, 3LL * d.n_angles, "angle") ||
       !check_idx(d.torsions, 4LL * d.n_torsions, "torsion") ||
       !check_idx(d.cmap_rows, 5LL * d.n_cmap, "cmap") ||
-      !check_idx(d.excl_pairs, 2LL * d.n_excl, "exclusion"))
+      !check_idx(d.excl_pairs, 2LL * d.n_excl, "exclusion") ||
+      !check_idx(d.exception_pairs, 2LL * d.n_exceptions, "exception"))
     return fail(ctx, PB2_EINVAL, buf);
   for (int k = 0; k < d.n_cmap; ++k)
     if (d.cmap_map[k] < 0 || d.cmap_map[k] >= d.n_cmap_maps) return bad("cmap map index out of range");
@@ -526,6 +529,8 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   std::vector<double> ccoef;
   std::vector<int32_t> cgrid;
   std::vector<int64_t> cmoff;
+  std::vector<int2> eidx;
+  std::vector<double4> epar;
   for (int s = 0; s < n_systems; ++s) {
     const pb2_system_desc &d = systems[s];
     const int o = b->off[s];
@@ -557,6 +562,11 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
       for (int c = 0; c < 5; ++c) cidx.push_back(at(d.cmap_rows[5 * k + c]));
       cidx.push_back(map_base + d.cmap_map[k]);
     }
+    for (int k = 0; k < d.n_exceptions; ++k) {
+      const double *p = d.exception_params + 3 * (size_t)k;
+      eidx.push_back(make_int2(at(d.exception_pairs[2 * k]), at(d.exception_pairs[2 * k + 1])));
+      epar.push_back(make_double4(d.k_coulomb * p[0], p[1], p[2], 0.0));
+    }
   }
 
   // terms in order of their (central) atom: with atoms in spatial order, the
@@ -578,6 +588,7 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   by_atom(bidx, bpar, [](const int2 &t) { return std::min(t.x, t.y); });
   by_atom(aidx, apar, [](const int4 &t) { return t.y; });
   by_atom(tidx, tpar, [](const int4 &t) { return std::min(t.y, t.z); });
+  by_atom(eidx, epar, [](const int2 &t) { return std::min(t.x, t.y); });
 
   // --- device allocation
   Dev &D = b->dev;
@@ -624,6 +635,9 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   B.n_angle = (int)aidx.size();
   B.n_tors = (int)tidx.size();
   B.n_cmap = (int)(cidx.size() / 6);
+  B.n_exc = (int)eidx.size();
+  int2 *d_eidx = D.alloc<int2>(eidx.size());
+  double4 *d_epar = D.alloc<double4>(epar.size());
   int2 *d_bidx = D.alloc<int2>(bidx.size());
   double2 *d_bpar = D.alloc<double2>(bpar.size());
   int4 *d_aidx = D.alloc<int4>(aidx.size());
@@ -655,7 +669,8 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
       (rc = upload(ctx, d_aidx, aidx)) || (rc = upload(ctx, d_apar, apar)) ||
       (rc = upload(ctx, d_tidx, tidx)) || (rc = upload(ctx, d_tpar, tpar)) ||
       (rc = upload(ctx, d_cidx, cidx)) || (rc = upload(ctx, d_ccoef, ccoef)) ||
-      (rc = upload(ctx, d_cgrid, cgrid)) || (rc = upload(ctx, d_cmoff, cmoff)))
+      (rc = upload(ctx, d_cgrid, cgrid)) || (rc = upload(ctx, d_cmoff, cmoff)) ||
+      (rc = upload(ctx, d_eidx, eidx)) || (rc = upload(ctx, d_epar, epar)))
     return rc;
   CUDA_TRY(ctx, cudaMemset(b->px, 0, N * sizeof(double)));
   CUDA_TRY(ctx, cudaMemset(b->py, 0, N * sizeof(double)));
@@ -681,8 +696,10 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   B.angle_idx = d_aidx; B.angle_par = d_apar;
   B.tors_idx = d_tidx; B.tors_par = d_tpar;
   B.cmap_idx = d_cidx; B.cmap_coeff = d_ccoef; B.cmap_grid = d_cgrid; B.cmap_map_off = d_cmoff;
+  B.exc_idx = d_eidx; B.exc_par = d_epar;
   if (!(params->terms & PB2_USE_BONDED)) B.n_bond = B.n_angle = B.n_tors = 0;
   if (!(params->terms & PB2_USE_CMAP)) B.n_cmap = 0;
+  if (!(params->terms & (PB2_USE_LJ | PB2_USE_COULOMB))) B.n_exc = 0;
 
   b->grid_bonded = 8 * ctx->sm_count;
   if ((rc = setup_items2(b.get(), b->params.tile_segment))) return rc;

@@ -6,7 +6,8 @@
 // +-0.999999 clip; dihedral angle b0 = r_i - r_j, b1 = r_k - r_j,
 // b2 = r_l - r_k, phi = atan2(y, x); torsion sum k (1 + cos(n phi - delta)))
 // and physics/cmap.py:316-376 (bicubic patch evaluation at angles mapped to
-// [0, 2 pi); phi from row atoms 0-3, psi from 1-4, system.py:99-102).
+// [0, 2 pi); phi from row atoms 0-3, psi from 1-4, system.py:99-102), and the
+// explicit 1-4 exception pairs of bonded.py:186-230.
 //
 // These terms are O(N) and stiff: a bond force k (r - r0) needs r - r0 to
 // ~1e-7 A, which float32 coordinates cannot give, so the arithmetic is
@@ -63,7 +64,7 @@ __device__ void dihedral(const BondedArgs &a, int i, int j, int k, int l, double
 }
 
 __global__ void bonded_kernel(const BondedArgs a) {
-  const int total = a.n_bond + a.n_angle + a.n_tors + a.n_cmap;
+  const int total = a.n_bond + a.n_angle + a.n_tors + a.n_cmap + a.n_exc;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
     int u = t;
     if (u < a.n_bond) {
@@ -118,7 +119,7 @@ __global__ void bonded_kernel(const BondedArgs a) {
       continue;
     }
     u -= a.n_tors;
-    {
+    if (u < a.n_cmap) {
       const int32_t *row = a.cmap_idx + (size_t)u * 6;
       const int m = row[5];
       const int G = a.cmap_grid[m];
@@ -160,12 +161,36 @@ __global__ void bonded_kernel(const BondedArgs a) {
         add_force(a, row[k + 1], scale(gpsi[k], -eb));
       }
       add_energy(a, row[0], PB2_TERM_CMAP, e);
+      continue;
+    }
+    u -= a.n_cmap;
+    {  // explicit 1-4 exception pair (bonded.py:211-228)
+      const int2 id = a.exc_idx[u];
+      const double4 p = a.exc_par[u];
+      const D3 d = sub(ld3(a, id.x), ld3(a, id.y));
+      const double r = sqrt(dot(d, d) + 1e-12);
+      const double inv = 1.0 / r;
+      double e = 0.0, dedr = 0.0;
+      if (a.terms & PB2_USE_LJ) {
+        const double sr = p.y * inv, s2 = sr * sr, s6 = s2 * s2 * s2;
+        e += 4.0 * p.z * (s6 * s6 - s6);
+        dedr += 4.0 * p.z * (6.0 * s6 - 12.0 * s6 * s6) * inv;
+      }
+      if (a.terms & PB2_USE_COULOMB) {
+        const double ec = p.x * inv;
+        e += ec;
+        dedr -= ec * inv;
+      }
+      const double g = dedr * inv;
+      add_force(a, id.x, scale(d, -g));
+      add_force(a, id.y, scale(d, g));
+      add_energy(a, id.x, PB2_TERM_EXCEPTION, e);
     }
   }
 }
 
 cudaError_t launch_bonded(const BondedArgs &a, int grid_cap, cudaStream_t st) {
-  const int total = a.n_bond + a.n_angle + a.n_tors + a.n_cmap;
+  const int total = a.n_bond + a.n_angle + a.n_tors + a.n_cmap + a.n_exc;
   if (total <= 0) return cudaSuccess;
   int grid = (total + 255) / 256;
   if (grid > grid_cap) grid = grid_cap;

@@ -75,6 +75,9 @@ struct BondedArgs {
   const double *cmap_coeff;
   const int32_t *cmap_grid;
   const int64_t *cmap_map_off;
+  int32_t n_exc;
+  const int2 *exc_idx;
+  const double4 *exc_par;  // (k_coulomb * charge product, sigma, epsilon, 0)
 };
 struct NlGrid {        // per-system cell grid of the neighbour-list build
   float x0, y0, z0, inv_cell;

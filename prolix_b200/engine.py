@@ -138,6 +138,18 @@ def prepare_system(system: dict, *, dt=None, kT=None, gamma=None, key=None, eps_
   out["kT"] = float(system.get("kT", kT if kT is not None else 300.0 * KB_KCAL))
   out["gamma"] = float(system.get("gamma", gamma if gamma is not None else akma_gamma(1.0)))
   out["origin"] = None if system.get("origin") is None else tuple(float(v) for v in system["origin"])
+  # explicit 1-4 exception pairs, ExclusionSpec field names (neighbor_list.py:44-50)
+  ep = system.get("exception_pairs")
+  if ep is not None and np.asarray(ep).size:
+    out["exception_pairs"] = _i32(ep, (-1, 2))
+    m = out["exception_pairs"].shape[0]
+    out["exception_params"] = _f64(np.stack([
+        np.asarray(system["exception_chargeprods"], dtype=np.float64).reshape(m),
+        np.asarray(system["exception_sigmas"], dtype=np.float64).reshape(m),
+        np.asarray(system["exception_epsilons"], dtype=np.float64).reshape(m)], axis=1))
+  else:
+    out["exception_pairs"] = np.zeros((0, 2), np.int32)
+    out["exception_params"] = np.zeros((0, 3))
   return out
 
 
@@ -176,6 +188,8 @@ def _desc(p) -> _lib.SystemDesc:
   if p["origin"] is not None:
     d.use_origin = 1
     d.origin[0], d.origin[1], d.origin[2] = p["origin"]
+  d.n_exceptions = p["exception_pairs"].shape[0]
+  d.exception_pairs, d.exception_params = _ip(p["exception_pairs"]), _dp(p["exception_params"])
   return d
 
 
@@ -238,7 +252,7 @@ class Batch:
 
   # ---------------------------------------------------------------- physics
   def energy_forces(self, stream=None):
-    """(energies (n_systems, 9) with columns TERM_NAMES, forces (n_atoms, 3))."""
+    """(energies (n_systems, 10) with columns TERM_NAMES, forces (n_atoms, 3))."""
     e = np.zeros((self.n_systems, _lib.NTERMS))
     f = np.zeros((self.n_atoms, 3))
     self._check(self.lib.pb2_energy_forces(self.handle, e.ctypes.data, f.ctypes.data, stream))

@@ -29,7 +29,8 @@ from ._lib import TERM_NAMES, USE_ALL
 _SYSTEM_KEYS = ("charges", "sigmas", "epsilons", "radii", "scaled_radii", "masses", "bonds",
                 "bond_params", "angles", "angle_params", "dihedrals", "dihedral_params",
                 "proper_dihedrals", "proper_dihedral_params", "cmap_torsions", "cmap_indices",
-                "cmap_energy_grids", "excl_pairs", "excl_kind")
+                "cmap_energy_grids", "excl_pairs", "excl_kind", "exception_pairs",
+                "exception_sigmas", "exception_epsilons", "exception_chargeprods")
 
 
 def system_to_dict(system) -> dict:
@@ -142,6 +143,12 @@ def make_energy_fn(displacement_fn, system, cutoff_distance: float = 9.0,
     pairs, kind, lj14, c14 = _exclusions_from_spec(exclusion_spec, n)
     sysd["excl_pairs"], sysd["excl_kind"] = pairs, kind
     sysd["lj14_scale"], sysd["coul14_scale"] = lj14, c14
+  if exclusion_spec is not None and "exception_pairs" not in sysd:
+    # explicit 1-4 overrides (system.py:149-159): their own energy term
+    for k in ("exception_pairs", "exception_sigmas", "exception_epsilons", "exception_chargeprods"):
+      v = getattr(exclusion_spec, k, None)
+      if v is not None:
+        sysd[k] = np.asarray(v)
   cutoff = float(kwargs.get("cutoff", cutoff_distance))
   eps_in = float(kwargs.get("solute_dielectric", 1.0))
   eps_out = float(kwargs.get("solvent_dielectric", 78.5))
@@ -166,6 +173,6 @@ def make_energy_fn(displacement_fn, system, cutoff_distance: float = 9.0,
   return {
       "bond": term("bond"), "angle": term("angle"), "dihedral": term("dihedral"),
       "improper": zero, "urey_bradley": zero, "cmap": term("cmap"), "lj": term("lj"),
-      "exception": zero, "electrostatics": electrostatics, "nonpolar": nonpolar,
+      "exception": term("exception"), "electrostatics": electrostatics, "nonpolar": nonpolar,
       "total": fn,
   }

@@ -27,7 +27,7 @@ def test_library_loads_and_exports_every_declared_symbol():
     assert hasattr(lib, name), name
   bound = {name for name, _, _ in _lib.SIGNATURES}
   assert set(declared) <= bound | {"pb2_ctx_create"}
-  assert lib.pb2_abi_version() == 1
+  assert lib.pb2_abi_version() == _lib.ABI_VERSION == 2
 
 
 def _struct_fields(text, name):
