@@ -53,7 +53,11 @@ TERMS = ("bond", "angle", "dihedral", "cmap", "lj", "coulomb", "gb", "nonpolar",
 
 def energy_forces(system, pos=None, cutoff=0.0, gb_cutoff=None, threads=0, eps_in=1.0,
                   eps_out=78.5, k=332.0637):
-  """(energies dict, forces) in FP64; CMAP is not included (0)."""
+  """(energies dict, forces) in FP64; CMAP is not included (0), nor are
+  explicit exclusion tables or exception pairs (the exclusions follow the
+  bonds; ``exception`` is reported as 0)."""
+  if "excl_pairs" in system or np.asarray(system.get("exception_pairs", np.zeros((0, 2)))).size:
+    raise NotImplementedError("the C oracle derives exclusions from the bonds and has no exception pairs")
   pos = _f(system["positions"] if pos is None else pos, (-1, 3))
   n = pos.shape[0]
   pairs, sv, se = topology.pair_scales(system.get("bonds", np.zeros((0, 2))), n)
@@ -88,7 +92,9 @@ def energy_forces(system, pos=None, cutoff=0.0, gb_cutoff=None, threads=0, eps_i
                                  int(threads))
   if rc != 0:
     raise MemoryError("C oracle allocation failed")
-  return dict(zip(TERMS, e.tolist())), f
+  out = dict(zip(TERMS, e.tolist()))
+  out["exception"] = 0.0
+  return out, f
 
 
 def threads() -> int:
