@@ -2,7 +2,9 @@
 hold for this path, and against published known-answer vectors of the
 third-party algorithms on the path.  CPU only."""
 
+import json
 import math
+import os
 
 import numpy as np
 import pytest
@@ -11,6 +13,8 @@ from oracle import bonded, energy, gbsa, integrator, prng
 from prolix_b200 import synth
 
 TAU = 1.0 / 1.0 - 1.0 / 78.5
+with open(os.path.join(os.path.dirname(__file__), "golden", "known_answers.json")) as _f:
+  KA = json.load(_f)
 
 
 def gb_only(system, pos, cutoff=0.0):
@@ -24,11 +28,11 @@ def gb_only(system, pos, cutoff=0.0):
 def test_born_ion():
   # prolix tests/physics/test_generalized_born.py:11-52: a single ion of
   # radius 2.0 has Born radius 2.0 - 0.09 and E = -1/2 k tau q^2 / B.
-  s = {"charges": [1.0], "radii": [2.0], "scaled_radii": [2.0]}
+  ka = KA["born_ion"]
+  s = {"charges": [ka["charge"]], "radii": [ka["radius"]], "scaled_radii": [ka["radius"]]}
   e, _, ex = gb_only(s, np.zeros((1, 3)))
-  b = 2.0 - 0.09
-  assert ex["born_radii"][0] == pytest.approx(b, rel=1e-12)
-  assert e == pytest.approx(-0.5 * gbsa.K_COULOMB * TAU / b, rel=1e-5)
+  assert ex["born_radii"][0] == pytest.approx(ka["born_radius"], rel=1e-12)
+  assert e == pytest.approx(ka["gb_energy"], rel=ka["gb_energy_rel"])
 
 
 def test_gb_gradient_matches_finite_difference():
@@ -80,35 +84,30 @@ def test_gb_nve_drift():
 
 def test_bond_and_angle_known_values():
   # prolix tests/physics/test_bonded.py:10-59
-  r = np.array([[0.0, 0.0, 0.0], [1.1, 0.0, 0.0]])
-  e, f = bonded.bonds(r, [[0, 1]], [[1.0, 100.0]])
-  assert e == pytest.approx(0.5)
-  assert f[1, 0] == pytest.approx(-10.0, abs=1e-5)
-  assert f[0, 0] == pytest.approx(10.0, abs=1e-5)
-  r = np.array([[1.0, 0.0, 0.0], [0.0, 0.0, 0.0], [0.0, 1.0, 0.0]])
-  e, _ = bonded.angles(r, [[0, 1, 2]], [[math.pi, 100.0]])
-  assert e == pytest.approx(0.5 * 100.0 * (math.pi / 2) ** 2, rel=1e-4)
+  kb, ka = KA["bond"], KA["angle"]
+  e, f = bonded.bonds(np.array(kb["positions"]), [[0, 1]], [kb["params"]])
+  assert e == pytest.approx(kb["energy"])
+  assert f[0, 0] == pytest.approx(kb["force_x"][0], abs=kb["force_abs"])
+  assert f[1, 0] == pytest.approx(kb["force_x"][1], abs=kb["force_abs"])
+  e, _ = bonded.angles(np.array(ka["positions"]), [[0, 1, 2]], [ka["params"]])
+  assert e == pytest.approx(ka["energy"], rel=ka["energy_rel"])
 
 
 def test_threefry_known_answer_vectors():
   # Random123 known-answer vectors for threefry2x32, 20 rounds
   u = np.uint32
-  cases = [((0, 0), (0, 0), (0x6B200159, 0x99BA4EFE)),
-           ((0xFFFFFFFF, 0xFFFFFFFF), (0xFFFFFFFF, 0xFFFFFFFF), (0x1CB996FC, 0xBB002BE7)),
-           ((0x13198A2E, 0x03707344), (0x243F6A88, 0x85A308D3), (0xC4923A9C, 0x483DF7A0))]
-  for key, ctr, want in cases:
+  for key, ctr, want in KA["threefry2x32_20"]["cases"]:
     got = prng.threefry2x32(u(key[0]), u(key[1]), u(ctr[0]), u(ctr[1]))
-    assert (int(got[0]), int(got[1])) == want
+    assert [int(got[0]), int(got[1])] == want
 
 
 def test_jax_split_documented_values():
   # jax.random.split(jax.random.PRNGKey(0)) as printed in JAX's documentation,
   # for the original and the partitionable (default) key layouts.
   k = prng.prng_key(0)
-  np.testing.assert_array_equal(prng.split(k, partitionable=False),
-                                [[4146024105, 967050713], [2718843009, 1272950319]])
-  np.testing.assert_array_equal(prng.split(k, partitionable=True),
-                                [[1797259609, 2579123966], [928981903, 3453687069]])
+  kv = KA["jax_split_prngkey0"]
+  np.testing.assert_array_equal(prng.split(k, partitionable=False), kv["original"])
+  np.testing.assert_array_equal(prng.split(k, partitionable=True), kv["partitionable"])
 
 
 def test_normal_sampler_statistics():
