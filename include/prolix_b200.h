@@ -210,6 +210,13 @@ int pb2_set_positions(pb2_batch *batch, const double *positions, void *stream);
 int pb2_langevin_init(pb2_batch *batch, void *stream);
 int pb2_langevin_run(pb2_batch *batch, int32_t n_steps, void *stream);
 
+/* Subtract each system's mean momentum, as jax_md's nvt_langevin init_fn
+ * does with center_velocity (prolix applies it over real atoms only,
+ * physics/settle.py:1121-1142); systems of one atom are left alone.  Call
+ * after pb2_langevin_init for jax_md's init; prolix's own BAOAB init
+ * (settle.py:1676-1696) does not center. */
+int pb2_langevin_center_momentum(pb2_batch *batch, void *stream);
+
 /* Read or write the integrator state; any pointer may be NULL.
  * x, p, f: (n_atoms_total, 3); keys: (n_systems, 2); steps: (n_systems). */
 int pb2_get_state(pb2_batch *batch, double *x, double *p, double *f, uint32_t *keys,

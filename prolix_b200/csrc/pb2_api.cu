@@ -1000,6 +1000,16 @@ extern "C" int pb2_langevin_init(pb2_batch *b, void *stream) {
   return PB2_OK;
 }
 
+extern "C" int pb2_langevin_center_momentum(pb2_batch *b, void *stream) {
+  if (!b) return PB2_EINVAL;
+  pb2_ctx *ctx = b->ctx;
+  cudaStream_t st = (cudaStream_t)stream;
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  CUDA_TRY(ctx, launch_center(int_args(b, b->key_parity, 0), st));
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  return PB2_OK;
+}
+
 extern "C" int pb2_langevin_run(pb2_batch *b, int32_t n_steps, void *stream) {
   if (!b || n_steps < 0) return PB2_EINVAL;
   pb2_ctx *ctx = b->ctx;

@@ -252,6 +252,40 @@ __global__ void init_kernel(const IntArgs a) {
   }
 }
 
+// Remove each system's mean momentum (jax_md's center_velocity at init,
+// applied by prolix over real atoms only, physics/settle.py:1121-1142); a
+// one-atom system keeps its momentum.  One block per system; the sums run
+// in a fixed order, so the result is deterministic.
+constexpr int kCenterThreads = 256;
+__global__ void __launch_bounds__(kCenterThreads) center_kernel(const IntArgs a) {
+  const SysInfo &S = a.sys[blockIdx.x];
+  if (S.n <= 1) return;
+  __shared__ double sh[3][kCenterThreads];
+  double sx = 0.0, sy = 0.0, sz = 0.0;
+  for (int l = threadIdx.x; l < S.n; l += kCenterThreads) {
+    const int i = S.off + l;
+    sx += a.px[i];
+    sy += a.py[i];
+    sz += a.pz[i];
+  }
+  sh[0][threadIdx.x] = sx;
+  sh[1][threadIdx.x] = sy;
+  sh[2][threadIdx.x] = sz;
+  __syncthreads();
+  for (int w = kCenterThreads / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+      for (int c = 0; c < 3; ++c) sh[c][threadIdx.x] += sh[c][threadIdx.x + w];
+    __syncthreads();
+  }
+  const double mx = sh[0][0] / S.n, my = sh[1][0] / S.n, mz = sh[2][0] / S.n;
+  for (int l = threadIdx.x; l < S.n; l += kCenterThreads) {
+    const int i = S.off + l;
+    a.px[i] -= mx;
+    a.py[i] -= my;
+    a.pz[i] -= mz;
+  }
+}
+
 // Refresh the float32 pair-kernel positions from the FP64 state.
 __global__ void posq_kernel(const IntArgs a) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_total; i += gridDim.x * blockDim.x) {
@@ -283,6 +317,10 @@ cudaError_t launch_finish(const IntArgs &a, cudaStream_t st) {
 }
 cudaError_t launch_init(const IntArgs &a, cudaStream_t st) {
   init_kernel<<<grid_for(a.n_total), 256, 0, st>>>(a);
+  return cudaGetLastError();
+}
+cudaError_t launch_center(const IntArgs &a, cudaStream_t st) {
+  center_kernel<<<a.n_sys, kCenterThreads, 0, st>>>(a);
   return cudaGetLastError();
 }
 cudaError_t launch_posq(const IntArgs &a, cudaStream_t st) {

@@ -182,6 +182,7 @@ cudaError_t launch_bbox(const SysInfo *sys, const int32_t *blk_sys, const float4
 cudaError_t launch_bonded(const BondedArgs &a, int grid_cap, cudaStream_t st);
 cudaError_t launch_step(const IntArgs &a, cudaStream_t st);
 cudaError_t launch_finish(const IntArgs &a, cudaStream_t st);
+cudaError_t launch_center(const IntArgs &a, cudaStream_t st);
 cudaError_t launch_init(const IntArgs &a, cudaStream_t st);
 cudaError_t launch_posq(const IntArgs &a, cudaStream_t st);
 // Host transfers: `user` maps each batch atom to its row in the caller's

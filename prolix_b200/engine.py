@@ -410,6 +410,11 @@ class Batch:
     self._check(self.lib.pb2_get_status(self.handle, s.ctypes.data, 1 if clear else 0, stream))
     return s
 
+  def center_momentum(self, stream=None):
+    """Subtract each system's mean momentum (jax_md center_velocity; a
+    one-atom system is left alone)."""
+    self._check(self.lib.pb2_langevin_center_momentum(self.handle, stream))
+
   def set_safeguards(self, vlimit=0.0, max_dx=0.0, force_cap=0.0):
     """Safeguards of prolix's batched Langevin step (batched_simulate.py:263-356):
     speed limit on |p/m| after the opening half kick, per-step displacement

@@ -3,8 +3,9 @@
 * ``nvt_langevin(energy_fn, shift_fn, dt, kT, gamma, mass)`` returns
   ``(init_fn, apply_fn)`` with jax_md's protocol, the integrator that prolix
   uses (physics/simulate.py:245, physics/settle.py:1114-1117, 1637-1746):
-  ``init_fn(key, R, mass=...)`` draws p = sqrt(m kT) normal(split(key)[1]) and
-  evaluates the force; ``apply_fn(state)`` advances one BAOAB step.  The state
+  ``init_fn(key, R, mass=...)`` draws p = sqrt(m kT) normal(split(key)[1]),
+  removes its mean as jax_md does (``center_velocity=True``) and evaluates
+  the force; ``apply_fn(state)`` advances one BAOAB step.  The state
   stays on the GPU; its arrays are read back when accessed.
 * ``run_minimization`` restates prolix's steepest descent with a 4-point
   backtracking line search (physics/simulate.py:141-196) on GPU energies and
@@ -111,11 +112,13 @@ def _as_energy_fn(energy_or_force_fn) -> EnergyFn:
 
 
 def nvt_langevin(energy_or_force_fn, shift_fn, dt: float, kT: float, gamma: float = 0.1,
-                 mass=1.0, **kwargs):
+                 mass=1.0, center_velocity: bool = True, **kwargs):
   """BAOAB Langevin (jax_md ``nvt_langevin`` protocol) on the GPU.
 
   dt and gamma are in the caller's time unit with masses in the matching
-  unit (AKMA: dt in tau, gamma in 1/tau, masses in amu).
+  unit (AKMA: dt in tau, gamma in 1/tau, masses in amu).  As in jax_md,
+  ``center_velocity`` removes the mean initial momentum of a system of more
+  than one atom; the draw itself is settle.py:1676-1696's.
   """
   efn = _as_energy_fn(energy_or_force_fn)
 
@@ -130,6 +133,8 @@ def nvt_langevin(energy_or_force_fn, shift_fn, dt: float, kT: float, gamma: floa
                          eps_in=efn.batch.prepared[0]["scal"]["eps_in"],
                          eps_out=efn.batch.prepared[0]["scal"]["eps_out"])
     batch.langevin_init()
+    if center_velocity:
+      batch.center_momentum()
     return NVTLangevinState(batch, m)
 
   def apply_fn(state: NVTLangevinState, n_steps: int = 1, **kw):

@@ -86,7 +86,7 @@ def test_nvt_langevin_protocol_matches_oracle():
   for _ in range(3):
     st = apply_fn(st)
   force = lambda r: oracle_terms(s, r, 0.0, 0.0)[1]
-  o = ointeg.init(force, key, s["positions"], s["masses"], kT)
+  o = ointeg.init(force, key, s["positions"], s["masses"], kT, center=True)
   o = ointeg.run(o, force, 3, dt, kT, gamma)
   assert st.step == 3
   assert np.max(np.abs(st.position - o.position)) < 1e-7
@@ -135,3 +135,24 @@ def test_device_pointer_entry_point_and_graph_capture():
     np.testing.assert_array_equal(f_dev.cpu().numpy(), f_ref)
     np.testing.assert_array_equal(e_dev.cpu().numpy(), e_ref)
     del g
+
+
+def test_center_momentum_matches_the_oracle_init():
+  # jax_md's center_velocity on each system of a ragged batch; a one-atom
+  # system keeps its momentum
+  keys = [prng.prng_key(k) for k in (3, 4, 5)]
+  systems = [dict(synth.make_chain(n, n, compact=True), key=k) for n, k in zip((130, 1, 77), keys)]
+  kT = 300 * engine.KB_KCAL
+  with engine.Batch(systems, terms=0) as b:
+    b.langevin_init()
+    b.center_momentum()
+    p = b.get_state(fields=("momentum",))["momentum"]
+  zero = lambda r: np.zeros_like(r)
+  for k, s in enumerate(systems):
+    lo, hi = b.offsets[k], b.offsets[k + 1]
+    o = ointeg.init(zero, keys[k], s["positions"], s["masses"], kT, center=True)
+    np.testing.assert_allclose(p[lo:hi], o.momentum, rtol=0, atol=1e-13 * np.abs(o.momentum).max())
+    if hi - lo > 1:
+      assert np.abs(p[lo:hi].sum(axis=0)).max() < 1e-11 * np.abs(p[lo:hi]).max()
+    else:
+      np.testing.assert_array_equal(p[lo:hi], o.momentum)
