@@ -87,7 +87,34 @@ class EnergyFn:
   def n_atoms(self) -> int:
     return self._batch.n_atoms
 
+  def _device_positions(self, r):
+    """r as a contiguous float64 (n, 3) CUDA torch tensor when it is a CUDA
+    array (a torch tensor or any DLPack producer), else None."""
+    dev = getattr(r, "__dlpack_device__", None)
+    if dev is None or dev()[0] != 2:  # 2: kDLCUDA
+      return None
+    import torch
+    t = r if isinstance(r, torch.Tensor) else torch.from_dlpack(r)
+    if t.device.index != self._batch.ctx.device:
+      raise ValueError(f"positions on cuda:{t.device.index}, the energy function on "
+                       f"cuda:{self._batch.ctx.device}")
+    return t.detach().to(torch.float64).reshape(self.n_atoms, 3).contiguous()
+
+  def _eval_device(self, t):
+    """(energies (NTERMS,), forces (n, 3)) as CUDA tensors, computed on the
+    caller's current stream without a host copy or synchronisation."""
+    import torch
+    e = torch.empty(len(TERM_NAMES), dtype=torch.float64, device=t.device)
+    f = torch.empty_like(t)
+    stream = torch.cuda.current_stream(t.device).cuda_stream
+    self._batch.energy_forces_device(t.data_ptr(), e.data_ptr(), f.data_ptr(), stream)
+    self._last = None  # the batch now holds these positions
+    return e, f
+
   def _eval(self, r):
+    t = self._device_positions(r)
+    if t is not None:
+      return self._eval_device(t)
     r = np.ascontiguousarray(np.asarray(r, dtype=np.float64).reshape(self.n_atoms, 3))
     if self._last is not None and np.array_equal(self._last[0], r):
       return self._last[1], self._last[2]
@@ -101,13 +128,19 @@ class EnergyFn:
     return {name: float(e[i]) for i, name in enumerate(TERM_NAMES)}
 
   def __call__(self, r, neighbor=None, **kwargs):
-    return float(self._eval(r)[0][-1])
+    """Total energy: a float, or a 0-d CUDA tensor when r is a CUDA array."""
+    e = self._eval(r)[0][-1]
+    return e if hasattr(e, "device") else float(e)
 
   def forces(self, r, neighbor=None, **kwargs):
-    return self._eval(r)[1].copy()
+    """-dE/dr (n, 3): NumPy, or a CUDA tensor when r is a CUDA array."""
+    f = self._eval(r)[1]
+    return f if hasattr(f, "device") else f.copy()
 
   def energy_and_forces(self, r, neighbor=None, **kwargs):
     e, f = self._eval(r)
+    if hasattr(f, "device"):
+      return e[-1], f
     return float(e[-1]), f.copy()
 
   def close(self):
@@ -116,6 +149,9 @@ class EnergyFn:
     self._last = None
 
   def born_radii(self, r):
+    t = self._device_positions(r)
+    if t is not None:
+      r = t.cpu().numpy()
     r = np.asarray(r, dtype=np.float64).reshape(self.n_atoms, 3)
     self._batch.set_positions(r)
     self._last = None

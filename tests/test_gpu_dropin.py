@@ -156,3 +156,22 @@ def test_center_momentum_matches_the_oracle_init():
       assert np.abs(p[lo:hi].sum(axis=0)).max() < 1e-11 * np.abs(p[lo:hi]).max()
     else:
       np.testing.assert_array_equal(p[lo:hi], o.momentum)
+
+
+def test_energy_fn_takes_cuda_arrays():
+  # a CUDA tensor (or any DLPack producer on the device) is evaluated on the
+  # device with no host copy; results equal the NumPy path bit for bit
+  import torch
+  s = synth.make_chain(180, 12, compact=True)
+  fn = make_energy_fn(None, s, implicit_solvent=True, cutoff=0.0)
+  e_host, f_host = fn.energy_and_forces(s["positions"])
+  t = torch.tensor(s["positions"], device="cuda")
+  e_dev, f_dev = fn(t), fn.forces(t)
+  assert e_dev.device.type == "cuda" and f_dev.device.type == "cuda" and tuple(f_dev.shape) == (180, 3)
+  assert float(e_dev) == e_host
+  np.testing.assert_array_equal(f_dev.cpu().numpy(), f_host)
+  assert float(fn(torch.from_dlpack(t))) == e_host
+  assert fn.terms(t)["total"] == e_host
+  assert fn(torch.tensor(s["positions"])) == e_host  # CPU tensor: host path
+  assert fn(s["positions"]) == e_host                # the host cache was dropped
+  np.testing.assert_allclose(fn.born_radii(t), fn.born_radii(s["positions"]), rtol=0)
