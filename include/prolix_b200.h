@@ -217,6 +217,16 @@ int pb2_langevin_run(pb2_batch *batch, int32_t n_steps, void *stream);
  * (settle.py:1676-1696) does not center. */
 int pb2_langevin_center_momentum(pb2_batch *batch, void *stream);
 
+/* New Langevin parameters for the following steps, per system (n_systems
+ * each; NULL keeps that parameter): dt (tau), kT (kcal/mol), gamma (1/tau).
+ * Replaces apply_fn's per-call dt / kT overrides (settle.py:1698-1700).
+ * c1 = exp(-gamma dt), c2 = sqrt(1 - c1^2) and the per-atom noise amplitude
+ * c2 sqrt(m kT) are recomputed exactly as at batch creation, so a batch
+ * created with these values steps bit for bit the same.  Captured graphs
+ * stay valid (they read the parameters from device memory). */
+int pb2_set_langevin_params(pb2_batch *batch, const double *dt, const double *kT, const double *gamma,
+                            void *stream);
+
 /* Read or write the integrator state; any pointer may be NULL.
  * x, p, f: (n_atoms_total, 3); keys: (n_systems, 2); steps: (n_systems). */
 int pb2_get_state(pb2_batch *batch, double *x, double *p, double *f, uint32_t *keys,

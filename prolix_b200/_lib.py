@@ -110,6 +110,7 @@ SIGNATURES = [
     ("pb2_get_status", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                       ctypes.c_void_p]),
     ("pb2_langevin_center_momentum", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    ("pb2_set_langevin_params", ctypes.c_int, [ctypes.c_void_p] * 5),
     ("pb2_set_safeguards", ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
                                           ctypes.c_double]),
     ("pb2_get_safeguards", ctypes.c_int, [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_double)] * 3),

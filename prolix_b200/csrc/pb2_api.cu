@@ -401,6 +401,7 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
     S.gb_cutoff2 = gb_cut_mode ? (float)(gb_cut * gb_cut) : 0.f;
     S.born_cut2 = born_mode ? (float)(born_cut * born_cut) : 0.f;
     S.clamp = born_mode ? 1 : 0;
+    b->gamma_host.push_back(d.gamma);
     S.dt = d.dt;
     S.half_dt = 0.5 * d.dt;
     S.c1 = std::exp(-d.gamma * d.dt);
@@ -996,6 +997,32 @@ extern "C" int pb2_langevin_init(pb2_batch *b, void *stream) {
   b->key_parity ^= 1;
   int rc = fresh_forces(b, st, false);
   if (rc || (rc = forces_not_from_step(b, st))) return rc;
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  return PB2_OK;
+}
+
+extern "C" int pb2_set_langevin_params(pb2_batch *b, const double *dt, const double *kT,
+                                       const double *gamma, void *stream) {
+  if (!b) return PB2_EINVAL;
+  pb2_ctx *ctx = b->ctx;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int S = b->n_sys;
+  for (int s = 0; s < S; ++s)
+    if ((dt && !(dt[s] > 0.0)) || (kT && !(kT[s] >= 0.0)) || (gamma && !(gamma[s] >= 0.0)))
+      return fail(ctx, PB2_EINVAL, "dt > 0, kT >= 0, gamma >= 0");
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));  // steps in flight read the old values
+  for (int s = 0; s < S; ++s) {
+    SysInfo &I = b->sys_host[s];
+    if (dt) I.dt = dt[s];
+    if (kT) I.kT = kT[s];
+    if (gamma) b->gamma_host[s] = gamma[s];
+    I.half_dt = 0.5 * I.dt;
+    I.c1 = std::exp(-b->gamma_host[s] * I.dt);
+    I.c2 = std::sqrt(1.0 - I.c1 * I.c1);
+  }
+  CUDA_TRY(ctx, cudaMemcpyAsync(b->sys, b->sys_host.data(), S * sizeof(SysInfo), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(ctx, launch_noise_scale(b->sys, b->atom_sys, b->mass, b->sigma, b->n_total, st));
   CUDA_TRY(ctx, cudaStreamSynchronize(st));
   return PB2_OK;
 }

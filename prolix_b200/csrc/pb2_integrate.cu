@@ -286,6 +286,16 @@ __global__ void __launch_bounds__(kCenterThreads) center_kernel(const IntArgs a)
   }
 }
 
+// Per-atom noise amplitude c2 sqrt(m kT) after new Langevin parameters, the
+// same correctly rounded operations as at batch creation.
+__global__ void noise_scale_kernel(const SysInfo *sys, const int32_t *atom_sys, const double *mass,
+                                   double *sigma, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const SysInfo &S = sys[atom_sys[i]];
+    sigma[i] = __dmul_rn(S.c2, __dsqrt_rn(__dmul_rn(mass[i], S.kT)));
+  }
+}
+
 // Refresh the float32 pair-kernel positions from the FP64 state.
 __global__ void posq_kernel(const IntArgs a) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_total; i += gridDim.x * blockDim.x) {
@@ -317,6 +327,11 @@ cudaError_t launch_finish(const IntArgs &a, cudaStream_t st) {
 }
 cudaError_t launch_init(const IntArgs &a, cudaStream_t st) {
   init_kernel<<<grid_for(a.n_total), 256, 0, st>>>(a);
+  return cudaGetLastError();
+}
+cudaError_t launch_noise_scale(const SysInfo *sys, const int32_t *atom_sys, const double *mass,
+                               double *sigma, int n, cudaStream_t st) {
+  noise_scale_kernel<<<grid_for(n), 256, 0, st>>>(sys, atom_sys, mass, sigma, n);
   return cudaGetLastError();
 }
 cudaError_t launch_center(const IntArgs &a, cudaStream_t st) {

@@ -94,6 +94,7 @@ struct pb2_batch {
   // safeguards of the batched Langevin step (vlimit, max_dx, force_cap; <= 0
   // off), the closing-force flag and the per-system cap counters
   double guard[3] = {0.0, 0.0, 0.0};
+  std::vector<double> gamma_host;  // per-system friction (1/tau); c1, c2 derive from it
   int32_t *guard_end = nullptr;
   uint32_t *warn_flags = nullptr;
   int32_t *warn_counts = nullptr;

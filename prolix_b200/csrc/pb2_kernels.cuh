@@ -183,6 +183,8 @@ cudaError_t launch_bonded(const BondedArgs &a, int grid_cap, cudaStream_t st);
 cudaError_t launch_step(const IntArgs &a, cudaStream_t st);
 cudaError_t launch_finish(const IntArgs &a, cudaStream_t st);
 cudaError_t launch_center(const IntArgs &a, cudaStream_t st);
+cudaError_t launch_noise_scale(const SysInfo *sys, const int32_t *atom_sys, const double *mass,
+                               double *sigma, int n, cudaStream_t st);
 cudaError_t launch_init(const IntArgs &a, cudaStream_t st);
 cudaError_t launch_posq(const IntArgs &a, cudaStream_t st);
 // Host transfers: `user` maps each batch atom to its row in the caller's

@@ -410,6 +410,18 @@ class Batch:
     self._check(self.lib.pb2_get_status(self.handle, s.ctypes.data, 1 if clear else 0, stream))
     return s
 
+  def set_langevin_params(self, dt=None, kT=None, gamma=None, stream=None):
+    """New dt (tau), kT (kcal/mol) and/or gamma (1/tau) for the following
+    steps: a scalar for every system or one value per system; None keeps."""
+    def arr(v):
+      if v is None:
+        return None
+      return np.ascontiguousarray(np.broadcast_to(np.asarray(v, dtype=np.float64), (self.n_systems,)))
+    d, k, g = arr(dt), arr(kT), arr(gamma)
+    self._check(self.lib.pb2_set_langevin_params(self.handle, None if d is None else d.ctypes.data,
+                                                 None if k is None else k.ctypes.data,
+                                                 None if g is None else g.ctypes.data, stream))
+
   def center_momentum(self, stream=None):
     """Subtract each system's mean momentum (jax_md center_velocity; a
     one-atom system is left alone)."""

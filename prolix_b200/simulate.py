@@ -138,6 +138,10 @@ def nvt_langevin(energy_or_force_fn, shift_fn, dt: float, kT: float, gamma: floa
     return NVTLangevinState(batch, m)
 
   def apply_fn(state: NVTLangevinState, n_steps: int = 1, **kw):
+    # per-call dt / kT overrides, as the reference's apply_fn pops them
+    # (physics/settle.py:1698-1700); they hold for the following calls too
+    if "dt" in kw or "kT" in kw:
+      state._batch.set_langevin_params(dt=kw.get("dt"), kT=kw.get("kT"))
     state._batch.langevin_run(int(n_steps))
     return NVTLangevinState(state._batch, state._mass)
 

@@ -136,6 +136,27 @@ def test_langevin_zero_force_is_bit_exact():
   assert st["step"][0] == 7
 
 
+def test_new_langevin_parameters_mid_run_are_bit_exact():
+  # F = 0: 3 steps, then new dt, kT and gamma for 4 more, equal the oracle's
+  # steps with those arguments bit for bit (noise and its amplitude)
+  s = synth.make_chain(83, 19, compact=True)
+  dt, kT, gamma = engine.akma_dt(1.0), 300 * engine.KB_KCAL, engine.akma_gamma(1.0)
+  dt2, kT2, gamma2 = engine.akma_dt(0.5), 450 * engine.KB_KCAL, engine.akma_gamma(5.0)
+  key = prng.prng_key(808)
+  with engine.Batch([s], terms=0, key=key, dt=dt, kT=kT, gamma=gamma) as b:
+    b.langevin_init()
+    b.langevin_run(3)
+    b.set_langevin_params(dt=dt2, kT=kT2, gamma=gamma2)
+    b.langevin_run(4)
+    st = b.get_state()
+  zero = lambda r: np.zeros_like(r)
+  o = ointeg.init(zero, key, s["positions"], s["masses"], kT)
+  o = ointeg.run(o, zero, 3, dt, kT, gamma)
+  o = ointeg.run(o, zero, 4, dt2, kT2, gamma2)
+  np.testing.assert_array_equal(st["momentum"], o.momentum)
+  np.testing.assert_array_equal(st["position"], o.position)
+
+
 def test_langevin_bonded_only_tracks_oracle():
   s = synth.make_chain(120, 8, compact=True, cmap=True)
   dt, kT, gamma = engine.akma_dt(1.0), 300 * engine.KB_KCAL, engine.akma_gamma(1.0)
