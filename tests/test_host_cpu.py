@@ -252,3 +252,17 @@ def test_bench_reads_the_kernels_series_tiers():
   assert 3.0 <= k["value"] <= 6.0 and 4.0 <= k["deriv"] <= 7.0
   f = bench.flops_per_pair(k)
   assert f["born"] == 4 * k["value"] + 14 and f["chain"] == 4 * k["deriv"] + 27 and f["force"] == 55.0
+
+
+def test_prepare_system_packs_exception_pairs():
+  # ExclusionSpec field names -> descriptor (pairs, (charge product, sigma, epsilon))
+  s = synth.make_chain(30, 2)
+  ex = dict(s, exception_pairs=np.array([[0, 3], [5, 8]]), exception_chargeprods=[0.1, -0.2],
+            exception_sigmas=[3.0, 3.1], exception_epsilons=[0.05, 0.07])
+  p = engine.prepare_system(ex)
+  assert p["exception_pairs"].dtype == np.int32 and p["exception_pairs"].shape == (2, 2)
+  np.testing.assert_array_equal(p["exception_params"], [[0.1, 3.0, 0.05], [-0.2, 3.1, 0.07]])
+  d = engine._desc(p)
+  assert d.n_exceptions == 2
+  q = engine.prepare_system(s)
+  assert q["exception_pairs"].shape == (0, 2) and engine._desc(q).n_exceptions == 0
