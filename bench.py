@@ -27,6 +27,7 @@ import math
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -129,6 +130,9 @@ def parse():
   ap.add_argument("--e2e-groups", type=lambda v: [int(x) for x in v.split(",")], default=[12],
                   help="streams the end-to-end leg splits the systems over (comma list; the first "
                        "is the reported value)")
+  ap.add_argument("--clocks-dir", default=None,
+                  help="folder for the nvidia-smi clock samples of the timed region "
+                       "(default: the system temporary folder)")
   ap.add_argument("--no-serving", action="store_true")
   ap.add_argument("--no-extra", action="store_true",
                   help="skip the single-system, neighbour-list and serving-sweep legs")
@@ -484,7 +488,8 @@ def main():
   flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
   ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
   ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-  clk_path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv")
+  clk_dir = args.clocks_dir or tempfile.gettempdir()
+  clk_path = os.path.join(clk_dir, f"clocks_rank{rank}.csv")
   os.makedirs(os.path.dirname(clk_path), exist_ok=True)
   clk = clocks_start(clk_path)
   replicas.barrier()
