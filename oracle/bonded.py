@@ -12,6 +12,13 @@ Reference formulas (prolix, src/prolix/physics/):
   b2 = r_l - r_k, phi = atan2(y, x));
 * periodic torsion: bonded.py:110-141, E = sum_terms k (1 + cos(n phi - delta)),
   params (D, T, 3) = (n, delta, k);
+* impropers: system.py:63-88 picks the form by the parameters' last axis:
+  3 -> periodic, the torsion formula above (make_dihedral_energy_fn);
+  2 -> harmonic (make_harmonic_improper_energy_fn, bonded.py:144-185),
+  params (M, T, 2) = (k, phi0), E = sum k d^2 with
+  d = ((phi - phi0 + pi) mod 2 pi) - pi (no factor 1/2);
+* Urey-Bradley: harmonic bonds between the 1-3 atoms, the bond formula
+  above on (r0, k) rows (system.py:93-95);
 * CMAP: cmap.py:62-389.  Grids are stored (psi, phi) and transposed to
   (phi, psi) (cmap.py:256-259); derivatives at the grid points come from
   periodic cubic splines (create_periodic_spline :62-124,
@@ -130,6 +137,40 @@ def torsions(pos, idx, params):
   dedphi = (-k * n * np.sin(ang)).sum(1)
   _scatter(f, idx, [-(dedphi[:, None] * dphi[c]) for c in range(4)])
   return float(e), f
+
+
+def harmonic_impropers(pos, idx, params):
+  """k d^2, d = ((phi - phi0 + pi) mod 2 pi) - pi, params (M, T, 2) = (k, phi0)
+  (bonded.py:178-183)."""
+  idx = np.asarray(idx, np.int64).reshape(-1, 4)
+  f = np.zeros_like(pos)
+  if idx.shape[0] == 0:
+    return 0.0, f
+  params = np.asarray(params, np.float64).reshape(idx.shape[0], -1, 2)
+  phi, dphi = dihedral(pos, idx)
+  k, phi0 = params[..., 0], params[..., 1]
+  d = np.mod(phi[:, None] - phi0 + np.pi, 2.0 * np.pi) - np.pi
+  e = (k * d * d).sum()
+  dedphi = (2.0 * k * d).sum(1)
+  _scatter(f, idx, [-(dedphi[:, None] * dphi[c]) for c in range(4)])
+  return float(e), f
+
+
+def impropers(pos, idx, params):
+  """Either improper form, chosen as system.py:77-83 does by the last axis
+  of the parameters (2: harmonic, else periodic)."""
+  params = np.asarray(params, np.float64)
+  if params.size and params.shape[-1] == 2:
+    return harmonic_impropers(pos, idx, params)
+  return torsions(pos, idx, params)
+
+
+def _first(system, *keys, default):
+  for k in keys:
+    v = system.get(k)
+    if v is not None and np.asarray(v).size:
+      return v
+  return default
 
 
 # ---------------------------------------------------------------- CMAP
@@ -260,17 +301,29 @@ def exception_pairs(pos, pairs, sigmas, epsilons, chargeprods, k_coul=332.0637):
 
 
 def bonded_all(system, pos):
-  """Energies (dict: bond, angle, dihedral, cmap) and the summed force."""
+  """Energies (dict: bond, angle, dihedral, improper, urey_bradley, cmap)
+  and the summed force.  Key names as make_energy_fn reads them
+  (system.py:46-95): ``dihedrals`` or ``proper_dihedrals``, ``impropers``
+  or ``improper_dihedrals`` with ``improper_params`` or
+  ``improper_dihedral_params``, ``urey_bradley_bonds`` /
+  ``urey_bradley_params``."""
   pos = np.asarray(pos, np.float64)
   eb, fb = bonds(pos, system.get("bonds", np.zeros((0, 2))),
                  system.get("bond_params", np.zeros((0, 2))))
   ea, fa = angles(pos, system.get("angles", np.zeros((0, 3))),
                   system.get("angle_params", np.zeros((0, 2))))
-  ed, fd = torsions(pos, system.get("dihedrals", np.zeros((0, 4))),
-                    system.get("dihedral_params", np.zeros((0, 1, 3))))
+  ed, fd = torsions(pos, _first(system, "dihedrals", "proper_dihedrals", default=np.zeros((0, 4))),
+                    _first(system, "dihedral_params", "proper_dihedral_params",
+                           default=np.zeros((0, 1, 3))))
+  ei, fi = impropers(pos, _first(system, "impropers", "improper_dihedrals", default=np.zeros((0, 4))),
+                     _first(system, "improper_params", "improper_dihedral_params",
+                            default=np.zeros((0, 1, 3))))
+  eu, fu = bonds(pos, _first(system, "urey_bradley_bonds", default=np.zeros((0, 2))),
+                 _first(system, "urey_bradley_params", default=np.zeros((0, 2))))
   if "cmap_torsions" in system:
     ec, fc = cmap(pos, system["cmap_torsions"], system["cmap_indices"],
                   system["cmap_energy_grids"])
   else:
     ec, fc = 0.0, np.zeros_like(pos)
-  return {"bond": eb, "angle": ea, "dihedral": ed, "cmap": ec}, fb + fa + fd + fc
+  return ({"bond": eb, "angle": ea, "dihedral": ed, "improper": ei, "urey_bradley": eu, "cmap": ec},
+          fb + fa + fd + fi + fu + fc)

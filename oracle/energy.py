@@ -3,7 +3,8 @@
 TEST INFRASTRUCTURE ONLY (see ``oracle/__init__.py``).
 
 Mirrors the term split of prolix ``make_energy_fn(..., implicit_solvent=True)``
-(system.py:229-270): bond, angle, dihedral, cmap, lj, and electrostatics as
+(system.py:229-270): bond, angle, dihedral, improper, Urey-Bradley, cmap, lj,
+and electrostatics as
 (GB polar, direct Coulomb) plus the ACE nonpolar term and the explicit 1-4
 exception pairs.
 """
@@ -14,7 +15,8 @@ import numpy as np
 
 from . import bonded, gbsa
 
-TERMS = ("bond", "angle", "dihedral", "cmap", "lj", "coulomb", "gb", "nonpolar", "exception")
+TERMS = ("bond", "angle", "dihedral", "cmap", "lj", "coulomb", "gb", "nonpolar", "exception",
+         "improper", "urey_bradley")
 
 
 def energy_forces(system, pos, cutoff=0.0, **kw):

@@ -88,6 +88,67 @@ def exclusion_pairs(bonds, n_atoms: int):
   return pairs, kind
 
 
+def pairs_from_padded_table(excl_indices, scales_vdw, scales_elec):
+  """(pairs, kind, lj14, coul14) from prolix's per-atom padded exclusion
+  table (``excl_indices`` (N, K) int, -1 padding; ``excl_scales_vdw`` /
+  ``excl_scales_elec`` (N, K); physics/neighbor_list.py:236-303).
+
+  The reference scales pair (i, j) by the entry for j in row i
+  (optimization.py:51-53).  The batch holds two classes: excluded (both
+  scales 0) and one 1-4 class with a common (vdw, elec) pair.  Entries with
+  both scales 1 change nothing and are dropped.  A table with other
+  scales, a j listed twice in a row (the reference would add the scales),
+  or rows that disagree with each other on a pair raises ``ValueError``.
+  """
+  idx = np.asarray(excl_indices, dtype=np.int64)
+  if idx.ndim != 2:
+    raise ValueError(f"excl_indices must be (N, K), got shape {idx.shape}")
+  n = idx.shape[0]
+  sv = np.broadcast_to(np.asarray(scales_vdw if scales_vdw is not None else np.zeros(idx.shape),
+                                  dtype=np.float64), idx.shape)
+  se = np.broadcast_to(np.asarray(scales_elec if scales_elec is not None else np.zeros(idx.shape),
+                                  dtype=np.float64), idx.shape)
+  rows, cols = np.nonzero(idx >= 0)
+  j = idx[rows, cols]
+  if j.size and j.max() >= n:
+    raise ValueError(f"excl_indices holds atom {int(j.max())} of a {n}-atom system")
+  v, e = sv[rows, cols], se[rows, cols]
+  keep = (j != rows) & ~((v == 1.0) & (e == 1.0))
+  rows, j, v, e = rows[keep], j[keep], v[keep], e[keep]
+  if rows.size:
+    fwd = np.sort(rows * n + j)
+    if np.any(fwd[1:] == fwd[:-1]):
+      raise ValueError("excl_indices lists an atom twice in one row (the reference would add "
+                       "the two scales); merge the entries")
+    if not np.array_equal(fwd, np.sort(j * n + rows)):
+      raise ValueError("excl_indices is not symmetric: a pair listed in row i must be listed "
+                       "in row j too (the reference scales each direction by its own row)")
+  excl = (v == 0.0) & (e == 0.0)
+  scaled = np.unique(np.stack([v[~excl], e[~excl]], axis=1), axis=0)
+  if scaled.shape[0] > 1:
+    raise ValueError(f"excl_scales hold {scaled.shape[0]} distinct (vdw, elec) 1-4 scale pairs; "
+                     "one class is supported")
+  lj14, c14 = (float(scaled[0, 0]), float(scaled[0, 1])) if scaled.shape[0] else \
+      (LJ14_DEFAULT, COUL14_DEFAULT)
+  a, b = np.minimum(rows, j), np.maximum(rows, j)
+  kind = np.where(excl, 0, 1)
+  key = a * n + b
+  order = np.lexsort((kind, key))
+  key, kind = key[order], kind[order]
+  first = np.concatenate([[True], key[1:] != key[:-1]]) if key.size else np.zeros(0, bool)
+  # both directions must agree on a pair's class
+  uk, inv = np.unique(key, return_inverse=True)
+  kmin = np.full(uk.size, 2)
+  kmax = np.full(uk.size, -1)
+  np.minimum.at(kmin, inv, kind)
+  np.maximum.at(kmax, inv, kind)
+  if np.any(kmin != kmax):
+    raise ValueError("excl_indices rows disagree on the scale of a pair")
+  key, kind = key[first], kind[first]
+  pairs = np.stack([key // n, key % n], axis=1).astype(np.int32).reshape(-1, 2)
+  return pairs, kind.astype(np.int32), lj14, c14
+
+
 def _periodic_spline_slopes(y: np.ndarray) -> np.ndarray:
   """First derivatives at the knots of the periodic cubic spline through y
   (uniform spacing h = 2 pi / n)."""
