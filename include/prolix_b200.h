@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define PB2_ABI_VERSION 2
+#define PB2_ABI_VERSION 3
 
 /* status codes */
 #define PB2_OK 0
@@ -58,11 +58,13 @@ extern "C" {
 #define PB2_TERM_GB 6
 #define PB2_TERM_NONPOLAR 7
 #define PB2_TERM_EXCEPTION 8 /* explicit 1-4 exception pairs (prolix bonded.py:186-230) */
-#define PB2_TERM_TOTAL 9
-#define PB2_NTERMS 10
+#define PB2_TERM_IMPROPER 9  /* impropers, periodic or harmonic (system.py:63-88) */
+#define PB2_TERM_UREY_BRADLEY 10 /* Urey-Bradley 1-3 springs (system.py:93-95) */
+#define PB2_TERM_TOTAL 11
+#define PB2_NTERMS 12
 
 /* term-enable bits (pb2_run_params.terms) */
-#define PB2_USE_BONDED 0x1u    /* bonds, angles, torsions */
+#define PB2_USE_BONDED 0x1u    /* bonds, angles, torsions, impropers, Urey-Bradley */
 #define PB2_USE_CMAP 0x2u
 #define PB2_USE_LJ 0x4u
 #define PB2_USE_COULOMB 0x8u
@@ -132,6 +134,23 @@ typedef struct pb2_system_desc {
   int32_t n_exceptions;
   const int32_t *exception_pairs;  /* (n_exceptions, 2) */
   const double *exception_params;  /* (n_exceptions, 3) = (charge product, sigma, epsilon) */
+
+  /* Impropers (prolix make_energy_fn, system.py:63-88; bonded.py:110-185).
+   * improper_form 0, periodic: params (n_impropers, T, 3) = (n, phase, k),
+   *   E = sum k (1 + cos(n phi - phase)), the torsion formula;
+   * improper_form 1, harmonic: params (n_impropers, T, 2) = (k, phi0),
+   *   E = sum k d^2 with d = ((phi - phi0 + pi) mod 2 pi) - pi (no 1/2).
+   * phi is the dihedral of atoms 0-1-2-3 of a row, as for torsions. */
+  int32_t n_impropers;
+  int32_t n_improper_terms;   /* T */
+  int32_t improper_form;      /* 0 periodic, 1 harmonic */
+  const int32_t *impropers;   /* (n_impropers, 4) */
+  const double *improper_params;
+
+  /* Urey-Bradley springs between 1-3 atoms (system.py:93-95): E = k/2 (r - r0)^2. */
+  int32_t n_urey_bradley;
+  const int32_t *urey_bradley_bonds;   /* (n_urey_bradley, 2) */
+  const double *urey_bradley_params;   /* (n_urey_bradley, 2) = (r0, k) */
 } pb2_system_desc;
 
 /* Batch-wide settings. */
@@ -154,6 +173,12 @@ typedef struct pb2_run_params {
                               (compact 32-atom blocks, which the pair kernels' bounding-box
                               tests favour); 1: in input order.  Either way every array
                               crossing this interface is in input order. */
+  int32_t pair_list;    /* 0: automatic: when every pair term in use has a cutoff, the pair
+                           kernels work from a skin-buffered list of 32-atom block pairs
+                           within cutoff + skin, rebuilt on the device when an atom has
+                           moved more than skin/2 since the last build (jax_md's
+                           dr_threshold rule, batched_simulate.py:1600-1622); -1: off (every
+                           block pair, culled by bounding boxes at each step) */
 } pb2_run_params;
 
 typedef struct pb2_ctx pb2_ctx;
@@ -223,7 +248,9 @@ int pb2_langevin_center_momentum(pb2_batch *batch, void *stream);
  * c1 = exp(-gamma dt), c2 = sqrt(1 - c1^2) and the per-atom noise amplitude
  * c2 sqrt(m kT) are recomputed exactly as at batch creation, so a batch
  * created with these values steps bit for bit the same.  Captured graphs
- * stay valid (they read the parameters from device memory). */
+ * stay valid (they read the parameters from device memory).  The call
+ * first waits for all work queued on the device, on every stream, so steps
+ * issued before it run with the old values. */
 int pb2_set_langevin_params(pb2_batch *batch, const double *dt, const double *kT, const double *gamma,
                             void *stream);
 
@@ -256,6 +283,16 @@ int pb2_set_full_state(pb2_batch *batch, const double *x, const double *p, const
  * other batches compute. */
 int pb2_langevin_run_host(pb2_batch *batch, double *x, double *p, double *f, int32_t n_steps,
                           void *stream, void *copy_in, void *copy_out);
+
+/* The same functional apply_fn (settle.py:1698-1744) on DEVICE arrays of the
+ * batch's device: x, p, f ((n_atoms_total, 3) FP64 row-major, f the forces
+ * at x) are read, n_steps steps run, and the new state is written back into
+ * them, all on `stream` without waiting.  This is what a jax.ffi handler
+ * binds (XLA owns the buffers).  Steps run as CUDA graphs of up to
+ * graph_chunk steps, captured the first time each chunk length is needed:
+ * make a first call with the same n_steps outside any stream capture. */
+int pb2_langevin_run_device(pb2_batch *batch, double *x, double *p, double *f, int32_t n_steps,
+                            void *stream);
 
 /*
  * Batched energy minimisation (replaces prolix batched_simulate.py:682-960,
@@ -349,18 +386,27 @@ int pb2_get_safeguards(const pb2_batch *batch, double *vlimit, double *max_dx, d
 int pb2_get_warn_counts(pb2_batch *batch, int32_t *counts, int reset, void *stream);
 
 /*
- * Neighbour list (cutoff > 0 only).  pb2_nl_build rebuilds unconditionally;
- * pb2_nl_check compares the displacement since the last build against
- * skin/2 (batched_simulate.py:1600-1622) and rebuilds where exceeded;
- * *rebuilt receives how many systems were rebuilt.  pb2_nl_get copies the
+ * Neighbour list (cutoff > 0 only), built by a cell list on the device
+ * (jax_md partition.neighbor_list layout, physics/neighbor_list.py:155-172;
+ * batched_simulate.py:1429-1464).  pb2_nl_build rebuilds unconditionally
+ * and returns when the capacity is known (the first build sizes it, as
+ * jax_md's allocate does).  pb2_nl_check compares each atom's displacement
+ * since the last build against skin/2 (batched_simulate.py:1600-1622) and
+ * rebuilds when any exceeds it, all decided on the device; with rebuilt
+ * non-NULL it waits and *rebuilt receives how many systems had moved that
+ * far, with rebuilt NULL it only enqueues (a list that outgrew its capacity
+ * is flagged with PB2_STATUS_NLOVERFLOW and grown at the next pb2_nl_check
+ * with rebuilt, pb2_nl_build or pb2_nl_get).  pb2_nl_get copies the
  * per-atom list in jax_md layout: (n_atoms_total, capacity) int32 local
  * indices, both (i, j) and (j, i) present, padded with the sentinel n_atoms
- * of the atom's system.
+ * of the atom's system.  pb2_nl_last_build_ms: device time of the last
+ * build's launches (CUDA events; diagnostic, no reference counterpart).
  */
 int pb2_nl_build(pb2_batch *batch, void *stream);
 int pb2_nl_check(pb2_batch *batch, int32_t *rebuilt, void *stream);
 int pb2_nl_capacity(const pb2_batch *batch, int32_t *capacity);
 int pb2_nl_get(pb2_batch *batch, int32_t *neighbors, void *stream);
+int pb2_nl_last_build_ms(pb2_batch *batch, double *ms);
 
 /* Device time of the last pb2_langevin_run with profiling enabled (eager
  * launches, CUDA events around each kernel), milliseconds summed over the
@@ -392,7 +438,10 @@ int pb2_fp32_peak(pb2_ctx *ctx, double *tflops);
  * is limited to PB2_NOALLOC_MAX_ATOMS; calls that overlap on the GPU race on
  * it and must be serialised.  The first call on a device looks the array up
  * (cudaGetSymbolAddress) with that device current: make it before any
- * stream capture.  ctx may be NULL (errors are then not recorded).
+ * stream capture (after a cudaDeviceReset the next call looks it up again).
+ * The buffers must be device memory of the current device, which must be
+ * the context's device when ctx is given (PB2_EINVAL otherwise).  ctx may
+ * be NULL (errors are then not recorded).
  */
 #define PB2_NOALLOC_MAX_ATOMS 32768
 int pb2_born_radii_noalloc(pb2_ctx *ctx, int32_t n_atoms, const double *positions,

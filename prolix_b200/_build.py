@@ -2,8 +2,13 @@
 
 * ``libprolix_b200.so``: the CUDA kernels and the C ABI (nvcc, sm_100a only).
 * ``libpb2_host.so``: host C helpers (synthetic chain growth).
+* ``libprolix_b200_ffi.so`` (only on request): the XLA FFI handlers of
+  ``csrc/ffi/pb2_ffi.cc``, which need the headers of an XLA / jaxlib
+  install (``xla/ffi/api/ffi.h``): ``python -m prolix_b200._build --ffi
+  <include dir>`` or ``PB2_XLA_FFI_INCLUDE=<include dir>``.  The default
+  build skips it.
 
-Both land next to this file so they travel with the source tree.
+All land next to this file so they travel with the source tree.
 """
 
 from __future__ import annotations
@@ -21,7 +26,7 @@ HOST_LIB = PKG / "libpb2_host.so"
 
 CUDA_SOURCES = ["pb2_api.cu", "pb2_pair.cu", "pb2_energy64.cu", "pb2_bonded.cu",
                 "pb2_integrate.cu", "pb2_nlist.cu", "pb2_noalloc.cu", "pb2_diag.cu",
-                "pb2_transfer.cu", "pb2_minimize.cu"]
+                "pb2_transfer.cu", "pb2_minimize.cu", "pb2_pairlist.cu"]
 CUDA_HEADERS = ["pb2_common.cuh", "pb2_kernels.cuh", "pb2_internal.h", "pb2_pairmath.cuh",
                 "pb2_threefry.cuh", "pb2_obc_series.cuh"]
 HOST_SOURCES = ["synth_chain.c"]
@@ -92,6 +97,41 @@ def build_cuda(force: bool = False, extra_flags=None) -> Path:
   return CUDA_LIB
 
 
+FFI_SOURCE = CSRC / "ffi" / "pb2_ffi.cc"
+FFI_LIB = PKG / "libprolix_b200_ffi.so"
+
+
+def build_ffi(xla_include: str) -> Path:
+  """The jax.ffi handler library, linked against libprolix_b200.so."""
+  inc = Path(xla_include)
+  if not (inc / "xla" / "ffi" / "api" / "ffi.h").exists():
+    raise FileNotFoundError(f"{inc}/xla/ffi/api/ffi.h not found: XLA FFI headers are required")
+  build_cuda()
+  cuda_inc = Path(_nvcc()).resolve().parent.parent / "include"
+  cxx = shutil.which("g++") or "c++"
+  tmp = FFI_LIB.with_suffix(".so.tmp")
+  subprocess.run([cxx, "-O2", "-std=c++17", "-shared", "-fPIC", "-I", str(inc), "-I", str(INCLUDE),
+                  "-I", str(cuda_inc), "-o", str(tmp), str(FFI_SOURCE), "-L", str(PKG),
+                  "-lprolix_b200", f"-Wl,-rpath,{PKG}", "-L", str(cuda_inc.parent / "lib64"),
+                  "-lcudart"], check=True)
+  os.replace(tmp, FFI_LIB)
+  return FFI_LIB
+
+
 def build_all(force: bool = False) -> None:
   build_host(force)
   build_cuda(force)
+  xla = os.environ.get("PB2_XLA_FFI_INCLUDE")
+  if xla:
+    build_ffi(xla)
+
+
+if __name__ == "__main__":
+  import argparse
+  ap = argparse.ArgumentParser(description="build the prolix_b200 native libraries in-tree")
+  ap.add_argument("--force", action="store_true")
+  ap.add_argument("--ffi", metavar="XLA_INCLUDE", help="also build the jax.ffi handlers")
+  args = ap.parse_args()
+  build_all(args.force)
+  if args.ffi:
+    build_ffi(args.ffi)

@@ -22,9 +22,9 @@ ERRORS = {
 }
 
 TERM_NAMES = ("bond", "angle", "dihedral", "cmap", "lj", "coulomb", "gb", "nonpolar", "exception",
-              "total")
-NTERMS = 10
-ABI_VERSION = 2  # PB2_ABI_VERSION of the structures mirrored below
+              "improper", "urey_bradley", "total")
+NTERMS = 12
+ABI_VERSION = 3  # PB2_ABI_VERSION of the structures mirrored below
 USE_BONDED, USE_CMAP, USE_LJ, USE_COULOMB, USE_GB = 0x1, 0x2, 0x4, 0x8, 0x10
 USE_ALL = 0x1F
 STATUS_NONFINITE, STATUS_NLOVERFLOW, STATUS_FORCE_RANGE = 0x1, 0x2, 0x4
@@ -52,6 +52,10 @@ class SystemDesc(ctypes.Structure):
       ("dt", ctypes.c_double), ("kT", ctypes.c_double), ("gamma", ctypes.c_double),
       ("use_origin", ctypes.c_int32), ("origin", ctypes.c_double * 3),
       ("n_exceptions", ctypes.c_int32), ("exception_pairs", _c_ip), ("exception_params", _c_dp),
+      ("n_impropers", ctypes.c_int32), ("n_improper_terms", ctypes.c_int32),
+      ("improper_form", ctypes.c_int32), ("impropers", _c_ip), ("improper_params", _c_dp),
+      ("n_urey_bradley", ctypes.c_int32), ("urey_bradley_bonds", _c_ip),
+      ("urey_bradley_params", _c_dp),
   ]
 
 
@@ -67,6 +71,7 @@ class RunParams(ctypes.Structure):
       ("gb_cutoff", ctypes.c_double),
       ("born_cutoff", ctypes.c_double),
       ("keep_atom_order", ctypes.c_int32),
+      ("pair_list", ctypes.c_int32),
   ]
 
 
@@ -93,6 +98,8 @@ SIGNATURES = [
     ("pb2_langevin_run_host", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                              ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
                                              ctypes.c_void_p, ctypes.c_void_p]),
+    ("pb2_langevin_run_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                               ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]),
     ("pb2_min_setup", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("pb2_min_sd", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_double, ctypes.c_int32,
                                   ctypes.c_double, ctypes.c_double, ctypes.c_void_p]),
@@ -120,6 +127,7 @@ SIGNATURES = [
     ("pb2_nl_check", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32), ctypes.c_void_p]),
     ("pb2_nl_capacity", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]),
     ("pb2_nl_get", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("pb2_nl_last_build_ms", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
     ("pb2_set_tile_segment", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     ("pb2_get_tile_segment", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]),
     ("pb2_set_profiling", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),

@@ -87,6 +87,27 @@ static PairArgs pair_args(pb2_batch *b) {
   a.fy = b->fy;
   a.fz = b->fz;
   a.energy = b->energy;
+  a.pl_ctl = b->pl_on ? b->pl_ctl : nullptr;
+  a.pl_items0 = b->pl_items[0];
+  a.pl_items1 = b->pl_items[1];
+  a.pl_jlist = b->pl_jlist;
+  return a;
+}
+
+static PlArgs pl_args(pb2_batch *b) {
+  PlArgs a;
+  a.sys = b->sys;
+  a.rows = b->pl_rows;
+  a.n_rows = b->n_pl_rows;
+  a.bbox = b->bbox;
+  a.posq = b->posq;
+  a.ref = b->pl_ref;
+  a.jlist = b->pl_jlist;
+  a.items0 = b->pl_items[0];
+  a.items1 = b->pl_items[1];
+  a.ctl = b->pl_ctl;
+  a.reach2 = b->pl_reach2;
+  a.seg = b->params.tile_segment;
   return a;
 }
 
@@ -229,6 +250,49 @@ static int setup_items2(pb2_batch *b, int seg) {
   return PB2_OK;
 }
 
+// The pair list of a cutoff run (pb2_pairlist.cu): rows (one per pair of
+// i-blocks), room for every j-block of each row, two item buffers sized for
+// the segment, and the control words, with the rebuild flag set so that the
+// first force evaluation builds it.
+static int setup_pair_list(pb2_batch *b, int seg) {
+  pb2_ctx *ctx = b->ctx;
+  if (!b->pl_on) return PB2_OK;
+  std::vector<PlRow> rows;
+  size_t jcap = 0, icap = 0;
+  for (int s = 0; s < b->n_sys; ++s) {
+    const int nblk = b->sys_host[s].nblk;
+    for (int ib = 0; ib < nblk; ib += 2) {
+      rows.push_back(PlRow{s, ib, (int32_t)jcap, 0});
+      jcap += (size_t)(nblk - ib);
+      icap += (size_t)((nblk - ib + seg - 1) / seg);
+    }
+  }
+  if (jcap > (size_t)INT32_MAX) return fail(ctx, PB2_EINVAL, "pair list too large");
+  Dev &D = b->dev;
+  if (!b->pl_rows) {
+    b->pl_rows = D.alloc<PlRow>(rows.size());
+    b->pl_jlist = D.alloc<int32_t>(std::max<size_t>(jcap, 1));
+    b->pl_ctl = D.alloc<int32_t>(PL_WORDS);
+    b->pl_ref = D.alloc<float4>(b->n_total);
+    if (!b->pl_rows || !b->pl_jlist || !b->pl_ctl || !b->pl_ref)
+      return fail(ctx, PB2_ENOMEM, "pair-list allocation failed");
+    CUDA_TRY(ctx, cudaMemcpy(b->pl_rows, rows.data(), rows.size() * sizeof(PlRow), cudaMemcpyHostToDevice));
+    b->n_pl_rows = (int)rows.size();
+  }
+  if (icap > b->pl_item_cap) {
+    for (auto &p : b->pl_items) {
+      D.release(p);
+      p = D.alloc<TileItem>(icap);
+      if (!p) return fail(ctx, PB2_ENOMEM, "pair-list item allocation failed");
+    }
+    b->pl_item_cap = icap;
+  }
+  const int32_t ctl[PL_WORDS] = {1, 0, 0, 0, 0, 0, 0, 0};  // dirty: rebuild at the next evaluation
+  CUDA_TRY(ctx, cudaMemcpy(b->pl_ctl, ctl, sizeof ctl, cudaMemcpyHostToDevice));
+  b->grid_pl = std::max(1, std::min(8 * ctx->sm_count, (b->n_pl_rows + 7) / 8));
+  return PB2_OK;
+}
+
 static int validate(pb2_ctx *ctx, const pb2_system_desc &d, int s) {
   char buf[256];
   auto bad = [&](const char *what) {
@@ -253,8 +317,13 @@ static int validate(pb2_ctx *ctx, const pb2_system_desc &d, int s) {
     return true;
   };
   if (d.n_bonds < 0 || d.n_angles < 0 || d.n_torsions < 0 || d.n_cmap < 0 || d.n_excl < 0 ||
-      d.n_exceptions < 0)
+      d.n_exceptions < 0 || d.n_impropers < 0 || d.n_urey_bradley < 0)
     return bad("negative term count");
+  if (d.n_impropers && (!d.impropers || !d.improper_params || d.n_improper_terms <= 0 ||
+                        (d.improper_form != 0 && d.improper_form != 1)))
+    return bad("improper arrays missing or improper_form not 0 (periodic) / 1 (harmonic)");
+  if (d.n_urey_bradley && (!d.urey_bradley_bonds || !d.urey_bradley_params))
+    return bad("Urey-Bradley arrays missing");
   if (d.n_bonds && (!d.bonds || !d.bond_params)) return bad("bond arrays missing");
   if (d.n_angles && (!d.angles || !d.angle_params)) return bad("angle arrays missing");
   if (d.n_torsions && (!d.torsions || !d.torsion_params || d.n_torsion_terms <= 0))
@@ -269,7 +338,9 @@ static int validate(pb2_ctx *ctx, const pb2_system_desc &d, int s) {
       !check_idx(d.torsions, 4LL * d.n_torsions, "torsion") ||
       !check_idx(d.cmap_rows, 5LL * d.n_cmap, "cmap") ||
       !check_idx(d.excl_pairs, 2LL * d.n_excl, "exclusion") ||
-      !check_idx(d.exception_pairs, 2LL * d.n_exceptions, "exception"))
+      !check_idx(d.exception_pairs, 2LL * d.n_exceptions, "exception") ||
+      !check_idx(d.impropers, 4LL * d.n_impropers, "improper") ||
+      !check_idx(d.urey_bradley_bonds, 2LL * d.n_urey_bradley, "Urey-Bradley"))
     return fail(ctx, PB2_EINVAL, buf);
   for (int k = 0; k < d.n_cmap; ++k)
     if (d.cmap_map[k] < 0 || d.cmap_map[k] >= d.n_cmap_maps) return bad("cmap map index out of range");
@@ -520,8 +591,8 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   b->sys_host = sinfo;
 
   // --- bonded tables (global atom indices)
-  std::vector<int2> bidx;
-  std::vector<double2> bpar;
+  std::vector<int2> bidx, uidx;  // bonds, Urey-Bradley springs
+  std::vector<double2> bpar, upar;
   std::vector<int4> aidx;
   std::vector<double2> apar;
   std::vector<int4> tidx;
@@ -550,8 +621,24 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
         const double *p = d.torsion_params + ((size_t)k * d.n_torsion_terms + t) * 3;
         tidx.push_back(make_int4(at(d.torsions[4 * k]), at(d.torsions[4 * k + 1]),
                                  at(d.torsions[4 * k + 2]), at(d.torsions[4 * k + 3])));
-        tpar.push_back(make_double4(p[0], p[1], p[2], 0.0));
+        tpar.push_back(make_double4(p[0], p[1], p[2], kTorsProper));
       }
+    for (int k = 0; k < d.n_impropers; ++k)
+      for (int t = 0; t < d.n_improper_terms; ++t) {
+        tidx.push_back(make_int4(at(d.impropers[4 * k]), at(d.impropers[4 * k + 1]),
+                                 at(d.impropers[4 * k + 2]), at(d.impropers[4 * k + 3])));
+        if (d.improper_form == 1) {
+          const double *p = d.improper_params + ((size_t)k * d.n_improper_terms + t) * 2;
+          tpar.push_back(make_double4(p[0], p[1], 0.0, kTorsHarmonic));
+        } else {
+          const double *p = d.improper_params + ((size_t)k * d.n_improper_terms + t) * 3;
+          tpar.push_back(make_double4(p[0], p[1], p[2], kTorsImproper));
+        }
+      }
+    for (int k = 0; k < d.n_urey_bradley; ++k) {
+      uidx.push_back(make_int2(at(d.urey_bradley_bonds[2 * k]), at(d.urey_bradley_bonds[2 * k + 1])));
+      upar.push_back(make_double2(d.urey_bradley_params[2 * k], d.urey_bradley_params[2 * k + 1]));
+    }
     const int map_base = (int)cgrid.size();
     const size_t per_map = (size_t)d.cmap_grid * d.cmap_grid * 16;
     for (int m = 0; m < d.n_cmap_maps && d.n_cmap > 0; ++m) {
@@ -587,6 +674,10 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
     par.swap(par2);
   };
   by_atom(bidx, bpar, [](const int2 &t) { return std::min(t.x, t.y); });
+  by_atom(uidx, upar, [](const int2 &t) { return std::min(t.x, t.y); });
+  const int n_bond_plain = (int)bidx.size();  // Urey-Bradley springs follow the bonds
+  bidx.insert(bidx.end(), uidx.begin(), uidx.end());
+  bpar.insert(bpar.end(), upar.begin(), upar.end());
   by_atom(aidx, apar, [](const int4 &t) { return t.y; });
   by_atom(tidx, tpar, [](const int4 &t) { return std::min(t.y, t.z); });
   by_atom(eidx, epar, [](const int2 &t) { return std::min(t.x, t.y); });
@@ -610,6 +701,23 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   b->blk_sys = D.alloc<int32_t>(blocks_total);
   b->n_blocks = blocks_total;
   b->cut = cutoff_mode || gb_cut_mode || born_mode;
+  {
+    // the pair list needs a finite reach for every pair term in use
+    const uint32_t t = params->terms;
+    const bool direct = (t & (PB2_USE_LJ | PB2_USE_COULOMB)) != 0, gbt = (t & PB2_USE_GB) != 0;
+    double reach = 0.0;
+    bool finite = b->cut && params->skin >= 0.0 && params->pair_list >= 0;
+    if (direct) {
+      finite = finite && cutoff_mode;
+      reach = std::max(reach, params->cutoff);
+    }
+    if (gbt) {
+      finite = finite && gb_cut_mode;
+      reach = std::max(reach, std::max(gb_cut, born_cut));
+    }
+    b->pl_on = finite && (direct || gbt);
+    b->pl_reach2 = (float)((reach + params->skin) * (reach + params->skin));
+  }
   b->q64 = D.alloc<double>(N);
   b->hs64 = D.alloc<double>(N);
   b->se64 = D.alloc<double>(N);
@@ -633,6 +741,7 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   b->excl_rows = D.alloc<ExclRow>(hrows.size());
   BondedArgs &B = b->bonded;
   B.n_bond = (int)bidx.size();
+  B.n_bond_plain = n_bond_plain;
   B.n_angle = (int)aidx.size();
   B.n_tors = (int)tidx.size();
   B.n_cmap = (int)(cidx.size() / 6);
@@ -704,10 +813,12 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
 
   b->grid_bonded = 8 * ctx->sm_count;
   if ((rc = setup_items2(b.get(), b->params.tile_segment))) return rc;
+  if ((rc = setup_pair_list(b.get(), b->params.tile_segment))) return rc;
   CUDA_TRY(ctx, cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking));
   CUDA_TRY(ctx, cudaEventCreate(&b->ev[0]));
   CUDA_TRY(ctx, cudaEventCreate(&b->ev[1]));
   for (auto &e : b->ev_io) CUDA_TRY(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  for (auto &e : b->nl_ev) CUDA_TRY(ctx, cudaEventCreate(&e));
   CUDA_TRY(ctx, cudaDeviceSynchronize());
   *out = b.release();
   return PB2_OK;
@@ -756,7 +867,12 @@ static cudaError_t enqueue_forces(pb2_batch *b, cudaStream_t st, bool bonded_ene
   Timer tm{b, st};
   PairArgs pa = pair_args(b);
   const bool gb = (b->params.terms & PB2_USE_GB) != 0;
-  if ((e = tm(kTimBbox, [&] { return launch_bbox(b->sys, b->blk_sys, b->posq, b->bbox, b->n_blocks, st); })) != cudaSuccess)
+  if ((e = tm(kTimBbox, [&] {
+         return launch_bbox(b->sys, b->blk_sys, b->posq, b->bbox, b->n_blocks, st,
+                            b->pl_on ? b->pl_ref : nullptr, b->pl_on ? b->pl_ctl : nullptr);
+       })) != cudaSuccess)
+    return e;
+  if (b->pl_on && (e = tm(kTimBbox, [&] { return launch_pl_update(pl_args(b), b->grid_pl, st); })) != cudaSuccess)
     return e;
   if (gb) {
     pa.sched = b->sched + 2 * PASS_BORN;
@@ -1011,7 +1127,9 @@ extern "C" int pb2_set_langevin_params(pb2_batch *b, const double *dt, const dou
     if ((dt && !(dt[s] > 0.0)) || (kT && !(kT[s] >= 0.0)) || (gamma && !(gamma[s] >= 0.0)))
       return fail(ctx, PB2_EINVAL, "dt > 0, kT >= 0, gamma >= 0");
   CUDA_TRY(ctx, cudaSetDevice(ctx->device));
-  CUDA_TRY(ctx, cudaStreamSynchronize(st));  // steps in flight read the old values
+  // steps already queued, on any stream of the device, finish with the old
+  // values: the per-system constants are overwritten in place
+  CUDA_TRY(ctx, cudaDeviceSynchronize());
   for (int s = 0; s < S; ++s) {
     SysInfo &I = b->sys_host[s];
     if (dt) I.dt = dt[s];
@@ -1146,8 +1264,12 @@ extern "C" int pb2_set_full_state(pb2_batch *b, const double *x, const double *p
 }
 
 
-extern "C" int pb2_langevin_run_host(pb2_batch *b, double *x, double *p, double *f, int32_t n_steps,
-                                     void *stream, void *copy_in, void *copy_out) {
+// The functional step on caller-held state: copies in on copy_in, steps on
+// stream, copies out on copy_out.  kind_in / kind_out are the directions of
+// the copies (host arrays, or the caller's device arrays).
+static int run_caller_state(pb2_batch *b, double *x, double *p, double *f, int32_t n_steps,
+                            void *stream, void *copy_in, void *copy_out, cudaMemcpyKind kind_in,
+                            cudaMemcpyKind kind_out) {
   if (!b || !x || !p || !f || n_steps < 0) return PB2_EINVAL;
   pb2_ctx *ctx = b->ctx;
   cudaStream_t st = (cudaStream_t)stream, ci = (cudaStream_t)copy_in, co = (cudaStream_t)copy_out;
@@ -1157,9 +1279,9 @@ extern "C" int pb2_langevin_run_host(pb2_batch *b, double *x, double *p, double 
   // in: the previous round trip's copies out of the staging buffer are done;
   // the three copies back to back, then one conversion
   CUDA_TRY(ctx, cudaStreamWaitEvent(ci, b->ev_io[2], 0));
-  CUDA_TRY(ctx, cudaMemcpyAsync(b->stage, x, bytes, cudaMemcpyHostToDevice, ci));
-  CUDA_TRY(ctx, cudaMemcpyAsync(b->stage + rows, p, bytes, cudaMemcpyHostToDevice, ci));
-  CUDA_TRY(ctx, cudaMemcpyAsync(b->stage + 2 * rows, f, bytes, cudaMemcpyHostToDevice, ci));
+  CUDA_TRY(ctx, cudaMemcpyAsync(b->stage, x, bytes, kind_in, ci));
+  CUDA_TRY(ctx, cudaMemcpyAsync(b->stage + rows, p, bytes, kind_in, ci));
+  CUDA_TRY(ctx, cudaMemcpyAsync(b->stage + 2 * rows, f, bytes, kind_in, ci));
   CUDA_TRY(ctx, cudaEventRecord(b->ev_io[0], ci));
   CUDA_TRY(ctx, cudaStreamWaitEvent(st, b->ev_io[0], 0));
   CUDA_TRY(ctx, launch_state_from_rows(b->stage, b->user, b->x, b->y, b->z, b->px, b->py, b->pz, b->fx, b->fy, b->fz,
@@ -1173,11 +1295,23 @@ extern "C" int pb2_langevin_run_host(pb2_batch *b, double *x, double *p, double 
                                      b->stage, N, st));
   CUDA_TRY(ctx, cudaEventRecord(b->ev_io[1], st));
   CUDA_TRY(ctx, cudaStreamWaitEvent(co, b->ev_io[1], 0));
-  CUDA_TRY(ctx, cudaMemcpyAsync(x, b->stage, bytes, cudaMemcpyDeviceToHost, co));
-  CUDA_TRY(ctx, cudaMemcpyAsync(p, b->stage + rows, bytes, cudaMemcpyDeviceToHost, co));
-  CUDA_TRY(ctx, cudaMemcpyAsync(f, b->stage + 2 * rows, bytes, cudaMemcpyDeviceToHost, co));
+  CUDA_TRY(ctx, cudaMemcpyAsync(x, b->stage, bytes, kind_out, co));
+  CUDA_TRY(ctx, cudaMemcpyAsync(p, b->stage + rows, bytes, kind_out, co));
+  CUDA_TRY(ctx, cudaMemcpyAsync(f, b->stage + 2 * rows, bytes, kind_out, co));
   CUDA_TRY(ctx, cudaEventRecord(b->ev_io[2], co));
   return PB2_OK;
+}
+
+extern "C" int pb2_langevin_run_host(pb2_batch *b, double *x, double *p, double *f, int32_t n_steps,
+                                     void *stream, void *copy_in, void *copy_out) {
+  return run_caller_state(b, x, p, f, n_steps, stream, copy_in, copy_out, cudaMemcpyHostToDevice,
+                          cudaMemcpyDeviceToHost);
+}
+
+extern "C" int pb2_langevin_run_device(pb2_batch *b, double *x, double *p, double *f, int32_t n_steps,
+                                       void *stream) {
+  return run_caller_state(b, x, p, f, n_steps, stream, stream, stream, cudaMemcpyDeviceToDevice,
+                          cudaMemcpyDeviceToDevice);
 }
 
 // ------------------------------------------------------------ minimisation
@@ -1616,6 +1750,7 @@ extern "C" int pb2_set_tile_segment(pb2_batch *b, int32_t segment) {
   b->n_items = (int)items.size();
   b->params.tile_segment = segment;
   if (int rc = setup_items2(b, segment)) return rc;
+  if (int rc = setup_pair_list(b, segment)) return rc;
   for (auto &kv : b->graphs) cudaGraphExecDestroy(kv.second);  // they captured the old list
   b->graphs.clear();
   for (auto &kv : b->min_graphs) cudaGraphExecDestroy(kv.second);

@@ -1,10 +1,14 @@
-// Bonded terms: harmonic bonds and angles, periodic torsions and CMAP, all
-// systems of the batch in one launch, one thread per term.
+// Bonded terms: harmonic bonds, Urey-Bradley springs and angles, periodic
+// torsions, periodic and harmonic impropers and CMAP, all systems of the
+// batch in one launch, one thread per term.
 //
-// Reference: prolix physics/bonded.py:20-141 (bond via jax_md
-// simple_spring_bond, E = k/2 (r - r0)^2; angle with the 1e-8 guard and the
+// Reference: prolix physics/bonded.py:20-185 (bond via jax_md
+// simple_spring_bond, E = k/2 (r - r0)^2, also for the Urey-Bradley 1-3
+// springs of system.py:93-95; angle with the 1e-8 guard and the
 // +-0.999999 clip; dihedral angle b0 = r_i - r_j, b1 = r_k - r_j,
-// b2 = r_l - r_k, phi = atan2(y, x); torsion sum k (1 + cos(n phi - delta)))
+// b2 = r_l - r_k, phi = atan2(y, x); torsion sum k (1 + cos(n phi - delta)),
+// also for periodic impropers; harmonic impropers k d^2 with
+// d = ((phi - phi0 + pi) mod 2 pi) - pi)
 // and physics/cmap.py:316-376 (bicubic patch evaluation at angles mapped to
 // [0, 2 pi); phi from row atoms 0-3, psi from 1-4, system.py:99-102), and the
 // explicit 1-4 exception pairs of bonded.py:186-230.
@@ -75,7 +79,8 @@ __global__ void bonded_kernel(const BondedArgs a) {
       const double g = p.y * (r - p.x) / r;
       add_force(a, id.x, scale(d, -g));
       add_force(a, id.y, scale(d, g));
-      add_energy(a, id.x, PB2_TERM_BOND, 0.5 * p.y * (r - p.x) * (r - p.x));
+      add_energy(a, id.x, u < a.n_bond_plain ? PB2_TERM_BOND : PB2_TERM_UREY_BRADLEY,
+                 0.5 * p.y * (r - p.x) * (r - p.x));
       continue;
     }
     u -= a.n_bond;
@@ -110,12 +115,25 @@ __global__ void bonded_kernel(const BondedArgs a) {
       double phi;
       D3 g[4];
       dihedral(a, id.x, id.y, id.z, id.w, phi, g);
-      const double ang = p.x * phi - p.y;
-      const double dedphi = -p.z * p.x * sin(ang);
+      double e, dedphi;
+      int term;
+      if (p.w == kTorsHarmonic) {  // (k, phi0): k d^2, d wrapped into [-pi, pi)
+        const double pi = 3.141592653589793, two_pi = 6.283185307179586;
+        double d = phi - p.y + pi;
+        d = d - two_pi * floor(d / two_pi) - pi;
+        e = p.x * d * d;
+        dedphi = 2.0 * p.x * d;
+        term = PB2_TERM_IMPROPER;
+      } else {  // (n, phase, k): k (1 + cos(n phi - phase))
+        const double ang = p.x * phi - p.y;
+        e = p.z * (1.0 + cos(ang));
+        dedphi = -p.z * p.x * sin(ang);
+        term = p.w == kTorsImproper ? PB2_TERM_IMPROPER : PB2_TERM_DIHEDRAL;
+      }
       const int ids[4] = {id.x, id.y, id.z, id.w};
 #pragma unroll
       for (int c = 0; c < 4; ++c) add_force(a, ids[c], scale(g[c], -dedphi));
-      add_energy(a, id.x, PB2_TERM_DIHEDRAL, p.z * (1.0 + cos(ang)));
+      add_energy(a, id.x, term, e);
       continue;
     }
     u -= a.n_tors;

@@ -67,6 +67,13 @@ struct TileItem {
   int32_t sys, iblk, jb0, jb1;
 };
 
+// One row of the pair list: the even i-block iblk (with iblk + 1) of system
+// sys; its live j-blocks are stored from pair_list_j[jbase], room for
+// nblk - iblk of them.
+struct PlRow {
+  int32_t sys, iblk, jbase, pad;
+};
+
 // Exclusion masks of one (i-block, j-block) tile: per i row, bit c set when
 // (row, col c) is excluded (1-2/1-3) or 1-4 scaled.
 struct ExclRow {

@@ -132,17 +132,32 @@ struct pb2_batch {
   double *lb_rho = nullptr, *lb_sys = nullptr, *lb_energy = nullptr;  // lb_sys: e0, gd, t
   int32_t *lb_int = nullptr;  // count, head, flags
   double m_par_host[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // kMinNPar stage parameters
+  // pair list of the cutoff runs (pb2_pairlist.cu): rows, j-block lists,
+  // two item buffers and the control words; on when every pair term of the
+  // batch has a cutoff
+  bool pl_on = false;
+  float pl_reach2 = 0.f;
+  PlRow *pl_rows = nullptr;
+  int n_pl_rows = 0;
+  int32_t *pl_jlist = nullptr;
+  TileItem *pl_items[2] = {nullptr, nullptr};
+  size_t pl_item_cap = 0;
+  int32_t *pl_ctl = nullptr;
+  float4 *pl_ref = nullptr;
+  int grid_pl = 1;
   // neighbour list (allocated on first build)
   Dev nl;
   bool nl_built = false;
   int nl_capacity = 0;
   int nl_cells = 0;
   NlGrid *nl_grid = nullptr;
+  int32_t *nl_cell_base = nullptr, *nl_cell_budget = nullptr, *nl_cell_sys = nullptr;
   int *nl_atom_cell = nullptr, *nl_cell_count = nullptr, *nl_cell_start = nullptr;
   int *nl_cell_cursor = nullptr, *nl_cell_atoms = nullptr, *nl_rows = nullptr, *nl_counts = nullptr;
-  int *nl_max_disp2 = nullptr;
-  unsigned *nl_error = nullptr;
+  int32_t *nl_sys_moved = nullptr, *nl_ctl = nullptr;
   double *nl_xref = nullptr;
+  cudaEvent_t nl_ev[2] = {nullptr, nullptr};  // around the last build's launches
+  bool nl_timed = false;
 
   ~pb2_batch() {
     for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
@@ -151,6 +166,8 @@ struct pb2_batch {
     for (auto &e : ev)
       if (e) cudaEventDestroy(e);
     for (auto &e : ev_io)
+      if (e) cudaEventDestroy(e);
+    for (auto &e : nl_ev)
       if (e) cudaEventDestroy(e);
   }
 };

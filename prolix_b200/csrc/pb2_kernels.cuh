@@ -27,6 +27,27 @@ struct PairArgs {
   long long *energy;
   int32_t cut;              // any cutoff active
   int32_t *sched;           // (next item, finished warps) of this pass; zero between launches
+  // pair list (cutoff runs; NULL otherwise): items come from pl_items[pl_ctl[1]],
+  // pl_ctl[2 + pl_ctl[1]] of them, and an item's tiles t in [jb0, jb1) are
+  // the j-blocks pl_jlist[t]
+  const int32_t *pl_ctl;
+  const TileItem *pl_items0, *pl_items1;
+  const int32_t *pl_jlist;
+};
+// Pair-list control words (PlArgs::ctl)
+enum { PL_DIRTY = 0, PL_CUR = 1, PL_COUNT0 = 2, PL_COUNT1 = 3, PL_NEW = 4, PL_DONE = 5, PL_WORDS = 8 };
+struct PlArgs {
+  const SysInfo *sys;
+  const PlRow *rows;
+  int32_t n_rows;
+  const float4 *bbox;
+  const float4 *posq;
+  float4 *ref;           // positions at the last build (displacement reference)
+  int32_t *jlist;
+  TileItem *items0, *items1;
+  int32_t *ctl;
+  float reach2;          // (largest pair-term cutoff + skin)^2
+  int32_t seg;           // tiles per work item
 };
 struct FinalizeArgs {
   const SysInfo *sys;
@@ -54,6 +75,8 @@ struct Energy64Args {
   long long *born_acc;
   long long *energy;
 };
+// torsion-list entry kinds (BondedArgs::tors_par .w)
+constexpr double kTorsProper = 0.0, kTorsImproper = 1.0, kTorsHarmonic = 2.0;
 struct BondedArgs {
   const int32_t *atom_sys;
   const double *x, *y, *z;
@@ -61,7 +84,8 @@ struct BondedArgs {
   long long *energy;
   int32_t energy_mode;
   uint32_t terms;
-  int32_t n_bond;
+  int32_t n_bond;        // bonds [0, n_bond_plain), then Urey-Bradley springs
+  int32_t n_bond_plain;
   const int2 *bond_idx;
   const double2 *bond_par;
   int32_t n_angle;
@@ -69,7 +93,8 @@ struct BondedArgs {
   const double2 *angle_par;
   int32_t n_tors;
   const int4 *tors_idx;
-  const double4 *tors_par;
+  const double4 *tors_par;  // .w: kTorsProper (n, phase, k), kTorsImproper (n, phase, k),
+                            // kTorsHarmonic (k, phi0)
   int32_t n_cmap;
   const int32_t *cmap_idx;
   const double *cmap_coeff;
@@ -79,26 +104,34 @@ struct BondedArgs {
   const int2 *exc_idx;
   const double4 *exc_par;  // (k_coulomb * charge product, sigma, epsilon, 0)
 };
-struct NlGrid {        // per-system cell grid of the neighbour-list build
+struct NlGrid {        // per-system cell grid of the neighbour-list build (written on the device)
   float x0, y0, z0, inv_cell;
-  int32_t nx, ny, nz, cell_base;
-  int32_t n, atom_off;
-  float reach2;         // (cutoff + skin)^2
-  int32_t pad;
+  int32_t nx, ny, nz;
+  int32_t stencil;      // cells searched on each side: ceil(reach / cell edge)
 };
+// Neighbour-list control words (NlArgs::ctl)
+enum { NL_DIRTY = 0, NL_MAXCOUNT = 1, NL_CELLFULL = 2, NL_DONE = 3, NL_WORDS = 4 };
 struct NlArgs {
+  const SysInfo *sys;
   const int32_t *atom_sys;
-  const NlGrid *grid;
+  const float4 *bbox;          // current block boxes
+  NlGrid *grid;                // per system
+  const int32_t *cell_base;    // per system: first cell of its cell budget
+  const int32_t *cell_budget;  // per system: cells it may use
+  const int32_t *cell_sys;     // per cell: its system
   const float4 *posq;
   const double *x, *y, *z;
-  double *xref;         // positions at the last build, SoA (3, n_total)
+  double *xref;                // positions at the last build, SoA (3, n_total)
   int *atom_cell, *cell_count, *cell_start, *cell_cursor, *cell_atoms;
   int *rows, *counts;
+  int32_t *sys_moved;          // per system: moved more than skin / 2 (the last check)
+  int32_t *ctl;                // NL_* words; the build kernels run only while ctl[NL_DIRTY] != 0
   int32_t capacity, n_total, n_cells, n_sys;
   uint32_t *status;
-  unsigned *error;
-  int *max_disp2;
+  float reach;                 // cutoff + skin
 };
+// The build (every kernel returns at once unless ctl[NL_DIRTY] is set; the
+// last one clears it) and the half-skin test that sets it.
 cudaError_t nl_launch_build(const NlArgs &a, cudaStream_t st);
 cudaError_t nl_launch_disp(const NlArgs &a, cudaStream_t st);
 struct IntArgs {
@@ -177,8 +210,14 @@ cudaError_t launch_energy64(int pass, const Energy64Args &a, int grid, cudaStrea
 cudaError_t launch_born_finalize(const FinalizeArgs &a, cudaStream_t st);
 int tile_kernel_occupancy(int pass, bool cut);
 int tile_kernel_warps(int pass);  // warps per block of a pair pass
+// Bounding boxes of every 32-atom block.  With pl_ref / pl_ctl set, also
+// flags the pair list for a rebuild (pl_ctl[PL_DIRTY]) when an atom moved
+// more than half the skin since the list was built.
 cudaError_t launch_bbox(const SysInfo *sys, const int32_t *blk_sys, const float4 *posq, float4 *bbox,
-                        int n_blocks, cudaStream_t st);
+                        int n_blocks, cudaStream_t st, const float4 *pl_ref = nullptr,
+                        int32_t *pl_ctl = nullptr);
+// Rebuild the pair list when flagged (one launch; returns at once when clean).
+cudaError_t launch_pl_update(const PlArgs &a, int grid, cudaStream_t st);
 cudaError_t launch_bonded(const BondedArgs &a, int grid_cap, cudaStream_t st);
 cudaError_t launch_step(const IntArgs &a, cudaStream_t st);
 cudaError_t launch_finish(const IntArgs &a, cudaStream_t st);

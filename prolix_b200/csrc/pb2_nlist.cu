@@ -8,15 +8,26 @@
 // atoms within cutoff + skin (both (i, j) and (j, i) present), padded with
 // the sentinel n_atoms of its system; capacity K per atom.
 //
-// Build, all systems of the batch at once:
-//   1. each atom's cell on a per-system grid of cells of edge >= cutoff +
-//      skin (atoms outside the grid are clamped to edge cells, which keeps
-//      every pair within reach in adjacent cells); counts per cell;
-//   2. exclusive scan of the counts; 3. scatter atoms to their cells;
-//   4. sort each cell by atom index (so list order is deterministic);
-//   5. one warp per atom scans the 27 neighbouring cells in a fixed order
-//      and compacts the hits with a ballot into its row.
-// The HBM traffic is dominated by step 5's row writes (4 B per entry).
+// Everything runs on the device, all systems of the batch at once, as a
+// fixed sequence of launches that needs no host decision:
+//   0. (check) each atom's displacement since the last build against
+//      skin/2 sets the rebuild flag and its system's moved flag;
+//   1. per system, a cell grid over the current block bounding boxes, cell
+//      edge reach/2 (searched two cells out), widened where the system
+//      would need more cells than its budget (2 per atom, at least 64);
+//   2. each atom's cell and the counts per cell;
+//   3. per system, an exclusive scan of its cells' counts;
+//   4. atoms scattered to their cells; 5. each cell sorted by atom index
+//      (list order is deterministic);
+//   6. one thread block per cell: the cell's atoms test, from shared memory,
+//      the atoms of the surrounding cells, each thread writing its atom's
+//      row; rows beyond the capacity only count (the largest count and an
+//      overflow bit are recorded for the host's next visit);
+//   7. the positions become the new displacement reference; the last block
+//      clears the flag.
+// Each kernel returns at once while the flag is clear, so a check that
+// finds nothing to do costs one launch per kernel and no host round trip.
+// The HBM traffic is dominated by step 6's row writes (4 B per entry).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -30,8 +41,76 @@
 namespace pb2 {
 
 constexpr int kMaxCellSort = 4096;  // atoms per cell handled by the in-block sort
+constexpr int kRowsThreads = 128;   // threads per cell block of the row pass
 
+__device__ __forceinline__ bool nl_dirty(const NlArgs &a) { return *(volatile int32_t *)&a.ctl[NL_DIRTY] != 0; }
+
+// 0. displacement since the last build (FP64 state) against skin/2
+__global__ void nl_disp_kernel(const NlArgs a) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_total; i += gridDim.x * blockDim.x) {
+    const int s = a.atom_sys[i];
+    const double dx = a.x[i] - a.xref[i], dy = a.y[i] - a.xref[a.n_total + i],
+                 dz = a.z[i] - a.xref[2 * (size_t)a.n_total + i];
+    if (dx * dx + dy * dy + dz * dz > a.sys[s].skin_half2) {
+      a.sys_moved[s] = 1;
+      a.ctl[NL_DIRTY] = 1;
+    }
+  }
+}
+
+// 1. per-system grid, one warp per system; also clears the system's cells
+__global__ void nl_grid_kernel(const NlArgs a) {
+  if (!nl_dirty(a)) return;
+  const int lane = threadIdx.x & 31;
+  const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int nw = (int)((gridDim.x * blockDim.x) >> 5);
+  for (int s = w; s < a.n_sys; s += nw) {
+    const SysInfo &S = a.sys[s];
+    float lo[3] = {1e30f, 1e30f, 1e30f}, hi[3] = {-1e30f, -1e30f, -1e30f};
+    for (int k = lane; k < S.nblk; k += 32) {
+      const float4 l = a.bbox[2 * (S.blk_base + k)], h = a.bbox[2 * (S.blk_base + k) + 1];
+      lo[0] = fminf(lo[0], l.x); lo[1] = fminf(lo[1], l.y); lo[2] = fminf(lo[2], l.z);
+      hi[0] = fmaxf(hi[0], h.x); hi[1] = fmaxf(hi[1], h.y); hi[2] = fmaxf(hi[2], h.z);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        lo[c] = fminf(lo[c], __shfl_xor_sync(kFull, lo[c], o));
+        hi[c] = fmaxf(hi[c], __shfl_xor_sync(kFull, hi[c], o));
+      }
+    const int budget = a.cell_budget[s];
+    // edge reach/2; widened until the grid fits the budget
+    double edge = 0.5 * (double)a.reach;
+    int n[3];
+    for (int it = 0; it < 64; ++it) {
+      long long cells = 1;
+      for (int c = 0; c < 3; ++c) {
+        n[c] = max(1, (int)ceil(((double)hi[c] - (double)lo[c]) / edge + 1e-6));
+        cells *= n[c];
+      }
+      if (cells <= budget) break;
+      edge *= fmax(1.01, cbrt((double)cells / budget));
+    }
+    if (lane == 0) {
+      NlGrid g;
+      g.x0 = lo[0]; g.y0 = lo[1]; g.z0 = lo[2];
+      g.inv_cell = (float)(1.0 / edge);
+      g.nx = n[0]; g.ny = n[1]; g.nz = n[2];
+      g.stencil = (int)ceil((double)a.reach / edge - 1e-9);
+      a.grid[s] = g;
+    }
+    const int base = a.cell_base[s];
+    for (int c = lane; c < budget; c += 32) {
+      a.cell_count[base + c] = 0;
+      a.cell_cursor[base + c] = 0;
+    }
+  }
+}
+
+// 2. cell of each atom (clamped into the grid) and the counts
 __global__ void nl_assign_kernel(const NlArgs a) {
+  if (!nl_dirty(a)) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_total; i += gridDim.x * blockDim.x) {
     const int s = a.atom_sys[i];
     const NlGrid g = a.grid[s];
@@ -42,42 +121,49 @@ __global__ void nl_assign_kernel(const NlArgs a) {
     cx = min(max(cx, 0), g.nx - 1);
     cy = min(max(cy, 0), g.ny - 1);
     cz = min(max(cz, 0), g.nz - 1);
-    const int c = g.cell_base + (cz * g.ny + cy) * g.nx + cx;
+    const int c = a.cell_base[s] + (cz * g.ny + cy) * g.nx + cx;
     a.atom_cell[i] = c;
     atomicAdd(&a.cell_count[c], 1);
   }
 }
 
-// Exclusive scan of cell_count into cell_start (single block, chunked);
-// cell_start[n_cells] = total.  Also clears the scatter cursors.
+// 3. exclusive scan of a system's cell counts, one block per system; cells
+// past the grid (unused budget) start at the system's end
 __global__ void nl_scan_kernel(const NlArgs a) {
+  if (!nl_dirty(a)) return;
   __shared__ int buf[1024];
   __shared__ int carry;
-  if (threadIdx.x == 0) carry = 0;
-  __syncthreads();
-  for (int base = 0; base < a.n_cells; base += 1024) {
-    const int i = base + threadIdx.x;
-    const int v = i < a.n_cells ? a.cell_count[i] : 0;
-    buf[threadIdx.x] = v;
+  for (int s = blockIdx.x; s < a.n_sys; s += gridDim.x) {
+    const SysInfo &S = a.sys[s];
+    const NlGrid g = a.grid[s];
+    const int base = a.cell_base[s], budget = a.cell_budget[s];
+    const int used = g.nx * g.ny * g.nz;
+    if (threadIdx.x == 0) carry = S.off;
     __syncthreads();
-    for (int o = 1; o < 1024; o <<= 1) {
-      const int t = threadIdx.x >= o ? buf[threadIdx.x - o] : 0;
+    for (int c0 = 0; c0 < used; c0 += 1024) {
+      const int c = c0 + threadIdx.x;
+      const int v = c < used ? a.cell_count[base + c] : 0;
+      buf[threadIdx.x] = v;
       __syncthreads();
-      buf[threadIdx.x] += t;
+      for (int o = 1; o < 1024; o <<= 1) {
+        const int t = threadIdx.x >= o ? buf[threadIdx.x - o] : 0;
+        __syncthreads();
+        buf[threadIdx.x] += t;
+        __syncthreads();
+      }
+      if (c < used) a.cell_start[base + c] = carry + buf[threadIdx.x] - v;
+      __syncthreads();
+      if (threadIdx.x == 1023) carry += buf[1023];
       __syncthreads();
     }
-    if (i < a.n_cells) {
-      a.cell_start[i] = carry + buf[threadIdx.x] - v;
-      a.cell_cursor[i] = 0;
-    }
-    __syncthreads();
-    if (threadIdx.x == 1023) carry += buf[1023];
+    for (int c = used + threadIdx.x; c <= budget; c += blockDim.x) a.cell_start[base + c] = S.off + S.n;
     __syncthreads();
   }
-  if (threadIdx.x == 0) a.cell_start[a.n_cells] = carry;
 }
 
+// 4. scatter atoms to their cells
 __global__ void nl_scatter_kernel(const NlArgs a) {
+  if (!nl_dirty(a)) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_total; i += gridDim.x * blockDim.x) {
     const int c = a.atom_cell[i];
     const int slot = atomicAdd(&a.cell_cursor[c], 1);
@@ -85,15 +171,16 @@ __global__ void nl_scatter_kernel(const NlArgs a) {
   }
 }
 
-// One block per cell: bitonic sort of the cell's atom indices in shared memory.
+// 5. one block per cell: bitonic sort of the cell's atom indices in shared memory
 __global__ void nl_sort_kernel(const NlArgs a) {
+  if (!nl_dirty(a)) return;
   __shared__ int v[kMaxCellSort];
   for (int c = blockIdx.x; c < a.n_cells; c += gridDim.x) {
     const int start = a.cell_start[c];
-    const int cnt = a.cell_start[c + 1] - start;
+    const int cnt = a.cell_count[c];
     if (cnt <= 1) continue;
     if (cnt > kMaxCellSort) {
-      if (threadIdx.x == 0) atomicOr(a.error, 1u);
+      if (threadIdx.x == 0) atomicOr(&a.ctl[NL_CELLFULL], 1);
       continue;
     }
     int m = 1;
@@ -117,97 +204,109 @@ __global__ void nl_sort_kernel(const NlArgs a) {
   }
 }
 
-// One warp per atom: scan the 27 cells around its cell, keep j != i within
-// reach, write local indices; count beyond the capacity only counts.
-__global__ void nl_rows_kernel(const NlArgs a) {
-  const int lane = threadIdx.x & 31;
-  const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  const int nw = (int)((gridDim.x * blockDim.x) >> 5);
-  for (int i = w; i < a.n_total; i += nw) {
-    const int s = a.atom_sys[i];
+// 6. rows: one block per cell, one thread per atom of the cell (in chunks);
+// the surrounding cells' atoms pass through shared memory in a fixed order
+__global__ void __launch_bounds__(kRowsThreads) nl_rows_kernel(const NlArgs a) {
+  if (!nl_dirty(a)) return;
+  __shared__ float4 sp[kRowsThreads];
+  __shared__ int sj[kRowsThreads];
+  for (int c = blockIdx.x; c < a.n_cells; c += gridDim.x) {
+    const int ci0 = a.cell_start[c], nci = a.cell_count[c];
+    if (nci == 0) continue;  // block-uniform
+    const int s = a.cell_sys[c];
+    const SysInfo &S = a.sys[s];
     const NlGrid g = a.grid[s];
-    const int off = g.atom_off;
-    const float4 p = a.posq[i];
-    const int lc = a.atom_cell[i] - g.cell_base;
+    const int lc = c - a.cell_base[s];
     const int cx = lc % g.nx, cy = (lc / g.nx) % g.ny, cz = lc / (g.nx * g.ny);
-    int count = 0;
-    int *row = a.rows + (size_t)i * a.capacity;
-    for (int dz = -1; dz <= 1; ++dz) {
-      const int z = cz + dz;
-      if (z < 0 || z >= g.nz) continue;
-      for (int dy = -1; dy <= 1; ++dy) {
-        const int y = cy + dy;
-        if (y < 0 || y >= g.ny) continue;
-        for (int dx = -1; dx <= 1; ++dx) {
-          const int x = cx + dx;
-          if (x < 0 || x >= g.nx) continue;
-          const int c = g.cell_base + (z * g.ny + y) * g.nx + x;
-          const int st = a.cell_start[c], en = a.cell_start[c + 1];
-          for (int b = st; b < en; b += 32) {
-            const int k = b + lane;
-            int j = -1;
-            bool hit = false;
-            if (k < en) {
-              j = a.cell_atoms[k];
-              if (j != i) {
-                const float4 q = a.posq[j];
-                const float ex = p.x - q.x, ey = p.y - q.y, ez = p.z - q.z;
-                hit = fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < g.reach2;
+    const float reach2 = a.reach * a.reach;
+    const int R = g.stencil;
+    for (int i0 = 0; i0 < nci; i0 += kRowsThreads) {
+      const int k = i0 + threadIdx.x;
+      const bool has_i = k < nci;
+      const int i = has_i ? a.cell_atoms[ci0 + k] : -1;
+      const float4 p = has_i ? a.posq[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+      int *row = has_i ? a.rows + (size_t)i * a.capacity : nullptr;
+      int count = 0;
+      for (int dz = -R; dz <= R; ++dz) {
+        const int z = cz + dz;
+        if (z < 0 || z >= g.nz) continue;
+        for (int dy = -R; dy <= R; ++dy) {
+          const int y = cy + dy;
+          if (y < 0 || y >= g.ny) continue;
+          for (int dx = -R; dx <= R; ++dx) {
+            const int x = cx + dx;
+            if (x < 0 || x >= g.nx) continue;
+            const int nc = a.cell_base[s] + (z * g.ny + y) * g.nx + x;
+            const int st = a.cell_start[nc], cnt = a.cell_count[nc];
+            for (int b = 0; b < cnt; b += kRowsThreads) {
+              __syncthreads();  // the previous chunk has been read
+              const int m = min(kRowsThreads, cnt - b);
+              if ((int)threadIdx.x < m) {
+                const int j = a.cell_atoms[st + b + threadIdx.x];
+                sj[threadIdx.x] = j;
+                sp[threadIdx.x] = a.posq[j];
+              }
+              __syncthreads();
+              if (has_i) {
+                for (int t = 0; t < m; ++t) {
+                  const float4 q = sp[t];
+                  const float ex = p.x - q.x, ey = p.y - q.y, ez = p.z - q.z;
+                  const int j = sj[t];
+                  if (fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < reach2 && j != i) {
+                    if (count < a.capacity) row[count] = j - S.off;
+                    ++count;
+                  }
+                }
               }
             }
-            const unsigned m = __ballot_sync(kFull, hit);
-            if (hit) {
-              const int slot = count + __popc(m & ((1u << lane) - 1u));
-              if (slot < a.capacity) row[slot] = j - off;
-            }
-            count += __popc(m);
           }
         }
       }
-    }
-    for (int t = count + lane; t < a.capacity; t += 32) row[t] = g.n;  // sentinel
-    if (lane == 0) {
-      a.counts[i] = count;
-      if (count > a.capacity) atomicOr(&a.status[s], (uint32_t)PB2_STATUS_NLOVERFLOW);
+      if (has_i) {
+        for (int t = count; t < a.capacity; ++t) row[t] = S.n;  // sentinel
+        a.counts[i] = count;
+        if (count > a.capacity) {
+          atomicOr(&a.status[s], (uint32_t)PB2_STATUS_NLOVERFLOW);
+        }
+        atomicMax(&a.ctl[NL_MAXCOUNT], count);
+      }
     }
   }
 }
 
-// Largest squared displacement per system since the last build (FP64).
-__global__ void nl_disp_kernel(const NlArgs a) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_total; i += gridDim.x * blockDim.x) {
-    const double dx = a.x[i] - a.xref[i], dy = a.y[i] - a.xref[a.n_total + i],
-                 dz = a.z[i] - a.xref[2 * (size_t)a.n_total + i];
-    const float d2 = (float)(dx * dx + dy * dy + dz * dz);
-    atomicMax(&a.max_disp2[a.atom_sys[i]], __float_as_int(d2));  // d2 >= 0: int order = float order
-  }
-}
-
+// 7. new displacement reference; the last block clears the rebuild flag
 __global__ void nl_ref_kernel(const NlArgs a) {
+  if (!nl_dirty(a)) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_total; i += gridDim.x * blockDim.x) {
     a.xref[i] = a.x[i];
     a.xref[a.n_total + i] = a.y[i];
     a.xref[2 * (size_t)a.n_total + i] = a.z[i];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&a.ctl[NL_DONE], 1) == (int)gridDim.x - 1) {
+      a.ctl[NL_DONE] = 0;
+      a.ctl[NL_DIRTY] = 0;
+      __threadfence();
+    }
   }
 }
 
 static int grid_for(int n, int per) { return std::max(1, std::min((n + per - 1) / per, 65535)); }
 
 cudaError_t nl_launch_build(const NlArgs &a, cudaStream_t st) {
-  cudaError_t e;
-  if ((e = cudaMemsetAsync(a.cell_count, 0, (size_t)a.n_cells * sizeof(int), st)) != cudaSuccess) return e;
+  nl_grid_kernel<<<grid_for(a.n_sys, 8), 256, 0, st>>>(a);
   nl_assign_kernel<<<grid_for(a.n_total, 256), 256, 0, st>>>(a);
-  nl_scan_kernel<<<1, 1024, 0, st>>>(a);
+  nl_scan_kernel<<<std::min(a.n_sys, 65535), 1024, 0, st>>>(a);
   nl_scatter_kernel<<<grid_for(a.n_total, 256), 256, 0, st>>>(a);
   nl_sort_kernel<<<grid_for(a.n_cells, 1), 256, 0, st>>>(a);
-  nl_rows_kernel<<<grid_for(a.n_total, 8), 256, 0, st>>>(a);
+  nl_rows_kernel<<<grid_for(a.n_cells, 1), kRowsThreads, 0, st>>>(a);
   nl_ref_kernel<<<grid_for(a.n_total, 256), 256, 0, st>>>(a);
   return cudaGetLastError();
 }
 
 cudaError_t nl_launch_disp(const NlArgs &a, cudaStream_t st) {
-  cudaError_t e;
-  if ((e = cudaMemsetAsync(a.max_disp2, 0, (size_t)a.n_sys * sizeof(int), st)) != cudaSuccess) return e;
   nl_disp_kernel<<<grid_for(a.n_total, 256), 256, 0, st>>>(a);
   return cudaGetLastError();
 }
@@ -224,8 +323,13 @@ static double nl_reach(const pb2_batch *b) {
 
 static NlArgs nl_args(pb2_batch *b) {
   NlArgs a;
+  a.sys = b->sys;
   a.atom_sys = b->atom_sys;
+  a.bbox = b->bbox;
   a.grid = b->nl_grid;
+  a.cell_base = b->nl_cell_base;
+  a.cell_budget = b->nl_cell_budget;
+  a.cell_sys = b->nl_cell_sys;
   a.posq = b->posq;
   a.x = b->x; a.y = b->y; a.z = b->z;
   a.xref = b->nl_xref;
@@ -236,79 +340,55 @@ static NlArgs nl_args(pb2_batch *b) {
   a.cell_atoms = b->nl_cell_atoms;
   a.rows = b->nl_rows;
   a.counts = b->nl_counts;
+  a.sys_moved = b->nl_sys_moved;
+  a.ctl = b->nl_ctl;
   a.capacity = b->nl_capacity;
   a.n_total = b->n_total;
   a.n_cells = b->nl_cells;
   a.n_sys = b->n_sys;
   a.status = b->status;
-  a.error = b->nl_error;
-  a.max_disp2 = b->nl_max_disp2;
+  a.reach = (float)nl_reach(b);
   return a;
 }
 
-// Per-system grids from the current block bounding boxes; (re)allocates
-// the cell arrays when the total cell count grows.
-static int nl_setup(pb2_batch *b, cudaStream_t st) {
+// Device arrays of the list, allocated once: per-system cell budgets of
+// max(64, 2 n) cells, the cell arrays over all budgets, the control words.
+static int nl_alloc(pb2_batch *b) {
   pb2_ctx *ctx = b->ctx;
-  const double reach = nl_reach(b);
-  CUDA_TRY(ctx, launch_posq(int_args_for_nl(b), st));
-  CUDA_TRY(ctx, launch_bbox(b->sys, b->blk_sys, b->posq, b->bbox, b->n_blocks, st));
-  std::vector<float4> bb(2 * (size_t)b->n_blocks);
-  CUDA_TRY(ctx, cudaMemcpyAsync(bb.data(), b->bbox, bb.size() * sizeof(float4), cudaMemcpyDeviceToHost, st));
-  CUDA_TRY(ctx, cudaStreamSynchronize(st));
-  std::vector<NlGrid> grids(b->n_sys);
-  int cells = 0;
+  if (b->nl_grid) return PB2_OK;
+  std::vector<int32_t> base(b->n_sys), budget(b->n_sys), cell_sys;
+  long long cells = 0;
   for (int s = 0; s < b->n_sys; ++s) {
-    const SysInfo &S = b->sys_host[s];
-    float lo[3] = {1e30f, 1e30f, 1e30f}, hi[3] = {-1e30f, -1e30f, -1e30f};
-    for (int k = 0; k < S.nblk; ++k) {
-      const float4 l = bb[2 * (size_t)(S.blk_base + k)], h = bb[2 * (size_t)(S.blk_base + k) + 1];
-      lo[0] = std::min(lo[0], l.x); lo[1] = std::min(lo[1], l.y); lo[2] = std::min(lo[2], l.z);
-      hi[0] = std::max(hi[0], h.x); hi[1] = std::max(hi[1], h.y); hi[2] = std::max(hi[2], h.z);
-    }
-    double cell = reach;
-    const double ext = std::max({hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]}) + 2.0 * reach;
-    if (ext / cell > 128.0) cell = ext / 128.0;
-    NlGrid &g = grids[s];
-    g.x0 = lo[0] - (float)reach; g.y0 = lo[1] - (float)reach; g.z0 = lo[2] - (float)reach;
-    g.inv_cell = (float)(1.0 / cell);
-    g.nx = std::max(1, (int)std::ceil((hi[0] - lo[0] + 2.0 * reach) / cell));
-    g.ny = std::max(1, (int)std::ceil((hi[1] - lo[1] + 2.0 * reach) / cell));
-    g.nz = std::max(1, (int)std::ceil((hi[2] - lo[2] + 2.0 * reach) / cell));
-    g.cell_base = cells;
-    g.n = S.n;
-    g.atom_off = S.off;
-    g.reach2 = (float)(reach * reach);
-    g.pad = 0;
-    cells += g.nx * g.ny * g.nz;
+    base[s] = (int32_t)cells;
+    budget[s] = std::max(64, 2 * b->sys_host[s].n);
+    cells += budget[s];
+    if (cells > INT32_MAX / 2) return fail(ctx, PB2_EINVAL, "neighbour-list cell budget too large");
+    cell_sys.insert(cell_sys.end(), budget[s], s);
   }
   Dev &D = b->nl;
-  if (!b->nl_grid) {
-    b->nl_grid = D.alloc<NlGrid>(b->n_sys);
-    b->nl_atom_cell = D.alloc<int>(b->n_total);
-    b->nl_counts = D.alloc<int>(b->n_total);
-    b->nl_xref = D.alloc<double>(3 * (size_t)b->n_total);
-    b->nl_max_disp2 = D.alloc<int>(b->n_sys);
-    b->nl_error = D.alloc<unsigned>(1);
-    b->nl_cell_atoms = D.alloc<int>(b->n_total);
-    if (!b->nl_grid || !b->nl_atom_cell || !b->nl_counts || !b->nl_xref || !b->nl_max_disp2 ||
-        !b->nl_error || !b->nl_cell_atoms)
-      return fail(ctx, PB2_ENOMEM, "neighbour-list allocation failed");
-    CUDA_TRY(ctx, cudaMemsetAsync(b->nl_error, 0, sizeof(unsigned), st));
-  }
-  if (cells > b->nl_cells) {
-    D.release(b->nl_cell_count);
-    D.release(b->nl_cell_start);
-    D.release(b->nl_cell_cursor);
-    b->nl_cell_count = D.alloc<int>(cells);
-    b->nl_cell_start = D.alloc<int>(cells + 1);
-    b->nl_cell_cursor = D.alloc<int>(cells);
-    if (!b->nl_cell_count || !b->nl_cell_start || !b->nl_cell_cursor)
-      return fail(ctx, PB2_ENOMEM, "neighbour-list cell allocation failed");
-  }
-  b->nl_cells = cells;
-  CUDA_TRY(ctx, cudaMemcpyAsync(b->nl_grid, grids.data(), grids.size() * sizeof(NlGrid),
-                                cudaMemcpyHostToDevice, st));
+  b->nl_cells = (int)cells;
+  b->nl_grid = D.alloc<NlGrid>(b->n_sys);
+  b->nl_cell_base = D.alloc<int32_t>(b->n_sys);
+  b->nl_cell_budget = D.alloc<int32_t>(b->n_sys);
+  b->nl_cell_sys = D.alloc<int32_t>(cells);
+  b->nl_cell_count = D.alloc<int>(cells);
+  b->nl_cell_start = D.alloc<int>(cells + 1);
+  b->nl_cell_cursor = D.alloc<int>(cells);
+  b->nl_atom_cell = D.alloc<int>(b->n_total);
+  b->nl_cell_atoms = D.alloc<int>(b->n_total);
+  b->nl_counts = D.alloc<int>(b->n_total);
+  b->nl_xref = D.alloc<double>(3 * (size_t)b->n_total);
+  b->nl_sys_moved = D.alloc<int32_t>(b->n_sys);
+  b->nl_ctl = D.alloc<int32_t>(NL_WORDS);
+  for (void *p : D.ptrs)
+    if (!p) return fail(ctx, PB2_ENOMEM, "neighbour-list allocation failed");
+  CUDA_TRY(ctx, cudaMemcpy(b->nl_cell_base, base.data(), base.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  CUDA_TRY(ctx, cudaMemcpy(b->nl_cell_budget, budget.data(), budget.size() * sizeof(int32_t),
+                           cudaMemcpyHostToDevice));
+  CUDA_TRY(ctx, cudaMemcpy(b->nl_cell_sys, cell_sys.data(), cell_sys.size() * sizeof(int32_t),
+                           cudaMemcpyHostToDevice));
+  CUDA_TRY(ctx, cudaMemset(b->nl_ctl, 0, NL_WORDS * sizeof(int32_t)));
+  CUDA_TRY(ctx, cudaMemset(b->nl_sys_moved, 0, b->n_sys * sizeof(int32_t)));
   return PB2_OK;
 }
 
@@ -321,15 +401,51 @@ static int nl_alloc_rows(pb2_batch *b, int capacity) {
   return PB2_OK;
 }
 
-static int nl_max_count(pb2_batch *b, cudaStream_t st, int *out) {
+// Current positions as the float32 pair-kernel layout and block boxes (the
+// grid kernel reads the boxes).
+static int nl_prepare(pb2_batch *b, cudaStream_t st) {
   pb2_ctx *ctx = b->ctx;
-  std::vector<int> c(b->n_total);
-  CUDA_TRY(ctx, cudaMemcpyAsync(c.data(), b->nl_counts, c.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
-  unsigned err = 0;
-  CUDA_TRY(ctx, cudaMemcpyAsync(&err, b->nl_error, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(ctx, launch_posq(int_args_for_nl(b), st));
+  CUDA_TRY(ctx, launch_bbox(b->sys, b->blk_sys, b->posq, b->bbox, b->n_blocks, st));
+  return PB2_OK;
+}
+
+// Enqueue a build of every system (no host wait), timed with events.
+static int nl_enqueue_build(pb2_batch *b, cudaStream_t st, bool force) {
+  pb2_ctx *ctx = b->ctx;
+  if (force) CUDA_TRY(ctx, cudaMemsetAsync(b->nl_ctl + NL_DIRTY, 1, 1, st));  // any nonzero byte
+  CUDA_TRY(ctx, cudaMemsetAsync(b->nl_ctl + NL_MAXCOUNT, 0, sizeof(int32_t), st));
+  CUDA_TRY(ctx, cudaEventRecord(b->nl_ev[0], st));
+  CUDA_TRY(ctx, nl_launch_build(nl_args(b), st));
+  CUDA_TRY(ctx, cudaEventRecord(b->nl_ev[1], st));
+  b->nl_timed = true;
+  return PB2_OK;
+}
+
+// Host visit: the largest row length of the last build; grow the rows (and
+// rebuild) when they were too short, unless the capacity is fixed.
+static int nl_settle(pb2_batch *b, cudaStream_t st) {
+  pb2_ctx *ctx = b->ctx;
+  int32_t ctl[NL_WORDS];
+  CUDA_TRY(ctx, cudaMemcpyAsync(ctl, b->nl_ctl, sizeof ctl, cudaMemcpyDeviceToHost, st));
   CUDA_TRY(ctx, cudaStreamSynchronize(st));
-  if (err) return fail(ctx, PB2_ENLOVERFLOW, "a neighbour-list cell holds more than 4096 atoms");
-  *out = c.empty() ? 0 : *std::max_element(c.begin(), c.end());
+  if (ctl[NL_CELLFULL]) return fail(ctx, PB2_ENLOVERFLOW, "a neighbour-list cell holds more than 4096 atoms");
+  const int maxc = ctl[NL_MAXCOUNT];
+  if (maxc <= b->nl_capacity) return PB2_OK;
+  const int fixed = b->params.nl_capacity;
+  if (fixed > 0) {
+    char buf[160];
+    snprintf(buf, sizeof buf, "neighbour-list capacity %d exceeded (an atom has %d neighbours)", fixed, maxc);
+    return fail(ctx, PB2_ENLOVERFLOW, buf);
+  }
+  int rc = nl_alloc_rows(b, ((maxc + maxc / 4 + 8 + 31) / 32) * 32);
+  if (rc) return rc;
+  // the overflow pass set the status bit; the rebuild supersedes it
+  CUDA_TRY(ctx, cudaMemsetAsync(b->status, 0, b->n_sys * sizeof(uint32_t), st));
+  if ((rc = nl_prepare(b, st)) || (rc = nl_enqueue_build(b, st, true))) return rc;
+  CUDA_TRY(ctx, cudaMemcpyAsync(ctl, b->nl_ctl, sizeof ctl, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  if (ctl[NL_MAXCOUNT] > b->nl_capacity) return fail(ctx, PB2_ENLOVERFLOW, "neighbour-list capacity did not settle");
   return PB2_OK;
 }
 
@@ -337,34 +453,13 @@ static int nl_build_all(pb2_batch *b, cudaStream_t st) {
   pb2_ctx *ctx = b->ctx;
   if (!(b->params.cutoff > 0.0 || b->params.gb_cutoff > 0.0))
     return fail(ctx, PB2_EINVAL, "a neighbour list needs cutoff > 0 (or gb_cutoff > 0)");
-  int rc = nl_setup(b, st);
+  int rc = nl_alloc(b);
   if (rc) return rc;
-  const int fixed = b->params.nl_capacity;
-  if (!b->nl_rows) {
-    rc = nl_alloc_rows(b, fixed > 0 ? fixed : 0);
-    if (rc) return rc;
-  }
-  for (int attempt = 0; attempt < 4; ++attempt) {
-    CUDA_TRY(ctx, nl_launch_build(nl_args(b), st));
-    int maxc = 0;
-    rc = nl_max_count(b, st, &maxc);
-    if (rc) return rc;
-    if (maxc <= b->nl_capacity) {
-      b->nl_built = true;
-      return PB2_OK;
-    }
-    if (fixed > 0) {
-      char buf[160];
-      snprintf(buf, sizeof buf, "neighbour-list capacity %d exceeded (an atom has %d neighbours)",
-               fixed, maxc);
-      return fail(ctx, PB2_ENLOVERFLOW, buf);
-    }
-    rc = nl_alloc_rows(b, ((maxc + maxc / 4 + 8 + 31) / 32) * 32);
-    if (rc) return rc;
-    // the overflow pass set the status bit; the rebuild supersedes it
-    CUDA_TRY(ctx, cudaMemsetAsync(b->status, 0, b->n_sys * sizeof(uint32_t), st));
-  }
-  return fail(ctx, PB2_ENLOVERFLOW, "neighbour-list capacity did not converge");
+  if (!b->nl_rows && (rc = nl_alloc_rows(b, std::max(b->params.nl_capacity, 0)))) return rc;
+  if ((rc = nl_prepare(b, st)) || (rc = nl_enqueue_build(b, st, true))) return rc;
+  if ((rc = nl_settle(b, st))) return rc;
+  b->nl_built = true;
+  return PB2_OK;
 }
 
 extern "C" int pb2_nl_build(pb2_batch *b, void *stream) {
@@ -377,26 +472,27 @@ extern "C" int pb2_nl_check(pb2_batch *b, int32_t *rebuilt, void *stream) {
   if (!b) return PB2_EINVAL;
   pb2_ctx *ctx = b->ctx;
   cudaStream_t st = (cudaStream_t)stream;
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   if (rebuilt) *rebuilt = 0;
   if (!b->nl_built) {
     const int rc = nl_build_all(b, st);
     if (rc == PB2_OK && rebuilt) *rebuilt = b->n_sys;
     return rc;
   }
+  int rc;
+  CUDA_TRY(ctx, cudaMemsetAsync(b->nl_sys_moved, 0, b->n_sys * sizeof(int32_t), st));
+  if ((rc = nl_prepare(b, st))) return rc;
   CUDA_TRY(ctx, nl_launch_disp(nl_args(b), st));
-  std::vector<int> d(b->n_sys);
-  CUDA_TRY(ctx, cudaMemcpyAsync(d.data(), b->nl_max_disp2, d.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
-  CUDA_TRY(ctx, cudaStreamSynchronize(st));
-  int moved = 0;
-  for (int s = 0; s < b->n_sys; ++s) {
-    float v;
-    std::memcpy(&v, &d[s], sizeof v);
-    if ((double)v > b->sys_host[s].skin_half2) ++moved;
-  }
-  if (moved == 0) return PB2_OK;
-  const int rc = nl_build_all(b, st);
-  if (rc == PB2_OK && rebuilt) *rebuilt = moved;
-  return rc;
+  if ((rc = nl_enqueue_build(b, st, false))) return rc;  // runs only if the check set the flag
+  if (!rebuilt) return PB2_OK;                             // asynchronous: overflow seen at the next visit
+  std::vector<int32_t> moved(b->n_sys);
+  CUDA_TRY(ctx, cudaMemcpyAsync(moved.data(), b->nl_sys_moved, moved.size() * sizeof(int32_t),
+                                cudaMemcpyDeviceToHost, st));
+  if ((rc = nl_settle(b, st))) return rc;
+  int n = 0;
+  for (int v : moved) n += v != 0;
+  *rebuilt = n;
+  return PB2_OK;
 }
 
 extern "C" int pb2_nl_capacity(const pb2_batch *b, int32_t *capacity) {
@@ -405,11 +501,24 @@ extern "C" int pb2_nl_capacity(const pb2_batch *b, int32_t *capacity) {
   return PB2_OK;
 }
 
+extern "C" int pb2_nl_last_build_ms(pb2_batch *b, double *ms) {
+  if (!b || !ms) return PB2_EINVAL;
+  pb2_ctx *ctx = b->ctx;
+  if (!b->nl_timed) return fail(ctx, PB2_EINVAL, "no neighbour-list build yet");
+  CUDA_TRY(ctx, cudaEventSynchronize(b->nl_ev[1]));
+  float t = 0.f;
+  CUDA_TRY(ctx, cudaEventElapsedTime(&t, b->nl_ev[0], b->nl_ev[1]));
+  *ms = t;
+  return PB2_OK;
+}
+
 extern "C" int pb2_nl_get(pb2_batch *b, int32_t *neighbors, void *stream) {
   if (!b || !neighbors) return PB2_EINVAL;
   pb2_ctx *ctx = b->ctx;
   if (!b->nl_built) return fail(ctx, PB2_EINVAL, "no neighbour list built yet");
   cudaStream_t st = (cudaStream_t)stream;
+  int rc = nl_settle(b, st);  // a build queued by an asynchronous check may have outgrown the rows
+  if (rc) return rc;
   const size_t cap = (size_t)b->nl_capacity;
   std::vector<int> rows((size_t)b->n_total * cap);
   CUDA_TRY(ctx, cudaMemcpyAsync(rows.data(), b->nl_rows, rows.size() * sizeof(int), cudaMemcpyDeviceToHost, st));

@@ -14,7 +14,11 @@
 // Host code reaches it only through cudaGetSymbolAddress: in host code the
 // array's name is a host-side stand-in, not a device address.  The address
 // is looked up once per device, on the first call made with that device
-// current; make that first call before any stream capture.
+// current; make that first call before any stream capture.  After a
+// cudaDeviceReset the cached address no longer names device memory and the
+// next call looks it up again (so that call, too, belongs outside a
+// capture).  Every buffer must be device memory of the current device, and
+// with a context that device must be the context's.
 //
 // All calls share the one array and it keeps the last call's contents, so
 // every call clears the part it uses first.  Calls whose kernels overlap on
@@ -23,6 +27,7 @@
 #include <mutex>
 
 #include "pb2_common.cuh"
+#include "pb2_internal.h"
 #include "pb2_kernels.cuh"
 #include "pb2_pairmath.cuh"
 
@@ -119,6 +124,16 @@ using namespace pb2;
 static std::mutex g_noalloc_lock;
 static long long *g_noalloc_addr[64];
 
+// True when p is device (or managed) memory of device dev.
+static bool on_device(const void *p, int dev) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();  // an unknown pointer leaves an error behind on old runtimes
+    return false;
+  }
+  return (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) && a.device == dev;
+}
+
 extern "C" int pb2_born_radii_noalloc(pb2_ctx *ctx, int32_t n_atoms, const double *positions,
                                       const double *radii, const double *scaled_radii,
                                       double cutoff, double *born, void *stream) {
@@ -130,9 +145,20 @@ extern "C" int pb2_born_radii_noalloc(pb2_ctx *ctx, int32_t n_atoms, const doubl
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
     return set_error(ctx, PB2_ENODEV, "pb2_born_radii_noalloc: no current CUDA device");
+  if (ctx && dev != ctx->device)
+    return set_error(ctx, PB2_EINVAL,
+                     "pb2_born_radii_noalloc: the current CUDA device is not the context's device");
+  if (!on_device(positions, dev) || !on_device(radii, dev) || !on_device(scaled_radii, dev) ||
+      !on_device(born, dev))
+    return set_error(ctx, PB2_EINVAL,
+                     "pb2_born_radii_noalloc: every buffer must be device memory of the current device");
   long long *scratch = nullptr;
   {
     std::lock_guard<std::mutex> lk(g_noalloc_lock);
+    // looked up once per device; a cudaDeviceReset in between unloads the
+    // module, the cached address stops being device memory, and it is
+    // looked up again
+    if (g_noalloc_addr[dev] && !on_device(g_noalloc_addr[dev], dev)) g_noalloc_addr[dev] = nullptr;
     if (!g_noalloc_addr[dev]) {
       void *p = nullptr;
       const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_sum);
@@ -151,6 +177,7 @@ extern "C" int pb2_born_radii_noalloc(pb2_ctx *ctx, int32_t n_atoms, const doubl
   const int grid_atoms = (n + 255) / 256;
   int grid_tiles = (int)((tiles + 7) / 8);
   if (grid_tiles > 4096) grid_tiles = 4096;
+  cudaGetLastError();  // an earlier, unrelated launch error is not this call's
   noalloc_clear<<<grid_atoms, 256, 0, st>>>(scratch, n);
   noalloc_born_tiles<<<grid_tiles, 256, 0, st>>>(positions, radii, scaled_radii, n, cut2, clamp, scratch);
   noalloc_born_finalize<<<grid_atoms, 256, 0, st>>>(radii, scratch, n, clamp, born);

@@ -539,12 +539,22 @@ __global__ void __launch_bounds__(kTileThreads<PASS>, kTileMinBlocks<PASS>)
   const uint32_t diag_mask = lane == 31 ? 0u : (0xffffffffu << (lane + 1));
   const float bscale = PASS == PASS_BORN ? (float)kBornScale : (float)kForceScale;
 
+  // a cutoff run with a pair list takes its items (and each item's j-blocks)
+  // from the list; otherwise items are contiguous j-block ranges
+  const bool plm = CUT && a.pl_ctl != nullptr;
+  const TileItem *items = a.items;
+  int n_items = a.n_items;
+  if (plm) {
+    const int cur = a.pl_ctl[PL_CUR];
+    items = cur ? a.pl_items1 : a.pl_items0;
+    n_items = a.pl_ctl[PL_COUNT0 + cur];
+  }
   for (;;) {
     int it = 0;
     if (lane == 0) it = atomicAdd(&a.sched[0], 1);
     it = __shfl_sync(kFull, it, 0);
-    if (it >= a.n_items) break;
-    const TileItem item = a.items[it];
+    if (it >= n_items) break;
+    const TileItem item = items[it];
     const SysInfo &S = a.sys[item.sys];
     const int n = S.n, off = S.off;
     K.cut2 = S.cutoff2; K.gcut2 = S.gb_cutoff2; K.bcut2 = S.born_cut2;
@@ -573,7 +583,8 @@ __global__ void __launch_bounds__(kTileThreads<PASS>, kTileMinBlocks<PASS>)
     }
 
     long long p0 = 0, p1 = 0, p2 = 0, p3 = 0, q0 = 0, q1 = 0, q2 = 0, q3 = 0;  // i-side sums
-    for (int jb = item.jb0; jb < item.jb1; ++jb) {
+    for (int tt = item.jb0; tt < item.jb1; ++tt) {
+      const int jb = plm ? a.pl_jlist[tt] : tt;
       const int gjb = S.blk_base + jb;
       // smallest bounding-box separation over the live tiles of the pair
       float d2 = 0.f;
@@ -705,16 +716,22 @@ __global__ void __launch_bounds__(kTileThreads<PASS>, kTileMinBlocks<PASS>)
 
 // Per-block bounding boxes of the float32 positions: one warp per block.
 __global__ void bbox_kernel(const SysInfo *sys, const int32_t *blk_sys, const float4 *posq,
-                            float4 *bbox, int n_blocks) {
+                            float4 *bbox, int n_blocks, const float4 *pl_ref, int32_t *pl_ctl) {
   const int lane = threadIdx.x & 31;
   const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int nw = (int)((gridDim.x * blockDim.x) >> 5);
+  bool moved = false;  // this lane saw an atom beyond skin / 2 of the pair list's reference
   for (int b = w; b < n_blocks; b += nw) {
     const SysInfo &S = sys[blk_sys[b]];
     const int lb = b - S.blk_base;
     const int l = lb * 32 + lane;
     const int i = S.off + (l < S.n ? l : lb * 32);
     const float4 p = posq[i];
+    if (pl_ref) {
+      const float4 r = pl_ref[i];
+      const float dx = p.x - r.x, dy = p.y - r.y, dz = p.z - r.z;
+      moved |= (double)fmaf(dx, dx, fmaf(dy, dy, dz * dz)) > S.skin_half2;
+    }
     float lo[3] = {p.x, p.y, p.z}, hi[3] = {p.x, p.y, p.z};
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1)
@@ -728,6 +745,7 @@ __global__ void bbox_kernel(const SysInfo *sys, const int32_t *blk_sys, const fl
       bbox[2 * b + 1] = make_float4(hi[0], hi[1], hi[2], 0.f);
     }
   }
+  if (pl_ctl && __any_sync(kFull, moved) && lane == 0) atomicOr(&pl_ctl[PL_DIRTY], 1);
 }
 
 // Born radii from the descreening sums, plus the per-atom GB self term
@@ -811,10 +829,10 @@ cudaError_t launch_tiles(int pass, const PairArgs &a, int grid, cudaStream_t st)
 }
 
 cudaError_t launch_bbox(const SysInfo *sys, const int32_t *blk_sys, const float4 *posq, float4 *bbox,
-                        int n_blocks, cudaStream_t st) {
+                        int n_blocks, cudaStream_t st, const float4 *pl_ref, int32_t *pl_ctl) {
   if (n_blocks <= 0) return cudaSuccess;
   const int grid = (n_blocks + 7) / 8;
-  bbox_kernel<<<grid, 256, 0, st>>>(sys, blk_sys, posq, bbox, n_blocks);
+  bbox_kernel<<<grid, 256, 0, st>>>(sys, blk_sys, posq, bbox, n_blocks, pl_ref, pl_ctl);
   return cudaGetLastError();
 }
 

@@ -81,6 +81,16 @@ def _ip(a):
   return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
 
 
+def _first(system, *keys):
+  """The first of ``keys`` that holds a non-empty array (the fallback order
+  of make_energy_fn, system.py:60-76), else None."""
+  for k in keys:
+    v = system.get(k)
+    if v is not None and np.asarray(v).size:
+      return v
+  return None
+
+
 def prepare_system(system: dict, *, dt=None, kT=None, gamma=None, key=None, eps_in=1.0,
                    eps_out=78.5, k_gb=K_COULOMB, k_coulomb=K_COULOMB,
                    lj14=topology.LJ14_DEFAULT, coul14=topology.COUL14_DEFAULT):
@@ -99,14 +109,40 @@ def prepare_system(system: dict, *, dt=None, kT=None, gamma=None, key=None, eps_
   out["bond_params"] = _f64(system.get("bond_params", np.zeros((0, 2))), (-1, 2))
   out["angles"] = _i32(system.get("angles", np.zeros((0, 3))), (-1, 3))
   out["angle_params"] = _f64(system.get("angle_params", np.zeros((0, 2))), (-1, 2))
-  dih = system.get("dihedrals", system.get("proper_dihedrals"))
+  dih = _first(system, "dihedrals", "proper_dihedrals")
   dih = _i32(np.zeros((0, 4)) if dih is None else dih, (-1, 4))
-  dp = system.get("dihedral_params", system.get("proper_dihedral_params"))
+  dp = _first(system, "dihedral_params", "proper_dihedral_params")
   dp = np.zeros((0, 1, 3)) if dp is None else np.asarray(dp, dtype=np.float64)
   if dp.ndim == 2:
     dp = dp[:, None, :]
   out["dihedrals"] = dih
   out["dihedral_params"] = _f64(dp).reshape(dih.shape[0], -1, 3) if dih.shape[0] else np.zeros((0, 1, 3))
+  # impropers: the parameters' last axis picks the form as system.py:77-83 does
+  # (2: harmonic (k, phi0), else periodic (n, phase, k))
+  imp = _first(system, "impropers", "improper_dihedrals")
+  imp = _i32(np.zeros((0, 4)) if imp is None else imp, (-1, 4))
+  ipar = _first(system, "improper_params", "improper_dihedral_params")
+  if imp.shape[0]:
+    if ipar is None:
+      raise ValueError("impropers given without improper_params")
+    ipar = np.asarray(ipar, dtype=np.float64)
+    if ipar.ndim == 2:
+      ipar = ipar[:, None, :]
+    width = ipar.shape[-1]
+    if width not in (2, 3):
+      raise ValueError(f"improper_params rows must be (k, phi0) or (n, phase, k), got {width} values")
+    out["improper_form"] = 1 if width == 2 else 0
+    out["improper_params"] = _f64(ipar).reshape(imp.shape[0], -1, width)
+  else:
+    out["improper_form"] = 0
+    out["improper_params"] = np.zeros((0, 1, 3))
+  out["impropers"] = imp
+  ub = _first(system, "urey_bradley_bonds")
+  out["urey_bradley_bonds"] = _i32(np.zeros((0, 2)) if ub is None else ub, (-1, 2))
+  ubp = _first(system, "urey_bradley_params")
+  if out["urey_bradley_bonds"].shape[0] and ubp is None:
+    raise ValueError("urey_bradley_bonds given without urey_bradley_params")
+  out["urey_bradley_params"] = _f64(np.zeros((0, 2)) if ubp is None else ubp, (-1, 2))
   if "cmap_torsions" in system and len(system["cmap_torsions"]):
     grids = np.asarray(system["cmap_energy_grids"], dtype=np.float64)
     if grids.ndim == 2:
@@ -123,6 +159,13 @@ def prepare_system(system: dict, *, dt=None, kT=None, gamma=None, key=None, eps_
   if "excl_pairs" in system:
     out["excl_pairs"] = _i32(system["excl_pairs"], (-1, 2))
     out["excl_kind"] = _i32(system["excl_kind"])
+  elif system.get("excl_indices") is not None:
+    # prolix's per-atom padded table (map_exclusions_to_dense_padded)
+    pairs, kind, t_lj14, t_c14 = topology.pairs_from_padded_table(
+        system["excl_indices"], system.get("excl_scales_vdw"), system.get("excl_scales_elec"))
+    out["excl_pairs"], out["excl_kind"] = pairs, kind
+    lj14 = system.get("lj14_scale", t_lj14)
+    coul14 = system.get("coul14_scale", t_c14)
   else:
     out["excl_pairs"], out["excl_kind"] = topology.exclusion_pairs(bonds, n)
   out["scal"] = dict(lj14=float(system.get("lj14_scale", lj14)),
@@ -190,6 +233,13 @@ def _desc(p) -> _lib.SystemDesc:
     d.origin[0], d.origin[1], d.origin[2] = p["origin"]
   d.n_exceptions = p["exception_pairs"].shape[0]
   d.exception_pairs, d.exception_params = _ip(p["exception_pairs"]), _dp(p["exception_params"])
+  d.n_impropers = p["impropers"].shape[0]
+  d.n_improper_terms = p["improper_params"].shape[1] if d.n_impropers else 1
+  d.improper_form = p["improper_form"]
+  d.impropers, d.improper_params = _ip(p["impropers"]), _dp(p["improper_params"])
+  d.n_urey_bradley = p["urey_bradley_bonds"].shape[0]
+  d.urey_bradley_bonds = _ip(p["urey_bradley_bonds"])
+  d.urey_bradley_params = _dp(p["urey_bradley_params"])
   return d
 
 
@@ -199,7 +249,7 @@ class Batch:
   def __init__(self, systems, *, cutoff=0.0, gb_cutoff=-1.0, born_cutoff=0.0, skin=2.0, terms=_lib.USE_ALL,
                device=0,
                tile_segment=0, graph_chunk=50, partitionable_keys=True, nl_capacity=0,
-               keep_atom_order=False, **system_defaults):
+               keep_atom_order=False, pair_list=True, **system_defaults):
     if isinstance(systems, dict):
       systems = [systems]
     if not systems:
@@ -218,7 +268,8 @@ class Batch:
                         graph_chunk=int(graph_chunk),
                         partitionable_keys=1 if partitionable_keys else 0,
                         gb_cutoff=float(gb_cutoff), born_cutoff=float(born_cutoff),
-                        keep_atom_order=1 if keep_atom_order else 0)
+                        keep_atom_order=1 if keep_atom_order else 0,
+                        pair_list=0 if pair_list else -1)
     h = ctypes.c_void_p()
     self.ctx.check(self.lib.pb2_batch_create(self.ctx.handle, self.n_systems, descs,
                                              ctypes.byref(rp), ctypes.byref(h)))
@@ -252,7 +303,7 @@ class Batch:
 
   # ---------------------------------------------------------------- physics
   def energy_forces(self, stream=None):
-    """(energies (n_systems, 10) with columns TERM_NAMES, forces (n_atoms, 3))."""
+    """(energies (n_systems, NTERMS) with columns TERM_NAMES, forces (n_atoms, 3))."""
     e = np.zeros((self.n_systems, _lib.NTERMS))
     f = np.zeros((self.n_atoms, 3))
     self._check(self.lib.pb2_energy_forces(self.handle, e.ctypes.data, f.ctypes.data, stream))
@@ -327,6 +378,16 @@ class Batch:
         raise ValueError(f"langevin_run_host: arrays must be writeable C-contiguous float64 ({self.n_atoms}, 3)")
     self._check(self.lib.pb2_langevin_run_host(self.handle, position.ctypes.data, momentum.ctypes.data,
                                                force.ctypes.data, int(n_steps), stream, copy_in, copy_out))
+
+  def langevin_run_device(self, position_ptr, momentum_ptr, force_ptr, n_steps, stream=None):
+    """pb2_langevin_run_device: the functional step on caller-owned device
+    arrays ((n_atoms, 3) float64 row-major, e.g. torch tensors'
+    data_ptr()), overwritten with the new state; asynchronous on
+    ``stream``."""
+    if not (position_ptr and momentum_ptr and force_ptr):
+      raise ValueError("langevin_run_device: three device pointers are required")
+    self._check(self.lib.pb2_langevin_run_device(self.handle, position_ptr, momentum_ptr, force_ptr,
+                                                 int(n_steps), stream))
 
   def energy_forces_device(self, positions_ptr, energies_ptr, forces_ptr, stream=None):
     """pb2_energy_forces_device on raw device pointers (e.g. a torch tensor's
@@ -470,10 +531,22 @@ class Batch:
   def nl_build(self, stream=None):
     self._check(self.lib.pb2_nl_build(self.handle, stream))
 
-  def nl_check(self, stream=None) -> int:
+  def nl_check(self, stream=None, wait=True):
+    """Rebuild the neighbour list if an atom moved more than skin/2 since the
+    last build.  wait=True: returns how many systems had; wait=False: only
+    enqueues the check (and rebuild), returns None."""
+    if not wait:
+      self._check(self.lib.pb2_nl_check(self.handle, None, stream))
+      return None
     r = ctypes.c_int32(0)
     self._check(self.lib.pb2_nl_check(self.handle, ctypes.byref(r), stream))
     return int(r.value)
+
+  def nl_last_build_ms(self) -> float:
+    """Device time of the last neighbour-list build (CUDA events)."""
+    t = ctypes.c_double(0.0)
+    self._check(self.lib.pb2_nl_last_build_ms(self.handle, ctypes.byref(t)))
+    return float(t.value)
 
   def nl_capacity(self) -> int:
     c = ctypes.c_int32(0)

@@ -25,7 +25,7 @@ import dataclasses
 import numpy as np
 
 from . import engine
-from .system import EnergyFn, make_energy_fn, system_to_dict
+from .system import EnergyFn, exclusion_spec_from_bonds, make_energy_fn, system_to_dict
 
 BOLTZMANN_KCAL = 0.0019872041
 
@@ -111,6 +111,15 @@ def _as_energy_fn(energy_or_force_fn) -> EnergyFn:
                   "prolix_b200.system.make_energy_fn (the GPU path carries the system)")
 
 
+def _use(batch, dt: float, kT: float):
+  """Make the batch step at (dt, kT), recomputing its constants only when
+  they change (the recomputation is exact: equal to a batch created with
+  the same values)."""
+  if batch.langevin_now != (dt, kT):
+    batch.set_langevin_params(dt=dt, kT=kT)
+    batch.langevin_now = (dt, kT)
+
+
 def nvt_langevin(energy_or_force_fn, shift_fn, dt: float, kT: float, gamma: float = 0.1,
                  mass=1.0, center_velocity: bool = True, **kwargs):
   """BAOAB Langevin (jax_md ``nvt_langevin`` protocol) on the GPU.
@@ -127,6 +136,8 @@ def nvt_langevin(energy_or_force_fn, shift_fn, dt: float, kT: float, gamma: floa
     n = efn.n_atoms
     m = np.broadcast_to(np.asarray(mass, dtype=np.float64).reshape(-1), (n,)).copy()
     sysd = dict(efn.system, positions=np.asarray(R, dtype=np.float64).reshape(n, 3), masses=m)
+    # the momenta are drawn at init's kT (settle.py:1676-1691); the steps
+    # run at the factory's kT unless a call passes its own
     batch = engine.Batch([sysd], cutoff=efn.cutoff, gb_cutoff=efn.gb_cutoff, born_cutoff=efn.born_cutoff,
                          key=np.asarray(key, dtype=np.uint32).reshape(2), dt=float(dt),
                          kT=_kT, gamma=float(gamma),
@@ -135,13 +146,14 @@ def nvt_langevin(energy_or_force_fn, shift_fn, dt: float, kT: float, gamma: floa
     batch.langevin_init()
     if center_velocity:
       batch.center_momentum()
+    batch.langevin_now = (float(dt), _kT)
+    _use(batch, float(dt), float(kT))
     return NVTLangevinState(batch, m)
 
   def apply_fn(state: NVTLangevinState, n_steps: int = 1, **kw):
-    # per-call dt / kT overrides, as the reference's apply_fn pops them
-    # (physics/settle.py:1698-1700); they hold for the following calls too
-    if "dt" in kw or "kT" in kw:
-      state._batch.set_langevin_params(dt=kw.get("dt"), kT=kw.get("kT"))
+    # per-call dt / kT overrides hold for that call only; later calls fall
+    # back to the factory's values (physics/settle.py:1698-1700)
+    _use(state._batch, float(kw.get("dt", dt)), float(kw.get("kT", kT)))
     state._batch.langevin_run(int(n_steps))
     return NVTLangevinState(state._batch, state._mass)
 
@@ -187,8 +199,14 @@ def run_simulation(system_params, initial_positions, temperature: float = 300.0,
   sysd = system_to_dict(system_params)
   r0 = np.asarray(initial_positions, dtype=np.float64)
   sysd["positions"] = r0
+  # the reference hands make_energy_fn a proxide Protein built from the
+  # parameters (physics/simulate.py:400-414); here its 1-2 / 1-3 / 1-4
+  # classes come from the bonds, as ExclusionSpec.from_protein derives them
+  spec = None
+  if "excl_pairs" not in sysd and sysd.get("excl_indices") is None:
+    spec = exclusion_spec_from_bonds(sysd.get("bonds", np.zeros((0, 2))), r0.shape[0])
   efn = make_energy_fn(None, sysd, implicit_solvent=True, solvent_dielectric=solvent_dielectric,
-                       solute_dielectric=solute_dielectric)
+                       solute_dielectric=solute_dielectric, exclusion_spec=spec)
   r = run_minimization(efn, r0, steps=min_steps)
   masses = np.asarray(sysd.get("masses", np.ones(r.shape[0])), dtype=np.float64)
   kT = BOLTZMANN_KCAL * temperature

@@ -8,8 +8,21 @@ mirrors prolix physics/system.py:29-271 for ``implicit_solvent=True``:
   Coulomb and LJ use ``cutoff`` (the ``cutoff`` keyword wins over
   ``cutoff_distance``, system.py:134; a cutoff <= 0 means all pairs), as the
   reference does (system.py:184-216);
-* exclusions: 1-2 and 1-3 pairs excluded, 1-4 pairs scaled (LJ 0.5,
-  Coulomb 0.83333333), from the bonds or from ``exclusion_spec``;
+* exclusions come from ``exclusion_spec`` (an ExclusionSpec or any object
+  with its fields; ``exclusion_spec_from_bonds`` builds one from a bond
+  list as ``ExclusionSpec.from_protein`` does) or from the system's own
+  ``excl_indices`` / ``excl_scales_vdw`` / ``excl_scales_elec`` table
+  (system.py:161-171).  With neither, Coulomb and LJ exclude no pair at
+  all: the reference then uses an empty (N, 0) table;
+* bonded terms: bonds, angles, dihedrals (or ``proper_dihedrals``),
+  impropers (``impropers`` or ``improper_dihedrals``; parameter rows of 2
+  values are harmonic (k, phi0), of 3 periodic (n, phase, k), as
+  system.py:77-83 decides), Urey-Bradley springs, CMAP and the
+  exclusion spec's explicit 1-4 exception pairs;
+* a dict key this path does not read raises ``ValueError`` (rather than
+  being dropped), except metadata the reference's energy factory ignores
+  too (masks of bonded terms, element and selection flags, constraint
+  and water tables);
 * the returned function gives the total energy; ``.forces(r)`` gives
   -dE/dr, ``.energy_and_forces(r)`` both;
 * ``return_decomposed=True`` returns the reference's dict of per-term
@@ -21,6 +34,8 @@ runs use ``space.free()``).  Everything runs on the GPU through the C ABI.
 
 from __future__ import annotations
 
+import dataclasses
+
 import numpy as np
 
 from . import engine, topology
@@ -28,21 +43,75 @@ from ._lib import TERM_NAMES, USE_ALL
 
 _SYSTEM_KEYS = ("charges", "sigmas", "epsilons", "radii", "scaled_radii", "masses", "bonds",
                 "bond_params", "angles", "angle_params", "dihedrals", "dihedral_params",
-                "proper_dihedrals", "proper_dihedral_params", "cmap_torsions", "cmap_indices",
-                "cmap_energy_grids", "excl_pairs", "excl_kind", "exception_pairs",
-                "exception_sigmas", "exception_epsilons", "exception_chargeprods")
+                "proper_dihedrals", "proper_dihedral_params", "impropers", "improper_params",
+                "improper_dihedrals", "improper_dihedral_params", "urey_bradley_bonds",
+                "urey_bradley_params", "cmap_torsions", "cmap_indices",
+                "cmap_energy_grids", "excl_indices", "excl_scales_vdw", "excl_scales_elec",
+                "excl_pairs", "excl_kind", "exception_pairs",
+                "exception_sigmas", "exception_epsilons", "exception_chargeprods", "atom_mask")
+# keys read by the batch itself (integrator settings, explicit 1-4 scales, origin)
+_ENGINE_KEYS = ("positions", "lj14_scale", "coul14_scale", "key", "seed", "dt", "kT", "gamma",
+                "origin", "solute_dielectric", "solvent_dielectric")
+# PhysicsSystem fields the reference's energy factory does not read either
+# (typing.py:256-336 against system.py:29-271): masks of bonded terms, atom
+# flags, constraint / water tables, the dense exclusion matrix, padding
+# metadata
+_IGNORED_KEYS = ("element_ids", "is_hydrogen", "is_backbone", "is_heavy", "protein_atom_mask",
+                 "water_atom_mask", "bond_mask", "angle_mask", "dihedral_mask", "improper_mask",
+                 "urey_bradley_mask", "cmap_mask", "constraint_pairs", "constraint_lengths",
+                 "constraint_mask", "water_indices", "water_mask", "n_real_atoms",
+                 "n_padded_atoms", "bucket_size", "box_size", "exclusion_mask",
+                 "nonbonded_cutoff", "pme_alpha", "pme_grid_points", "atom_names",
+                 "residue_names", "residue_index", "cmap_coeffs")
 
 
 def system_to_dict(system) -> dict:
-  """Accept a dict or any object with prolix's PhysicsSystem attribute names."""
+  """Accept a dict or any object with prolix's PhysicsSystem attribute names.
+
+  A dict key that is neither read here nor ignored by the reference's
+  energy factory raises ``ValueError``; so does an ``atom_mask`` with
+  padding atoms (the reference zeroes their ACE term, system.py:230; a
+  batch holds real atoms only)."""
   if isinstance(system, dict):
-    return dict(system)
-  out = {}
-  for k in _SYSTEM_KEYS + ("positions",):
-    v = getattr(system, k, None)
-    if v is not None:
-      out[k] = np.asarray(v)
+    unknown = sorted(set(system) - set(_SYSTEM_KEYS) - set(_ENGINE_KEYS) - set(_IGNORED_KEYS))
+    if unknown:
+      raise ValueError(f"system keys not understood by the implicit-solvent energy: {unknown}")
+    out = {k: v for k, v in system.items() if k not in _IGNORED_KEYS}
+  else:
+    out = {}
+    for k in _SYSTEM_KEYS + ("positions",):
+      v = getattr(system, k, None)
+      if v is not None:
+        out[k] = np.asarray(v)
+  mask = out.pop("atom_mask", None)
+  if mask is not None and not np.all(np.asarray(mask, dtype=bool)):
+    raise ValueError("atom_mask marks padding atoms; pass the real atoms only "
+                     "(a batch stores systems unpadded)")
   return out
+
+
+@dataclasses.dataclass(frozen=True)
+class ExclusionSpec:
+  """prolix's ExclusionSpec fields (physics/neighbor_list.py:25-50)."""
+  idx_12_13: np.ndarray
+  idx_14: np.ndarray
+  scale_14_elec: float
+  scale_14_vdw: float
+  n_atoms: int
+  exception_pairs: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros((0, 2), np.int32))
+  exception_sigmas: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros(0))
+  exception_epsilons: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros(0))
+  exception_chargeprods: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros(0))
+
+
+def exclusion_spec_from_bonds(bonds, n_atoms: int, coulomb14scale: float = 0.83333333,
+                              lj14scale: float = 0.5) -> ExclusionSpec:
+  """``ExclusionSpec.from_protein`` for a bond list without explicit 1-4
+  parameters (neighbor_list.py:52-142): 1-2 and 1-3 pairs excluded, 1-4
+  pairs scaled."""
+  pairs, kind = topology.exclusion_pairs(bonds, n_atoms)
+  return ExclusionSpec(idx_12_13=pairs[kind == 0], idx_14=pairs[kind == 1],
+                       scale_14_elec=coulomb14scale, scale_14_vdw=lj14scale, n_atoms=int(n_atoms))
 
 
 def _exclusions_from_spec(spec, n):
@@ -165,6 +234,9 @@ def make_energy_fn(displacement_fn, system, cutoff_distance: float = 9.0,
   if not implicit_solvent:
     raise NotImplementedError(
         "prolix_b200 implements the implicit-solvent path only (implicit_solvent=True)")
+  if kwargs.get("use_pbc", False):
+    raise NotImplementedError("prolix_b200 implements free-space implicit solvent only "
+                              "(use_pbc=True selects the reference's PME path)")
   sysd = system_to_dict(system)
   n = int(np.asarray(sysd["charges"]).shape[0])
   if n == 0:
@@ -175,10 +247,16 @@ def make_energy_fn(displacement_fn, system, cutoff_distance: float = 9.0,
     sysd["radii"] = np.ones(n)
   if "scaled_radii" not in sysd or sysd["scaled_radii"] is None:
     sysd["scaled_radii"] = np.asarray(sysd["radii"])
-  if exclusion_spec is not None and "excl_pairs" not in sysd:
+  has_table = sysd.get("excl_indices") is not None and np.asarray(sysd["excl_indices"]).size > 0
+  if exclusion_spec is not None and "excl_pairs" not in sysd and not has_table:
+    # the spec is used only when the system has no table of its own (system.py:161-162)
     pairs, kind, lj14, c14 = _exclusions_from_spec(exclusion_spec, n)
     sysd["excl_pairs"], sysd["excl_kind"] = pairs, kind
     sysd["lj14_scale"], sysd["coul14_scale"] = lj14, c14
+  elif "excl_pairs" not in sysd and not has_table:
+    # no spec and no table: the reference's (N, 0) table excludes nothing
+    sysd["excl_pairs"] = np.zeros((0, 2), np.int32)
+    sysd["excl_kind"] = np.zeros(0, np.int32)
   if exclusion_spec is not None and "exception_pairs" not in sysd:
     # explicit 1-4 overrides (system.py:149-159): their own energy term
     for k in ("exception_pairs", "exception_sigmas", "exception_epsilons", "exception_chargeprods"):
@@ -205,10 +283,10 @@ def make_energy_fn(displacement_fn, system, cutoff_distance: float = 9.0,
   def nonpolar(r, born_radii=None):
     return fn.terms(r)["nonpolar"]
 
-  zero = lambda r, n=None: 0.0
   return {
       "bond": term("bond"), "angle": term("angle"), "dihedral": term("dihedral"),
-      "improper": zero, "urey_bradley": zero, "cmap": term("cmap"), "lj": term("lj"),
+      "improper": term("improper"), "urey_bradley": term("urey_bradley"), "cmap": term("cmap"),
+      "lj": term("lj"),
       "exception": term("exception"), "electrostatics": electrostatics, "nonpolar": nonpolar,
       "total": fn,
   }

@@ -11,7 +11,7 @@ from oracle import gbsa as ogbsa
 from oracle import integrator as ointeg
 from oracle import prng
 from prolix_b200 import engine, simulate, synth
-from prolix_b200.system import make_energy_fn
+from prolix_b200.system import exclusion_spec_from_bonds, make_energy_fn
 
 pytestmark = pytest.mark.gpu
 
@@ -24,10 +24,14 @@ def oracle_terms(s, pos, cutoff, gb_cutoff):
   return e, fb + fn, ex
 
 
+def spec_of(s):
+  return exclusion_spec_from_bonds(s["bonds"], len(s["charges"]))
+
+
 def test_make_energy_fn_default_semantics():
   # prolix: GB all pairs, LJ/Coulomb with cutoff_distance = 9.0
   s = synth.make_chain(400, 6, compact=True, cmap=True)
-  fn = make_energy_fn(None, s, implicit_solvent=True)
+  fn = make_energy_fn(None, s, implicit_solvent=True, exclusion_spec=spec_of(s))
   e_ref, f_ref, _ = oracle_terms(s, s["positions"], 9.0, 0.0)
   assert fn(s["positions"]) == pytest.approx(e_ref["total"], rel=1e-6, abs=1e-6)
   f = fn.forces(s["positions"])
@@ -39,7 +43,8 @@ def test_make_energy_fn_default_semantics():
 
 def test_decomposed_dict_and_cutoff_keyword():
   s = synth.make_chain(200, 7, compact=True)
-  d = make_energy_fn(None, s, implicit_solvent=True, return_decomposed=True, cutoff=0.0)
+  d = make_energy_fn(None, s, implicit_solvent=True, return_decomposed=True, cutoff=0.0,
+                     exclusion_spec=spec_of(s))
   assert set(d) == {"bond", "angle", "dihedral", "improper", "urey_bradley", "cmap", "lj",
                     "exception", "electrostatics", "nonpolar", "total"}
   e_ref, _, ex = oracle_terms(s, s["positions"], 0.0, 0.0)
@@ -60,8 +65,36 @@ def test_exclusion_spec_object():
   spec = types.SimpleNamespace(idx_12_13=np.concatenate([p12, p13]), idx_14=p14,
                                scale_14_elec=0.83333333, scale_14_vdw=0.5)
   fa = make_energy_fn(None, s, implicit_solvent=True, exclusion_spec=spec, cutoff=0.0)
-  fb = make_energy_fn(None, s, implicit_solvent=True, cutoff=0.0)
+  fb = make_energy_fn(None, s, implicit_solvent=True, exclusion_spec=spec_of(s), cutoff=0.0)
   assert fa(s["positions"]) == fb(s["positions"])
+  e_ref = oracle_terms(s, s["positions"], 0.0, 0.0)[0]
+  assert fa(s["positions"]) == pytest.approx(e_ref["total"], rel=1e-6)
+
+
+def test_no_exclusion_information_excludes_nothing():
+  # a dict without excl_indices and no exclusion_spec: the reference's
+  # (N, 0) table (system.py:161-171), so 1-2 / 1-3 / 1-4 pairs interact fully
+  s = synth.make_chain(120, 9)
+  fn = make_energy_fn(None, s, implicit_solvent=True, cutoff=0.0)
+  none = dict(s, excl_pairs=np.zeros((0, 2), np.int32), excl_kind=np.zeros(0, np.int32))
+  e_ref, f_ref, _ = oracle_terms(none, s["positions"], 0.0, 0.0)
+  t = fn.terms(s["positions"])
+  for k in ("lj", "coulomb"):
+    assert t[k] == pytest.approx(e_ref[k], rel=1e-6), k
+  f = fn.forces(s["positions"])
+  assert np.linalg.norm(f - f_ref) / np.linalg.norm(f_ref) < 1e-5
+
+
+def test_unknown_system_keys_raise():
+  s = synth.make_chain(60, 3)
+  with pytest.raises(ValueError, match="virtual_site_params"):
+    make_energy_fn(None, dict(s, virtual_site_params=np.zeros((1, 12))), implicit_solvent=True)
+  with pytest.raises(ValueError, match="atom_mask"):
+    make_energy_fn(None, dict(s, atom_mask=np.arange(60) < 50), implicit_solvent=True)
+  # metadata the reference's energy factory ignores too is accepted
+  fn = make_energy_fn(None, dict(s, bond_mask=np.ones(59, bool), is_heavy=np.ones(60, bool)),
+                      implicit_solvent=True)
+  fn.close()
 
 
 def test_separate_gb_and_direct_cutoffs():
@@ -78,7 +111,7 @@ def test_separate_gb_and_direct_cutoffs():
 
 def test_nvt_langevin_protocol_matches_oracle():
   s = synth.make_chain(150, 11)
-  fn = make_energy_fn(None, s, implicit_solvent=True, cutoff=0.0)
+  fn = make_energy_fn(None, s, implicit_solvent=True, cutoff=0.0, exclusion_spec=spec_of(s))
   dt, kT, gamma = engine.akma_dt(1.0), 300 * engine.KB_KCAL, engine.akma_gamma(1.0)
   key = prng.prng_key(17)
   init_fn, apply_fn = simulate.nvt_langevin(fn, None, dt=dt, kT=kT, gamma=gamma, mass=s["masses"])
@@ -96,7 +129,7 @@ def test_nvt_langevin_protocol_matches_oracle():
 def test_minimization_and_run_simulation():
   s = synth.make_chain(300, 12, compact=True)
   pos = s["positions"] + np.random.default_rng(0).normal(0, 0.15, size=s["positions"].shape)
-  fn = make_energy_fn(None, dict(s, positions=pos), implicit_solvent=True)
+  fn = make_energy_fn(None, dict(s, positions=pos), implicit_solvent=True, exclusion_spec=spec_of(s))
   e0 = fn(pos)
   r = simulate.run_minimization(fn, pos, sd_steps=30)
   assert fn(r) < e0
@@ -163,7 +196,7 @@ def test_energy_fn_takes_cuda_arrays():
   # device with no host copy; results equal the NumPy path bit for bit
   import torch
   s = synth.make_chain(180, 12, compact=True)
-  fn = make_energy_fn(None, s, implicit_solvent=True, cutoff=0.0)
+  fn = make_energy_fn(None, s, implicit_solvent=True, cutoff=0.0, exclusion_spec=spec_of(s))
   e_host, f_host = fn.energy_and_forces(s["positions"])
   t = torch.tensor(s["positions"], device="cuda")
   e_dev, f_dev = fn(t), fn.forces(t)

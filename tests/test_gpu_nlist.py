@@ -75,3 +75,44 @@ def test_neighbour_list_needs_a_cutoff():
   with engine.Batch([s]) as b:
     with pytest.raises(_lib.PB2Error):
       b.nl_build()
+
+
+@pytest.mark.parametrize("cutoffs", [dict(cutoff=9.0), dict(cutoff=8.0, gb_cutoff=12.0),
+                                     dict(cutoff=10.0, born_cutoff=7.0)])
+def test_pair_list_steps_equal_the_unlisted_steps(cutoffs):
+  # the pair kernels on the skin-buffered block-pair list give the same bits
+  # as scanning every block pair; a small skin makes the list rebuild often
+  # during the run (a list that missed a rebuild would drop pairs)
+  systems = synth.make_batch(5, 77, 300, 1500, compact=True, **synth.PHYSICAL_RANGES)
+  fields = ("position", "momentum", "force")
+  out = []
+  for pl in (True, False):
+    with engine.Batch(systems, skin=0.2, pair_list=pl, dt=engine.akma_dt(2.0),
+                      kT=600 * engine.KB_KCAL, **cutoffs) as b:
+      e0, f0 = b.energy_forces()
+      b.langevin_init()
+      b.langevin_run(120)
+      st = b.get_state(fields=fields)
+      out.append((e0, f0, st))
+  (ea, fa, sa), (eb, fb, sb) = out
+  np.testing.assert_array_equal(fa, fb)
+  np.testing.assert_array_equal(ea, eb)
+  for f in fields:
+    np.testing.assert_array_equal(sa[f], sb[f])
+  assert np.isfinite(sa["position"]).all()
+
+
+def test_asynchronous_check_rebuilds_on_the_device():
+  # the check and the rebuild it triggers are enqueued without a host wait;
+  # a list that outgrows its rows is grown at the next host visit (nl_get)
+  s = synth.make_chain(900, 14, compact=True)
+  with engine.Batch([s], cutoff=6.0, skin=1.0) as b:
+    b.nl_build()
+    cap0 = b.nl_capacity()
+    assert b.nl_last_build_ms() > 0.0
+    pos = s["positions"] * 0.8  # compress: every atom moves well past skin/2, rows grow
+    b.set_positions(pos)
+    assert b.nl_check(wait=False) is None
+    rows = b.nl_get()
+    assert b.nl_capacity() >= cap0
+  _check_rows(rows, [dict(s, positions=pos)], 7.0)

@@ -1,0 +1,97 @@
+"""The CUDA path, through the prolix-facing ``make_energy_fn`` drop-in and
+the C ABI, against values computed by prolix's own source code
+(``tests/golden/ref_fixtures.npz``; see ``tests/golden/make_ref_fixtures.py``).
+
+Each synthetic case is handed over as the reference would receive it: a
+system dict with the reference's own padded exclusion table
+(``excl_indices`` / ``excl_scales_vdw`` / ``excl_scales_elec`` from
+``map_exclusions_to_dense_padded``), or, for the explicit 1-4 case, an
+ExclusionSpec object.  Tolerances: per-term energy relative 1e-6 (+1e-6
+kcal/mol), force relative RMS 1e-5, Born radii relative 2e-6.
+"""
+
+import os
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+
+import ref_cases  # noqa: E402
+from prolix_b200 import topology  # noqa: E402
+from prolix_b200.system import ExclusionSpec, make_energy_fn  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+FIX = np.load(ref_cases.FIXTURE)
+TERMS = [str(t) for t in FIX["term_names"]]
+E_REL, E_ABS, F_RMS, B_REL = 1e-6, 1e-6, 1e-5, 2e-6
+
+
+def _energy_fn(name):
+  s, cutoff = ref_cases.case_system(name)
+  s = {k: v for k, v in s.items() if k != "seed"}
+  spec = None
+  if f"{name}/exception_pairs" in FIX:
+    pairs, _ = topology.exclusion_pairs(s["bonds"], len(s["charges"]))
+    p = FIX[f"{name}/exception_params"]
+    spec = ExclusionSpec(idx_12_13=pairs, idx_14=np.zeros((0, 2), np.int32),
+                         scale_14_elec=0.83333333, scale_14_vdw=0.5, n_atoms=len(s["charges"]),
+                         exception_pairs=FIX[f"{name}/exception_pairs"],
+                         exception_chargeprods=p[:, 0], exception_sigmas=p[:, 1],
+                         exception_epsilons=p[:, 2])
+  else:
+    s.update(excl_indices=FIX[f"{name}/excl_indices"],
+             excl_scales_vdw=FIX[f"{name}/excl_scales_vdw"],
+             excl_scales_elec=FIX[f"{name}/excl_scales_elec"])
+  fn = make_energy_fn(None, s, cutoff_distance=cutoff, implicit_solvent=True, exclusion_spec=spec)
+  return fn, s
+
+
+@pytest.mark.parametrize("name", list(ref_cases.CASES))
+def test_energy_terms_forces_and_born_radii_match_the_reference(name):
+  fn, s = _energy_fn(name)
+  try:
+    r = s["positions"]
+    terms = fn.terms(r)
+    ref = FIX[f"{name}/terms"]
+    for i, t in enumerate(TERMS):
+      assert terms[t] == pytest.approx(ref[i], rel=E_REL, abs=E_ABS), t
+    f = fn.forces(r)
+    fr = FIX[f"{name}/forces"]
+    assert np.linalg.norm(f - fr) / np.linalg.norm(fr) < F_RMS
+    np.testing.assert_allclose(fn.born_radii(r), FIX[f"{name}/born_radii"], rtol=B_REL)
+  finally:
+    fn.close()
+
+
+def test_decomposed_improper_and_urey_bradley_entries():
+  name = "chain166_harmonic_imp"
+  s, _ = ref_cases.case_system(name)
+  s = {k: v for k, v in s.items() if k != "seed"}
+  s.update(excl_indices=FIX[f"{name}/excl_indices"], excl_scales_vdw=FIX[f"{name}/excl_scales_vdw"],
+           excl_scales_elec=FIX[f"{name}/excl_scales_elec"])
+  d = make_energy_fn(None, s, cutoff_distance=0.0, implicit_solvent=True, return_decomposed=True)
+  ref = FIX[f"{name}/terms"]
+  r = s["positions"]
+  assert d["improper"](r) == pytest.approx(ref[TERMS.index("improper")], rel=E_REL)
+  assert d["urey_bradley"](r) == pytest.approx(ref[TERMS.index("urey_bradley")], rel=E_REL)
+  d["total"].close()
+
+
+def test_real_protein_born_radii_gb_and_ace_match_the_reference():
+  c = ref_cases.PQR_CASE
+  pos, q, rad, sr = (FIX[f"{c}/{k}"] for k in ("positions", "charges", "radii", "scaled_radii"))
+  n = pos.shape[0]
+  s = {"positions": pos, "charges": q, "radii": rad, "scaled_radii": sr, "sigmas": np.ones(n),
+       "epsilons": np.zeros(n)}
+  fn = make_energy_fn(None, s, cutoff_distance=0.0, implicit_solvent=True)
+  try:
+    terms = fn.terms(pos)
+    assert terms["gb"] == pytest.approx(float(FIX[f"{c}/gb"]), rel=E_REL)
+    assert terms["nonpolar"] == pytest.approx(float(FIX[f"{c}/nonpolar"]), rel=E_REL)
+    np.testing.assert_allclose(fn.born_radii(pos), FIX[f"{c}/born_radii"], rtol=B_REL)
+  finally:
+    fn.close()

@@ -36,6 +36,27 @@ def test_run_host_matches_device_state_path():
         assert np.array_equal(host[f], st[f]), f
 
 
+def test_run_device_matches_device_state_path():
+  # the jax.ffi form: caller-owned device arrays in and out, on one stream
+  systems = _systems()
+  fields = ("position", "momentum", "force")
+  with engine.Batch(systems) as a, engine.Batch(systems) as b:
+    a.langevin_init()
+    b.langevin_init()
+    st = a.get_state(fields=fields)
+    dev = {f: torch.tensor(st[f], device="cuda") for f in fields}
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(2):
+      b.langevin_run_device(dev["position"].data_ptr(), dev["momentum"].data_ptr(),
+                            dev["force"].data_ptr(), 3, stream)
+      torch.cuda.synchronize()
+      a.set_full_state(st["position"], st["momentum"], st["force"])
+      a.langevin_run(3)
+      st = a.get_state(fields=fields)
+      for f in fields:
+        assert np.array_equal(dev[f].cpu().numpy(), st[f]), f
+
+
 def test_grouped_streams_match_one_batch():
   systems = _systems()
   fields = ("position", "momentum", "force")

@@ -27,7 +27,7 @@ def test_library_loads_and_exports_every_declared_symbol():
     assert hasattr(lib, name), name
   bound = {name for name, _, _ in _lib.SIGNATURES}
   assert set(declared) <= bound | {"pb2_ctx_create"}
-  assert lib.pb2_abi_version() == _lib.ABI_VERSION == 2
+  assert lib.pb2_abi_version() == _lib.ABI_VERSION == 3
 
 
 def _struct_fields(text, name):
@@ -266,3 +266,15 @@ def test_prepare_system_packs_exception_pairs():
   assert d.n_exceptions == 2
   q = engine.prepare_system(s)
   assert q["exception_pairs"].shape == (0, 2) and engine._desc(q).n_exceptions == 0
+
+
+def test_ffi_handlers_are_source_behind_a_build_flag():
+  # the jax.ffi handlers exist as source; building them needs XLA's headers,
+  # which this image lacks, and the default build leaves them out
+  src = ROOT / "prolix_b200" / "csrc" / "ffi" / "pb2_ffi.cc"
+  text = src.read_text()
+  for name in ("pb2_ffi_energy_forces", "pb2_ffi_baoab", "pb2_energy_forces_device",
+               "pb2_langevin_run_device"):
+    assert name in text
+  with pytest.raises(FileNotFoundError, match="XLA FFI headers"):
+    _build.build_ffi(str(ROOT / "no_such_xla_include"))

@@ -1,5 +1,5 @@
 """The allocation-free Born-radius entry point, checked against the regular
-batch entry point.
+batch entry point and against the FP64 oracle.
 
 pb2_born_radii_noalloc serves callers that cannot call cudaMalloc (an XLA
 custom-call handler that may only use the buffers it is handed, code running
@@ -14,7 +14,8 @@ import ctypes
 import numpy as np
 import pytest
 
-from prolix_b200 import _lib, engine, synth
+from oracle import gbsa as ogbsa
+from prolix_b200 import engine, synth
 
 pytestmark = pytest.mark.gpu
 
@@ -46,6 +47,9 @@ def test_noalloc_born_radii_match_batch_entry_point(cutoff):
       with engine.Batch([s], cutoff=cutoff) as b:
         ref = b.born_radii()
       np.testing.assert_allclose(got, ref, rtol=2e-6)
+      oracle = ogbsa.born_radii(np.asarray(s["positions"]), np.asarray(s["radii"]),
+                                np.asarray(s["scaled_radii"]), cutoff)[0]
+      np.testing.assert_allclose(got, oracle, rtol=2e-6)
 
 
 def test_noalloc_rejects_too_many_atoms():
