@@ -132,7 +132,7 @@ def parse():
                        "is the reported value)")
   ap.add_argument("--clocks-dir", default=None,
                   help="folder for the nvidia-smi clock samples of the timed region "
-                       "(default: the system temporary folder)")
+                       "(default: a new folder under the system temporary folder)")
   ap.add_argument("--no-serving", action="store_true")
   ap.add_argument("--no-extra", action="store_true",
                   help="skip the single-system, neighbour-list and serving-sweep legs")
@@ -141,6 +141,9 @@ def parse():
   ap.add_argument("--serving-step-scale", type=float, default=0.05)
   ap.add_argument("--keep-atom-order", action="store_true",
                   help="store atoms in input order instead of the default spatial order")
+  ap.add_argument("--nlist-only", action="store_true",
+                  help="only build the neighbour list of the 20,000-atom globule at 20 + 2 A "
+                       "a few times (a short command for profiling the list build)")
   ap.add_argument("--segment", type=int, default=0,
                   help="tile work-item segment; 0 runs the autotuner")
   return ap.parse_args()
@@ -344,48 +347,65 @@ def plain_run(systems, stream, steps):
 
 
 def single_system_runs(stream, hbm_peak):
-  """The single-system configurations: N = 2,500 with CMAP and a 20 A cutoff
-  (neighbour list with 2 A skin), and the 20,000-atom globule all pairs and
-  at 20 A.  Device atom-steps/s of 50-step graph chunks, plus the
-  neighbour-list build (one pb2_nl_build, wall time around the call, which
-  includes its capacity check) with the bytes its rows and reference
-  positions write against the measured HBM bandwidth."""
+  """The single-system configurations.
+
+  * config 1: the 166-atom chain, all pairs, 1,000 BAOAB steps at 1 fs;
+  * config 2: N = 2,500 with CMAP and a 20 A cutoff, 2 A skin: the pair
+    kernels step from the block-pair list rebuilt on the device on the
+    half-skin rule, timed against the same run scanning every block pair
+    (``pair_list=False``);
+  * config 4: the 20,000-atom globule all pairs, and at 20 A (both ways).
+
+  Device atom-steps/s of 50-step graph chunks.  For each cutoff run, the
+  jax_md-layout neighbour list is built on the device: its device time
+  (CUDA events around the build's launches, the median of 10 builds) and
+  the bytes its rows write (every slot of every row) against the measured
+  HBM bandwidth."""
   import torch
   from prolix_b200 import engine, synth
+
+  def timed(b, steps):
+    b.langevin_init()
+    b.langevin_run(50, stream)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    b.langevin_run(steps, stream)
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
   out = {}
-  for name, n, cutoff, steps in (("n2500_cut20", 2500, 20.0, 200), ("n20000_all", 20000, 0.0, 50),
-                                 ("n20000_cut20", 20000, 20.0, 50)):
-    sd = synth.make_chain(n, 2500 if n == 2500 else 4242, compact=True, cmap=True,
-                          **synth.PHYSICAL_RANGES)
+  for name, n, cutoff, steps, seed, cmap in (
+      ("n166_all", 166, 0.0, 1000, 1, False), ("n2500_cut20", 2500, 20.0, 200, 2500, True),
+      ("n20000_all", 20000, 0.0, 50, 4242, True), ("n20000_cut20", 20000, 20.0, 50, 4242, True)):
+    sd = synth.make_chain(n, seed, compact=n > 166, cmap=cmap, **synth.PHYSICAL_RANGES)
     with engine.Batch([sd], cutoff=cutoff, skin=2.0) as b:
-      b.langevin_init()
-      b.langevin_run(50, stream)
-      torch.cuda.synchronize()
-      e0 = torch.cuda.Event(enable_timing=True)
-      e1 = torch.cuda.Event(enable_timing=True)
-      e0.record()
-      b.langevin_run(steps, stream)
-      e1.record()
-      torch.cuda.synchronize()
-      ms = e0.elapsed_time(e1)
+      ms = timed(b, steps)
       rec = {"atoms": n, "cutoff": cutoff, "steps": steps, "ms_per_step": ms / steps,
              "atom_steps_per_s": n * steps / (ms * 1e-3)}
       if cutoff > 0:
+        rec["pair_list"] = "block pairs within cutoff + 2 A skin, rebuilt on the device at skin/2"
         b.nl_build(stream)  # sizes the rows
         cap = b.nl_capacity()
-        reps = 10
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for _ in range(reps):
+        times = []
+        for _ in range(10):
           b.nl_build(stream)
-        torch.cuda.synchronize()
-        t = (time.perf_counter() - t0) / reps
-        nbytes = n * cap * 4 + n * 24  # rows + reference positions
+          times.append(b.nl_last_build_ms())
+        t = float(np.median(times)) * 1e-3
+        nbytes = n * cap * 4
         rec["nlist"] = {"capacity": cap, "build_ms": t * 1e3, "bytes_written": nbytes,
                         "achieved_gbs": nbytes / t / 1e9, "peak_gbs": hbm_peak,
                         "frac": nbytes / t / 1e9 / hbm_peak,
-                        "note": "wall time of pb2_nl_build incl. host-side grid setup and capacity check"}
-      out[name] = rec
+                        "note": "device time of the cell-list build's launches (CUDA events), "
+                                "median of 10; bytes = every slot of every row"}
+    if cutoff > 0:
+      with engine.Batch([sd], cutoff=cutoff, skin=2.0, pair_list=False) as b:
+        ms2 = timed(b, steps)
+      rec["without_pair_list"] = {"ms_per_step": ms2 / steps,
+                                  "atom_steps_per_s": n * steps / (ms2 * 1e-3)}
+    out[name] = rec
   return out
 
 
@@ -455,10 +475,26 @@ def serving_sweep(args):
   return res
 
 
+def nlist_only():
+  """Three device-side builds of the jax_md-layout list of the 20,000-atom
+  globule (cutoff 20 A, skin 2 A), each timed with CUDA events."""
+  from prolix_b200 import engine, synth
+  sd = synth.make_chain(20000, 4242, compact=True, cmap=True, **synth.PHYSICAL_RANGES)
+  with engine.Batch([sd], cutoff=20.0, skin=2.0) as b:
+    b.nl_build()
+    times = []
+    for _ in range(3):
+      b.nl_build()
+      times.append(b.nl_last_build_ms())
+    print(json.dumps({"nlist_build_ms": times, "capacity": b.nl_capacity()}))
+
+
 def main():
   args = parse()
   if args.impl == "reference":
     return run_reference(args)
+  if args.nlist_only:
+    return nlist_only()
   import torch
   from prolix_b200 import replicas
   ws, rank, local = replicas.env()
@@ -488,8 +524,10 @@ def main():
   flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
   ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
   ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-  clk_dir = args.clocks_dir or tempfile.gettempdir()
-  clk_path = os.path.join(clk_dir, f"clocks_rank{rank}.csv")
+  # a folder of this run's own unless one is given, so concurrent runs on a
+  # host never share a sample file
+  clk_dir = args.clocks_dir or tempfile.mkdtemp(prefix="pb2_clocks_")
+  clk_path = os.path.join(clk_dir, f"clocks_rank{rank}_{os.getpid()}.csv")
   os.makedirs(os.path.dirname(clk_path), exist_ok=True)
   clk = clocks_start(clk_path)
   replicas.barrier()
@@ -531,9 +569,12 @@ def main():
     passes[p] = {"ms": ms, "tflops": tf, "frac": (tf / peak if tf and peak else None),
                  "mufu_tops": mufu, "xu_frac": mufu / xu_peak if mufu else None}
   dom = max(("born", "force", "chain"), key=lambda p: per_kernel[p])
+  nominal = 128 * 2 * torch.cuda.get_device_properties(local).multi_processor_count * 1965e6 / 1e12
   roofline = {"kernel": f"tile_kernel pass '{dom}'", "bound": "fp32",
               "achieved": passes[dom]["tflops"], "peak": peak, "unit": "TFLOP/s",
               "frac": passes[dom]["frac"],
+              "frac_of_nominal": (passes[dom]["tflops"] / nominal if passes[dom]["tflops"] else None),
+              "nominal_peak": nominal,
               "traffic": TRAFFIC_BYTES.get(dom),
               "peak_source": "FP32 FMA throughput measured in this run (pb2_fp32_peak)",
               "xu_peak_tops": xu_peak,
@@ -651,7 +692,10 @@ def main():
         "cpu_baseline": cpu,
         "cpu_baseline_numpy": cpu_numpy,
         # per timed step: step, bbox, born, finalize, force, chain, bonded, finish
-        "gpu_launches": int(args.steps * 8),
+        # per timed step (a one-step graph): the step kernel (with the block
+        # boxes), the descreening (with the Born radii), force and chain (with
+        # the bonded terms) passes, and the closing half kick
+        "gpu_launches": int(args.steps * 5),
     }
     print(json.dumps(line), flush=True)
   if pg:

@@ -396,15 +396,18 @@ int pb2_get_warn_counts(pb2_batch *batch, int32_t *counts, int reset, void *stre
  * non-NULL it waits and *rebuilt receives how many systems had moved that
  * far, with rebuilt NULL it only enqueues (a list that outgrew its capacity
  * is flagged with PB2_STATUS_NLOVERFLOW and grown at the next pb2_nl_check
- * with rebuilt, pb2_nl_build or pb2_nl_get).  pb2_nl_get copies the
- * per-atom list in jax_md layout: (n_atoms_total, capacity) int32 local
- * indices, both (i, j) and (j, i) present, padded with the sentinel n_atoms
- * of the atom's system.  pb2_nl_last_build_ms: device time of the last
+ * with rebuilt, pb2_nl_build or pb2_nl_capacity).  pb2_nl_capacity waits
+ * for the device and reports the row width after any such growth.
+ * pb2_nl_get copies the per-atom list in jax_md layout into a buffer of that
+ * width: (n_atoms_total, capacity) int32 local indices, both (i, j) and
+ * (j, i) present, padded with the sentinel n_atoms of the atom's system; it
+ * returns PB2_ENLOVERFLOW, writing nothing, when a build queued after the
+ * capacity query needs wider rows.  pb2_nl_last_build_ms: device time of the last
  * build's launches (CUDA events; diagnostic, no reference counterpart).
  */
 int pb2_nl_build(pb2_batch *batch, void *stream);
 int pb2_nl_check(pb2_batch *batch, int32_t *rebuilt, void *stream);
-int pb2_nl_capacity(const pb2_batch *batch, int32_t *capacity);
+int pb2_nl_capacity(pb2_batch *batch, int32_t *capacity);
 int pb2_nl_get(pb2_batch *batch, int32_t *neighbors, void *stream);
 int pb2_nl_last_build_ms(pb2_batch *batch, double *ms);
 

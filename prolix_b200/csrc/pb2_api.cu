@@ -91,6 +91,13 @@ static PairArgs pair_args(pb2_batch *b) {
   a.pl_items0 = b->pl_items[0];
   a.pl_items1 = b->pl_items[1];
   a.pl_jlist = b->pl_jlist;
+  a.bonded = b->bonded;
+  a.n_bonded_chunks = 0;
+  a.sys_items = nullptr;
+  a.sys_done = b->sys_done;
+  a.fin = FinalizeArgs{};
+  a.pl_sys_items0 = b->pl_sys_items[0];
+  a.pl_sys_items1 = b->pl_sys_items[1];
   return a;
 }
 
@@ -105,6 +112,9 @@ static PlArgs pl_args(pb2_batch *b) {
   a.jlist = b->pl_jlist;
   a.items0 = b->pl_items[0];
   a.items1 = b->pl_items[1];
+  a.sys_items0 = b->pl_sys_items[0];
+  a.sys_items1 = b->pl_sys_items[1];
+  a.n_sys = b->n_sys;
   a.ctl = b->pl_ctl;
   a.reach2 = b->pl_reach2;
   a.seg = b->params.tile_segment;
@@ -139,6 +149,11 @@ static IntArgs int_args(pb2_batch *b, int parity, int finish_prev) {
   a.guard_end = b->guard_end;
   a.warn_flags = b->warn_flags;
   a.warn_counts = b->warn_counts;
+  a.blk_sys = b->blk_sys;
+  a.bbox = b->bbox;
+  a.n_blocks = b->n_blocks;
+  a.pl_ref = b->pl_on ? b->pl_ref : nullptr;
+  a.pl_ctl = b->pl_on ? b->pl_ctl : nullptr;
   return a;
 }
 
@@ -242,6 +257,15 @@ static int setup_items2(pb2_batch *b, int seg) {
   if (!items.empty())
     CUDA_TRY(ctx, cudaMemcpy(b->items2, items.data(), items.size() * sizeof(TileItem), cudaMemcpyHostToDevice));
   b->n_items2 = (int)items.size();
+  std::vector<int32_t> per_sys(b->n_sys, 0);
+  for (const TileItem &t : items) ++per_sys[t.sys];
+  if (!b->sys_items) {
+    b->sys_items = b->dev.alloc<int32_t>(b->n_sys);
+    b->sys_done = b->dev.alloc<int32_t>(b->n_sys);
+    if (!b->sys_items || !b->sys_done) return fail(ctx, PB2_ENOMEM, "work-item allocation failed");
+    CUDA_TRY(ctx, cudaMemset(b->sys_done, 0, b->n_sys * sizeof(int32_t)));
+  }
+  CUDA_TRY(ctx, cudaMemcpy(b->sys_items, per_sys.data(), per_sys.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
   for (int p = 0; p < 3; ++p) {
     const int cap = tile_kernel_occupancy(p, b->cut) * ctx->sm_count;
     const int w = tile_kernel_warps(p);
@@ -274,7 +298,10 @@ static int setup_pair_list(pb2_batch *b, int seg) {
     b->pl_jlist = D.alloc<int32_t>(std::max<size_t>(jcap, 1));
     b->pl_ctl = D.alloc<int32_t>(PL_WORDS);
     b->pl_ref = D.alloc<float4>(b->n_total);
-    if (!b->pl_rows || !b->pl_jlist || !b->pl_ctl || !b->pl_ref)
+    b->pl_sys_items[0] = D.alloc<int32_t>(b->n_sys);
+    b->pl_sys_items[1] = D.alloc<int32_t>(b->n_sys);
+    if (!b->pl_rows || !b->pl_jlist || !b->pl_ctl || !b->pl_ref || !b->pl_sys_items[0] ||
+        !b->pl_sys_items[1])
       return fail(ctx, PB2_ENOMEM, "pair-list allocation failed");
     CUDA_TRY(ctx, cudaMemcpy(b->pl_rows, rows.data(), rows.size() * sizeof(PlRow), cudaMemcpyHostToDevice));
     b->n_pl_rows = (int)rows.size();
@@ -289,6 +316,7 @@ static int setup_pair_list(pb2_batch *b, int seg) {
   }
   const int32_t ctl[PL_WORDS] = {1, 0, 0, 0, 0, 0, 0, 0};  // dirty: rebuild at the next evaluation
   CUDA_TRY(ctx, cudaMemcpy(b->pl_ctl, ctl, sizeof ctl, cudaMemcpyHostToDevice));
+  for (auto p : b->pl_sys_items) CUDA_TRY(ctx, cudaMemset(p, 0, b->n_sys * sizeof(int32_t)));
   b->grid_pl = std::max(1, std::min(8 * ctx->sm_count, (b->n_pl_rows + 7) / 8));
   return PB2_OK;
 }
@@ -861,13 +889,15 @@ struct Timer {
 
 // Force kernels on the current posq; force accumulators must be zero (or
 // hold contributions to keep) and born_acc zero.  bonded_energy: also
-// accumulate the (FP64) bonded energies.
-static cudaError_t enqueue_forces(pb2_batch *b, cudaStream_t st, bool bonded_energy) {
+// accumulate the (FP64) bonded energies.  boxes_ready: the step kernel just
+// wrote the block boxes (and ran the pair list's displacement test).
+static cudaError_t enqueue_forces(pb2_batch *b, cudaStream_t st, bool bonded_energy,
+                                  bool boxes_ready = false) {
   cudaError_t e;
   Timer tm{b, st};
   PairArgs pa = pair_args(b);
   const bool gb = (b->params.terms & PB2_USE_GB) != 0;
-  if ((e = tm(kTimBbox, [&] {
+  if (!boxes_ready && (e = tm(kTimBbox, [&] {
          return launch_bbox(b->sys, b->blk_sys, b->posq, b->bbox, b->n_blocks, st,
                             b->pl_on ? b->pl_ref : nullptr, b->pl_on ? b->pl_ctl : nullptr);
        })) != cudaSuccess)
@@ -875,9 +905,6 @@ static cudaError_t enqueue_forces(pb2_batch *b, cudaStream_t st, bool bonded_ene
   if (b->pl_on && (e = tm(kTimBbox, [&] { return launch_pl_update(pl_args(b), b->grid_pl, st); })) != cudaSuccess)
     return e;
   if (gb) {
-    pa.sched = b->sched + 2 * PASS_BORN;
-    if ((e = tm(kTimBorn, [&] { return launch_tiles(PASS_BORN, pa, b->grid_pair[PASS_BORN], st); })) != cudaSuccess)
-      return e;
     FinalizeArgs fa;
     fa.sys = b->sys;
     fa.atom_sys = b->atom_sys;
@@ -890,17 +917,39 @@ static cudaError_t enqueue_forces(pb2_batch *b, cudaStream_t st, bool bonded_ene
     fa.born64 = nullptr;
     fa.n_total = b->n_total;
     fa.energy_mode = 0;
-    if ((e = tm(kTimFinalize, [&] { return launch_born_finalize(fa, st); })) != cudaSuccess) return e;
+    // the descreening pass finalizes each system as its last item completes
+    // (profiling keeps the separate launch, to time it)
+    const bool fuse_finalize = !b->profiling;
+    PairArgs pb = pa;
+    pb.sched = b->sched + 2 * PASS_BORN;
+    if (fuse_finalize) {
+      pb.sys_items = b->sys_items;
+      pb.fin = fa;
+    }
+    if ((e = tm(kTimBorn, [&] { return launch_tiles(PASS_BORN, pb, b->grid_pair[PASS_BORN], st); })) != cudaSuccess)
+      return e;
+    if (!fuse_finalize &&
+        (e = tm(kTimFinalize, [&] { return launch_born_finalize(fa, st); })) != cudaSuccess)
+      return e;
   }
   pa.sched = b->sched + 2 * PASS_FORCE;
   if ((e = tm(kTimForce, [&] { return launch_tiles(PASS_FORCE, pa, b->grid_pair[PASS_FORCE], st); })) != cudaSuccess)
     return e;
   pa.sched = b->sched + 2 * PASS_CHAIN;
+  BondedArgs ba = b->bonded;
+  ba.energy_mode = bonded_energy ? 1 : 0;
+  const int n_bonded = ba.n_bond + ba.n_angle + ba.n_tors + ba.n_cmap + ba.n_exc;
+  // the bonded terms ride along as the chain pass's tail work, except when
+  // their energies are wanted or there is no chain pass
+  const bool fuse_bonded = gb && !bonded_energy && !b->profiling;
+  if (fuse_bonded) {
+    pa.bonded = ba;
+    pa.n_bonded_chunks = (n_bonded + kBondedChunk - 1) / kBondedChunk;
+  }
   if (gb)
     if ((e = tm(kTimChain, [&] { return launch_tiles(PASS_CHAIN, pa, b->grid_pair[PASS_CHAIN], st); })) != cudaSuccess)
       return e;
-  BondedArgs ba = b->bonded;
-  ba.energy_mode = bonded_energy ? 1 : 0;
+  if (fuse_bonded) return cudaSuccess;
   return tm(kTimBonded, [&] { return launch_bonded(ba, b->grid_bonded, st); });
 }
 
@@ -1062,7 +1111,7 @@ static int run_eager(pb2_batch *b, int n_steps, cudaStream_t st) {
   for (int t = 0; t < n_steps; ++t) {
     const IntArgs ia = int_args(b, b->key_parity, t > 0);
     CUDA_TRY(ctx, tm(kTimStep, [&] { return launch_step(ia, st); }));
-    CUDA_TRY(ctx, enqueue_forces(b, st, false));
+    CUDA_TRY(ctx, enqueue_forces(b, st, false, true));
     b->key_parity ^= 1;
   }
   const IntArgs fa = int_args(b, b->key_parity, 0);
@@ -1084,7 +1133,7 @@ static int get_graph(pb2_batch *b, int chunk, int parity, cudaGraphExec_t *out) 
   int p = parity;
   for (int t = 0; t < chunk && err == cudaSuccess; ++t) {
     err = launch_step(int_args(b, p, t > 0), cs);
-    if (err == cudaSuccess) err = enqueue_forces(b, cs, false);
+    if (err == cudaSuccess) err = enqueue_forces(b, cs, false, true);
     p ^= 1;
   }
   if (err == cudaSuccess) err = launch_finish(int_args(b, p, 0), cs);

@@ -12,9 +12,10 @@
 //
 // Kernel boundaries: step_kernel applies the final half kick of the
 // previous step (when finish_prev), the first half kick, A, O, A of the new
-// step, converts the new positions for the float32 pair kernels and clears
-// the force accumulators; the force kernels then run; finish_kernel applies
-// the last half kick of a chunk.  Keys live in two buffers: a step reads
+// step, converts the new positions for the float32 pair kernels, writes the
+// 32-atom blocks' bounding boxes and clears the force accumulators; the
+// force kernels then run; finish_kernel applies the last half kick of a
+// chunk.  Keys live in two buffers: a step reads
 // buffer `parity` and writes the advanced key to the other.
 #include "pb2_common.cuh"
 #include "pb2_kernels.cuh"
@@ -29,15 +30,46 @@ __device__ __forceinline__ void check_fix(const IntArgs &a, int s, long long v) 
   if (v == LLONG_MAX || v == LLONG_MIN) atomicOr(&a.status[s], (uint32_t)PB2_STATUS_FORCE_RANGE);
 }
 
-__device__ __forceinline__ void write_posq(const IntArgs &a, int i, const SysInfo &S, double x,
-                                           double y, double z) {
-  a.posq[i] = make_float4((float)(x - S.ox), (float)(y - S.oy), (float)(z - S.oz), (float)a.charge[i]);
+__device__ __forceinline__ float4 write_posq(const IntArgs &a, int i, const SysInfo &S, double x,
+                                             double y, double z) {
+  const float4 q = make_float4((float)(x - S.ox), (float)(y - S.oy), (float)(z - S.oz), (float)a.charge[i]);
+  a.posq[i] = q;
+  return q;
 }
 
-__global__ void step_kernel(const IntArgs a) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_total; i += gridDim.x * blockDim.x) {
-    const int s = a.atom_sys[i];
-    const SysInfo &S = a.sys[s];
+// The step kernels map one warp to one 32-atom block (lane l: atom l of the
+// block), so that the block's bounding box of the new positions -- what the
+// pair kernels cull tiles by -- comes out of the same launch, and so does
+// the pair list's displacement test.  Lanes past a system's last atom take
+// the block's first atom for the box.
+__device__ __forceinline__ void block_box(const IntArgs &a, int b, int lane, bool valid, float4 q) {
+  const float4 q0 = make_float4(__shfl_sync(kFull, q.x, 0), __shfl_sync(kFull, q.y, 0),
+                                __shfl_sync(kFull, q.z, 0), 0.f);
+  if (!valid) q = q0;
+  float lo[3] = {q.x, q.y, q.z}, hi[3] = {q.x, q.y, q.z};
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      lo[c] = fminf(lo[c], __shfl_xor_sync(kFull, lo[c], o));
+      hi[c] = fmaxf(hi[c], __shfl_xor_sync(kFull, hi[c], o));
+    }
+  if (lane == 0) {
+    a.bbox[2 * b] = make_float4(lo[0], lo[1], lo[2], 0.f);
+    a.bbox[2 * b + 1] = make_float4(hi[0], hi[1], hi[2], 0.f);
+  }
+}
+
+__device__ __forceinline__ bool moved_past_half_skin(const IntArgs &a, int i, const SysInfo &S, float4 q) {
+  if (!a.pl_ref) return false;
+  const float4 r = a.pl_ref[i];
+  const float dx = q.x - r.x, dy = q.y - r.y, dz = q.z - r.z;
+  return (double)fmaf(dx, dx, fmaf(dy, dy, dz * dz)) > S.skin_half2;
+}
+
+// One atom's plain BAOAB step; returns the float32 position it wrote.
+__device__ __forceinline__ float4 step_atom(const IntArgs &a, int i, int s, const SysInfo &S) {
+  {
     const int loc = i - S.off;
     const int rnd = a.user[i] - S.off;  // the atom's index in the caller's order: its noise
     const double h = S.half_dt;
@@ -64,7 +96,7 @@ __global__ void step_kernel(const IntArgs a) {
     }
     a.px[i] = p[0]; a.py[i] = p[1]; a.pz[i] = p[2];
     a.x[i] = x[0]; a.y[i] = x[1]; a.z[i] = x[2];
-    write_posq(a, i, S, x[0], x[1], x[2]);
+    const float4 q = write_posq(a, i, S, x[0], x[1], x[2]);
     if (!(isfinite(x[0]) && isfinite(x[1]) && isfinite(x[2]) && isfinite(p[0]) &&
           isfinite(p[1]) && isfinite(p[2])))
       atomicOr(&a.status[s], (uint32_t)PB2_STATUS_NONFINITE);
@@ -74,7 +106,28 @@ __global__ void step_kernel(const IntArgs a) {
       kout[1] = knew[1];
       a.steps[s] += 1;
     }
+    return q;
   }
+}
+
+__global__ void step_kernel(const IntArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int nw = (int)((gridDim.x * blockDim.x) >> 5);
+  bool moved = false;
+  for (int b = w; b < a.n_blocks; b += nw) {
+    const int s = a.blk_sys[b];
+    const SysInfo &S = a.sys[s];
+    const int l = (b - S.blk_base) * 32 + lane;
+    const bool valid = l < S.n;
+    float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (valid) {
+      q = step_atom(a, S.off + l, s, S);
+      moved |= moved_past_half_skin(a, S.off + l, S, q);
+    }
+    block_box(a, b, lane, valid, q);
+  }
+  if (a.pl_ctl && __any_sync(kFull, moved) && lane == 0) atomicOr(&a.pl_ctl[PL_DIRTY], 1);
 }
 
 // Safeguarded step: prolix's batched Langevin step (batched_simulate.py:218-382)
@@ -115,11 +168,10 @@ __device__ __forceinline__ void fold_warns(const IntArgs &a, int s) {
   }
 }
 
-__global__ void step_guarded_kernel(const IntArgs a) {
-  const bool cap_open = a.finish_prev || *a.guard_end;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_total; i += gridDim.x * blockDim.x) {
-    const int s = a.atom_sys[i];
-    const SysInfo &S = a.sys[s];
+// One atom's safeguarded step; returns the float32 position it wrote.
+__device__ __forceinline__ float4 step_guarded_atom(const IntArgs &a, int i, int s, const SysInfo &S,
+                                                    bool cap_open) {
+  {
     const int loc = i - S.off;
     const int rnd = a.user[i] - S.off;
     const double h = S.half_dt;
@@ -174,7 +226,7 @@ __global__ void step_guarded_kernel(const IntArgs a) {
     }
     a.px[i] = p[0]; a.py[i] = p[1]; a.pz[i] = p[2];
     a.x[i] = x[0]; a.y[i] = x[1]; a.z[i] = x[2];
-    write_posq(a, i, S, x[0], x[1], x[2]);
+    const float4 q = write_posq(a, i, S, x[0], x[1], x[2]);
     if (!(isfinite(x[0]) && isfinite(x[1]) && isfinite(x[2]) && isfinite(p[0]) &&
           isfinite(p[1]) && isfinite(p[2])))
       atomicOr(&a.status[s], (uint32_t)PB2_STATUS_NONFINITE);
@@ -186,7 +238,29 @@ __global__ void step_guarded_kernel(const IntArgs a) {
       a.steps[s] += 1;
       fold_warns(a, s);
     }
+    return q;
   }
+}
+
+__global__ void step_guarded_kernel(const IntArgs a) {
+  const bool cap_open = a.finish_prev || *a.guard_end;
+  const int lane = threadIdx.x & 31;
+  const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int nw = (int)((gridDim.x * blockDim.x) >> 5);
+  bool moved = false;
+  for (int b = w; b < a.n_blocks; b += nw) {
+    const int s = a.blk_sys[b];
+    const SysInfo &S = a.sys[s];
+    const int l = (b - S.blk_base) * 32 + lane;
+    const bool valid = l < S.n;
+    float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (valid) {
+      q = step_guarded_atom(a, S.off + l, s, S, cap_open);
+      moved |= moved_past_half_skin(a, S.off + l, S, q);
+    }
+    block_box(a, b, lane, valid, q);
+  }
+  if (a.pl_ctl && __any_sync(kFull, moved) && lane == 0) atomicOr(&a.pl_ctl[PL_DIRTY], 1);
 }
 
 __global__ void finish_guarded_kernel(const IntArgs a) {
@@ -312,10 +386,12 @@ static int grid_for(int n) {
 static bool guarded(const IntArgs &a) { return a.vlimit > 0.0 || a.max_dx > 0.0 || a.force_cap > 0.0; }
 
 cudaError_t launch_step(const IntArgs &a, cudaStream_t st) {
+  const int grid = (a.n_blocks + 7) / 8;  // 8 warps, one 32-atom block each
+  if (grid <= 0) return cudaSuccess;
   if (guarded(a))
-    step_guarded_kernel<<<grid_for(a.n_total), 256, 0, st>>>(a);
+    step_guarded_kernel<<<grid, 256, 0, st>>>(a);
   else
-    step_kernel<<<grid_for(a.n_total), 256, 0, st>>>(a);
+    step_kernel<<<grid, 256, 0, st>>>(a);
   return cudaGetLastError();
 }
 cudaError_t launch_finish(const IntArgs &a, cudaStream_t st) {

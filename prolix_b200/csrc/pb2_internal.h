@@ -102,6 +102,8 @@ struct pb2_batch {
   int n_items = 0;
   TileItem *items2 = nullptr;  // pair kernels: items over pairs of i-blocks
   int n_items2 = 0;
+  int32_t *sys_items = nullptr;  // items2 per system (the descreening pass's completion count)
+  int32_t *sys_done = nullptr;   // items of each system completed in the current pass
   int2 *excl_ent = nullptr;
   ExclRow *excl_rows = nullptr;
   BondedArgs bonded{};
@@ -141,6 +143,7 @@ struct pb2_batch {
   int n_pl_rows = 0;
   int32_t *pl_jlist = nullptr;
   TileItem *pl_items[2] = {nullptr, nullptr};
+  int32_t *pl_sys_items[2] = {nullptr, nullptr};
   size_t pl_item_cap = 0;
   int32_t *pl_ctl = nullptr;
   float4 *pl_ref = nullptr;

@@ -9,72 +9,6 @@ namespace pb2 {
 // Record a message as the context's last error (ctx may be NULL); returns code.
 int set_error(pb2_ctx *ctx, int code, const char *msg);
 
-enum { PASS_BORN = 0, PASS_FORCE = 1, PASS_CHAIN = 2 };
-struct PairArgs {
-  const SysInfo *sys;
-  const TileItem *items;
-  int32_t n_items;
-  uint32_t terms;
-  const int2 *excl_ent;
-  const ExclRow *excl_rows;
-  const float4 *posq;
-  const float4 *par;
-  const float4 *born;
-  const float4 *bbox;       // per global block: (lo, hi) of the float32 positions
-  long long *born_acc;
-  long long *dedb_acc;
-  long long *fx, *fy, *fz;
-  long long *energy;
-  int32_t cut;              // any cutoff active
-  int32_t *sched;           // (next item, finished warps) of this pass; zero between launches
-  // pair list (cutoff runs; NULL otherwise): items come from pl_items[pl_ctl[1]],
-  // pl_ctl[2 + pl_ctl[1]] of them, and an item's tiles t in [jb0, jb1) are
-  // the j-blocks pl_jlist[t]
-  const int32_t *pl_ctl;
-  const TileItem *pl_items0, *pl_items1;
-  const int32_t *pl_jlist;
-};
-// Pair-list control words (PlArgs::ctl)
-enum { PL_DIRTY = 0, PL_CUR = 1, PL_COUNT0 = 2, PL_COUNT1 = 3, PL_NEW = 4, PL_DONE = 5, PL_WORDS = 8 };
-struct PlArgs {
-  const SysInfo *sys;
-  const PlRow *rows;
-  int32_t n_rows;
-  const float4 *bbox;
-  const float4 *posq;
-  float4 *ref;           // positions at the last build (displacement reference)
-  int32_t *jlist;
-  TileItem *items0, *items1;
-  int32_t *ctl;
-  float reach2;          // (largest pair-term cutoff + skin)^2
-  int32_t seg;           // tiles per work item
-};
-struct FinalizeArgs {
-  const SysInfo *sys;
-  const int32_t *atom_sys;
-  const double *radius;
-  const double *charge;
-  long long *born_acc;
-  float4 *born;
-  long long *dedb_acc;
-  long long *energy;
-  double *born64;   // NULL, or FP64 Born radii out
-  int32_t n_total;
-  int32_t energy_mode;
-};
-struct Energy64Args {
-  const SysInfo *sys;
-  const TileItem *items;
-  int32_t n_items;
-  uint32_t terms;
-  const int2 *excl_ent;
-  const ExclRow *excl_rows;
-  const double *x, *y, *z;
-  const double *q, *hs, *se, *ro, *sr;  // charge, sigma/2, sqrt(eps), rho~, scaled radius
-  const double *born64;
-  long long *born_acc;
-  long long *energy;
-};
 // torsion-list entry kinds (BondedArgs::tors_par .w)
 constexpr double kTorsProper = 0.0, kTorsImproper = 1.0, kTorsHarmonic = 2.0;
 struct BondedArgs {
@@ -104,6 +38,88 @@ struct BondedArgs {
   const int2 *exc_idx;
   const double4 *exc_par;  // (k_coulomb * charge product, sigma, epsilon, 0)
 };
+enum { PASS_BORN = 0, PASS_FORCE = 1, PASS_CHAIN = 2 };
+struct FinalizeArgs {
+  const SysInfo *sys;
+  const int32_t *atom_sys;
+  const double *radius;
+  const double *charge;
+  long long *born_acc;
+  float4 *born;
+  long long *dedb_acc;
+  long long *energy;
+  double *born64;   // NULL, or FP64 Born radii out
+  int32_t n_total;
+  int32_t energy_mode;
+};
+struct PairArgs {
+  const SysInfo *sys;
+  const TileItem *items;
+  int32_t n_items;
+  uint32_t terms;
+  const int2 *excl_ent;
+  const ExclRow *excl_rows;
+  const float4 *posq;
+  const float4 *par;
+  const float4 *born;
+  const float4 *bbox;       // per global block: (lo, hi) of the float32 positions
+  long long *born_acc;
+  long long *dedb_acc;
+  long long *fx, *fy, *fz;
+  long long *energy;
+  int32_t cut;              // any cutoff active
+  int32_t *sched;           // (next item, finished warps) of this pass; zero between launches
+  // pair list (cutoff runs; NULL otherwise): items come from pl_items[pl_ctl[1]],
+  // pl_ctl[2 + pl_ctl[1]] of them, and an item's tiles t in [jb0, jb1) are
+  // the j-blocks pl_jlist[t]
+  const int32_t *pl_ctl;
+  const TileItem *pl_items0, *pl_items1;
+  const int32_t *pl_jlist;
+  // chain pass: after its tiles, the warps take the bonded terms in chunks
+  // of kBondedChunk (0 chunks: the bonded kernel runs on its own)
+  BondedArgs bonded;
+  int32_t n_bonded_chunks;
+  // descreening pass: with sys_items set, the warp that completes a
+  // system's sys_items[s]-th item finalizes its Born radii (fin); sys_done
+  // counts completed items and is reset by that warp
+  const int32_t *sys_items;
+  int32_t *sys_done;
+  FinalizeArgs fin;
+  const int32_t *pl_sys_items0, *pl_sys_items1;  // per-system item counts of the pair list's buffers
+};
+constexpr int kBondedChunk = 256;
+// Pair-list control words (PlArgs::ctl)
+enum { PL_DIRTY = 0, PL_CUR = 1, PL_COUNT0 = 2, PL_COUNT1 = 3, PL_NEW = 4, PL_DONE = 5, PL_WORDS = 8 };
+struct PlArgs {
+  const SysInfo *sys;
+  const PlRow *rows;
+  int32_t n_rows;
+  const float4 *bbox;
+  const float4 *posq;
+  float4 *ref;           // positions at the last build (displacement reference)
+  int32_t *jlist;
+  TileItem *items0, *items1;
+  int32_t *sys_items0, *sys_items1;  // per-system item counts of each buffer
+  int32_t n_sys;
+  int32_t *ctl;
+  float reach2;          // (largest pair-term cutoff + skin)^2
+  int32_t seg;           // tiles per work item
+};
+
+struct Energy64Args {
+  const SysInfo *sys;
+  const TileItem *items;
+  int32_t n_items;
+  uint32_t terms;
+  const int2 *excl_ent;
+  const ExclRow *excl_rows;
+  const double *x, *y, *z;
+  const double *q, *hs, *se, *ro, *sr;  // charge, sigma/2, sqrt(eps), rho~, scaled radius
+  const double *born64;
+  long long *born_acc;
+  long long *energy;
+};
+
 struct NlGrid {        // per-system cell grid of the neighbour-list build (written on the device)
   float x0, y0, z0, inv_cell;
   int32_t nx, ny, nz;
@@ -161,6 +177,14 @@ struct IntArgs {
   int32_t *guard_end;     // 1: the force accumulators hold a step's closing force
   uint32_t *warn_flags;   // (2, n_sys) caps that fired, by key parity; kWarnBit*
   int32_t *warn_counts;   // (n_sys, 4) in prolix's warn order (typing.py:559-563)
+  // the step kernels also write the block bounding boxes of the new
+  // positions (one warp per 32-atom block) and, with a pair list, raise its
+  // rebuild flag when an atom moved more than skin/2 from pl_ref
+  const int32_t *blk_sys;
+  float4 *bbox;
+  int32_t n_blocks;
+  const float4 *pl_ref;
+  int32_t *pl_ctl;
 };
 // warn_counts columns (prolix typing.py:559-563) and their warn_flags bits
 enum { kWarnVlimit = 0, kWarnForceCap = 1, kWarnConstr = 2, kWarnDxCap = 3, kWarnTypes = 4 };

@@ -495,9 +495,18 @@ extern "C" int pb2_nl_check(pb2_batch *b, int32_t *rebuilt, void *stream) {
   return PB2_OK;
 }
 
-extern "C" int pb2_nl_capacity(const pb2_batch *b, int32_t *capacity) {
+extern "C" int pb2_nl_capacity(pb2_batch *b, int32_t *capacity) {
   if (!b || !capacity) return PB2_EINVAL;
-  *capacity = b->nl_built ? b->nl_capacity : 0;
+  pb2_ctx *ctx = b->ctx;
+  *capacity = 0;
+  if (!b->nl_built) return PB2_OK;
+  // a host visit: a build an asynchronous check queued may have outgrown the
+  // rows; grow them now, before the caller sizes its buffer
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  CUDA_TRY(ctx, cudaDeviceSynchronize());
+  int rc = nl_settle(b, nullptr);
+  if (rc) return rc;
+  *capacity = b->nl_capacity;
   return PB2_OK;
 }
 
@@ -517,8 +526,14 @@ extern "C" int pb2_nl_get(pb2_batch *b, int32_t *neighbors, void *stream) {
   pb2_ctx *ctx = b->ctx;
   if (!b->nl_built) return fail(ctx, PB2_EINVAL, "no neighbour list built yet");
   cudaStream_t st = (cudaStream_t)stream;
-  int rc = nl_settle(b, st);  // a build queued by an asynchronous check may have outgrown the rows
-  if (rc) return rc;
+  // the caller's buffer has the capacity pb2_nl_capacity reported; a build
+  // queued since then that needs more rows is reported, not written
+  int32_t maxc = 0;
+  CUDA_TRY(ctx, cudaMemcpyAsync(&maxc, b->nl_ctl + NL_MAXCOUNT, sizeof maxc, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  if (maxc > b->nl_capacity)
+    return fail(ctx, PB2_ENLOVERFLOW, "the neighbour list outgrew its capacity: call pb2_nl_capacity "
+                                      "(which grows it) and pass a buffer of that width");
   const size_t cap = (size_t)b->nl_capacity;
   std::vector<int> rows((size_t)b->n_total * cap);
   CUDA_TRY(ctx, cudaMemcpyAsync(rows.data(), b->nl_rows, rows.size() * sizeof(int), cudaMemcpyDeviceToHost, st));

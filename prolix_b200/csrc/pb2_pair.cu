@@ -31,6 +31,7 @@
 // scheduling order.
 #include <algorithm>
 
+#include "pb2_bonded.cuh"
 #include "pb2_common.cuh"
 #include "pb2_kernels.cuh"
 #include "pb2_obc_series.cuh"
@@ -478,6 +479,52 @@ __device__ __forceinline__ void run_bc_tile2(const PData2 &I, const JTile &jt, A
   }
 }
 
+// One atom's Born radius from its descreening sum, and the per-atom GB
+// self term and ACE as the initial dE/dB; clears the sum.
+__device__ __forceinline__ void finalize_atom(const FinalizeArgs &a, int i, int s, const SysInfo &S) {
+  const bool nl = S.clamp != 0;
+  const double isum = (double)__ldcg(&a.born_acc[i]) * kBornInv;
+  a.born_acc[i] = 0;
+  const double r_in = a.radius[i];
+  const double rad = nl ? fmax(r_in, 1e-6) : r_in;
+  double ro = rad - kDielOffset;
+  if (nl) ro = fmax(ro, 1e-4);
+  const double psi = ro * isum;
+  const double arg = kObcAlpha * psi - kObcBeta * psi * psi + kObcGamma * psi * psi * psi;
+  const double th = tanh(arg);
+  const double dr = nl ? fmax(rad, 1e-4) : rad;
+  double inv_b = 1.0 / ro - th / dr;
+  bool clamped = false;
+  if (nl && inv_b < 1e-4) {
+    inv_b = 1e-4;
+    clamped = true;
+  }
+  const double B = 1.0 / inv_b;
+  const double dpsi = (kObcAlpha - 2.0 * kObcBeta * psi + 3.0 * kObcGamma * psi * psi) * ro;
+  const double dbdi = clamped ? 0.0 : B * B * (1.0 - th * th) / dr * dpsi;
+  a.born[i] = make_float4((float)B, (float)inv_b, (float)dbdi, 0.f);
+  if (a.born64) a.born64[i] = B;
+  const double q = a.charge[i];
+  const double r_nm = (r_in - kDielOffset) / 10.0 + 0.009;
+  const double x = r_nm / (B / 10.0);
+  const double x3 = x * x * x;
+  const double ace = kAceCoeff * (r_nm + 0.14) * (r_nm + 0.14) * x3 * x3 * kKjToKcal;
+  const double dedb = -S.pref_d * q * q * inv_b * inv_b - 6.0 * ace * inv_b;
+  a.dedb_acc[i] = to_fix(dedb, kForceScale);
+  if (a.energy_mode) {
+    long long *e = a.energy + (size_t)s * PB2_NTERMS;
+    atomic_add_fix(&e[PB2_TERM_GB], to_fix(S.pref_d * q * q * inv_b, kEnergyScale));
+    atomic_add_fix(&e[PB2_TERM_NONPOLAR], to_fix(ace, kEnergyScale));
+  }
+}
+
+__global__ void born_finalize(const FinalizeArgs a) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_total; i += gridDim.x * blockDim.x) {
+    const int s = a.atom_sys[i];
+    finalize_atom(a, i, s, a.sys[s]);
+  }
+}
+
 // ------------------------------------------------------------------- kernel
 
 // One warp per work item (system, even i-block ib, j-blocks [jb0, jb1)):
@@ -516,7 +563,7 @@ template <int PASS>
 constexpr int kTileMinBlocks = PASS == PASS_BORN ? PB2_MINB_BORN : (PASS == PASS_CHAIN ? PB2_MINB_CHAIN : PB2_MINB_FORCE);
 template <int PASS, bool CUT, bool ALL = false>
 __global__ void __launch_bounds__(kTileThreads<PASS>, kTileMinBlocks<PASS>)
-    tile2_kernel(const PairArgs a) {
+    tile2_kernel(const __grid_constant__ PairArgs a) {
   const int lane = threadIdx.x & 31;
   const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
   TileConst K;
@@ -544,16 +591,29 @@ __global__ void __launch_bounds__(kTileThreads<PASS>, kTileMinBlocks<PASS>)
   const bool plm = CUT && a.pl_ctl != nullptr;
   const TileItem *items = a.items;
   int n_items = a.n_items;
+  const int32_t *sys_items = a.sys_items;
   if (plm) {
     const int cur = a.pl_ctl[PL_CUR];
     items = cur ? a.pl_items1 : a.pl_items0;
     n_items = a.pl_ctl[PL_COUNT0 + cur];
+    if (sys_items) sys_items = cur ? a.pl_sys_items1 : a.pl_sys_items0;
   }
   for (;;) {
     int it = 0;
     if (lane == 0) it = atomicAdd(&a.sched[0], 1);
     it = __shfl_sync(kFull, it, 0);
-    if (it >= n_items) break;
+    if (it >= n_items) {
+      if constexpr (PASS == PASS_CHAIN) {
+        // tail work: a chunk of the bonded terms (FP64, their own forces)
+        const int c = it - n_items;
+        if (c < a.n_bonded_chunks) {
+          const int t1 = min((c + 1) * kBondedChunk, bonded_total(a.bonded));
+          for (int t = c * kBondedChunk + lane; t < t1; t += 32) bonded_term(a.bonded, t);
+          continue;
+        }
+      }
+      break;
+    }
     const TileItem item = items[it];
     const SysInfo &S = a.sys[item.sys];
     const int n = S.n, off = S.off;
@@ -693,6 +753,22 @@ __global__ void __launch_bounds__(kTileThreads<PASS>, kTileMinBlocks<PASS>)
     if (PASS == PASS_BORN) {
       if (iv0 && p0 != 0) atomic_add_fix(&a.born_acc[ig0], p0);
       if (iv1 && q0 != 0) atomic_add_fix(&a.born_acc[ig1], q0);
+      if (sys_items) {
+        // the warp that completes a system's last item turns its sums into
+        // Born radii: first its queued closed-form pairs, which may belong
+        // to this item, then a release fence before the count
+        if (Q.n > 0) cf_drain<PASS>(Q, lane);
+        __threadfence();
+        __syncwarp();
+        int last = 0;
+        if (lane == 0) last = atomicAdd(&a.sys_done[item.sys], 1) == sys_items[item.sys] - 1;
+        if (__shfl_sync(kFull, last, 0)) {
+          __threadfence();
+#pragma unroll 4
+          for (int l = lane; l < n; l += 32) finalize_atom(a.fin, off + l, item.sys, S);
+          if (lane == 0) a.sys_done[item.sys] = 0;  // ready for the next launch
+        }
+      }
     } else {
       if (iv0) {
         atomic_add_fix(&a.fx[ig0], p0); atomic_add_fix(&a.fy[ig0], p1); atomic_add_fix(&a.fz[ig0], p2);
@@ -753,46 +829,6 @@ __global__ void bbox_kernel(const SysInfo *sys, const int32_t *blk_sys, const fl
 // (:600-648), written as the initial value of dE/dB.  Clears the sums.
 // FP64: one evaluation per atom.
 
-__global__ void born_finalize(const FinalizeArgs a) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_total; i += gridDim.x * blockDim.x) {
-    const int s = a.atom_sys[i];
-    const SysInfo &S = a.sys[s];
-    const bool nl = S.clamp != 0;
-    const double isum = (double)a.born_acc[i] * kBornInv;
-    a.born_acc[i] = 0;
-    const double r_in = a.radius[i];
-    const double rad = nl ? fmax(r_in, 1e-6) : r_in;
-    double ro = rad - kDielOffset;
-    if (nl) ro = fmax(ro, 1e-4);
-    const double psi = ro * isum;
-    const double arg = kObcAlpha * psi - kObcBeta * psi * psi + kObcGamma * psi * psi * psi;
-    const double th = tanh(arg);
-    const double dr = nl ? fmax(rad, 1e-4) : rad;
-    double inv_b = 1.0 / ro - th / dr;
-    bool clamped = false;
-    if (nl && inv_b < 1e-4) {
-      inv_b = 1e-4;
-      clamped = true;
-    }
-    const double B = 1.0 / inv_b;
-    const double dpsi = (kObcAlpha - 2.0 * kObcBeta * psi + 3.0 * kObcGamma * psi * psi) * ro;
-    const double dbdi = clamped ? 0.0 : B * B * (1.0 - th * th) / dr * dpsi;
-    a.born[i] = make_float4((float)B, (float)inv_b, (float)dbdi, 0.f);
-    if (a.born64) a.born64[i] = B;
-    const double q = a.charge[i];
-    const double r_nm = (r_in - kDielOffset) / 10.0 + 0.009;
-    const double x = r_nm / (B / 10.0);
-    const double x3 = x * x * x;
-    const double ace = kAceCoeff * (r_nm + 0.14) * (r_nm + 0.14) * x3 * x3 * kKjToKcal;
-    const double dedb = -S.pref_d * q * q * inv_b * inv_b - 6.0 * ace * inv_b;
-    a.dedb_acc[i] = to_fix(dedb, kForceScale);
-    if (a.energy_mode) {
-      long long *e = a.energy + (size_t)s * PB2_NTERMS;
-      atomic_add_fix(&e[PB2_TERM_GB], to_fix(S.pref_d * q * q * inv_b, kEnergyScale));
-      atomic_add_fix(&e[PB2_TERM_NONPOLAR], to_fix(ace, kEnergyScale));
-    }
-  }
-}
 
 // --------------------------------------------------------------- launchers
 

@@ -68,24 +68,34 @@ __global__ void pl_update_kernel(const PlArgs a) {
     }
     const int nit = (cnt + a.seg - 1) / a.seg;
     int base = 0;
-    if (lane == 0 && nit > 0) base = atomicAdd(&a.ctl[PL_NEW], nit);
+    if (lane == 0 && nit > 0) {
+      base = atomicAdd(&a.ctl[PL_NEW], nit);
+      atomicAdd(&(nxt ? a.sys_items1 : a.sys_items0)[row.sys], nit);
+    }
     base = __shfl_sync(kFull, base, 0);
     for (int k = lane; k < nit; k += 32)
       out[base + k] = TileItem{row.sys, ib, row.jbase + k * a.seg, row.jbase + min((k + 1) * a.seg, cnt)};
   }
-  // the last warp publishes the new list and clears the flag
+  // the last warp publishes the new list, clears the per-system counts of
+  // the buffer the next build will write, and clears the flag
   __syncwarp();
+  int last = 0;
   if (lane == 0) {
     __threadfence();
-    if (atomicAdd(&a.ctl[PL_DONE], 1) == nw - 1) {
-      __threadfence();
+    last = atomicAdd(&a.ctl[PL_DONE], 1) == nw - 1;
+  }
+  if (__shfl_sync(kFull, last, 0)) {
+    __threadfence();
+    int32_t *old_counts = nxt ? a.sys_items0 : a.sys_items1;
+    for (int s = lane; s < a.n_sys; s += 32) old_counts[s] = 0;
+    if (lane == 0) {
       a.ctl[PL_COUNT0 + nxt] = atomicAdd(&a.ctl[PL_NEW], 0);
       a.ctl[PL_NEW] = 0;
       a.ctl[PL_DONE] = 0;
       a.ctl[PL_CUR] = nxt;
       a.ctl[PL_DIRTY] = 0;
-      __threadfence();
     }
+    __threadfence();
   }
 }
 
