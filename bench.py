@@ -136,9 +136,14 @@ def parse():
   ap.add_argument("--no-serving", action="store_true")
   ap.add_argument("--no-extra", action="store_true",
                   help="skip the single-system, neighbour-list and serving-sweep legs")
-  ap.add_argument("--serving-requests", type=int, default=32)
-  ap.add_argument("--serving-rate", type=float, default=20.0)
-  ap.add_argument("--serving-step-scale", type=float, default=0.05)
+  ap.add_argument("--serving-requests", type=int, default=200,
+                  help="requests per rate of the served stream")
+  ap.add_argument("--serving-rates", type=lambda v: [float(x) for x in v.split(",")],
+                  default=[10.0, 20.0, 50.0, 100.0, 200.0, 500.0],
+                  help="arrival rates (req/s) of the serving sweep; the headline serving entry is "
+                       "the 20 req/s one when present, else the first")
+  ap.add_argument("--serving-step-scale", type=float, default=1.0,
+                  help="scales the requests' step counts (1.0: log-uniform 1,000-50,000)")
   ap.add_argument("--keep-atom-order", action="store_true",
                   help="store atoms in input order instead of the default spatial order")
   ap.add_argument("--nlist-only", action="store_true",
@@ -307,17 +312,27 @@ def run_reference(args):
   return 0
 
 
-def serving_bench(args):
+def serving_sweep(args):
+  """The served request stream at each rate: Poisson arrivals, N
+  log-uniform 100-10,000 atoms, K log-uniform 1,000-50,000 steps (times
+  --serving-step-scale), the same seeded requests at every rate, admitted
+  against a 150 GB HBM budget into device-resident cohorts.  p50/p99 are
+  end-to-end latencies (arrival to result on the host)."""
   from prolix_b200 import serving
-  reqs = serving.poisson_requests(args.serving_requests, args.serving_rate, WORKLOAD_SEED,
-                                  step_scale=args.serving_step_scale)
-  srv = serving.Server(chunk=50)
-  srv.run(reqs)
-  rep = srv.report()
-  rep.update({"rate_per_s": args.serving_rate, "atoms": "log-uniform 100-10,000",
-              "steps": f"log-uniform 1,000-50,000 x {args.serving_step_scale}",
-              "hbm_budget_gb": 150})
-  return rep
+  res = {}
+  for rate in args.serving_rates:
+    reqs = serving.poisson_requests(args.serving_requests, rate, WORKLOAD_SEED,
+                                    step_scale=args.serving_step_scale)
+    srv = serving.Server(chunk=50, hbm_budget_bytes=150e9)
+    t0 = time.perf_counter()
+    srv.run(reqs)
+    rep = srv.report()
+    rep["wall_s"] = time.perf_counter() - t0
+    rep.update({"rate_per_s": rate, "atoms": "log-uniform 100-10,000",
+                "steps": f"log-uniform 1,000-50,000 x {args.serving_step_scale}",
+                "hbm_budget_gb": 150})
+    res[str(int(rate))] = rep
+  return res
 
 
 def plain_run(systems, stream, steps):
@@ -459,22 +474,6 @@ def minimize_run(systems, stream):
           "rms_grad_median_before": float(np.median(rms0)), "rms_grad_median_after": float(np.median(rms1))}
 
 
-def serving_sweep(args):
-  from prolix_b200 import serving
-  res = {}
-  for rate in (10.0, 50.0, 100.0, 200.0, 500.0):
-    # the same requests (sizes, step counts) as the 20 req/s leg, arriving
-    # at this rate
-    reqs = serving.poisson_requests(args.serving_requests, rate, WORKLOAD_SEED,
-                                    step_scale=args.serving_step_scale)
-    srv = serving.Server(chunk=50)
-    srv.run(reqs)
-    rep = srv.report()
-    res[str(int(rate))] = {k: rep[k] for k in ("completed", "failed", "p50_s", "p99_s",
-                                               "atom_steps_per_s", "ticks")}
-  return res
-
-
 def nlist_only():
   """Three device-side builds of the jax_md-layout list of the 20,000-atom
   globule (cutoff 20 A, skin 2 A), each timed with CUDA events."""
@@ -514,9 +513,11 @@ def main():
   from prolix_b200 import autotune
   if args.segment > 0:
     batch.set_tile_segment(args.segment)
-    tuned = {"segment": args.segment, "timings": None}
+    tuned = {"segment": args.segment, "timings": None}  # block shapes and fusion: defaults
   else:
     tuned = autotune.tune(batch, candidates=(2, 4, 8, 16, 32), steps=3, use_cache=False)
+  batch_shapes = [batch.block_shape(p) for p in range(3)]
+  batch_fusion = batch.fusion()
   for _ in range(args.warmup):  # also captures the one-step graph
     batch.langevin_run(1, stream)
   torch.cuda.synchronize()
@@ -652,15 +653,18 @@ def main():
   if rank == 0:
     if not args.no_plain:
       plain = plain_run(systems, stream, steps=10)
+    sweep = None
     if not args.no_serving:
-      serving_rep = serving_bench(args)
+      sweep = serving_sweep(args)
+      head = "20" if "20" in sweep else next(iter(sweep))
+      serving_rep = dict(sweep[head], sweep={k: {f: v[f] for f in (
+          "completed", "failed", "p50_s", "p99_s", "atom_steps_per_s", "span_s", "wall_s",
+          "cohorts", "ticks")} for k, v in sweep.items()})
     extra = None
     if not args.no_extra:
       extra = {"single_system": single_system_runs(stream, hbm_peak),
                "minimize": minimize_run(systems, stream),
                "nl_born_dense_gb": split_run(systems, stream)}
-      if not args.no_serving:
-        extra["serving_sweep"] = serving_sweep(args)
     if not args.no_cpu:
       v, sample, threads, _ = cpu_reference_run(systems, budget_s=12.0)
       cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
@@ -679,6 +683,10 @@ def main():
                    "parallelism": f"replicas x{ws}",
                    "l2": "256 MB buffer written between timed steps",
                    "tile_segment": tuned["segment"],
+                   "block_shapes": {p: list(batch_shapes[k]) for k, p in
+                                    enumerate(("born", "force", "chain"))},
+                   "fusion": {"bonded_in_chain": bool(batch_fusion & 1),
+                              "born_finalize_in_descreening": bool(batch_fusion & 2)},
                    "autotune_ms_per_step": tuned["timings"]},
         "clocks": clocks,
         "roofline": roofline,

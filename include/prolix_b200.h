@@ -386,9 +386,10 @@ int pb2_get_safeguards(const pb2_batch *batch, double *vlimit, double *max_dx, d
 int pb2_get_warn_counts(pb2_batch *batch, int32_t *counts, int reset, void *stream);
 
 /*
- * Neighbour list (cutoff > 0 only), built by a cell list on the device
- * (jax_md partition.neighbor_list layout, physics/neighbor_list.py:155-172;
- * batched_simulate.py:1429-1464).  pb2_nl_build rebuilds unconditionally
+ * Neighbour list (cutoff > 0 only), built on the device with the batch's
+ * spatially sorted 32-atom blocks as the cells (block bounding boxes in place
+ * of a cell stencil), in jax_md partition.neighbor_list's layout
+ * (physics/neighbor_list.py:155-172; batched_simulate.py:1429-1464).  pb2_nl_build rebuilds unconditionally
  * and returns when the capacity is known (the first build sizes it, as
  * jax_md's allocate does).  pb2_nl_check compares each atom's displacement
  * since the last build against skin/2 (batched_simulate.py:1600-1622) and
@@ -421,6 +422,30 @@ int pb2_nl_last_build_ms(pb2_batch *batch, double *ms);
  * counterpart (prolix's tile sizes are fixed, physics/tiling.py:29-50). */
 int pb2_set_tile_segment(pb2_batch *batch, int32_t segment);
 int pb2_get_tile_segment(const pb2_batch *batch, int32_t *segment);
+
+/* Block shape of a pair pass (pass 0 descreening, 1 force, 2 chain rule):
+ * threads per block and the resident blocks per SM its registers are sized
+ * for.  Each pass is compiled for a few shapes: pb2_block_shapes fills up to
+ * capacity of them and returns how many there are; pb2_set_block_shape
+ * picks one (PB2_EINVAL if not compiled) and drops captured graphs.  The
+ * autotuner's other knob; no reference counterpart. */
+int pb2_block_shapes(int32_t pass, int32_t *threads, int32_t *min_blocks, int32_t capacity);
+int pb2_set_block_shape(pb2_batch *batch, int32_t pass, int32_t threads, int32_t min_blocks);
+int pb2_get_block_shape(const pb2_batch *batch, int32_t pass, int32_t *threads, int32_t *min_blocks);
+
+/* Which per-step work rides inside the pair passes instead of a launch of
+ * its own (an MD step is then four launches: step, descreening, force,
+ * chain rule): PB2_FUSE_BONDED, the bonded terms as the chain pass's tail
+ * work; PB2_FUSE_FINALIZE, each system's Born radii computed by the
+ * descreening warp that completes the system (one warp per system: a gain
+ * for small systems, a tail for large ones).  Defaults: bonded fused,
+ * finalize fused when every system has at most 256 atoms; the autotuner
+ * times the alternatives.  Results are bit-identical either way.  No
+ * reference counterpart. */
+#define PB2_FUSE_BONDED 0x1
+#define PB2_FUSE_FINALIZE 0x2
+int pb2_set_fusion(pb2_batch *batch, int32_t flags);
+int pb2_get_fusion(const pb2_batch *batch, int32_t *flags);
 
 int pb2_set_profiling(pb2_batch *batch, int enable);
 int pb2_last_timings(pb2_batch *batch, double *out_ms);

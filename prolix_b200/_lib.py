@@ -27,6 +27,7 @@ NTERMS = 12
 ABI_VERSION = 3  # PB2_ABI_VERSION of the structures mirrored below
 USE_BONDED, USE_CMAP, USE_LJ, USE_COULOMB, USE_GB = 0x1, 0x2, 0x4, 0x8, 0x10
 USE_ALL = 0x1F
+FUSE_BONDED, FUSE_FINALIZE = 0x1, 0x2
 STATUS_NONFINITE, STATUS_NLOVERFLOW, STATUS_FORCE_RANGE = 0x1, 0x2, 0x4
 
 _c_dp = ctypes.POINTER(ctypes.c_double)
@@ -130,6 +131,12 @@ SIGNATURES = [
     ("pb2_nl_last_build_ms", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
     ("pb2_set_tile_segment", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     ("pb2_get_tile_segment", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]),
+    ("pb2_block_shapes", ctypes.c_int, [ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32]),
+    ("pb2_set_block_shape", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
+    ("pb2_get_block_shape", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
+                                           ctypes.POINTER(ctypes.c_int32)]),
+    ("pb2_set_fusion", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    ("pb2_get_fusion", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]),
     ("pb2_set_profiling", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("pb2_last_timings", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     ("pb2_fp32_peak", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),

@@ -1,14 +1,24 @@
-"""Autotuner for the pair kernels' work-item shape.
+"""Autotuner for the pair kernels' work shapes and the step's schedule.
 
-The knob is the number of 32 x 32 tiles per work item (``tile_segment``):
-short items balance the dynamically scheduled passes better, long items
-amortise loading a warp's i-block.  The best value depends on the size mix
-of the batch, so it is measured: each candidate runs a few full MD steps
-(CUDA events on the launching stream), the fastest wins, and the choice is
-cached in JSON keyed by GPU name and a workload bucket (number of systems,
-total atoms, largest system, cutoff mode, each rounded to a power of two).
-The batch's state is snapshotted before tuning and restored after, so
-tuning does not advance the simulation.
+Three knobs, tuned in turn, each by timing a few full MD steps per
+candidate (CUDA events on the launching stream; the fastest wins):
+
+* ``tile_segment``: 32 x 32 tiles per work item.  Short items balance the
+  dynamically scheduled passes better, long items amortise loading a
+  warp's i-block.
+* the block shape of each pair pass (threads per block, resident blocks
+  per SM the registers are sized for), among the shapes compiled for it
+  (``Batch.block_shapes``): more, smaller blocks against fewer registers
+  per thread.
+* fusion (``_lib.FUSE_*``): the bonded terms as the chain pass's tail work,
+  and each system's Born radii finalized by the descreening warp that
+  completes it, against launches of their own.
+
+The best choice depends on the size mix of the batch; it is cached in JSON
+keyed by GPU name and a workload bucket (number of systems, total atoms,
+largest system, cutoff mode, each rounded to a power of two).  The batch's
+state is snapshotted before tuning and restored after, so tuning does not
+advance the simulation.
 
 Cache file: ``$PROLIX_B200_TUNE_CACHE`` or ~/.cache/prolix_b200/autotune.json.
 """
@@ -64,10 +74,9 @@ def _gpu_name() -> str:
     return "unknown_gpu"
 
 
-def measure(batch, segment: int, steps: int = 4) -> float:
-  """Mean ms per MD step of ``batch`` with ``segment`` tiles per item."""
+def _time(batch, steps: int) -> float:
+  """Mean ms per MD step of ``batch`` as it is configured now."""
   import torch
-  batch.set_tile_segment(segment)
   stream = torch.cuda.current_stream().cuda_stream
   batch.langevin_run(1, stream)  # capture
   e0 = torch.cuda.Event(enable_timing=True)
@@ -80,25 +89,67 @@ def measure(batch, segment: int, steps: int = 4) -> float:
   return e0.elapsed_time(e1) / steps
 
 
-def tune(batch, candidates=CANDIDATES, steps: int = 4, use_cache: bool = True) -> dict:
-  """Pick ``tile_segment`` for ``batch`` (set on the batch) and return
-  {"segment", "ms", "timings", "cached", "key"}."""
+def measure(batch, segment: int, steps: int = 4) -> float:
+  """Mean ms per MD step of ``batch`` with ``segment`` tiles per item."""
+  batch.set_tile_segment(segment)
+  return _time(batch, steps)
+
+
+def apply(batch, choice: dict):
+  """Set a tuned (or cached) choice on the batch."""
+  batch.set_tile_segment(int(choice["segment"]))
+  for p, shape in enumerate(choice.get("shapes") or []):
+    batch.set_block_shape(p, int(shape[0]), int(shape[1]))
+  if choice.get("fusion") is not None:
+    batch.set_fusion(int(choice["fusion"]))
+
+
+def tune(batch, candidates=CANDIDATES, steps: int = 4, use_cache: bool = True,
+         shapes: bool = True, fusion: bool = True) -> dict:
+  """Pick ``tile_segment``, then each pair pass's block shape, then the
+  fusion flags for ``batch`` (set on the batch) and return {"segment",
+  "shapes", "fusion", "ms", "timings", "cached", "key"}."""
   key = bucket_key(batch, _gpu_name())
   path = cache_path()
   data = _load(path) if use_cache else {}
-  if use_cache and key in data:
-    seg = int(data[key]["segment"])
-    batch.set_tile_segment(seg)
-    return {"segment": seg, "ms": data[key].get("ms"), "timings": data[key].get("timings"),
-            "cached": True, "key": key}
+  if use_cache and key in data and "shapes" in data[key]:
+    apply(batch, data[key])
+    return {**data[key], "cached": True, "key": key}
   snap = batch.get_state()
   timings = {}
   for c in candidates:
-    timings[str(c)] = measure(batch, c, steps)
-  best = min(timings, key=timings.get)
-  batch.set_tile_segment(int(best))
+    timings[f"segment={c}"] = measure(batch, c, steps)
+  best_seg = min(candidates, key=lambda c: timings[f"segment={c}"])
+  batch.set_tile_segment(int(best_seg))
+  best_ms = timings[f"segment={best_seg}"]
+  chosen_shapes = [list(batch.block_shape(p)) for p in range(3)]
+  if shapes:
+    for p in range(3):
+      for t, m in batch.block_shapes(p):
+        if [t, m] == chosen_shapes[p]:
+          continue
+        batch.set_block_shape(p, t, m)
+        ms = _time(batch, steps)
+        timings[f"pass{p}={t}x{m}"] = ms
+        if ms < best_ms:
+          best_ms = ms
+          chosen_shapes[p] = [t, m]
+        batch.set_block_shape(p, *chosen_shapes[p])
+  chosen_fusion = batch.fusion()
+  if fusion:
+    for f in range(4):
+      if f == chosen_fusion:
+        continue
+      batch.set_fusion(f)
+      ms = _time(batch, steps)
+      timings[f"fusion={f}"] = ms
+      if ms < best_ms:
+        best_ms = ms
+        chosen_fusion = f
+      batch.set_fusion(chosen_fusion)
   batch.set_state(position=snap["position"], momentum=snap["momentum"], key=snap["key"])
-  result = {"segment": int(best), "ms": timings[best], "timings": timings}
+  result = {"segment": int(best_seg), "shapes": chosen_shapes, "fusion": int(chosen_fusion),
+            "ms": best_ms, "timings": timings}
   if use_cache:
     data[key] = result
     _store(path, data)

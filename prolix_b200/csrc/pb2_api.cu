@@ -246,6 +246,14 @@ static std::vector<TileItem> build_items2(const std::vector<SysInfo> &sinfo, int
   return items;
 }
 
+// Grid of pair pass p for its block shape: one resident wave (warps take
+// items dynamically), no more warps than items.
+static void set_pair_grid(pb2_batch *b, int p) {
+  const int cap = tile_kernel_occupancy(p, b->cut, b->shape[p]) * b->ctx->sm_count;
+  const int w = tile_kernel_warps(p, b->shape[p]);
+  b->grid_pair[p] = std::max(1, std::min(cap, (b->n_items2 + w - 1) / w));
+}
+
 // (Re)build the pair kernels' two-i-block work list and their grids (one
 // resident wave each; warps take items dynamically).
 static int setup_items2(pb2_batch *b, int seg) {
@@ -266,11 +274,7 @@ static int setup_items2(pb2_batch *b, int seg) {
     CUDA_TRY(ctx, cudaMemset(b->sys_done, 0, b->n_sys * sizeof(int32_t)));
   }
   CUDA_TRY(ctx, cudaMemcpy(b->sys_items, per_sys.data(), per_sys.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
-  for (int p = 0; p < 3; ++p) {
-    const int cap = tile_kernel_occupancy(p, b->cut) * ctx->sm_count;
-    const int w = tile_kernel_warps(p);
-    b->grid_pair[p] = std::max(1, std::min(cap, (b->n_items2 + w - 1) / w));
-  }
+  for (int p = 0; p < 3; ++p) set_pair_grid(b, p);
   return PB2_OK;
 }
 
@@ -842,6 +846,13 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   b->grid_bonded = 8 * ctx->sm_count;
   if ((rc = setup_items2(b.get(), b->params.tile_segment))) return rc;
   if ((rc = setup_pair_list(b.get(), b->params.tile_segment))) return rc;
+  {
+    // a system's Born radii are finalized by one warp when fused: worth it
+    // for small systems only (the autotuner may change this)
+    int nmax = 0;
+    for (int s = 0; s < n_systems; ++s) nmax = std::max(nmax, b->sys_host[s].n);
+    b->fuse = PB2_FUSE_BONDED | (nmax <= 256 ? PB2_FUSE_FINALIZE : 0);
+  }
   CUDA_TRY(ctx, cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking));
   CUDA_TRY(ctx, cudaEventCreate(&b->ev[0]));
   CUDA_TRY(ctx, cudaEventCreate(&b->ev[1]));
@@ -919,21 +930,21 @@ static cudaError_t enqueue_forces(pb2_batch *b, cudaStream_t st, bool bonded_ene
     fa.energy_mode = 0;
     // the descreening pass finalizes each system as its last item completes
     // (profiling keeps the separate launch, to time it)
-    const bool fuse_finalize = !b->profiling;
+    const bool fuse_finalize = !b->profiling && (b->fuse & PB2_FUSE_FINALIZE);
     PairArgs pb = pa;
     pb.sched = b->sched + 2 * PASS_BORN;
     if (fuse_finalize) {
       pb.sys_items = b->sys_items;
       pb.fin = fa;
     }
-    if ((e = tm(kTimBorn, [&] { return launch_tiles(PASS_BORN, pb, b->grid_pair[PASS_BORN], st); })) != cudaSuccess)
+    if ((e = tm(kTimBorn, [&] { return launch_tiles(PASS_BORN, pb, b->grid_pair[PASS_BORN], b->shape[PASS_BORN], st); })) != cudaSuccess)
       return e;
     if (!fuse_finalize &&
         (e = tm(kTimFinalize, [&] { return launch_born_finalize(fa, st); })) != cudaSuccess)
       return e;
   }
   pa.sched = b->sched + 2 * PASS_FORCE;
-  if ((e = tm(kTimForce, [&] { return launch_tiles(PASS_FORCE, pa, b->grid_pair[PASS_FORCE], st); })) != cudaSuccess)
+  if ((e = tm(kTimForce, [&] { return launch_tiles(PASS_FORCE, pa, b->grid_pair[PASS_FORCE], b->shape[PASS_FORCE], st); })) != cudaSuccess)
     return e;
   pa.sched = b->sched + 2 * PASS_CHAIN;
   BondedArgs ba = b->bonded;
@@ -941,13 +952,13 @@ static cudaError_t enqueue_forces(pb2_batch *b, cudaStream_t st, bool bonded_ene
   const int n_bonded = ba.n_bond + ba.n_angle + ba.n_tors + ba.n_cmap + ba.n_exc;
   // the bonded terms ride along as the chain pass's tail work, except when
   // their energies are wanted or there is no chain pass
-  const bool fuse_bonded = gb && !bonded_energy && !b->profiling;
+  const bool fuse_bonded = gb && !bonded_energy && !b->profiling && (b->fuse & PB2_FUSE_BONDED);
   if (fuse_bonded) {
     pa.bonded = ba;
     pa.n_bonded_chunks = (n_bonded + kBondedChunk - 1) / kBondedChunk;
   }
   if (gb)
-    if ((e = tm(kTimChain, [&] { return launch_tiles(PASS_CHAIN, pa, b->grid_pair[PASS_CHAIN], st); })) != cudaSuccess)
+    if ((e = tm(kTimChain, [&] { return launch_tiles(PASS_CHAIN, pa, b->grid_pair[PASS_CHAIN], b->shape[PASS_CHAIN], st); })) != cudaSuccess)
       return e;
   if (fuse_bonded) return cudaSuccess;
   return tm(kTimBonded, [&] { return launch_bonded(ba, b->grid_bonded, st); });
@@ -1810,6 +1821,67 @@ extern "C" int pb2_set_tile_segment(pb2_batch *b, int32_t segment) {
 extern "C" int pb2_get_tile_segment(const pb2_batch *b, int32_t *segment) {
   if (!b || !segment) return PB2_EINVAL;
   *segment = b->params.tile_segment;
+  return PB2_OK;
+}
+
+extern "C" int pb2_block_shapes(int32_t pass, int32_t *threads, int32_t *min_blocks, int32_t capacity) {
+  if (pass < 0 || pass > 2) return PB2_EINVAL;
+  for (int k = 0; k < kShapesPerPass && k < capacity; ++k) {
+    int t = 0, m = 0;
+    tile_shape(pass, k, &t, &m);
+    if (threads) threads[k] = t;
+    if (min_blocks) min_blocks[k] = m;
+  }
+  return kShapesPerPass;
+}
+
+extern "C" int pb2_set_block_shape(pb2_batch *b, int32_t pass, int32_t threads, int32_t min_blocks) {
+  if (!b || pass < 0 || pass > 2) return PB2_EINVAL;
+  pb2_ctx *ctx = b->ctx;
+  int found = -1;
+  for (int k = 0; k < kShapesPerPass; ++k) {
+    int t = 0, m = 0;
+    tile_shape(pass, k, &t, &m);
+    if (t == threads && m == min_blocks) found = k;
+  }
+  if (found < 0) return fail(ctx, PB2_EINVAL, "block shape not compiled for this pass (see pb2_block_shapes)");
+  if (found == b->shape[pass]) return PB2_OK;
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  CUDA_TRY(ctx, cudaDeviceSynchronize());
+  b->shape[pass] = found;
+  set_pair_grid(b, pass);
+  for (auto &kv : b->graphs) cudaGraphExecDestroy(kv.second);  // they captured the old kernel
+  b->graphs.clear();
+  for (auto &kv : b->min_graphs) cudaGraphExecDestroy(kv.second);
+  b->min_graphs.clear();
+  return PB2_OK;
+}
+
+extern "C" int pb2_get_block_shape(const pb2_batch *b, int32_t pass, int32_t *threads, int32_t *min_blocks) {
+  if (!b || pass < 0 || pass > 2 || !threads || !min_blocks) return PB2_EINVAL;
+  int t = 0, m = 0;
+  tile_shape(pass, b->shape[pass], &t, &m);
+  *threads = t;
+  *min_blocks = m;
+  return PB2_OK;
+}
+
+extern "C" int pb2_set_fusion(pb2_batch *b, int32_t flags) {
+  if (!b || (flags & ~(PB2_FUSE_BONDED | PB2_FUSE_FINALIZE))) return PB2_EINVAL;
+  if (flags == b->fuse) return PB2_OK;
+  CUDA_TRY(b->ctx, cudaSetDevice(b->ctx->device));
+  CUDA_TRY(b->ctx, cudaDeviceSynchronize());
+  b->fuse = flags;
+  for (auto &kv : b->graphs) cudaGraphExecDestroy(kv.second);  // they captured the old schedule
+  b->graphs.clear();
+  for (auto &kv : b->min_graphs) cudaGraphExecDestroy(kv.second);
+  b->min_graphs.clear();
+  return PB2_OK;
+}
+
+extern "C" int pb2_get_fusion(const pb2_batch *b, int32_t *flags) {
+  if (!b || !flags) return PB2_EINVAL;
+  *flags = b->fuse;
   return PB2_OK;
 }
 

@@ -61,8 +61,10 @@ __device__ __forceinline__ int bonded_total(const BondedArgs &a) {
 }
 
 // Term t of the batch: bonds (then Urey-Bradley springs), angles, torsions
-// and impropers, CMAP, exception pairs, in that index order.
-static __device__ __noinline__ void bonded_term(const BondedArgs &a, int t) {
+// and impropers, CMAP, exception pairs, in that index order.  Inlined into
+// the bonded kernel; bonded_term_call keeps it out of line for the chain
+// pass, whose hot loop should not grow.
+static __device__ __forceinline__ void bonded_term(const BondedArgs &a, int t) {
   {
     int u = t;
     if (u < a.n_bond) {
@@ -200,5 +202,7 @@ static __device__ __noinline__ void bonded_term(const BondedArgs &a, int t) {
     }
   }
 }
+
+static __device__ __noinline__ void bonded_term_call(const BondedArgs &a, int t) { bonded_term(a, t); }
 
 }  // namespace pb2

@@ -111,6 +111,8 @@ struct pb2_batch {
   bool forces_valid = false;
   bool cut = false;  // any cutoff active  // force accumulators hold F(x) of the current state
   int grid_pair[3] = {1, 1, 1};
+  int shape[3] = {0, 0, 0};  // block shape of each pair pass (index into the compiled shapes)
+  int fuse = PB2_FUSE_BONDED;  // PB2_FUSE_* bits: work folded into the pair passes
   int grid_bonded = 1;
   cudaStream_t cap_stream = nullptr;
   std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
@@ -152,11 +154,7 @@ struct pb2_batch {
   Dev nl;
   bool nl_built = false;
   int nl_capacity = 0;
-  int nl_cells = 0;
-  NlGrid *nl_grid = nullptr;
-  int32_t *nl_cell_base = nullptr, *nl_cell_budget = nullptr, *nl_cell_sys = nullptr;
-  int *nl_atom_cell = nullptr, *nl_cell_count = nullptr, *nl_cell_start = nullptr;
-  int *nl_cell_cursor = nullptr, *nl_cell_atoms = nullptr, *nl_rows = nullptr, *nl_counts = nullptr;
+  int *nl_rows = nullptr, *nl_counts = nullptr;
   int32_t *nl_sys_moved = nullptr, *nl_ctl = nullptr;
   double *nl_xref = nullptr;
   cudaEvent_t nl_ev[2] = {nullptr, nullptr};  // around the last build's launches

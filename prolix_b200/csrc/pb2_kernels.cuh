@@ -120,31 +120,22 @@ struct Energy64Args {
   long long *energy;
 };
 
-struct NlGrid {        // per-system cell grid of the neighbour-list build (written on the device)
-  float x0, y0, z0, inv_cell;
-  int32_t nx, ny, nz;
-  int32_t stencil;      // cells searched on each side: ceil(reach / cell edge)
-};
 // Neighbour-list control words (NlArgs::ctl)
-enum { NL_DIRTY = 0, NL_MAXCOUNT = 1, NL_CELLFULL = 2, NL_DONE = 3, NL_WORDS = 4 };
+enum { NL_DIRTY = 0, NL_MAXCOUNT = 1, NL_DONE = 2, NL_WORDS = 4 };
 struct NlArgs {
   const SysInfo *sys;
   const int32_t *atom_sys;
+  const int32_t *blk_sys;      // per global 32-atom block: its system
   const float4 *bbox;          // current block boxes
-  NlGrid *grid;                // per system
-  const int32_t *cell_base;    // per system: first cell of its cell budget
-  const int32_t *cell_budget;  // per system: cells it may use
-  const int32_t *cell_sys;     // per cell: its system
   const float4 *posq;
   const double *x, *y, *z;
   double *xref;                // positions at the last build, SoA (3, n_total)
-  int *atom_cell, *cell_count, *cell_start, *cell_cursor, *cell_atoms;
   int *rows, *counts;
   int32_t *sys_moved;          // per system: moved more than skin / 2 (the last check)
   int32_t *ctl;                // NL_* words; the build kernels run only while ctl[NL_DIRTY] != 0
-  int32_t capacity, n_total, n_cells, n_sys;
+  int32_t capacity, n_total, n_blocks, n_sys;
   uint32_t *status;
-  float reach;                 // cutoff + skin
+  float reach2;                // (cutoff + skin)^2
 };
 // The build (every kernel returns at once unless ctl[NL_DIRTY] is set; the
 // last one clears it) and the half-skin test that sets it.
@@ -229,11 +220,15 @@ struct LbfgsArgs {
   double tol, max_step;
 };
 cudaError_t launch_lbfgs(int op, const LbfgsArgs &a, int last_trial, cudaStream_t st);
-cudaError_t launch_tiles(int pass, const PairArgs &a, int grid, cudaStream_t st);
+// Block shapes of the pair kernels: kShapesPerPass compiled per pass;
+// tile_shape gives (threads, min blocks per SM) of one (-1: no such shape).
+constexpr int kShapesPerPass = 3;
+int tile_shape(int pass, int shape, int *threads, int *min_blocks);
+cudaError_t launch_tiles(int pass, const PairArgs &a, int grid, int shape, cudaStream_t st);
 cudaError_t launch_energy64(int pass, const Energy64Args &a, int grid, cudaStream_t st);
 cudaError_t launch_born_finalize(const FinalizeArgs &a, cudaStream_t st);
-int tile_kernel_occupancy(int pass, bool cut);
-int tile_kernel_warps(int pass);  // warps per block of a pair pass
+int tile_kernel_occupancy(int pass, bool cut, int shape);
+int tile_kernel_warps(int pass, int shape);  // warps per block of a pair pass
 // Bounding boxes of every 32-atom block.  With pl_ref / pl_ctl set, also
 // flags the pair list for a rebuild (pl_ctl[PL_DIRTY]) when an atom moved
 // more than half the skin since the list was built.

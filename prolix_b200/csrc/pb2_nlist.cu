@@ -1,4 +1,4 @@
-// Neighbour lists in jax_md's layout, built with a cell list on the GPU.
+// Neighbour lists in jax_md's layout, built on the GPU.
 //
 // Reference: jax_md partition.neighbor_list as prolix uses it
 // (physics/neighbor_list.py:155-172; batched_simulate.py:1429-1464), the
@@ -8,26 +8,26 @@
 // atoms within cutoff + skin (both (i, j) and (j, i) present), padded with
 // the sentinel n_atoms of its system; capacity K per atom.
 //
-// Everything runs on the device, all systems of the batch at once, as a
-// fixed sequence of launches that needs no host decision:
+// The spatial cells are the batch's own 32-atom blocks: each system's atoms
+// are stored in a recursive-bisection order, so a block is a compact
+// cluster, and its bounding box is already computed for the pair kernels.
+// A cell grid is not built: the block boxes play its part, a box test
+// standing in for the cell stencil.  One warp per block (lane = the block's
+// atom, = one row): for every block of the system whose box comes within
+// cutoff + skin of its own, the warp stages that block's 32 positions in
+// shared memory and each lane tests them in index order, appending hits to
+// its row.  Rows are therefore in stored-atom order, the same every build.
+// A row longer than the capacity only counts (the largest count and an
+// overflow bit are recorded for the host's next visit).
+//
+// Everything runs on the device as a fixed sequence of launches that needs
+// no host decision:
 //   0. (check) each atom's displacement since the last build against
 //      skin/2 sets the rebuild flag and its system's moved flag;
-//   1. per system, a cell grid over the current block bounding boxes, cell
-//      edge reach/2 (searched two cells out), widened where the system
-//      would need more cells than its budget (2 per atom, at least 64);
-//   2. each atom's cell and the counts per cell;
-//   3. per system, an exclusive scan of its cells' counts;
-//   4. atoms scattered to their cells; 5. each cell sorted by atom index
-//      (list order is deterministic);
-//   6. one thread block per cell: the cell's atoms test, from shared memory,
-//      the atoms of the surrounding cells, each thread writing its atom's
-//      row; rows beyond the capacity only count (the largest count and an
-//      overflow bit are recorded for the host's next visit);
-//   7. the positions become the new displacement reference; the last block
-//      clears the flag.
-// Each kernel returns at once while the flag is clear, so a check that
-// finds nothing to do costs one launch per kernel and no host round trip.
-// The HBM traffic is dominated by step 6's row writes (4 B per entry).
+//   1. the rows; 2. the positions become the new displacement reference,
+//      and the last block clears the flag.
+// Each kernel returns at once while the flag is clear.  The HBM traffic is
+// the row writes (4 B per slot).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -40,10 +40,18 @@
 
 namespace pb2 {
 
-constexpr int kMaxCellSort = 4096;  // atoms per cell handled by the in-block sort
-constexpr int kRowsThreads = 128;   // threads per cell block of the row pass
+constexpr int kRowsWarps = 8;  // warps (blocks of atoms) per thread block of the row pass
 
 __device__ __forceinline__ bool nl_dirty(const NlArgs &a) { return *(volatile int32_t *)&a.ctl[NL_DIRTY] != 0; }
+
+__device__ __forceinline__ float nl_box_dist2(const float4 *bbox, int a, int b) {
+  const float4 alo = bbox[2 * a], ahi = bbox[2 * a + 1];
+  const float4 blo = bbox[2 * b], bhi = bbox[2 * b + 1];
+  const float dx = fmaxf(0.f, fmaxf(alo.x - bhi.x, blo.x - ahi.x));
+  const float dy = fmaxf(0.f, fmaxf(alo.y - bhi.y, blo.y - ahi.y));
+  const float dz = fmaxf(0.f, fmaxf(alo.z - bhi.z, blo.z - ahi.z));
+  return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+}
 
 // 0. displacement since the last build (FP64 state) against skin/2
 __global__ void nl_disp_kernel(const NlArgs a) {
@@ -58,223 +66,51 @@ __global__ void nl_disp_kernel(const NlArgs a) {
   }
 }
 
-// 1. per-system grid, one warp per system; also clears the system's cells
-__global__ void nl_grid_kernel(const NlArgs a) {
+// 1. rows: one warp per block of atoms
+__global__ void __launch_bounds__(32 * kRowsWarps) nl_rows_kernel(const NlArgs a) {
   if (!nl_dirty(a)) return;
-  const int lane = threadIdx.x & 31;
+  __shared__ float4 sp[kRowsWarps][32];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  float4 *jt = sp[wib];
   const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int nw = (int)((gridDim.x * blockDim.x) >> 5);
-  for (int s = w; s < a.n_sys; s += nw) {
+  for (int ib = w; ib < a.n_blocks; ib += nw) {
+    const int s = a.blk_sys[ib];
     const SysInfo &S = a.sys[s];
-    float lo[3] = {1e30f, 1e30f, 1e30f}, hi[3] = {-1e30f, -1e30f, -1e30f};
-    for (int k = lane; k < S.nblk; k += 32) {
-      const float4 l = a.bbox[2 * (S.blk_base + k)], h = a.bbox[2 * (S.blk_base + k) + 1];
-      lo[0] = fminf(lo[0], l.x); lo[1] = fminf(lo[1], l.y); lo[2] = fminf(lo[2], l.z);
-      hi[0] = fmaxf(hi[0], h.x); hi[1] = fmaxf(hi[1], h.y); hi[2] = fmaxf(hi[2], h.z);
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        lo[c] = fminf(lo[c], __shfl_xor_sync(kFull, lo[c], o));
-        hi[c] = fmaxf(hi[c], __shfl_xor_sync(kFull, hi[c], o));
-      }
-    const int budget = a.cell_budget[s];
-    // edge reach/2; widened until the grid fits the budget
-    double edge = 0.5 * (double)a.reach;
-    int n[3];
-    for (int it = 0; it < 64; ++it) {
-      long long cells = 1;
-      for (int c = 0; c < 3; ++c) {
-        n[c] = max(1, (int)ceil(((double)hi[c] - (double)lo[c]) / edge + 1e-6));
-        cells *= n[c];
-      }
-      if (cells <= budget) break;
-      edge *= fmax(1.01, cbrt((double)cells / budget));
-    }
-    if (lane == 0) {
-      NlGrid g;
-      g.x0 = lo[0]; g.y0 = lo[1]; g.z0 = lo[2];
-      g.inv_cell = (float)(1.0 / edge);
-      g.nx = n[0]; g.ny = n[1]; g.nz = n[2];
-      g.stencil = (int)ceil((double)a.reach / edge - 1e-9);
-      a.grid[s] = g;
-    }
-    const int base = a.cell_base[s];
-    for (int c = lane; c < budget; c += 32) {
-      a.cell_count[base + c] = 0;
-      a.cell_cursor[base + c] = 0;
-    }
-  }
-}
-
-// 2. cell of each atom (clamped into the grid) and the counts
-__global__ void nl_assign_kernel(const NlArgs a) {
-  if (!nl_dirty(a)) return;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_total; i += gridDim.x * blockDim.x) {
-    const int s = a.atom_sys[i];
-    const NlGrid g = a.grid[s];
+    const int li = (ib - S.blk_base) * 32 + lane;  // the lane's atom, local index
+    const bool has_i = li < S.n;
+    const int i = S.off + (has_i ? li : 0);
     const float4 p = a.posq[i];
-    int cx = (int)floorf((p.x - g.x0) * g.inv_cell);
-    int cy = (int)floorf((p.y - g.y0) * g.inv_cell);
-    int cz = (int)floorf((p.z - g.z0) * g.inv_cell);
-    cx = min(max(cx, 0), g.nx - 1);
-    cy = min(max(cy, 0), g.ny - 1);
-    cz = min(max(cz, 0), g.nz - 1);
-    const int c = a.cell_base[s] + (cz * g.ny + cy) * g.nx + cx;
-    a.atom_cell[i] = c;
-    atomicAdd(&a.cell_count[c], 1);
-  }
-}
-
-// 3. exclusive scan of a system's cell counts, one block per system; cells
-// past the grid (unused budget) start at the system's end
-__global__ void nl_scan_kernel(const NlArgs a) {
-  if (!nl_dirty(a)) return;
-  __shared__ int buf[1024];
-  __shared__ int carry;
-  for (int s = blockIdx.x; s < a.n_sys; s += gridDim.x) {
-    const SysInfo &S = a.sys[s];
-    const NlGrid g = a.grid[s];
-    const int base = a.cell_base[s], budget = a.cell_budget[s];
-    const int used = g.nx * g.ny * g.nz;
-    if (threadIdx.x == 0) carry = S.off;
-    __syncthreads();
-    for (int c0 = 0; c0 < used; c0 += 1024) {
-      const int c = c0 + threadIdx.x;
-      const int v = c < used ? a.cell_count[base + c] : 0;
-      buf[threadIdx.x] = v;
-      __syncthreads();
-      for (int o = 1; o < 1024; o <<= 1) {
-        const int t = threadIdx.x >= o ? buf[threadIdx.x - o] : 0;
-        __syncthreads();
-        buf[threadIdx.x] += t;
-        __syncthreads();
-      }
-      if (c < used) a.cell_start[base + c] = carry + buf[threadIdx.x] - v;
-      __syncthreads();
-      if (threadIdx.x == 1023) carry += buf[1023];
-      __syncthreads();
-    }
-    for (int c = used + threadIdx.x; c <= budget; c += blockDim.x) a.cell_start[base + c] = S.off + S.n;
-    __syncthreads();
-  }
-}
-
-// 4. scatter atoms to their cells
-__global__ void nl_scatter_kernel(const NlArgs a) {
-  if (!nl_dirty(a)) return;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_total; i += gridDim.x * blockDim.x) {
-    const int c = a.atom_cell[i];
-    const int slot = atomicAdd(&a.cell_cursor[c], 1);
-    a.cell_atoms[a.cell_start[c] + slot] = i;
-  }
-}
-
-// 5. one block per cell: bitonic sort of the cell's atom indices in shared memory
-__global__ void nl_sort_kernel(const NlArgs a) {
-  if (!nl_dirty(a)) return;
-  __shared__ int v[kMaxCellSort];
-  for (int c = blockIdx.x; c < a.n_cells; c += gridDim.x) {
-    const int start = a.cell_start[c];
-    const int cnt = a.cell_count[c];
-    if (cnt <= 1) continue;
-    if (cnt > kMaxCellSort) {
-      if (threadIdx.x == 0) atomicOr(&a.ctl[NL_CELLFULL], 1);
-      continue;
-    }
-    int m = 1;
-    while (m < cnt) m <<= 1;
-    for (int t = threadIdx.x; t < m; t += blockDim.x) v[t] = t < cnt ? a.cell_atoms[start + t] : 0x7fffffff;
-    __syncthreads();
-    for (int k = 2; k <= m; k <<= 1)
-      for (int j = k >> 1; j > 0; j >>= 1) {
-        for (int t = threadIdx.x; t < m; t += blockDim.x) {
-          const int p = t ^ j;
-          if (p > t) {
-            const bool up = (t & k) == 0;
-            const int x = v[t], y = v[p];
-            if ((x > y) == up) { v[t] = y; v[p] = x; }
-          }
-        }
-        __syncthreads();
-      }
-    for (int t = threadIdx.x; t < cnt; t += blockDim.x) a.cell_atoms[start + t] = v[t];
-    __syncthreads();
-  }
-}
-
-// 6. rows: one block per cell, one thread per atom of the cell (in chunks);
-// the surrounding cells' atoms pass through shared memory in a fixed order
-__global__ void __launch_bounds__(kRowsThreads) nl_rows_kernel(const NlArgs a) {
-  if (!nl_dirty(a)) return;
-  __shared__ float4 sp[kRowsThreads];
-  __shared__ int sj[kRowsThreads];
-  for (int c = blockIdx.x; c < a.n_cells; c += gridDim.x) {
-    const int ci0 = a.cell_start[c], nci = a.cell_count[c];
-    if (nci == 0) continue;  // block-uniform
-    const int s = a.cell_sys[c];
-    const SysInfo &S = a.sys[s];
-    const NlGrid g = a.grid[s];
-    const int lc = c - a.cell_base[s];
-    const int cx = lc % g.nx, cy = (lc / g.nx) % g.ny, cz = lc / (g.nx * g.ny);
-    const float reach2 = a.reach * a.reach;
-    const int R = g.stencil;
-    for (int i0 = 0; i0 < nci; i0 += kRowsThreads) {
-      const int k = i0 + threadIdx.x;
-      const bool has_i = k < nci;
-      const int i = has_i ? a.cell_atoms[ci0 + k] : -1;
-      const float4 p = has_i ? a.posq[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-      int *row = has_i ? a.rows + (size_t)i * a.capacity : nullptr;
-      int count = 0;
-      for (int dz = -R; dz <= R; ++dz) {
-        const int z = cz + dz;
-        if (z < 0 || z >= g.nz) continue;
-        for (int dy = -R; dy <= R; ++dy) {
-          const int y = cy + dy;
-          if (y < 0 || y >= g.ny) continue;
-          for (int dx = -R; dx <= R; ++dx) {
-            const int x = cx + dx;
-            if (x < 0 || x >= g.nx) continue;
-            const int nc = a.cell_base[s] + (z * g.ny + y) * g.nx + x;
-            const int st = a.cell_start[nc], cnt = a.cell_count[nc];
-            for (int b = 0; b < cnt; b += kRowsThreads) {
-              __syncthreads();  // the previous chunk has been read
-              const int m = min(kRowsThreads, cnt - b);
-              if ((int)threadIdx.x < m) {
-                const int j = a.cell_atoms[st + b + threadIdx.x];
-                sj[threadIdx.x] = j;
-                sp[threadIdx.x] = a.posq[j];
-              }
-              __syncthreads();
-              if (has_i) {
-                for (int t = 0; t < m; ++t) {
-                  const float4 q = sp[t];
-                  const float ex = p.x - q.x, ey = p.y - q.y, ez = p.z - q.z;
-                  const int j = sj[t];
-                  if (fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < reach2 && j != i) {
-                    if (count < a.capacity) row[count] = j - S.off;
-                    ++count;
-                  }
-                }
-              }
-            }
-          }
-        }
-      }
+    int *row = a.rows + (size_t)i * a.capacity;
+    int count = 0;
+    for (int jb = 0; jb < S.nblk; ++jb) {
+      if (nl_box_dist2(a.bbox, ib, S.blk_base + jb) >= a.reach2) continue;  // warp-uniform
+      const int lj0 = jb * 32;
+      const int nj = min(32, S.n - lj0);
+      __syncwarp();  // the previous block's positions have been read
+      if (lane < nj) jt[lane] = a.posq[S.off + lj0 + lane];
+      __syncwarp();
       if (has_i) {
-        for (int t = count; t < a.capacity; ++t) row[t] = S.n;  // sentinel
-        a.counts[i] = count;
-        if (count > a.capacity) {
-          atomicOr(&a.status[s], (uint32_t)PB2_STATUS_NLOVERFLOW);
+        for (int t = 0; t < nj; ++t) {
+          const float4 q = jt[t];  // one address for the whole warp: a broadcast
+          const float ex = p.x - q.x, ey = p.y - q.y, ez = p.z - q.z;
+          if (fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < a.reach2 && lj0 + t != li) {
+            if (count < a.capacity) row[count] = lj0 + t;
+            ++count;
+          }
         }
-        atomicMax(&a.ctl[NL_MAXCOUNT], count);
       }
+    }
+    if (has_i) {
+      for (int t = count; t < a.capacity; ++t) row[t] = S.n;  // sentinel
+      a.counts[i] = count;
+      if (count > a.capacity) atomicOr(&a.status[s], (uint32_t)PB2_STATUS_NLOVERFLOW);
+      atomicMax(&a.ctl[NL_MAXCOUNT], count);
     }
   }
 }
 
-// 7. new displacement reference; the last block clears the rebuild flag
+// 2. new displacement reference; the last block clears the rebuild flag
 __global__ void nl_ref_kernel(const NlArgs a) {
   if (!nl_dirty(a)) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_total; i += gridDim.x * blockDim.x) {
@@ -296,12 +132,7 @@ __global__ void nl_ref_kernel(const NlArgs a) {
 static int grid_for(int n, int per) { return std::max(1, std::min((n + per - 1) / per, 65535)); }
 
 cudaError_t nl_launch_build(const NlArgs &a, cudaStream_t st) {
-  nl_grid_kernel<<<grid_for(a.n_sys, 8), 256, 0, st>>>(a);
-  nl_assign_kernel<<<grid_for(a.n_total, 256), 256, 0, st>>>(a);
-  nl_scan_kernel<<<std::min(a.n_sys, 65535), 1024, 0, st>>>(a);
-  nl_scatter_kernel<<<grid_for(a.n_total, 256), 256, 0, st>>>(a);
-  nl_sort_kernel<<<grid_for(a.n_cells, 1), 256, 0, st>>>(a);
-  nl_rows_kernel<<<grid_for(a.n_cells, 1), kRowsThreads, 0, st>>>(a);
+  nl_rows_kernel<<<grid_for(a.n_blocks, kRowsWarps), 32 * kRowsWarps, 0, st>>>(a);
   nl_ref_kernel<<<grid_for(a.n_total, 256), 256, 0, st>>>(a);
   return cudaGetLastError();
 }
@@ -325,68 +156,37 @@ static NlArgs nl_args(pb2_batch *b) {
   NlArgs a;
   a.sys = b->sys;
   a.atom_sys = b->atom_sys;
+  a.blk_sys = b->blk_sys;
   a.bbox = b->bbox;
-  a.grid = b->nl_grid;
-  a.cell_base = b->nl_cell_base;
-  a.cell_budget = b->nl_cell_budget;
-  a.cell_sys = b->nl_cell_sys;
   a.posq = b->posq;
   a.x = b->x; a.y = b->y; a.z = b->z;
   a.xref = b->nl_xref;
-  a.atom_cell = b->nl_atom_cell;
-  a.cell_count = b->nl_cell_count;
-  a.cell_start = b->nl_cell_start;
-  a.cell_cursor = b->nl_cell_cursor;
-  a.cell_atoms = b->nl_cell_atoms;
   a.rows = b->nl_rows;
   a.counts = b->nl_counts;
   a.sys_moved = b->nl_sys_moved;
   a.ctl = b->nl_ctl;
   a.capacity = b->nl_capacity;
   a.n_total = b->n_total;
-  a.n_cells = b->nl_cells;
+  a.n_blocks = b->n_blocks;
   a.n_sys = b->n_sys;
   a.status = b->status;
-  a.reach = (float)nl_reach(b);
+  const float reach = (float)nl_reach(b);
+  a.reach2 = reach * reach;
   return a;
 }
 
-// Device arrays of the list, allocated once: per-system cell budgets of
-// max(64, 2 n) cells, the cell arrays over all budgets, the control words.
+// Device arrays of the list, allocated once: counts, reference positions,
+// moved flags, control words (the rows follow the capacity).
 static int nl_alloc(pb2_batch *b) {
   pb2_ctx *ctx = b->ctx;
-  if (b->nl_grid) return PB2_OK;
-  std::vector<int32_t> base(b->n_sys), budget(b->n_sys), cell_sys;
-  long long cells = 0;
-  for (int s = 0; s < b->n_sys; ++s) {
-    base[s] = (int32_t)cells;
-    budget[s] = std::max(64, 2 * b->sys_host[s].n);
-    cells += budget[s];
-    if (cells > INT32_MAX / 2) return fail(ctx, PB2_EINVAL, "neighbour-list cell budget too large");
-    cell_sys.insert(cell_sys.end(), budget[s], s);
-  }
+  if (b->nl_ctl) return PB2_OK;
   Dev &D = b->nl;
-  b->nl_cells = (int)cells;
-  b->nl_grid = D.alloc<NlGrid>(b->n_sys);
-  b->nl_cell_base = D.alloc<int32_t>(b->n_sys);
-  b->nl_cell_budget = D.alloc<int32_t>(b->n_sys);
-  b->nl_cell_sys = D.alloc<int32_t>(cells);
-  b->nl_cell_count = D.alloc<int>(cells);
-  b->nl_cell_start = D.alloc<int>(cells + 1);
-  b->nl_cell_cursor = D.alloc<int>(cells);
-  b->nl_atom_cell = D.alloc<int>(b->n_total);
-  b->nl_cell_atoms = D.alloc<int>(b->n_total);
   b->nl_counts = D.alloc<int>(b->n_total);
   b->nl_xref = D.alloc<double>(3 * (size_t)b->n_total);
   b->nl_sys_moved = D.alloc<int32_t>(b->n_sys);
   b->nl_ctl = D.alloc<int32_t>(NL_WORDS);
   for (void *p : D.ptrs)
     if (!p) return fail(ctx, PB2_ENOMEM, "neighbour-list allocation failed");
-  CUDA_TRY(ctx, cudaMemcpy(b->nl_cell_base, base.data(), base.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
-  CUDA_TRY(ctx, cudaMemcpy(b->nl_cell_budget, budget.data(), budget.size() * sizeof(int32_t),
-                           cudaMemcpyHostToDevice));
-  CUDA_TRY(ctx, cudaMemcpy(b->nl_cell_sys, cell_sys.data(), cell_sys.size() * sizeof(int32_t),
-                           cudaMemcpyHostToDevice));
   CUDA_TRY(ctx, cudaMemset(b->nl_ctl, 0, NL_WORDS * sizeof(int32_t)));
   CUDA_TRY(ctx, cudaMemset(b->nl_sys_moved, 0, b->n_sys * sizeof(int32_t)));
   return PB2_OK;
@@ -429,7 +229,6 @@ static int nl_settle(pb2_batch *b, cudaStream_t st) {
   int32_t ctl[NL_WORDS];
   CUDA_TRY(ctx, cudaMemcpyAsync(ctl, b->nl_ctl, sizeof ctl, cudaMemcpyDeviceToHost, st));
   CUDA_TRY(ctx, cudaStreamSynchronize(st));
-  if (ctl[NL_CELLFULL]) return fail(ctx, PB2_ENLOVERFLOW, "a neighbour-list cell holds more than 4096 atoms");
   const int maxc = ctl[NL_MAXCOUNT];
   if (maxc <= b->nl_capacity) return PB2_OK;
   const int fixed = b->params.nl_capacity;

@@ -537,32 +537,11 @@ __global__ void born_finalize(const FinalizeArgs a) {
 // atomic counter (items are sorted by cost, largest first), and the last
 // warp to finish resets the counter for the next launch.
 // ALL: GB, Coulomb and LJ all enabled (the term switches fold away).
-#ifndef PB2_MINB_BORN
-#define PB2_MINB_BORN 3
-#endif
-#ifndef PB2_MINB_CHAIN
-#define PB2_MINB_CHAIN 2
-#endif
-#ifndef PB2_MINB_FORCE
-#define PB2_MINB_FORCE 2
-#endif
-// threads per block of each pass (a multiple of 32, at most 256)
-#ifndef PB2_THREADS_BORN
-#define PB2_THREADS_BORN 256
-#endif
-#ifndef PB2_THREADS_FORCE
-#define PB2_THREADS_FORCE 256
-#endif
-#ifndef PB2_THREADS_CHAIN
-#define PB2_THREADS_CHAIN 256
-#endif
-template <int PASS>
-constexpr int kTileThreads =
-    PASS == PASS_BORN ? PB2_THREADS_BORN : (PASS == PASS_CHAIN ? PB2_THREADS_CHAIN : PB2_THREADS_FORCE);
-template <int PASS>
-constexpr int kTileMinBlocks = PASS == PASS_BORN ? PB2_MINB_BORN : (PASS == PASS_CHAIN ? PB2_MINB_CHAIN : PB2_MINB_FORCE);
-template <int PASS, bool CUT, bool ALL = false>
-__global__ void __launch_bounds__(kTileThreads<PASS>, kTileMinBlocks<PASS>)
+// THREADS, MINB: the block shape (threads per block, and the blocks per SM
+// the register budget is sized for); every pass is compiled for the shapes
+// of kShapes and the autotuner picks one per pass at run time.
+template <int PASS, bool CUT, bool ALL, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB)
     tile2_kernel(const __grid_constant__ PairArgs a) {
   const int lane = threadIdx.x & 31;
   const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
@@ -573,7 +552,7 @@ __global__ void __launch_bounds__(kTileThreads<PASS>, kTileMinBlocks<PASS>)
   K.src = (lane + 1) & 31;
   K.lane = lane;
   // closed-form queues of the descreening and chain passes, one per warp
-  constexpr int kWarps = kTileThreads<PASS> / 32;
+  constexpr int kWarps = THREADS / 32;
   __shared__ int2 s_cfq[PASS == PASS_FORCE ? 1 : kWarps][PASS == PASS_FORCE ? 1 : kCfCap];
   // the j-block of the current tile, one JTile per warp (2 KB)
   __shared__ JTile s_jt[kWarps];
@@ -608,7 +587,7 @@ __global__ void __launch_bounds__(kTileThreads<PASS>, kTileMinBlocks<PASS>)
         const int c = it - n_items;
         if (c < a.n_bonded_chunks) {
           const int t1 = min((c + 1) * kBondedChunk, bonded_total(a.bonded));
-          for (int t = c * kBondedChunk + lane; t < t1; t += 32) bonded_term(a.bonded, t);
+          for (int t = c * kBondedChunk + lane; t < t1; t += 32) bonded_term_call(a.bonded, t);
           continue;
         }
       }
@@ -832,32 +811,51 @@ __global__ void bbox_kernel(const SysInfo *sys, const int32_t *blk_sys, const fl
 
 // --------------------------------------------------------------- launchers
 
-template <int PASS, bool CUT, bool ALL>
+// Block shapes compiled for each pass (threads, min blocks per SM); entry 0
+// is the default.  The descreening pass holds fewer registers, so its
+// shapes allow more resident blocks.
+struct Shape {
+  int threads, minb;
+};
+constexpr Shape kShapes[3][kShapesPerPass] = {
+    {{256, 3}, {256, 2}, {128, 6}},   // descreening
+    {{256, 2}, {128, 4}, {128, 5}},   // force
+    {{256, 2}, {128, 4}, {128, 5}}};  // chain rule
+
+template <int PASS, bool CUT, bool ALL, int SH>
 static void launch_one(const PairArgs &a, int grid, cudaStream_t st) {
-  tile2_kernel<PASS, CUT, ALL><<<grid, kTileThreads<PASS>, 0, st>>>(a);
+  constexpr Shape sh = kShapes[PASS][SH];
+  tile2_kernel<PASS, CUT, ALL, sh.threads, sh.minb><<<grid, sh.threads, 0, st>>>(a);
 }
 
-cudaError_t launch_tiles(int pass, const PairArgs &a, int grid, cudaStream_t st) {
-  if (a.n_items <= 0) return cudaSuccess;
-  const bool cut = a.cut != 0;
+template <int PASS, bool CUT, bool ALL>
+static void launch_shaped(const PairArgs &a, int grid, int shape, cudaStream_t st) {
+  switch (shape) {
+    case 1: launch_one<PASS, CUT, ALL, 1>(a, grid, st); break;
+    case 2: launch_one<PASS, CUT, ALL, 2>(a, grid, st); break;
+    default: launch_one<PASS, CUT, ALL, 0>(a, grid, st);
+  }
+}
+
+cudaError_t launch_tiles(int pass, const PairArgs &a, int grid, int shape, cudaStream_t st) {
   switch (pass) {
     case PASS_BORN:
-      if (cut) launch_one<PASS_BORN, true, false>(a, grid, st);
-      else launch_one<PASS_BORN, false, false>(a, grid, st);
+      if (a.cut) launch_shaped<PASS_BORN, true, false>(a, grid, shape, st);
+      else launch_shaped<PASS_BORN, false, false>(a, grid, shape, st);
       break;
     case PASS_CHAIN:
-      if (cut) launch_one<PASS_CHAIN, true, false>(a, grid, st);
-      else launch_one<PASS_CHAIN, false, false>(a, grid, st);
+      if (a.cut) launch_shaped<PASS_CHAIN, true, false>(a, grid, shape, st);
+      else launch_shaped<PASS_CHAIN, false, false>(a, grid, shape, st);
       break;
     default: {
       const int all_terms = PB2_USE_GB | PB2_USE_LJ | PB2_USE_COULOMB;
       const bool all = (a.terms & all_terms) == all_terms;
-      if (cut) {
-        if (all) launch_one<PASS_FORCE, true, true>(a, grid, st);
-        else launch_one<PASS_FORCE, true, false>(a, grid, st);
+      if (a.cut) {
+        if (all) launch_shaped<PASS_FORCE, true, true>(a, grid, shape, st);
+        else launch_shaped<PASS_FORCE, true, false>(a, grid, shape, st);
       } else {
-        if (all) launch_one<PASS_FORCE, false, true>(a, grid, st);
-        else launch_one<PASS_FORCE, false, false>(a, grid, st);
+        if (all) launch_shaped<PASS_FORCE, false, true>(a, grid, shape, st);
+        else launch_shaped<PASS_FORCE, false, false>(a, grid, shape, st);
       }
     }
   }
@@ -879,24 +877,47 @@ cudaError_t launch_born_finalize(const FinalizeArgs &a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-template <int PASS, bool CUT, bool ALL>
+template <int PASS, bool CUT, bool ALL, int SH>
 static int occ_one() {
+  constexpr Shape sh = kShapes[PASS][SH];
   int blocks = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, tile2_kernel<PASS, CUT, ALL>, kTileThreads<PASS>, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, tile2_kernel<PASS, CUT, ALL, sh.threads, sh.minb>,
+                                                sh.threads, 0);
   return blocks;
 }
 
-int tile_kernel_warps(int pass) {
-  return pass == PASS_BORN ? kTileThreads<PASS_BORN> / 32
-                           : (pass == PASS_CHAIN ? kTileThreads<PASS_CHAIN> / 32 : kTileThreads<PASS_FORCE> / 32);
+template <int PASS, bool CUT, bool ALL>
+static int occ_shaped(int shape) {
+  switch (shape) {
+    case 1: return occ_one<PASS, CUT, ALL, 1>();
+    case 2: return occ_one<PASS, CUT, ALL, 2>();
+    default: return occ_one<PASS, CUT, ALL, 0>();
+  }
 }
 
-int tile_kernel_occupancy(int pass, bool cut) {
+int tile_shape(int pass, int shape, int *threads, int *min_blocks) {
+  if (pass < 0 || pass > 2 || shape < 0 || shape >= kShapesPerPass) return -1;
+  *threads = kShapes[pass][shape].threads;
+  *min_blocks = kShapes[pass][shape].minb;
+  return 0;
+}
+
+int tile_kernel_warps(int pass, int shape) {
+  int t = 256, m = 0;
+  tile_shape(pass, shape, &t, &m);
+  return t / 32;
+}
+
+int tile_kernel_occupancy(int pass, bool cut, int shape) {
   int blocks;
-  if (pass == PASS_BORN) blocks = cut ? occ_one<PASS_BORN, true, false>() : occ_one<PASS_BORN, false, false>();
-  else if (pass == PASS_CHAIN) blocks = cut ? occ_one<PASS_CHAIN, true, false>() : occ_one<PASS_CHAIN, false, false>();
-  else if (cut) blocks = std::min(occ_one<PASS_FORCE, true, false>(), occ_one<PASS_FORCE, true, true>());
-  else blocks = std::min(occ_one<PASS_FORCE, false, false>(), occ_one<PASS_FORCE, false, true>());
+  if (pass == PASS_BORN)
+    blocks = cut ? occ_shaped<PASS_BORN, true, false>(shape) : occ_shaped<PASS_BORN, false, false>(shape);
+  else if (pass == PASS_CHAIN)
+    blocks = cut ? occ_shaped<PASS_CHAIN, true, false>(shape) : occ_shaped<PASS_CHAIN, false, false>(shape);
+  else if (cut)
+    blocks = std::min(occ_shaped<PASS_FORCE, true, false>(shape), occ_shaped<PASS_FORCE, true, true>(shape));
+  else
+    blocks = std::min(occ_shaped<PASS_FORCE, false, false>(shape), occ_shaped<PASS_FORCE, false, true>(shape));
   return blocks > 0 ? blocks : 1;
 }
 

@@ -14,8 +14,10 @@
 // side, so box separations shrink by at most the skin).  The pair kernels
 // still skip listed tiles that are beyond the cutoff at the current step.
 //
-// Everything stays on the device: the bounding-box kernel raises the
-// rebuild flag, and this kernel, launched every step of a cutoff run
+// Everything stays on the device: the step kernel (or, outside a step, the
+// bounding-box kernel) raises the rebuild flag when an atom has moved more
+// than skin/2 from the positions of the last build, and this kernel,
+// launched every step of a cutoff run
 // (inside the captured step graphs), returns at once unless the flag is
 // set.  A rebuild writes the new items into the buffer the pair kernels
 // are not reading, and the last warp to finish publishes it, so no launch

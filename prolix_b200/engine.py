@@ -528,6 +528,35 @@ class Batch:
     return t
 
   # neighbour list
+  # ---------------------------------------------------------------- schedule
+  def block_shapes(self, pass_: int) -> list:
+    """(threads, min blocks per SM) compiled for pair pass 0 (descreening),
+    1 (force) or 2 (chain rule)."""
+    t = (ctypes.c_int32 * 8)()
+    m = (ctypes.c_int32 * 8)()
+    n = self.lib.pb2_block_shapes(int(pass_), t, m, 8)
+    if n < 0:
+      self._check(n)
+    return [(int(t[k]), int(m[k])) for k in range(min(n, 8))]
+
+  def set_block_shape(self, pass_: int, threads: int, min_blocks: int):
+    self._check(self.lib.pb2_set_block_shape(self.handle, int(pass_), int(threads), int(min_blocks)))
+
+  def block_shape(self, pass_: int) -> tuple:
+    t, m = ctypes.c_int32(0), ctypes.c_int32(0)
+    self._check(self.lib.pb2_get_block_shape(self.handle, int(pass_), ctypes.byref(t), ctypes.byref(m)))
+    return int(t.value), int(m.value)
+
+  def set_fusion(self, flags: int):
+    """_lib.FUSE_* bits: the bonded terms in the chain pass, the Born-radius
+    finalize in the descreening pass."""
+    self._check(self.lib.pb2_set_fusion(self.handle, int(flags)))
+
+  def fusion(self) -> int:
+    f = ctypes.c_int32(0)
+    self._check(self.lib.pb2_get_fusion(self.handle, ctypes.byref(f)))
+    return int(f.value)
+
   def nl_build(self, stream=None):
     self._check(self.lib.pb2_nl_build(self.handle, stream))
 

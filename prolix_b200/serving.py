@@ -1,20 +1,26 @@
 """Continuous-batching server for "run K Langevin steps of system S" jobs.
 
-Requests that arrive while others run join the device batch at the next
-tick: each tick advances every running system by the same number of steps
-(at most ``chunk``, and never past the nearest completion), then finished,
-cancelled or failed requests end, and waiting requests are admitted while
-the running systems stay inside the atom and HBM budgets.  All systems of a
-tick share one launch per kernel (the ragged batch), so short and long,
-small and large jobs overlap on the GPU.  The batch is rebuilt when
-requests are admitted (their initial momenta and forces come from one
-langevin_init of the new batch) or when ended systems, which keep stepping
-unread until then, hold a quarter of its atoms.
+Requests that arrive while others run are admitted at the next tick, while
+the running systems stay inside the atom and HBM budgets.  Each admission
+wave becomes a cohort: one device batch holding just the admitted systems,
+created from their descriptions (the only upload) and initialised on the
+device.  Running cohorts are never rebuilt and their state never leaves the
+device: each tick advances every cohort by the same number of steps on its
+own CUDA stream, so all cohorts' kernels overlap on the GPU, and only a
+cohort in which a request has just finished is read back (the finished
+systems' positions, momenta and keys are the result).  A cohort whose
+requests have all ended is released; one with some ended systems keeps
+stepping them unread until its last request ends.
+
+The step count of a tick is the largest of chunk, chunk/2, chunk/5,
+chunk/10, 1 (and 1-step divisions thereof) that does not pass the nearest
+completion, so every cohort captures at most a handful of step graphs.
 
 Systems never interact and forces use order-independent fixed-point sums,
 so a request's result is bit-identical whether it ran alone or in any mix
 (checked by tests/test_gpu_serving.py).  A request whose state turns
-non-finite is evicted with an error; the others carry on unchanged.
+non-finite (the step kernels' status bits) is evicted with an error; the
+others carry on unchanged.
 
 This has no counterpart in prolix (whose batched runs are offline
 ``batched_produce`` calls, batched_simulate.py:1125-1163); it drives the
@@ -68,27 +74,47 @@ class Result:
 @dataclasses.dataclass
 class _Slot:
   req: Request
-  x: np.ndarray
-  p: np.ndarray
-  f: np.ndarray   # forces at x: a rebuilt batch restores them instead of re-evaluating
-  key: np.ndarray
   done: int
   admitted: float
 
 
-_FIELDS = ("position", "momentum", "force", "key")
+class _Cohort:
+  """The systems admitted together: one device batch, one stream."""
+
+  def __init__(self, batch, slots, stream):
+    self.batch = batch
+    self.slots = slots    # batch system index -> running slot, None once its request ended
+    self.stream = stream  # a stream object with a .cuda_stream handle, or None
+
+  def live(self) -> bool:
+    return any(s is not None for s in self.slots)
+
+  def atoms(self) -> int:
+    return int(np.sum(self.batch.sizes))
+
+
+_FIELDS = ("position", "momentum", "key")
 
 
 def _percentile(v, q):
   return float(np.percentile(np.asarray(v), q)) if len(v) else float("nan")
 
 
+def _tick_steps(chunk: int, limit: int) -> int:
+  """The largest of chunk, chunk/2, chunk/5, chunk/10 and 1 not above limit."""
+  for d in (1, 2, 5, 10):
+    n = max(1, chunk // d)
+    if n <= limit:
+      return n
+  return 1
+
+
 class Server:
-  """Admission by budget, resident state, continuous batching."""
+  """Admission by budget, device-resident cohorts, continuous batching."""
 
   def __init__(self, device: int = 0, hbm_budget_bytes: float = 150e9,
                max_batch_atoms: int = 1_000_000, chunk: int = 50, cutoff: float = 0.0,
-               clock=time.perf_counter, batch_factory=None):
+               clock=time.perf_counter, batch_factory=None, stream_factory=None):
     self.device = device
     self.batch_factory = batch_factory or engine.Batch
     self.hbm_budget = float(hbm_budget_bytes)
@@ -98,16 +124,22 @@ class Server:
     self.clock = clock
     self.t0 = clock()
     self.queue: deque[Request] = deque()
-    self.active: list[_Slot] = []
+    self.cohorts: list[_Cohort] = []
     self.results: dict[int, Result] = {}
     self.cancelled: set[int] = set()
     self._next_id = 0
-    self._batch = None
-    self._slot_of: list = []  # batch system index -> running slot, None once its request ended
     self.atom_steps = 0
     self.ticks = 0
+    self.cohorts_created = 0
+    self.readbacks = 0
+    self._streams = stream_factory
+    self._sync = None
     if self.batch_factory is engine.Batch:
       engine.Context.get(device)  # open the device now, not inside the first request
+      if self._streams is None:
+        import torch
+        self._streams = lambda: torch.cuda.Stream(device=device)
+        self._sync = lambda: torch.cuda.synchronize(device)
 
   # ------------------------------------------------------------------ api
   def now(self) -> float:
@@ -124,7 +156,7 @@ class Server:
       self.results[req.rid] = Result(req.rid, None, None, None, 0, req.arrival, float("nan"),
                                      self.now(), error="system larger than the server budget")
       return req.rid
-    if "excl_pairs" not in req.system:  # once per request, not on every batch rebuild
+    if "excl_pairs" not in req.system:  # once per request, not per cohort
       pairs, kind = topology.exclusion_pairs(req.system.get("bonds", np.zeros((0, 2))), n)
       req.system = dict(req.system, excl_pairs=pairs, excl_kind=kind)
     self.queue.append(req)
@@ -133,17 +165,21 @@ class Server:
   def cancel(self, rid: int):
     self.cancelled.add(rid)
 
+  @property
+  def active(self) -> list:
+    """Running requests' slots."""
+    return [s for c in self.cohorts for s in c.slots if s is not None]
+
   def idle(self) -> bool:
-    return not self.queue and not self.active
+    return not self.queue and not self.cohorts
 
   # ------------------------------------------------------------------ internals
   def _used(self):
-    atoms = sum(len(s.req.system["charges"]) for s in self.active)
+    atoms = sum(c.atoms() for c in self.cohorts)  # ended systems still hold their memory
     return atoms, atoms * BYTES_PER_ATOM
 
   def _admit(self, now: float) -> list:
-    """Take waiting requests while the budget allows (first come, first
-    served); they join the batch at the next rebuild."""
+    """Take waiting requests while the budget allows (first come, first served)."""
     atoms, used = self._used()
     admitted = []
     while self.queue and self.queue[0].arrival <= now:
@@ -157,10 +193,6 @@ class Server:
       if atoms + n > self.max_atoms or used + n * BYTES_PER_ATOM > self.hbm_budget:
         break  # first-come first-served: wait for room
       self.queue.popleft()
-      # fix the system's float32 frame for its lifetime (bit-identical forces
-      # whatever batch it runs in)
-      if req.system.get("origin") is None:
-        req.system = dict(req.system, origin=engine.default_origin(req.system["positions"]))
       admitted.append(req)
       atoms += n
       used += n * BYTES_PER_ATOM
@@ -170,114 +202,86 @@ class Server:
     self.results[req.rid] = Result(req.rid, None, None, None, 0, req.arrival, admitted, now,
                                    error=msg)
 
-  def _build(self, admitted, now):
-    """A new batch of the running systems and the admitted requests.  Each
-    system is described by its submitted positions, which fix its stored
-    atom order.  One langevin_init draws the admitted requests' momenta from
-    their keys and evaluates their forces (the same bits as alone); then every
-    running system's saved state is restored, forces included, since forces
-    depend only on the system's own float32 frame."""
-    run_sys = [dict(s.req.system, key=tuple(int(v) for v in s.key), dt=s.req.dt, kT=s.req.kT,
-                    gamma=s.req.gamma) for s in self.active]
-    new_sys = [dict(r.system, key=r.key, dt=r.dt, kT=r.kT, gamma=r.gamma) for r in admitted]
-    if self._batch is not None:
-      self._batch.close()
-      self._batch = None
-    batch = self.batch_factory(run_sys + new_sys, cutoff=self.cutoff, device=self.device,
+  def _new_cohort(self, admitted, now):
+    """A batch of just the admitted requests: their descriptions are the
+    only upload; momenta and forces come from one langevin_init."""
+    systems = [dict(r.system, key=r.key, dt=r.dt, kT=r.kT, gamma=r.gamma) for r in admitted]
+    batch = self.batch_factory(systems, cutoff=self.cutoff, device=self.device,
                                graph_chunk=self.chunk)
-    self._batch = batch
-    nr = len(run_sys)
-    slot_of = list(self.active)
-    st = None
-    if admitted:
-      batch.langevin_init()
-      st = batch.get_state(fields=_FIELDS)
-      status = batch.status(clear=True)
-      for k, r in enumerate(admitted):
-        b = nr + k
-        lo, hi = batch.offsets[b], batch.offsets[b + 1]
-        x = st["position"][lo:hi]
-        if status[b] & (STATUS_NONFINITE | STATUS_FORCE_RANGE) or not np.isfinite(x).all():
-          self._fail(r, now, now, "non-finite initial state")
-          slot_of.append(None)
-          continue
-        slot_of.append(_Slot(r, x.copy(), st["momentum"][lo:hi].copy(), st["force"][lo:hi].copy(),
-                             st["key"][b].copy(), 0, now))
-    self._slot_of = slot_of  # batch system index -> running slot (None: its request ended)
-    self.active = [s for s in slot_of if s is not None]
-    if nr:
-      # the running systems' saved state (the admitted ones keep the init's)
-      def rows(field, st_field):
-        return np.concatenate([getattr(slot_of[b], field) if b < nr
-                               else st[st_field][batch.offsets[b]:batch.offsets[b + 1]]
-                               for b in range(len(slot_of))])
-      keys = np.stack([slot_of[b].key if b < nr else st["key"][b] for b in range(len(slot_of))])
-      batch.set_full_state(rows("x", "position"), rows("p", "momentum"), rows("f", "force"), key=keys)
+    self.cohorts_created += 1
+    batch.langevin_init()
+    status = batch.status(clear=True)
+    slots = []
+    for k, r in enumerate(admitted):
+      if status[k] & (STATUS_NONFINITE | STATUS_FORCE_RANGE):
+        self._fail(r, now, now, "non-finite initial state")
+        slots.append(None)
+      else:
+        slots.append(_Slot(r, 0, now))
+    cohort = _Cohort(batch, slots, self._streams() if self._streams else None)
+    if cohort.live():
+      self.cohorts.append(cohort)
+    else:
+      batch.close()
 
-  def _save(self):
-    st = self._batch.get_state(fields=_FIELDS)
-    for b, s in enumerate(self._slot_of):
-      if s is None:
-        continue
-      lo, hi = self._batch.offsets[b], self._batch.offsets[b + 1]
-      s.x = st["position"][lo:hi].copy()
-      s.p = st["momentum"][lo:hi].copy()
-      s.f = st["force"][lo:hi].copy()
-      s.key = st["key"][b].copy()
-    return self._batch.status(clear=True)
-
-  def _ended_atoms(self) -> int:
-    return sum(self._batch.sizes[b] for b, s in enumerate(self._slot_of) if s is None)
+  def _retire(self):
+    keep = []
+    for c in self.cohorts:
+      if c.live():
+        keep.append(c)
+      else:
+        c.batch.close()
+    self.cohorts = keep
 
   def tick(self) -> bool:
-    """Admit, advance every running system, retire.  False when idle.
-
-    The batch is rebuilt only when requests are admitted, or when systems
-    whose requests have ended make up more than a quarter of its atoms:
-    until then they keep stepping unread (each system is independent, so
-    the others' results do not change)."""
+    """Admit, advance every cohort, retire.  False when idle."""
     now = self.now()
     admitted = self._admit(now)
     if self.cancelled:
-      for b, s in enumerate(self._slot_of):
-        if s is not None and s.req.rid in self.cancelled:
-          self._slot_of[b] = None
-      for s in self.active:
-        if s.req.rid in self.cancelled and s.req.rid not in self.results:
-          self._fail(s.req, s.admitted, now, "cancelled")
-      self.active = [s for s in self.active if s.req.rid not in self.cancelled]
-    if not self.active and not admitted:
-      if self._batch is not None:
-        self._batch.close()
-        self._batch = None
-        self._slot_of = []
+      for c in self.cohorts:
+        for b, s in enumerate(c.slots):
+          if s is not None and s.req.rid in self.cancelled:
+            if s.req.rid not in self.results:
+              self._fail(s.req, s.admitted, now, "cancelled")
+            c.slots[b] = None
+    if admitted:
+      self._new_cohort(admitted, now)
+    self._retire()
+    if not self.cohorts:
       return bool(self.queue)
-    if (admitted or self._batch is None
-        or self._ended_atoms() * 4 > int(np.sum(self._batch.sizes))):
-      self._build(admitted, now)
-      if not self.active:
-        return bool(self.queue)
-    n = min(self.chunk, min(s.req.n_steps - s.done for s in self.active))
-    self._batch.langevin_run(n)
-    status = self._save()
+    remaining = min(s.req.n_steps - s.done for s in self.active)
+    n = _tick_steps(self.chunk, remaining)
+    for c in self.cohorts:
+      c.batch.langevin_run(n, c.stream.cuda_stream if c.stream is not None else None)
+    if self._sync:
+      self._sync()
     self.ticks += 1
     now = self.now()
-    for b, s in enumerate(self._slot_of):
-      if s is None:
-        continue
-      s.done += n
-      self.atom_steps += n * len(s.req.system["charges"])
-      ended = True
-      if status[b] & (STATUS_NONFINITE | STATUS_FORCE_RANGE) or not np.isfinite(s.x).all():
-        self._fail(s.req, s.admitted, now, "non-finite state: evicted")
-      elif s.done >= s.req.n_steps:
-        self.results[s.req.rid] = Result(s.req.rid, s.x, s.p, s.key, s.done, s.req.arrival,
-                                         s.admitted, now)
-      else:
-        ended = False
-      if ended:
-        self._slot_of[b] = None
-    self.active = [s for s in self._slot_of if s is not None]
+    for c in self.cohorts:
+      status = c.batch.status(clear=True)
+      st = None
+      for b, s in enumerate(c.slots):
+        if s is None:
+          continue
+        s.done += n
+        self.atom_steps += n * len(s.req.system["charges"])
+        if status[b] & (STATUS_NONFINITE | STATUS_FORCE_RANGE):
+          self._fail(s.req, s.admitted, now, "non-finite state: evicted")
+          c.slots[b] = None
+        elif s.done >= s.req.n_steps:
+          if st is None:  # a finished request: the cohort's state comes back once
+            st = c.batch.get_state(fields=_FIELDS)
+            self.readbacks += 1
+          lo, hi = c.batch.offsets[b], c.batch.offsets[b + 1]
+          x = st["position"][lo:hi].copy()
+          if not np.isfinite(x).all():
+            self._fail(s.req, s.admitted, now, "non-finite state: evicted")
+          else:
+            self.results[s.req.rid] = Result(s.req.rid, x, st["momentum"][lo:hi].copy(),
+                                             st["key"][b].copy(), s.done, s.req.arrival,
+                                             s.admitted, now)
+          c.slots[b] = None
+    self._retire()
     return True
 
   def run(self, requests=(), until_idle=True, sleep=time.sleep):
@@ -287,7 +291,7 @@ class Server:
       now = self.now()
       while pending and pending[0].arrival <= now:
         self.submit(pending.popleft())
-      if self.active or (self.queue and self.queue[0].arrival <= now):
+      if self.cohorts or (self.queue and self.queue[0].arrival <= now):
         self.tick()
       elif pending:
         sleep(max(0.0, pending[0].arrival - self.now()))
@@ -295,9 +299,9 @@ class Server:
         sleep(max(0.0, self.queue[0].arrival - self.now()))
       elif until_idle:
         break
-    if self._batch is not None:
-      self._batch.close()
-      self._batch = None
+    for c in self.cohorts:
+      c.batch.close()
+    self.cohorts = []
     return self.results
 
   def report(self) -> dict:
@@ -309,7 +313,7 @@ class Server:
             "p50_s": _percentile(lat, 50), "p99_s": _percentile(lat, 99),
             "atom_steps": int(self.atom_steps), "span_s": span,
             "atom_steps_per_s": self.atom_steps / span if span > 0 else float("nan"),
-            "ticks": self.ticks}
+            "ticks": self.ticks, "cohorts": self.cohorts_created, "readbacks": self.readbacks}
 
 
 def poisson_requests(n: int, rate: float, seed: int, n_lo=100, n_hi=10_000, k_lo=1_000,

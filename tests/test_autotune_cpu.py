@@ -15,8 +15,26 @@ class FakeBatch:
     self.state = {"position": np.arange(6.0).reshape(2, 3), "momentum": np.ones((2, 3)),
                   "key": np.array([[1, 2]], dtype=np.uint32)}
 
+    self.shapes = [(256, 3), (256, 2), (256, 2)]
+    self.fuse = 1
+
   def set_tile_segment(self, s):
     self.seg = s
+
+  def block_shapes(self, p):
+    return [(256, 3), (128, 6)] if p == 0 else [(256, 2), (128, 4)]
+
+  def set_block_shape(self, p, t, m):
+    self.shapes[p] = (t, m)
+
+  def block_shape(self, p):
+    return self.shapes[p]
+
+  def set_fusion(self, f):
+    self.fuse = f
+
+  def fusion(self):
+    return self.fuse
 
   def get_state(self):
     return {k: v.copy() for k, v in self.state.items()}
@@ -35,11 +53,26 @@ def test_bucket_key_rounds_to_powers_of_two():
 def test_tune_picks_fastest_and_caches(tmp_path, monkeypatch):
   monkeypatch.setenv("PROLIX_B200_TUNE_CACHE", str(tmp_path / "t.json"))
   cost = {2: 3.0, 4: 1.5, 8: 2.0}
-  monkeypatch.setattr(autotune, "measure", lambda b, s, steps=4: cost[s])
+
+  def timed(b, steps=4):
+    # segment cost, minus a gain for a 128-thread force pass and for
+    # fusion 3; everything else unchanged
+    ms = cost[b.seg]
+    if b.shapes[1] == (128, 4):
+      ms -= 0.2
+    if b.fuse == 3:
+      ms -= 0.1
+    return ms
+
+  monkeypatch.setattr(autotune, "measure", lambda b, s, steps=4: (b.set_tile_segment(s), timed(b))[1])
+  monkeypatch.setattr(autotune, "_time", timed)
   monkeypatch.setattr(autotune, "_gpu_name", lambda: "FAKE")
   fb = FakeBatch([100, 200])
   r = autotune.tune(fb, candidates=(2, 4, 8))
   assert r["segment"] == 4 and fb.seg == 4 and not r["cached"]
+  assert r["shapes"] == [[256, 3], [128, 4], [256, 2]] and fb.shapes[1] == (128, 4)
+  assert r["fusion"] == 3 and fb.fuse == 3
+  assert abs(r["ms"] - 1.2) < 1e-12
   fb2 = FakeBatch([100, 200])
   r2 = autotune.tune(fb2, candidates=(2, 4, 8))
-  assert r2["cached"] and fb2.seg == 4
+  assert r2["cached"] and fb2.seg == 4 and fb2.shapes[1] == (128, 4) and fb2.fuse == 3

@@ -1,5 +1,6 @@
-"""Autotuner on the GPU: any tile segment gives bit-identical forces, and
-tuning leaves the simulation state exactly as it was."""
+"""Autotuner on the GPU: any tile segment, block shape or fusion choice
+gives bit-identical forces and steps, and tuning leaves the simulation
+state exactly as it was."""
 
 import numpy as np
 import pytest
@@ -20,6 +21,39 @@ def test_forces_independent_of_tile_segment():
       b.set_tile_segment(seg)
       assert b.tile_segment() == seg
       np.testing.assert_array_equal(b.forces(), ref)
+
+
+def test_block_shapes_and_fusion_leave_results_bitwise_equal():
+  from oracle import energy as oenergy
+  systems = _systems()
+  fields = ("position", "momentum", "force")
+  with engine.Batch(systems) as b:
+    ref = b.forces()
+    b.langevin_init()
+    b.langevin_run(7)
+    ref_st = b.get_state(fields=fields)
+  for p in range(3):
+    with engine.Batch(systems) as b:
+      for t, m in b.block_shapes(p):
+        b.set_block_shape(p, t, m)
+        assert b.block_shape(p) == (t, m)
+        np.testing.assert_array_equal(b.forces(), ref)
+  for f in range(4):
+    with engine.Batch(systems) as b:
+      b.set_fusion(f)
+      assert b.fusion() == f
+      b.langevin_init()
+      b.langevin_run(7)
+      st = b.get_state(fields=fields)
+      for k in fields:
+        np.testing.assert_array_equal(st[k], ref_st[k])
+  # and the tuned choice matches the oracle
+  s = systems[1]
+  e_ref, f_ref, _ = oenergy.energy_forces(s, s["positions"])
+  with engine.Batch([s]) as b:
+    autotune.tune(b, candidates=(4, 16), steps=2, use_cache=False)
+    f = b.forces()
+  assert np.linalg.norm(f - f_ref) / np.linalg.norm(f_ref) < 1e-5
 
 
 def test_tune_restores_state_and_caches(tmp_path, monkeypatch):

@@ -26,6 +26,8 @@ def oracle(s, cutoff, gb_cutoff):
   e = dict(e)
   e["cmap"] = ec
   e["total"] += ec
+  for k in ("improper", "urey_bradley", "exception"):  # none in these systems
+    e.setdefault(k, 0.0)
   return e, f + fc
 
 

@@ -29,7 +29,7 @@ class FakeBatch:
   def langevin_init(self):
     pass
 
-  def langevin_run(self, n):
+  def langevin_run(self, n, stream=None):
     self.x = self.x + 0.001 * n
     self.p = self.p + n
 
@@ -105,24 +105,47 @@ def test_poisson_stream_is_seeded():
   assert all(np.diff([r.arrival for r in a]) > 0)
 
 
-def test_ended_requests_do_not_force_a_rebuild():
-  # four requests admitted together, ending one after another: the batch is
-  # built once for the admission and rebuilt only when the ended systems
-  # hold more than a quarter of its atoms; every request still gets exactly
-  # its steps
+def test_cohorts_are_never_rebuilt_and_state_stays_put():
+  # each admission wave becomes one cohort batch; running cohorts are never
+  # rebuilt or reloaded (set_full_state is never called), their state is read
+  # only when one of their requests finishes, and every request still gets
+  # exactly its steps
   clk = Clock()
   built = []
 
+  class NoReload(FakeBatch):
+    def set_full_state(self, *a, **k):
+      raise AssertionError("a running cohort's state was reloaded")
+
+    set_state = set_full_state
+
   def factory(systems, **kw):
     built.append(len(systems))
-    return FakeBatch(systems, **kw)
+    return NoReload(systems, **kw)
 
   srv = serving.Server(chunk=10, clock=clk, batch_factory=factory)
   reqs = [_req(i, 10, steps, 0.0) for i, steps in enumerate((10, 20, 30, 40))]
+  reqs += [_req(4, 10, 15, 0.05), _req(5, 10, 25, 0.05)]
+  orig_tick = srv.tick
+
+  def tick():
+    clk.t += 0.01
+    return orig_tick()
+
+  srv.tick = tick
   res = srv.run(reqs, sleep=clk.sleep)
   for r in reqs:
     assert res[r.rid].error is None and res[r.rid].steps == r.n_steps
     np.testing.assert_allclose(res[r.rid].momentum, r.n_steps)
-  # one build with all four; after two have ended (half the atoms) a
-  # rebuild with the remaining two; the last one alone when three have ended
-  assert built[0] == 4 and len(built) <= 3 and all(b < 4 for b in built[1:])
+  assert built == [4, 2]
+  rep = srv.report()
+  assert rep["cohorts"] == 2 and rep["readbacks"] <= len(reqs)
+
+
+def test_tick_lengths_come_from_a_small_set():
+  seen = set()
+  for limit in range(1, 200):
+    n = serving._tick_steps(50, limit)
+    assert 1 <= n <= min(50, limit)
+    seen.add(n)
+  assert seen <= {50, 25, 10, 5, 1}
