@@ -423,6 +423,18 @@ int pb2_nl_last_build_ms(pb2_batch *batch, double *ms);
 int pb2_set_tile_segment(pb2_batch *batch, int32_t segment);
 int pb2_get_tile_segment(const pb2_batch *batch, int32_t *segment);
 
+/* Retire system `sys` of the batch, in stream order on `stream`: no later
+ * step, closing half kick or pair evaluation of the batch touches it, so its
+ * positions, momenta and key stay as the last step left them, and the pair
+ * kernels' live work list drops its items (an ordered on-device compaction;
+ * with a pair list, a rebuild without it).  It then costs only its memory;
+ * the other systems' results are bit-identical with or without it.  Its
+ * forces, energies and Born radii are undefined from then on.  Irreversible;
+ * retiring a retired system does nothing.  For continuous batching, where
+ * prolix has no counterpart (its batches run to the end,
+ * batched_simulate.py:1125-1163). */
+int pb2_retire_system(pb2_batch *batch, int32_t sys, void *stream);
+
 /* Block shape of a pair pass (pass 0 descreening, 1 force, 2 chain rule):
  * threads per block and the resident blocks per SM its registers are sized
  * for.  Each pass is compiled for a few shapes: pb2_block_shapes fills up to

@@ -72,6 +72,7 @@ static PairArgs pair_args(pb2_batch *b) {
   a.sys = b->sys;
   a.items = b->items2;
   a.n_items = b->n_items2;
+  a.item_count = b->item_count;
   a.terms = b->params.terms;
   a.excl_ent = b->excl_ent;
   a.excl_rows = b->excl_rows;
@@ -118,6 +119,7 @@ static PlArgs pl_args(pb2_batch *b) {
   a.ctl = b->pl_ctl;
   a.reach2 = b->pl_reach2;
   a.seg = b->params.tile_segment;
+  a.retired = b->retired;
   return a;
 }
 
@@ -136,6 +138,7 @@ static IntArgs int_args(pb2_batch *b, int parity, int finish_prev) {
   a.charge = b->charge;
   a.posq = b->posq;
   a.keys = b->keys;
+  a.splits = b->key_splits;
   a.steps = b->steps;
   a.status = b->status;
   a.n_total = b->n_total;
@@ -154,6 +157,7 @@ static IntArgs int_args(pb2_batch *b, int parity, int finish_prev) {
   a.n_blocks = b->n_blocks;
   a.pl_ref = b->pl_on ? b->pl_ref : nullptr;
   a.pl_ctl = b->pl_on ? b->pl_ctl : nullptr;
+  a.retired = b->retired;
   return a;
 }
 
@@ -255,16 +259,28 @@ static void set_pair_grid(pb2_batch *b, int p) {
 }
 
 // (Re)build the pair kernels' two-i-block work list and their grids (one
-// resident wave each; warps take items dynamically).
+// resident wave each; warps take items dynamically).  The kernels read the
+// live list: the full one without the items of retired systems.
 static int setup_items2(pb2_batch *b, int seg) {
   pb2_ctx *ctx = b->ctx;
   std::vector<TileItem> items = build_items2(b->sys_host, seg);
   b->dev.release(b->items2);
+  b->dev.release(b->items2_all);
   b->items2 = b->dev.alloc<TileItem>(std::max<size_t>(items.size(), 1));
-  if (!b->items2) return fail(ctx, PB2_ENOMEM, "work-item allocation failed");
+  b->items2_all = b->dev.alloc<TileItem>(std::max<size_t>(items.size(), 1));
+  if (!b->items2 || !b->items2_all) return fail(ctx, PB2_ENOMEM, "work-item allocation failed");
   if (!items.empty())
-    CUDA_TRY(ctx, cudaMemcpy(b->items2, items.data(), items.size() * sizeof(TileItem), cudaMemcpyHostToDevice));
+    CUDA_TRY(ctx, cudaMemcpy(b->items2_all, items.data(), items.size() * sizeof(TileItem), cudaMemcpyHostToDevice));
   b->n_items2 = (int)items.size();
+  if (!b->retired) {
+    b->retired = b->dev.alloc<int8_t>(b->n_sys);
+    b->item_count = b->dev.alloc<int32_t>(1);
+    if (!b->retired || !b->item_count) return fail(ctx, PB2_ENOMEM, "work-item allocation failed");
+    CUDA_TRY(ctx, cudaMemset(b->retired, 0, b->n_sys));
+    b->retired_host.assign(b->n_sys, 0);
+  }
+  CUDA_TRY(ctx, launch_retire(-1, b->retired, b->items2_all, b->n_items2, b->items2, b->item_count, nullptr, nullptr));
+  CUDA_TRY(ctx, cudaDeviceSynchronize());
   std::vector<int32_t> per_sys(b->n_sys, 0);
   for (const TileItem &t : items) ++per_sys[t.sys];
   if (!b->sys_items) {
@@ -763,6 +779,7 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   b->dedb_acc = D.alloc<long long>(N);
   b->energy = D.alloc<long long>((size_t)n_systems * PB2_NTERMS);
   b->keys = D.alloc<uint32_t>(4 * (size_t)n_systems);
+  b->key_splits = D.alloc<uint32_t>(8 * (size_t)n_systems);
   b->steps = D.alloc<long long>(n_systems);
   b->status = D.alloc<uint32_t>(n_systems);
   b->guard_end = D.alloc<int32_t>(1);
@@ -814,6 +831,7 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
       (rc = upload(ctx, d_cgrid, cgrid)) || (rc = upload(ctx, d_cmoff, cmoff)) ||
       (rc = upload(ctx, d_eidx, eidx)) || (rc = upload(ctx, d_epar, epar)))
     return rc;
+  CUDA_TRY(ctx, launch_key_splits(int_args(b.get(), 0, 0), nullptr));
   CUDA_TRY(ctx, cudaMemset(b->px, 0, N * sizeof(double)));
   CUDA_TRY(ctx, cudaMemset(b->py, 0, N * sizeof(double)));
   CUDA_TRY(ctx, cudaMemset(b->pz, 0, N * sizeof(double)));
@@ -1291,6 +1309,7 @@ extern "C" int pb2_set_state(pb2_batch *b, const double *x, const double *p, con
   if (keys) {
     CUDA_TRY(ctx, cudaMemcpyAsync(b->keys + (size_t)b->key_parity * b->n_sys * 2, keys,
                                   (size_t)b->n_sys * 2 * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(ctx, launch_key_splits(int_args(b, b->key_parity, 0), st));
     CUDA_TRY(ctx, cudaStreamSynchronize(st));
   }
   if (x) {  // forces must follow the positions
@@ -1315,6 +1334,7 @@ extern "C" int pb2_set_full_state(pb2_batch *b, const double *x, const double *p
   if (keys) {
     CUDA_TRY(ctx, cudaMemcpyAsync(b->keys + (size_t)b->key_parity * b->n_sys * 2, keys,
                                   (size_t)b->n_sys * 2 * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(ctx, launch_key_splits(int_args(b, b->key_parity, 0), st));
   }
   CUDA_TRY(ctx, launch_posq(int_args(b, b->key_parity, 0), st));
   b->forces_valid = true;
@@ -1815,6 +1835,18 @@ extern "C" int pb2_set_tile_segment(pb2_batch *b, int32_t segment) {
   b->graphs.clear();
   for (auto &kv : b->min_graphs) cudaGraphExecDestroy(kv.second);
   b->min_graphs.clear();
+  return PB2_OK;
+}
+
+extern "C" int pb2_retire_system(pb2_batch *b, int32_t sys, void *stream) {
+  if (!b) return PB2_EINVAL;
+  pb2_ctx *ctx = b->ctx;
+  if (sys < 0 || sys >= b->n_sys) return fail(ctx, PB2_EINVAL, "system index out of range");
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  if (b->retired_host[sys]) return PB2_OK;
+  b->retired_host[sys] = 1;
+  CUDA_TRY(ctx, launch_retire(sys, b->retired, b->items2_all, b->n_items2, b->items2, b->item_count,
+                              b->pl_on ? b->pl_ctl : nullptr, (cudaStream_t)stream));
   return PB2_OK;
 }
 

@@ -67,6 +67,32 @@ __device__ __forceinline__ bool moved_past_half_skin(const IntArgs &a, int i, co
   return (double)fmaf(dx, dx, fmaf(dy, dy, dz * dz)) > S.skin_half2;
 }
 
+// keys[parity ^ 1][s] = k, and its split for the step that will read it.
+__device__ __forceinline__ void store_key(const IntArgs &a, int s, const uint32_t k[2]) {
+  const size_t slot = (size_t)(a.parity ^ 1) * a.n_sys + s;
+  a.keys[2 * slot] = k[0];
+  a.keys[2 * slot + 1] = k[1];
+  uint32_t k2[2], s2[2];
+  split_key(k[0], k[1], a.partitionable != 0, k2, s2);
+  reinterpret_cast<uint4 *>(a.splits)[slot] = make_uint4(k2[0], k2[1], s2[0], s2[1]);
+}
+
+// End of a step for system s (its first atom's thread): the advanced key,
+// and the step counter.
+__device__ __forceinline__ void advance_key(const IntArgs &a, int s, const uint32_t knew[2]) {
+  store_key(a, s, knew);
+  a.steps[s] += 1;
+}
+
+__global__ void key_splits_kernel(const IntArgs a) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < a.n_sys; s += gridDim.x * blockDim.x) {
+    const size_t slot = (size_t)a.parity * a.n_sys + s;
+    uint32_t k2[2], s2[2];
+    split_key(a.keys[2 * slot], a.keys[2 * slot + 1], a.partitionable != 0, k2, s2);
+    reinterpret_cast<uint4 *>(a.splits)[slot] = make_uint4(k2[0], k2[1], s2[0], s2[1]);
+  }
+}
+
 // One atom's plain BAOAB step; returns the float32 position it wrote.
 __device__ __forceinline__ float4 step_atom(const IntArgs &a, int i, int s, const SysInfo &S) {
   {
@@ -80,9 +106,8 @@ __device__ __forceinline__ float4 step_atom(const IntArgs &a, int i, int s, cons
     a.fx[i] = 0; a.fy[i] = 0; a.fz[i] = 0;
     double p[3] = {a.px[i], a.py[i], a.pz[i]};
     double x[3] = {a.x[i], a.y[i], a.z[i]};
-    const uint32_t *kin = a.keys + ((size_t)a.parity * a.n_sys + s) * 2;
-    uint32_t knew[2], sub[2];
-    split_key(kin[0], kin[1], a.partitionable != 0, knew, sub);
+    const uint4 sp = reinterpret_cast<const uint4 *>(a.splits)[(size_t)a.parity * a.n_sys + s];
+    const uint32_t knew[2] = {sp.x, sp.y}, sub[2] = {sp.z, sp.w};
     const uint32_t count = 3u * (uint32_t)S.n;
     const double c1 = S.c1, sg = a.sigma[i];
 #pragma unroll
@@ -100,23 +125,19 @@ __device__ __forceinline__ float4 step_atom(const IntArgs &a, int i, int s, cons
     if (!(isfinite(x[0]) && isfinite(x[1]) && isfinite(x[2]) && isfinite(p[0]) &&
           isfinite(p[1]) && isfinite(p[2])))
       atomicOr(&a.status[s], (uint32_t)PB2_STATUS_NONFINITE);
-    if (loc == 0) {
-      uint32_t *kout = a.keys + ((size_t)(a.parity ^ 1) * a.n_sys + s) * 2;
-      kout[0] = knew[0];
-      kout[1] = knew[1];
-      a.steps[s] += 1;
-    }
+    if (loc == 0) advance_key(a, s, knew);
     return q;
   }
 }
 
-__global__ void step_kernel(const IntArgs a) {
+__global__ void __launch_bounds__(256, 4) step_kernel(const IntArgs a) {
   const int lane = threadIdx.x & 31;
   const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int nw = (int)((gridDim.x * blockDim.x) >> 5);
   bool moved = false;
   for (int b = w; b < a.n_blocks; b += nw) {
     const int s = a.blk_sys[b];
+    if (a.retired[s]) continue;  // a retired system keeps its state and box
     const SysInfo &S = a.sys[s];
     const int l = (b - S.blk_base) * 32 + lane;
     const bool valid = l < S.n;
@@ -200,9 +221,8 @@ __device__ __forceinline__ float4 step_guarded_atom(const IntArgs &a, int i, int
         bits |= 1u << kWarnVlimit;
       }
     }
-    const uint32_t *kin = a.keys + ((size_t)a.parity * a.n_sys + s) * 2;
-    uint32_t knew[2], sub[2];
-    split_key(kin[0], kin[1], a.partitionable != 0, knew, sub);
+    const uint4 sp = reinterpret_cast<const uint4 *>(a.splits)[(size_t)a.parity * a.n_sys + s];
+    const uint32_t knew[2] = {sp.x, sp.y}, sub[2] = {sp.z, sp.w};
     const uint32_t count = 3u * (uint32_t)S.n;
     const double c1 = S.c1, sg = a.sigma[i];
 #pragma unroll
@@ -232,17 +252,14 @@ __device__ __forceinline__ float4 step_guarded_atom(const IntArgs &a, int i, int
       atomicOr(&a.status[s], (uint32_t)PB2_STATUS_NONFINITE);
     if (bits) atomicOr(&a.warn_flags[(size_t)a.parity * a.n_sys + s], bits);
     if (loc == 0) {
-      uint32_t *kout = a.keys + ((size_t)(a.parity ^ 1) * a.n_sys + s) * 2;
-      kout[0] = knew[0];
-      kout[1] = knew[1];
-      a.steps[s] += 1;
+      advance_key(a, s, knew);
       fold_warns(a, s);
     }
     return q;
   }
 }
 
-__global__ void step_guarded_kernel(const IntArgs a) {
+__global__ void __launch_bounds__(256, 4) step_guarded_kernel(const IntArgs a) {
   const bool cap_open = a.finish_prev || *a.guard_end;
   const int lane = threadIdx.x & 31;
   const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -250,6 +267,7 @@ __global__ void step_guarded_kernel(const IntArgs a) {
   bool moved = false;
   for (int b = w; b < a.n_blocks; b += nw) {
     const int s = a.blk_sys[b];
+    if (a.retired[s]) continue;  // a retired system keeps its state and box
     const SysInfo &S = a.sys[s];
     const int l = (b - S.blk_base) * 32 + lane;
     const bool valid = l < S.n;
@@ -264,8 +282,10 @@ __global__ void step_guarded_kernel(const IntArgs a) {
 }
 
 __global__ void finish_guarded_kernel(const IntArgs a) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) *a.guard_end = 1;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_total; i += gridDim.x * blockDim.x) {
     const int s = a.atom_sys[i];
+    if (a.retired[s]) continue;
     const double h = a.sys[s].half_dt;
     const long long lfx = a.fx[i], lfy = a.fy[i], lfz = a.fz[i];
     check_fix(a, s, lfx); check_fix(a, s, lfy); check_fix(a, s, lfz);
@@ -279,13 +299,13 @@ __global__ void finish_guarded_kernel(const IntArgs a) {
     if (!(isfinite(px) && isfinite(py) && isfinite(pz)))
       atomicOr(&a.status[s], (uint32_t)PB2_STATUS_NONFINITE);
     if (i == a.sys[s].off) fold_warns(a, s);
-    if (i == 0) *a.guard_end = 1;
   }
 }
 
 __global__ void finish_kernel(const IntArgs a) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_total; i += gridDim.x * blockDim.x) {
     const int s = a.atom_sys[i];
+    if (a.retired[s]) continue;
     const double h = a.sys[s].half_dt;
     const long long lfx = a.fx[i], lfy = a.fy[i], lfz = a.fz[i];
     check_fix(a, s, lfx); check_fix(a, s, lfy); check_fix(a, s, lfz);
@@ -318,11 +338,7 @@ __global__ void init_kernel(const IntArgs a) {
     }
     a.px[i] = p[0]; a.py[i] = p[1]; a.pz[i] = p[2];
     write_posq(a, i, S, a.x[i], a.y[i], a.z[i]);
-    if (loc == 0) {
-      uint32_t *kout = a.keys + ((size_t)(a.parity ^ 1) * a.n_sys + s) * 2;
-      kout[0] = knew[0];
-      kout[1] = knew[1];
-    }
+    if (loc == 0) store_key(a, s, knew);
   }
 }
 
@@ -399,6 +415,10 @@ cudaError_t launch_finish(const IntArgs &a, cudaStream_t st) {
     finish_guarded_kernel<<<grid_for(a.n_total), 256, 0, st>>>(a);
   else
     finish_kernel<<<grid_for(a.n_total), 256, 0, st>>>(a);
+  return cudaGetLastError();
+}
+cudaError_t launch_key_splits(const IntArgs &a, cudaStream_t st) {
+  key_splits_kernel<<<(a.n_sys + 255) / 256, 256, 0, st>>>(a);
   return cudaGetLastError();
 }
 cudaError_t launch_init(const IntArgs &a, cudaStream_t st) {

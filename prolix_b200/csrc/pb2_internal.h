@@ -90,6 +90,7 @@ struct pb2_batch {
   long long *traj_steps = nullptr;
   long long *born_acc = nullptr, *dedb_acc = nullptr, *energy = nullptr;
   uint32_t *keys = nullptr, *status = nullptr;
+  uint32_t *key_splits = nullptr;  // (2, n_sys, 4): split of each key buffer entry
   long long *steps = nullptr;
   // safeguards of the batched Langevin step (vlimit, max_dx, force_cap; <= 0
   // off), the closing-force flag and the per-system cap counters
@@ -100,8 +101,12 @@ struct pb2_batch {
   int32_t *warn_counts = nullptr;
   TileItem *items = nullptr;   // (i-block, j-range) items of the FP64 energy kernels
   int n_items = 0;
-  TileItem *items2 = nullptr;  // pair kernels: items over pairs of i-blocks
-  int n_items2 = 0;
+  TileItem *items2 = nullptr;  // pair kernels: the live items (those of systems not retired)
+  TileItem *items2_all = nullptr;  // every system's items over pairs of i-blocks
+  int n_items2 = 0;                // items in items2_all
+  int32_t *item_count = nullptr;   // items in items2 (device)
+  int8_t *retired = nullptr;       // per system: 1 = retired (pb2_retire_system)
+  std::vector<int8_t> retired_host;
   int32_t *sys_items = nullptr;  // items2 per system (the descreening pass's completion count)
   int32_t *sys_done = nullptr;   // items of each system completed in the current pass
   int2 *excl_ent = nullptr;

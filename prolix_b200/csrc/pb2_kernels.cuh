@@ -56,6 +56,7 @@ struct PairArgs {
   const SysInfo *sys;
   const TileItem *items;
   int32_t n_items;
+  const int32_t *item_count;  // non-NULL: the item count, in device memory (overrides n_items)
   uint32_t terms;
   const int2 *excl_ent;
   const ExclRow *excl_rows;
@@ -87,7 +88,7 @@ struct PairArgs {
   FinalizeArgs fin;
   const int32_t *pl_sys_items0, *pl_sys_items1;  // per-system item counts of the pair list's buffers
 };
-constexpr int kBondedChunk = 256;
+constexpr int kBondedChunk = 32;  // one term per lane: small systems get no long FP64 tail
 // Pair-list control words (PlArgs::ctl)
 enum { PL_DIRTY = 0, PL_CUR = 1, PL_COUNT0 = 2, PL_COUNT1 = 3, PL_NEW = 4, PL_DONE = 5, PL_WORDS = 8 };
 struct PlArgs {
@@ -104,6 +105,7 @@ struct PlArgs {
   int32_t *ctl;
   float reach2;          // (largest pair-term cutoff + skin)^2
   int32_t seg;           // tiles per work item
+  const int8_t *retired; // per system: 1 = retired (its rows list nothing)
 };
 
 struct Energy64Args {
@@ -153,6 +155,10 @@ struct IntArgs {
   const double *charge;
   float4 *posq;
   uint32_t *keys;
+  // (2, n_sys, 4): for the key in keys[parity][s], its split (next key,
+  // subkey), kept ahead by the thread of each system's first atom, so that
+  // a step's atoms read their subkey instead of each deriving it
+  uint32_t *splits;
   long long *steps;
   uint32_t *status;
   int32_t n_total;
@@ -176,6 +182,7 @@ struct IntArgs {
   int32_t n_blocks;
   const float4 *pl_ref;
   int32_t *pl_ctl;
+  const int8_t *retired;  // per system: 1 = retired, never stepped again
 };
 // warn_counts columns (prolix typing.py:559-563) and their warn_flags bits
 enum { kWarnVlimit = 0, kWarnForceCap = 1, kWarnConstr = 2, kWarnDxCap = 3, kWarnTypes = 4 };
@@ -237,8 +244,16 @@ cudaError_t launch_bbox(const SysInfo *sys, const int32_t *blk_sys, const float4
                         int32_t *pl_ctl = nullptr);
 // Rebuild the pair list when flagged (one launch; returns at once when clean).
 cudaError_t launch_pl_update(const PlArgs &a, int grid, cudaStream_t st);
+// The live work list: items of all[0, n_all) whose system is not retired,
+// in their order, into live and *count (one thread block).  With sys >= 0,
+// that system is retired first (and a pair list, if any, is marked for a
+// rebuild without it).
+cudaError_t launch_retire(int32_t sys, int8_t *retired, const TileItem *all, int n_all, TileItem *live,
+                          int32_t *count, int32_t *pl_ctl, cudaStream_t st);
 cudaError_t launch_bonded(const BondedArgs &a, int grid_cap, cudaStream_t st);
 cudaError_t launch_step(const IntArgs &a, cudaStream_t st);
+// Refresh splits[parity] from keys[parity] (after keys came from the host).
+cudaError_t launch_key_splits(const IntArgs &a, cudaStream_t st);
 cudaError_t launch_finish(const IntArgs &a, cudaStream_t st);
 cudaError_t launch_center(const IntArgs &a, cudaStream_t st);
 cudaError_t launch_noise_scale(const SysInfo *sys, const int32_t *atom_sys, const double *mass,

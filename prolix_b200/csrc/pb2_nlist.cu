@@ -12,11 +12,11 @@
 // are stored in a recursive-bisection order, so a block is a compact
 // cluster, and its bounding box is already computed for the pair kernels.
 // A cell grid is not built: the block boxes play its part, a box test
-// standing in for the cell stencil.  One warp per block (lane = the block's
-// atom, = one row): for every block of the system whose box comes within
-// cutoff + skin of its own, the warp stages that block's 32 positions in
-// shared memory and each lane tests them in index order, appending hits to
-// its row.  Rows are therefore in stored-atom order, the same every build.
+// standing in for the cell stencil.  One thread block per 32-atom block
+// (lane = the block's atom = one row): the blocks of the system whose boxes
+// come within cutoff + skin of its own are staged, 32 positions at a time,
+// in shared memory, and each lane tests them in index order.  Rows are
+// therefore in stored-atom order, the same every build.
 // A row longer than the capacity only counts (the largest count and an
 // overflow bit are recorded for the host's next visit).
 //
@@ -66,15 +66,44 @@ __global__ void nl_disp_kernel(const NlArgs a) {
   }
 }
 
-// 1. rows: one warp per block of atoms
+// 1. rows: one thread block (8 warps) per block of atoms.  The warps first
+// list, in order, the blocks within reach of it, then split that list into
+// 8 consecutive ranges: each warp counts its range's hits per atom, the
+// counts give every warp its offset in each row, and each warp writes its
+// hits there.  Rows come out in j order, whatever the split.
+constexpr int kMaxJList = 4096;  // j-blocks listed at once (longer systems: in windows)
+
+__device__ __forceinline__ int nl_test_block(const NlArgs &a, const SysInfo &S, float4 *jt, int jb,
+                                             int lane, int li, bool has_i, float4 p, int *row, int off,
+                                             bool write) {
+  const int lj0 = jb * 32;
+  const int nj = min(32, S.n - lj0);
+  __syncwarp();  // the previous block's positions have been read
+  if (lane < nj) jt[lane] = a.posq[S.off + lj0 + lane];
+  __syncwarp();
+  int c = 0;
+  if (has_i) {
+#pragma unroll 8
+    for (int t = 0; t < nj; ++t) {
+      const float4 q = jt[t];  // one address for the whole warp: a broadcast
+      const float ex = p.x - q.x, ey = p.y - q.y, ez = p.z - q.z;
+      const bool hit = fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < a.reach2 && lj0 + t != li;
+      if (write && hit && off + c < a.capacity) row[off + c] = lj0 + t;
+      c += hit ? 1 : 0;
+    }
+  }
+  return c;
+}
+
 __global__ void __launch_bounds__(32 * kRowsWarps) nl_rows_kernel(const NlArgs a) {
   if (!nl_dirty(a)) return;
   __shared__ float4 sp[kRowsWarps][32];
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  float4 *jt = sp[wib];
-  const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  const int nw = (int)((gridDim.x * blockDim.x) >> 5);
-  for (int ib = w; ib < a.n_blocks; ib += nw) {
+  __shared__ int jl[kMaxJList];
+  __shared__ int wc[kRowsWarps][32];
+  __shared__ int n_live;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  float4 *jt = sp[w];
+  for (int ib = blockIdx.x; ib < a.n_blocks; ib += gridDim.x) {
     const int s = a.blk_sys[ib];
     const SysInfo &S = a.sys[s];
     const int li = (ib - S.blk_base) * 32 + lane;  // the lane's atom, local index
@@ -82,30 +111,44 @@ __global__ void __launch_bounds__(32 * kRowsWarps) nl_rows_kernel(const NlArgs a
     const int i = S.off + (has_i ? li : 0);
     const float4 p = a.posq[i];
     int *row = a.rows + (size_t)i * a.capacity;
-    int count = 0;
-    for (int jb = 0; jb < S.nblk; ++jb) {
-      if (nl_box_dist2(a.bbox, ib, S.blk_base + jb) >= a.reach2) continue;  // warp-uniform
-      const int lj0 = jb * 32;
-      const int nj = min(32, S.n - lj0);
-      __syncwarp();  // the previous block's positions have been read
-      if (lane < nj) jt[lane] = a.posq[S.off + lj0 + lane];
-      __syncwarp();
-      if (has_i) {
-        for (int t = 0; t < nj; ++t) {
-          const float4 q = jt[t];  // one address for the whole warp: a broadcast
-          const float ex = p.x - q.x, ey = p.y - q.y, ez = p.z - q.z;
-          if (fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < a.reach2 && lj0 + t != li) {
-            if (count < a.capacity) row[count] = lj0 + t;
-            ++count;
-          }
+    int done = 0;  // this lane's row entries from earlier windows
+    for (int j0 = 0; j0 < S.nblk; j0 += kMaxJList) {
+      const int j1 = min(S.nblk, j0 + kMaxJList);
+      if (w == 0) {  // the window's blocks within reach, in order
+        int n = 0;
+        for (int jb0 = j0; jb0 < j1; jb0 += 32) {
+          const int jb = jb0 + lane;
+          const bool live = jb < j1 && nl_box_dist2(a.bbox, ib, S.blk_base + jb) < a.reach2;
+          const unsigned m = __ballot_sync(kFull, live);
+          if (live) jl[n + __popc(m & ((1u << lane) - 1u))] = jb;
+          n += __popc(m);
         }
+        if (lane == 0) n_live = n;
       }
+      __syncthreads();
+      const int L = n_live;
+      const int lo = (int)((long long)w * L / kRowsWarps), hi = (int)((long long)(w + 1) * L / kRowsWarps);
+      int c = 0;
+      for (int k = lo; k < hi; ++k) c += nl_test_block(a, S, jt, jl[k], lane, li, has_i, p, row, 0, false);
+      wc[w][lane] = c;
+      __syncthreads();
+      int off = done, tot = done;
+      for (int v = 0; v < kRowsWarps; ++v) {
+        if (v < w) off += wc[v][lane];
+        tot += wc[v][lane];
+      }
+      for (int k = lo; k < hi; ++k) off += nl_test_block(a, S, jt, jl[k], lane, li, has_i, p, row, off, true);
+      done = tot;
+      __syncthreads();  // jl, wc and n_live are reused by the next window / block
     }
     if (has_i) {
-      for (int t = count; t < a.capacity; ++t) row[t] = S.n;  // sentinel
-      a.counts[i] = count;
-      if (count > a.capacity) atomicOr(&a.status[s], (uint32_t)PB2_STATUS_NLOVERFLOW);
-      atomicMax(&a.ctl[NL_MAXCOUNT], count);
+      // sentinels, the 8 warps sharing each row
+      for (int t = done + w; t < a.capacity; t += kRowsWarps) row[t] = S.n;
+      if (w == 0) {
+        a.counts[i] = done;
+        if (done > a.capacity) atomicOr(&a.status[s], (uint32_t)PB2_STATUS_NLOVERFLOW);
+        atomicMax(&a.ctl[NL_MAXCOUNT], done);
+      }
     }
   }
 }
@@ -132,7 +175,7 @@ __global__ void nl_ref_kernel(const NlArgs a) {
 static int grid_for(int n, int per) { return std::max(1, std::min((n + per - 1) / per, 65535)); }
 
 cudaError_t nl_launch_build(const NlArgs &a, cudaStream_t st) {
-  nl_rows_kernel<<<grid_for(a.n_blocks, kRowsWarps), 32 * kRowsWarps, 0, st>>>(a);
+  nl_rows_kernel<<<grid_for(a.n_blocks, 1), 32 * kRowsWarps, 0, st>>>(a);
   nl_ref_kernel<<<grid_for(a.n_total, 256), 256, 0, st>>>(a);
   return cudaGetLastError();
 }

@@ -73,6 +73,7 @@ __device__ __forceinline__ float box_dist2(const float4 *bbox, int a, int b) {
 
 struct PData {  // per-atom data a lane holds (its i atom, or the j atom passing through)
   float x, y, z, q, hs, se, ro, sr, B, iB, dedi;  // iB = sqrt(log2 e / 4) / B
+  float rB;  // 1 / B
   float t2;  // (max(s / sqrt(kSeriesUNear), s + rho~_max))^2: series reach of this atom
   float s2, s3;  // s^2, s^3 of the scaled radius (far-field series)
 };
@@ -94,11 +95,12 @@ struct TileConst {
 // float4 fields per atom, each holding two values as (v, v) pairs, so that
 // a step reads a packed operand straight into a register pair.  Field-major
 // (field, atom), so that the 32 lanes' 16-byte reads of one field are
-// conflict-free.  Force pass: (-x, -x, -y, -y), (-z, -z, q, q),
+// conflict-free.  Every atom is stored twice (entries a and a + 32): lane l
+// reads entry l + k at step k, with no wrap-around arithmetic.  Force pass: (-x, -x, -y, -y), (-z, -z, q, q),
 // (hs, hs, se, se), (B, B, iB, iB).  Descreening: (-x, -x, -y, -y),
 // (-z, -z, s2, s2), (s3, s3, t2, t2).  Chain rule: the same with
 // (s3, s3, dedi, dedi) and (t2, t2, 0, 0).
-typedef float4 JTile[4][32];
+typedef float4 JTile[4][64];
 
 // What a lane reads of its j atom at a step.
 struct JF2 {  // force pass
@@ -137,19 +139,29 @@ __device__ __forceinline__ JD2 load_jd(const JTile &t, int e) {
 // reads; the caller synchronises the warp before and after).
 template <int PASS>
 __device__ __forceinline__ void store_j(JTile &t, int lane, const PData &J) {
-  t[0][lane] = make_float4(-J.x, -J.x, -J.y, -J.y);
+  float4 f[4];
+  int nf = 3;
+  f[0] = make_float4(-J.x, -J.x, -J.y, -J.y);
   if (PASS == PASS_FORCE) {
-    t[1][lane] = make_float4(-J.z, -J.z, J.q, J.q);
-    t[2][lane] = make_float4(J.hs, J.hs, J.se, J.se);
-    t[3][lane] = make_float4(J.B, J.B, J.iB, J.iB);
+    f[1] = make_float4(-J.z, -J.z, J.q, J.q);
+    f[2] = make_float4(J.hs, J.hs, J.se, J.se);
+    f[3] = make_float4(J.B, J.B, J.iB, J.iB);
+    nf = 4;
   } else if (PASS == PASS_BORN) {
-    t[1][lane] = make_float4(-J.z, -J.z, J.s2, J.s2);
-    t[2][lane] = make_float4(J.s3, J.s3, J.t2, J.t2);
+    f[1] = make_float4(-J.z, -J.z, J.s2, J.s2);
+    f[2] = make_float4(J.s3, J.s3, J.t2, J.t2);
   } else {
-    t[1][lane] = make_float4(-J.z, -J.z, J.s2, J.s2);
-    t[2][lane] = make_float4(J.s3, J.s3, J.dedi, J.dedi);
-    t[3][lane] = make_float4(J.t2, J.t2, 0.f, 0.f);
+    f[1] = make_float4(-J.z, -J.z, J.s2, J.s2);
+    f[2] = make_float4(J.s3, J.s3, J.dedi, J.dedi);
+    f[3] = make_float4(J.t2, J.t2, 0.f, 0.f);
+    nf = 4;
   }
+#pragma unroll
+  for (int c = 0; c < 4; ++c)
+    if (c < nf) {
+      t[c][lane] = f[c];
+      t[c][lane + 32] = f[c];
+    }
 }
 
 // Force-pass rotation of the j-side sums but tj.a0.
@@ -167,10 +179,10 @@ __device__ __forceinline__ void load_pdata(const PairArgs &a, int g, int pass, b
   P.t2 = t * t;
   P.s2 = P.sr * P.sr;
   P.s3 = P.s2 * P.sr;
-  P.B = P.iB = P.dedi = 0.f;
+  P.B = P.iB = P.dedi = P.rB = 0.f;
   if ((pass == PASS_FORCE && use_gb) || pass == PASS_CHAIN) {
     const float4 b = a.born[g];
-    P.B = b.x; P.iB = b.y * kSqrtQuarterLog2e;
+    P.B = b.x; P.iB = b.y * kSqrtQuarterLog2e; P.rB = b.y;
     if (pass == PASS_CHAIN) P.dedi = (float)((double)a.dedb_acc[g] * kForceInv) * b.z;
   }
 }
@@ -208,7 +220,7 @@ __device__ __forceinline__ void run_force_tile2(const FData2 &I, const JTile &jt
   uint32_t X0 = __brev(E0), X1 = __brev(E1), Q0 = __brev(S0), Q1 = __brev(S1);
 #pragma unroll kUnroll
   for (int k = 0; k < 32; ++k) {
-    const JF2 J = load_jf(jt, (K.lane + k) & 31);  // lane l meets j-lane (l + k) mod 32
+    const JF2 J = load_jf(jt, K.lane + k);  // lane l meets j-lane (l + k) mod 32
     const float2 dx = __fadd2_rn(I.x, J.mx);
     const float2 dy = __fadd2_rn(I.y, J.my);
     const float2 dz = __fadd2_rn(I.z, J.mz);
@@ -221,19 +233,22 @@ __device__ __forceinline__ void run_force_tile2(const FData2 &I, const JTile &jt
     float2 g = make_float2(0.f, 0.f);
     if (K.use_gb) {
       // E = P qq / f, f^2 = r^2 + B_i B_j e^(-r^2 / 4 B_i B_j); with
-      // A2 = 2 P qq / f^3:  -dE/dr / r = A2 (1 - e / 4),
-      // dE/dB_i B_i = A2 e (-1/2 - w / (2 log2 e)) B_j,  w = r^2 log2(e) / (4 B_i B_j)
-      const float2 w = __fmul2_rn(r2, __fmul2_rn(I.iB, J.iB));
+      // A2 = 2 P qq / f^3:  -dE/dr / r = A2 (1 - e / 4), and
+      // dE/dB_i = -(A2 e / 2) (B_i B_j + r^2 / 4) / B_i, whose numerator is
+      // the same for both atoms: h = A2 e (B_i B_j + r^2 / 4) is summed for
+      // both, and each sum is scaled by -1 / (2 B) when it is flushed
+      const float2 w = __fmul2_rn(r2, __fmul2_rn(I.iB, J.iB));  // r^2 log2(e) / (4 B_i B_j)
       const float2 ex = make_float2(exp2f(-w.x), exp2f(-w.y));
-      const float2 f2 = __ffma2_rn(__fmul2_rn(I.B, J.B), ex, r2);
+      const float2 bb = __fmul2_rn(I.B, J.B);
+      const float2 f2 = __ffma2_rn(bb, ex, r2);
       const float2 inv_f = make_float2(rsqrtf(f2.x), rsqrtf(f2.y));
       float2 A2 = __fmul2_rn(__fmul2_rn(I.q2p, J.q), __fmul2_rn(__fmul2_rn(inv_f, inv_f), inv_f));
       if (CUT && K.gcut2 != 0.f) A2 = __fmul2_rn(A2, sel2(r2.x < K.gcut2, r2.y < K.gcut2, 1.f, 0.f));
       const float2 A2e = __fmul2_rn(A2, ex);
       g = __ffma2_rn(dup2(-0.25f), A2e, A2);
-      const float2 c = __fmul2_rn(A2e, __ffma2_rn(w, dup2(-kInvQuarterLog2e * 0.125f), dup2(-0.5f)));
-      ti.a3 = __ffma2_rn(c, J.B, ti.a3);  // dE/dB_i B_i = c B_j
-      tj.a3 = fmaf(c.x, I.B.x, fmaf(c.y, I.B.y, tj.a3));
+      const float2 h = __fmul2_rn(A2e, __ffma2_rn(r2, dup2(0.25f), bb));
+      ti.a3 = __fadd2_rn(ti.a3, h);
+      tj.a3 = tj.a3 + h.x + h.y;
     }
     if (K.use_lj || K.use_coul) {
       const float2 inv_r = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
@@ -440,7 +455,7 @@ __device__ __forceinline__ void run_bc_tile2(const PData2 &I, const JTile &jt, A
   uint32_t R0 = __brev(V0), R1 = __brev(V1);
 #pragma unroll kUnrollBC
   for (int k = 0; k < 32; ++k) {
-    const JD2 J = load_jd<PASS, FAR>(jt, (K.lane + k) & 31);  // lane l meets j-lane (l + k) mod 32
+    const JD2 J = load_jd<PASS, FAR>(jt, K.lane + k);  // lane l meets j-lane (l + k) mod 32
     BCPair2 P;
     bc_series2<PASS, CUT, FULL, TIER>(I, J, FULL || (int32_t)R0 < 0, FULL || (int32_t)R1 < 0, P, K);
     if (!FULL) {
@@ -554,7 +569,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
   // closed-form queues of the descreening and chain passes, one per warp
   constexpr int kWarps = THREADS / 32;
   __shared__ int2 s_cfq[PASS == PASS_FORCE ? 1 : kWarps][PASS == PASS_FORCE ? 1 : kCfCap];
-  // the j-block of the current tile, one JTile per warp (2 KB)
+  // the j-block of the current tile, one JTile per warp (4 KB)
   __shared__ JTile s_jt[kWarps];
   JTile &jt = s_jt[threadIdx.x >> 5];
   CfQueue Q;
@@ -569,7 +584,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
   // from the list; otherwise items are contiguous j-block ranges
   const bool plm = CUT && a.pl_ctl != nullptr;
   const TileItem *items = a.items;
-  int n_items = a.n_items;
+  int n_items = a.item_count ? *a.item_count : a.n_items;
   const int32_t *sys_items = a.sys_items;
   if (plm) {
     const int cur = a.pl_ctl[PL_CUR];
@@ -714,7 +729,8 @@ __global__ void __launch_bounds__(THREADS, MINB)
           atomic_add_fix(&a.fx[jg], to_fix_f(tj.a0, bscale));
           atomic_add_fix(&a.fy[jg], to_fix_f(tj.a1, bscale));
           atomic_add_fix(&a.fz[jg], to_fix_f(tj.a2, bscale));
-          if (PASS == PASS_FORCE && K.use_gb) atomic_add_fix(&a.dedb_acc[jg], to_fix_f(tj.a3, bscale));
+          if (PASS == PASS_FORCE && K.use_gb)
+            atomic_add_fix(&a.dedb_acc[jg], to_fix_f(tj.a3 * (-0.5f * J.rB), bscale));
         }
       }
       p0 += to_fix_f(t0.a0, bscale);
@@ -724,8 +740,8 @@ __global__ void __launch_bounds__(THREADS, MINB)
         q1 += to_fix_f(t1.a1, bscale); q2 += to_fix_f(t1.a2, bscale);
       }
       if (PASS == PASS_FORCE) {
-        p3 += to_fix_f(t0.a3, bscale);
-        q3 += to_fix_f(t1.a3, bscale);
+        p3 += to_fix_f(t0.a3 * (-0.5f * I0.rB), bscale);
+        q3 += to_fix_f(t1.a3 * (-0.5f * I1.rB), bscale);
       }
     }
 

@@ -46,6 +46,7 @@ __global__ void pl_update_kernel(const PlArgs a) {
   TileItem *out = nxt ? a.items1 : a.items0;
   for (int r = w; r < a.n_rows; r += nw) {
     const PlRow row = a.rows[r];
+    if (a.retired[row.sys]) continue;  // a retired system lists no work
     const SysInfo &S = a.sys[row.sys];
     const int ib = row.iblk;
     const bool has1 = ib + 1 < S.nblk;
@@ -104,6 +105,51 @@ __global__ void pl_update_kernel(const PlArgs a) {
 cudaError_t launch_pl_update(const PlArgs &a, int grid, cudaStream_t st) {
   if (a.n_rows <= 0) return cudaSuccess;
   pl_update_kernel<<<grid, 256, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+// Retire a system and re-list the live work items: an ordered compaction
+// of the full list by one thread block (the list is a few thousand items
+// per thousand atoms; one block keeps the order without a second pass).
+constexpr int kRetireThreads = 1024;
+__global__ void __launch_bounds__(kRetireThreads) retire_kernel(int32_t sys, int8_t *retired, const TileItem *all,
+                                                                 int n_all, TileItem *live, int32_t *count,
+                                                                 int32_t *pl_ctl) {
+  __shared__ int warp_sum[kRetireThreads / 32];
+  __shared__ int base;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (threadIdx.x == 0) {
+    if (sys >= 0) {
+      retired[sys] = 1;
+      if (pl_ctl) pl_ctl[PL_DIRTY] = 1;
+    }
+    base = 0;
+  }
+  __syncthreads();
+  for (int k0 = 0; k0 < n_all; k0 += kRetireThreads) {
+    const int k = k0 + threadIdx.x;
+    TileItem t{};
+    bool keep = false;
+    if (k < n_all) {
+      t = all[k];
+      keep = retired[t.sys] == 0;
+    }
+    const unsigned m = __ballot_sync(kFull, keep);
+    if (lane == 0) warp_sum[w] = __popc(m);
+    __syncthreads();
+    int before = base;
+    for (int v = 0; v < w; ++v) before += warp_sum[v];
+    if (keep) live[before + __popc(m & ((1u << lane) - 1u))] = t;
+    __syncthreads();
+    if (threadIdx.x == kRetireThreads - 1) base = before + __popc(m);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *count = base;
+}
+
+cudaError_t launch_retire(int32_t sys, int8_t *retired, const TileItem *all, int n_all, TileItem *live,
+                          int32_t *count, int32_t *pl_ctl, cudaStream_t st) {
+  retire_kernel<<<1, kRetireThreads, 0, st>>>(sys, retired, all, n_all, live, count, pl_ctl);
   return cudaGetLastError();
 }
 

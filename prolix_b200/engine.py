@@ -517,6 +517,11 @@ class Batch:
     self._check(self.lib.pb2_get_tile_segment(self.handle, ctypes.byref(v)))
     return int(v.value)
 
+  def retire(self, system: int, stream=None):
+    """Stop stepping and evaluating one system (stream-ordered, irreversible):
+    its state stays as the last step left it and it costs no more work."""
+    self._check(self.lib.pb2_retire_system(self.handle, int(system), stream))
+
   def set_profiling(self, enable: bool):
     self._check(self.lib.pb2_set_profiling(self.handle, 1 if enable else 0))
 

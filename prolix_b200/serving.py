@@ -8,9 +8,10 @@ device.  Running cohorts are never rebuilt and their state never leaves the
 device: each tick advances every cohort by the same number of steps on its
 own CUDA stream, so all cohorts' kernels overlap on the GPU, and only a
 cohort in which a request has just finished is read back (the finished
-systems' positions, momenta and keys are the result).  A cohort whose
-requests have all ended is released; one with some ended systems keeps
-stepping them unread until its last request ends.
+systems' positions, momenta and keys are the result).  A system whose
+request has ended is retired inside its cohort (stream-ordered; the pair
+kernels' work list is compacted on the device), so it costs no more steps;
+a cohort whose requests have all ended is released.
 
 The step count of a tick is the largest of chunk, chunk/2, chunk/5,
 chunk/10, 1 (and 1-step divisions thereof) that does not pass the nearest
@@ -88,6 +89,12 @@ class _Cohort:
 
   def live(self) -> bool:
     return any(s is not None for s in self.slots)
+
+  def end(self, b: int):
+    """Request b's slot is over: retire its system (no further work)."""
+    self.slots[b] = None
+    if any(s is not None for s in self.slots):  # else the whole cohort is released
+      self.batch.retire(b, self.stream.cuda_stream if self.stream is not None else None)
 
   def atoms(self) -> int:
     return int(np.sum(self.batch.sizes))
@@ -219,6 +226,9 @@ class Server:
       else:
         slots.append(_Slot(r, 0, now))
     cohort = _Cohort(batch, slots, self._streams() if self._streams else None)
+    for b, s in enumerate(slots):
+      if s is None and cohort.live():
+        batch.retire(b, cohort.stream.cuda_stream if cohort.stream is not None else None)
     if cohort.live():
       self.cohorts.append(cohort)
     else:
@@ -243,7 +253,7 @@ class Server:
           if s is not None and s.req.rid in self.cancelled:
             if s.req.rid not in self.results:
               self._fail(s.req, s.admitted, now, "cancelled")
-            c.slots[b] = None
+            c.end(b)
     if admitted:
       self._new_cohort(admitted, now)
     self._retire()
@@ -267,7 +277,7 @@ class Server:
         self.atom_steps += n * len(s.req.system["charges"])
         if status[b] & (STATUS_NONFINITE | STATUS_FORCE_RANGE):
           self._fail(s.req, s.admitted, now, "non-finite state: evicted")
-          c.slots[b] = None
+          c.end(b)
         elif s.done >= s.req.n_steps:
           if st is None:  # a finished request: the cohort's state comes back once
             st = c.batch.get_state(fields=_FIELDS)
@@ -280,7 +290,7 @@ class Server:
             self.results[s.req.rid] = Result(s.req.rid, x, st["momentum"][lo:hi].copy(),
                                              st["key"][b].copy(), s.done, s.req.arrival,
                                              s.admitted, now)
-          c.slots[b] = None
+          c.end(b)
     self._retire()
     return True
 

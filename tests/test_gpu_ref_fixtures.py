@@ -92,6 +92,12 @@ def test_real_protein_born_radii_gb_and_ace_match_the_reference():
     terms = fn.terms(pos)
     assert terms["gb"] == pytest.approx(float(FIX[f"{c}/gb"]), rel=E_REL)
     assert terms["nonpolar"] == pytest.approx(float(FIX[f"{c}/nonpolar"]), rel=E_REL)
-    np.testing.assert_allclose(fn.born_radii(pos), FIX[f"{c}/born_radii"], rtol=B_REL)
+    # deeply buried atoms (B up to ~14 A against rho~ ~1.7 A) amplify the
+    # float32 descreening sum's rounding in 1/B = 1/rho~ - tanh(...)/rho by
+    # about B / rho~, so the protein's largest radii get a wider bound; the
+    # energies above hold the standard one
+    got = fn.born_radii(pos)
+    ref = FIX[f"{c}/born_radii"]
+    np.testing.assert_allclose(got, ref, rtol=B_REL * np.maximum(1.0, ref / 4.0))
   finally:
     fn.close()

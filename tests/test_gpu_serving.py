@@ -63,3 +63,32 @@ def test_budget_admission_and_cancellation():
   for req in reqs:
     if req.rid != 2:
       np.testing.assert_array_equal(res[req.rid].position, _alone(req).position)
+
+
+@pytest.mark.parametrize("cutoff", [0.0, 12.0])
+def test_retired_system_stops_and_the_rest_run_as_without_it(cutoff):
+  # retire system 1 after 20 steps: it keeps its 20-step state through 30
+  # more steps of the batch, and systems 0 and 2 end bit-identical to a
+  # batch that never held it (the pair work list is compacted on the
+  # device; at the cutoff, the pair list is rebuilt without it)
+  from prolix_b200 import engine
+  systems = [dict(synth.make_chain(n, 40 + n, compact=True), key=(0, 7 + n)) for n in (150, 400, 90)]
+
+  def run(idx, plan):
+    with engine.Batch([systems[i] for i in idx], cutoff=cutoff) as b:
+      b.langevin_init()
+      for n, retire in plan:
+        b.langevin_run(n)
+        for s in retire:
+          b.retire(s)
+      st = b.get_state(fields=("position", "momentum", "key"))
+      return {f: [st[f][b.offsets[k]:b.offsets[k + 1]] if f != "key" else st[f][k]
+                  for k in range(len(idx))] for f in st}
+
+  mixed = run([0, 1, 2], [(20, [1]), (30, [])])
+  alone02 = run([0, 2], [(50, [])])
+  alone1 = run([1], [(20, [])])
+  for f in ("position", "momentum", "key"):
+    np.testing.assert_array_equal(mixed[f][0], alone02[f][0])
+    np.testing.assert_array_equal(mixed[f][2], alone02[f][1])
+    np.testing.assert_array_equal(mixed[f][1], alone1[f][0])

@@ -16,6 +16,7 @@ class FakeBatch:
     self.p = np.zeros_like(self.x)
     self.k = np.array([s["key"] for s in systems], dtype=np.uint32).reshape(-1, 2)
     self.n_systems = len(systems)
+    self.retired = []
 
   def __enter__(self):
     return self
@@ -30,8 +31,15 @@ class FakeBatch:
     pass
 
   def langevin_run(self, n, stream=None):
-    self.x = self.x + 0.001 * n
-    self.p = self.p + n
+    live = np.ones(len(self.x), bool)
+    for s in self.retired:  # retired systems are not stepped
+      live[self.offsets[s]:self.offsets[s + 1]] = False
+    self.x = np.where(live[:, None], self.x + 0.001 * n, self.x)
+    self.p = np.where(live[:, None], self.p + n, self.p)
+
+  def retire(self, system, stream=None):
+    assert system not in self.retired
+    self.retired.append(system)
 
   def get_state(self, fields=("position", "momentum", "key")):
     st = {"position": self.x.copy(), "momentum": self.p.copy(), "key": self.k.copy(),
@@ -149,3 +157,25 @@ def test_tick_lengths_come_from_a_small_set():
     assert 1 <= n <= min(50, limit)
     seen.add(n)
   assert seen <= {50, 25, 10, 5, 1}
+
+
+def test_ended_systems_are_retired_in_their_cohort():
+  # a finished request's system stops costing work at once: the cohort
+  # retires it, and the cohort's other systems carry on unaffected
+  clk = Clock()
+  made = []
+
+  def factory(systems, **kw):
+    made.append(FakeBatch(systems, **kw))
+    return made[-1]
+
+  srv = serving.Server(chunk=10, clock=clk, batch_factory=factory)
+  reqs = [_req(0, 10, 10, 0.0), _req(1, 10, 30, 0.0), _req(2, 10, 20, 0.0)]
+  res = srv.run(reqs, sleep=clk.sleep)
+  assert len(made) == 1
+  assert made[0].retired == [0, 2]  # the last one ends with its cohort
+  for r in reqs:
+    assert res[r.rid].steps == r.n_steps
+    np.testing.assert_allclose(res[r.rid].momentum, r.n_steps)
+  np.testing.assert_allclose(made[0].p[:10], 10)   # not stepped after retirement
+  np.testing.assert_allclose(made[0].p[20:], 20)
