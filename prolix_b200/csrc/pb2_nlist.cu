@@ -13,10 +13,10 @@
 // cluster, and its bounding box is already computed for the pair kernels.
 // A cell grid is not built: the block boxes play its part, a box test
 // standing in for the cell stencil.  One thread block per 32-atom block
-// (lane = the block's atom = one row): the blocks of the system whose boxes
-// come within cutoff + skin of its own are staged, 32 positions at a time,
-// in shared memory, and each lane tests them in index order.  Rows are
-// therefore in stored-atom order, the same every build.
+// (its 32 rows): the blocks of the system whose boxes come within
+// cutoff + skin of its own are listed, and their atoms are tested 32 at a
+// time (lane = candidate), in index order.  Rows are therefore in
+// stored-atom order, the same every build.
 // A row longer than the capacity only counts (the largest count and an
 // overflow bit are recorded for the host's next visit).
 //
@@ -40,7 +40,7 @@
 
 namespace pb2 {
 
-constexpr int kRowsWarps = 8;  // warps (blocks of atoms) per thread block of the row pass
+constexpr int kRowsWarps = 8;  // warps per thread block of the row pass (4 rows each)
 
 __device__ __forceinline__ bool nl_dirty(const NlArgs &a) { return *(volatile int32_t *)&a.ctl[NL_DIRTY] != 0; }
 
@@ -66,88 +66,75 @@ __global__ void nl_disp_kernel(const NlArgs a) {
   }
 }
 
-// 1. rows: one thread block (8 warps) per block of atoms.  The warps first
-// list, in order, the blocks within reach of it, then split that list into
-// 8 consecutive ranges: each warp counts its range's hits per atom, the
-// counts give every warp its offset in each row, and each warp writes its
-// hits there.  Rows come out in j order, whatever the split.
+// 1. rows: one thread block (8 warps) per block of atoms; warp w owns the
+// block's rows 4w .. 4w + 3.  Warp 0 lists, in order, the blocks within
+// reach of this one; then each warp walks that list one j-block at a time,
+// lane = candidate atom: one position load serves the warp's four rows,
+// and each row's hits are compacted by a ballot and stored as one
+// contiguous run (coalesced), so rows come out in j order.
 constexpr int kMaxJList = 4096;  // j-blocks listed at once (longer systems: in windows)
-
-__device__ __forceinline__ int nl_test_block(const NlArgs &a, const SysInfo &S, float4 *jt, int jb,
-                                             int lane, int li, bool has_i, float4 p, int *row, int off,
-                                             bool write) {
-  const int lj0 = jb * 32;
-  const int nj = min(32, S.n - lj0);
-  __syncwarp();  // the previous block's positions have been read
-  if (lane < nj) jt[lane] = a.posq[S.off + lj0 + lane];
-  __syncwarp();
-  int c = 0;
-  if (has_i) {
-#pragma unroll 8
-    for (int t = 0; t < nj; ++t) {
-      const float4 q = jt[t];  // one address for the whole warp: a broadcast
-      const float ex = p.x - q.x, ey = p.y - q.y, ez = p.z - q.z;
-      const bool hit = fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < a.reach2 && lj0 + t != li;
-      if (write && hit && off + c < a.capacity) row[off + c] = lj0 + t;
-      c += hit ? 1 : 0;
-    }
-  }
-  return c;
-}
+constexpr int kRowsPerWarp = 32 / kRowsWarps;
 
 __global__ void __launch_bounds__(32 * kRowsWarps) nl_rows_kernel(const NlArgs a) {
   if (!nl_dirty(a)) return;
-  __shared__ float4 sp[kRowsWarps][32];
   __shared__ int jl[kMaxJList];
-  __shared__ int wc[kRowsWarps][32];
   __shared__ int n_live;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  float4 *jt = sp[w];
+  const unsigned below = (1u << lane) - 1u;
   for (int ib = blockIdx.x; ib < a.n_blocks; ib += gridDim.x) {
     const int s = a.blk_sys[ib];
     const SysInfo &S = a.sys[s];
-    const int li = (ib - S.blk_base) * 32 + lane;  // the lane's atom, local index
-    const bool has_i = li < S.n;
-    const int i = S.off + (has_i ? li : 0);
-    const float4 p = a.posq[i];
-    int *row = a.rows + (size_t)i * a.capacity;
-    int done = 0;  // this lane's row entries from earlier windows
+    const int l0 = (ib - S.blk_base) * 32 + w * kRowsPerWarp;  // the warp's first row, local index
+    float4 p[kRowsPerWarp];
+    int cnt[kRowsPerWarp];
+#pragma unroll
+    for (int r = 0; r < kRowsPerWarp; ++r) {
+      p[r] = a.posq[S.off + min(l0 + r, S.n - 1)];
+      cnt[r] = 0;
+    }
     for (int j0 = 0; j0 < S.nblk; j0 += kMaxJList) {
       const int j1 = min(S.nblk, j0 + kMaxJList);
-      if (w == 0) {  // the window's blocks within reach, in order
+      __syncthreads();  // the previous window's list is no longer read
+      if (w == 0) {
         int n = 0;
         for (int jb0 = j0; jb0 < j1; jb0 += 32) {
           const int jb = jb0 + lane;
           const bool live = jb < j1 && nl_box_dist2(a.bbox, ib, S.blk_base + jb) < a.reach2;
           const unsigned m = __ballot_sync(kFull, live);
-          if (live) jl[n + __popc(m & ((1u << lane) - 1u))] = jb;
+          if (live) jl[n + __popc(m & below)] = jb;
           n += __popc(m);
         }
         if (lane == 0) n_live = n;
       }
       __syncthreads();
+      if (l0 >= S.n) continue;  // a warp past the system's last atom has no rows
       const int L = n_live;
-      const int lo = (int)((long long)w * L / kRowsWarps), hi = (int)((long long)(w + 1) * L / kRowsWarps);
-      int c = 0;
-      for (int k = lo; k < hi; ++k) c += nl_test_block(a, S, jt, jl[k], lane, li, has_i, p, row, 0, false);
-      wc[w][lane] = c;
-      __syncthreads();
-      int off = done, tot = done;
-      for (int v = 0; v < kRowsWarps; ++v) {
-        if (v < w) off += wc[v][lane];
-        tot += wc[v][lane];
+      for (int k = 0; k < L; ++k) {
+        const int lj = jl[k] * 32 + lane;
+        const bool vj = lj < S.n;
+        const float4 q = a.posq[S.off + (vj ? lj : 0)];
+#pragma unroll
+        for (int r = 0; r < kRowsPerWarp; ++r) {
+          const float ex = p[r].x - q.x, ey = p[r].y - q.y, ez = p[r].z - q.z;
+          const bool hit = vj && l0 + r < S.n && lj != l0 + r && fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < a.reach2;
+          const unsigned m = __ballot_sync(kFull, hit);
+          const int t = cnt[r] + __popc(m & below);
+          if (hit && t < a.capacity) a.rows[(size_t)(S.off + l0 + r) * a.capacity + t] = lj;
+          cnt[r] += __popc(m);
+        }
       }
-      for (int k = lo; k < hi; ++k) off += nl_test_block(a, S, jt, jl[k], lane, li, has_i, p, row, off, true);
-      done = tot;
-      __syncthreads();  // jl, wc and n_live are reused by the next window / block
     }
-    if (has_i) {
-      // sentinels, the 8 warps sharing each row
-      for (int t = done + w; t < a.capacity; t += kRowsWarps) row[t] = S.n;
-      if (w == 0) {
-        a.counts[i] = done;
-        if (done > a.capacity) atomicOr(&a.status[s], (uint32_t)PB2_STATUS_NLOVERFLOW);
-        atomicMax(&a.ctl[NL_MAXCOUNT], done);
+#pragma unroll
+    for (int r = 0; r < kRowsPerWarp; ++r) {
+      const int li = l0 + r;
+      if (li >= S.n) break;
+      const int i = S.off + li;
+      int *row = a.rows + (size_t)i * a.capacity;
+      for (int t = cnt[r] + lane; t < a.capacity; t += 32) row[t] = S.n;  // sentinels
+      if (lane == 0) {
+        a.counts[i] = cnt[r];
+        if (cnt[r] > a.capacity) atomicOr(&a.status[s], (uint32_t)PB2_STATUS_NLOVERFLOW);
+        atomicMax(&a.ctl[NL_MAXCOUNT], cnt[r]);
       }
     }
   }

@@ -7,7 +7,8 @@ system dict with the reference's own padded exclusion table
 (``excl_indices`` / ``excl_scales_vdw`` / ``excl_scales_elec`` from
 ``map_exclusions_to_dense_padded``), or, for the explicit 1-4 case, an
 ExclusionSpec object.  Tolerances: per-term energy relative 1e-6 (+1e-6
-kcal/mol), force relative RMS 1e-5, Born radii relative 2e-6.
+kcal/mol), force relative RMS 1e-5, Born radii relative 2e-6 (the real
+protein: scaled by each radius' sensitivity to the descreening sum).
 """
 
 import os
@@ -92,12 +93,33 @@ def test_real_protein_born_radii_gb_and_ace_match_the_reference():
     terms = fn.terms(pos)
     assert terms["gb"] == pytest.approx(float(FIX[f"{c}/gb"]), rel=E_REL)
     assert terms["nonpolar"] == pytest.approx(float(FIX[f"{c}/nonpolar"]), rel=E_REL)
-    # deeply buried atoms (B up to ~14 A against rho~ ~1.7 A) amplify the
-    # float32 descreening sum's rounding in 1/B = 1/rho~ - tanh(...)/rho by
-    # about B / rho~, so the protein's largest radii get a wider bound; the
-    # energies above hold the standard one
+    # the float32 descreening sums hold psi = rho~ sum_j I_ij to 1.5e-6
+    # relative (2,144 atoms, each summing ~2,000 series terms); B = 1 / (1/rho~ - tanh(a(psi)) / rho) turns that into
+    # |dB/B| = amp |dpsi/psi| with amp = B (1 - th^2) psi a'(psi) / rho, which
+    # reaches ~4.9 on the protein's buried atoms (B up to 49 A) against ~2 on
+    # the synthetic chains, so each radius is held to 1.5e-6 max(2, amp); the
+    # energies above keep the standard bound
     got = fn.born_radii(pos)
     ref = FIX[f"{c}/born_radii"]
-    np.testing.assert_allclose(got, ref, rtol=B_REL * np.maximum(1.0, ref / 4.0))
+    bound = 1.5e-6 * np.maximum(2.0, _psi_amplification(ref, rad))
+    err = np.abs(got - ref) / np.abs(ref)
+    k = int(np.argmax(err / bound))
+    assert np.all(err <= bound), (k, err[k], bound[k], ref[k])
   finally:
     fn.close()
+
+
+def _psi_amplification(born, radius):
+  """amp_i = B (1 - th^2) psi a'(psi) / rho for the OBC2 rescale
+  a(psi) = psi - 0.8 psi^2 + 4.85 psi^3 (generalized_born.py:18-21, :84-94),
+  with th and psi recovered from the radius B itself."""
+  ro = radius - 0.09
+  th = radius * (1.0 / ro - 1.0 / born)
+  target = np.arctanh(th)
+  psi = target.copy()
+  for _ in range(50):  # a is increasing (a' > 0 everywhere): Newton converges
+    a = psi - 0.8 * psi**2 + 4.85 * psi**3
+    da = 1.0 - 1.6 * psi + 14.55 * psi**2
+    psi = psi - (a - target) / da
+  da = 1.0 - 1.6 * psi + 14.55 * psi**2
+  return born * (1.0 - th**2) * psi * da / radius
