@@ -75,6 +75,10 @@ extern "C" {
 #define PB2_STATUS_NONFINITE 0x1u
 #define PB2_STATUS_NLOVERFLOW 0x2u
 #define PB2_STATUS_FORCE_RANGE 0x4u /* |F| beyond the fixed-point range */
+/* a bounded device-side wait gave up; that evaluation's results for the
+ * system are invalid (never expected: the waits are for work already in
+ * flight on the same launch) */
+#define PB2_STATUS_WAIT_TIMEOUT 0x8u
 
 /* One system, host arrays.  Atom indices are local to the system. */
 typedef struct pb2_system_desc {
@@ -447,13 +451,14 @@ int pb2_get_block_shape(const pb2_batch *batch, int32_t pass, int32_t *threads, 
 
 /* Which per-step work rides inside the pair passes instead of a launch of
  * its own (an MD step is then four launches: step, descreening, force,
- * chain rule): PB2_FUSE_BONDED, the bonded terms as the chain pass's tail
- * work; PB2_FUSE_FINALIZE, each system's Born radii computed by the
- * descreening warp that completes the system (one warp per system: a gain
- * for small systems, a tail for large ones).  Defaults: bonded fused,
- * finalize fused when every system has at most 256 atoms; the autotuner
- * times the alternatives.  Results are bit-identical either way.  No
- * reference counterpart. */
+ * chain rule; a cutoff run with a pair list adds the list's update):
+ * PB2_FUSE_BONDED, the bonded terms as the chain pass's tail work, 32 terms
+ * per chunk; PB2_FUSE_FINALIZE, the Born radii as the descreening pass's
+ * tail work, one chunk per 32-atom block, each started once its system's
+ * pair items have all been summed (a bounded wait on work already in
+ * flight; PB2_STATUS_WAIT_TIMEOUT if it ever gives up).  Default: both; the
+ * autotuner times the alternatives.  Results are bit-identical either way.
+ * No reference counterpart. */
 #define PB2_FUSE_BONDED 0x1
 #define PB2_FUSE_FINALIZE 0x2
 int pb2_set_fusion(pb2_batch *batch, int32_t flags);
@@ -465,6 +470,14 @@ int pb2_last_timings(pb2_batch *batch, double *out_ms);
 /* Measured FP32 FMA throughput of the context's GPU (TFLOP/s), the roofline
  * denominator of the pair kernels.  Diagnostic: no reference counterpart. */
 int pb2_fp32_peak(pb2_ctx *ctx, double *tflops);
+/* Checks the integrator's FP64 division (a precomputed reciprocal and two
+ * Markstein corrections) bit for bit against the correctly rounded division
+ * on n seeded operand pairs (masses 0.5-512, momenta of any sign and
+ * exponents -40..40, plus structured cases).  mismatches: pairs whose bits
+ * differ; example (may be NULL): the first such (p, m).  Diagnostic, no
+ * reference counterpart. */
+int pb2_diag_div_check(pb2_ctx *ctx, long long n, unsigned long long seed, long long *mismatches,
+                       double *example);
 
 /*
  * Born radii of one system with no device allocation (no counterpart in the

@@ -27,7 +27,7 @@ HOST_LIB = PKG / "libpb2_host.so"
 CUDA_SOURCES = ["pb2_api.cu", "pb2_pair.cu", "pb2_energy64.cu", "pb2_bonded.cu",
                 "pb2_integrate.cu", "pb2_nlist.cu", "pb2_noalloc.cu", "pb2_diag.cu",
                 "pb2_transfer.cu", "pb2_minimize.cu", "pb2_pairlist.cu"]
-CUDA_HEADERS = ["pb2_common.cuh", "pb2_kernels.cuh", "pb2_internal.h", "pb2_pairmath.cuh",
+CUDA_HEADERS = ["pb2_common.cuh", "pb2_divide.cuh", "pb2_kernels.cuh", "pb2_internal.h", "pb2_pairmath.cuh",
                 "pb2_threefry.cuh", "pb2_obc_series.cuh", "pb2_bonded.cuh"]
 HOST_SOURCES = ["synth_chain.c"]
 

@@ -28,7 +28,7 @@ ABI_VERSION = 3  # PB2_ABI_VERSION of the structures mirrored below
 USE_BONDED, USE_CMAP, USE_LJ, USE_COULOMB, USE_GB = 0x1, 0x2, 0x4, 0x8, 0x10
 USE_ALL = 0x1F
 FUSE_BONDED, FUSE_FINALIZE = 0x1, 0x2
-STATUS_NONFINITE, STATUS_NLOVERFLOW, STATUS_FORCE_RANGE = 0x1, 0x2, 0x4
+STATUS_NONFINITE, STATUS_NLOVERFLOW, STATUS_FORCE_RANGE, STATUS_WAIT_TIMEOUT = 0x1, 0x2, 0x4, 0x8
 
 _c_dp = ctypes.POINTER(ctypes.c_double)
 _c_ip = ctypes.POINTER(ctypes.c_int32)
@@ -141,6 +141,8 @@ SIGNATURES = [
     ("pb2_set_profiling", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("pb2_last_timings", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     ("pb2_fp32_peak", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
+    ("pb2_diag_div_check", ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_ulonglong,
+                                          ctypes.POINTER(ctypes.c_longlong), ctypes.c_void_p]),
     ("pb2_born_radii_noalloc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
                                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
                                               ctypes.c_void_p, ctypes.c_void_p]),

@@ -286,8 +286,10 @@ static int setup_items2(pb2_batch *b, int seg) {
   if (!b->sys_items) {
     b->sys_items = b->dev.alloc<int32_t>(b->n_sys);
     b->sys_done = b->dev.alloc<int32_t>(b->n_sys);
-    if (!b->sys_items || !b->sys_done) return fail(ctx, PB2_ENOMEM, "work-item allocation failed");
+    b->sys_fin = b->dev.alloc<int32_t>(b->n_sys);
+    if (!b->sys_items || !b->sys_done || !b->sys_fin) return fail(ctx, PB2_ENOMEM, "work-item allocation failed");
     CUDA_TRY(ctx, cudaMemset(b->sys_done, 0, b->n_sys * sizeof(int32_t)));
+    CUDA_TRY(ctx, cudaMemset(b->sys_fin, 0, b->n_sys * sizeof(int32_t)));
   }
   CUDA_TRY(ctx, cudaMemcpy(b->sys_items, per_sys.data(), per_sys.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
   for (int p = 0; p < 3; ++p) set_pair_grid(b, p);
@@ -865,11 +867,7 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   if ((rc = setup_items2(b.get(), b->params.tile_segment))) return rc;
   if ((rc = setup_pair_list(b.get(), b->params.tile_segment))) return rc;
   {
-    // a system's Born radii are finalized by one warp when fused: worth it
-    // for small systems only (the autotuner may change this)
-    int nmax = 0;
-    for (int s = 0; s < n_systems; ++s) nmax = std::max(nmax, b->sys_host[s].n);
-    b->fuse = PB2_FUSE_BONDED | (nmax <= 256 ? PB2_FUSE_FINALIZE : 0);
+    b->fuse = PB2_FUSE_BONDED | PB2_FUSE_FINALIZE;  // the autotuner may change this
   }
   CUDA_TRY(ctx, cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking));
   CUDA_TRY(ctx, cudaEventCreate(&b->ev[0]));
@@ -946,8 +944,13 @@ static cudaError_t enqueue_forces(pb2_batch *b, cudaStream_t st, bool bonded_ene
     fa.born64 = nullptr;
     fa.n_total = b->n_total;
     fa.energy_mode = 0;
-    // the descreening pass finalizes each system as its last item completes
-    // (profiling keeps the separate launch, to time it)
+    fa.blk_sys = b->blk_sys;
+    fa.n_blocks = b->n_blocks;
+    fa.sys_fin = b->sys_fin;
+    fa.retired = b->retired;
+    fa.status = b->status;
+    // the descreening pass finalizes each block once its system's items are
+    // summed (profiling keeps the separate launch, to time it)
     const bool fuse_finalize = !b->profiling && (b->fuse & PB2_FUSE_FINALIZE);
     PairArgs pb = pa;
     pb.sched = b->sched + 2 * PASS_BORN;

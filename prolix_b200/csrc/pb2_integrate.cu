@@ -18,6 +18,7 @@
 // chunk.  Keys live in two buffers: a step reads
 // buffer `parity` and writes the advanced key to the other.
 #include "pb2_common.cuh"
+#include "pb2_divide.cuh"
 #include "pb2_kernels.cuh"
 #include "pb2_threefry.cuh"
 
@@ -100,6 +101,7 @@ __device__ __forceinline__ float4 step_atom(const IntArgs &a, int i, int s, cons
     const int rnd = a.user[i] - S.off;  // the atom's index in the caller's order: its noise
     const double h = S.half_dt;
     const double m = a.mass[i];
+    const double rm = __drcp_rn(m);  // p / m = div_by(p, m, rm), correctly rounded
     const long long lfx = a.fx[i], lfy = a.fy[i], lfz = a.fz[i];
     check_fix(a, s, lfx); check_fix(a, s, lfy); check_fix(a, s, lfz);
     const double f[3] = {fix_to_d(lfx), fix_to_d(lfy), fix_to_d(lfz)};
@@ -114,10 +116,10 @@ __device__ __forceinline__ float4 step_atom(const IntArgs &a, int i, int s, cons
     for (int c = 0; c < 3; ++c) {
       if (a.finish_prev) p[c] = __dadd_rn(p[c], __dmul_rn(h, f[c]));
       p[c] = __dadd_rn(p[c], __dmul_rn(h, f[c]));
-      x[c] = __dadd_rn(x[c], __dmul_rn(h, __ddiv_rn(p[c], m)));
+      x[c] = __dadd_rn(x[c], __dmul_rn(h, div_by(p[c], m, rm)));
       const float xi = normal_from_bits(random_bits32(sub, 3u * (uint32_t)rnd + c, count, a.partitionable != 0));
       p[c] = __dadd_rn(__dmul_rn(c1, p[c]), __dmul_rn(sg, (double)xi));
-      x[c] = __dadd_rn(x[c], __dmul_rn(h, __ddiv_rn(p[c], m)));
+      x[c] = __dadd_rn(x[c], __dmul_rn(h, div_by(p[c], m, rm)));
     }
     a.px[i] = p[0]; a.py[i] = p[1]; a.pz[i] = p[2];
     a.x[i] = x[0]; a.y[i] = x[1]; a.z[i] = x[2];
@@ -197,6 +199,7 @@ __device__ __forceinline__ float4 step_guarded_atom(const IntArgs &a, int i, int
     const int rnd = a.user[i] - S.off;
     const double h = S.half_dt;
     const double m = a.mass[i];
+    const double rm = __drcp_rn(m);  // p / m = div_by(p, m, rm), correctly rounded
     const long long lfx = a.fx[i], lfy = a.fy[i], lfz = a.fz[i];
     check_fix(a, s, lfx); check_fix(a, s, lfy); check_fix(a, s, lfz);
     double f[3] = {fix_to_d(lfx), fix_to_d(lfy), fix_to_d(lfz)};
@@ -213,7 +216,7 @@ __device__ __forceinline__ float4 step_guarded_atom(const IntArgs &a, int i, int
       p[c] = __dadd_rn(p[c], __dmul_rn(h, f[c]));
     }
     if (a.vlimit > 0.0) {
-      const double vm = norm3(__ddiv_rn(p[0], m), __ddiv_rn(p[1], m), __ddiv_rn(p[2], m), 1e-30);
+      const double vm = norm3(div_by(p[0], m, rm), div_by(p[1], m, rm), div_by(p[2], m, rm), 1e-30);
       if (vm > a.vlimit) {
         const double sc = fmin(1.0, __ddiv_rn(a.vlimit, __dadd_rn(vm, 1e-30)));
 #pragma unroll
@@ -227,10 +230,10 @@ __device__ __forceinline__ float4 step_guarded_atom(const IntArgs &a, int i, int
     const double c1 = S.c1, sg = a.sigma[i];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      x[c] = __dadd_rn(x[c], __dmul_rn(h, __ddiv_rn(p[c], m)));
+      x[c] = __dadd_rn(x[c], __dmul_rn(h, div_by(p[c], m, rm)));
       const float xi = normal_from_bits(random_bits32(sub, 3u * (uint32_t)rnd + c, count, a.partitionable != 0));
       p[c] = __dadd_rn(__dmul_rn(c1, p[c]), __dmul_rn(sg, (double)xi));
-      x[c] = __dadd_rn(x[c], __dmul_rn(h, __ddiv_rn(p[c], m)));
+      x[c] = __dadd_rn(x[c], __dmul_rn(h, div_by(p[c], m, rm)));
     }
     if (a.max_dx > 0.0) {
       const double d[3] = {__dsub_rn(x[0], xo[0]), __dsub_rn(x[1], xo[1]), __dsub_rn(x[2], xo[2])};

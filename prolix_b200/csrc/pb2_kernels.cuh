@@ -51,6 +51,12 @@ struct FinalizeArgs {
   double *born64;   // NULL, or FP64 Born radii out
   int32_t n_total;
   int32_t energy_mode;
+  // finalize as the descreening pass's tail chunks (one per 32-atom block)
+  const int32_t *blk_sys;
+  int32_t n_blocks;
+  int32_t *sys_fin;        // per system: chunks finished in this launch
+  const int8_t *retired;   // per system: retired systems are skipped
+  uint32_t *status;
 };
 struct PairArgs {
   const SysInfo *sys;
@@ -80,9 +86,10 @@ struct PairArgs {
   // of kBondedChunk (0 chunks: the bonded kernel runs on its own)
   BondedArgs bonded;
   int32_t n_bonded_chunks;
-  // descreening pass: with sys_items set, the warp that completes a
-  // system's sys_items[s]-th item finalizes its Born radii (fin); sys_done
-  // counts completed items and is reset by that warp
+  // descreening pass: with sys_items set, the warps count each system's
+  // completed items in sys_done, and after the items come fin.n_blocks
+  // finalize chunks, each waiting until its system's count reaches
+  // sys_items[s]; the system's last chunk resets both counters
   const int32_t *sys_items;
   int32_t *sys_done;
   FinalizeArgs fin;

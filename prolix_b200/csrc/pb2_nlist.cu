@@ -68,10 +68,11 @@ __global__ void nl_disp_kernel(const NlArgs a) {
 
 // 1. rows: one thread block (8 warps) per block of atoms; warp w owns the
 // block's rows 4w .. 4w + 3.  Warp 0 lists, in order, the blocks within
-// reach of this one; then each warp walks that list one j-block at a time,
-// lane = candidate atom: one position load serves the warp's four rows,
-// and each row's hits are compacted by a ballot and stored as one
-// contiguous run (coalesced), so rows come out in j order.
+// reach of this one; each warp narrows that list, 32 blocks at a time, to
+// the blocks within reach of one of its own four atoms, and walks those one
+// j-block at a time, lane = candidate atom: one position load serves the
+// warp's four rows, and each row's hits are compacted by a ballot and
+// stored as one contiguous run (coalesced), so rows come out in j order.
 constexpr int kMaxJList = 4096;  // j-blocks listed at once (longer systems: in windows)
 constexpr int kRowsPerWarp = 32 / kRowsWarps;
 
@@ -109,18 +110,35 @@ __global__ void __launch_bounds__(32 * kRowsWarps) nl_rows_kernel(const NlArgs a
       __syncthreads();
       if (l0 >= S.n) continue;  // a warp past the system's last atom has no rows
       const int L = n_live;
-      for (int k = 0; k < L; ++k) {
-        const int lj = jl[k] * 32 + lane;
-        const bool vj = lj < S.n;
-        const float4 q = a.posq[S.off + (vj ? lj : 0)];
+      for (int k0 = 0; k0 < L; k0 += 32) {
+        // the listed blocks within reach of one of the warp's four atoms
+        // (lane = block; the margin keeps the test conservative under
+        // rounding), then their atoms, lane = candidate
+        bool near = false;
+        if (k0 + lane < L) {
+          const int gjb = S.blk_base + jl[k0 + lane];
+          const float4 lo = a.bbox[2 * gjb], hi = a.bbox[2 * gjb + 1];
 #pragma unroll
-        for (int r = 0; r < kRowsPerWarp; ++r) {
-          const float ex = p[r].x - q.x, ey = p[r].y - q.y, ez = p[r].z - q.z;
-          const bool hit = vj && l0 + r < S.n && lj != l0 + r && fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < a.reach2;
-          const unsigned m = __ballot_sync(kFull, hit);
-          const int t = cnt[r] + __popc(m & below);
-          if (hit && t < a.capacity) a.rows[(size_t)(S.off + l0 + r) * a.capacity + t] = lj;
-          cnt[r] += __popc(m);
+          for (int r = 0; r < kRowsPerWarp; ++r) {
+            const float dx = fmaxf(0.f, fmaxf(lo.x - p[r].x, p[r].x - hi.x));
+            const float dy = fmaxf(0.f, fmaxf(lo.y - p[r].y, p[r].y - hi.y));
+            const float dz = fmaxf(0.f, fmaxf(lo.z - p[r].z, p[r].z - hi.z));
+            near |= fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < a.reach2 * 1.0001f;
+          }
+        }
+        for (unsigned blocks = __ballot_sync(kFull, near); blocks != 0u; blocks &= blocks - 1u) {
+          const int lj = jl[k0 + __ffs(blocks) - 1] * 32 + lane;
+          const bool vj = lj < S.n;
+          const float4 q = a.posq[S.off + (vj ? lj : 0)];
+#pragma unroll
+          for (int r = 0; r < kRowsPerWarp; ++r) {
+            const float ex = p[r].x - q.x, ey = p[r].y - q.y, ez = p[r].z - q.z;
+            const bool hit = vj && l0 + r < S.n && lj != l0 + r && fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < a.reach2;
+            const unsigned m = __ballot_sync(kFull, hit);
+            const int t = cnt[r] + __popc(m & below);
+            if (hit && t < a.capacity) a.rows[(size_t)(S.off + l0 + r) * a.capacity + t] = lj;
+            cnt[r] += __popc(m);
+          }
         }
       }
     }

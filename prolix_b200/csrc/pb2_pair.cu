@@ -533,6 +533,48 @@ __device__ __forceinline__ void finalize_atom(const FinalizeArgs &a, int i, int 
   }
 }
 
+// Spins of the bounded waits (each after a 128 ns sleep): ~0.5 s at most.
+constexpr int kWaitSpins = 1 << 22;
+
+// Finalize chunk c (the batch's 32-atom block c) of the descreening pass:
+// wait until every item of its system has been counted, then turn the
+// block's sums into Born radii.  Every waited-for item was taken by a warp
+// of this launch that is running, so the wait ends; it is bounded all the
+// same, and a wait that gives up flags the system and skips the block.
+__device__ __noinline__ void finalize_chunk(const PairArgs &a, int c, const int32_t *sys_items, int lane) {
+  const int s = a.fin.blk_sys[c];
+  if (a.fin.retired && a.fin.retired[s]) return;
+  const SysInfo &S = a.sys[s];
+  int ok = 1;
+  if (lane == 0) {
+    const int want = sys_items[s];
+    const volatile int32_t *done = a.sys_done + s;
+    for (int spin = 0; *done < want; ++spin) {
+      if (spin >= kWaitSpins) {
+        ok = 0;
+        atomicOr(&a.fin.status[s], (uint32_t)PB2_STATUS_WAIT_TIMEOUT);
+        break;
+      }
+      __nanosleep(128);
+    }
+  }
+  ok = __shfl_sync(kFull, ok, 0);
+  __threadfence();  // acquire: the counted items' sums are visible to every lane
+  if (ok) {
+    const int l = (c - S.blk_base) * 32 + lane;
+    if (l < S.n) finalize_atom(a.fin, S.off + l, s, S);
+  }
+  __syncwarp();
+  if (lane == 0) {
+    // the system's last chunk (all of them past their wait) resets the
+    // counters for the next launch
+    if (atomicAdd(&a.fin.sys_fin[s], 1) == S.nblk - 1) {
+      a.sys_done[s] = 0;
+      a.fin.sys_fin[s] = 0;
+    }
+  }
+}
+
 __global__ void born_finalize(const FinalizeArgs a) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_total; i += gridDim.x * blockDim.x) {
     const int s = a.atom_sys[i];
@@ -572,6 +614,10 @@ __global__ void __launch_bounds__(THREADS, MINB)
   // the j-block of the current tile, one JTile per warp (4 KB)
   __shared__ JTile s_jt[kWarps];
   JTile &jt = s_jt[threadIdx.x >> 5];
+#ifdef PB2_ISUM_SMEM
+  __shared__ long long s_isum[PASS == PASS_FORCE ? kWarps : 1][8][32];
+  long long *si = &s_isum[PASS == PASS_FORCE ? (threadIdx.x >> 5) : 0][0][lane];
+#endif
   CfQueue Q;
   Q.c = {a.posq, a.par, a.born, a.dedb_acc, a.born_acc, a.fx, a.fy, a.fz};
   Q.q = s_cfq[PASS == PASS_FORCE ? 0 : (threadIdx.x >> 5)];
@@ -597,6 +643,15 @@ __global__ void __launch_bounds__(THREADS, MINB)
     if (lane == 0) it = atomicAdd(&a.sched[0], 1);
     it = __shfl_sync(kFull, it, 0);
     if (it >= n_items) {
+      if constexpr (PASS == PASS_BORN) {
+        // tail work: the Born radii of one 32-atom block, once its system's
+        // items have all been summed
+        const int c = it - n_items;
+        if (sys_items && c < a.fin.n_blocks) {
+          finalize_chunk(a, c, sys_items, lane);
+          continue;
+        }
+      }
       if constexpr (PASS == PASS_CHAIN) {
         // tail work: a chunk of the bonded terms (FP64, their own forces)
         const int c = it - n_items;
@@ -636,7 +691,24 @@ __global__ void __launch_bounds__(THREADS, MINB)
       else if (has1 && lane < 2 * kExclPerBlock) ent = a.excl_ent[gib1 * kExclPerBlock + lane - kExclPerBlock];
     }
 
+#ifndef PB2_HOIST_IF
+#define PB2_HOIST_IF 1
+#endif
+#if PB2_HOIST_IF
+    // the force pass's packed i-side data, once per item
+    FData2 IF{};
+    if constexpr (PASS == PASS_FORCE)
+      IF = {make_float2(I0.x, I1.x), make_float2(I0.y, I1.y), make_float2(I0.z, I1.z),
+            make_float2(I0.hs, I1.hs), make_float2(I0.se, I1.se),
+            make_float2(I0.B, I1.B), make_float2(I0.iB, I1.iB),
+            make_float2(2.f * K.pref * I0.q, 2.f * K.pref * I1.q),
+            make_float2(K.kcoul * I0.q, K.kcoul * I1.q)};
+#endif
     long long p0 = 0, p1 = 0, p2 = 0, p3 = 0, q0 = 0, q1 = 0, q2 = 0, q3 = 0;  // i-side sums
+#ifdef PB2_ISUM_SMEM
+    if constexpr (PASS == PASS_FORCE)
+      for (int k = 0; k < 8; ++k) si[32 * k] = 0;
+#endif
     for (int tt = item.jb0; tt < item.jb1; ++tt) {
       const int jb = plm ? a.pl_jlist[tt] : tt;
       const int gjb = S.blk_base + jb;
@@ -685,11 +757,13 @@ __global__ void __launch_bounds__(THREADS, MINB)
           const ExclRow r = a.excl_rows[roff + lane];
           E1 = rotr32(r.excl, lane); S1 = rotr32(r.s14, lane);
         }
+#if !PB2_HOIST_IF
         const FData2 IF = {make_float2(I0.x, I1.x), make_float2(I0.y, I1.y), make_float2(I0.z, I1.z),
                            make_float2(I0.hs, I1.hs), make_float2(I0.se, I1.se),
                            make_float2(I0.B, I1.B), make_float2(I0.iB, I1.iB),
                            make_float2(2.f * K.pref * I0.q, 2.f * K.pref * I1.q),
                            make_float2(K.kcoul * I0.q, K.kcoul * I1.q)};
+#endif
         Acc2F tf = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
         if (hit) run_force_tile2<CUT, false, true>(IF, jt, tf, tj, V0, V1, E0, E1, S0, S1, K);
         else if (!full) run_force_tile2<CUT, false, false>(IF, jt, tf, tj, V0, V1, E0, E1, S0, S1, K);
@@ -733,6 +807,15 @@ __global__ void __launch_bounds__(THREADS, MINB)
             atomic_add_fix(&a.dedb_acc[jg], to_fix_f(tj.a3 * (-0.5f * J.rB), bscale));
         }
       }
+#ifdef PB2_ISUM_SMEM
+      if constexpr (PASS == PASS_FORCE) {
+        si[0] += to_fix_f(t0.a0, bscale); si[32] += to_fix_f(t0.a1, bscale);
+        si[64] += to_fix_f(t0.a2, bscale); si[96] += to_fix_f(t0.a3 * (-0.5f * I0.rB), bscale);
+        si[128] += to_fix_f(t1.a0, bscale); si[160] += to_fix_f(t1.a1, bscale);
+        si[192] += to_fix_f(t1.a2, bscale); si[224] += to_fix_f(t1.a3 * (-0.5f * I1.rB), bscale);
+        continue;
+      }
+#endif
       p0 += to_fix_f(t0.a0, bscale);
       q0 += to_fix_f(t1.a0, bscale);
       if (PASS != PASS_BORN) {
@@ -744,25 +827,23 @@ __global__ void __launch_bounds__(THREADS, MINB)
         q3 += to_fix_f(t1.a3 * (-0.5f * I1.rB), bscale);
       }
     }
+#ifdef PB2_ISUM_SMEM
+    if constexpr (PASS == PASS_FORCE) {
+      p0 = si[0]; p1 = si[32]; p2 = si[64]; p3 = si[96];
+      q0 = si[128]; q1 = si[160]; q2 = si[192]; q3 = si[224];
+    }
+#endif
 
     if (PASS == PASS_BORN) {
       if (iv0 && p0 != 0) atomic_add_fix(&a.born_acc[ig0], p0);
       if (iv1 && q0 != 0) atomic_add_fix(&a.born_acc[ig1], q0);
       if (sys_items) {
-        // the warp that completes a system's last item turns its sums into
-        // Born radii: first its queued closed-form pairs, which may belong
-        // to this item, then a release fence before the count
+        // count the item as summed: first the warp's queued closed-form
+        // pairs, which may belong to it, then a release fence
         if (Q.n > 0) cf_drain<PASS>(Q, lane);
         __threadfence();
         __syncwarp();
-        int last = 0;
-        if (lane == 0) last = atomicAdd(&a.sys_done[item.sys], 1) == sys_items[item.sys] - 1;
-        if (__shfl_sync(kFull, last, 0)) {
-          __threadfence();
-#pragma unroll 4
-          for (int l = lane; l < n; l += 32) finalize_atom(a.fin, off + l, item.sys, S);
-          if (lane == 0) a.sys_done[item.sys] = 0;  // ready for the next launch
-        }
+        if (lane == 0) atomicAdd(&a.sys_done[item.sys], 1);
       }
     } else {
       if (iv0) {
@@ -835,7 +916,11 @@ struct Shape {
 };
 constexpr Shape kShapes[3][kShapesPerPass] = {
     {{256, 3}, {256, 2}, {128, 6}},   // descreening
+#ifdef PB2_EXP_FORCE_128x3
+    {{256, 2}, {128, 4}, {128, 3}},   // force
+#else
     {{256, 2}, {128, 4}, {128, 5}},   // force
+#endif
     {{256, 2}, {128, 4}, {128, 5}}};  // chain rule
 
 template <int PASS, bool CUT, bool ALL, int SH>
