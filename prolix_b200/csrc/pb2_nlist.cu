@@ -76,6 +76,24 @@ __global__ void nl_disp_kernel(const NlArgs a) {
 constexpr int kMaxJList = 4096;  // j-blocks listed at once (longer systems: in windows)
 constexpr int kRowsPerWarp = 32 / kRowsWarps;
 
+// One j-block's 32 candidates (lane = candidate lj at q) against the
+// warp's rows l0 .. l0 + 3: each row's hits are compacted by a ballot and
+// stored as one contiguous run.  DIAG: the block holds the rows' own atoms.
+template <bool DIAG>
+__device__ __forceinline__ void nl_rows_block(const NlArgs &a, const SysInfo &S, const float4 *p, float4 q, int lj,
+                                              int l0, unsigned below, int *cnt) {
+#pragma unroll
+  for (int r = 0; r < kRowsPerWarp; ++r) {
+    const float ex = p[r].x - q.x, ey = p[r].y - q.y, ez = p[r].z - q.z;
+    bool hit = fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < a.reach2;
+    if (DIAG) hit = hit && lj != l0 + r;
+    const unsigned m = __ballot_sync(kFull, hit);
+    const int t = cnt[r] + __popc(m & below);
+    if (hit && t < a.capacity) a.rows[(size_t)(S.off + l0 + r) * a.capacity + t] = lj;
+    cnt[r] += __popc(m);
+  }
+}
+
 __global__ void __launch_bounds__(32 * kRowsWarps) nl_rows_kernel(const NlArgs a) {
   if (!nl_dirty(a)) return;
   __shared__ int jl[kMaxJList];
@@ -91,8 +109,10 @@ __global__ void __launch_bounds__(32 * kRowsWarps) nl_rows_kernel(const NlArgs a
 #pragma unroll
     for (int r = 0; r < kRowsPerWarp; ++r) {
       p[r] = a.posq[S.off + min(l0 + r, S.n - 1)];
+      if (l0 + r >= S.n) p[r].x = -1e30f;  // no row: never within reach of an atom
       cnt[r] = 0;
     }
+    const int own = ib - S.blk_base;
     for (int j0 = 0; j0 < S.nblk; j0 += kMaxJList) {
       const int j1 = min(S.nblk, j0 + kMaxJList);
       __syncthreads();  // the previous window's list is no longer read
@@ -127,18 +147,12 @@ __global__ void __launch_bounds__(32 * kRowsWarps) nl_rows_kernel(const NlArgs a
           }
         }
         for (unsigned blocks = __ballot_sync(kFull, near); blocks != 0u; blocks &= blocks - 1u) {
-          const int lj = jl[k0 + __ffs(blocks) - 1] * 32 + lane;
-          const bool vj = lj < S.n;
-          const float4 q = a.posq[S.off + (vj ? lj : 0)];
-#pragma unroll
-          for (int r = 0; r < kRowsPerWarp; ++r) {
-            const float ex = p[r].x - q.x, ey = p[r].y - q.y, ez = p[r].z - q.z;
-            const bool hit = vj && l0 + r < S.n && lj != l0 + r && fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < a.reach2;
-            const unsigned m = __ballot_sync(kFull, hit);
-            const int t = cnt[r] + __popc(m & below);
-            if (hit && t < a.capacity) a.rows[(size_t)(S.off + l0 + r) * a.capacity + t] = lj;
-            cnt[r] += __popc(m);
-          }
+          const int jb = jl[k0 + __ffs(blocks) - 1];
+          const int lj = jb * 32 + lane;
+          float4 q = a.posq[S.off + min(lj, S.n - 1)];
+          if (lj >= S.n) q.x = 1e30f;  // no atom: never within reach of a row
+          if (jb == own) nl_rows_block<true>(a, S, p, q, lj, l0, below, cnt);  // skips i = j
+          else nl_rows_block<false>(a, S, p, q, lj, l0, below, cnt);
         }
       }
     }
