@@ -113,8 +113,8 @@ CLOSED_FORM_FLOPS_PER_PAIR = {"born": 80.0, "force": 70.0, "chain": 90.0}
 BYTES_PER_ATOM_STEP = 184
 # DRAM traffic per launch of each pair pass on this workload
 # (dram__bytes_read.sum + dram__bytes_write.sum of one `ncu --set full`
-# capture; profiles/pair_kernels_ragged512.md gives the command)
-TRAFFIC_BYTES = {"born": 24.17e6, "force": 71.60e6, "chain": 47.37e6}
+# capture of the three passes, default block shapes and fusion)
+TRAFFIC_BYTES = {"born": 33.58e6, "force": 71.35e6, "chain": 127.49e6}
 
 
 def parse():

@@ -1,4 +1,4 @@
-// BAOAB Langevin integrator, all systems of the batch.
+// BAOAB Langevin integrator, all systems of the batch, one thread per atom.
 //
 // Order and arithmetic follow prolix physics/settle.py:1698-1744 with the
 // step helpers :2064-2087 (the jax_md nvt_langevin order):
@@ -10,10 +10,8 @@
 // expressions, so with identical forces the update is bit-identical to the
 // CPU restatement.
 //
-// Kernel boundaries: step3_kernel (one thread per atom and component; the
-// safeguarded step_guarded_kernel, one thread per atom) applies the final
-// half kick of the previous step (when finish_prev), the first half kick, A,
-// O, A of the new
+// Kernel boundaries: step_kernel applies the final half kick of the
+// previous step (when finish_prev), the first half kick, A, O, A of the new
 // step, converts the new positions for the float32 pair kernels, writes the
 // 32-atom blocks' bounding boxes and clears the force accumulators; the
 // force kernels then run; finish_kernel applies the last half kick of a
@@ -96,80 +94,62 @@ __global__ void key_splits_kernel(const IntArgs a) {
   }
 }
 
-// The plain step, three warps per 32-atom block: warp c updates component
-// c (x, y or z) of the block's 32 atoms, so a thread carries one third of an
-// atom's work (one threefry draw, two divisions) and the SM holds three
-// times as many independent threads, which is what hides the memory latency
-// of this short launch.  Per component, in the reference's order:
-// p += dt/2 F (twice after a step whose closing kick was deferred), x +=
-// dt/2 p/m, p = c1 p + c2 sqrt(m kT) xi, x += dt/2 p/m, every FP64 operation
-// correctly rounded.  The new float32 positions meet in shared
-// memory: each warp reduces its component's bounding-box extent, and warp 0
-// writes posq, runs the pair list's displacement test and advances the
-// system's key.
-__global__ void __launch_bounds__(96, 12) step3_kernel(const IntArgs a) {
-  __shared__ float pos[3][32];
-  const int b = blockIdx.x;
-  const int s = a.blk_sys[b];
-  if (a.retired[s]) return;  // a retired system keeps its state and box
-  const SysInfo &S = a.sys[s];
-  const int lane = threadIdx.x & 31, c = threadIdx.x >> 5;
-  const int l = (b - S.blk_base) * 32 + lane;
-  const bool valid = l < S.n;
-  const int i = S.off + (valid ? l : 0);
-  const double org = c == 0 ? S.ox : (c == 1 ? S.oy : S.oz);
-  const uint4 sp = reinterpret_cast<const uint4 *>(a.splits)[(size_t)a.parity * a.n_sys + s];
-  if (valid) {
-    long long *fc = c == 0 ? a.fx : (c == 1 ? a.fy : a.fz);
-    double *pc = c == 0 ? a.px : (c == 1 ? a.py : a.pz);
-    double *xc = c == 0 ? a.x : (c == 1 ? a.y : a.z);
+// One atom's plain BAOAB step; returns the float32 position it wrote.
+__device__ __forceinline__ float4 step_atom(const IntArgs &a, int i, int s, const SysInfo &S) {
+  {
+    const int loc = i - S.off;
     const int rnd = a.user[i] - S.off;  // the atom's index in the caller's order: its noise
     const double h = S.half_dt;
     const double m = a.mass[i];
-    const double rm = __drcp_rn(m);
-    const long long lf = fc[i];
-    check_fix(a, s, lf);
-    const double f = fix_to_d(lf);
-    fc[i] = 0;
-    double p = pc[i], x = xc[i];
-    const uint32_t sub[2] = {sp.z, sp.w};
+    const double rm = __drcp_rn(m);  // p / m = div_by(p, m, rm), correctly rounded
+    const long long lfx = a.fx[i], lfy = a.fy[i], lfz = a.fz[i];
+    check_fix(a, s, lfx); check_fix(a, s, lfy); check_fix(a, s, lfz);
+    const double f[3] = {fix_to_d(lfx), fix_to_d(lfy), fix_to_d(lfz)};
+    a.fx[i] = 0; a.fy[i] = 0; a.fz[i] = 0;
+    double p[3] = {a.px[i], a.py[i], a.pz[i]};
+    double x[3] = {a.x[i], a.y[i], a.z[i]};
+    const uint4 sp = reinterpret_cast<const uint4 *>(a.splits)[(size_t)a.parity * a.n_sys + s];
+    const uint32_t knew[2] = {sp.x, sp.y}, sub[2] = {sp.z, sp.w};
     const uint32_t count = 3u * (uint32_t)S.n;
-    if (a.finish_prev) p = __dadd_rn(p, __dmul_rn(h, f));
-    p = __dadd_rn(p, __dmul_rn(h, f));
-    x = __dadd_rn(x, __dmul_rn(h, div_by(p, m, rm)));
-    const float xi = normal_from_bits(random_bits32(sub, 3u * (uint32_t)rnd + c, count, a.partitionable != 0));
-    p = __dadd_rn(__dmul_rn(S.c1, p), __dmul_rn(a.sigma[i], (double)xi));
-    x = __dadd_rn(x, __dmul_rn(h, div_by(p, m, rm)));
-    pc[i] = p;
-    xc[i] = x;
-    pos[c][lane] = (float)(x - org);
-    if (!(isfinite(x) && isfinite(p))) atomicOr(&a.status[s], (uint32_t)PB2_STATUS_NONFINITE);
-  }
-  __syncthreads();
-  // the block's extent along component c (lanes past the system's last atom
-  // take the block's first atom)
-  float lo = pos[c][valid ? lane : 0], hi = lo;
+    const double c1 = S.c1, sg = a.sigma[i];
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    lo = fminf(lo, __shfl_xor_sync(kFull, lo, o));
-    hi = fmaxf(hi, __shfl_xor_sync(kFull, hi, o));
-  }
-  if (lane == 0) {
-    reinterpret_cast<float *>(&a.bbox[2 * b])[c] = lo;
-    reinterpret_cast<float *>(&a.bbox[2 * b + 1])[c] = hi;
-    if (c == 0) {
-      a.bbox[2 * b].w = 0.f;
-      a.bbox[2 * b + 1].w = 0.f;
+    for (int c = 0; c < 3; ++c) {
+      if (a.finish_prev) p[c] = __dadd_rn(p[c], __dmul_rn(h, f[c]));
+      p[c] = __dadd_rn(p[c], __dmul_rn(h, f[c]));
+      x[c] = __dadd_rn(x[c], __dmul_rn(h, div_by(p[c], m, rm)));
+      const float xi = normal_from_bits(random_bits32(sub, 3u * (uint32_t)rnd + c, count, a.partitionable != 0));
+      p[c] = __dadd_rn(__dmul_rn(c1, p[c]), __dmul_rn(sg, (double)xi));
+      x[c] = __dadd_rn(x[c], __dmul_rn(h, div_by(p[c], m, rm)));
     }
+    a.px[i] = p[0]; a.py[i] = p[1]; a.pz[i] = p[2];
+    a.x[i] = x[0]; a.y[i] = x[1]; a.z[i] = x[2];
+    const float4 q = write_posq(a, i, S, x[0], x[1], x[2]);
+    if (!(isfinite(x[0]) && isfinite(x[1]) && isfinite(x[2]) && isfinite(p[0]) &&
+          isfinite(p[1]) && isfinite(p[2])))
+      atomicOr(&a.status[s], (uint32_t)PB2_STATUS_NONFINITE);
+    if (loc == 0) advance_key(a, s, knew);
+    return q;
   }
-  if (c != 0) return;
+}
+
+__global__ void __launch_bounds__(256, 4) step_kernel(const IntArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int nw = (int)((gridDim.x * blockDim.x) >> 5);
   bool moved = false;
-  if (valid) {
-    const float4 q = make_float4(pos[0][lane], pos[1][lane], pos[2][lane], (float)a.charge[i]);
-    a.posq[i] = q;
-    moved = moved_past_half_skin(a, i, S, q);
-    const uint32_t knew[2] = {sp.x, sp.y};
-    if (l == 0) advance_key(a, s, knew);
+  for (int b = w; b < a.n_blocks; b += nw) {
+    const int s = a.blk_sys[b];
+    const SysInfo &S = a.sys[s];
+    const int blk_base = S.blk_base, n = S.n;  // loaded beside the retired flag, not after it
+    if (a.retired[s]) continue;  // a retired system keeps its state and box
+    const int l = (b - blk_base) * 32 + lane;
+    const bool valid = l < n;
+    float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (valid) {
+      q = step_atom(a, S.off + l, s, S);
+      moved |= moved_past_half_skin(a, S.off + l, S, q);
+    }
+    block_box(a, b, lane, valid, q);
   }
   if (a.pl_ctl && __any_sync(kFull, moved) && lane == 0) atomicOr(&a.pl_ctl[PL_DIRTY], 1);
 }
@@ -291,10 +271,11 @@ __global__ void __launch_bounds__(256, 4) step_guarded_kernel(const IntArgs a) {
   bool moved = false;
   for (int b = w; b < a.n_blocks; b += nw) {
     const int s = a.blk_sys[b];
-    if (a.retired[s]) continue;  // a retired system keeps its state and box
     const SysInfo &S = a.sys[s];
-    const int l = (b - S.blk_base) * 32 + lane;
-    const bool valid = l < S.n;
+    const int blk_base = S.blk_base, n = S.n;  // loaded beside the retired flag, not after it
+    if (a.retired[s]) continue;  // a retired system keeps its state and box
+    const int l = (b - blk_base) * 32 + lane;
+    const bool valid = l < n;
     float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
     if (valid) {
       q = step_guarded_atom(a, S.off + l, s, S, cap_open);
@@ -426,11 +407,12 @@ static int grid_for(int n) {
 static bool guarded(const IntArgs &a) { return a.vlimit > 0.0 || a.max_dx > 0.0 || a.force_cap > 0.0; }
 
 cudaError_t launch_step(const IntArgs &a, cudaStream_t st) {
-  if (a.n_blocks <= 0) return cudaSuccess;
+  const int grid = (a.n_blocks + 7) / 8;  // 8 warps, one 32-atom block each
+  if (grid <= 0) return cudaSuccess;
   if (guarded(a))
-    step_guarded_kernel<<<(a.n_blocks + 7) / 8, 256, 0, st>>>(a);  // 8 warps, one 32-atom block each
+    step_guarded_kernel<<<grid, 256, 0, st>>>(a);
   else
-    step3_kernel<<<a.n_blocks, 96, 0, st>>>(a);  // 3 warps (x, y, z) per 32-atom block
+    step_kernel<<<grid, 256, 0, st>>>(a);
   return cudaGetLastError();
 }
 cudaError_t launch_finish(const IntArgs &a, cudaStream_t st) {

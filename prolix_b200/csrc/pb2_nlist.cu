@@ -76,21 +76,40 @@ __global__ void nl_disp_kernel(const NlArgs a) {
 constexpr int kMaxJList = 4096;  // j-blocks listed at once (longer systems: in windows)
 constexpr int kRowsPerWarp = 32 / kRowsWarps;
 
-// One j-block's 32 candidates (lane = candidate lj at q) against the
-// warp's rows l0 .. l0 + 3: each row's hits are compacted by a ballot and
-// stored as one contiguous run.  DIAG: the block holds the rows' own atoms.
+// One j-block's 32 candidates (lane = candidate lj; nq = minus its
+// position, duplicated) against the warp's rows l0 .. l0 + 3, whose
+// positions are held in pairs (rows 0, 1 and 2, 3) so that the distances
+// run as packed f32x2 arithmetic (per component the same roundings as the
+// scalar fmaf chain).  Each row's hits are compacted by a ballot and stored
+// as one contiguous run.  DIAG: the block holds the rows' own atoms.
+struct NlRows4 {
+  float2 x[2], y[2], z[2];
+};
+
+__device__ __forceinline__ void nl_hit_row(const NlArgs &a, const SysInfo &S, bool hit, int lj, int row, unsigned below,
+                                           int &cnt) {
+  const unsigned m = __ballot_sync(kFull, hit);
+  const int t = cnt + __popc(m & below);
+  if (hit && t < a.capacity) a.rows[(size_t)(S.off + row) * a.capacity + t] = lj;
+  cnt += __popc(m);
+}
+
 template <bool DIAG>
-__device__ __forceinline__ void nl_rows_block(const NlArgs &a, const SysInfo &S, const float4 *p, float4 q, int lj,
+__device__ __forceinline__ void nl_rows_block(const NlArgs &a, const SysInfo &S, const NlRows4 &P, float4 q, int lj,
                                               int l0, unsigned below, int *cnt) {
+  const float2 nqx = make_float2(-q.x, -q.x), nqy = make_float2(-q.y, -q.y), nqz = make_float2(-q.z, -q.z);
 #pragma unroll
-  for (int r = 0; r < kRowsPerWarp; ++r) {
-    const float ex = p[r].x - q.x, ey = p[r].y - q.y, ez = p[r].z - q.z;
-    bool hit = fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < a.reach2;
-    if (DIAG) hit = hit && lj != l0 + r;
-    const unsigned m = __ballot_sync(kFull, hit);
-    const int t = cnt[r] + __popc(m & below);
-    if (hit && t < a.capacity) a.rows[(size_t)(S.off + l0 + r) * a.capacity + t] = lj;
-    cnt[r] += __popc(m);
+  for (int h = 0; h < 2; ++h) {
+    const float2 ex = __fadd2_rn(P.x[h], nqx), ey = __fadd2_rn(P.y[h], nqy), ez = __fadd2_rn(P.z[h], nqz);
+    const float2 d2 = __ffma2_rn(ex, ex, __ffma2_rn(ey, ey, __fmul2_rn(ez, ez)));
+    const int r0 = 2 * h, r1 = 2 * h + 1;
+    bool hit0 = d2.x < a.reach2, hit1 = d2.y < a.reach2;
+    if (DIAG) {
+      hit0 = hit0 && lj != l0 + r0;
+      hit1 = hit1 && lj != l0 + r1;
+    }
+    nl_hit_row(a, S, hit0, lj, l0 + r0, below, cnt[r0]);
+    nl_hit_row(a, S, hit1, lj, l0 + r1, below, cnt[r1]);
   }
 }
 
@@ -111,6 +130,14 @@ __global__ void __launch_bounds__(32 * kRowsWarps) nl_rows_kernel(const NlArgs a
       p[r] = a.posq[S.off + min(l0 + r, S.n - 1)];
       if (l0 + r >= S.n) p[r].x = -1e30f;  // no row: never within reach of an atom
       cnt[r] = 0;
+    }
+    static_assert(kRowsPerWarp == 4, "rows are paired");
+    NlRows4 P;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      P.x[h] = make_float2(p[2 * h].x, p[2 * h + 1].x);
+      P.y[h] = make_float2(p[2 * h].y, p[2 * h + 1].y);
+      P.z[h] = make_float2(p[2 * h].z, p[2 * h + 1].z);
     }
     const int own = ib - S.blk_base;
     for (int j0 = 0; j0 < S.nblk; j0 += kMaxJList) {
@@ -151,8 +178,8 @@ __global__ void __launch_bounds__(32 * kRowsWarps) nl_rows_kernel(const NlArgs a
           const int lj = jb * 32 + lane;
           float4 q = a.posq[S.off + min(lj, S.n - 1)];
           if (lj >= S.n) q.x = 1e30f;  // no atom: never within reach of a row
-          if (jb == own) nl_rows_block<true>(a, S, p, q, lj, l0, below, cnt);  // skips i = j
-          else nl_rows_block<false>(a, S, p, q, lj, l0, below, cnt);
+          if (jb == own) nl_rows_block<true>(a, S, P, q, lj, l0, below, cnt);  // skips i = j
+          else nl_rows_block<false>(a, S, P, q, lj, l0, below, cnt);
         }
       }
     }
