@@ -699,11 +699,11 @@ def main():
         "e2e": e2e,
         "cpu_baseline": cpu,
         "cpu_baseline_numpy": cpu_numpy,
-        # per timed step: step, bbox, born, finalize, force, chain, bonded, finish
         # per timed step (a one-step graph): the step kernel (with the block
-        # boxes), the descreening (with the Born radii), force and chain (with
-        # the bonded terms) passes, and the closing half kick
-        "gpu_launches": int(args.steps * 5),
+        # boxes), the descreening, force and chain passes, the Born finalize
+        # and the bonded terms unless fused into those passes, and the
+        # closing half kick of the one-step run
+        "gpu_launches": int(args.steps * (5 + (0 if batch_fusion & 1 else 1) + (0 if batch_fusion & 2 else 1))),
     }
     print(json.dumps(line), flush=True)
   if pg:

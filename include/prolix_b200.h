@@ -439,6 +439,13 @@ int pb2_get_tile_segment(const pb2_batch *batch, int32_t *segment);
  * batched_simulate.py:1125-1163). */
 int pb2_retire_system(pb2_batch *batch, int32_t sys, void *stream);
 
+/* Test hook for the bounded device waits: raises the number of descreening
+ * items the fused Born finalize of system `sys` waits for by `hold` (0
+ * restores it), so that its wait runs out (about a second) and the system
+ * is flagged with PB2_STATUS_WAIT_TIMEOUT while the other systems' results
+ * stay exact.  Not for a batch with a pair list.  Waits for the device. */
+int pb2_test_hold_system(pb2_batch *batch, int32_t sys, int32_t hold);
+
 /* Block shape of a pair pass (pass 0 descreening, 1 force, 2 chain rule):
  * threads per block and the resident blocks per SM its registers are sized
  * for.  Each pass is compiled for a few shapes: pb2_block_shapes fills up to

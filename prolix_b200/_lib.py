@@ -132,6 +132,7 @@ SIGNATURES = [
     ("pb2_set_tile_segment", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     ("pb2_get_tile_segment", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]),
     ("pb2_retire_system", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]),
+    ("pb2_test_hold_system", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32]),
     ("pb2_block_shapes", ctypes.c_int, [ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32]),
     ("pb2_set_block_shape", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
     ("pb2_get_block_shape", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),

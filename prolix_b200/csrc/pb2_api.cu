@@ -292,6 +292,7 @@ static int setup_items2(pb2_batch *b, int seg) {
     CUDA_TRY(ctx, cudaMemset(b->sys_fin, 0, b->n_sys * sizeof(int32_t)));
   }
   CUDA_TRY(ctx, cudaMemcpy(b->sys_items, per_sys.data(), per_sys.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  b->sys_items_host = per_sys;
   for (int p = 0; p < 3; ++p) set_pair_grid(b, p);
   return PB2_OK;
 }
@@ -1850,6 +1851,18 @@ extern "C" int pb2_retire_system(pb2_batch *b, int32_t sys, void *stream) {
   b->retired_host[sys] = 1;
   CUDA_TRY(ctx, launch_retire(sys, b->retired, b->items2_all, b->n_items2, b->items2, b->item_count,
                               b->pl_on ? b->pl_ctl : nullptr, (cudaStream_t)stream));
+  return PB2_OK;
+}
+
+extern "C" int pb2_test_hold_system(pb2_batch *b, int32_t sys, int32_t hold) {
+  if (!b) return PB2_EINVAL;
+  pb2_ctx *ctx = b->ctx;
+  if (sys < 0 || sys >= b->n_sys || hold < 0) return fail(ctx, PB2_EINVAL, "bad system or hold");
+  if (b->pl_on) return fail(ctx, PB2_EINVAL, "the pair list writes its own item counts");
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  CUDA_TRY(ctx, cudaDeviceSynchronize());
+  const int32_t v = b->sys_items_host[sys] + hold;
+  CUDA_TRY(ctx, cudaMemcpy(b->sys_items + sys, &v, sizeof v, cudaMemcpyHostToDevice));
   return PB2_OK;
 }
 

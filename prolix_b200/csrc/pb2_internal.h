@@ -108,6 +108,7 @@ struct pb2_batch {
   int8_t *retired = nullptr;       // per system: 1 = retired (pb2_retire_system)
   std::vector<int8_t> retired_host;
   int32_t *sys_items = nullptr;  // items2 per system (the descreening pass's completion count)
+  std::vector<int32_t> sys_items_host;
   int32_t *sys_done = nullptr;   // items of each system completed in the current pass
   int32_t *sys_fin = nullptr;    // finalize chunks of each system completed in the current pass
   int2 *excl_ent = nullptr;

@@ -123,21 +123,18 @@ __global__ void __launch_bounds__(32 * kRowsWarps) nl_rows_kernel(const NlArgs a
     const int s = a.blk_sys[ib];
     const SysInfo &S = a.sys[s];
     const int l0 = (ib - S.blk_base) * 32 + w * kRowsPerWarp;  // the warp's first row, local index
-    float4 p[kRowsPerWarp];
     int cnt[kRowsPerWarp];
-#pragma unroll
-    for (int r = 0; r < kRowsPerWarp; ++r) {
-      p[r] = a.posq[S.off + min(l0 + r, S.n - 1)];
-      if (l0 + r >= S.n) p[r].x = -1e30f;  // no row: never within reach of an atom
-      cnt[r] = 0;
-    }
     static_assert(kRowsPerWarp == 4, "rows are paired");
     NlRows4 P;
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      P.x[h] = make_float2(p[2 * h].x, p[2 * h + 1].x);
-      P.y[h] = make_float2(p[2 * h].y, p[2 * h + 1].y);
-      P.z[h] = make_float2(p[2 * h].z, p[2 * h + 1].z);
+      float4 u = a.posq[S.off + min(l0 + 2 * h, S.n - 1)], v = a.posq[S.off + min(l0 + 2 * h + 1, S.n - 1)];
+      if (l0 + 2 * h >= S.n) u.x = -1e30f;  // no row: never within reach of an atom
+      if (l0 + 2 * h + 1 >= S.n) v.x = -1e30f;
+      P.x[h] = make_float2(u.x, v.x);
+      P.y[h] = make_float2(u.y, v.y);
+      P.z[h] = make_float2(u.z, v.z);
+      cnt[2 * h] = cnt[2 * h + 1] = 0;
     }
     const int own = ib - S.blk_base;
     for (int j0 = 0; j0 < S.nblk; j0 += kMaxJList) {
@@ -167,9 +164,12 @@ __global__ void __launch_bounds__(32 * kRowsWarps) nl_rows_kernel(const NlArgs a
           const float4 lo = a.bbox[2 * gjb], hi = a.bbox[2 * gjb + 1];
 #pragma unroll
           for (int r = 0; r < kRowsPerWarp; ++r) {
-            const float dx = fmaxf(0.f, fmaxf(lo.x - p[r].x, p[r].x - hi.x));
-            const float dy = fmaxf(0.f, fmaxf(lo.y - p[r].y, p[r].y - hi.y));
-            const float dz = fmaxf(0.f, fmaxf(lo.z - p[r].z, p[r].z - hi.z));
+            const float px = r & 1 ? P.x[r >> 1].y : P.x[r >> 1].x;
+            const float py = r & 1 ? P.y[r >> 1].y : P.y[r >> 1].x;
+            const float pz = r & 1 ? P.z[r >> 1].y : P.z[r >> 1].x;
+            const float dx = fmaxf(0.f, fmaxf(lo.x - px, px - hi.x));
+            const float dy = fmaxf(0.f, fmaxf(lo.y - py, py - hi.y));
+            const float dz = fmaxf(0.f, fmaxf(lo.z - pz, pz - hi.z));
             near |= fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < a.reach2 * 1.0001f;
           }
         }

@@ -533,8 +533,9 @@ __device__ __forceinline__ void finalize_atom(const FinalizeArgs &a, int i, int 
   }
 }
 
-// Spins of the bounded waits (each after a 128 ns sleep): ~0.5 s at most.
-constexpr int kWaitSpins = 1 << 22;
+// Spins of the bounded waits (each a 128 ns sleep and an L2 read): about a
+// second at most; a wait for work in flight ends within one item (~0.1 ms).
+constexpr int kWaitSpins = 1 << 20;
 
 // Finalize chunk c (the batch's 32-atom block c) of the descreening pass:
 // wait until every item of its system has been counted, then turn the
@@ -560,9 +561,10 @@ __device__ __noinline__ void finalize_chunk(const PairArgs &a, int c, const int3
   }
   ok = __shfl_sync(kFull, ok, 0);
   __threadfence();  // acquire: the counted items' sums are visible to every lane
-  if (ok) {
-    const int l = (c - S.blk_base) * 32 + lane;
-    if (l < S.n) finalize_atom(a.fin, S.off + l, s, S);
+  const int l = (c - S.blk_base) * 32 + lane;
+  if (l < S.n) {
+    if (ok) finalize_atom(a.fin, S.off + l, s, S);
+    else a.fin.born_acc[S.off + l] = 0;  // the next evaluation starts from zero all the same
   }
   __syncwarp();
   if (lane == 0) {
