@@ -516,7 +516,8 @@ def main():
     tuned = {"segment": args.segment, "timings": None}  # block shapes and fusion: defaults
   else:
     tuned = autotune.tune(batch, candidates=(2, 4, 8, 16, 32), steps=3, use_cache=False)
-  batch_shapes = [batch.block_shape(p) for p in range(3)]
+  batch_shapes = [batch.block_shape(p) for p in range(4)]
+  batch_force_blocks = batch.force_blocks()
   batch_fusion = batch.fusion()
   for _ in range(args.warmup):  # also captures the one-step graph
     batch.langevin_run(1, stream)
@@ -684,7 +685,8 @@ def main():
                    "l2": "256 MB buffer written between timed steps",
                    "tile_segment": tuned["segment"],
                    "block_shapes": {p: list(batch_shapes[k]) for k, p in
-                                    enumerate(("born", "force", "chain"))},
+                                    enumerate(("born", "force", "chain", "force_four_blocks"))},
+                   "force_iblocks_per_warp": batch_force_blocks,
                    "fusion": {"bonded_in_chain": bool(batch_fusion & 1),
                               "born_finalize_in_descreening": bool(batch_fusion & 2)},
                    "autotune_ms_per_step": tuned["timings"]},

@@ -446,15 +446,24 @@ int pb2_retire_system(pb2_batch *batch, int32_t sys, void *stream);
  * stay exact.  Not for a batch with a pair list.  Waits for the device. */
 int pb2_test_hold_system(pb2_batch *batch, int32_t sys, int32_t hold);
 
-/* Block shape of a pair pass (pass 0 descreening, 1 force, 2 chain rule):
- * threads per block and the resident blocks per SM its registers are sized
- * for.  Each pass is compiled for a few shapes: pb2_block_shapes fills up to
- * capacity of them and returns how many there are; pb2_set_block_shape
- * picks one (PB2_EINVAL if not compiled) and drops captured graphs.  The
- * autotuner's other knob; no reference counterpart. */
+/* Block shape of a pair pass (pass 0 descreening, 1 force, 2 chain rule,
+ * 3 the force pass's four-block kernel): threads per block and the resident
+ * blocks per SM its registers are sized for.  Each pass is compiled for a
+ * few shapes: pb2_block_shapes fills up to capacity of them and returns how
+ * many there are; pb2_set_block_shape picks one (PB2_EINVAL if not
+ * compiled) and drops captured graphs.  The autotuner's other knob; no
+ * reference counterpart. */
 int pb2_block_shapes(int32_t pass, int32_t *threads, int32_t *min_blocks, int32_t capacity);
 int pb2_set_block_shape(pb2_batch *batch, int32_t pass, int32_t threads, int32_t min_blocks);
 int pb2_get_block_shape(const pb2_batch *batch, int32_t pass, int32_t *threads, int32_t *min_blocks);
+
+/* I-blocks per warp of the force pass: 2, or 4 (two packed pairs of
+ * i-blocks share every j atom's loads; used without a pair list, where the
+ * list's rows are pairs of i-blocks).  Both give the same forces and dE/dB
+ * bit for bit; setting it drops captured graphs.  No reference
+ * counterpart. */
+int pb2_set_force_blocks(pb2_batch *batch, int32_t blocks);
+int pb2_get_force_blocks(const pb2_batch *batch, int32_t *blocks);
 
 /* Which per-step work rides inside the pair passes instead of a launch of
  * its own (an MD step is then four launches: step, descreening, force,

@@ -137,6 +137,8 @@ SIGNATURES = [
     ("pb2_set_block_shape", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
     ("pb2_get_block_shape", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
                                            ctypes.POINTER(ctypes.c_int32)]),
+    ("pb2_set_force_blocks", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    ("pb2_get_force_blocks", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]),
     ("pb2_set_fusion", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     ("pb2_get_fusion", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]),
     ("pb2_set_profiling", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),

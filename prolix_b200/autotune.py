@@ -9,7 +9,8 @@ candidate (CUDA events on the launching stream; the fastest wins):
 * the block shape of each pair pass (threads per block, resident blocks
   per SM the registers are sized for), among the shapes compiled for it
   (``Batch.block_shapes``): more, smaller blocks against fewer registers
-  per thread.
+  per thread; and for the force pass, two or four i-blocks per warp (four
+  share each j atom's loads, at more registers), each with its shapes.
 * fusion (``_lib.FUSE_*``): the bonded terms as the chain pass's tail work,
   and each system's Born radii finalized by the descreening warp that
   completes it, against launches of their own.
@@ -100,6 +101,8 @@ def apply(batch, choice: dict):
   batch.set_tile_segment(int(choice["segment"]))
   for p, shape in enumerate(choice.get("shapes") or []):
     batch.set_block_shape(p, int(shape[0]), int(shape[1]))
+  if choice.get("force_blocks") is not None:
+    batch.set_force_blocks(int(choice["force_blocks"]))
   if choice.get("fusion") is not None:
     batch.set_fusion(int(choice["fusion"]))
 
@@ -112,7 +115,7 @@ def tune(batch, candidates=CANDIDATES, steps: int = 4, use_cache: bool = True,
   key = bucket_key(batch, _gpu_name())
   path = cache_path()
   data = _load(path) if use_cache else {}
-  if use_cache and key in data and "shapes" in data[key]:
+  if use_cache and key in data and "force_blocks" in data[key]:
     apply(batch, data[key])
     return {**data[key], "cached": True, "key": key}
   snap = batch.get_state()
@@ -122,7 +125,8 @@ def tune(batch, candidates=CANDIDATES, steps: int = 4, use_cache: bool = True,
   best_seg = min(candidates, key=lambda c: timings[f"segment={c}"])
   batch.set_tile_segment(int(best_seg))
   best_ms = timings[f"segment={best_seg}"]
-  chosen_shapes = [list(batch.block_shape(p)) for p in range(3)]
+  chosen_shapes = [list(batch.block_shape(p)) for p in range(4)]
+  chosen_blocks = batch.force_blocks()
   if shapes:
     for p in range(3):
       for t, m in batch.block_shapes(p):
@@ -135,6 +139,19 @@ def tune(batch, candidates=CANDIDATES, steps: int = 4, use_cache: bool = True,
           best_ms = ms
           chosen_shapes[p] = [t, m]
         batch.set_block_shape(p, *chosen_shapes[p])
+    # the force pass with four i-blocks per warp, in each of its shapes
+    # (without a pair list: with one, the force pass keeps two)
+    batch.set_force_blocks(4)
+    for t, m in batch.block_shapes(3):
+      batch.set_block_shape(3, t, m)
+      ms = _time(batch, steps)
+      timings[f"force4={t}x{m}"] = ms
+      if ms < best_ms:
+        best_ms = ms
+        chosen_shapes[3] = [t, m]
+        chosen_blocks = 4
+    batch.set_block_shape(3, *chosen_shapes[3])
+    batch.set_force_blocks(chosen_blocks)
   chosen_fusion = batch.fusion()
   if fusion:
     for f in range(4):
@@ -148,8 +165,8 @@ def tune(batch, candidates=CANDIDATES, steps: int = 4, use_cache: bool = True,
         chosen_fusion = f
       batch.set_fusion(chosen_fusion)
   batch.set_state(position=snap["position"], momentum=snap["momentum"], key=snap["key"])
-  result = {"segment": int(best_seg), "shapes": chosen_shapes, "fusion": int(chosen_fusion),
-            "ms": best_ms, "timings": timings}
+  result = {"segment": int(best_seg), "shapes": chosen_shapes, "force_blocks": int(chosen_blocks),
+            "fusion": int(chosen_fusion), "ms": best_ms, "timings": timings}
   if use_cache:
     data[key] = result
     _store(path, data)

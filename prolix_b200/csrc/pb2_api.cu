@@ -250,6 +250,29 @@ static std::vector<TileItem> build_items2(const std::vector<SysInfo> &sinfo, int
   return items;
 }
 
+// Work items of the four-block force kernel: i-blocks ib, ib % 4 == 0 (with
+// ib + 1 .. ib + 3), against j-blocks [j0, j1), j0 >= ib; sorted by cost.
+static std::vector<TileItem> build_items4(const std::vector<SysInfo> &sinfo, int seg) {
+  std::vector<TileItem> items;
+  for (int s = 0; s < (int)sinfo.size(); ++s) {
+    const int nblk = sinfo[s].nblk;
+    for (int ib = 0; ib < nblk; ib += 4)
+      for (int j0 = ib; j0 < nblk; j0 += seg) items.push_back(TileItem{s, ib, j0, std::min(j0 + seg, nblk)});
+  }
+  std::stable_sort(items.begin(), items.end(), [](const TileItem &p, const TileItem &q) {
+    return (p.jb1 - p.jb0) > (q.jb1 - q.jb0);
+  });
+  return items;
+}
+
+static void set_force4_grid(pb2_batch *b) {
+  const int cap = force4_occupancy(b->cut, b->shape4) * b->ctx->sm_count;
+  int t = 0, m = 0;
+  force4_shape(b->shape4, &t, &m);
+  const int w = t / 32;
+  b->grid4 = std::max(1, std::min(cap, (b->n_items4 + w - 1) / w));
+}
+
 // Grid of pair pass p for its block shape: one resident wave (warps take
 // items dynamically), no more warps than items.
 static void set_pair_grid(pb2_batch *b, int p) {
@@ -280,6 +303,19 @@ static int setup_items2(pb2_batch *b, int seg) {
     b->retired_host.assign(b->n_sys, 0);
   }
   CUDA_TRY(ctx, launch_retire(-1, b->retired, b->items2_all, b->n_items2, b->items2, b->item_count, nullptr, nullptr));
+  {
+    std::vector<TileItem> items4 = build_items4(b->sys_host, seg);
+    b->dev.release(b->items4);
+    b->dev.release(b->items4_all);
+    b->items4 = b->dev.alloc<TileItem>(std::max<size_t>(items4.size(), 1));
+    b->items4_all = b->dev.alloc<TileItem>(std::max<size_t>(items4.size(), 1));
+    if (!b->item_count4) b->item_count4 = b->dev.alloc<int32_t>(1);
+    if (!b->items4 || !b->items4_all || !b->item_count4) return fail(ctx, PB2_ENOMEM, "work-item allocation failed");
+    if (!items4.empty())
+      CUDA_TRY(ctx, cudaMemcpy(b->items4_all, items4.data(), items4.size() * sizeof(TileItem), cudaMemcpyHostToDevice));
+    b->n_items4 = (int)items4.size();
+    CUDA_TRY(ctx, launch_retire(-1, b->retired, b->items4_all, b->n_items4, b->items4, b->item_count4, nullptr, nullptr));
+  }
   CUDA_TRY(ctx, cudaDeviceSynchronize());
   std::vector<int32_t> per_sys(b->n_sys, 0);
   for (const TileItem &t : items) ++per_sys[t.sys];
@@ -294,6 +330,7 @@ static int setup_items2(pb2_batch *b, int seg) {
   CUDA_TRY(ctx, cudaMemcpy(b->sys_items, per_sys.data(), per_sys.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
   b->sys_items_host = per_sys;
   for (int p = 0; p < 3; ++p) set_pair_grid(b, p);
+  set_force4_grid(b);
   return PB2_OK;
 }
 
@@ -966,8 +1003,17 @@ static cudaError_t enqueue_forces(pb2_batch *b, cudaStream_t st, bool bonded_ene
       return e;
   }
   pa.sched = b->sched + 2 * PASS_FORCE;
-  if ((e = tm(kTimForce, [&] { return launch_tiles(PASS_FORCE, pa, b->grid_pair[PASS_FORCE], b->shape[PASS_FORCE], st); })) != cudaSuccess)
+  if (b->force_blocks == 4 && !b->pl_on) {
+    PairArgs p4 = pa;
+    p4.items = b->items4;
+    p4.n_items = b->n_items4;
+    p4.item_count = b->item_count4;
+    if ((e = tm(kTimForce, [&] { return launch_force4(p4, b->grid4, b->shape4, st); })) != cudaSuccess) return e;
+  } else if ((e = tm(kTimForce, [&] {
+                return launch_tiles(PASS_FORCE, pa, b->grid_pair[PASS_FORCE], b->shape[PASS_FORCE], st);
+              })) != cudaSuccess) {
     return e;
+  }
   pa.sched = b->sched + 2 * PASS_CHAIN;
   BondedArgs ba = b->bonded;
   ba.energy_mode = bonded_energy ? 1 : 0;
@@ -1851,6 +1897,8 @@ extern "C" int pb2_retire_system(pb2_batch *b, int32_t sys, void *stream) {
   b->retired_host[sys] = 1;
   CUDA_TRY(ctx, launch_retire(sys, b->retired, b->items2_all, b->n_items2, b->items2, b->item_count,
                               b->pl_on ? b->pl_ctl : nullptr, (cudaStream_t)stream));
+  CUDA_TRY(ctx, launch_retire(-1, b->retired, b->items4_all, b->n_items4, b->items4, b->item_count4, nullptr,
+                              (cudaStream_t)stream));
   return PB2_OK;
 }
 
@@ -1872,11 +1920,16 @@ extern "C" int pb2_get_tile_segment(const pb2_batch *b, int32_t *segment) {
   return PB2_OK;
 }
 
+static void any_shape(int pass, int k, int *t, int *m) {
+  if (pass == 3) force4_shape(k, t, m);
+  else tile_shape(pass, k, t, m);
+}
+
 extern "C" int pb2_block_shapes(int32_t pass, int32_t *threads, int32_t *min_blocks, int32_t capacity) {
-  if (pass < 0 || pass > 2) return PB2_EINVAL;
+  if (pass < 0 || pass > 3) return PB2_EINVAL;
   for (int k = 0; k < kShapesPerPass && k < capacity; ++k) {
     int t = 0, m = 0;
-    tile_shape(pass, k, &t, &m);
+    any_shape(pass, k, &t, &m);
     if (threads) threads[k] = t;
     if (min_blocks) min_blocks[k] = m;
   }
@@ -1884,20 +1937,25 @@ extern "C" int pb2_block_shapes(int32_t pass, int32_t *threads, int32_t *min_blo
 }
 
 extern "C" int pb2_set_block_shape(pb2_batch *b, int32_t pass, int32_t threads, int32_t min_blocks) {
-  if (!b || pass < 0 || pass > 2) return PB2_EINVAL;
+  if (!b || pass < 0 || pass > 3) return PB2_EINVAL;
   pb2_ctx *ctx = b->ctx;
   int found = -1;
   for (int k = 0; k < kShapesPerPass; ++k) {
     int t = 0, m = 0;
-    tile_shape(pass, k, &t, &m);
+    any_shape(pass, k, &t, &m);
     if (t == threads && m == min_blocks) found = k;
   }
   if (found < 0) return fail(ctx, PB2_EINVAL, "block shape not compiled for this pass (see pb2_block_shapes)");
-  if (found == b->shape[pass]) return PB2_OK;
+  if (found == (pass == 3 ? b->shape4 : b->shape[pass])) return PB2_OK;
   CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   CUDA_TRY(ctx, cudaDeviceSynchronize());
-  b->shape[pass] = found;
-  set_pair_grid(b, pass);
+  if (pass == 3) {
+    b->shape4 = found;
+    set_force4_grid(b);
+  } else {
+    b->shape[pass] = found;
+    set_pair_grid(b, pass);
+  }
   for (auto &kv : b->graphs) cudaGraphExecDestroy(kv.second);  // they captured the old kernel
   b->graphs.clear();
   for (auto &kv : b->min_graphs) cudaGraphExecDestroy(kv.second);
@@ -1906,11 +1964,30 @@ extern "C" int pb2_set_block_shape(pb2_batch *b, int32_t pass, int32_t threads, 
 }
 
 extern "C" int pb2_get_block_shape(const pb2_batch *b, int32_t pass, int32_t *threads, int32_t *min_blocks) {
-  if (!b || pass < 0 || pass > 2 || !threads || !min_blocks) return PB2_EINVAL;
+  if (!b || pass < 0 || pass > 3 || !threads || !min_blocks) return PB2_EINVAL;
   int t = 0, m = 0;
-  tile_shape(pass, b->shape[pass], &t, &m);
+  any_shape(pass, pass == 3 ? b->shape4 : b->shape[pass], &t, &m);
   *threads = t;
   *min_blocks = m;
+  return PB2_OK;
+}
+
+extern "C" int pb2_set_force_blocks(pb2_batch *b, int32_t blocks) {
+  if (!b || (blocks != 2 && blocks != 4)) return PB2_EINVAL;
+  if (blocks == b->force_blocks) return PB2_OK;
+  CUDA_TRY(b->ctx, cudaSetDevice(b->ctx->device));
+  CUDA_TRY(b->ctx, cudaDeviceSynchronize());
+  b->force_blocks = blocks;
+  for (auto &kv : b->graphs) cudaGraphExecDestroy(kv.second);  // they captured the other kernel
+  b->graphs.clear();
+  for (auto &kv : b->min_graphs) cudaGraphExecDestroy(kv.second);
+  b->min_graphs.clear();
+  return PB2_OK;
+}
+
+extern "C" int pb2_get_force_blocks(const pb2_batch *b, int32_t *blocks) {
+  if (!b || !blocks) return PB2_EINVAL;
+  *blocks = b->force_blocks;
   return PB2_OK;
 }
 

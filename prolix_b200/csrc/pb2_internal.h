@@ -105,6 +105,12 @@ struct pb2_batch {
   TileItem *items2_all = nullptr;  // every system's items over pairs of i-blocks
   int n_items2 = 0;                // items in items2_all
   int32_t *item_count = nullptr;   // items in items2 (device)
+  // the four-block force kernel's items (i-blocks ib % 4 == 0): all, live, counts
+  TileItem *items4_all = nullptr, *items4 = nullptr;
+  int n_items4 = 0;
+  int32_t *item_count4 = nullptr;
+  int force_blocks = 2;  // i-blocks per warp of the force pass (2 or 4; 4 only without a pair list)
+  int shape4 = 0, grid4 = 1;
   int8_t *retired = nullptr;       // per system: 1 = retired (pb2_retire_system)
   std::vector<int8_t> retired_host;
   int32_t *sys_items = nullptr;  // items2 per system (the descreening pass's completion count)

@@ -255,6 +255,11 @@ cudaError_t launch_pl_update(const PlArgs &a, int grid, cudaStream_t st);
 // in their order, into live and *count (one thread block).  With sys >= 0,
 // that system is retired first (and a pair list, if any, is marked for a
 // rebuild without it).
+// The force pass with four i-blocks per warp (items with iblk % 4 == 0);
+// the same sums as launch_tiles(PASS_FORCE) bit for bit.
+cudaError_t launch_force4(const PairArgs &a, int grid, int shape, cudaStream_t st);
+int force4_occupancy(bool cut, int shape);
+int force4_shape(int shape, int *threads, int *min_blocks);
 cudaError_t launch_retire(int32_t sys, int8_t *retired, const TileItem *all, int n_all, TileItem *live,
                           int32_t *count, int32_t *pl_ctl, cudaStream_t st);
 cudaError_t launch_bonded(const BondedArgs &a, int grid_cap, cudaStream_t st);

@@ -210,80 +210,119 @@ struct Acc2F {
   float2 a0, a1, a2, a3;
 };
 
+// The masks of one packed pair of i-blocks (bit-reversed, tested through
+// the sign bit and shifted once per step): pair validity, exclusion, 1-4.
+struct ForceMasks {
+  uint32_t R0, R1, X0, X1, Q0, Q1;
+};
+__device__ __forceinline__ ForceMasks force_masks(uint32_t V0, uint32_t V1, uint32_t E0, uint32_t E1, uint32_t S0,
+                                                  uint32_t S1) {
+  return ForceMasks{__brev(V0), __brev(V1), __brev(E0), __brev(E1), __brev(S0), __brev(S1)};
+}
+
+// One step of one packed pair of i-blocks against the j atom J: the i-side
+// sums into ti, the j-side sums into tj (not rotated here).  Both the
+// two-block and the four-block force kernels step through this function,
+// so their sums are the same bit for bit.
+template <bool CUT, bool FULL, bool EXCL>
+__device__ __forceinline__ void force_pair_step(const FData2 &I, const JF2 &J, Acc2F &ti, Acc &tj, ForceMasks &M,
+                                                const TileConst &K) {
+  const float2 dx = __fadd2_rn(I.x, J.mx);
+  const float2 dy = __fadd2_rn(I.y, J.my);
+  const float2 dz = __fadd2_rn(I.z, J.mz);
+  float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+  if (!FULL) {
+    r2 = make_float2((int32_t)M.R0 < 0 ? r2.x : kFarR2, (int32_t)M.R1 < 0 ? r2.y : kFarR2);
+    M.R0 <<= 1;
+    M.R1 <<= 1;
+  }
+  float2 g = make_float2(0.f, 0.f);
+  if (K.use_gb) {
+    // E = P qq / f, f^2 = r^2 + B_i B_j e^(-r^2 / 4 B_i B_j); with
+    // A2 = 2 P qq / f^3:  -dE/dr / r = A2 (1 - e / 4), and
+    // dE/dB_i = -(A2 e / 2) (B_i B_j + r^2 / 4) / B_i, whose numerator is
+    // the same for both atoms: h = A2 e (B_i B_j + r^2 / 4) is summed for
+    // both, and each sum is scaled by -1 / (2 B) when it is flushed
+    const float2 w = __fmul2_rn(r2, __fmul2_rn(I.iB, J.iB));  // r^2 log2(e) / (4 B_i B_j)
+    const float2 ex = make_float2(exp2f(-w.x), exp2f(-w.y));
+    const float2 bb = __fmul2_rn(I.B, J.B);
+    const float2 f2 = __ffma2_rn(bb, ex, r2);
+    const float2 inv_f = make_float2(rsqrtf(f2.x), rsqrtf(f2.y));
+    float2 A2 = __fmul2_rn(__fmul2_rn(I.q2p, J.q), __fmul2_rn(__fmul2_rn(inv_f, inv_f), inv_f));
+    if (CUT && K.gcut2 != 0.f) A2 = __fmul2_rn(A2, sel2(r2.x < K.gcut2, r2.y < K.gcut2, 1.f, 0.f));
+    const float2 A2e = __fmul2_rn(A2, ex);
+    g = __ffma2_rn(dup2(-0.25f), A2e, A2);
+    const float2 h = __fmul2_rn(A2e, __ffma2_rn(r2, dup2(0.25f), bb));
+    ti.a3 = __fadd2_rn(ti.a3, h);
+    tj.a3 = tj.a3 + h.x + h.y;
+  }
+  if (K.use_lj || K.use_coul) {
+    const float2 inv_r = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+    const float2 inv_r2 = __fmul2_rn(inv_r, inv_r);
+    float2 sc_c = dup2(1.f), sc_l = dup2(1.f);  // exclusion and 1-4 factors
+    if (EXCL) {
+      const bool x0 = (int32_t)M.X0 < 0, x1 = (int32_t)M.X1 < 0, q0 = (int32_t)M.Q0 < 0, q1 = (int32_t)M.Q1 < 0;
+      sc_c = make_float2(x0 ? 0.f : (q0 ? K.coul14 : 1.f), x1 ? 0.f : (q1 ? K.coul14 : 1.f));
+      sc_l = make_float2(x0 ? 0.f : (q0 ? K.lj14 : 1.f), x1 ? 0.f : (q1 ? K.lj14 : 1.f));
+      M.X0 <<= 1; M.X1 <<= 1; M.Q0 <<= 1; M.Q1 <<= 1;
+    }
+    float2 s = make_float2(0.f, 0.f);  // (-dE/dr) r for Coulomb and LJ
+    if (K.use_coul) {
+      s = __fmul2_rn(__fmul2_rn(I.qk, J.q), inv_r);
+      if (EXCL) s = __fmul2_rn(s, sc_c);
+    }
+    if (K.use_lj) {
+      const float2 sig = __fadd2_rn(I.hs, J.hs);
+      const float2 sr2 = __fmul2_rn(__fmul2_rn(sig, sig), inv_r2);
+      const float2 s6 = __fmul2_rn(__fmul2_rn(sr2, sr2), sr2);
+      float2 eps24 = __fmul2_rn(I.se, J.se);  // se = sqrt(24 eps)
+      if (EXCL) eps24 = __fmul2_rn(eps24, sc_l);
+      s = __ffma2_rn(__fmul2_rn(eps24, s6), __ffma2_rn(dup2(2.0f), s6, dup2(-1.0f)), s);
+    }
+    if (CUT && K.cut2 != 0.f) s = __fmul2_rn(s, sel2(r2.x < K.cut2, r2.y < K.cut2, 1.f, 0.f));
+    g = __ffma2_rn(s, inv_r2, g);
+  }
+  ti.a0 = __ffma2_rn(g, dx, ti.a0);
+  ti.a1 = __ffma2_rn(g, dy, ti.a1);
+  ti.a2 = __ffma2_rn(g, dz, ti.a2);
+  tj.a0 = fmaf(-g.x, dx.x, fmaf(-g.y, dx.y, tj.a0));
+  tj.a1 = fmaf(-g.x, dy.x, fmaf(-g.y, dy.y, tj.a1));
+  tj.a2 = fmaf(-g.x, dz.x, fmaf(-g.y, dz.y, tj.a2));
+}
+
+__device__ __forceinline__ void rotate_force(Acc &tj, int src, const TileConst &K) {
+  tj.a0 = shfl_next(tj.a0, src);
+  rotate_force_rest(tj, src, K);
+}
+
 template <bool CUT, bool FULL, bool EXCL>
 __device__ __forceinline__ void run_force_tile2(const FData2 &I, const JTile &jt, Acc2F &ti, Acc &tj, uint32_t V0,
                                                 uint32_t V1, uint32_t E0, uint32_t E1, uint32_t S0,
                                                 uint32_t S1, const TileConst &K) {
-  const int src = K.src;
   // step k tests the sign bits of the bit-reversed masks shifted left k times
-  uint32_t R0 = __brev(V0), R1 = __brev(V1);
-  uint32_t X0 = __brev(E0), X1 = __brev(E1), Q0 = __brev(S0), Q1 = __brev(S1);
+  ForceMasks M = force_masks(V0, V1, E0, E1, S0, S1);
 #pragma unroll kUnroll
   for (int k = 0; k < 32; ++k) {
     const JF2 J = load_jf(jt, K.lane + k);  // lane l meets j-lane (l + k) mod 32
-    const float2 dx = __fadd2_rn(I.x, J.mx);
-    const float2 dy = __fadd2_rn(I.y, J.my);
-    const float2 dz = __fadd2_rn(I.z, J.mz);
-    float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
-    if (!FULL) {
-      r2 = make_float2((int32_t)R0 < 0 ? r2.x : kFarR2, (int32_t)R1 < 0 ? r2.y : kFarR2);
-      R0 <<= 1;
-      R1 <<= 1;
-    }
-    float2 g = make_float2(0.f, 0.f);
-    if (K.use_gb) {
-      // E = P qq / f, f^2 = r^2 + B_i B_j e^(-r^2 / 4 B_i B_j); with
-      // A2 = 2 P qq / f^3:  -dE/dr / r = A2 (1 - e / 4), and
-      // dE/dB_i = -(A2 e / 2) (B_i B_j + r^2 / 4) / B_i, whose numerator is
-      // the same for both atoms: h = A2 e (B_i B_j + r^2 / 4) is summed for
-      // both, and each sum is scaled by -1 / (2 B) when it is flushed
-      const float2 w = __fmul2_rn(r2, __fmul2_rn(I.iB, J.iB));  // r^2 log2(e) / (4 B_i B_j)
-      const float2 ex = make_float2(exp2f(-w.x), exp2f(-w.y));
-      const float2 bb = __fmul2_rn(I.B, J.B);
-      const float2 f2 = __ffma2_rn(bb, ex, r2);
-      const float2 inv_f = make_float2(rsqrtf(f2.x), rsqrtf(f2.y));
-      float2 A2 = __fmul2_rn(__fmul2_rn(I.q2p, J.q), __fmul2_rn(__fmul2_rn(inv_f, inv_f), inv_f));
-      if (CUT && K.gcut2 != 0.f) A2 = __fmul2_rn(A2, sel2(r2.x < K.gcut2, r2.y < K.gcut2, 1.f, 0.f));
-      const float2 A2e = __fmul2_rn(A2, ex);
-      g = __ffma2_rn(dup2(-0.25f), A2e, A2);
-      const float2 h = __fmul2_rn(A2e, __ffma2_rn(r2, dup2(0.25f), bb));
-      ti.a3 = __fadd2_rn(ti.a3, h);
-      tj.a3 = tj.a3 + h.x + h.y;
-    }
-    if (K.use_lj || K.use_coul) {
-      const float2 inv_r = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
-      const float2 inv_r2 = __fmul2_rn(inv_r, inv_r);
-      float2 sc_c = dup2(1.f), sc_l = dup2(1.f);  // exclusion and 1-4 factors
-      if (EXCL) {
-        const bool x0 = (int32_t)X0 < 0, x1 = (int32_t)X1 < 0, q0 = (int32_t)Q0 < 0, q1 = (int32_t)Q1 < 0;
-        sc_c = make_float2(x0 ? 0.f : (q0 ? K.coul14 : 1.f), x1 ? 0.f : (q1 ? K.coul14 : 1.f));
-        sc_l = make_float2(x0 ? 0.f : (q0 ? K.lj14 : 1.f), x1 ? 0.f : (q1 ? K.lj14 : 1.f));
-        X0 <<= 1; X1 <<= 1; Q0 <<= 1; Q1 <<= 1;
-      }
-      float2 s = make_float2(0.f, 0.f);  // (-dE/dr) r for Coulomb and LJ
-      if (K.use_coul) {
-        s = __fmul2_rn(__fmul2_rn(I.qk, J.q), inv_r);
-        if (EXCL) s = __fmul2_rn(s, sc_c);
-      }
-      if (K.use_lj) {
-        const float2 sig = __fadd2_rn(I.hs, J.hs);
-        const float2 sr2 = __fmul2_rn(__fmul2_rn(sig, sig), inv_r2);
-        const float2 s6 = __fmul2_rn(__fmul2_rn(sr2, sr2), sr2);
-        float2 eps24 = __fmul2_rn(I.se, J.se);  // se = sqrt(24 eps)
-        if (EXCL) eps24 = __fmul2_rn(eps24, sc_l);
-        s = __ffma2_rn(__fmul2_rn(eps24, s6), __ffma2_rn(dup2(2.0f), s6, dup2(-1.0f)), s);
-      }
-      if (CUT && K.cut2 != 0.f) s = __fmul2_rn(s, sel2(r2.x < K.cut2, r2.y < K.cut2, 1.f, 0.f));
-      g = __ffma2_rn(s, inv_r2, g);
-    }
-    ti.a0 = __ffma2_rn(g, dx, ti.a0);
-    ti.a1 = __ffma2_rn(g, dy, ti.a1);
-    ti.a2 = __ffma2_rn(g, dz, ti.a2);
-    tj.a0 = fmaf(-g.x, dx.x, fmaf(-g.y, dx.y, tj.a0));
-    tj.a1 = fmaf(-g.x, dy.x, fmaf(-g.y, dy.y, tj.a1));
-    tj.a2 = fmaf(-g.x, dz.x, fmaf(-g.y, dz.y, tj.a2));
-    tj.a0 = shfl_next(tj.a0, src);
-    rotate_force_rest(tj, src, K);
+    force_pair_step<CUT, FULL, EXCL>(I, J, ti, tj, M, K);
+    rotate_force(tj, K.src, K);
+  }
+}
+
+// Four i-blocks: two packed pairs share each step's j atom (one set of
+// shared-memory loads for four pairs); each pair keeps its own j-side sums,
+// so the sums are those of two two-block tiles.
+template <bool CUT, bool FULL, bool EXCL>
+__device__ __forceinline__ void run_force_tile4(const FData2 &Ia, const FData2 &Ib, const JTile &jt, Acc2F &ta,
+                                                Acc2F &tb, Acc &tja, Acc &tjb, ForceMasks Ma, ForceMasks Mb,
+                                                const TileConst &K) {
+#pragma unroll 1
+  for (int k = 0; k < 32; ++k) {
+    const JF2 J = load_jf(jt, K.lane + k);
+    force_pair_step<CUT, FULL, EXCL>(Ia, J, ta, tja, Ma, K);
+    force_pair_step<CUT, FULL, EXCL>(Ib, J, tb, tjb, Mb, K);
+    rotate_force(tja, K.src, K);
+    rotate_force(tjb, K.src, K);
   }
 }
 
@@ -868,6 +907,180 @@ __global__ void __launch_bounds__(THREADS, MINB)
   }
 }
 
+// The force pass with four i-blocks per warp: work items (system, i-block
+// ib with ib % 4 == 0, j-blocks [jb0, jb1)); lane l owns atom l of blocks
+// ib .. ib + 3, in two packed pairs (ib, ib + 1) and (ib + 2, ib + 3) that
+// share every step's j atom.  Tiles below the diagonal (j-block before an
+// i-block) are masked to zero, and each pair's sums, masks and exclusions
+// are those of the two-block kernel's tile for the same blocks, so the
+// forces and dE/dB are the same bit for bit (j-side sums of the two pairs
+// are added in fixed point before their one atomic).
+template <bool CUT, bool ALL, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) force4_kernel(const __grid_constant__ PairArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+  TileConst K;
+  K.use_gb = ALL || (a.terms & PB2_USE_GB) != 0;
+  K.use_lj = ALL || (a.terms & PB2_USE_LJ) != 0;
+  K.use_coul = ALL || (a.terms & PB2_USE_COULOMB) != 0;
+  K.src = (lane + 1) & 31;
+  K.lane = lane;
+  constexpr int kWarps = THREADS / 32;
+  __shared__ JTile s_jt[kWarps];
+  __shared__ long long s_ps[kWarps][16][32];
+  JTile &jt = s_jt[threadIdx.x >> 5];
+  long long *ps = &s_ps[threadIdx.x >> 5][0][lane];
+  const uint32_t diag_mask = lane == 31 ? 0u : (0xffffffffu << (lane + 1));
+  const float bscale = (float)kForceScale;
+  const int n_items = a.item_count ? *a.item_count : a.n_items;
+  for (;;) {
+    int it = 0;
+    if (lane == 0) it = atomicAdd(&a.sched[0], 1);
+    it = __shfl_sync(kFull, it, 0);
+    if (it >= n_items) break;
+    const TileItem item = a.items[it];
+    const SysInfo &S = a.sys[item.sys];
+    const int n = S.n, off = S.off;
+    K.cut2 = S.cutoff2; K.gcut2 = S.gb_cutoff2; K.bcut2 = S.born_cut2;
+    K.pref = S.pref; K.kcoul = S.kcoul; K.lj14 = S.lj14; K.coul14 = S.coul14;
+    const int ib = item.iblk;
+    int gib[4], ig[4];
+    bool has[4], iv[4];
+    PData I[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      has[k] = ib + k < S.nblk;
+      gib[k] = S.blk_base + (has[k] ? ib + k : ib);
+      const int il = (ib + k) * 32 + lane;
+      iv[k] = il < n;  // false whenever !has[k]
+      ig[k] = off + (iv[k] ? il : n - 1);
+      load_pdata(a, ig[k], PASS_FORCE, K.use_gb, S.ro_max, I[k]);
+    }
+    const float reach2 = CUT ? ((K.gcut2 == 0.f || K.cut2 == 0.f) ? 0.f : fmaxf(K.gcut2, K.cut2)) : 0.f;
+    FData2 IF[2];
+    float rB[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) rB[k] = I[k].rB;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const PData &P0 = I[2 * h], &P1 = I[2 * h + 1];
+      IF[h] = {make_float2(P0.x, P1.x), make_float2(P0.y, P1.y), make_float2(P0.z, P1.z),
+               make_float2(P0.hs, P1.hs), make_float2(P0.se, P1.se),
+               make_float2(P0.B, P1.B), make_float2(P0.iB, P1.iB),
+               make_float2(2.f * K.pref * P0.q, 2.f * K.pref * P1.q),
+               make_float2(K.kcoul * P0.q, K.kcoul * P1.q)};
+    }
+    // exclusion entries: ent[h], lanes 0-15 for block ib + 2h, 16-31 for ib + 2h + 1
+    int2 ent[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      ent[h] = make_int2(-1, -1);
+      if (lane < kExclPerBlock) {
+        if (has[2 * h]) ent[h] = a.excl_ent[gib[2 * h] * kExclPerBlock + lane];
+      } else if (has[2 * h + 1]) {
+        ent[h] = a.excl_ent[gib[2 * h + 1] * kExclPerBlock + lane - kExclPerBlock];
+      }
+    }
+    // i-side fixed-point sums, (block, component) x lane, in shared memory
+    // (registers hold the two packed pairs' data and sums)
+#pragma unroll
+    for (int k = 0; k < 16; ++k) ps[32 * k] = 0;
+    for (int jb = item.jb0; jb < item.jb1; ++jb) {
+      const int gjb = S.blk_base + jb;
+      if (CUT && reach2 > 0.f) {
+        // smallest box separation over the blocks with a tile on or above the diagonal
+        float d2 = box_dist2(a.bbox, gib[0], gjb);
+#pragma unroll
+        for (int k = 1; k < 4; ++k)
+          if (has[k] && jb >= ib + k) d2 = fminf(d2, box_dist2(a.bbox, gib[k], gjb));
+        if (d2 >= reach2) continue;  // no pair within reach
+      }
+      const int jl0 = jb * 32;
+      const int jl = jl0 + lane;
+      const bool jvalid = jl < n;
+      const int jg = off + (jvalid ? jl : n - 1);
+      PData J;
+      load_pdata(a, jg, PASS_FORCE, K.use_gb, S.ro_max, J);
+      __syncwarp();  // every lane is done with the previous tile's j data
+      store_j<PASS_FORCE>(jt, lane, J);
+      __syncwarp();
+      const int nj = n - jl0;
+      const uint32_t jmask = nj >= 32 ? 0xffffffffu : ((1u << nj) - 1u);
+      uint32_t C[4], V[4];
+      bool all_full = true;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        C[k] = iv[k] ? jmask : 0u;
+        if (jb == ib + k) C[k] &= diag_mask;
+        else if (jb < ib + k) C[k] = 0u;  // below the diagonal: another tile's pairs
+        V[k] = rotr32(C[k], lane);
+        all_full = all_full && C[k] == 0xffffffffu;
+      }
+      const bool full = __all_sync(kFull, all_full);
+      uint32_t E[4] = {0u, 0u, 0u, 0u}, Sx[4] = {0u, 0u, 0u, 0u};
+      bool any_hit = false;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const unsigned hit = __ballot_sync(kFull, ent[h].x == jb);
+        const unsigned hit0 = hit & 0xffffu, hit1 = hit & 0xffff0000u;
+        if (hit0) {
+          const int roff = __shfl_sync(kFull, ent[h].y, __ffs(hit0) - 1);
+          const ExclRow r = a.excl_rows[roff + lane];
+          E[2 * h] = rotr32(r.excl, lane); Sx[2 * h] = rotr32(r.s14, lane);
+        }
+        if (hit1) {
+          const int roff = __shfl_sync(kFull, ent[h].y, __ffs(hit1) - 1);
+          const ExclRow r = a.excl_rows[roff + lane];
+          E[2 * h + 1] = rotr32(r.excl, lane); Sx[2 * h + 1] = rotr32(r.s14, lane);
+        }
+        any_hit = any_hit || hit != 0u;
+      }
+      const ForceMasks Ma = force_masks(V[0], V[1], E[0], E[1], Sx[0], Sx[1]);
+      const ForceMasks Mb = force_masks(V[2], V[3], E[2], E[3], Sx[2], Sx[3]);
+      Acc2F tf[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+        tf[h] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+      Acc tja = {0.f, 0.f, 0.f, 0.f}, tjb = {0.f, 0.f, 0.f, 0.f};
+      if (any_hit) run_force_tile4<CUT, false, true>(IF[0], IF[1], jt, tf[0], tf[1], tja, tjb, Ma, Mb, K);
+      else if (!full) run_force_tile4<CUT, false, false>(IF[0], IF[1], jt, tf[0], tf[1], tja, tjb, Ma, Mb, K);
+      else run_force_tile4<CUT, true, false>(IF[0], IF[1], jt, tf[0], tf[1], tja, tjb, Ma, Mb, K);
+
+      // j partials are back in their home lanes: both pairs' sums, added in
+      // fixed point, in one atomic per component
+      if (jvalid) {
+        atomic_add_fix(&a.fx[jg], to_fix_f(tja.a0, bscale) + to_fix_f(tjb.a0, bscale));
+        atomic_add_fix(&a.fy[jg], to_fix_f(tja.a1, bscale) + to_fix_f(tjb.a1, bscale));
+        atomic_add_fix(&a.fz[jg], to_fix_f(tja.a2, bscale) + to_fix_f(tjb.a2, bscale));
+        if (K.use_gb)
+          atomic_add_fix(&a.dedb_acc[jg], to_fix_f(tja.a3 * (-0.5f * J.rB), bscale) +
+                                              to_fix_f(tjb.a3 * (-0.5f * J.rB), bscale));
+      }
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        long long *p0 = ps + 32 * 4 * (2 * h), *p1 = ps + 32 * 4 * (2 * h + 1);
+        p0[0] += to_fix_f(tf[h].a0.x, bscale); p0[32] += to_fix_f(tf[h].a1.x, bscale);
+        p0[64] += to_fix_f(tf[h].a2.x, bscale); p0[96] += to_fix_f(tf[h].a3.x * (-0.5f * rB[2 * h]), bscale);
+        p1[0] += to_fix_f(tf[h].a0.y, bscale); p1[32] += to_fix_f(tf[h].a1.y, bscale);
+        p1[64] += to_fix_f(tf[h].a2.y, bscale); p1[96] += to_fix_f(tf[h].a3.y * (-0.5f * rB[2 * h + 1]), bscale);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (iv[k]) {
+        const long long *pk = ps + 32 * 4 * k;
+        atomic_add_fix(&a.fx[ig[k]], pk[0]); atomic_add_fix(&a.fy[ig[k]], pk[32]);
+        atomic_add_fix(&a.fz[ig[k]], pk[64]);
+        if (K.use_gb) atomic_add_fix(&a.dedb_acc[ig[k]], pk[96]);
+      }
+    }
+  }
+  if (lane == 0 && atomicAdd(&a.sched[1], 1) == nwarps - 1) {
+    a.sched[0] = 0;
+    a.sched[1] = 0;
+  }
+}
+
 // Per-block bounding boxes of the float32 positions: one warp per block.
 __global__ void bbox_kernel(const SysInfo *sys, const int32_t *blk_sys, const float4 *posq,
                             float4 *bbox, int n_blocks, const float4 *pl_ref, int32_t *pl_ctl) {
@@ -996,6 +1209,62 @@ static int occ_shaped(int shape) {
     case 2: return occ_one<PASS, CUT, ALL, 2>();
     default: return occ_one<PASS, CUT, ALL, 0>();
   }
+}
+
+// Four-block force kernel: its own block shapes (more registers per thread
+// for the four i atoms' data and sums).
+constexpr Shape kShapes4[kShapesPerPass] = {{128, 3}, {128, 2}, {64, 5}};
+
+template <bool CUT, bool ALL, int SH>
+static void launch_force4_one(const PairArgs &a, int grid, cudaStream_t st) {
+  constexpr Shape sh = kShapes4[SH];
+  force4_kernel<CUT, ALL, sh.threads, sh.minb><<<grid, sh.threads, 0, st>>>(a);
+}
+template <bool CUT, bool ALL>
+static void launch_force4_shaped(const PairArgs &a, int grid, int shape, cudaStream_t st) {
+  switch (shape) {
+    case 1: launch_force4_one<CUT, ALL, 1>(a, grid, st); break;
+    case 2: launch_force4_one<CUT, ALL, 2>(a, grid, st); break;
+    default: launch_force4_one<CUT, ALL, 0>(a, grid, st);
+  }
+}
+cudaError_t launch_force4(const PairArgs &a, int grid, int shape, cudaStream_t st) {
+  if (grid <= 0) return cudaSuccess;
+  const bool all = (a.terms & (PB2_USE_GB | PB2_USE_LJ | PB2_USE_COULOMB)) ==
+                   (PB2_USE_GB | PB2_USE_LJ | PB2_USE_COULOMB);
+  if (a.cut) {
+    if (all) launch_force4_shaped<true, true>(a, grid, shape, st);
+    else launch_force4_shaped<true, false>(a, grid, shape, st);
+  } else {
+    if (all) launch_force4_shaped<false, true>(a, grid, shape, st);
+    else launch_force4_shaped<false, false>(a, grid, shape, st);
+  }
+  return cudaGetLastError();
+}
+template <bool CUT, bool ALL, int SH>
+static int occ_force4_one() {
+  constexpr Shape sh = kShapes4[SH];
+  int blocks = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, force4_kernel<CUT, ALL, sh.threads, sh.minb>, sh.threads, 0);
+  return blocks;
+}
+template <bool CUT, bool ALL>
+static int occ_force4_shaped(int shape) {
+  switch (shape) {
+    case 1: return occ_force4_one<CUT, ALL, 1>();
+    case 2: return occ_force4_one<CUT, ALL, 2>();
+    default: return occ_force4_one<CUT, ALL, 0>();
+  }
+}
+int force4_occupancy(bool cut, int shape) {
+  return cut ? std::min(occ_force4_shaped<true, true>(shape), occ_force4_shaped<true, false>(shape))
+             : std::min(occ_force4_shaped<false, true>(shape), occ_force4_shaped<false, false>(shape));
+}
+int force4_shape(int shape, int *threads, int *min_blocks) {
+  if (shape < 0 || shape >= kShapesPerPass) return -1;
+  *threads = kShapes4[shape].threads;
+  *min_blocks = kShapes4[shape].minb;
+  return 0;
 }
 
 int tile_shape(int pass, int shape, int *threads, int *min_blocks) {

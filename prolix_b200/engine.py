@@ -536,7 +536,7 @@ class Batch:
   # ---------------------------------------------------------------- schedule
   def block_shapes(self, pass_: int) -> list:
     """(threads, min blocks per SM) compiled for pair pass 0 (descreening),
-    1 (force) or 2 (chain rule)."""
+    1 (force), 2 (chain rule) or 3 (the force pass's four-block kernel)."""
     t = (ctypes.c_int32 * 8)()
     m = (ctypes.c_int32 * 8)()
     n = self.lib.pb2_block_shapes(int(pass_), t, m, 8)
@@ -551,6 +551,15 @@ class Batch:
     t, m = ctypes.c_int32(0), ctypes.c_int32(0)
     self._check(self.lib.pb2_get_block_shape(self.handle, int(pass_), ctypes.byref(t), ctypes.byref(m)))
     return int(t.value), int(m.value)
+
+  def set_force_blocks(self, blocks: int):
+    """I-blocks per warp of the force pass, 2 or 4 (the same forces bit for bit)."""
+    self._check(self.lib.pb2_set_force_blocks(self.handle, int(blocks)))
+
+  def force_blocks(self) -> int:
+    v = ctypes.c_int32(0)
+    self._check(self.lib.pb2_get_force_blocks(self.handle, ctypes.byref(v)))
+    return int(v.value)
 
   def set_fusion(self, flags: int):
     """_lib.FUSE_* bits: the bonded terms in the chain pass, the Born-radius

@@ -15,14 +15,21 @@ class FakeBatch:
     self.state = {"position": np.arange(6.0).reshape(2, 3), "momentum": np.ones((2, 3)),
                   "key": np.array([[1, 2]], dtype=np.uint32)}
 
-    self.shapes = [(256, 3), (256, 2), (256, 2)]
+    self.shapes = [(256, 3), (256, 2), (256, 2), (128, 3)]
     self.fuse = 1
+    self.fblocks = 2
 
   def set_tile_segment(self, s):
     self.seg = s
 
   def block_shapes(self, p):
-    return [(256, 3), (128, 6)] if p == 0 else [(256, 2), (128, 4)]
+    return {0: [(256, 3), (128, 6)], 3: [(128, 3), (128, 2)]}.get(p, [(256, 2), (128, 4)])
+
+  def set_force_blocks(self, n):
+    self.fblocks = n
+
+  def force_blocks(self):
+    return self.fblocks
 
   def set_block_shape(self, p, t, m):
     self.shapes[p] = (t, m)
@@ -58,8 +65,10 @@ def test_tune_picks_fastest_and_caches(tmp_path, monkeypatch):
     # segment cost, minus a gain for a 128-thread force pass and for
     # fusion 3; everything else unchanged
     ms = cost[b.seg]
-    if b.shapes[1] == (128, 4):
+    if b.fblocks == 2 and b.shapes[1] == (128, 4):
       ms -= 0.2
+    if b.fblocks == 4:
+      ms -= 0.3 if b.shapes[3] == (128, 2) else 0.1
     if b.fuse == 3:
       ms -= 0.1
     return ms
@@ -70,9 +79,11 @@ def test_tune_picks_fastest_and_caches(tmp_path, monkeypatch):
   fb = FakeBatch([100, 200])
   r = autotune.tune(fb, candidates=(2, 4, 8))
   assert r["segment"] == 4 and fb.seg == 4 and not r["cached"]
-  assert r["shapes"] == [[256, 3], [128, 4], [256, 2]] and fb.shapes[1] == (128, 4)
+  # four i-blocks in the force pass at 128x2 (-0.3) beats two at 128x4 (-0.2)
+  assert r["shapes"] == [[256, 3], [128, 4], [256, 2], [128, 2]] and fb.shapes[3] == (128, 2)
+  assert r["force_blocks"] == 4 and fb.fblocks == 4
   assert r["fusion"] == 3 and fb.fuse == 3
-  assert abs(r["ms"] - 1.2) < 1e-12
+  assert abs(r["ms"] - 1.1) < 1e-12
   fb2 = FakeBatch([100, 200])
   r2 = autotune.tune(fb2, candidates=(2, 4, 8))
-  assert r2["cached"] and fb2.seg == 4 and fb2.shapes[1] == (128, 4) and fb2.fuse == 3
+  assert r2["cached"] and fb2.seg == 4 and fb2.shapes[3] == (128, 2) and fb2.fblocks == 4 and fb2.fuse == 3

@@ -38,6 +38,13 @@ def test_block_shapes_and_fusion_leave_results_bitwise_equal():
         b.set_block_shape(p, t, m)
         assert b.block_shape(p) == (t, m)
         np.testing.assert_array_equal(b.forces(), ref)
+  with engine.Batch(systems) as b:
+    b.set_force_blocks(4)
+    assert b.force_blocks() == 4
+    for t, m in b.block_shapes(3):
+      b.set_block_shape(3, t, m)
+      assert b.block_shape(3) == (t, m)
+      np.testing.assert_array_equal(b.forces(), ref)
   for f in range(4):
     with engine.Batch(systems) as b:
       b.set_fusion(f)
@@ -70,3 +77,23 @@ def test_tune_restores_state_and_caches(tmp_path, monkeypatch):
       np.testing.assert_array_equal(before[k], after[k])
     res2 = autotune.tune(b, candidates=(2, 8), steps=2)
     assert res2["cached"] and res2["segment"] == res["segment"]
+
+
+@pytest.mark.parametrize("cutoff", [0.0, 9.0])
+def test_four_block_force_kernel_equals_the_two_block_one(cutoff):
+  # ragged sizes (a system of one block, partial blocks, i-block counts not
+  # multiples of 4), exclusions and 1-4 pairs, with and without a cutoff
+  # (no pair list, so the four-block kernel runs): forces and trajectories
+  # are the same bit for bit
+  systems = [synth.make_chain(n, 40 + k, compact=True) for k, n in enumerate([20, 97, 130, 260, 1000])]
+  out = {}
+  for blocks in (2, 4):
+    with engine.Batch(systems, cutoff=cutoff, pair_list=False) as b:
+      b.set_force_blocks(blocks)
+      f = b.forces()
+      b.langevin_init()
+      b.langevin_run(5)
+      out[blocks] = (f, b.get_state(fields=("position", "momentum")))
+  np.testing.assert_array_equal(out[2][0], out[4][0])
+  for k in ("position", "momentum"):
+    np.testing.assert_array_equal(out[2][1][k], out[4][1][k])
