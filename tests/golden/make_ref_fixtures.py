@@ -29,6 +29,9 @@ makes each value:
 * GB polar and Born radii: ``compute_gb_energy`` with the dense
   ``1 - eye`` mask that make_energy_fn passes (system.py:196-207); ACE:
   ``compute_ace_nonpolar_energy`` (generalized_born.py:600-648);
+* the NL-Born + dense-GB split: ``compute_born_radii_neighbor_list`` and the
+  forward of ``gb_energy_split_vjp`` (generalized_born.py:266-337, :706-770)
+  with the rows of every pair within the Born cutoff;
 * the remaining forces (GB + ACE, and the bonded terms together) by a
   fourth-order central difference of those reference energies,
   h = 1e-4 A.  The difference is checked below against the reference's
@@ -196,37 +199,77 @@ def _init_worker(kind, payload):
   _CASE = _build_case(kind, payload)
 
 
+class _JaxGather(np.ndarray):
+  """An array whose integer-array indexing clamps out-of-range indices to
+  the last row, as a JAX gather does (the reference's NL functions index
+  positions with rows padded by N and mask those entries afterwards)."""
+
+  def __getitem__(self, idx):
+    if isinstance(idx, np.ndarray) and idx.dtype.kind in "iu":
+      idx = np.clip(idx, 0, self.shape[0] - 1)
+    return np.asarray(np.ndarray.__getitem__(self, idx))
+
+
+class SplitCase:
+  """The NL-Born + dense-GB split: ``gb_energy_split_vjp``'s forward
+  (NL Born radii, then the dense GB sum) plus ACE on the same radii."""
+
+  def __init__(self):
+    s, _ = ref_cases.case_system(ref_cases.SPLIT_BASE)
+    self.s = s
+    r = np.asarray(s["positions"], np.float64)
+    self.cutoff = ref_cases.split_cutoff(r)
+    self.nbr = ref_cases.split_neighbors(r, self.cutoff)
+
+  def terms(self, r):
+    g = _mods()["generalized_born"]
+    q = np.asarray(self.s["charges"], np.float64)
+    rad = np.asarray(self.s["radii"], np.float64)
+    sr = np.asarray(self.s["scaled_radii"], np.float64)
+    rg = np.asarray(r, np.float64).view(_JaxGather)
+    born = np.asarray(g.compute_born_radii_neighbor_list(rg, rad, self.nbr, scaled_radii=sr))
+    e_gb = float(g.gb_energy_split_vjp(rg, q, rad, self.nbr, sr))
+    e_ace = float(np.sum(g.compute_ace_nonpolar_energy(rad, born)))
+    return e_gb, e_ace, born
+
+  def group_energy(self, r, group):
+    e_gb, e_ace, _ = self.terms(r)
+    return e_gb + e_ace
+
+
 def _build_case(kind, payload):
   if kind == "synthetic":
     s, cutoff = ref_cases.case_system(payload)
     explicit = ref_cases.exception_table(s) if ref_cases.CASES[payload][5] == "exceptions" else None
     return RefCase(s, cutoff, explicit)
+  if kind == "split":
+    return SplitCase()
   raise ValueError(kind)
 
 
 def _fd_chunk(args):
   """-dE/dx of one energy group for the coordinates in ``coords``."""
-  group, coords, r0 = args
+  group, coords, r0, h = args
   out = []
   for (a, c) in coords:
     vals = []
     for k in (-2, -1, 1, 2):
       r = np.array(r0, copy=True)
-      r[a, c] += k * FD_H
+      r[a, c] += k * h
       vals.append(_CASE.group_energy(r, group))
     em2, em1, ep1, ep2 = vals
-    out.append(-(8.0 * (ep1 - em1) - (ep2 - em2)) / (12.0 * FD_H))
+    out.append(-(8.0 * (ep1 - em1) - (ep2 - em2)) / (12.0 * h))
   return out
 
 
-def fd_forces(kind, payload, group, r0, workers):
+def fd_forces(kind, payload, group, r0, workers, h=FD_H):
   n = r0.shape[0]
   coords = [(a, c) for a in range(n) for c in range(3)]
   chunks = [coords[i::workers * 4] for i in range(workers * 4)]
   ctx = multiprocessing.get_context("spawn")
   with concurrent.futures.ProcessPoolExecutor(workers, mp_context=ctx, initializer=_init_worker,
                                               initargs=(kind, payload)) as ex:
-    results = list(ex.map(_fd_chunk, [(group, ch, r0) for ch in chunks]))
+    results = list(ex.map(_fd_chunk, [(group, ch, r0, h) for ch in chunks]))
   f = np.zeros((n, 3))
   for ch, vals in zip(chunks, results):
     for (a, c), v in zip(ch, vals):
@@ -293,6 +336,24 @@ def synthetic_case(name, workers):
   return out
 
 
+def split_case(workers):
+  """Born radii, GB and ACE energies of the NL-Born + dense-GB split from the
+  reference's functions, and the GB + ACE forces by finite differences of
+  them (the cutoff is clear of every pair distance by more than the
+  difference steps, so no pair enters or leaves the list)."""
+  t0 = time.time()
+  case = SplitCase()
+  r = np.asarray(case.s["positions"], np.float64)
+  e_gb, e_ace, born = case.terms(r)
+  f = fd_forces("split", None, "gb", r, workers, h=ref_cases.SPLIT_FD_H)
+  print(f"{ref_cases.SPLIT_CASE}: cutoff {case.cutoff}, GB {e_gb:.8f}, ACE {e_ace:.8f}, "
+        f"{time.time() - t0:.0f} s", flush=True)
+  return {"born_cutoff": np.array(case.cutoff), "gb": np.array(e_gb), "nonpolar": np.array(e_ace),
+          "born_radii": born, "forces_gb_ace": f,
+          "input_digest": np.array(ref_cases.digest(r, case.s["charges"], case.s["radii"],
+                                                    case.s["scaled_radii"]))}
+
+
 def pqr_case(src):
   g = _mods()["generalized_born"]
   path = os.path.join(os.path.dirname(src.rstrip("/")), PQR)
@@ -308,16 +369,22 @@ def pqr_case(src):
 
 
 def main():
+  """All cases; ``--only NAME`` recomputes one case into the existing file."""
   np.seterr(divide="ignore", invalid="ignore")  # the reference masks its own i = j divisions
   src = os.environ.get("PROLIX_REFERENCE_SRC", ref_loader.DEFAULT_SRC)
   _mods()
   workers = min(8, os.cpu_count() or 1)
+  only = sys.argv[sys.argv.index("--only") + 1] if "--only" in sys.argv else None
   out = {"term_names": np.array(TERMS + ("total",))}
-  for name in ref_cases.CASES:
-    for k, v in synthetic_case(name, workers).items():
+  if only is not None:
+    out.update(dict(np.load(ref_cases.FIXTURE)))
+  cases = [(name, lambda name=name: synthetic_case(name, workers)) for name in ref_cases.CASES]
+  cases += [(ref_cases.PQR_CASE, lambda: pqr_case(src)), (ref_cases.SPLIT_CASE, lambda: split_case(workers))]
+  for name, make in cases:
+    if only is not None and name != only:
+      continue
+    for k, v in make().items():
       out[f"{name}/{k}"] = v
-  for k, v in pqr_case(src).items():
-    out[f"{ref_cases.PQR_CASE}/{k}"] = v
   np.savez_compressed(ref_cases.FIXTURE, **out)
   print(f"wrote {ref_cases.FIXTURE} ({os.path.getsize(ref_cases.FIXTURE) // 1024} KiB)")
 

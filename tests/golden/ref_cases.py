@@ -35,6 +35,37 @@ CASES = {
     "chain166_exceptions": (166, 2, True, False, 0.0, "exceptions"),
 }
 PQR_CASE = "pqr1a00_chainA"
+# the NL-Born + dense-GB split (generalized_born.py:706-817) on the 600-atom
+# globule's inputs: Born radii from the pairs within SPLIT_CUTOFF, GB pair
+# terms over all pairs
+SPLIT_CASE = "globule600_nlborn"
+SPLIT_BASE = "globule600_cut9"
+SPLIT_CUTOFFS = tuple(10.0 + 0.001 * k for k in range(50))
+SPLIT_MARGIN = 3e-5  # no pair distance within this of the cutoff (float32 rounding and FD steps stay on one side)
+SPLIT_FD_H = 1e-5    # the split case's finite-difference step (2 h < SPLIT_MARGIN)
+
+
+def split_cutoff(pos) -> float:
+  """The first of SPLIT_CUTOFFS with no pair distance within SPLIT_MARGIN."""
+  d = np.linalg.norm(pos[:, None, :] - pos[None, :, :], axis=-1)
+  for c in SPLIT_CUTOFFS:
+    if not np.any(np.abs(d - c) < SPLIT_MARGIN):
+      return c
+  raise ValueError("no cutoff clear of the pair distances")
+
+
+def split_neighbors(pos, cutoff: float):
+  """(N, K) neighbour rows of the pairs within ``cutoff`` (both directions,
+  padded with N), as the reference's NL functions take them."""
+  n = pos.shape[0]
+  d = np.linalg.norm(pos[:, None, :] - pos[None, :, :], axis=-1)
+  within = (d < cutoff) & ~np.eye(n, dtype=bool)
+  k = int(within.sum(axis=1).max())
+  rows = np.full((n, k), n, dtype=np.int32)
+  for i in range(n):
+    j = np.nonzero(within[i])[0]
+    rows[i, :j.size] = j
+  return rows
 # OBC2 scale factors by element (the defaults of OpenMM's GBSAOBCForce
 # parameter sets, which prolix's OpenMM parity tests compare against)
 OBC_SCALE = {"H": 0.85, "C": 0.72, "N": 0.79, "O": 0.85, "S": 0.96}

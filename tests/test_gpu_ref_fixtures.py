@@ -123,3 +123,23 @@ def _psi_amplification(born, radius):
     psi = psi - (a - target) / da
   da = 1.0 - 1.6 * psi + 14.55 * psi**2
   return born * (1.0 - th**2) * psi * da / radius
+
+
+def test_nl_born_dense_gb_split_matches_the_reference():
+  # the born_cutoff path (NL Born radii, dense GB pair terms) against
+  # prolix's compute_born_radii_neighbor_list and gb_energy_split_vjp run
+  # from its own source; GB and ACE alone
+  from prolix_b200 import _lib, engine
+  c = ref_cases.SPLIT_CASE
+  s, _ = ref_cases.case_system(ref_cases.SPLIT_BASE)
+  s = {k: v for k, v in s.items() if k != "seed"}
+  bc = float(FIX[f"{c}/born_cutoff"])
+  with engine.Batch([s], cutoff=0.0, gb_cutoff=0.0, born_cutoff=bc, terms=_lib.USE_GB) as b:
+    e, f = b.energy_forces()
+    born = b.born_radii()
+  np.testing.assert_allclose(born, FIX[f"{c}/born_radii"], rtol=B_REL)
+  for k in ("gb", "nonpolar"):
+    i = TERMS.index(k)
+    assert e[0][i] == pytest.approx(float(FIX[f"{c}/{k}"]), rel=E_REL, abs=E_ABS), k
+  fr = FIX[f"{c}/forces_gb_ace"]
+  assert np.linalg.norm(f - fr) / np.linalg.norm(fr) < F_RMS

@@ -144,3 +144,23 @@ def test_padded_table_conversion_rejects_what_the_batch_cannot_hold():
   sv2 = np.array([[0.5, 1.0], [0.5, 0.4], [0.4, 1.0]])
   with pytest.raises(ValueError, match="one class"):
     topology.pairs_from_padded_table(idx2, sv2, np.full((3, 2), 0.8))
+
+
+def test_nl_born_dense_gb_split_matches_the_reference():
+  # prolix's compute_born_radii_neighbor_list and gb_energy_split_vjp
+  # (generalized_born.py:266-337, :706-770), run from its own source with
+  # every pair within the Born cutoff listed: the oracle's born_cutoff path
+  c = ref_cases.SPLIT_CASE
+  s, _ = ref_cases.case_system(ref_cases.SPLIT_BASE)
+  r = np.asarray(s["positions"])
+  assert str(FIX[f"{c}/input_digest"]) == ref_cases.digest(r, s["charges"], s["radii"], s["scaled_radii"])
+  bc = float(FIX[f"{c}/born_cutoff"])
+  assert bc == ref_cases.split_cutoff(r)
+  # GB and ACE alone: no LJ (eps = 0), no direct Coulomb (k = 0)
+  e, f, ex = ogbsa.nonbonded(dict(s, epsilons=np.zeros(len(r))), r, 0.0, k_coul=0.0, gb_cutoff=0.0,
+                             born_cutoff=bc)
+  np.testing.assert_allclose(ex["born_radii"], FIX[f"{c}/born_radii"], rtol=1e-12)
+  assert e["gb"] == pytest.approx(float(FIX[f"{c}/gb"]), rel=E_REL)
+  assert e["nonpolar"] == pytest.approx(float(FIX[f"{c}/nonpolar"]), rel=E_REL)
+  fr = FIX[f"{c}/forces_gb_ace"]
+  assert np.linalg.norm(f - fr) / np.linalg.norm(fr) < F_REL
