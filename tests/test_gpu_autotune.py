@@ -81,11 +81,12 @@ def test_tune_restores_state_and_caches(tmp_path, monkeypatch):
 
 @pytest.mark.parametrize("cutoff", [0.0, 9.0])
 def test_four_block_force_kernel_equals_the_two_block_one(cutoff):
-  # ragged sizes (a system of one block, partial blocks, i-block counts not
+  # ragged sizes (one atom, one block, partial blocks, i-block counts not
   # multiples of 4), exclusions and 1-4 pairs, with and without a cutoff
   # (no pair list, so the four-block kernel runs): forces and trajectories
   # are the same bit for bit
-  systems = [synth.make_chain(n, 40 + k, compact=True) for k, n in enumerate([20, 97, 130, 260, 1000])]
+  sizes = [1, 2, 20, 31, 32, 33, 64, 97, 128, 129, 130, 160, 193, 260, 1000]
+  systems = [synth.make_chain(n, 40 + k, compact=True) for k, n in enumerate(sizes)]
   out = {}
   for blocks in (2, 4):
     with engine.Batch(systems, cutoff=cutoff, pair_list=False) as b:
