@@ -202,6 +202,28 @@ struct FData2 {  // the lane's two i atoms, packed, for the force pass
   float2 qk;   // k_C q_i
 };
 __device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
+
+// The two lanes of a packed pair through the MUFU, written straight into one
+// 64-bit register so that the packed operations that read the result find
+// it in an aligned register pair (the same instructions rsqrtf and exp2f
+// issue under -ftz).
+__device__ __forceinline__ float2 unpack2(unsigned long long p) {
+  float2 r;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(p));
+  return r;
+}
+__device__ __forceinline__ float2 rsqrt2(float2 v) {
+  unsigned long long p;
+  asm("{\n\t.reg .f32 a, b;\n\trsqrt.approx.ftz.f32 a, %1;\n\trsqrt.approx.ftz.f32 b, %2;\n\tmov.b64 %0, {a, b};\n\t}"
+      : "=l"(p) : "f"(v.x), "f"(v.y));
+  return unpack2(p);
+}
+__device__ __forceinline__ float2 exp2neg2(float2 w) {  // 2^-w per lane
+  unsigned long long p;
+  asm("{\n\t.reg .f32 a, b;\n\tneg.f32 a, %1;\n\tneg.f32 b, %2;\n\tex2.approx.ftz.f32 a, a;\n\tex2.approx.ftz.f32 b, b;\n\tmov.b64 %0, {a, b};\n\t}"
+      : "=l"(p) : "f"(w.x), "f"(w.y));
+  return unpack2(p);
+}
 __device__ __forceinline__ float2 sel2(bool a, bool b, float va, float vb) {
   return make_float2(a ? va : vb, b ? va : vb);
 }
@@ -244,10 +266,10 @@ __device__ __forceinline__ void force_pair_step(const FData2 &I, const JF2 &J, A
     // the same for both atoms: h = A2 e (B_i B_j + r^2 / 4) is summed for
     // both, and each sum is scaled by -1 / (2 B) when it is flushed
     const float2 w = __fmul2_rn(r2, __fmul2_rn(I.iB, J.iB));  // r^2 log2(e) / (4 B_i B_j)
-    const float2 ex = make_float2(exp2f(-w.x), exp2f(-w.y));
+    const float2 ex = exp2neg2(w);
     const float2 bb = __fmul2_rn(I.B, J.B);
     const float2 f2 = __ffma2_rn(bb, ex, r2);
-    const float2 inv_f = make_float2(rsqrtf(f2.x), rsqrtf(f2.y));
+    const float2 inv_f = rsqrt2(f2);
     float2 A2 = __fmul2_rn(__fmul2_rn(I.q2p, J.q), __fmul2_rn(__fmul2_rn(inv_f, inv_f), inv_f));
     if (CUT && K.gcut2 != 0.f) A2 = __fmul2_rn(A2, sel2(r2.x < K.gcut2, r2.y < K.gcut2, 1.f, 0.f));
     const float2 A2e = __fmul2_rn(A2, ex);
@@ -257,7 +279,7 @@ __device__ __forceinline__ void force_pair_step(const FData2 &I, const JF2 &J, A
     tj.a3 = tj.a3 + h.x + h.y;
   }
   if (K.use_lj || K.use_coul) {
-    const float2 inv_r = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+    const float2 inv_r = rsqrt2(r2);
     const float2 inv_r2 = __fmul2_rn(inv_r, inv_r);
     float2 sc_c = dup2(1.f), sc_l = dup2(1.f);  // exclusion and 1-4 factors
     if (EXCL) {
@@ -386,7 +408,7 @@ __device__ __forceinline__ void bc_series2(const PData2 &I, const JD2 &J, bool o
   // FULL: every pair of the tile exists (no cutoff): no select
   P.r2 = (FULL && !CUT) ? r2 : make_float2(ok0 ? r2.x : kFarR2, ok1 ? r2.y : kFarR2);
   // every lane evaluates, so the warp ballot that follows is reached by all lanes
-  P.inv_r = make_float2(rsqrtf(P.r2.x), rsqrtf(P.r2.y));
+  P.inv_r = rsqrt2(P.r2);
   const float2 inv_r2 = __fmul2_rn(P.inv_r, P.inv_r);
   const float2 inv_r4 = __fmul2_rn(inv_r2, inv_r2);
   if (PASS == PASS_BORN) {
