@@ -86,30 +86,30 @@ struct NlRows4 {
   float2 x[2], y[2], z[2];
 };
 
-__device__ __forceinline__ void nl_hit_row(const NlArgs &a, const SysInfo &S, bool hit, int lj, int row, unsigned below,
-                                           int &cnt) {
+// row: the row's first slot; cap: its capacity.
+__device__ __forceinline__ void nl_hit_row(bool hit, int lj, int *row, int cap, unsigned below, int &cnt) {
   const unsigned m = __ballot_sync(kFull, hit);
   const int t = cnt + __popc(m & below);
-  if (hit && t < a.capacity) a.rows[(size_t)(S.off + row) * a.capacity + t] = lj;
+  if (hit && t < cap) row[t] = lj;
   cnt += __popc(m);
 }
 
 template <bool DIAG>
-__device__ __forceinline__ void nl_rows_block(const NlArgs &a, const SysInfo &S, const NlRows4 &P, float4 q, int lj,
-                                              int l0, unsigned below, int *cnt) {
+__device__ __forceinline__ void nl_rows_block(const NlRows4 &P, float4 q, int lj, int l0, float reach2,
+                                              int *const *row, int cap, unsigned below, int *cnt) {
   const float2 nqx = make_float2(-q.x, -q.x), nqy = make_float2(-q.y, -q.y), nqz = make_float2(-q.z, -q.z);
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
     const float2 ex = __fadd2_rn(P.x[h], nqx), ey = __fadd2_rn(P.y[h], nqy), ez = __fadd2_rn(P.z[h], nqz);
     const float2 d2 = __ffma2_rn(ex, ex, __ffma2_rn(ey, ey, __fmul2_rn(ez, ez)));
     const int r0 = 2 * h, r1 = 2 * h + 1;
-    bool hit0 = d2.x < a.reach2, hit1 = d2.y < a.reach2;
+    bool hit0 = d2.x < reach2, hit1 = d2.y < reach2;
     if (DIAG) {
       hit0 = hit0 && lj != l0 + r0;
       hit1 = hit1 && lj != l0 + r1;
     }
-    nl_hit_row(a, S, hit0, lj, l0 + r0, below, cnt[r0]);
-    nl_hit_row(a, S, hit1, lj, l0 + r1, below, cnt[r1]);
+    nl_hit_row(hit0, lj, row[r0], cap, below, cnt[r0]);
+    nl_hit_row(hit1, lj, row[r1], cap, below, cnt[r1]);
   }
 }
 
@@ -119,49 +119,61 @@ __global__ void __launch_bounds__(32 * kRowsWarps) nl_rows_kernel(const NlArgs a
   __shared__ int n_live;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const unsigned below = (1u << lane) - 1u;
+  const int cap = a.capacity;
+  const float reach2 = a.reach2;
   for (int ib = blockIdx.x; ib < a.n_blocks; ib += gridDim.x) {
     const int s = a.blk_sys[ib];
-    const SysInfo &S = a.sys[s];
-    const int l0 = (ib - S.blk_base) * 32 + w * kRowsPerWarp;  // the warp's first row, local index
+    // the system's fields in registers: the row stores could alias them
+    const int off = a.sys[s].off, n = a.sys[s].n, nblk = a.sys[s].nblk, blk_base = a.sys[s].blk_base;
+    const int l0 = (ib - blk_base) * 32 + w * kRowsPerWarp;  // the warp's first row, local index
     int cnt[kRowsPerWarp];
+    int *row[kRowsPerWarp];  // each row's first slot
     static_assert(kRowsPerWarp == 4, "rows are paired");
     NlRows4 P;
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      float4 u = a.posq[S.off + min(l0 + 2 * h, S.n - 1)], v = a.posq[S.off + min(l0 + 2 * h + 1, S.n - 1)];
-      if (l0 + 2 * h >= S.n) u.x = -1e30f;  // no row: never within reach of an atom
-      if (l0 + 2 * h + 1 >= S.n) v.x = -1e30f;
+      float4 u = a.posq[off + min(l0 + 2 * h, n - 1)], v = a.posq[off + min(l0 + 2 * h + 1, n - 1)];
+      if (l0 + 2 * h >= n) u.x = -1e30f;  // no row: never within reach of an atom
+      if (l0 + 2 * h + 1 >= n) v.x = -1e30f;
       P.x[h] = make_float2(u.x, v.x);
       P.y[h] = make_float2(u.y, v.y);
       P.z[h] = make_float2(u.z, v.z);
       cnt[2 * h] = cnt[2 * h + 1] = 0;
     }
-    const int own = ib - S.blk_base;
-    for (int j0 = 0; j0 < S.nblk; j0 += kMaxJList) {
-      const int j1 = min(S.nblk, j0 + kMaxJList);
+#pragma unroll
+    for (int r = 0; r < kRowsPerWarp; ++r) row[r] = a.rows + (size_t)(off + min(l0 + r, n - 1)) * cap;
+    const int own = ib - blk_base;
+    for (int j0 = 0; j0 < nblk; j0 += kMaxJList) {
+      const int j1 = min(nblk, j0 + kMaxJList);
       __syncthreads();  // the previous window's list is no longer read
       if (w == 0) {
-        int n = 0;
+        int nl = 0;
         for (int jb0 = j0; jb0 < j1; jb0 += 32) {
           const int jb = jb0 + lane;
-          const bool live = jb < j1 && nl_box_dist2(a.bbox, ib, S.blk_base + jb) < a.reach2;
+          const bool live = jb < j1 && nl_box_dist2(a.bbox, ib, blk_base + jb) < reach2;
           const unsigned m = __ballot_sync(kFull, live);
-          if (live) jl[n + __popc(m & below)] = jb;
-          n += __popc(m);
+          if (live) jl[nl + __popc(m & below)] = jb;
+          nl += __popc(m);
         }
-        if (lane == 0) n_live = n;
+        if (lane == 0) n_live = nl;
       }
       __syncthreads();
-      if (l0 >= S.n) continue;  // a warp past the system's last atom has no rows
+      if (l0 >= n) continue;  // a warp past the system's last atom has no rows
       const int L = n_live;
       for (int k0 = 0; k0 < L; k0 += 32) {
         // the listed blocks within reach of one of the warp's four atoms
         // (lane = block; the margin keeps the test conservative under
         // rounding), then their atoms, lane = candidate
-        bool near = false;
+        // A block whose every atom is within reach of all four rows (its box's
+        // farthest corner is, by the same rounded operations as the atom
+        // test, so each atom's computed distance is no larger) is stored
+        // without its distances: the same slots in the same order.
+        bool near = false, inside = false;
         if (k0 + lane < L) {
-          const int gjb = S.blk_base + jl[k0 + lane];
+          const int jb = jl[k0 + lane];
+          const int gjb = blk_base + jb;
           const float4 lo = a.bbox[2 * gjb], hi = a.bbox[2 * gjb + 1];
+          inside = jb != own && jb * 32 + 32 <= n;
 #pragma unroll
           for (int r = 0; r < kRowsPerWarp; ++r) {
             const float px = r & 1 ? P.x[r >> 1].y : P.x[r >> 1].x;
@@ -170,29 +182,53 @@ __global__ void __launch_bounds__(32 * kRowsWarps) nl_rows_kernel(const NlArgs a
             const float dx = fmaxf(0.f, fmaxf(lo.x - px, px - hi.x));
             const float dy = fmaxf(0.f, fmaxf(lo.y - py, py - hi.y));
             const float dz = fmaxf(0.f, fmaxf(lo.z - pz, pz - hi.z));
-            near |= fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < a.reach2 * 1.0001f;
+            near |= fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < reach2 * 1.0001f;
+            const float fx = fmaxf(fabsf(px - lo.x), fabsf(hi.x - px));
+            const float fy = fmaxf(fabsf(py - lo.y), fabsf(hi.y - py));
+            const float fz = fmaxf(fabsf(pz - lo.z), fabsf(hi.z - pz));
+            inside = inside && fmaf(fx, fx, fmaf(fy, fy, fz * fz)) < reach2;
           }
         }
+        const unsigned in_m = __ballot_sync(kFull, inside);
         for (unsigned blocks = __ballot_sync(kFull, near); blocks != 0u; blocks &= blocks - 1u) {
-          const int jb = jl[k0 + __ffs(blocks) - 1];
+          const int k = __ffs(blocks) - 1;
+          const int jb = jl[k0 + k];
           const int lj = jb * 32 + lane;
-          float4 q = a.posq[S.off + min(lj, S.n - 1)];
-          if (lj >= S.n) q.x = 1e30f;  // no atom: never within reach of a row
-          if (jb == own) nl_rows_block<true>(a, S, P, q, lj, l0, below, cnt);  // skips i = j
-          else nl_rows_block<false>(a, S, P, q, lj, l0, below, cnt);
+          if ((in_m >> k) & 1u) {
+#pragma unroll
+            for (int r = 0; r < kRowsPerWarp; ++r) {
+              const int t = cnt[r] + lane;
+              if (t < cap) row[r][t] = lj;
+              cnt[r] += 32;
+            }
+            continue;
+          }
+          float4 q = a.posq[off + min(lj, n - 1)];
+          if (lj >= n) q.x = 1e30f;  // no atom: never within reach of a row
+          if (jb == own) nl_rows_block<true>(P, q, lj, l0, reach2, row, cap, below, cnt);  // skips i = j
+          else nl_rows_block<false>(P, q, lj, l0, reach2, row, cap, below, cnt);
         }
       }
     }
 #pragma unroll
     for (int r = 0; r < kRowsPerWarp; ++r) {
       const int li = l0 + r;
-      if (li >= S.n) break;
-      const int i = S.off + li;
-      int *row = a.rows + (size_t)i * a.capacity;
-      for (int t = cnt[r] + lane; t < a.capacity; t += 32) row[t] = S.n;  // sentinels
+      if (li >= n) break;
+      const int i = off + li;
+      // sentinels; with rows of a multiple of 4 slots (each row 16-byte
+      // aligned) as 16-byte stores after at most 3 single slots
+      int *rp = row[r];
+      if ((cap & 3) == 0 && (reinterpret_cast<uintptr_t>(a.rows) & 15) == 0) {
+        const int ta = min(cap, (cnt[r] + 3) & ~3);
+        if (cnt[r] + lane < ta) rp[cnt[r] + lane] = n;
+        const int4 s4 = make_int4(n, n, n, n);
+        for (int t = ta + 4 * lane; t < cap; t += 128) *reinterpret_cast<int4 *>(rp + t) = s4;
+      } else {
+        for (int t = cnt[r] + lane; t < cap; t += 32) rp[t] = n;
+      }
       if (lane == 0) {
         a.counts[i] = cnt[r];
-        if (cnt[r] > a.capacity) atomicOr(&a.status[s], (uint32_t)PB2_STATUS_NLOVERFLOW);
+        if (cnt[r] > cap) atomicOr(&a.status[s], (uint32_t)PB2_STATUS_NLOVERFLOW);
         atomicMax(&a.ctl[NL_MAXCOUNT], cnt[r]);
       }
     }

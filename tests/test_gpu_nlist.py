@@ -46,6 +46,44 @@ def test_cell_list_matches_brute_force_ragged():
     off += n
 
 
+def test_long_reach_rows_match_brute_force():
+  # reach 16 A against 32-atom blocks of a compact chain: many blocks lie
+  # wholly within reach of a warp's four rows and are stored without their
+  # distances, beside blocks that are tested atom by atom
+  systems = [synth.make_chain(n, 410 + k, compact=True) for k, n in enumerate([3000, 777])]
+  with engine.Batch(systems, cutoff=14.0, skin=2.0) as b:
+    b.nl_build()
+    rows = b.nl_get()
+    b.nl_build()
+    again = b.nl_get()
+  np.testing.assert_array_equal(rows, again)
+  _check_rows(rows, systems, 16.0)
+  off = 0
+  for s in systems:
+    n = len(s["charges"])
+    for r in rows[off:off + n]:
+      got = r[r != n]
+      assert (r[len(got):] == n).all()  # sentinels after the neighbours
+    off += n
+
+
+def test_capacity_not_a_multiple_of_four():
+  # an odd fixed capacity: the sentinels go one slot at a time
+  s = synth.make_chain(500, 12, compact=True)
+  out = []
+  for cap in (None, 501):
+    kw = {} if cap is None else dict(nl_capacity=cap)
+    with engine.Batch([s], cutoff=9.0, skin=2.0, **kw) as b:
+      b.nl_build()
+      out.append(b.nl_get())
+  auto, odd = out
+  assert odd.shape[1] == 501
+  for ra, ro in zip(auto, odd):
+    got = ro[ro != 500]
+    np.testing.assert_array_equal(got, ra[ra != 500])
+    assert (ro[len(got):] == 500).all()
+
+
 def test_skin_rebuild_rule():
   s = synth.make_chain(500, 8, compact=True)
   with engine.Batch([s], cutoff=9.0, skin=2.0) as b:
