@@ -130,7 +130,7 @@ struct Energy64Args {
 };
 
 // Neighbour-list control words (NlArgs::ctl)
-enum { NL_DIRTY = 0, NL_MAXCOUNT = 1, NL_DONE = 2, NL_WORDS = 4 };
+enum { NL_DIRTY = 0, NL_MAXCOUNT = 1, NL_DONE = 2, NL_NEXT = 3, NL_WORDS = 4 };
 struct NlArgs {
   const SysInfo *sys;
   const int32_t *atom_sys;

@@ -12,11 +12,11 @@
 // are stored in a recursive-bisection order, so a block is a compact
 // cluster, and its bounding box is already computed for the pair kernels.
 // A cell grid is not built: the block boxes play its part, a box test
-// standing in for the cell stencil.  One thread block per 32-atom block
-// (its 32 rows): the blocks of the system whose boxes come within
-// cutoff + skin of its own are listed, and their atoms are tested 32 at a
-// time (lane = candidate), in index order.  Rows are therefore in
-// stored-atom order, the same every build.
+// standing in for the cell stencil.  One warp per four rows: the blocks of
+// the system whose boxes come within cutoff + skin of one of its atoms are
+// walked in index order, their atoms tested 32 at a time (lane =
+// candidate).  Rows are therefore in stored-atom order, the same every
+// build, whichever warp built them.
 // A row longer than the capacity only counts (the largest count and an
 // overflow bit are recorded for the host's next visit).
 //
@@ -25,10 +25,11 @@
 //   0. (check) each atom's displacement since the last build against
 //      skin/2 sets the rebuild flag and its system's moved flag;
 //   1. the rows; 2. the positions become the new displacement reference,
-//      and the last block clears the flag.
+//      and the last block clears the flag and the rows' unit counter.
 // Each kernel returns at once while the flag is clear.  The HBM traffic is
 // the row writes (4 B per slot).
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -66,15 +67,14 @@ __global__ void nl_disp_kernel(const NlArgs a) {
   }
 }
 
-// 1. rows: one thread block (8 warps) per block of atoms; warp w owns the
-// block's rows 4w .. 4w + 3.  Warp 0 lists, in order, the blocks within
-// reach of this one; each warp narrows that list, 32 blocks at a time, to
-// the blocks within reach of one of its own four atoms, and walks those one
-// j-block at a time, lane = candidate atom: one position load serves the
-// warp's four rows, and each row's hits are compacted by a ballot and
-// stored as one contiguous run (coalesced), so rows come out in j order.
-constexpr int kMaxJList = 4096;  // j-blocks listed at once (longer systems: in windows)
-constexpr int kRowsPerWarp = 32 / kRowsWarps;
+// 1. rows: a warp unit is four rows of a 32-atom block.  The warp tests the
+// boxes of its system's blocks, 32 at a time (lane = block), against its
+// four atoms, and walks the blocks within reach one at a time, lane =
+// candidate atom: one position load serves the four rows, and each row's
+// hits are compacted by a ballot and stored as one contiguous run
+// (coalesced), so rows come out in j order.  The warps of one resident wave
+// take units from a counter until none is left.
+constexpr int kRowsPerWarp = 4;
 
 // One j-block's 32 candidates (lane = candidate lj; nq = minus its
 // position, duplicated) against the warp's rows l0 .. l0 + 3, whose
@@ -113,125 +113,121 @@ __device__ __forceinline__ void nl_rows_block(const NlRows4 &P, float4 q, int lj
   }
 }
 
+// The rows of one warp unit: four rows of a 32-atom block against every
+// block of its system, culled by box (lane = block, 32 at a time), then the
+// near blocks' atoms, lane = candidate.
+__device__ __forceinline__ void nl_rows_unit(const NlArgs &a, int ib, int w, int lane, unsigned below, int cap,
+                                             float reach2) {
+  const int s = a.blk_sys[ib];
+  // the system's fields in registers: the row stores could alias them
+  const int off = a.sys[s].off, n = a.sys[s].n, nblk = a.sys[s].nblk, blk_base = a.sys[s].blk_base;
+  const int l0 = (ib - blk_base) * 32 + w * kRowsPerWarp;  // the unit's first row, local index
+  if (l0 >= n) return;  // past the system's last atom: no rows
+  int cnt[kRowsPerWarp];
+  int *row[kRowsPerWarp];  // each row's first slot
+  static_assert(kRowsPerWarp == 4, "rows are paired");
+  NlRows4 P;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    float4 u = a.posq[off + min(l0 + 2 * h, n - 1)], v = a.posq[off + min(l0 + 2 * h + 1, n - 1)];
+    if (l0 + 2 * h >= n) u.x = -1e30f;  // no row: never within reach of an atom
+    if (l0 + 2 * h + 1 >= n) v.x = -1e30f;
+    P.x[h] = make_float2(u.x, v.x);
+    P.y[h] = make_float2(u.y, v.y);
+    P.z[h] = make_float2(u.z, v.z);
+    cnt[2 * h] = cnt[2 * h + 1] = 0;
+  }
+#pragma unroll
+  for (int r = 0; r < kRowsPerWarp; ++r) row[r] = a.rows + (size_t)(off + min(l0 + r, n - 1)) * cap;
+  const int own = ib - blk_base;
+  for (int c0 = 0; c0 < nblk; c0 += 32) {
+    // the blocks within reach of one of the unit's four atoms (the margin
+    // keeps the test conservative under rounding).  A block whose every
+    // atom is within reach of all four rows (its box's farthest corner is,
+    // by the same rounded operations as the atom test, so each atom's
+    // computed distance is no larger) is stored without its distances: the
+    // same slots in the same order.
+    bool near = false, inside = false;
+    if (c0 + lane < nblk) {
+      const int jb = c0 + lane;
+      const float4 lo = a.bbox[2 * (blk_base + jb)], hi = a.bbox[2 * (blk_base + jb) + 1];
+      inside = jb != own && jb * 32 + 32 <= n;
+#pragma unroll
+      for (int r = 0; r < kRowsPerWarp; ++r) {
+        const float px = r & 1 ? P.x[r >> 1].y : P.x[r >> 1].x;
+        const float py = r & 1 ? P.y[r >> 1].y : P.y[r >> 1].x;
+        const float pz = r & 1 ? P.z[r >> 1].y : P.z[r >> 1].x;
+        const float dx = fmaxf(0.f, fmaxf(lo.x - px, px - hi.x));
+        const float dy = fmaxf(0.f, fmaxf(lo.y - py, py - hi.y));
+        const float dz = fmaxf(0.f, fmaxf(lo.z - pz, pz - hi.z));
+        near |= fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < reach2 * 1.0001f;
+        const float fx = fmaxf(fabsf(px - lo.x), fabsf(hi.x - px));
+        const float fy = fmaxf(fabsf(py - lo.y), fabsf(hi.y - py));
+        const float fz = fmaxf(fabsf(pz - lo.z), fabsf(hi.z - pz));
+        inside = inside && fmaf(fx, fx, fmaf(fy, fy, fz * fz)) < reach2;
+      }
+    }
+    const unsigned in_m = __ballot_sync(kFull, inside);
+    for (unsigned blocks = __ballot_sync(kFull, near); blocks != 0u; blocks &= blocks - 1u) {
+      const int k = __ffs(blocks) - 1;
+      const int jb = c0 + k;
+      const int lj = jb * 32 + lane;
+      if ((in_m >> k) & 1u) {
+#pragma unroll
+        for (int r = 0; r < kRowsPerWarp; ++r) {
+          const int t = cnt[r] + lane;
+          if (t < cap) row[r][t] = lj;
+          cnt[r] += 32;
+        }
+        continue;
+      }
+      float4 q = a.posq[off + min(lj, n - 1)];
+      if (lj >= n) q.x = 1e30f;  // no atom: never within reach of a row
+      if (jb == own) nl_rows_block<true>(P, q, lj, l0, reach2, row, cap, below, cnt);  // skips i = j
+      else nl_rows_block<false>(P, q, lj, l0, reach2, row, cap, below, cnt);
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < kRowsPerWarp; ++r) {
+    const int li = l0 + r;
+    if (li >= n) break;
+    const int i = off + li;
+    // sentinels; with rows of a multiple of 4 slots (each row 16-byte
+    // aligned) as 16-byte stores after at most 3 single slots
+    int *rp = row[r];
+    if ((cap & 3) == 0 && (reinterpret_cast<uintptr_t>(a.rows) & 15) == 0) {
+      const int ta = min(cap, (cnt[r] + 3) & ~3);
+      if (cnt[r] + lane < ta) rp[cnt[r] + lane] = n;
+      const int4 s4 = make_int4(n, n, n, n);
+      for (int t = ta + 4 * lane; t < cap; t += 128) *reinterpret_cast<int4 *>(rp + t) = s4;
+    } else {
+      for (int t = cnt[r] + lane; t < cap; t += 32) rp[t] = n;
+    }
+    if (lane == 0) {
+      a.counts[i] = cnt[r];
+      if (cnt[r] > cap) atomicOr(&a.status[s], (uint32_t)PB2_STATUS_NLOVERFLOW);
+      atomicMax(&a.ctl[NL_MAXCOUNT], cnt[r]);
+    }
+  }
+}
+
+// Each warp takes units (a 32-atom block's four rows) from a counter in
+// ctl[NL_NEXT] until none is left, so that the blocks' uneven costs (a
+// globule's core against its surface) spread over every SM; the reference
+// kernel resets the counter after the build.
 __global__ void __launch_bounds__(32 * kRowsWarps) nl_rows_kernel(const NlArgs a) {
   if (!nl_dirty(a)) return;
-  __shared__ int jl[kMaxJList];
-  __shared__ int n_live;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
   const unsigned below = (1u << lane) - 1u;
   const int cap = a.capacity;
   const float reach2 = a.reach2;
-  for (int ib = blockIdx.x; ib < a.n_blocks; ib += gridDim.x) {
-    const int s = a.blk_sys[ib];
-    // the system's fields in registers: the row stores could alias them
-    const int off = a.sys[s].off, n = a.sys[s].n, nblk = a.sys[s].nblk, blk_base = a.sys[s].blk_base;
-    const int l0 = (ib - blk_base) * 32 + w * kRowsPerWarp;  // the warp's first row, local index
-    int cnt[kRowsPerWarp];
-    int *row[kRowsPerWarp];  // each row's first slot
-    static_assert(kRowsPerWarp == 4, "rows are paired");
-    NlRows4 P;
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      float4 u = a.posq[off + min(l0 + 2 * h, n - 1)], v = a.posq[off + min(l0 + 2 * h + 1, n - 1)];
-      if (l0 + 2 * h >= n) u.x = -1e30f;  // no row: never within reach of an atom
-      if (l0 + 2 * h + 1 >= n) v.x = -1e30f;
-      P.x[h] = make_float2(u.x, v.x);
-      P.y[h] = make_float2(u.y, v.y);
-      P.z[h] = make_float2(u.z, v.z);
-      cnt[2 * h] = cnt[2 * h + 1] = 0;
-    }
-#pragma unroll
-    for (int r = 0; r < kRowsPerWarp; ++r) row[r] = a.rows + (size_t)(off + min(l0 + r, n - 1)) * cap;
-    const int own = ib - blk_base;
-    for (int j0 = 0; j0 < nblk; j0 += kMaxJList) {
-      const int j1 = min(nblk, j0 + kMaxJList);
-      __syncthreads();  // the previous window's list is no longer read
-      if (w == 0) {
-        int nl = 0;
-        for (int jb0 = j0; jb0 < j1; jb0 += 32) {
-          const int jb = jb0 + lane;
-          const bool live = jb < j1 && nl_box_dist2(a.bbox, ib, blk_base + jb) < reach2;
-          const unsigned m = __ballot_sync(kFull, live);
-          if (live) jl[nl + __popc(m & below)] = jb;
-          nl += __popc(m);
-        }
-        if (lane == 0) n_live = nl;
-      }
-      __syncthreads();
-      if (l0 >= n) continue;  // a warp past the system's last atom has no rows
-      const int L = n_live;
-      for (int k0 = 0; k0 < L; k0 += 32) {
-        // the listed blocks within reach of one of the warp's four atoms
-        // (lane = block; the margin keeps the test conservative under
-        // rounding), then their atoms, lane = candidate
-        // A block whose every atom is within reach of all four rows (its box's
-        // farthest corner is, by the same rounded operations as the atom
-        // test, so each atom's computed distance is no larger) is stored
-        // without its distances: the same slots in the same order.
-        bool near = false, inside = false;
-        if (k0 + lane < L) {
-          const int jb = jl[k0 + lane];
-          const int gjb = blk_base + jb;
-          const float4 lo = a.bbox[2 * gjb], hi = a.bbox[2 * gjb + 1];
-          inside = jb != own && jb * 32 + 32 <= n;
-#pragma unroll
-          for (int r = 0; r < kRowsPerWarp; ++r) {
-            const float px = r & 1 ? P.x[r >> 1].y : P.x[r >> 1].x;
-            const float py = r & 1 ? P.y[r >> 1].y : P.y[r >> 1].x;
-            const float pz = r & 1 ? P.z[r >> 1].y : P.z[r >> 1].x;
-            const float dx = fmaxf(0.f, fmaxf(lo.x - px, px - hi.x));
-            const float dy = fmaxf(0.f, fmaxf(lo.y - py, py - hi.y));
-            const float dz = fmaxf(0.f, fmaxf(lo.z - pz, pz - hi.z));
-            near |= fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < reach2 * 1.0001f;
-            const float fx = fmaxf(fabsf(px - lo.x), fabsf(hi.x - px));
-            const float fy = fmaxf(fabsf(py - lo.y), fabsf(hi.y - py));
-            const float fz = fmaxf(fabsf(pz - lo.z), fabsf(hi.z - pz));
-            inside = inside && fmaf(fx, fx, fmaf(fy, fy, fz * fz)) < reach2;
-          }
-        }
-        const unsigned in_m = __ballot_sync(kFull, inside);
-        for (unsigned blocks = __ballot_sync(kFull, near); blocks != 0u; blocks &= blocks - 1u) {
-          const int k = __ffs(blocks) - 1;
-          const int jb = jl[k0 + k];
-          const int lj = jb * 32 + lane;
-          if ((in_m >> k) & 1u) {
-#pragma unroll
-            for (int r = 0; r < kRowsPerWarp; ++r) {
-              const int t = cnt[r] + lane;
-              if (t < cap) row[r][t] = lj;
-              cnt[r] += 32;
-            }
-            continue;
-          }
-          float4 q = a.posq[off + min(lj, n - 1)];
-          if (lj >= n) q.x = 1e30f;  // no atom: never within reach of a row
-          if (jb == own) nl_rows_block<true>(P, q, lj, l0, reach2, row, cap, below, cnt);  // skips i = j
-          else nl_rows_block<false>(P, q, lj, l0, reach2, row, cap, below, cnt);
-        }
-      }
-    }
-#pragma unroll
-    for (int r = 0; r < kRowsPerWarp; ++r) {
-      const int li = l0 + r;
-      if (li >= n) break;
-      const int i = off + li;
-      // sentinels; with rows of a multiple of 4 slots (each row 16-byte
-      // aligned) as 16-byte stores after at most 3 single slots
-      int *rp = row[r];
-      if ((cap & 3) == 0 && (reinterpret_cast<uintptr_t>(a.rows) & 15) == 0) {
-        const int ta = min(cap, (cnt[r] + 3) & ~3);
-        if (cnt[r] + lane < ta) rp[cnt[r] + lane] = n;
-        const int4 s4 = make_int4(n, n, n, n);
-        for (int t = ta + 4 * lane; t < cap; t += 128) *reinterpret_cast<int4 *>(rp + t) = s4;
-      } else {
-        for (int t = cnt[r] + lane; t < cap; t += 32) rp[t] = n;
-      }
-      if (lane == 0) {
-        a.counts[i] = cnt[r];
-        if (cnt[r] > cap) atomicOr(&a.status[s], (uint32_t)PB2_STATUS_NLOVERFLOW);
-        atomicMax(&a.ctl[NL_MAXCOUNT], cnt[r]);
-      }
-    }
+  const int n_units = a.n_blocks * (32 / kRowsPerWarp);
+  for (;;) {
+    int u = 0;
+    if (lane == 0) u = atomicAdd(&a.ctl[NL_NEXT], 1);
+    u = __shfl_sync(kFull, u, 0);
+    if (u >= n_units) break;
+    nl_rows_unit(a, u / (32 / kRowsPerWarp), u % (32 / kRowsPerWarp), lane, below, cap, reach2);
   }
 }
 
@@ -248,6 +244,7 @@ __global__ void nl_ref_kernel(const NlArgs a) {
     __threadfence();
     if (atomicAdd(&a.ctl[NL_DONE], 1) == (int)gridDim.x - 1) {
       a.ctl[NL_DONE] = 0;
+      a.ctl[NL_NEXT] = 0;
       a.ctl[NL_DIRTY] = 0;
       __threadfence();
     }
@@ -256,8 +253,27 @@ __global__ void nl_ref_kernel(const NlArgs a) {
 
 static int grid_for(int n, int per) { return std::max(1, std::min((n + per - 1) / per, 65535)); }
 
+// Resident thread blocks of the rows kernel on the current device (one
+// wave: the warps take their units from the counter).
+// The first query for a device comes from the list's allocation, outside
+// any stream capture.
+static int nl_rows_grid(int n_blocks) {
+  static std::atomic<int> cached[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
+  int g = cached[dev].load(std::memory_order_relaxed);
+  if (g == 0) {
+    int sms = 0, per = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, nl_rows_kernel, 32 * kRowsWarps, 0);
+    g = std::max(1, sms * std::max(per, 1));
+    cached[dev].store(g, std::memory_order_relaxed);
+  }
+  return std::max(1, std::min(n_blocks, g));
+}
+
 cudaError_t nl_launch_build(const NlArgs &a, cudaStream_t st) {
-  nl_rows_kernel<<<grid_for(a.n_blocks, 1), 32 * kRowsWarps, 0, st>>>(a);
+  nl_rows_kernel<<<nl_rows_grid(a.n_blocks), 32 * kRowsWarps, 0, st>>>(a);
   nl_ref_kernel<<<grid_for(a.n_total, 256), 256, 0, st>>>(a);
   return cudaGetLastError();
 }
@@ -314,6 +330,7 @@ static int nl_alloc(pb2_batch *b) {
     if (!p) return fail(ctx, PB2_ENOMEM, "neighbour-list allocation failed");
   CUDA_TRY(ctx, cudaMemset(b->nl_ctl, 0, NL_WORDS * sizeof(int32_t)));
   CUDA_TRY(ctx, cudaMemset(b->nl_sys_moved, 0, b->n_sys * sizeof(int32_t)));
+  nl_rows_grid(b->n_blocks);  // the device's occupancy, queried outside any capture
   return PB2_OK;
 }
 
