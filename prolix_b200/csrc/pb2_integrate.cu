@@ -31,9 +31,13 @@ __device__ __forceinline__ void check_fix(const IntArgs &a, int s, long long v) 
   if (v == LLONG_MAX || v == LLONG_MIN) atomicOr(&a.status[s], (uint32_t)PB2_STATUS_FORCE_RANGE);
 }
 
+__device__ __forceinline__ float4 posq_of(double x, double y, double z, const double3 &o, double charge) {
+  return make_float4((float)(x - o.x), (float)(y - o.y), (float)(z - o.z), (float)charge);
+}
+
 __device__ __forceinline__ float4 write_posq(const IntArgs &a, int i, const SysInfo &S, double x,
                                              double y, double z) {
-  const float4 q = make_float4((float)(x - S.ox), (float)(y - S.oy), (float)(z - S.oz), (float)a.charge[i]);
+  const float4 q = posq_of(x, y, z, make_double3(S.ox, S.oy, S.oz), a.charge[i]);
   a.posq[i] = q;
   return q;
 }
@@ -61,10 +65,25 @@ __device__ __forceinline__ void block_box(const IntArgs &a, int b, int lane, boo
   }
 }
 
-__device__ __forceinline__ bool moved_past_half_skin(const IntArgs &a, int i, const SysInfo &S, float4 q) {
+// The charge and the pair list's reference position, loaded before the
+// step's stores: the FP64 stores could alias the charge and the posq store
+// the reference, and a load ordered after them adds a memory latency at the
+// end of every thread.
+struct StepExtra {
+  double charge;
+  float4 ref;  // zero without a list
+};
+__device__ __forceinline__ StepExtra step_extra(const IntArgs &a, int i) {
+  StepExtra e;
+  e.charge = a.charge[i];
+  e.ref = a.pl_ref ? a.pl_ref[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+  return e;
+}
+
+__device__ __forceinline__ bool moved_past_half_skin(const IntArgs &a, const StepExtra &e, const SysInfo &S,
+                                                     float4 q) {
   if (!a.pl_ref) return false;
-  const float4 r = a.pl_ref[i];
-  const float dx = q.x - r.x, dy = q.y - r.y, dz = q.z - r.z;
+  const float dx = q.x - e.ref.x, dy = q.y - e.ref.y, dz = q.z - e.ref.z;
   return (double)fmaf(dx, dx, fmaf(dy, dy, dz * dz)) > S.skin_half2;
 }
 
@@ -95,7 +114,7 @@ __global__ void key_splits_kernel(const IntArgs a) {
 }
 
 // One atom's plain BAOAB step; returns the float32 position it wrote.
-__device__ __forceinline__ float4 step_atom(const IntArgs &a, int i, int s, const SysInfo &S) {
+__device__ __forceinline__ float4 step_atom(const IntArgs &a, int i, int s, const SysInfo &S, const StepExtra &e) {
   {
     const int loc = i - S.off;
     const int rnd = a.user[i] - S.off;  // the atom's index in the caller's order: its noise
@@ -123,7 +142,8 @@ __device__ __forceinline__ float4 step_atom(const IntArgs &a, int i, int s, cons
     }
     a.px[i] = p[0]; a.py[i] = p[1]; a.pz[i] = p[2];
     a.x[i] = x[0]; a.y[i] = x[1]; a.z[i] = x[2];
-    const float4 q = write_posq(a, i, S, x[0], x[1], x[2]);
+    const float4 q = posq_of(x[0], x[1], x[2], make_double3(S.ox, S.oy, S.oz), e.charge);
+    a.posq[i] = q;
     if (!(isfinite(x[0]) && isfinite(x[1]) && isfinite(x[2]) && isfinite(p[0]) &&
           isfinite(p[1]) && isfinite(p[2])))
       atomicOr(&a.status[s], (uint32_t)PB2_STATUS_NONFINITE);
@@ -146,8 +166,9 @@ __global__ void __launch_bounds__(256, 4) step_kernel(const IntArgs a) {
     const bool valid = l < n;
     float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
     if (valid) {
-      q = step_atom(a, S.off + l, s, S);
-      moved |= moved_past_half_skin(a, S.off + l, S, q);
+      const StepExtra e = step_extra(a, S.off + l);
+      q = step_atom(a, S.off + l, s, S, e);
+      moved |= moved_past_half_skin(a, e, S, q);
     }
     block_box(a, b, lane, valid, q);
   }
@@ -194,7 +215,7 @@ __device__ __forceinline__ void fold_warns(const IntArgs &a, int s) {
 
 // One atom's safeguarded step; returns the float32 position it wrote.
 __device__ __forceinline__ float4 step_guarded_atom(const IntArgs &a, int i, int s, const SysInfo &S,
-                                                    bool cap_open) {
+                                                    const StepExtra &e, bool cap_open) {
   {
     const int loc = i - S.off;
     const int rnd = a.user[i] - S.off;
@@ -250,7 +271,8 @@ __device__ __forceinline__ float4 step_guarded_atom(const IntArgs &a, int i, int
     }
     a.px[i] = p[0]; a.py[i] = p[1]; a.pz[i] = p[2];
     a.x[i] = x[0]; a.y[i] = x[1]; a.z[i] = x[2];
-    const float4 q = write_posq(a, i, S, x[0], x[1], x[2]);
+    const float4 q = posq_of(x[0], x[1], x[2], make_double3(S.ox, S.oy, S.oz), e.charge);
+    a.posq[i] = q;
     if (!(isfinite(x[0]) && isfinite(x[1]) && isfinite(x[2]) && isfinite(p[0]) &&
           isfinite(p[1]) && isfinite(p[2])))
       atomicOr(&a.status[s], (uint32_t)PB2_STATUS_NONFINITE);
@@ -278,8 +300,9 @@ __global__ void __launch_bounds__(256, 4) step_guarded_kernel(const IntArgs a) {
     const bool valid = l < n;
     float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
     if (valid) {
-      q = step_guarded_atom(a, S.off + l, s, S, cap_open);
-      moved |= moved_past_half_skin(a, S.off + l, S, q);
+      const StepExtra e = step_extra(a, S.off + l);
+      q = step_guarded_atom(a, S.off + l, s, S, e, cap_open);
+      moved |= moved_past_half_skin(a, e, S, q);
     }
     block_box(a, b, lane, valid, q);
   }
