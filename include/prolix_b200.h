@@ -472,8 +472,9 @@ int pb2_get_force_blocks(const pb2_batch *batch, int32_t *blocks);
  * per chunk; PB2_FUSE_FINALIZE, the Born radii as the descreening pass's
  * tail work, one chunk per 32-atom block, each started once its system's
  * pair items have all been summed (a bounded wait on work already in
- * flight; PB2_STATUS_WAIT_TIMEOUT if it ever gives up).  Default: both; the
- * autotuner times the alternatives.  Results are bit-identical either way.
+ * flight; PB2_STATUS_WAIT_TIMEOUT if it ever gives up).  Default:
+ * PB2_FUSE_BONDED (five launches per step); the autotuner times the
+ * alternatives.  Results are bit-identical either way.
  * No reference counterpart. */
 #define PB2_FUSE_BONDED 0x1
 #define PB2_FUSE_FINALIZE 0x2

@@ -905,7 +905,7 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   if ((rc = setup_items2(b.get(), b->params.tile_segment))) return rc;
   if ((rc = setup_pair_list(b.get(), b->params.tile_segment))) return rc;
   {
-    b->fuse = PB2_FUSE_BONDED | PB2_FUSE_FINALIZE;  // the autotuner may change this
+    b->fuse = PB2_FUSE_BONDED;  // the autotuner may change this
   }
   CUDA_TRY(ctx, cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking));
   CUDA_TRY(ctx, cudaEventCreate(&b->ev[0]));
