@@ -114,7 +114,7 @@ BYTES_PER_ATOM_STEP = 184
 # DRAM traffic per launch of each pair pass on this workload
 # (dram__bytes_read.sum + dram__bytes_write.sum of one `ncu --set full`
 # capture of the three passes, default block shapes and fusion)
-TRAFFIC_BYTES = {"born": 33.58e6, "force": 71.35e6, "chain": 127.49e6}
+TRAFFIC_BYTES = {"born": 24.19e6, "force": 71.33e6, "chain": 127.59e6}
 
 
 def parse():
