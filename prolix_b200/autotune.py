@@ -12,8 +12,9 @@ candidate (CUDA events on the launching stream; the fastest wins):
   per thread; and for the force pass, two or four i-blocks per warp (four
   share each j atom's loads, at more registers), each with its shapes.
 * fusion (``_lib.FUSE_*``): the bonded terms as the chain pass's tail work,
-  and each system's Born radii finalized by the descreening warp that
-  completes it, against launches of their own.
+  and the Born radii finalized as the descreening pass's tail work (one
+  chunk per 32-atom block, started once its system's items are summed),
+  against launches of their own.
 
 The best choice depends on the size mix of the batch; it is cached in JSON
 keyed by GPU name and a workload bucket (number of systems, total atoms,
