@@ -82,6 +82,8 @@ struct PData {  // per-atom data a lane holds (its i atom, or the j atom passing
 // sqrt(log2(e)/4) so that exp(-r^2 / (4 B_i B_j)) = exp2(-r^2 iB_i iB_j).
 constexpr float kInvQuarterLog2e = 2.7725887222397811f;
 constexpr float kSqrtQuarterLog2e = 0.60056120439322491f;
+constexpr float kSixthRoot2 = 1.12246204830937298f;  // 2^(1/6)
+constexpr float kSqrtHalf = 0.70710678118654752f;
 struct Acc {
   float a0, a1, a2, a3;
 };
@@ -185,6 +187,11 @@ __device__ __forceinline__ void load_pdata(const PairArgs &a, int g, int pass, b
     P.B = b.x; P.iB = b.y * kSqrtQuarterLog2e; P.rB = b.y;
     if (pass == PASS_CHAIN) P.dedi = (float)((double)a.dedb_acc[g] * kForceInv) * b.z;
   }
+  if (pass == PASS_FORCE) {  // the force pass's scaled per-atom factors (force_pair_step)
+    P.hs *= kSixthRoot2;
+    P.se *= kSqrtHalf;
+    P.B *= 2.f;
+  }
 }
 
 // ---------------------------------------------------------------- force pass
@@ -265,16 +272,21 @@ __device__ __forceinline__ void force_pair_step(const FData2 &I, const JF2 &J, A
     // dE/dB_i = -(A2 e / 2) (B_i B_j + r^2 / 4) / B_i, whose numerator is
     // the same for both atoms: h = A2 e (B_i B_j + r^2 / 4) is summed for
     // both, and each sum is scaled by -1 / (2 B) when it is flushed
-    const float2 w = __fmul2_rn(r2, __fmul2_rn(I.iB, J.iB));  // r^2 log2(e) / (4 B_i B_j)
-    const float2 ex = exp2neg2(w);
+    // No packed constants (each would be rematerialised into a register
+    // pair): B is doubled per atom, so bb = 4 B_i B_j, and the MUFU returns
+    // ex = e / 4 from the argument r^2 log2(e) / (4 B_i B_j) + 2, formed per
+    // lane with the constant as an immediate; then f^2 = bb ex + r^2,
+    // -dE/dr / r = A2 - A2 ex and h = A2 ex (bb + r^2).
+    const float2 iBB = __fmul2_rn(I.iB, J.iB);
+    const float2 ex = exp2neg2(make_float2(__fmaf_rn(r2.x, iBB.x, 2.f), __fmaf_rn(r2.y, iBB.y, 2.f)));
     const float2 bb = __fmul2_rn(I.B, J.B);
     const float2 f2 = __ffma2_rn(bb, ex, r2);
     const float2 inv_f = rsqrt2(f2);
     float2 A2 = __fmul2_rn(__fmul2_rn(I.q2p, J.q), __fmul2_rn(__fmul2_rn(inv_f, inv_f), inv_f));
     if (CUT && K.gcut2 != 0.f) A2 = __fmul2_rn(A2, sel2(r2.x < K.gcut2, r2.y < K.gcut2, 1.f, 0.f));
     const float2 A2e = __fmul2_rn(A2, ex);
-    g = __ffma2_rn(dup2(-0.25f), A2e, A2);
-    const float2 h = __fmul2_rn(A2e, __ffma2_rn(r2, dup2(0.25f), bb));
+    g = make_float2(__fsub_rn(A2.x, A2e.x), __fsub_rn(A2.y, A2e.y));
+    const float2 h = __fmul2_rn(A2e, __fadd2_rn(bb, r2));
     ti.a3 = __fadd2_rn(ti.a3, h);
     tj.a3 = tj.a3 + h.x + h.y;
   }
@@ -297,9 +309,11 @@ __device__ __forceinline__ void force_pair_step(const FData2 &I, const JF2 &J, A
       const float2 sig = __fadd2_rn(I.hs, J.hs);
       const float2 sr2 = __fmul2_rn(__fmul2_rn(sig, sig), inv_r2);
       const float2 s6 = __fmul2_rn(__fmul2_rn(sr2, sr2), sr2);
-      float2 eps24 = __fmul2_rn(I.se, J.se);  // se = sqrt(24 eps)
-      if (EXCL) eps24 = __fmul2_rn(eps24, sc_l);
-      s = __ffma2_rn(__fmul2_rn(eps24, s6), __ffma2_rn(dup2(2.0f), s6, dup2(-1.0f)), s);
+      // sigma scaled by 2^(1/6) per atom: s6 = 2 (sigma / r)^6; se_i se_j =
+      // 12 eps: e6 = 24 eps (sigma / r)^6, times 2 (sigma / r)^6 - 1 = s6 - 1
+      float2 eps = __fmul2_rn(I.se, J.se);
+      if (EXCL) eps = __fmul2_rn(eps, sc_l);
+      s = __ffma2_rn(__fmul2_rn(eps, s6), make_float2(__fadd_rn(s6.x, -1.f), __fadd_rn(s6.y, -1.f)), s);
     }
     if (CUT && K.cut2 != 0.f) s = __fmul2_rn(s, sel2(r2.x < K.cut2, r2.y < K.cut2, 1.f, 0.f));
     g = __ffma2_rn(s, inv_r2, g);
