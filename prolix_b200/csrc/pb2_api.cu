@@ -158,6 +158,7 @@ static IntArgs int_args(pb2_batch *b, int parity, int finish_prev) {
   a.pl_ref = b->pl_on ? b->pl_ref : nullptr;
   a.pl_ctl = b->pl_on ? b->pl_ctl : nullptr;
   a.retired = b->retired;
+  a.blk_info = b->blk_info;
   return a;
 }
 
@@ -537,6 +538,7 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   std::vector<uint32_t> hkeys(4 * (size_t)n_systems, 0u);
   std::vector<int2> hent((size_t)blocks_total * kExclPerBlock, make_int2(-1, -1));
   std::vector<int32_t> hblk_sys(blocks_total);
+  std::vector<int4> hblk_info(blocks_total);
   std::vector<ExclRow> hrows;
   std::vector<TileItem> hitems;
   int blk_base = 0;
@@ -669,7 +671,10 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
       }
       S.ro_max = romax;
     }
-    for (int bk = 0; bk < S.nblk; ++bk) hblk_sys[blk_base + bk] = s;
+    for (int bk = 0; bk < S.nblk; ++bk) {
+      hblk_sys[blk_base + bk] = s;
+      hblk_info[blk_base + bk] = make_int4(s, S.off + 32 * bk, std::min(32, S.n - 32 * bk), 0);
+    }
     hkeys[2 * (size_t)s] = d.key[0];
     hkeys[2 * (size_t)s + 1] = d.key[1];
     blk_base += S.nblk;
@@ -787,6 +792,7 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
   b->bbox = D.alloc<float4>(2 * (size_t)blocks_total);
   b->sched = D.alloc<int32_t>(8);
   b->blk_sys = D.alloc<int32_t>(blocks_total);
+  b->blk_info = D.alloc<int4>(blocks_total);
   b->n_blocks = blocks_total;
   b->cut = cutoff_mode || gb_cut_mode || born_mode;
   {
@@ -862,7 +868,8 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
       (rc = upload(ctx, b->se64, hse)) || (rc = upload(ctx, b->ro64, hro)) ||
       (rc = upload(ctx, b->sr64, hsr)) || (rc = upload(ctx, b->user, b->user_host)) ||
       (rc = upload(ctx, b->devidx, b->dev_host)) ||
-      (rc = upload(ctx, b->keys, hkeys)) || (rc = upload(ctx, b->blk_sys, hblk_sys)) || (rc = upload(ctx, b->items, hitems)) ||
+      (rc = upload(ctx, b->keys, hkeys)) || (rc = upload(ctx, b->blk_sys, hblk_sys)) ||
+      (rc = upload(ctx, b->blk_info, hblk_info)) || (rc = upload(ctx, b->items, hitems)) ||
       (rc = upload(ctx, b->excl_ent, hent)) || (rc = upload(ctx, b->excl_rows, hrows)) ||
       (rc = upload(ctx, d_bidx, bidx)) || (rc = upload(ctx, d_bpar, bpar)) ||
       (rc = upload(ctx, d_aidx, aidx)) || (rc = upload(ctx, d_apar, apar)) ||
@@ -871,6 +878,7 @@ extern "C" int pb2_batch_create(pb2_ctx *ctx, int32_t n_systems, const pb2_syste
       (rc = upload(ctx, d_cgrid, cgrid)) || (rc = upload(ctx, d_cmoff, cmoff)) ||
       (rc = upload(ctx, d_eidx, eidx)) || (rc = upload(ctx, d_epar, epar)))
     return rc;
+  warm_step_launch(b->n_blocks);
   CUDA_TRY(ctx, launch_key_splits(int_args(b.get(), 0, 0), nullptr));
   CUDA_TRY(ctx, cudaMemset(b->px, 0, N * sizeof(double)));
   CUDA_TRY(ctx, cudaMemset(b->py, 0, N * sizeof(double)));

@@ -17,6 +17,9 @@
 // force kernels then run; finish_kernel applies the last half kick of a
 // chunk.  Keys live in two buffers: a step reads
 // buffer `parity` and writes the advanced key to the other.
+#include <algorithm>
+#include <atomic>
+
 #include "pb2_common.cuh"
 #include "pb2_divide.cuh"
 #include "pb2_kernels.cuh"
@@ -113,65 +116,118 @@ __global__ void key_splits_kernel(const IntArgs a) {
   }
 }
 
-// One atom's plain BAOAB step; returns the float32 position it wrote.
-__device__ __forceinline__ float4 step_atom(const IntArgs &a, int i, int s, const SysInfo &S, const StepExtra &e) {
-  {
-    const int loc = i - S.off;
-    const int rnd = a.user[i] - S.off;  // the atom's index in the caller's order: its noise
-    const double h = S.half_dt;
-    const double m = a.mass[i];
-    const double rm = __drcp_rn(m);  // p / m = div_by(p, m, rm), correctly rounded
-    const long long lfx = a.fx[i], lfy = a.fy[i], lfz = a.fz[i];
-    check_fix(a, s, lfx); check_fix(a, s, lfy); check_fix(a, s, lfz);
-    const double f[3] = {fix_to_d(lfx), fix_to_d(lfy), fix_to_d(lfz)};
-    a.fx[i] = 0; a.fy[i] = 0; a.fz[i] = 0;
-    double p[3] = {a.px[i], a.py[i], a.pz[i]};
-    double x[3] = {a.x[i], a.y[i], a.z[i]};
-    const uint4 sp = reinterpret_cast<const uint4 *>(a.splits)[(size_t)a.parity * a.n_sys + s];
-    const uint32_t knew[2] = {sp.x, sp.y}, sub[2] = {sp.z, sp.w};
-    const uint32_t count = 3u * (uint32_t)S.n;
-    const double c1 = S.c1, sg = a.sigma[i];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      if (a.finish_prev) p[c] = __dadd_rn(p[c], __dmul_rn(h, f[c]));
-      p[c] = __dadd_rn(p[c], __dmul_rn(h, f[c]));
-      x[c] = __dadd_rn(x[c], __dmul_rn(h, div_by(p[c], m, rm)));
-      const float xi = normal_from_bits(random_bits32(sub, 3u * (uint32_t)rnd + c, count, a.partitionable != 0));
-      p[c] = __dadd_rn(__dmul_rn(c1, p[c]), __dmul_rn(sg, (double)xi));
-      x[c] = __dadd_rn(x[c], __dmul_rn(h, div_by(p[c], m, rm)));
-    }
-    a.px[i] = p[0]; a.py[i] = p[1]; a.pz[i] = p[2];
-    a.x[i] = x[0]; a.y[i] = x[1]; a.z[i] = x[2];
-    const float4 q = posq_of(x[0], x[1], x[2], make_double3(S.ox, S.oy, S.oz), e.charge);
-    a.posq[i] = q;
-    if (!(isfinite(x[0]) && isfinite(x[1]) && isfinite(x[2]) && isfinite(p[0]) &&
-          isfinite(p[1]) && isfinite(p[2])))
-      atomicOr(&a.status[s], (uint32_t)PB2_STATUS_NONFINITE);
-    if (loc == 0) advance_key(a, s, knew);
-    return q;
-  }
+// The plain step: a persistent grid (one resident wave) whose warps each
+// take 32-atom blocks in turn (lane l: atom l of the block) and copy the
+// next block's inputs into shared memory (cp.async, 8 bytes per lane and
+// array) while they step the current one, so that a block's load latency
+// hides behind the previous block's arithmetic.
+struct StepIn {  // one block's inputs, [component][lane]
+  double x[3][32], p[3][32];
+  long long f[3][32];
+  double m[32], sg[32], q[32];
+  int user[32];
+};
+constexpr int kStepWarps = 4;  // warps per thread block of the plain step
+
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// Block info (system, first atom, atoms): lanes past the block's last atom
+// copy its first atom (never used).
+__device__ __forceinline__ void issue_block(const IntArgs &a, int4 info, int lane, StepIn &B) {
+  const int i = info.y + (lane < info.z ? lane : 0);
+  cp_async8(&B.x[0][lane], a.x + i); cp_async8(&B.x[1][lane], a.y + i); cp_async8(&B.x[2][lane], a.z + i);
+  cp_async8(&B.p[0][lane], a.px + i); cp_async8(&B.p[1][lane], a.py + i); cp_async8(&B.p[2][lane], a.pz + i);
+  cp_async8(&B.f[0][lane], a.fx + i); cp_async8(&B.f[1][lane], a.fy + i); cp_async8(&B.f[2][lane], a.fz + i);
+  cp_async8(&B.m[lane], a.mass + i); cp_async8(&B.sg[lane], a.sigma + i); cp_async8(&B.q[lane], a.charge + i);
+  cp_async4(&B.user[lane], a.user + i);
 }
 
-__global__ void __launch_bounds__(256, 4) step_kernel(const IntArgs a) {
-  const int lane = threadIdx.x & 31;
-  const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  const int nw = (int)((gridDim.x * blockDim.x) >> 5);
-  bool moved = false;
-  for (int b = w; b < a.n_blocks; b += nw) {
-    const int s = a.blk_sys[b];
-    const SysInfo &S = a.sys[s];
-    const int blk_base = S.blk_base, n = S.n;  // loaded beside the retired flag, not after it
-    if (a.retired[s]) continue;  // a retired system keeps its state and box
-    const int l = (b - blk_base) * 32 + lane;
-    const bool valid = l < n;
-    float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (valid) {
-      const StepExtra e = step_extra(a, S.off + l);
-      q = step_atom(a, S.off + l, s, S, e);
-      moved |= moved_past_half_skin(a, e, S, q);
-    }
-    block_box(a, b, lane, valid, q);
+// One atom's plain BAOAB step from its copied inputs; returns the float32
+// position it wrote.
+__device__ __forceinline__ float4 step_atom(const IntArgs &a, int i, int s, const SysInfo &S, const StepIn &B,
+                                            int lane) {
+  const int loc = i - S.off;
+  const int rnd = B.user[lane] - S.off;  // the atom's index in the caller's order: its noise
+  const double h = S.half_dt;
+  const double m = B.m[lane];
+  const double rm = __drcp_rn(m);  // p / m = div_by(p, m, rm), correctly rounded
+  const long long lfx = B.f[0][lane], lfy = B.f[1][lane], lfz = B.f[2][lane];
+  check_fix(a, s, lfx); check_fix(a, s, lfy); check_fix(a, s, lfz);
+  const double f[3] = {fix_to_d(lfx), fix_to_d(lfy), fix_to_d(lfz)};
+  a.fx[i] = 0; a.fy[i] = 0; a.fz[i] = 0;
+  double p[3] = {B.p[0][lane], B.p[1][lane], B.p[2][lane]};
+  double x[3] = {B.x[0][lane], B.x[1][lane], B.x[2][lane]};
+  const uint4 sp = reinterpret_cast<const uint4 *>(a.splits)[(size_t)a.parity * a.n_sys + s];
+  const uint32_t knew[2] = {sp.x, sp.y}, sub[2] = {sp.z, sp.w};
+  const uint32_t count = 3u * (uint32_t)S.n;
+  const double c1 = S.c1, sg = B.sg[lane];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    if (a.finish_prev) p[c] = __dadd_rn(p[c], __dmul_rn(h, f[c]));
+    p[c] = __dadd_rn(p[c], __dmul_rn(h, f[c]));
+    x[c] = __dadd_rn(x[c], __dmul_rn(h, div_by(p[c], m, rm)));
+    const float xi = normal_from_bits(random_bits32(sub, 3u * (uint32_t)rnd + c, count, a.partitionable != 0));
+    p[c] = __dadd_rn(__dmul_rn(c1, p[c]), __dmul_rn(sg, (double)xi));
+    x[c] = __dadd_rn(x[c], __dmul_rn(h, div_by(p[c], m, rm)));
   }
+  a.px[i] = p[0]; a.py[i] = p[1]; a.pz[i] = p[2];
+  a.x[i] = x[0]; a.y[i] = x[1]; a.z[i] = x[2];
+  const float4 q = posq_of(x[0], x[1], x[2], make_double3(S.ox, S.oy, S.oz), B.q[lane]);
+  a.posq[i] = q;
+  if (!(isfinite(x[0]) && isfinite(x[1]) && isfinite(x[2]) && isfinite(p[0]) &&
+        isfinite(p[1]) && isfinite(p[2])))
+    atomicOr(&a.status[s], (uint32_t)PB2_STATUS_NONFINITE);
+  if (loc == 0) advance_key(a, s, knew);
+  return q;
+}
+
+// Six blocks of 128 threads per SM (80 registers): at eight (64 registers)
+// the step spilled and ran slower.
+__global__ void __launch_bounds__(32 * kStepWarps, 6) step_kernel(const IntArgs a) {
+  __shared__ StepIn s_in[kStepWarps][2];
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  const int nw = (int)gridDim.x * kStepWarps;
+  int b = (int)blockIdx.x * kStepWarps + wl;
+  bool moved = false;
+  const int4 none = make_int4(0, 0, 0, 0);
+  int4 info = b < a.n_blocks ? a.blk_info[b] : none;
+  if (b < a.n_blocks) issue_block(a, info, lane, s_in[wl][0]);
+  cp_async_commit();
+  int4 info_next = b + nw < a.n_blocks ? a.blk_info[b + nw] : none;
+  for (int it = 0; b < a.n_blocks; b += nw, ++it) {
+    const int bn = b + nw;
+    if (bn < a.n_blocks) issue_block(a, info_next, lane, s_in[wl][(it + 1) & 1]);
+    cp_async_commit();
+    const int4 cur = info;
+    info = info_next;
+    info_next = bn + nw < a.n_blocks ? a.blk_info[bn + nw] : none;
+    cp_async_wait<1>();  // this block's copies (all but the newest group) have landed
+    const int s = cur.x;
+    if (!a.retired[s]) {  // a retired system keeps its state and box
+      const SysInfo &S = a.sys[s];
+      const bool valid = lane < cur.z;
+      float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (valid) {
+        StepExtra e;  // the charge comes from the copied inputs
+        e.ref = a.pl_ref ? a.pl_ref[cur.y + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
+        q = step_atom(a, cur.y + lane, s, S, s_in[wl][it & 1], lane);
+        moved |= moved_past_half_skin(a, e, S, q);
+      }
+      block_box(a, b, lane, valid, q);
+    }
+    __syncwarp();  // the buffer is read before the next block's copies refill it
+  }
+  cp_async_wait<0>();
   if (a.pl_ctl && __any_sync(kFull, moved) && lane == 0) atomicOr(&a.pl_ctl[PL_DIRTY], 1);
 }
 
@@ -429,13 +485,31 @@ static int grid_for(int n) {
 
 static bool guarded(const IntArgs &a) { return a.vlimit > 0.0 || a.max_dx > 0.0 || a.force_cap > 0.0; }
 
+// Resident thread blocks of the plain step on the current device.
+static int step_grid(int n_blocks) {
+  static std::atomic<int> cached[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
+  int g = cached[dev].load(std::memory_order_relaxed);
+  if (g == 0) {
+    int sms = 0, per = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, step_kernel, 32 * kStepWarps, 0);
+    g = std::max(1, sms * std::max(per, 1));
+    cached[dev].store(g, std::memory_order_relaxed);
+  }
+  return std::max(1, std::min((n_blocks + kStepWarps - 1) / kStepWarps, g));
+}
+
+void warm_step_launch(int n_blocks) { step_grid(n_blocks); }
+
 cudaError_t launch_step(const IntArgs &a, cudaStream_t st) {
   const int grid = (a.n_blocks + 7) / 8;  // 8 warps, one 32-atom block each
   if (grid <= 0) return cudaSuccess;
   if (guarded(a))
     step_guarded_kernel<<<grid, 256, 0, st>>>(a);
   else
-    step_kernel<<<grid, 256, 0, st>>>(a);
+    step_kernel<<<step_grid(a.n_blocks), 32 * kStepWarps, 0, st>>>(a);
   return cudaGetLastError();
 }
 cudaError_t launch_finish(const IntArgs &a, cudaStream_t st) {

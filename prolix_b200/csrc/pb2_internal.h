@@ -116,6 +116,7 @@ struct pb2_batch {
   int32_t *sys_items = nullptr;  // items2 per system (the descreening pass's completion count)
   std::vector<int32_t> sys_items_host;
   int32_t *sys_done = nullptr;   // items of each system completed in the current pass
+  int4 *blk_info = nullptr;      // per 32-atom block: system, first atom, atoms
   int32_t *sys_fin = nullptr;    // finalize chunks of each system completed in the current pass
   int2 *excl_ent = nullptr;
   ExclRow *excl_rows = nullptr;

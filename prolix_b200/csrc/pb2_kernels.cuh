@@ -190,6 +190,7 @@ struct IntArgs {
   const float4 *pl_ref;
   int32_t *pl_ctl;
   const int8_t *retired;  // per system: 1 = retired, never stepped again
+  const int4 *blk_info;   // per 32-atom block: system, first atom, atoms (the plain step)
 };
 // warn_counts columns (prolix typing.py:559-563) and their warn_flags bits
 enum { kWarnVlimit = 0, kWarnForceCap = 1, kWarnConstr = 2, kWarnDxCap = 3, kWarnTypes = 4 };
@@ -264,6 +265,8 @@ cudaError_t launch_retire(int32_t sys, int8_t *retired, const TileItem *all, int
                           int32_t *count, int32_t *pl_ctl, cudaStream_t st);
 cudaError_t launch_bonded(const BondedArgs &a, int grid_cap, cudaStream_t st);
 cudaError_t launch_step(const IntArgs &a, cudaStream_t st);
+// The plain step kernel's grid for this device, queried once outside any capture.
+void warm_step_launch(int n_blocks);
 // Refresh splits[parity] from keys[parity] (after keys came from the host).
 cudaError_t launch_key_splits(const IntArgs &a, cudaStream_t st);
 cudaError_t launch_finish(const IntArgs &a, cudaStream_t st);
