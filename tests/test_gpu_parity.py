@@ -136,6 +136,30 @@ def test_langevin_zero_force_is_bit_exact():
   assert st["step"][0] == 7
 
 
+def test_langevin_zero_force_ragged_batch_is_bit_exact():
+  # The plain step over a ragged batch of block-boundary sizes (one atom,
+  # partial and whole 32-atom blocks) and larger systems, about 11,000
+  # blocks in all: several per resident warp, each stepped while the warp
+  # copies in its next one, which often belongs to another system.  Every
+  # system equals the FP64 oracle bit for bit.
+  sizes = (1, 31, 32, 33, 97, 2, 64, 65) + tuple(1500 + 23 * k for k in range(120))
+  keys = [prng.prng_key(500 + k) for k in range(len(sizes))]
+  systems = [dict(synth.make_chain(n, 600 + n, compact=True), key=k) for n, k in zip(sizes, keys)]
+  dt, kT, gamma = engine.akma_dt(1.0), 300 * engine.KB_KCAL, engine.akma_gamma(1.0)
+  with engine.Batch(systems, terms=0, dt=dt, kT=kT, gamma=gamma) as b:
+    b.langevin_init()
+    b.langevin_run(5)
+    st = b.get_state()
+  zero = lambda r: np.zeros_like(r)
+  for k, s in enumerate(systems):
+    lo, hi = b.offsets[k], b.offsets[k + 1]
+    o = ointeg.init(zero, keys[k], s["positions"], s["masses"], kT)
+    o = ointeg.run(o, zero, 5, dt, kT, gamma)
+    np.testing.assert_array_equal(st["momentum"][lo:hi], o.momentum)
+    np.testing.assert_array_equal(st["position"][lo:hi], o.position)
+    np.testing.assert_array_equal(st["key"][k], o.key)
+
+
 def test_new_langevin_parameters_mid_run_are_bit_exact():
   # F = 0: 3 steps, then new dt, kT and gamma for 4 more, equal the oracle's
   # steps with those arguments bit for bit (noise and its amplitude)
