@@ -127,6 +127,8 @@ def parse():
   ap.add_argument("--no-plain", action="store_true")
   ap.add_argument("--no-cpu", action="store_true")
   ap.add_argument("--no-e2e", action="store_true")
+  ap.add_argument("--e2e-tune", type=int, default=1,
+                  help="end-to-end leg: 1 runs the autotuner on the first group and applies its choice to all")
   ap.add_argument("--e2e-groups", type=lambda v: [int(x) for x in v.split(",")], default=[12],
                   help="streams the end-to-end leg splits the systems over (comma list; the first "
                        "is the reported value)")
@@ -609,9 +611,17 @@ def main():
     e2e_steps = 10
     nbytes = 3 * 3 * 8 * n_atoms
     by_groups = {}
+    group_choice = None
     for g in args.e2e_groups:
       with streamed.StreamedEnsemble(systems, groups=g, device=local) as ens:
         ens.langevin_init()
+        if args.e2e_tune and g == args.e2e_groups[0]:
+          # the groups are alike in size: the autotuner's choice for the first
+          # serves them all (its timing steps advance that group's trajectory,
+          # which the timed steps below then continue)
+          group_choice = autotune.tune(ens.batches[0], candidates=(8, 16, 32), steps=3, use_cache=False)
+          for bt in ens.batches:
+            autotune.apply(bt, group_choice)
         host = ens.get_state()
         ens.synchronize()
         for it in range(2 + e2e_steps):
@@ -640,6 +650,8 @@ def main():
     e2e = {"value": by_groups[head], "unit": UNIT,
            "h2d_bytes_per_step": int(nbytes), "d2h_bytes_per_step": int(nbytes),
            "steps": e2e_steps, "host_buffers": "page-locked", "groups": int(head),
+           "group_tuning": None if group_choice is None else
+           {k: group_choice.get(k) for k in ("segment", "shapes", "force_blocks", "fusion")},
            "by_groups": by_groups,
            "pipelined_no_host_wait": pipelined,
            "path": "pb2_langevin_run_host(1 step, x, p, F) per group of systems, one stream per group; "
