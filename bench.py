@@ -615,13 +615,15 @@ def main():
     for g in args.e2e_groups:
       with streamed.StreamedEnsemble(systems, groups=g, device=local) as ens:
         ens.langevin_init()
-        if args.e2e_tune and g == args.e2e_groups[0]:
+        if args.e2e_tune:
           # the groups are alike in size: the autotuner's choice for the first
           # serves them all (its timing steps advance that group's trajectory,
           # which the timed steps below then continue)
-          group_choice = autotune.tune(ens.batches[0], candidates=(8, 16, 32), steps=3, use_cache=False)
+          choice = autotune.tune(ens.batches[0], candidates=(8, 16, 32), steps=3, use_cache=False)
           for bt in ens.batches:
-            autotune.apply(bt, group_choice)
+            autotune.apply(bt, choice)
+          if g == args.e2e_groups[0]:
+            group_choice = choice
         host = ens.get_state()
         ens.synchronize()
         for it in range(2 + e2e_steps):
