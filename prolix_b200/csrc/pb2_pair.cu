@@ -691,10 +691,6 @@ __global__ void __launch_bounds__(THREADS, MINB)
   // the j-block of the current tile, one JTile per warp (4 KB)
   __shared__ JTile s_jt[kWarps];
   JTile &jt = s_jt[threadIdx.x >> 5];
-#ifdef PB2_ISUM_SMEM
-  __shared__ long long s_isum[PASS == PASS_FORCE ? kWarps : 1][8][32];
-  long long *si = &s_isum[PASS == PASS_FORCE ? (threadIdx.x >> 5) : 0][0][lane];
-#endif
   CfQueue Q;
   Q.c = {a.posq, a.par, a.born, a.dedb_acc, a.born_acc, a.fx, a.fy, a.fz};
   Q.q = s_cfq[PASS == PASS_FORCE ? 0 : (threadIdx.x >> 5)];
@@ -768,10 +764,6 @@ __global__ void __launch_bounds__(THREADS, MINB)
       else if (has1 && lane < 2 * kExclPerBlock) ent = a.excl_ent[gib1 * kExclPerBlock + lane - kExclPerBlock];
     }
 
-#ifndef PB2_HOIST_IF
-#define PB2_HOIST_IF 1
-#endif
-#if PB2_HOIST_IF
     // the force pass's packed i-side data, once per item
     FData2 IF{};
     if constexpr (PASS == PASS_FORCE)
@@ -780,12 +772,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
             make_float2(I0.B, I1.B), make_float2(I0.iB, I1.iB),
             make_float2(2.f * K.pref * I0.q, 2.f * K.pref * I1.q),
             make_float2(K.kcoul * I0.q, K.kcoul * I1.q)};
-#endif
     long long p0 = 0, p1 = 0, p2 = 0, p3 = 0, q0 = 0, q1 = 0, q2 = 0, q3 = 0;  // i-side sums
-#ifdef PB2_ISUM_SMEM
-    if constexpr (PASS == PASS_FORCE)
-      for (int k = 0; k < 8; ++k) si[32 * k] = 0;
-#endif
     for (int tt = item.jb0; tt < item.jb1; ++tt) {
       const int jb = plm ? a.pl_jlist[tt] : tt;
       const int gjb = S.blk_base + jb;
@@ -834,13 +821,6 @@ __global__ void __launch_bounds__(THREADS, MINB)
           const ExclRow r = a.excl_rows[roff + lane];
           E1 = rotr32(r.excl, lane); S1 = rotr32(r.s14, lane);
         }
-#if !PB2_HOIST_IF
-        const FData2 IF = {make_float2(I0.x, I1.x), make_float2(I0.y, I1.y), make_float2(I0.z, I1.z),
-                           make_float2(I0.hs, I1.hs), make_float2(I0.se, I1.se),
-                           make_float2(I0.B, I1.B), make_float2(I0.iB, I1.iB),
-                           make_float2(2.f * K.pref * I0.q, 2.f * K.pref * I1.q),
-                           make_float2(K.kcoul * I0.q, K.kcoul * I1.q)};
-#endif
         Acc2F tf = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
         if (hit) run_force_tile2<CUT, false, true>(IF, jt, tf, tj, V0, V1, E0, E1, S0, S1, K);
         else if (!full) run_force_tile2<CUT, false, false>(IF, jt, tf, tj, V0, V1, E0, E1, S0, S1, K);
@@ -884,15 +864,6 @@ __global__ void __launch_bounds__(THREADS, MINB)
             atomic_add_fix(&a.dedb_acc[jg], to_fix_f(tj.a3 * (-0.5f * J.rB), bscale));
         }
       }
-#ifdef PB2_ISUM_SMEM
-      if constexpr (PASS == PASS_FORCE) {
-        si[0] += to_fix_f(t0.a0, bscale); si[32] += to_fix_f(t0.a1, bscale);
-        si[64] += to_fix_f(t0.a2, bscale); si[96] += to_fix_f(t0.a3 * (-0.5f * I0.rB), bscale);
-        si[128] += to_fix_f(t1.a0, bscale); si[160] += to_fix_f(t1.a1, bscale);
-        si[192] += to_fix_f(t1.a2, bscale); si[224] += to_fix_f(t1.a3 * (-0.5f * I1.rB), bscale);
-        continue;
-      }
-#endif
       p0 += to_fix_f(t0.a0, bscale);
       q0 += to_fix_f(t1.a0, bscale);
       if (PASS != PASS_BORN) {
@@ -904,12 +875,6 @@ __global__ void __launch_bounds__(THREADS, MINB)
         q3 += to_fix_f(t1.a3 * (-0.5f * I1.rB), bscale);
       }
     }
-#ifdef PB2_ISUM_SMEM
-    if constexpr (PASS == PASS_FORCE) {
-      p0 = si[0]; p1 = si[32]; p2 = si[64]; p3 = si[96];
-      q0 = si[128]; q1 = si[160]; q2 = si[192]; q3 = si[224];
-    }
-#endif
 
     if (PASS == PASS_BORN) {
       if (iv0 && p0 != 0) atomic_add_fix(&a.born_acc[ig0], p0);
@@ -1167,11 +1132,7 @@ struct Shape {
 };
 constexpr Shape kShapes[3][kShapesPerPass] = {
     {{256, 3}, {256, 2}, {128, 6}},   // descreening
-#ifdef PB2_EXP_FORCE_128x3
-    {{256, 2}, {128, 4}, {128, 3}},   // force
-#else
     {{256, 2}, {128, 4}, {128, 5}},   // force
-#endif
     {{256, 2}, {128, 4}, {128, 5}}};  // chain rule
 
 template <int PASS, bool CUT, bool ALL, int SH>
