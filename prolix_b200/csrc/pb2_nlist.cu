@@ -74,16 +74,20 @@ __global__ void nl_disp_kernel(const NlArgs a) {
 // hits are compacted by a ballot and stored as one contiguous run
 // (coalesced), so rows come out in j order.  The warps of one resident wave
 // take units from a counter until none is left.
-constexpr int kRowsPerWarp = 4;
+// A unit is 2 NH rows: four (NH = 2) in general, two (NH = 1) when a
+// build has so few blocks that four-row units would leave most resident
+// warps idle (each unit's blocks are walked in sequence, so more, shorter
+// units finish sooner there).
 
 // One j-block's 32 candidates (lane = candidate lj; nq = minus its
-// position, duplicated) against the warp's rows l0 .. l0 + 3, whose
+// position, duplicated) against the warp's rows l0 .. l0 + 2 NH - 1, whose
 // positions are held in pairs (rows 0, 1 and 2, 3) so that the distances
 // run as packed f32x2 arithmetic (per component the same roundings as the
 // scalar fmaf chain).  Each row's hits are compacted by a ballot and stored
 // as one contiguous run.  DIAG: the block holds the rows' own atoms.
-struct NlRows4 {
-  float2 x[2], y[2], z[2];
+template <int NH>
+struct NlRows {
+  float2 x[NH], y[NH], z[NH];
 };
 
 // row: the row's first slot; cap: its capacity.
@@ -94,12 +98,12 @@ __device__ __forceinline__ void nl_hit_row(bool hit, int lj, int *row, int cap, 
   cnt += __popc(m);
 }
 
-template <bool DIAG>
-__device__ __forceinline__ void nl_rows_block(const NlRows4 &P, float4 q, int lj, int l0, float reach2,
+template <bool DIAG, int NH>
+__device__ __forceinline__ void nl_rows_block(const NlRows<NH> &P, float4 q, int lj, int l0, float reach2,
                                               int *const *row, int cap, unsigned below, int *cnt) {
   const float2 nqx = make_float2(-q.x, -q.x), nqy = make_float2(-q.y, -q.y), nqz = make_float2(-q.z, -q.z);
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
+  for (int h = 0; h < NH; ++h) {
     const float2 ex = __fadd2_rn(P.x[h], nqx), ey = __fadd2_rn(P.y[h], nqy), ez = __fadd2_rn(P.z[h], nqz);
     const float2 d2 = __ffma2_rn(ex, ex, __ffma2_rn(ey, ey, __fmul2_rn(ez, ez)));
     const int r0 = 2 * h, r1 = 2 * h + 1;
@@ -113,11 +117,13 @@ __device__ __forceinline__ void nl_rows_block(const NlRows4 &P, float4 q, int lj
   }
 }
 
-// The rows of one warp unit: four rows of a 32-atom block against every
+// The rows of one warp unit: 2 NH rows of a 32-atom block against every
 // block of its system, culled by box (lane = block, 32 at a time), then the
 // near blocks' atoms, lane = candidate.
+template <int NH>
 __device__ __forceinline__ void nl_rows_unit(const NlArgs &a, int ib, int w, int lane, unsigned below, int cap,
                                              float reach2) {
+  constexpr int kRowsPerWarp = 2 * NH;
   const int s = a.blk_sys[ib];
   // the system's fields in registers: the row stores could alias them
   const int off = a.sys[s].off, n = a.sys[s].n, nblk = a.sys[s].nblk, blk_base = a.sys[s].blk_base;
@@ -125,10 +131,9 @@ __device__ __forceinline__ void nl_rows_unit(const NlArgs &a, int ib, int w, int
   if (l0 >= n) return;  // past the system's last atom: no rows
   int cnt[kRowsPerWarp];
   int *row[kRowsPerWarp];  // each row's first slot
-  static_assert(kRowsPerWarp == 4, "rows are paired");
-  NlRows4 P;
+  NlRows<NH> P;
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
+  for (int h = 0; h < NH; ++h) {
     float4 u = a.posq[off + min(l0 + 2 * h, n - 1)], v = a.posq[off + min(l0 + 2 * h + 1, n - 1)];
     if (l0 + 2 * h >= n) u.x = -1e30f;  // no row: never within reach of an atom
     if (l0 + 2 * h + 1 >= n) v.x = -1e30f;
@@ -141,9 +146,9 @@ __device__ __forceinline__ void nl_rows_unit(const NlArgs &a, int ib, int w, int
   for (int r = 0; r < kRowsPerWarp; ++r) row[r] = a.rows + (size_t)(off + min(l0 + r, n - 1)) * cap;
   const int own = ib - blk_base;
   for (int c0 = 0; c0 < nblk; c0 += 32) {
-    // the blocks within reach of one of the unit's four atoms (the margin
-    // keeps the test conservative under rounding).  A block whose every
-    // atom is within reach of all four rows (its box's farthest corner is,
+    // the blocks within reach of one of the unit's atoms (the margin keeps
+    // the test conservative under rounding).  A block whose every atom is
+    // within reach of all the unit's rows (its box's farthest corner is,
     // by the same rounded operations as the atom test, so each atom's
     // computed distance is no larger) is stored without its distances: the
     // same slots in the same order.
@@ -183,8 +188,8 @@ __device__ __forceinline__ void nl_rows_unit(const NlArgs &a, int ib, int w, int
       }
       float4 q = a.posq[off + min(lj, n - 1)];
       if (lj >= n) q.x = 1e30f;  // no atom: never within reach of a row
-      if (jb == own) nl_rows_block<true>(P, q, lj, l0, reach2, row, cap, below, cnt);  // skips i = j
-      else nl_rows_block<false>(P, q, lj, l0, reach2, row, cap, below, cnt);
+      if (jb == own) nl_rows_block<true, NH>(P, q, lj, l0, reach2, row, cap, below, cnt);  // skips i = j
+      else nl_rows_block<false, NH>(P, q, lj, l0, reach2, row, cap, below, cnt);
     }
   }
 #pragma unroll
@@ -211,11 +216,13 @@ __device__ __forceinline__ void nl_rows_unit(const NlArgs &a, int ib, int w, int
   }
 }
 
-// Each warp takes units (a 32-atom block's four rows) from a counter in
+// Each warp takes units (2 NH rows of a 32-atom block) from a counter in
 // ctl[NL_NEXT] until none is left, so that the blocks' uneven costs (a
 // globule's core against its surface) spread over every SM; the reference
 // kernel resets the counter after the build.
+template <int NH>
 __global__ void __launch_bounds__(32 * kRowsWarps) nl_rows_kernel(const NlArgs a) {
+  constexpr int kRowsPerWarp = 2 * NH;
   if (!nl_dirty(a)) return;
   const int lane = threadIdx.x & 31;
   const unsigned below = (1u << lane) - 1u;
@@ -227,7 +234,7 @@ __global__ void __launch_bounds__(32 * kRowsWarps) nl_rows_kernel(const NlArgs a
     if (lane == 0) u = atomicAdd(&a.ctl[NL_NEXT], 1);
     u = __shfl_sync(kFull, u, 0);
     if (u >= n_units) break;
-    nl_rows_unit(a, u / (32 / kRowsPerWarp), u % (32 / kRowsPerWarp), lane, below, cap, reach2);
+    nl_rows_unit<NH>(a, u / (32 / kRowsPerWarp), u % (32 / kRowsPerWarp), lane, below, cap, reach2);
   }
 }
 
@@ -253,11 +260,12 @@ __global__ void nl_ref_kernel(const NlArgs a) {
 
 static int grid_for(int n, int per) { return std::max(1, std::min((n + per - 1) / per, 65535)); }
 
-// Resident thread blocks of the rows kernel on the current device (one
-// wave: the warps take their units from the counter).
+// Resident thread blocks of the rows kernel (2 NH rows per unit) on the
+// current device: one wave, whose warps take their units from the counter.
 // The first query for a device comes from the list's allocation, outside
 // any stream capture.
-static int nl_rows_grid(int n_blocks) {
+template <int NH>
+static int nl_rows_resident() {
   static std::atomic<int> cached[64];
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
@@ -265,15 +273,28 @@ static int nl_rows_grid(int n_blocks) {
   if (g == 0) {
     int sms = 0, per = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, nl_rows_kernel, 32 * kRowsWarps, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, nl_rows_kernel<NH>, 32 * kRowsWarps, 0);
     g = std::max(1, sms * std::max(per, 1));
     cached[dev].store(g, std::memory_order_relaxed);
   }
-  return std::max(1, std::min(n_blocks, g));
+  return g;
+}
+
+static void nl_rows_warm() {
+  nl_rows_resident<1>();
+  nl_rows_resident<2>();
 }
 
 cudaError_t nl_launch_build(const NlArgs &a, cudaStream_t st) {
-  nl_rows_kernel<<<nl_rows_grid(a.n_blocks), 32 * kRowsWarps, 0, st>>>(a);
+  // two-row units when even they fit in one wave of resident warps
+  const long long units2 = 16LL * a.n_blocks;
+  if (units2 <= (long long)nl_rows_resident<1>() * kRowsWarps) {
+    const int grid = (int)std::max(1LL, std::min((units2 + kRowsWarps - 1) / kRowsWarps,
+                                                  (long long)nl_rows_resident<1>()));
+    nl_rows_kernel<1><<<grid, 32 * kRowsWarps, 0, st>>>(a);
+  } else {
+    nl_rows_kernel<2><<<std::max(1, std::min(a.n_blocks, nl_rows_resident<2>())), 32 * kRowsWarps, 0, st>>>(a);
+  }
   nl_ref_kernel<<<grid_for(a.n_total, 256), 256, 0, st>>>(a);
   return cudaGetLastError();
 }
@@ -330,7 +351,7 @@ static int nl_alloc(pb2_batch *b) {
     if (!p) return fail(ctx, PB2_ENOMEM, "neighbour-list allocation failed");
   CUDA_TRY(ctx, cudaMemset(b->nl_ctl, 0, NL_WORDS * sizeof(int32_t)));
   CUDA_TRY(ctx, cudaMemset(b->nl_sys_moved, 0, b->n_sys * sizeof(int32_t)));
-  nl_rows_grid(b->n_blocks);  // the device's occupancy, queried outside any capture
+  nl_rows_warm();  // the device's occupancy, queried outside any capture
   return PB2_OK;
 }
 

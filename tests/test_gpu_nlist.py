@@ -67,6 +67,17 @@ def test_long_reach_rows_match_brute_force():
     off += n
 
 
+def test_large_build_matches_brute_force():
+  # 469 blocks: more two-row units than one wave of resident warps holds on
+  # a B200, so the build takes four-row units (the smaller builds of the
+  # other tests take two-row ones)
+  s = synth.make_chain(15000, 77, compact=True)
+  with engine.Batch([s], cutoff=9.0, skin=2.0) as b:
+    b.nl_build()
+    rows = b.nl_get()
+  _check_rows(rows, [s], 11.0)
+
+
 def test_capacity_not_a_multiple_of_four():
   # an odd fixed capacity: the sentinels go one slot at a time
   s = synth.make_chain(500, 12, compact=True)
